@@ -1,0 +1,237 @@
+"""ctypes binding of the CPU oracle (avbd_oracle.cpp). TEST INFRASTRUCTURE: imported only by
+tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg, never by the product."""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+from build import build  # noqa: E402
+
+_lib = None
+
+BODY_REC = 43
+FORCE_REC = 47
+K_MANIFOLD, K_JOINT, K_SPRING, K_IGNORE = 0, 1, 2, 3
+NO_COLOR = 255
+PENDING = 256
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, '_build', 'liboracle.so')
+        if not os.path.exists(path):
+            path = build()
+        L = ctypes.CDLL(path)
+        P, D, I, U = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_uint
+        L.orc_create.restype = P
+        L.orc_create.argtypes = [I]
+        L.orc_destroy.argtypes = [P]
+        L.orc_set_params.argtypes = [P, D, U]
+        L.orc_add_body.argtypes = [P, D]
+        L.orc_body_count.argtypes = [P]
+        L.orc_get_body.argtypes = [P, I, D]
+        L.orc_set_body.argtypes = [P, I, D]
+        L.orc_add_joint.argtypes = [P, I, I, D, D, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_add_spring.argtypes = [P, I, I, D, D, ctypes.c_double, ctypes.c_double]
+        L.orc_add_ignore.argtypes = [P, I, I]
+        L.orc_force_count.argtypes = [P]
+        L.orc_get_force.argtypes = [P, I, D]
+        L.orc_set_joint.argtypes = [P, I, D]
+        L.orc_manifold_count.argtypes = [P]
+        L.orc_contact_count.argtypes = [P]
+        L.orc_get_manifolds.argtypes = [P, D, D]
+        L.orc_set_contact_penalty.argtypes = [P, ctypes.c_double]
+        L.orc_step.argtypes = [P]
+        L.orc_step_gpu.argtypes = [P, ctypes.POINTER(U), ctypes.POINTER(I)]
+        L.orc_pairs.argtypes = [P, ctypes.POINTER(U), I]
+        L.orc_pairs.restype = I
+        L.orc_narrowphase.argtypes = [P, I, I, I, D, D]
+        L.orc_narrowphase.restype = I
+        L.orc_color_graph.argtypes = [I, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(U), I, I, ctypes.POINTER(I)]
+        L.orc_hash32.argtypes = [U]
+        L.orc_hash32.restype = U
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def body_record(b) -> np.ndarray:
+    r = np.zeros(BODY_REC)
+    r[0:3] = b.pos
+    r[3:7] = b.rot
+    r[7:10] = b.vel
+    r[10:13] = b.ang_vel
+    r[13:16] = b.prev_vel
+    r[16:19] = b.size
+    r[19] = b.mass
+    r[20:23] = b.moment
+    r[23] = b.friction
+    r[24] = b.radius
+    r[25] = b.shape
+    r[26:29] = b.initial_pos
+    r[29:33] = b.initial_rot
+    r[33:36] = b.inertial_pos
+    r[36:40] = b.inertial_rot
+    r[40] = b.groups
+    r[41] = b.mask
+    r[42] = NO_COLOR
+    return r
+
+
+class Oracle:
+    """One CPU solver instance (fp32=False: double, the reference's precision)."""
+
+    def __init__(self, scene=None, fp32: bool = False, flags: int = 0):
+        self.L = lib()
+        self.h = self.L.orc_create(1 if fp32 else 0)
+        self.fp32 = fp32
+        self.force_of = []  # scene force index -> oracle force index
+        if scene is not None:
+            self.load(scene, flags)
+
+    def __del__(self):
+        if getattr(self, 'h', None):
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def set_params(self, p, flags: int = 0):
+        arr = np.array([p.dt, p.gravity, p.iterations, p.alpha, p.beta_lin, p.beta_ang, p.gamma, p.contact_margin], dtype=np.float64)
+        self.L.orc_set_params(self.h, _dp(arr), flags)
+
+    def load(self, scene, flags: int = 0):
+        self.set_params(scene.params, flags)
+        for b in scene.bodies:
+            self.L.orc_add_body(self.h, _dp(body_record(b)))
+        for f in scene.forces:
+            rA = np.array(f.rA, dtype=np.float64)
+            rB = np.array(f.rB, dtype=np.float64)
+            if f.kind == 'joint':
+                k = self.L.orc_add_joint(self.h, f.a, f.b, _dp(rA), _dp(rB), f.stiffness_lin, f.stiffness_ang, f.fracture)
+                rec = self.force(k)
+                rec[24] = 1.0 if f.fracture_linear else 0.0
+                rec[27] = f.yield_force
+                rec[28] = f.break_bend
+                if f.rest is not None:
+                    rec[29:33] = f.rest
+                    rec[33] = 1
+                if f.rest_start is not None:
+                    rec[34:38] = f.rest_start
+                    rec[38] = 1
+                rec[3:6] = f.penalty_lin
+                rec[6:9] = f.penalty_ang
+                self.set_joint(k, rec)
+            elif f.kind == 'spring':
+                k = self.L.orc_add_spring(self.h, f.a, f.b, _dp(rA), _dp(rB), f.spring_stiffness, f.spring_rest)
+            else:
+                k = self.L.orc_add_ignore(self.h, f.a, f.b)
+            self.force_of.append(k)
+
+    # --- state ---
+    @property
+    def body_count(self):
+        return self.L.orc_body_count(self.h)
+
+    def body(self, i) -> np.ndarray:
+        r = np.zeros(BODY_REC)
+        self.L.orc_get_body(self.h, i, _dp(r))
+        return r
+
+    def bodies(self) -> np.ndarray:
+        return np.stack([self.body(i) for i in range(self.body_count)]) if self.body_count else np.zeros((0, BODY_REC))
+
+    def set_body(self, i, rec):
+        rec = np.ascontiguousarray(rec, dtype=np.float64)
+        self.L.orc_set_body(self.h, i, _dp(rec))
+
+    @property
+    def force_count(self):
+        return self.L.orc_force_count(self.h)
+
+    def force(self, i) -> np.ndarray:
+        r = np.zeros(FORCE_REC)
+        self.L.orc_get_force(self.h, i, _dp(r))
+        return r
+
+    def set_joint(self, i, rec):
+        rec = np.ascontiguousarray(rec, dtype=np.float64)
+        self.L.orc_set_joint(self.h, i, _dp(rec))
+
+    def manifolds(self):
+        nm = self.L.orc_manifold_count(self.h)
+        nc = self.L.orc_contact_count(self.h)
+        m = np.zeros((max(nm, 1), 8))
+        c = np.zeros((max(nc, 1), 17))
+        self.L.orc_get_manifolds(self.h, _dp(m), _dp(c))
+        return m[:nm], c[:nc]
+
+    def set_contact_penalty(self, pen):
+        self.L.orc_set_contact_penalty(self.h, pen)
+
+    # --- stepping ---
+    def step(self, n: int = 1):
+        for _ in range(n):
+            self.L.orc_step(self.h)
+
+    def step_gpu(self, fixed_colors=None):
+        stats = (ctypes.c_int * 3)()
+        if fixed_colors is None:
+            self.L.orc_step_gpu(self.h, None, stats)
+        else:
+            fc = np.ascontiguousarray(fixed_colors, dtype=np.uint32)
+            self.L.orc_step_gpu(self.h, fc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), stats)
+        return {'colors': stats[0], 'clashes': stats[1], 'rounds': stats[2]}
+
+    def pairs(self) -> np.ndarray:
+        cap = 1 << 16
+        while True:
+            out = np.zeros(2 * cap, dtype=np.uint32)
+            n = self.L.orc_pairs(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), cap)
+            if n <= cap:
+                return out[: 2 * n].reshape(-1, 2)
+            cap = n
+
+    def narrowphase(self, a, b, face_bias=False):
+        out = np.zeros(8 * 7)
+        normal = np.zeros(3)
+        n = self.L.orc_narrowphase(self.h, a, b, 1 if face_bias else 0, _dp(out), _dp(normal))
+        rows = out[: 7 * n].reshape(-1, 7)
+        return [(int(r[0]), r[1:4].copy(), r[4:7].copy()) for r in rows], normal
+
+    def colors(self) -> np.ndarray:
+        return self.bodies()[:, 42].astype(np.uint32)
+
+
+def sequential_colors(scene) -> np.ndarray:
+    """One colour per dynamic body, newest first: the reference's Gauss-Seidel order
+    (gpu/solver.ts:1365-1372)."""
+    colors = np.full(len(scene.bodies), NO_COLOR, dtype=np.uint32)
+    nxt = 0
+    for i in range(len(scene.bodies) - 1, -1, -1):
+        if scene.bodies[i].mass > 0:
+            colors[i] = nxt
+            nxt += 1
+    assert nxt <= 64, f'{nxt} dynamic bodies, at most 64'
+    return colors
+
+
+def color_graph(n, dynamic, start, nbr, state, cap=64, max_rounds=64):
+    L = lib()
+    dyn = np.ascontiguousarray(dynamic, dtype=np.uint8)
+    st = np.ascontiguousarray(start, dtype=np.int32)
+    nb = np.ascontiguousarray(nbr, dtype=np.int32) if len(nbr) else np.zeros(1, dtype=np.int32)
+    s = np.ascontiguousarray(state, dtype=np.uint32).copy()
+    stats = (ctypes.c_int * 3)()
+    L.orc_color_graph(n, dyn.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                      nb.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), s.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), cap, max_rounds, stats)
+    return s, {'colors': stats[0], 'clashes': stats[1], 'rounds': stats[2]}
