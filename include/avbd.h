@@ -1,0 +1,208 @@
+/*
+ * avbd.h: C ABI of the B200 (sm_100a) backend for three-avbd's 3D Augmented Vertex Block Descent step.
+ *
+ * This is the drop-in boundary for the reference's `GpuSolver3D` (src/avbd3d/gpu/solver.ts:598),
+ * the object `World` (src/lib/world.ts:729-731) delegates every physics call to. A host binding
+ * (N-API/FFI from TypeScript, ctypes from Python) implements the GpuSolver3D member list on top of
+ * these functions; each declaration below names the reference member it replaces.
+ *
+ * Conventions:
+ *   - Every function returns an int status: AVBD_OK (0) or a negative AVBD_ERR_* code, and leaves
+ *     the world unchanged on invalid input (the reference throws before any state change,
+ *     gpu/solver.ts appendJoints). avbd_last_error() gives the message.
+ *   - Host buffers are caller-owned; device buffers are world-owned. One CUDA stream per world:
+ *     a world is not thread-safe, distinct worlds are.
+ *   - Records are the reference's GPU records, bit-compatible: a body is 40 floats
+ *     (src/avbd3d/gpu/layout.ts:8-59), a joint 40 floats plus a 4-int info
+ *     (layout.ts:77-110, 232-243), a manifold 8 words and a contact 16 words (layout.ts:118-127).
+ *   - Overflow of pair/contact storage is a counter bit, not an error (layout.ts C_OVERFLOW);
+ *     storage grows at the next step, as the reference's adapt() does (gpu/solver.ts:2362-2377).
+ */
+#ifndef AVBD_H
+#define AVBD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AVBD_ABI_VERSION 1
+
+enum {
+  AVBD_OK = 0,
+  AVBD_ERR_INVALID = -1,   /* bad argument (index, count, NaN, size) */
+  AVBD_ERR_CAPACITY = -2,  /* past a fixed capacity (bodies, joints) */
+  AVBD_ERR_CUDA = -3,      /* a CUDA call failed; the message says which */
+  AVBD_ERR_TIMEOUT = -4,   /* a bounded device wait gave up (the step's results are not valid) */
+  AVBD_ERR_NO_DEVICE = -5, /* no CUDA device, or not sm_100 */
+};
+
+/* Shape codes in avbd_body.shape (layout.ts:143-151). */
+#define AVBD_SHAPE_BOX 0
+#define AVBD_SHAPE_SPHERE 1
+#define AVBD_SHAPE_SAIL 2
+/* Joint slot types (avbd_joint_info.type, layout.ts:153-154, avbd2d/gpu/layout.ts:74). */
+#define AVBD_T_NONE 0
+#define AVBD_T_JOINT 1
+#define AVBD_T_SPRING 2
+/* GPU-only rules (gpu/solver.ts:174-231; the reference's parity tests turn every one off). */
+#define AVBD_FLAG_MATCH_NEAREST 1u
+#define AVBD_FLAG_FACE_BIAS 2u
+#define AVBD_FLAG_START_AT_REST 8u
+#define AVBD_FLAG_MASS_PENALTY 16u
+/* Contact key bit: static friction held last step (layout.ts:130). */
+#define AVBD_STICK_BIT 0x80000000u
+/* Colour state (avbd2d/gpu/layout.ts:42-43, wgsl-topology.ts:81). */
+#define AVBD_NO_COLOR 255u
+#define AVBD_PENDING 256u
+#define AVBD_MAX_COLORS 64u
+/* Unbounded stiffness / thresholds are stored as BIG; a row is hard at >= 1e30 (avbd2d/gpu/layout.ts:99-100). */
+#define AVBD_BIG 3.0e38f
+
+/* One body: the reference's 10-vec4 record (layout.ts:8-59, struct Body at :219-230). */
+typedef struct avbd_body {
+  float pos[3], friction;
+  float rot[4];            /* quaternion x, y, z, w */
+  float initial_pos[3];    /* x- (pose at the start of the step) */
+  float flags;             /* 1: rewritten slot (no contact history), 2: disabled, 4: cold */
+  float initial_rot[4];
+  float size[3], mass;     /* full widths; mass 0 = static */
+  float moment[3], radius; /* principal moments; bounding radius */
+  float inertial_pos[3];   /* inertial target y */
+  float moved_step;        /* reserved (contact reuse bookkeeping) */
+  float inertial_rot[4];
+  float vel[3], prev_up_vel; /* velocity; last step's velocity along up */
+  float ang_vel[3], shape;   /* angular velocity; AVBD_SHAPE_* */
+} avbd_body;
+
+/* One joint or spring slot: the reference's 10-vec4 record (layout.ts:77-110, :232-243). */
+typedef struct avbd_joint {
+  float pen_lin[3], stiffness_lin; /* spring: w = its stiffness */
+  float pen_ang[3], stiffness_ang;
+  float lam_lin[3], fracture;      /* fracture on |lam_ang| (negative: on |lam_lin| too); BIG: never */
+  float lam_ang[3], torque_arm;
+  float c0_lin[4];
+  float c0_ang[3], yield_force;    /* BIG: never yields */
+  float r_a[3], spring_rest;       /* r_a: world point when a = -1 */
+  float r_b[3], break_bend;        /* BIG: never */
+  float rest[4];                   /* rotB = rotA * rest */
+  float rest_start[4];
+} avbd_joint;
+
+typedef struct avbd_joint_info {
+  int32_t type; /* AVBD_T_* */
+  int32_t a;    /* body index, -1: the world */
+  int32_t b;
+  int32_t meta; /* 0 */
+} avbd_joint_info;
+
+/* A contact pair (layout.ts:118-120, struct Manifold :245-248): a > b, contacts [first, first+count). */
+typedef struct avbd_manifold {
+  uint32_t a, b, first, count;
+  float normal[3], friction; /* normal from B to A */
+} avbd_manifold;
+
+/* A contact point (layout.ts:122-127, struct Contact :254-263). */
+typedef struct avbd_contact {
+  float r_a[3];
+  uint32_t key; /* feature | AVBD_STICK_BIT */
+  float r_b[3], c0_n;
+  float pen[3], c0_t1;
+  float lam[3], c0_t2;
+} avbd_contact;
+
+/* SolverParams (ref/solver.ts:139-165) and the GPU flags (gpu/solver.ts:174-231). */
+typedef struct avbd_params {
+  float dt, gravity, alpha, beta_lin, beta_ang, gamma;
+  float contact_margin;
+  int32_t iterations;
+  uint32_t flags; /* AVBD_FLAG_* */
+  float up[3];    /* unit vector; gravity pulls along -up */
+} avbd_params;
+
+typedef struct avbd_config {
+  uint32_t body_capacity;  /* 0: 1024 */
+  uint32_t joint_capacity; /* 0: 256 */
+  uint32_t pair_capacity;  /* 0: max(65536, 8 x body_capacity); grows on overflow */
+  int32_t device;          /* CUDA device ordinal */
+} avbd_config;
+
+/* readCounters (gpu/solver.ts:2305-2309). */
+typedef struct avbd_counters {
+  uint32_t pairs, contacts, manifolds, overflow; /* overflow: 1 pairs, 2 contacts, 4 manifolds */
+  uint32_t clashes, colors, rounds, error;       /* error: nonzero after a bounded wait gave up */
+  uint32_t steps, pair_capacity, reserved0, reserved1;
+} avbd_counters;
+
+typedef struct avbd_world avbd_world;
+
+/* Library. */
+int avbd_abi_version(void);
+/* Device name and SM count, for reports. */
+int avbd_device_info(int device, char* name, size_t name_cap, int* sm_count);
+
+/* Construction: `new GpuSolver3D(device, ref, options)` (gpu/solver.ts:722) / World.create (world.ts:880-927). */
+int avbd_world_create(const avbd_config* config, avbd_world** out);
+/* destroy() (gpu/solver.ts:2439-2459): idempotent on NULL. */
+int avbd_world_destroy(avbd_world* world);
+const char* avbd_last_error(const avbd_world* world);
+
+/* params (GpuParams3D, gpu/solver.ts:163-231). */
+int avbd_set_params(avbd_world* world, const avbd_params* params);
+int avbd_get_params(const avbd_world* world, avbd_params* params);
+/* Defaults of the reference's SolverParams with every GPU-only rule off and up = +z. */
+int avbd_default_params(avbd_params* params);
+
+/* addBodies (gpu/solver.ts:1469-1481): appends; *first = index of the first. */
+int avbd_add_bodies(avbd_world* world, const avbd_body* bodies, uint32_t n, uint32_t* first);
+/* rewriteBodies / patchBody (gpu/solver.ts:1113-1139): overwrite bodies [first, first+n);
+ * keep_contacts != 0 keeps their contact history (seedFrom), else the slots start fresh. */
+int avbd_write_bodies(avbd_world* world, uint32_t first, const avbd_body* bodies, uint32_t n, int keep_contacts);
+/* appendJoints / appendSprings (gpu/solver.ts:1484-1533): appends slots; *first = first slot. */
+int avbd_add_joints(avbd_world* world, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* first);
+/* seedFrom's joint rewrite (gpu/solver.ts:1330-1331). */
+int avbd_write_joints(avbd_world* world, uint32_t first, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n);
+/* releaseJoints (world.ts) / disableConstraint (gpu/solver.ts:1941-1947): slot stops acting. */
+int avbd_release_joints(avbd_world* world, const uint32_t* slots, uint32_t n);
+/* IgnoreCollision pairs (ref/forces.ts:384-390; no-collide table gpu/no-collide.ts). */
+int avbd_add_ignore_pairs(avbd_world* world, const uint32_t* pairs_ab, uint32_t n);
+/* setFilters (gpu/solver.ts): groups_mask[2i] = groups, [2i+1] = collides-with mask. */
+int avbd_set_filters(avbd_world* world, uint32_t first, const uint32_t* groups_mask, uint32_t n);
+/* seedFrom's contact import (gpu/solver.ts:1320-1359): last step's manifolds and contacts, the
+ * next step's warm-start source. manifold.first indexes `contacts`. */
+int avbd_seed_contacts(avbd_world* world, const avbd_manifold* manifolds, uint32_t n_manifolds, const avbd_contact* contacts,
+                       uint32_t n_contacts);
+/* fixedColors (gpu/solver.ts:560, 2130-2134): one colour per body (AVBD_NO_COLOR for none), or
+ * NULL to return to the Jones-Plassmann colouring. */
+int avbd_set_fixed_colors(avbd_world* world, const uint32_t* colors, uint32_t n);
+
+/* step() (gpu/solver.ts:2112-2295): n steps, enqueued on the world's stream (asynchronous). */
+int avbd_step(avbd_world* world, int n);
+/* Waits for the world's stream; reports a device error or a bounded wait that gave up. */
+int avbd_synchronize(avbd_world* world);
+
+/* Readbacks (synchronous): readBodies / readJoints / readContactList / readPairs / readCounters
+ * (gpu/solver.ts:2297-2360). *n receives the number available; at most `cap` are written. */
+int avbd_read_bodies(avbd_world* world, avbd_body* dst, uint32_t cap, uint32_t* n);
+int avbd_read_joints(avbd_world* world, avbd_joint* dst, avbd_joint_info* info, uint32_t cap, uint32_t* n);
+int avbd_read_contacts(avbd_world* world, avbd_manifold* manifolds, uint32_t manifold_cap, uint32_t* n_manifolds, avbd_contact* contacts,
+                       uint32_t contact_cap, uint32_t* n_contacts);
+int avbd_read_pairs(avbd_world* world, uint32_t* dst_ab, uint32_t cap, uint32_t* n);
+int avbd_read_colors(avbd_world* world, uint32_t* dst, uint32_t cap, uint32_t* n);
+int avbd_read_counters(avbd_world* world, avbd_counters* counters);
+
+/* Asynchronous pose readback into caller memory (pinned for overlap): World.read (world.ts:2102-2224). */
+int avbd_read_bodies_async(avbd_world* world, avbd_body* dst, uint32_t cap);
+
+/* Device-side timing of the last `avbd_step` call's kernels, per phase (ms): collision,
+ * topology + solve (profileNextStep, gpu/solver.ts:1951-1953). Requires enable != 0 before stepping. */
+int avbd_enable_timing(avbd_world* world, int enable);
+int avbd_last_timing(avbd_world* world, float* collision_ms, float* solve_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AVBD_H */

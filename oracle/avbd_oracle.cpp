@@ -1012,18 +1012,13 @@ inline ColorResult jpColor(int n, const std::vector<char>& dynamic, const std::v
       } else dst[b] = s;
     }
   };
-  // Rounds in pairs (A -> B -> A) until a pair starts with nothing pending
+  // Rounds in pairs (A -> B -> A) while anything is pending, at most maxRounds
   while (pendingCount > 0 && res.rounds < maxRounds) {
     round(A, Bs);
     round(Bs, A);
     res.rounds += 2;
     pendingCount = 0;
-    for (int b = 0; b < n; b++) if (dynamic[b] && (A[b] & PENDING) && (A[b] & 0xff) != uint32_t(cap - 1)) pendingCount++;
-    // A body parked at cap-1 still pending has nowhere to go: it stays a clash
-    int parked = 0;
-    for (int b = 0; b < n; b++) if (dynamic[b] && (A[b] & PENDING) && (A[b] & 0xff) == uint32_t(cap - 1)) parked++;
-    if (pendingCount == 0) break;
-    (void)parked;
+    for (int b = 0; b < n; b++) if (dynamic[b] && (A[b] & PENDING)) pendingCount++;
   }
   // count: NO_COLOR -> cap-1, pending kept (colorCount, wgsl-topology.ts:277-304)
   for (int b = 0; b < n; b++) {
@@ -1158,6 +1153,16 @@ template <class T> struct Solver {
   }
 
   // --- GPU mode ---------------------------------------------------------------------------------
+  static Body<float> toFloat(const Body<T>& b) {
+    Body<float> f;
+    for (int k = 0; k < 3; k++) { f.pos[k] = float(b.pos[k]); f.size[k] = float(b.size[k]); }
+    for (int k = 0; k < 4; k++) f.rot[k] = float(b.rot[k]);
+    f.mass = float(b.mass);
+    f.radius = float(b.radius);
+    f.friction = float(b.friction);
+    f.shape = b.shape;
+    return f;
+  }
   std::vector<Rec32> records32() const {
     std::vector<Rec32> r(bodies.size());
     for (size_t i = 0; i < bodies.size(); i++) {
@@ -1219,9 +1224,12 @@ template <class T> struct Solver {
       int a = int(p.first), b = int(p.second);
       Body<T>& A = bodies[a];
       Body<T>& B = bodies[b];
-      V3<T> normal;
-      Found<T> found = narrowphase(A, B, (flags & FLAG_FACE_BIAS) != 0, normal);
-      if (found.count == 0) continue;
+      // The GPU's own arithmetic (f32) finds the contacts, so both sides solve one contact set
+      Body<float> fA = toFloat(A), fB = toFloat(B);
+      V3<float> nf;
+      Found<float> ff = narrowphase(fA, fB, (flags & FLAG_FACE_BIAS) != 0, nf);
+      if (ff.count == 0) continue;
+      V3<T> normal{T(nf[0]), T(nf[1]), T(nf[2])};
       auto m = std::make_unique<Manifold<T>>(this, a, b);
       m->friction = std::sqrt(A.friction * B.friction);
       m->basis = orthonormal(normal);
@@ -1234,11 +1242,12 @@ template <class T> struct Solver {
         T mA = A.mass <= 0 ? T(3.4e38) : A.mass, mB = B.mass <= 0 ? T(3.4e38) : B.mass;
         penaltyMin = clampv(tmin(mA, mB) / (dt * dt), T(PENALTY_MIN), T(PENALTY_MAX));
       }
-      for (int i = 0; i < found.count; i++) {
+      for (int i = 0; i < ff.count; i++) {
         Contact<T> c;
-        c.feature = found.feature[i];
-        c.rA = rotate(conjugate(A.rot), sub3(found.xA[i], A.pos));
-        c.rB = rotate(conjugate(B.rot), sub3(found.xB[i], B.pos));
+        c.feature = ff.feature[i];
+        V3<float> ra = rotate(conjugate(fA.rot), sub3(ff.xA[i], fA.pos)), rb = rotate(conjugate(fB.rot), sub3(ff.xB[i], fB.pos));
+        c.rA = V3<T>{T(ra[0]), T(ra[1]), T(ra[2])};
+        c.rB = V3<T>{T(rb[0]), T(rb[1]), T(rb[2])};
         const Contact<T>* pc = nullptr;
         if (old) {
           for (auto& o : *old) if (o.feature == c.feature) { pc = &o; break; }
@@ -1314,7 +1323,7 @@ template <class T> struct Solver {
       }
       start[n] = int(nbr.size());
       for (int b = 0; b < n; b++) state[b] = bodies[b].color;
-      ColorResult r = jpColor(n, dynamic, start, nbr, state, MAX_COLORS, 64);
+      ColorResult r = jpColor(n, dynamic, start, nbr, state, MAX_COLORS, 32);
       lastColors = r.colors;
       lastClashes = r.clashes;
       lastRounds = r.rounds;

@@ -12,7 +12,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
-from build import build  # noqa: E402
+from build_oracle import build  # noqa: E402
 
 _lib = None
 

@@ -1,0 +1,167 @@
+"""Test helpers: the CPU oracle's state as C-ABI records (the reference's seedFrom, gpu/solver.ts:1320-1359)."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+import avbd_b200
+from avbd_b200 import BODY_DTYPE, CONTACT_DTYPE, INFO_DTYPE, JOINT_DTYPE, MANIFOLD_DTYPE
+from avbd_b200 import _abi
+from avbd_b200.solver import finite
+from oracle import K_IGNORE, K_JOINT, K_MANIFOLD, K_SPRING, NO_COLOR, Oracle
+
+STICK_BIT = _abi.STICK_BIT
+
+
+def body_records(o: Oracle) -> np.ndarray:
+    b = o.bodies()
+    out = np.zeros(len(b), dtype=BODY_DTYPE)
+    out['pos'] = b[:, 0:3]
+    out['friction'] = b[:, 23]
+    out['rot'] = b[:, 3:7]
+    out['initial_pos'] = b[:, 26:29]
+    out['flags'] = 0.0
+    out['initial_rot'] = b[:, 29:33]
+    out['size'] = b[:, 16:19]
+    out['mass'] = b[:, 19]
+    out['moment'] = b[:, 20:23]
+    out['radius'] = b[:, 24]
+    out['inertial_pos'] = b[:, 33:36]
+    out['inertial_rot'] = b[:, 36:40]
+    out['vel'] = b[:, 7:10]
+    out['prev_up_vel'] = b[:, 15]  # up = +z
+    out['ang_vel'] = b[:, 10:13]
+    out['shape'] = b[:, 25]
+    return out
+
+
+def joint_records(o: Oracle):
+    """Live joints and springs in force order (as GpuSolver3D's constructor and seedFrom take them), and ignore pairs."""
+    recs, infos, ignores = [], [], []
+    for i in range(o.force_count):
+        r = o.force(i)
+        kind = int(r[0])
+        if kind == K_MANIFOLD:
+            continue
+        if kind == K_IGNORE:
+            ignores.append((int(r[1]), int(r[2])))
+            continue
+        rec = np.zeros(1, dtype=JOINT_DTYPE)[0]
+        info = np.zeros(1, dtype=INFO_DTYPE)[0]
+        info['a'], info['b'] = int(r[1]), int(r[2])
+        if kind == K_JOINT:
+            broken = r[26] != 0
+            rec['pen_lin'] = r[3:6]
+            rec['stiffness_lin'] = 0.0 if broken else finite(r[21])
+            rec['pen_ang'] = r[6:9]
+            rec['stiffness_ang'] = 0.0 if broken else finite(r[22])
+            rec['lam_lin'] = r[9:12]
+            rec['fracture'] = -finite(r[23]) if r[24] else finite(r[23])
+            rec['lam_ang'] = r[12:15]
+            rec['torque_arm'] = r[25]
+            rec['c0_lin'][:3] = r[15:18]
+            rec['c0_ang'] = r[18:21]
+            rec['yield_force'] = finite(r[27])
+            rec['break_bend'] = finite(r[28])
+            rest = r[29:33] if r[33] else np.array([0, 0, 0, 1.0])
+            rec['rest'] = rest
+            rec['rest_start'] = r[34:38] if r[38] else rest
+            rec['r_a'] = r[39:42]
+            rec['r_b'] = r[42:45]
+            info['type'] = _abi.T_JOINT
+        else:
+            rec['stiffness_lin'] = r[45]
+            rec['r_a'] = r[39:42]
+            rec['spring_rest'] = r[46]
+            rec['r_b'] = r[42:45]
+            rec['rest'] = [0, 0, 0, 1]
+            rec['rest_start'] = [0, 0, 0, 1]
+            info['type'] = _abi.T_SPRING
+        recs.append(rec)
+        infos.append(info)
+    return np.array(recs, dtype=JOINT_DTYPE), np.array(infos, dtype=INFO_DTYPE), np.array(ignores, dtype=np.uint32).reshape(-1, 2)
+
+
+def contact_records(o: Oracle):
+    m, c = o.manifolds()
+    man = np.zeros(len(m), dtype=MANIFOLD_DTYPE)
+    con = np.zeros(len(c), dtype=CONTACT_DTYPE)
+    k = 0
+    for i, r in enumerate(m):
+        cnt = int(r[3])
+        man[i]['a'], man[i]['b'], man[i]['first'], man[i]['count'] = int(r[1]), int(r[2]), k, cnt
+        man[i]['normal'] = r[4:7]
+        man[i]['friction'] = r[7]
+        k += cnt
+    for j, q in enumerate(c):
+        con[j]['r_a'] = q[2:5]
+        con[j]['key'] = (int(q[0]) & 0xFFFFFFFF) | (STICK_BIT if q[1] else 0)
+        con[j]['r_b'] = q[5:8]
+        con[j]['c0_n'] = q[8]
+        con[j]['pen'] = q[11:14]
+        con[j]['c0_t1'] = q[9]
+        con[j]['lam'] = q[14:17]
+        con[j]['c0_t2'] = q[10]
+    return man, con
+
+
+def params_struct(p, flags: int = 0):
+    s = _abi.Params(dt=p.dt, gravity=p.gravity, alpha=p.alpha, beta_lin=p.beta_lin, beta_ang=p.beta_ang, gamma=p.gamma,
+                    contact_margin=p.contact_margin, iterations=p.iterations, flags=flags)
+    s.up[0], s.up[1], s.up[2] = 0.0, 0.0, 1.0
+    return s
+
+
+def cuda_from_oracle(o: Oracle, params, flags: int = 0, seed: bool = True, **kw) -> avbd_b200.CudaSolver3D:
+    """A fresh CUDA world holding the oracle's state (`new GpuSolver3D(device, ref)` + `seedFrom(ref)`)."""
+    bodies = body_records(o)
+    joints, info, ignores = joint_records(o)
+    w = avbd_b200.CudaSolver3D(body_capacity=max(len(bodies), 1), joint_capacity=max(len(joints), 16), **kw)
+    w.params = params_struct(params, flags)
+    w.add_bodies(bodies)
+    if len(joints):
+        w.add_joints(joints, info)
+    if len(ignores):
+        w.add_ignore_pairs(ignores)
+    if seed:
+        # seedFrom writes the bodies back keeping their contact history (gpu/solver.ts:1325-1327)
+        w.write_bodies(0, bodies, keep_contacts=True)
+        man, con = contact_records(o)
+        w.seed_contacts(man, con)
+    return w
+
+
+def oracle_sequential_colors(o: Oracle) -> np.ndarray:
+    b = o.bodies()
+    colors = np.full(len(b), NO_COLOR, dtype=np.uint32)
+    nxt = 0
+    for i in range(len(b) - 1, -1, -1):
+        if b[i, 19] > 0:
+            colors[i] = nxt
+            nxt += 1
+    assert nxt <= 64
+    return colors
+
+
+def pose_diff(cuda_bodies: np.ndarray, oracle_bodies: np.ndarray) -> float:
+    d = 0.0
+    if len(oracle_bodies):
+        d = max(float(np.abs(cuda_bodies['pos'] - oracle_bodies[:, 0:3]).max()), float(np.abs(cuda_bodies['rot'] - oracle_bodies[:, 3:7]).max()))
+    return d
+
+
+def lcg(seed: int):
+    """The reference tests' generator: seed = seed * 1103515245 + 12345 (mod 2^32), / 2^32."""
+    state = [seed & 0xFFFFFFFF]
+
+    def rand():
+        state[0] = (state[0] * 1103515245 + 12345) & 0xFFFFFFFF
+        return state[0] / 2 ** 32
+    return rand
+
+
+def qnormalize(q):
+    l = math.sqrt((q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) + q[3] * q[3])
+    return [q[0] / l, q[1] / l, q[2] / l, q[3] / l]

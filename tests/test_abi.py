@@ -1,0 +1,60 @@
+"""The C-ABI library loads and exports every symbol include/avbd.h declares (no GPU needed)."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+import avbd_b200
+from avbd_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, 'include', 'avbd.h')).read()
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    return sorted(set(re.findall(r'\b(avbd_[a-z0-9_]+)\s*\(', text)))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = avbd_b200.load()
+    names = declared_functions()
+    assert len(names) >= 25
+    for name in names:
+        assert hasattr(lib, name), f'{name} is declared in avbd.h but not exported'
+        assert name in _abi.SIGNATURES, f'{name} has no ctypes signature'
+
+
+def test_record_layouts_match_the_reference():
+    # layout.ts:15 BODY_FLOATS = 40, :77 JOINT_FLOATS = 40, :118 MANIFOLD_WORDS = 8, :123 CONTACT_WORDS = 16
+    assert _abi.BODY_DTYPE.itemsize == 40 * 4
+    assert _abi.JOINT_DTYPE.itemsize == 40 * 4
+    assert _abi.MANIFOLD_DTYPE.itemsize == 8 * 4
+    assert _abi.CONTACT_DTYPE.itemsize == 16 * 4
+    assert ctypes.sizeof(_abi.Params) == 12 * 4
+
+
+def test_defaults_and_invalid_arguments_without_a_device():
+    lib = avbd_b200.load()
+    p = _abi.Params()
+    assert lib.avbd_default_params(ctypes.byref(p)) == 0
+    assert abs(p.dt - 1 / 60) < 1e-7 and p.iterations == 10 and p.gravity == -10.0 and tuple(p.up) == (0.0, 0.0, 1.0)
+    assert lib.avbd_abi_version() == 1
+    assert lib.avbd_world_create(None, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_world_destroy(None) == 0
+    assert lib.avbd_step(None, 1) == _abi.AVBD_ERR_INVALID
+
+
+def test_create_fails_loudly_without_a_b200():
+    """There is no CPU fallback: without a B200 the world cannot be made."""
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip('a GPU is present')
+    with pytest.raises(avbd_b200.AvbdError):
+        avbd_b200.CudaSolver3D(avbd_b200.scenes.demo_scene('Ground'))

@@ -1,0 +1,172 @@
+"""The CPU oracle against the reference's golden trajectories and its own invariants (no GPU)."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from avbd_b200.scenes import DEMO_SCENES, Scene, demo_scene
+from oracle import Oracle, color_graph, lib
+from _util import lcg, qnormalize
+
+GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
+
+
+@pytest.mark.parametrize('index', range(len(DEMO_SCENES)))
+def test_golden_trajectory(index):
+    """tests/avbd3d-ref.test.ts:27-49: every scene at frames 1, 10, 60, 120, 180, force count and
+    pose within 1e-9 of upstream avbd-demo3d (double, no FMA)."""
+    name = DEMO_SCENES[index][0]
+    golden = json.load(open(os.path.join(GOLDEN, f'scene-{index}.json')))
+    assert golden['scene'] == name
+    o = Oracle(demo_scene(name))
+    frame = 0
+    for sample in golden['samples']:
+        while frame < sample['frame']:
+            o.step()
+            frame += 1
+        assert o.force_count == sample['forces'], f'{name} frame {frame}: force count'
+        if sample['bodies']:
+            b = o.bodies()
+            g = np.array(sample['bodies'])
+            diff = max(np.abs(b[:, 0:3] - g[:, 0:3]).max(), np.abs(b[:, 3:7] - g[:, 3:7]).max())
+            assert diff < 1e-9, f'{name} frame {frame}: pose diff {diff}'
+
+
+def test_stack_rests_within_margin():
+    """tests/avbd3d-ref.test.ts:51-60: the stack settles about one collision margin deep per contact."""
+    o = Oracle(demo_scene('Stack'))
+    o.step(900)
+    b = o.bodies()
+    for i in range(1, len(b)):
+        assert abs(b[i, 2] - i) < 0.011 * i
+        assert np.hypot(b[i, 0], b[i, 1]) < 1e-6
+        assert np.linalg.norm(b[i, 7:10]) < 1e-3
+
+
+def _random_box_pairs(count=300, seed=7):
+    """The narrowphase known-answer procedure (tests-gpu/avbd3d-gpu.gpu.test.ts:101-142)."""
+    rand = lcg(seed)
+    s = Scene('box pairs')
+    s.params.gravity = 0.0
+    s.params.iterations = 0
+    for p in range(count):
+        base = [(p % 20) * 20, (p // 20) * 20, 0]
+        for k in range(2):
+            size = [0.4 + rand() * 1.6, 0.4 + rand() * 1.6, 0.4 + rand() * 1.6]
+            off = [0, 0, 0] if k == 0 else [(rand() - 0.5) * 1.2, (rand() - 0.5) * 1.2, (rand() - 0.5) * 1.2]
+            i = s.box(size, 1, 0.5, [base[0] + off[0], base[1] + off[1], base[2] + off[2]])
+            s.bodies[i].rot = qnormalize([rand() - 0.5, rand() - 0.5, rand() - 0.5, rand() - 0.5])
+    return s
+
+
+def test_narrowphase_f32_matches_f64_features():
+    """Random poses have no exact ties: the f32 restatement finds the f64 reference's contacts with the same keys."""
+    s = _random_box_pairs()
+    o64, o32 = Oracle(s), Oracle(s, fp32=True)
+    mismatched = total = 0
+    for p in range(300):
+        c64, _ = o64.narrowphase(2 * p + 1, 2 * p)
+        c32, _ = o32.narrowphase(2 * p + 1, 2 * p)
+        assert len(c64) == len(c32), f'pair {p}'
+        total += len(c64)
+        for f, ra, rb in c64:
+            match = [g for g in c32 if np.linalg.norm(g[1] - ra) < 1e-3 and np.linalg.norm(g[2] - rb) < 1e-3]
+            assert match, f'pair {p}: contact missing'
+            mismatched += match[0][0] != f
+    assert total > 300 and mismatched == 0
+
+
+def test_pair_rule_matches_brute_force_definition():
+    """The grid-accelerated pair set equals the broadphase rule's definition (sphere, AABB, face axes,
+    ignored pairs, not both static) over all pairs (tests-gpu/avbd3d-gpu.gpu.test.ts:144-205)."""
+    rand = lcg(11)
+    s = Scene('boxes')
+    for i in range(600):
+        big = i % 499 == 0
+        size = [30, 30, 1] if big else [0.3 + rand(), 0.3 + rand(), 0.3 + rand()]
+        k = s.box(size, 1 if rand() < 0.9 else 0, 0.5, [(rand() - 0.5) * 20, (rand() - 0.5) * 20, (rand() - 0.5) * 20])
+        if not big:
+            s.bodies[k].rot = qnormalize([rand() - 0.5, rand() - 0.5, rand() - 0.5, rand() - 0.5])
+    s.ignore(2, 1)
+    o = Oracle(s)
+    got = {tuple(p) for p in o.pairs().tolist()}
+    B = s.bodies
+    f32 = np.float32
+
+    def rot(q, v):
+        q = [f32(x) for x in q]
+        v = [f32(x) for x in v]
+        ux, uy, uz, w = q
+        tx = (uy * v[2] - uz * v[1]) * f32(2)
+        ty = (uz * v[0] - ux * v[2]) * f32(2)
+        tz = (ux * v[1] - uy * v[0]) * f32(2)
+        return np.array([v[0] + tx * w + (uy * tz - uz * ty), v[1] + ty * w + (uz * tx - ux * tz), v[2] + tz * w + (ux * ty - uy * tx)], dtype=f32)
+    axes = [[rot(b.rot, e) for e in ([1, 0, 0], [0, 1, 0], [0, 0, 1])] for b in B]
+    half = [np.float32(np.array(b.size)) * f32(0.5) for b in B]
+    expected = set()
+    for i in range(len(B)):
+        for j in range(i):
+            if B[i].mass <= 0 and B[j].mass <= 0:
+                continue
+            if (i, j) == (2, 1):
+                continue
+            d = np.float32(np.array(B[i].pos)) - np.float32(np.array(B[j].pos))
+            r = f32(B[i].radius) + f32(B[j].radius)
+            if float(d @ d) > float(r * r) * (1 + 1e-6):
+                continue
+            ai = sum(np.abs(axes[i][k]) * half[i][k] for k in range(3))
+            aj = sum(np.abs(axes[j][k]) * half[j][k] for k in range(3))
+            if np.any(np.abs(d) > ai + aj + 1e-4):
+                continue
+            ext = lambda b, n: sum(half[b][k] * abs(float(n @ axes[b][k])) for k in range(3))
+            if any(abs(float(d @ n)) - ext(i, n) - ext(j, n) > 1e-3 for n in axes[i] + axes[j]):
+                continue
+            expected.add((i, j))
+    # Only pairs within f32 rounding of a threshold may differ between the two evaluations
+    assert len(got ^ expected) <= 2, sorted(got ^ expected)
+    assert len(got) > 50
+
+
+def test_colouring_is_proper_and_deterministic():
+    rng = np.random.default_rng(5)
+    n = 2000
+    edges = set()
+    for _ in range(6000):
+        a, b = rng.integers(0, n, 2)
+        if a != b:
+            edges.add((int(max(a, b)), int(min(a, b))))
+    nbr = [[] for _ in range(n)]
+    for a, b in edges:
+        nbr[a].append(b)
+        nbr[b].append(a)
+    start = np.zeros(n + 1, dtype=np.int32)
+    for i in range(n):
+        start[i + 1] = start[i] + len(nbr[i])
+    flat = np.array([j for i in range(n) for j in nbr[i]], dtype=np.int32)
+    dyn = np.ones(n, dtype=np.uint8)
+    state = np.full(n, 255, dtype=np.uint32)
+    s1, st1 = color_graph(n, dyn, start, flat, state)
+    s2, _ = color_graph(n, dyn, start, flat, state)
+    assert np.array_equal(s1, s2)
+    assert st1['clashes'] == 0
+    col = s1 & 0xFF
+    for a, b in edges:
+        assert col[a] != col[b]
+    # Incremental: recolouring the same graph from its own colours keeps a proper colouring with no more colours
+    s3, st3 = color_graph(n, dyn, start, flat, s1)
+    assert st3['clashes'] == 0 and st3['colors'] <= st1['colors']
+
+
+def test_hash32_matches_reference_priorities():
+    """lowbias32 (avbd2d/soa/coloring.ts:24-32) on a few inputs computed by hand from its definition."""
+    L = lib()
+    def ref(x):
+        x &= 0xFFFFFFFF
+        x ^= x >> 16; x = (x * 0x7feb352d) & 0xFFFFFFFF
+        x ^= x >> 15; x = (x * 0x846ca68b) & 0xFFFFFFFF
+        x ^= x >> 16
+        return x
+    for v in [0, 1, 2, 12345, 0x9e3779b9, 0xFFFFFFFF]:
+        assert L.orc_hash32(v) == ref(v)

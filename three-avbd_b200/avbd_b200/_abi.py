@@ -1,0 +1,138 @@
+"""ctypes view of include/avbd.h: loads libavbd_cuda.so and declares every entry point.
+
+The record dtypes are byte-for-byte the C structs (and the reference's GPU records: a body is 40
+floats, src/avbd3d/gpu/layout.ts:8-59; a joint 40 floats, layout.ts:77-110; a manifold 8 words and a
+contact 16 words, layout.ts:118-127). There is no CPU fallback: if the library or a B200 is missing,
+the solver raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libavbd_cuda.so')
+
+AVBD_OK = 0
+AVBD_ERR_INVALID = -1
+AVBD_ERR_CAPACITY = -2
+AVBD_ERR_CUDA = -3
+AVBD_ERR_TIMEOUT = -4
+AVBD_ERR_NO_DEVICE = -5
+
+SHAPE_BOX, SHAPE_SPHERE, SHAPE_SAIL = 0, 1, 2
+T_NONE, T_JOINT, T_SPRING = 0, 1, 2
+FLAG_MATCH_NEAREST, FLAG_FACE_BIAS, FLAG_START_AT_REST, FLAG_MASS_PENALTY = 1, 2, 8, 16
+STICK_BIT = 0x80000000
+NO_COLOR = 255
+PENDING = 256
+MAX_COLORS = 64
+BIG = np.float32(3.0e38)
+
+BODY_DTYPE = np.dtype([
+    ('pos', '<f4', 3), ('friction', '<f4'), ('rot', '<f4', 4), ('initial_pos', '<f4', 3), ('flags', '<f4'),
+    ('initial_rot', '<f4', 4), ('size', '<f4', 3), ('mass', '<f4'), ('moment', '<f4', 3), ('radius', '<f4'),
+    ('inertial_pos', '<f4', 3), ('moved_step', '<f4'), ('inertial_rot', '<f4', 4), ('vel', '<f4', 3), ('prev_up_vel', '<f4'),
+    ('ang_vel', '<f4', 3), ('shape', '<f4'),
+])
+JOINT_DTYPE = np.dtype([
+    ('pen_lin', '<f4', 3), ('stiffness_lin', '<f4'), ('pen_ang', '<f4', 3), ('stiffness_ang', '<f4'),
+    ('lam_lin', '<f4', 3), ('fracture', '<f4'), ('lam_ang', '<f4', 3), ('torque_arm', '<f4'),
+    ('c0_lin', '<f4', 4), ('c0_ang', '<f4', 3), ('yield_force', '<f4'), ('r_a', '<f4', 3), ('spring_rest', '<f4'),
+    ('r_b', '<f4', 3), ('break_bend', '<f4'), ('rest', '<f4', 4), ('rest_start', '<f4', 4),
+])
+INFO_DTYPE = np.dtype([('type', '<i4'), ('a', '<i4'), ('b', '<i4'), ('meta', '<i4')])
+MANIFOLD_DTYPE = np.dtype([('a', '<u4'), ('b', '<u4'), ('first', '<u4'), ('count', '<u4'), ('normal', '<f4', 3), ('friction', '<f4')])
+CONTACT_DTYPE = np.dtype([
+    ('r_a', '<f4', 3), ('key', '<u4'), ('r_b', '<f4', 3), ('c0_n', '<f4'), ('pen', '<f4', 3), ('c0_t1', '<f4'),
+    ('lam', '<f4', 3), ('c0_t2', '<f4'),
+])
+assert BODY_DTYPE.itemsize == 160 and JOINT_DTYPE.itemsize == 160 and MANIFOLD_DTYPE.itemsize == 32 and CONTACT_DTYPE.itemsize == 64
+
+
+class Params(ctypes.Structure):
+    _fields_ = [('dt', ctypes.c_float), ('gravity', ctypes.c_float), ('alpha', ctypes.c_float), ('beta_lin', ctypes.c_float),
+                ('beta_ang', ctypes.c_float), ('gamma', ctypes.c_float), ('contact_margin', ctypes.c_float), ('iterations', ctypes.c_int32),
+                ('flags', ctypes.c_uint32), ('up', ctypes.c_float * 3)]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [('body_capacity', ctypes.c_uint32), ('joint_capacity', ctypes.c_uint32), ('pair_capacity', ctypes.c_uint32), ('device', ctypes.c_int32)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ('pairs', 'contacts', 'manifolds', 'overflow', 'clashes', 'colors', 'rounds', 'error', 'steps',
+                                                'pair_capacity', 'reserved0', 'reserved1')]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if not n.startswith('reserved')}
+
+
+# Every function include/avbd.h declares, with its argument types (the C-ABI symbol table)
+P, U, I, VP = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p
+PU = ctypes.POINTER(ctypes.c_uint32)
+SIGNATURES = {
+    'avbd_abi_version': ([], I),
+    'avbd_device_info': ([I, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int)], I),
+    'avbd_world_create': ([ctypes.POINTER(Config), ctypes.POINTER(P)], I),
+    'avbd_world_destroy': ([P], I),
+    'avbd_last_error': ([P], ctypes.c_char_p),
+    'avbd_set_params': ([P, ctypes.POINTER(Params)], I),
+    'avbd_get_params': ([P, ctypes.POINTER(Params)], I),
+    'avbd_default_params': ([ctypes.POINTER(Params)], I),
+    'avbd_add_bodies': ([P, VP, U, PU], I),
+    'avbd_write_bodies': ([P, U, VP, U, I], I),
+    'avbd_add_joints': ([P, VP, VP, U, PU], I),
+    'avbd_write_joints': ([P, U, VP, VP, U], I),
+    'avbd_release_joints': ([P, PU, U], I),
+    'avbd_add_ignore_pairs': ([P, PU, U], I),
+    'avbd_set_filters': ([P, U, PU, U], I),
+    'avbd_seed_contacts': ([P, VP, U, VP, U], I),
+    'avbd_set_fixed_colors': ([P, PU, U], I),
+    'avbd_step': ([P, I], I),
+    'avbd_synchronize': ([P], I),
+    'avbd_read_bodies': ([P, VP, U, PU], I),
+    'avbd_read_joints': ([P, VP, VP, U, PU], I),
+    'avbd_read_contacts': ([P, VP, U, PU, VP, U, PU], I),
+    'avbd_read_pairs': ([P, PU, U, PU], I),
+    'avbd_read_colors': ([P, PU, U, PU], I),
+    'avbd_read_counters': ([P, ctypes.POINTER(Counters)], I),
+    'avbd_read_bodies_async': ([P, VP, U], I),
+    'avbd_enable_timing': ([P, I], I),
+    'avbd_last_timing': ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)], I),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """The CUDA library, with every declared symbol bound. Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f'{path} is missing: build it with three-avbd_b200/build.py (there is no CPU fallback)')
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+class AvbdError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f'avbd error {code}: {message}')
+        self.code = code
+
+
+def ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def uptr(a: np.ndarray):
+    return a.ctypes.data_as(PU)

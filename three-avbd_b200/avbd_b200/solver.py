@@ -1,0 +1,345 @@
+"""`CudaSolver3D`: the host-side mirror of the reference's `GpuSolver3D` (src/avbd3d/gpu/solver.ts:598)
+over the C ABI, with the members `World` calls (step, readBodies, readJoints, readCounters,
+readContactList, readPairs, addBodies, appendJoints, setFilters, params, destroy) and the
+validation surface the reference's parity tests use (seedFrom's imports, fixedColors,
+sequentialColors).
+
+Packing follows GpuSolver3D.pack / writeJoint (solver.ts:1176-1256): f64 scene values rounded to
+f32, Infinity stored as BIG, a rewritten slot flagged so it starts without contact history.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _abi
+from ._abi import (BODY_DTYPE, CONTACT_DTYPE, INFO_DTYPE, JOINT_DTYPE, MANIFOLD_DTYPE, NO_COLOR, AvbdError, Counters, Params, ptr, uptr)
+from .scenes import SHAPE_SPHERE, Scene
+
+
+def finite(x: float) -> float:
+    """Infinity is never stored on the device: BIG stands for it (avbd2d/gpu/layout.ts:1-4, gpu/solver.ts:115)."""
+    if x == math.inf:
+        return float(_abi.BIG)
+    if x == -math.inf:
+        return -float(_abi.BIG)
+    return float(x)
+
+
+def pack_bodies(bodies, up=(0.0, 0.0, 1.0)) -> np.ndarray:
+    """Scene bodies (f64) as device records (GpuSolver3D.pack, solver.ts:1176-1212)."""
+    out = np.zeros(len(bodies), dtype=BODY_DTYPE)
+    for k, b in enumerate(bodies):
+        r = out[k]
+        r['pos'] = b.pos
+        r['friction'] = b.friction
+        r['rot'] = b.rot
+        r['initial_pos'] = b.initial_pos
+        r['flags'] = 1.0
+        r['initial_rot'] = b.initial_rot
+        r['size'] = b.size
+        r['mass'] = b.mass
+        r['moment'] = b.moment
+        r['radius'] = b.radius
+        r['inertial_pos'] = b.inertial_pos
+        r['inertial_rot'] = b.inertial_rot
+        r['vel'] = b.vel
+        r['prev_up_vel'] = b.prev_vel[0] * up[0] + b.prev_vel[1] * up[1] + b.prev_vel[2] * up[2]
+        r['ang_vel'] = b.ang_vel
+        r['shape'] = float(b.shape)
+    return out
+
+
+def torque_arm(size_a, size_b) -> float:
+    """forces.ts:145-146: |sA + sB|^2 (sA = 0 for the world)."""
+    s = [size_a[k] + size_b[k] for k in range(3)]
+    return s[0] * s[0] + s[1] * s[1] + s[2] * s[2]
+
+
+def pack_force(f, bodies) -> tuple[np.ndarray, np.ndarray]:
+    """A scene joint/spring as (record, info) (GpuSolver3D.writeJoint, solver.ts:1214-1247)."""
+    rec = np.zeros(1, dtype=JOINT_DTYPE)[0]
+    info = np.zeros(1, dtype=INFO_DTYPE)[0]
+    if f.kind == 'joint':
+        rec['pen_lin'] = f.penalty_lin
+        rec['stiffness_lin'] = finite(f.stiffness_lin)
+        rec['pen_ang'] = f.penalty_ang
+        rec['stiffness_ang'] = finite(f.stiffness_ang)
+        rec['fracture'] = -finite(f.fracture) if f.fracture_linear else finite(f.fracture)
+        sa = bodies[f.a].size if f.a >= 0 else [0.0, 0.0, 0.0]
+        rec['torque_arm'] = torque_arm(sa, bodies[f.b].size)
+        rec['yield_force'] = finite(f.yield_force)
+        rec['break_bend'] = finite(f.break_bend)
+        rest = f.rest if f.rest is not None else [0.0, 0.0, 0.0, 1.0]
+        rec['rest'] = rest
+        rec['rest_start'] = f.rest_start if f.rest_start is not None else rest
+        rec['r_a'] = f.rA
+        rec['r_b'] = f.rB
+        info['type'] = _abi.T_JOINT
+    elif f.kind == 'spring':
+        rec['stiffness_lin'] = f.spring_stiffness
+        rec['r_a'] = f.rA
+        rec['spring_rest'] = f.spring_rest
+        rec['r_b'] = f.rB
+        rec['rest'] = [0.0, 0.0, 0.0, 1.0]
+        rec['rest_start'] = [0.0, 0.0, 0.0, 1.0]
+        info['type'] = _abi.T_SPRING
+    else:
+        raise ValueError(f.kind)
+    info['a'] = f.a
+    info['b'] = f.b
+    return rec, info
+
+
+def morton_order(positions: np.ndarray) -> np.ndarray:
+    """Body order along a Z curve of the starting positions, 10 bits per axis (solver.ts:462-485)."""
+    lo = positions.min(axis=0)
+    hi = positions.max(axis=0)
+    q = np.minimum(1023, np.floor((positions - lo) / np.maximum(hi - lo, 1e-9) * 1024)).astype(np.uint64)
+
+    def spread(x):
+        x = x & 0x3FF
+        x = (x | (x << 16)) & 0x30000FF
+        x = (x | (x << 8)) & 0x300F00F
+        x = (x | (x << 4)) & 0x30C30C3
+        x = (x | (x << 2)) & 0x9249249
+        return x
+
+    code = spread(q[:, 0]) | (spread(q[:, 1]) << 1) | (spread(q[:, 2]) << 2)
+    return np.lexsort((np.arange(len(code)), code))
+
+
+class CudaSolver3D:
+    """One world on one B200. Mirrors GpuSolver3D's construction from a scene (`new GpuSolver3D(device,
+    ref, {spatialSort})`): bodies and joints are uploaded in creation order (or Morton order with
+    `spatial_sort=True`; `gpu_index` maps scene indices, as refToGpu does)."""
+
+    def __init__(self, scene: Scene | None = None, *, body_capacity: int | None = None, joint_capacity: int | None = None,
+                 pair_capacity: int = 0, device: int = 0, spatial_sort: bool = False):
+        self.lib = _abi.load()
+        n = len(scene.bodies) if scene else 0
+        nj = sum(1 for f in scene.forces if f.kind != 'ignore') if scene else 0
+        cfg = _abi.Config(body_capacity=body_capacity or max(n, 1), joint_capacity=joint_capacity or max(nj, 16), pair_capacity=pair_capacity,
+                          device=device)
+        self.handle = ctypes.c_void_p()
+        code = self.lib.avbd_world_create(ctypes.byref(cfg), ctypes.byref(self.handle))
+        if code != _abi.AVBD_OK:
+            raise AvbdError(code, 'avbd_world_create failed (a B200 with the CUDA library is required; there is no CPU fallback)')
+        self.order = np.arange(n)
+        self.gpu_index = np.arange(n)
+        self.fixed_colors = None
+        if scene is not None:
+            self.params = scene.params
+            if spatial_sort and n:
+                self.order = morton_order(np.array([b.pos for b in scene.bodies]))
+                self.gpu_index = np.empty(n, dtype=np.int64)
+                self.gpu_index[self.order] = np.arange(n)
+            self.add_bodies(pack_bodies([scene.bodies[i] for i in self.order]))
+            recs, infos, ignores = [], [], []
+            for f in scene.forces:
+                if f.kind == 'ignore':
+                    ignores.append((int(self.gpu_index[f.a]), int(self.gpu_index[f.b])))
+                    continue
+                r, i = pack_force(f, scene.bodies)
+                i['a'] = int(self.gpu_index[f.a]) if f.a >= 0 else -1
+                i['b'] = int(self.gpu_index[f.b])
+                recs.append(r)
+                infos.append(i)
+            if recs:
+                self.add_joints(np.array(recs, dtype=JOINT_DTYPE), np.array(infos, dtype=INFO_DTYPE))
+            if ignores:
+                self.add_ignore_pairs(np.array(ignores, dtype=np.uint32))
+
+    # --- lifetime ---
+    def destroy(self):
+        if getattr(self, 'handle', None) and self.handle.value:
+            self.lib.avbd_world_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def _check(self, code: int):
+        if code != _abi.AVBD_OK:
+            msg = self.lib.avbd_last_error(self.handle)
+            raise AvbdError(code, msg.decode() if msg else '')
+
+    # --- params (GpuParams3D) ---
+    @property
+    def params(self):
+        p = Params()
+        self._check(self.lib.avbd_get_params(self.handle, ctypes.byref(p)))
+        return p
+
+    @params.setter
+    def params(self, sp):
+        """Accepts a scenes.Params (the reference's SolverParams + GPU flags) or a ctypes Params."""
+        if isinstance(sp, Params):
+            self._check(self.lib.avbd_set_params(self.handle, ctypes.byref(sp)))
+            return
+        flags = (_abi.FLAG_MATCH_NEAREST if sp.match_nearest else 0) | (_abi.FLAG_FACE_BIAS if sp.face_bias else 0) | \
+                (_abi.FLAG_START_AT_REST if sp.start_at_rest else 0) | (_abi.FLAG_MASS_PENALTY if sp.mass_penalty else 0)
+        p = Params(dt=sp.dt, gravity=sp.gravity, alpha=sp.alpha, beta_lin=sp.beta_lin, beta_ang=sp.beta_ang, gamma=sp.gamma,
+                   contact_margin=sp.contact_margin, iterations=sp.iterations, flags=flags)
+        p.up[0], p.up[1], p.up[2] = 0.0, 0.0, 1.0
+        self._check(self.lib.avbd_set_params(self.handle, ctypes.byref(p)))
+
+    # --- scene edits ---
+    def add_bodies(self, records: np.ndarray) -> int:
+        records = np.ascontiguousarray(records, dtype=BODY_DTYPE)
+        first = ctypes.c_uint32()
+        self._check(self.lib.avbd_add_bodies(self.handle, ptr(records), len(records), ctypes.byref(first)))
+        return first.value
+
+    def write_bodies(self, first: int, records: np.ndarray, keep_contacts: bool = False):
+        records = np.ascontiguousarray(records, dtype=BODY_DTYPE)
+        self._check(self.lib.avbd_write_bodies(self.handle, first, ptr(records), len(records), 1 if keep_contacts else 0))
+
+    def add_joints(self, records: np.ndarray, info: np.ndarray) -> int:
+        records = np.ascontiguousarray(records, dtype=JOINT_DTYPE)
+        info = np.ascontiguousarray(info, dtype=INFO_DTYPE)
+        first = ctypes.c_uint32()
+        self._check(self.lib.avbd_add_joints(self.handle, ptr(records), ptr(info), len(records), ctypes.byref(first)))
+        return first.value
+
+    def write_joints(self, first: int, records: np.ndarray, info: np.ndarray):
+        records = np.ascontiguousarray(records, dtype=JOINT_DTYPE)
+        info = np.ascontiguousarray(info, dtype=INFO_DTYPE)
+        self._check(self.lib.avbd_write_joints(self.handle, first, ptr(records), ptr(info), len(records)))
+
+    def release_joints(self, slots):
+        s = np.ascontiguousarray(slots, dtype=np.uint32)
+        self._check(self.lib.avbd_release_joints(self.handle, uptr(s), len(s)))
+
+    def add_ignore_pairs(self, pairs: np.ndarray):
+        p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)
+        self._check(self.lib.avbd_add_ignore_pairs(self.handle, uptr(p), len(p)))
+
+    def set_filters(self, first: int, groups_mask: np.ndarray):
+        g = np.ascontiguousarray(groups_mask, dtype=np.uint32).reshape(-1, 2)
+        self._check(self.lib.avbd_set_filters(self.handle, first, uptr(g), len(g)))
+
+    def seed_contacts(self, manifolds: np.ndarray, contacts: np.ndarray):
+        m = np.ascontiguousarray(manifolds, dtype=MANIFOLD_DTYPE)
+        c = np.ascontiguousarray(contacts, dtype=CONTACT_DTYPE)
+        self._check(self.lib.avbd_seed_contacts(self.handle, ptr(m), len(m), ptr(c), len(c)))
+
+    def set_fixed_colors(self, colors):
+        if colors is None:
+            self._check(self.lib.avbd_set_fixed_colors(self.handle, None, 0))
+        else:
+            c = np.ascontiguousarray(colors, dtype=np.uint32)
+            self._check(self.lib.avbd_set_fixed_colors(self.handle, uptr(c), len(c)))
+        self.fixed_colors = colors
+
+    def sequential_colors(self) -> np.ndarray:
+        """One colour per dynamic body, newest first: the reference's Gauss-Seidel order
+        (GpuSolver3D.sequentialColors, solver.ts:1365-1372). At most 64 dynamic bodies."""
+        b = self.read_bodies()
+        colors = np.full(len(b), NO_COLOR, dtype=np.uint32)
+        nxt = 0
+        for i in range(len(b) - 1, -1, -1):
+            if b[i]['mass'] > 0:
+                colors[i] = nxt
+                nxt += 1
+        if nxt > _abi.MAX_COLORS:
+            raise ValueError(f'sequential_colors: {nxt} dynamic bodies, at most {_abi.MAX_COLORS}')
+        return colors
+
+    # --- stepping ---
+    def step(self, n: int = 1):
+        self._check(self.lib.avbd_step(self.handle, n))
+
+    def synchronize(self):
+        self._check(self.lib.avbd_synchronize(self.handle))
+
+    def enable_timing(self, on: bool = True):
+        self._check(self.lib.avbd_enable_timing(self.handle, 1 if on else 0))
+
+    def last_timing(self):
+        a, b = ctypes.c_float(), ctypes.c_float()
+        self._check(self.lib.avbd_last_timing(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    # --- readbacks ---
+    @property
+    def body_count(self) -> int:
+        n = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_bodies(self.handle, None, 0, ctypes.byref(n)))
+        return n.value
+
+    def read_bodies(self) -> np.ndarray:
+        n = self.body_count
+        out = np.zeros(n, dtype=BODY_DTYPE)
+        cnt = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_bodies(self.handle, ptr(out), n, ctypes.byref(cnt)))
+        return out
+
+    def read_bodies_into(self, out: np.ndarray, sync: bool = True):
+        """Pose readback into caller memory (pinned for overlap), World.read's path."""
+        self._check(self.lib.avbd_read_bodies_async(self.handle, ptr(out), len(out)))
+        if sync:
+            self.synchronize()
+
+    def read_joints(self):
+        n = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_joints(self.handle, None, None, 0, ctypes.byref(n)))
+        recs = np.zeros(n.value, dtype=JOINT_DTYPE)
+        info = np.zeros(n.value, dtype=INFO_DTYPE)
+        self._check(self.lib.avbd_read_joints(self.handle, ptr(recs), ptr(info), n.value, ctypes.byref(n)))
+        return recs, info
+
+    def read_counters(self) -> dict:
+        c = Counters()
+        self._check(self.lib.avbd_read_counters(self.handle, ctypes.byref(c)))
+        return c.as_dict()
+
+    def read_contacts(self):
+        nm, nc = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.lib.avbd_read_contacts(self.handle, None, 0, ctypes.byref(nm), None, 0, ctypes.byref(nc)))
+        m = np.zeros(nm.value, dtype=MANIFOLD_DTYPE)
+        c = np.zeros(nc.value, dtype=CONTACT_DTYPE)
+        self._check(self.lib.avbd_read_contacts(self.handle, ptr(m), nm.value, ctypes.byref(nm), ptr(c), nc.value, ctypes.byref(nc)))
+        return m, c
+
+    def read_contact_list(self) -> list[dict]:
+        """readContactList (solver.ts:2311-2346): every point with its pair's bodies and normal."""
+        m, c = self.read_contacts()
+        out = []
+        for rec in m:
+            for k in range(int(rec['first']), int(rec['first'] + rec['count'])):
+                key = int(c[k]['key'])
+                out.append({'a': int(rec['a']), 'b': int(rec['b']), 'feature': key & ~_abi.STICK_BIT, 'stick': bool(key & _abi.STICK_BIT),
+                            'rA': c[k]['r_a'].astype(np.float64), 'rB': c[k]['r_b'].astype(np.float64), 'pen': c[k]['pen'].astype(np.float64),
+                            'lam': c[k]['lam'].astype(np.float64), 'normal': rec['normal'].astype(np.float64)})
+        return out
+
+    def read_pairs(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_pairs(self.handle, None, 0, ctypes.byref(n)))
+        out = np.zeros(2 * n.value, dtype=np.uint32)
+        self._check(self.lib.avbd_read_pairs(self.handle, uptr(out), n.value, ctypes.byref(n)))
+        return out.reshape(-1, 2)
+
+    def read_colors(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_colors(self.handle, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=np.uint32)
+        self._check(self.lib.avbd_read_colors(self.handle, uptr(out), n.value, ctypes.byref(n)))
+        return out
+
+
+def device_info(device: int = 0):
+    lib = _abi.load()
+    name = ctypes.create_string_buffer(256)
+    sms = ctypes.c_int()
+    code = lib.avbd_device_info(device, name, 256, ctypes.byref(sms))
+    if code != _abi.AVBD_OK:
+        return None
+    return name.value.decode(), sms.value

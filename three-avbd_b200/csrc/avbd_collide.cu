@@ -1,0 +1,739 @@
+// Collision phase of the B200 AVBD step: last step's pairs into the warm-start hash, cell keys,
+// a stable LSD radix sort of (cell hash, body), cell ranges, pair emission, and the narrowphase.
+//
+// This file is compiled with --fmad=false: every product and sum is rounded on its own, in the
+// operation order of the reference's WGSL (src/avbd3d/gpu/wgsl-collision.ts), so the pair tests
+// and the SAT axis choice (hence the feature keys) agree bit for bit with an f32 CPU
+// restatement compiled with -ffp-contract=off.
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
+#include "avbd_device.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace avbd {
+
+constexpr int RADIX_BITS = 8, RADIX = 1 << RADIX_BITS, SORT_THREADS = 256, SORT_ITEMS = 8, SORT_TILE = SORT_THREADS * SORT_ITEMS;
+constexpr int GS_BLOCKS = 148 * 8;  // grid-stride kernels over device-side counts
+
+__device__ inline bool enabled(const DWorld& w, uint32_t i) {
+  uint32_t f = (uint32_t)w.ipos[i].w;
+  return (f & 2u) == 0u;
+}
+
+// --- begin: rotate counters (wgsl-collision.ts:96-107) -------------------------------------------
+__global__ void k_begin(DWorld w, StepParams p) {
+  uint32_t* c = w.counters;
+  uint32_t pairs = c[C_PAIRS];
+  c[C_PREV_PAIRS] = pairs < p.pairCap ? pairs : p.pairCap;
+  c[C_PAIRS] = 0;
+  c[C_CONTACTS] = 0;
+  c[C_MANIFOLDS] = 0;
+  c[C_OVERFLOW] = 0;
+  c[C_CLASHES] = 0;
+  c[C_COLORS] = 0;
+  c[C_ROUNDS] = 0;
+  c[C_ERROR] = 0;
+  for (int k = 0; k < 2 * MAX_ROUND_PAIRS + 2; k++) c[C_PENDING + k] = 0;
+}
+
+// --- last step's pairs into the hash table (wgsl-collision.ts:354-368), compare-and-swap probing ---
+__global__ void k_hash_insert(DWorld w, StepParams p) {
+  const int prev = 1 - p.cur;
+  const uint32_t count = w.counters[C_PREV_PAIRS];
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < count; m += gridDim.x * blockDim.x) {
+    uint4 ids = w.mIds[prev][m];
+    if ((ids.w & 15u) == 0u) continue;
+    // Rewritten slots have no contact history
+    if (w.ipos[ids.x].w != 0.0f || w.ipos[ids.y].w != 0.0f) continue;
+    uint32_t h = pairHash(ids.x, ids.y) & p.hashMask;
+    for (uint32_t probe = 0; probe <= p.hashMask; probe++) {
+      if (atomicCAS(&w.hash[h], 0u, m + 1u) == 0u) break;
+      h = (h + 1u) & p.hashMask;
+    }
+  }
+}
+
+__device__ inline int hashFind(const DWorld& w, const StepParams& p, uint32_t a, uint32_t b) {
+  const int prev = 1 - p.cur;
+  uint32_t h = pairHash(a, b) & p.hashMask;
+  for (uint32_t probe = 0; probe <= p.hashMask; probe++) {
+    uint32_t v = w.hash[h];
+    if (v == 0u) return -1;
+    uint4 ids = w.mIds[prev][v - 1u];
+    if (ids.x == a && ids.y == b) return int(v - 1u);
+    h = (h + 1u) & p.hashMask;
+  }
+  return -1;
+}
+
+// --- grid keys: cellHash (wgsl-collision.ts:121-128), one level -----------------------------------
+__device__ inline int4 cellOf(float3 x, float size) {
+  return make_int4((int)floorf(x.x / size), (int)floorf(x.y / size), (int)floorf(x.z / size), 0);
+}
+__device__ inline uint32_t cellHash(int4 c, uint32_t mask) {
+  return (((uint32_t)c.x * 73856093u) ^ ((uint32_t)c.y * 19349663u) ^ ((uint32_t)c.z * 83492791u)) & mask;
+}
+
+__global__ void k_cell_keys(DWorld w, StepParams p) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n) return;
+  bool small = enabled(w, i) && w.moment[i].w <= p.largeThreshold;
+  int4 c = cellOf(f3(w.pos[i]), p.cellSize);
+  w.cell[i] = c;
+  w.keyA[i] = small ? cellHash(c, p.tableMask) : p.tableMask + 1u;  // large and disabled bodies sort last
+  w.valA[i] = i;
+}
+
+// --- stable LSD radix sort of (key, value) -----------------------------------------------------------
+// Per pass: per-tile digit histogram, one exclusive scan over (digit, tile), and a stable scatter
+// ranking each tile's keys with warp match + per-warp digit counts.
+__global__ void __launch_bounds__(SORT_THREADS) k_radix_hist(const uint32_t* keys, uint32_t n, int shift, uint32_t* hist, uint32_t tiles) {
+  __shared__ uint32_t counts[RADIX];
+  counts[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t base = blockIdx.x * SORT_TILE;
+  for (int r = 0; r < SORT_ITEMS; r++) {
+    uint32_t i = base + r * SORT_THREADS + threadIdx.x;
+    if (i < n) atomicAdd(&counts[(keys[i] >> shift) & (RADIX - 1)], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * tiles + blockIdx.x] = counts[threadIdx.x];
+}
+
+// Exclusive scan of `len` words in place by one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_single(uint32_t* data, uint32_t len) {
+  __shared__ uint32_t warpSums[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < len; base += 1024) {
+    uint32_t i = base + threadIdx.x;
+    uint32_t v = i < len ? data[i] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t s = warpSums[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      warpSums[lane] = s;
+    }
+    __syncthreads();
+    uint32_t incl = x + (warp > 0 ? warpSums[warp - 1] : 0u) + carry;
+    if (i < len) data[i] = incl - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = incl;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_radix_scatter(const uint32_t* keysIn, const uint32_t* valsIn, uint32_t* keysOut, uint32_t* valsOut,
+                                                                uint32_t n, int shift, const uint32_t* hist, uint32_t tiles) {
+  __shared__ uint32_t running[RADIX];
+  __shared__ uint32_t warpCount[SORT_THREADS / 32][RADIX];
+  __shared__ uint32_t tileCount[RADIX];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  running[threadIdx.x] = hist[threadIdx.x * tiles + blockIdx.x];
+  uint32_t base = blockIdx.x * SORT_TILE;
+  for (int r = 0; r < SORT_ITEMS; r++) {
+    for (int k = 0; k < SORT_THREADS / 32; k++) warpCount[k][threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t i = base + r * SORT_THREADS + threadIdx.x;
+    bool live = i < n;
+    uint32_t key = live ? keysIn[i] : 0u;
+    uint32_t digit = live ? (key >> shift) & (RADIX - 1) : 0xffffffffu;
+    uint32_t peers = __match_any_sync(0xffffffffu, digit);
+    uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    if (live && rank == 0) warpCount[warp][digit] = __popc(peers);
+    __syncthreads();
+    {
+      uint32_t s = 0;
+      for (int k = 0; k < SORT_THREADS / 32; k++) {
+        uint32_t c = warpCount[k][threadIdx.x];
+        warpCount[k][threadIdx.x] = s;
+        s += c;
+      }
+      tileCount[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (live) {
+      uint32_t pos = running[digit] + warpCount[warp][digit] + rank;
+      keysOut[pos] = key;
+      valsOut[pos] = valsIn[i];
+    }
+    __syncthreads();
+    running[threadIdx.x] += tileCount[threadIdx.x];
+  }
+}
+
+// --- cell ranges in the sorted order -------------------------------------------------------------------
+__global__ void k_cell_ranges(const uint32_t* keys, uint32_t n, uint32_t* start, uint32_t* end, uint32_t sentinel) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k = keys[i];
+  if (k == sentinel) return;
+  if (i == 0 || keys[i - 1] != k) start[k] = i;
+  if (i == n - 1 || keys[i + 1] != k) end[k] = i + 1;
+}
+
+// --- pair tests (wgsl-collision.ts:150-234) ------------------------------------------------------------
+struct Shape {
+  float3 ax0, ax1, ax2, h;
+  bool sphere;
+};
+__device__ inline Shape shapeOf(const DWorld& w, uint32_t i) {
+  float4 q = w.rot[i];
+  Shape s;
+  float4 sz = w.size[i];
+  s.h = make_float3(sz.x * 0.5f, sz.y * 0.5f, sz.z * 0.5f);
+  s.sphere = w.avel[i].w == SHAPE_SPHERE_F;
+  s.ax0 = qrotate(q, make_float3(1.0f, 0.0f, 0.0f));
+  s.ax1 = qrotate(q, make_float3(0.0f, 1.0f, 0.0f));
+  s.ax2 = qrotate(q, make_float3(0.0f, 0.0f, 1.0f));
+  return s;
+}
+__device__ inline float extentOf(const Shape& s, float3 n) {
+  if (s.sphere) return s.h.x;
+  return s.h.x * fabsf(dot3(n, s.ax0)) + s.h.y * fabsf(dot3(n, s.ax1)) + s.h.z * fabsf(dot3(n, s.ax2));
+}
+__device__ inline float3 aabbHalf(const Shape& s) {
+  if (s.sphere) return make_float3(s.h.x, s.h.x, s.h.x);
+  return abs3(s.ax0) * s.h.x + abs3(s.ax1) * s.h.y + abs3(s.ax2) * s.h.z;
+}
+__device__ inline bool faceSeparated(const Shape& A, const Shape& B, float3 d) {
+  const float3 a[3] = {A.ax0, A.ax1, A.ax2};
+  const float3 b[3] = {B.ax0, B.ax1, B.ax2};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (fabsf(dot3(d, a[k])) - extentOf(A, a[k]) - extentOf(B, a[k]) > 1e-3f) return true;
+    if (fabsf(dot3(d, b[k])) - extentOf(A, b[k]) - extentOf(B, b[k]) > 1e-3f) return true;
+  }
+  return false;
+}
+
+struct Probe {
+  uint32_t index;
+  float3 pos, aabb;
+  float radius;
+  bool dynamic;
+  uint2 filter;
+  Shape shape;
+};
+__device__ inline Probe probeOf(const DWorld& w, uint32_t i) {
+  Probe P;
+  P.index = i;
+  P.pos = f3(w.pos[i]);
+  P.radius = w.moment[i].w;
+  P.shape = shapeOf(w, i);
+  P.aabb = aabbHalf(P.shape);
+  P.dynamic = w.size[i].w > 0.0f;
+  P.filter = w.filters[i];
+  return P;
+}
+
+// No-collide list, binary search (wgsl-collision.ts:53-76)
+__device__ inline bool ignored(const DWorld& w, const StepParams& p, uint32_t hi, uint32_t lo) {
+  const uint32_t* t = w.nocollide;
+  uint32_t first = 0, count = p.nNoCollide;
+  while (count > 0u) {
+    uint32_t step = count / 2u, mid = first + step;
+    uint32_t mh = t[3u * mid], ml = t[3u * mid + 1u];
+    if (mh < hi || (mh == hi && ml < lo)) {
+      first = mid + 1u;
+      count -= step + 1u;
+    } else {
+      count = step;
+    }
+  }
+  for (uint32_t k = first; k < p.nNoCollide; k++) {
+    if (t[3u * k] != hi || t[3u * k + 1u] != lo) break;
+    uint32_t j = t[3u * k + 2u];
+    if (j == 0xffffffffu) return true;
+    float4 pl = w.joint[j * JOINT_VEC4 + J_PEN_LIN], pa = w.joint[j * JOINT_VEC4 + J_PEN_ANG];
+    if (pl.w != 0.0f || pa.w != 0.0f) return true;
+  }
+  return false;
+}
+
+__device__ inline void emitPair(const DWorld& w, const StepParams& p, uint32_t a, uint32_t b) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(&w.counters[C_PAIRS], g.size());
+  base = g.shfl(base, 0);
+  uint32_t slot = base + g.thread_rank();
+  if (slot >= p.pairCap) {
+    atomicOr(&w.counters[C_OVERFLOW], 1u);
+    return;
+  }
+  w.pairs[slot] = make_uint2(a, b);
+}
+
+__device__ inline void testPair(const DWorld& w, const StepParams& p, const Probe& P, uint32_t j) {
+  if (!enabled(w, j)) return;
+  if (!P.dynamic && w.size[j].w <= 0.0f) return;
+  uint2 fj = w.filters[j];
+  if ((P.filter.x & fj.y) == 0u || (fj.x & P.filter.y) == 0u) return;
+  float3 d = P.pos - f3(w.pos[j]);
+  float r = P.radius + w.moment[j].w;
+  if (dot3(d, d) > r * r) return;
+  Shape B = shapeOf(w, j);
+  float3 bh = aabbHalf(B);
+  if (fabsf(d.x) > P.aabb.x + bh.x + 1e-4f || fabsf(d.y) > P.aabb.y + bh.y + 1e-4f || fabsf(d.z) > P.aabb.z + bh.z + 1e-4f) return;
+  if (faceSeparated(P.shape, B, d)) return;
+  uint32_t a = max(P.index, j), b = min(P.index, j);
+  if (ignored(w, p, a, b)) return;
+  emitPair(w, p, a, b);
+}
+
+// findPairs + findFixedLarge (wgsl-collision.ts:242-323): a dynamic body probes the 27 cells around
+// it (same-level dynamic pairs belong to the higher index, fixed pairs to the mover) and the large
+// bodies; a small fixed body probes the large dynamic ones.
+__global__ void __launch_bounds__(128) k_find_pairs(DWorld w, StepParams p, const uint32_t* sortedVals) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n || !enabled(w, i)) return;
+  bool dyn = w.size[i].w > 0.0f;
+  bool small = w.moment[i].w <= p.largeThreshold;
+  if (!dyn) {
+    if (!small || p.anyDynamicLarge == 0u) return;
+    Probe P = probeOf(w, i);
+    for (uint32_t k = 0; k < p.nLarge; k++) {
+      uint32_t l = w.large[k];
+      if (!enabled(w, l) || w.size[l].w <= 0.0f) continue;
+      testPair(w, p, P, l);
+    }
+    return;
+  }
+  Probe P = probeOf(w, i);
+  if (small) {
+    int4 c = w.cell[i];
+    for (int oz = -1; oz <= 1; oz++)
+      for (int oy = -1; oy <= 1; oy++)
+        for (int ox = -1; ox <= 1; ox++) {
+          int4 cc = make_int4(c.x + ox, c.y + oy, c.z + oz, 0);
+          uint32_t h = cellHash(cc, p.tableMask);
+          uint32_t end = w.cellEnd[h];
+          for (uint32_t k = w.cellStart[h]; k < end; k++) {
+            uint32_t j = sortedVals[k];
+            if (j == i || (j > i && w.size[j].w > 0.0f)) continue;
+            int4 cj = w.cell[j];
+            if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
+            testPair(w, p, P, j);
+          }
+        }
+  }
+  for (uint32_t k = 0; k < p.nLarge; k++) {
+    uint32_t l = w.large[k];
+    if (l == i || (!small && l < i && w.size[l].w > 0.0f)) continue;
+    testPair(w, p, P, l);
+  }
+}
+
+// --- narrowphase: box SAT + clipping (wgsl-collision.ts:385-599, ref/collide.ts) ---------------------
+constexpr float SAT_AXIS_EPSILON = 1.0e-6f, PLANE_EPSILON = 1.0e-5f, CONTACT_MERGE_DIST_SQ = 1.0e-6f;
+constexpr uint32_t AXIS_FACE_A = 0, AXIS_FACE_B = 1, AXIS_EDGE = 2;
+
+struct Box {
+  float3 c, h;
+  float3 ax[3];
+};
+struct Sat {
+  uint32_t kind, ia, ib;
+  float sep;
+  float3 n;
+  bool valid;
+};
+struct Found {
+  uint32_t feature[MAX_CONTACTS];
+  float3 xA[MAX_CONTACTS], xB[MAX_CONTACTS];
+  uint32_t count;
+};
+
+__device__ inline Box makeBox(const DWorld& w, uint32_t i) {
+  float4 q = w.rot[i];
+  float4 sz = w.size[i];
+  Box b;
+  b.c = f3(w.pos[i]);
+  b.h = make_float3(sz.x * 0.5f, sz.y * 0.5f, sz.z * 0.5f);
+  b.ax[0] = qrotate(q, make_float3(1.0f, 0.0f, 0.0f));
+  b.ax[1] = qrotate(q, make_float3(0.0f, 1.0f, 0.0f));
+  b.ax[2] = qrotate(q, make_float3(0.0f, 0.0f, 1.0f));
+  return b;
+}
+__device__ inline float projRadius(const Box& b, float3 n) {
+  return b.h.x * fabsf(dot3(n, b.ax[0])) + b.h.y * fabsf(dot3(n, b.ax[1])) + b.h.z * fabsf(dot3(n, b.ax[2]));
+}
+__device__ inline bool testAxis(const Box& A, const Box& B, float3 delta, float3 axis, uint32_t kind, uint32_t ia, uint32_t ib, Sat& best) {
+  float lenSq = dot3(axis, axis);
+  if (lenSq < SAT_AXIS_EPSILON) return true;
+  float invLen = 1.0f / sqrtf(lenSq);
+  float3 n = axis * invLen;
+  if (dot3(n, delta) < 0.0f) n = -n;
+  float distance = fabsf(dot3(delta, n));
+  float rA = projRadius(A, n);
+  float rB = projRadius(B, n);
+  float sep = distance - (rA + rB);
+  if (sep > 0.0f) return false;
+  if (!best.valid || sep > best.sep) {
+    best.valid = true;
+    best.kind = kind;
+    best.ia = ia;
+    best.ib = ib;
+    best.sep = sep;
+    best.n = n;
+  }
+  return true;
+}
+__device__ inline float3 support(const Box& b, float3 dir) {
+  float sx = dot3(dir, b.ax[0]) >= 0.0f ? 1.0f : -1.0f;
+  float sy = dot3(dir, b.ax[1]) >= 0.0f ? 1.0f : -1.0f;
+  float sz = dot3(dir, b.ax[2]) >= 0.0f ? 1.0f : -1.0f;
+  float3 p = b.c + b.ax[0] * (b.h.x * sx);
+  p = p + b.ax[1] * (b.h.y * sy);
+  return p + b.ax[2] * (b.h.z * sz);
+}
+__device__ inline void addFound(Found& f, float3 xA, float3 xB, uint32_t feature) {
+  float3 mid = (xA + xB) * 0.5f;
+  for (uint32_t i = 0; i < f.count; i++) {
+    float3 m = (f.xA[i] + f.xB[i]) * 0.5f;
+    float3 d = mid - m;
+    if (dot3(d, d) < CONTACT_MERGE_DIST_SQ) return;
+  }
+  if (f.count >= MAX_CONTACTS) return;
+  f.feature[f.count] = feature;
+  f.xA[f.count] = xA;
+  f.xB[f.count] = xB;
+  f.count++;
+}
+// Sutherland-Hodgman against dot(pn, x) <= offset (a quad clipped by four planes keeps <= 8 vertices)
+__device__ inline uint32_t clipPlane(const float3* src, uint32_t n, float3* dst, float3 pn, float offset) {
+  if (n == 0u) return 0u;
+  uint32_t count = 0;
+  float3 a = src[n - 1u];
+  float da = dot3(pn, a) - offset;
+  for (uint32_t i = 0; i < n; i++) {
+    float3 b = src[i];
+    float db = dot3(pn, b) - offset;
+    bool aIn = da <= PLANE_EPSILON, bIn = db <= PLANE_EPSILON;
+    if (aIn != bIn) {
+      float t = 0.0f;
+      float denom = da - db;
+      if (fabsf(denom) > SAT_AXIS_EPSILON) t = fminf(fmaxf(da / denom, 0.0f), 1.0f);
+      if (count < 8u) dst[count++] = a + (b - a) * t;
+    }
+    if (bIn && count < 8u) dst[count++] = b;
+    a = b;
+    da = db;
+  }
+  return count;
+}
+__device__ inline uint32_t faceU(uint32_t k) { return k == 0u ? 1u : 0u; }
+__device__ inline uint32_t faceV(uint32_t k) { return k != 2u ? 2u : 1u; }
+
+__device__ void faceManifold(const Box& A, const Box& B, bool refIsA, uint32_t refAxis, float3 nAB, Found& found) {
+  const Box& R = refIsA ? A : B;
+  const Box& I = refIsA ? B : A;
+  float3 outward = refIsA ? nAB : -nAB;
+  float rs = dot3(outward, R.ax[refAxis]) >= 0.0f ? 1.0f : -1.0f;
+  float3 rn = R.ax[refAxis] * rs;
+  float3 rc = R.c + rn * comp(R.h, refAxis);
+  float3 ru = R.ax[faceU(refAxis)], rv = R.ax[faceV(refAxis)];
+  float eu = comp(R.h, faceU(refAxis)), ev = comp(R.h, faceV(refAxis));
+  uint32_t incAxis = 0;
+  float bestDot = -3.4028234663852886e38f;
+  for (uint32_t k = 0; k < 3u; k++) {
+    float d = fabsf(dot3(I.ax[k], rn));
+    if (d > bestDot) {
+      bestDot = d;
+      incAxis = k;
+    }
+  }
+  float is = dot3(I.ax[incAxis], rn) > 0.0f ? -1.0f : 1.0f;
+  float3 fn = I.ax[incAxis] * is;
+  float3 fc = I.c + fn * comp(I.h, incAxis);
+  float3 u = I.ax[faceU(incAxis)], v = I.ax[faceV(incAxis)];
+  float eU = comp(I.h, faceU(incAxis)), eV = comp(I.h, faceV(incAxis));
+  float3 poly[8], tmp[8];
+  // vert(su, sv) = fc + u (su eU) + v (sv eV)
+  poly[0] = (fc + u * (1.0f * eU)) + v * (1.0f * eV);
+  poly[1] = (fc + u * (-1.0f * eU)) + v * (1.0f * eV);
+  poly[2] = (fc + u * (-1.0f * eU)) + v * (-1.0f * eV);
+  poly[3] = (fc + u * (1.0f * eU)) + v * (-1.0f * eV);
+  uint32_t n = 4;
+  float3 nru = -ru, nrv = -rv;
+  n = clipPlane(poly, n, tmp, ru, dot3(ru, rc) + eu);
+  n = clipPlane(tmp, n, poly, nru, dot3(nru, rc) + eu);
+  n = clipPlane(poly, n, tmp, rv, dot3(rv, rc) + ev);
+  n = clipPlane(tmp, n, poly, nrv, dot3(nrv, rc) + ev);
+  if (n == 0u) return;
+  uint32_t prefix = ((refIsA ? AXIS_FACE_A : AXIS_FACE_B) << 24) | (refAxis << 16) | (incAxis << 8);
+  for (uint32_t i = 0; i < n && found.count < MAX_CONTACTS; i++) {
+    float3 q = poly[i];
+    float dist = dot3(q - rc, rn);
+    if (dist > PLANE_EPSILON) continue;
+    float3 onRef = q + rn * (-dist);
+    addFound(found, refIsA ? onRef : q, refIsA ? q : onRef, prefix | i);
+  }
+  if (found.count == 0u) addFound(found, support(A, nAB), support(B, -nAB), prefix);
+}
+__device__ inline void supportEdge(const Box& b, uint32_t k, float3 dir, float3& e0, float3& e1) {
+  uint32_t k1 = (k + 1u) % 3u, k2 = (k + 2u) % 3u;
+  float s1 = dot3(dir, b.ax[k1]) >= 0.0f ? 1.0f : -1.0f;
+  float s2 = dot3(dir, b.ax[k2]) >= 0.0f ? 1.0f : -1.0f;
+  float3 c = b.c + b.ax[k1] * (comp(b.h, k1) * s1);
+  c = c + b.ax[k2] * (comp(b.h, k2) * s2);
+  float3 e = b.ax[k] * comp(b.h, k);
+  e0 = c - e;
+  e1 = c + e;
+}
+__device__ void edgeContact(const Box& A, const Box& B, uint32_t ia, uint32_t ib, float3 nAB, Found& found) {
+  float3 p0, p1, q0, q1;
+  supportEdge(A, ia, nAB, p0, p1);
+  supportEdge(B, ib, -nAB, q0, q1);
+  float3 d1 = p1 - p0, d2 = q1 - q0, r = p0 - q0;
+  float a = dot3(d1, d1), e = dot3(d2, d2), f = dot3(d2, r);
+  float s = 0.0f, t = 0.0f;
+  if (a <= SAT_AXIS_EPSILON && e <= SAT_AXIS_EPSILON) {
+  } else if (a <= SAT_AXIS_EPSILON) {
+    t = fminf(fmaxf(f / e, 0.0f), 1.0f);
+  } else {
+    float c = dot3(d1, r);
+    if (e <= SAT_AXIS_EPSILON) {
+      s = fminf(fmaxf(-c / a, 0.0f), 1.0f);
+    } else {
+      float b = dot3(d1, d2);
+      float denom = a * e - b * b;
+      if (fabsf(denom) > SAT_AXIS_EPSILON) s = fminf(fmaxf((b * f - c * e) / denom, 0.0f), 1.0f);
+      t = (b * s + f) / e;
+      if (t < 0.0f) {
+        t = 0.0f;
+        s = fminf(fmaxf(-c / a, 0.0f), 1.0f);
+      } else if (t > 1.0f) {
+        t = 1.0f;
+        s = fminf(fmaxf((b - c) / a, 0.0f), 1.0f);
+      }
+    }
+  }
+  uint32_t key = (AXIS_EDGE << 24) | (ia << 8) | ib;
+  addFound(found, p0 + d1 * s, q0 + d2 * t, key);
+  if (found.count == 0u) addFound(found, support(A, nAB), support(B, -nAB), key);
+}
+// collide (wgsl-collision.ts:656-683); sat.n points from A towards B
+__device__ void collideBoxes(const Box& A, const Box& B, bool faceBias, Sat& sat, Found& found) {
+  float3 delta = B.c - A.c;
+  Sat face, edge;
+  face.valid = false;
+  edge.valid = false;
+  face.sep = 0.0f;
+  edge.sep = 0.0f;
+  for (uint32_t i = 0; i < 3u; i++)
+    if (!testAxis(A, B, delta, A.ax[i], AXIS_FACE_A, i, 0u, face)) return;
+  for (uint32_t i = 0; i < 3u; i++)
+    if (!testAxis(A, B, delta, B.ax[i], AXIS_FACE_B, 0u, i, face)) return;
+  for (uint32_t i = 0; i < 3u; i++)
+    for (uint32_t j = 0; j < 3u; j++)
+      if (!testAxis(A, B, delta, cross3(A.ax[i], B.ax[j]), AXIS_EDGE, i, j, edge)) return;
+  if (!face.valid) return;
+  Sat best = face;
+  if (edge.valid) {
+    bool edgeWins = 0.95f * edge.sep > face.sep + 0.01f;
+    if (faceBias) edgeWins = edge.sep > 0.95f * face.sep + 0.01f;
+    if (edgeWins) best = edge;
+  }
+  sat = best;
+  if (best.kind == AXIS_EDGE) edgeContact(A, B, best.ia, best.ib, best.n, found);
+  else faceManifold(A, B, best.kind == AXIS_FACE_A, best.kind == AXIS_FACE_A ? best.ia : best.ib, best.n, found);
+}
+// Spheres (wgsl-collision.ts:604-653)
+__device__ void sphereSphere(const Box& A, const Box& B, Sat& sat, Found& found) {
+  float3 d = B.c - A.c;
+  float dist = sqrtf(dot3(d, d));
+  if (dist > A.h.x + B.h.x) return;
+  float3 n = make_float3(0.0f, 0.0f, 1.0f);
+  if (dist > 0.0f) n = d / dist;
+  sat.n = n;
+  addFound(found, A.c + n * A.h.x, B.c - n * B.h.x, SPHERE_FEATURE);
+}
+__device__ bool sphereBox(const Box& S, const Box& X, float4 qX, float3& onSphere, float3& onBox, float3& nOut) {
+  float3 p = qrotate(qconj(qX), S.c - X.c);
+  float3 q = make_float3(fminf(fmaxf(p.x, -X.h.x), X.h.x), fminf(fmaxf(p.y, -X.h.y), X.h.y), fminf(fmaxf(p.z, -X.h.z), X.h.z));
+  float r = S.h.x;
+  float3 nLocal;
+  float3 ob = q;
+  if (p.x != q.x || p.y != q.y || p.z != q.z) {
+    float3 d = p - q;
+    float dist = sqrtf(dot3(d, d));
+    if (dist > r) return false;
+    nLocal = d / dist;
+  } else {
+    float3 depth = X.h - abs3(p);
+    int k = 0;
+    if (depth.y < comp(depth, k)) k = 1;
+    if (depth.z < comp(depth, k)) k = 2;
+    float s = comp(p, k) >= 0.0f ? 1.0f : -1.0f;
+    nLocal = make_float3(k == 0 ? s : 0.0f, k == 1 ? s : 0.0f, k == 2 ? s : 0.0f);
+    if (k == 0) ob.x = s * X.h.x;
+    else if (k == 1) ob.y = s * X.h.y;
+    else ob.z = s * X.h.z;
+  }
+  float3 n = qrotate(qX, nLocal);
+  nOut = -n;
+  onBox = X.c + qrotate(qX, ob);
+  onSphere = S.c - n * r;
+  return true;
+}
+
+// Contact pair p: manifold slot p with its points at 8p .. 8p+count-1, warm-started from last step's
+// pair (a, b) by feature key (wgsl-collision.ts:767-892).
+__global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
+  const int cur = p.cur, prev = 1 - cur;
+  uint32_t total = w.counters[C_PAIRS];
+  if (total > p.pairCap) total = p.pairCap;
+  for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < total; pi += gridDim.x * blockDim.x) {
+    uint2 pr = w.pairs[pi];
+    uint32_t a = pr.x, b = pr.y;
+    Box A = makeBox(w, a), B = makeBox(w, b);
+    Sat sat;
+    sat.n = make_float3(0.0f, 0.0f, 0.0f);
+    sat.valid = false;
+    Found found;
+    found.count = 0;
+    bool sphereA = w.avel[a].w == SHAPE_SPHERE_F, sphereB = w.avel[b].w == SHAPE_SPHERE_F;
+    float4 qA = w.rot[a], qB = w.rot[b];
+    if (sphereA && sphereB) {
+      sphereSphere(A, B, sat, found);
+    } else if (sphereA || sphereB) {
+      float3 onS, onX, nn;
+      if (sphereA) {
+        bool hit = sphereBox(A, B, qB, onS, onX, nn);
+        sat.n = nn;
+        if (hit) addFound(found, onS, onX, SPHERE_FEATURE);
+      } else {
+        bool hit = sphereBox(B, A, qA, onS, onX, nn);
+        sat.n = -nn;
+        if (hit) addFound(found, onX, onS, SPHERE_FEATURE);
+      }
+    } else {
+      collideBoxes(A, B, (p.flags & FLAG_FACE_BIAS) != 0u, sat, found);
+    }
+    uint32_t count = found.count;
+    float3 n = -sat.n;
+    float fa = w.pos[a].w, fb = w.pos[b].w;
+    w.mIds[cur][pi] = make_uint4(a, b, pi * MAX_CONTACTS, count | (p.step << 4));
+    w.mGeo[cur][pi] = make_float4(n.x, n.y, n.z, sqrtf(fa * fb));
+    {
+      cg::coalesced_group g = cg::coalesced_threads();
+      uint32_t pts = cg::reduce(g, count, cg::plus<uint32_t>());
+      uint32_t nonEmpty = cg::reduce(g, count > 0u ? 1u : 0u, cg::plus<uint32_t>());
+      if (g.thread_rank() == 0) {
+        atomicAdd(&w.counters[C_CONTACTS], pts);
+        atomicAdd(&w.counters[C_MANIFOLDS], nonEmpty);
+      }
+    }
+    if (count == 0u) continue;
+    float3 t1, t2;
+    orthonormal(n, t1, t2);
+    bool anySphere = sphereA || sphereB;
+    uint32_t prevFirst = 0, prevCount = 0;
+    int pm = hashFind(w, p, a, b);
+    if (pm >= 0) {
+      uint4 pid = w.mIds[prev][pm];
+      prevFirst = pid.z;
+      prevCount = min(pid.w & 15u, (uint32_t)MAX_CONTACTS);
+    }
+    bool matchNearest = (p.flags & FLAG_MATCH_NEAREST) != 0u;
+    float minSide = fminf(fminf(fminf(A.h.x, A.h.y), A.h.z), fminf(fminf(B.h.x, B.h.y), B.h.z)) * 2.0f;
+    float penaltyMin = PENALTY_MIN;
+    if (p.flags & FLAG_MASS_PENALTY) {
+      float mA = w.size[a].w <= 0.0f ? 3.4e38f : w.size[a].w;
+      float mB = w.size[b].w <= 0.0f ? 3.4e38f : w.size[b].w;
+      penaltyMin = fminf(fmaxf(fminf(mA, mB) / (p.dt * p.dt), PENALTY_MIN), PENALTY_MAX);
+    }
+    float3 cA = A.c, cB = B.c;
+    for (uint32_t i = 0; i < count; i++) {
+      float3 rA = qrotate(qconj(qA), found.xA[i] - cA);
+      float3 rB = qrotate(qconj(qB), found.xB[i] - cB);
+      float3 pen = make_float3(0.0f, 0.0f, 0.0f), lam = make_float3(0.0f, 0.0f, 0.0f);
+      uint32_t stick = 0;
+      int j = -1;
+      for (uint32_t c = prevFirst; c < prevFirst + prevCount; c++) {
+        if ((__float_as_uint(w.cRA[prev][c].w) & ~STICK_BIT) == found.feature[i]) {
+          j = int(c);
+          break;
+        }
+      }
+      if (j < 0 && matchNearest) {
+        float bestDist = NEAREST_FRACTION * minSide;
+        for (uint32_t c = prevFirst; c < prevFirst + prevCount; c++) {
+          float3 d = f3(w.cRA[prev][c]) - rA;
+          float dist = sqrtf(dot3(d, d));
+          if (dist <= bestDist) {
+            bestDist = dist;
+            j = int(c);
+          }
+        }
+      }
+      if (j >= 0) {
+        float4 pra = w.cRA[prev][j];
+        pen = f3(w.cPen[prev][j]);
+        lam = f3(w.cLam[prev][j]);
+        stick = __float_as_uint(pra.w) & STICK_BIT;
+        if (stick != 0u && !anySphere) {
+          rA = f3(pra);
+          rB = f3(w.cRB[prev][j]);
+        }
+      }
+      float3 d = (qrotate(qA, rA) + cA) - (qrotate(qB, rB) + cB);
+      float c0x = dot3(n, d) + p.margin, c0y = dot3(t1, d), c0z = dot3(t2, d);
+      lam = lam * p.alpha * p.gamma;
+      pen = make_float3(fminf(fmaxf(pen.x * p.gamma, PENALTY_MIN), PENALTY_MAX), fminf(fmaxf(pen.y * p.gamma, PENALTY_MIN), PENALTY_MAX),
+                        fminf(fmaxf(pen.z * p.gamma, PENALTY_MIN), PENALTY_MAX));
+      pen.x = fmaxf(pen.x, penaltyMin);
+      uint32_t slot = pi * MAX_CONTACTS + i;
+      w.cRA[cur][slot] = make_float4(rA.x, rA.y, rA.z, __uint_as_float(found.feature[i] | stick));
+      w.cRB[cur][slot] = make_float4(rB.x, rB.y, rB.z, c0x);
+      w.cPen[cur][slot] = make_float4(pen.x, pen.y, pen.z, c0y);
+      w.cLam[cur][slot] = make_float4(lam.x, lam.y, lam.z, c0z);
+    }
+  }
+}
+
+// Host: the collision phase, enqueued on `s`.
+void launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s) {
+  const uint32_t n = p.n;
+  k_begin<<<1, 1, 0, s>>>(w, p);
+  cudaMemsetAsync(w.hash, 0, (size_t(p.hashMask) + 1) * 4, s);
+  k_hash_insert<<<GS_BLOCKS, 256, 0, s>>>(w, p);
+  cudaMemsetAsync(w.cellStart, 0, size_t(tableSize) * 4, s);
+  cudaMemsetAsync(w.cellEnd, 0, size_t(tableSize) * 4, s);
+  if (n > 0) {
+    k_cell_keys<<<grid_for(n, 256), 256, 0, s>>>(w, p);
+    // Keys <= tableSize (the sentinel): as many 8-bit passes as those bits need
+    int bits = 1;
+    while ((1u << bits) <= tableSize) bits++;
+    int passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
+    uint32_t tiles = grid_for(n, SORT_TILE);
+    uint32_t *kin = w.keyA, *vin = w.valA, *kout = w.keyB, *vout = w.valB;
+    for (int pass = 0; pass < passes; pass++) {
+      int shift = pass * RADIX_BITS;
+      k_radix_hist<<<tiles, SORT_THREADS, 0, s>>>(kin, n, shift, w.radixHist, tiles);
+      k_scan_single<<<1, 1024, 0, s>>>(w.radixHist, RADIX * tiles);
+      k_radix_scatter<<<tiles, SORT_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, w.radixHist, tiles);
+      uint32_t* t = kin; kin = kout; kout = t;
+      t = vin; vin = vout; vout = t;
+    }
+    k_cell_ranges<<<grid_for(n, 256), 256, 0, s>>>(kin, n, w.cellStart, w.cellEnd, p.tableMask + 1u);
+    k_find_pairs<<<grid_for(n, 128), 128, 0, s>>>(w, p, vin);
+  }
+  k_narrowphase<<<GS_BLOCKS, 128, 0, s>>>(w, p);
+}
+
+}  // namespace avbd

@@ -1,0 +1,156 @@
+// Device-side layout and maths of the B200 AVBD step.
+//
+// Body state is structure-of-arrays of float4 (one 128-bit load per field); the field meanings
+// are the reference's body record (src/avbd3d/gpu/layout.ts:8-59). Contacts live in fixed slots,
+// eight per broadphase pair (pair p's points at 8p .. 8p+7), in four float4 arrays with the
+// reference's contact words (layout.ts:122-127): no atomics are needed to place them and the
+// points of one manifold are contiguous.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace avbd {
+
+constexpr float PENALTY_MIN = 1.0f;        // ref/body.ts:8
+constexpr float PENALTY_MAX = 1e10f;       // ref/body.ts:9
+constexpr float STICK_THRESH = 0.00001f;   // ref/body.ts:11
+constexpr float PIVOT_FLOOR = 1e-5f;       // gpu/layout.ts:192
+constexpr float BIG = 3.0e38f;             // avbd2d/gpu/layout.ts:99
+constexpr float HARD = 1e30f;              // avbd2d/gpu/layout.ts:100
+constexpr uint32_t STICK_BIT = 0x80000000u;
+constexpr uint32_t SPHERE_FEATURE = 3u << 24;
+constexpr uint32_t NO_COLOR = 255u, PENDING = 256u;
+constexpr int MAX_COLORS = 64;
+constexpr int MAX_CONTACTS = 8;
+constexpr float SHAPE_SPHERE_F = 1.0f;
+constexpr uint32_t T_NONE = 0, T_JOINT = 1, T_SPRING = 2;
+constexpr uint32_t FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_START_AT_REST = 8, FLAG_MASS_PENALTY = 16;
+constexpr float REST_SPEED = 0.1f;
+constexpr float NEAREST_FRACTION = 0.05f;
+constexpr uint32_t OWNER_BIT = 0x80000000u;  // incidence entry: this body updates the constraint's dual
+
+// Counter words (device memory)
+enum : int {
+  C_PAIRS = 0, C_CONTACTS = 1, C_MANIFOLDS = 2, C_OVERFLOW = 3, C_CLASHES = 4, C_COLORS = 5, C_ROUNDS = 6, C_ERROR = 7,
+  C_PREV_PAIRS = 8, C_PENDING = 16,  // 16..16+2*MAX_ROUND_PAIRS: pending counts per round pair
+  COUNTER_WORDS = 128,
+};
+constexpr int MAX_ROUND_PAIRS = 32;
+// Error bits
+constexpr uint32_t ERR_BARRIER_TIMEOUT = 1, ERR_ADJ_OVERFLOW = 2, ERR_INC_OVERFLOW = 4;
+
+// Joint record words (layout.ts:84-110), as float4 slots
+enum : int { J_PEN_LIN = 0, J_PEN_ANG = 1, J_LAM_LIN = 2, J_LAM_ANG = 3, J_C0_LIN = 4, J_C0_ANG = 5, J_RA = 6, J_RB = 7, J_REST = 8, J_REST_START = 9, JOINT_VEC4 = 10 };
+
+struct StepParams {
+  float dt, gravity, alpha, betaLin, betaAng, gamma, margin;
+  uint32_t flags;
+  int iterations;
+  float upx, upy, upz;
+  // broadphase
+  float cellSize, largeThreshold;
+  uint32_t tableMask, nLarge, nNoCollide, anyDynamicLarge;
+  // sizes
+  uint32_t n, nj, pairCap, hashMask, incCap, adjCap;
+  uint32_t step;
+  uint32_t fixedColors;  // colours come from the host (validation), no Jones-Plassmann
+  uint32_t colorCap;
+  int cur;               // which manifold/contact buffers this step writes
+};
+
+struct DWorld {
+  // bodies (SoA, capacity bodyCap)
+  float4 *pos, *rot, *ipos, *irot, *size, *moment, *ypos, *yrot, *vel, *avel;
+  uint2* filters;
+  // joints: JOINT_VEC4 float4 per slot, AoS (a joint row reads the whole record)
+  float4* joint;
+  int4* jinfo;
+  // broadphase statics: large body indices, then (hi, lo, slot) no-collide triples sorted by (hi, lo)
+  uint32_t *large, *nocollide;
+  // broadphase scratch
+  uint32_t *keyA, *keyB, *valA, *valB, *radixHist;
+  int4* cell;
+  uint32_t *cellStart, *cellEnd;
+  uint2* pairs;
+  // contact pairs and points, double-buffered (cur: this step, 1 - cur: last step)
+  uint4* mIds[2];   // a, b, first (= 8 * slot), count | step << 4
+  float4* mGeo[2];  // normal (B to A), friction
+  float4 *cRA[2], *cRB[2], *cPen[2], *cLam[2];
+  uint32_t* hash;   // last step's pairs: slot + 1, open addressing
+  // topology
+  uint32_t *adjStart, *adjFill, *adjList;
+  uint32_t *colorA, *colorB, *colorHist, *colorStart, *colorBodies, *fixedColor;
+  uint32_t *incStart, *incList;
+  uint32_t* scanScratch;
+  // bookkeeping
+  uint32_t* counters;
+  uint32_t* barrier;  // [0] arrive count, [1] generation
+};
+
+// --- vector / quaternion helpers (operation order of the reference's WGSL, wgsl layout.ts:307-340) ---
+__host__ __device__ inline float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+__host__ __device__ inline float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ inline float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ inline float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__host__ __device__ inline float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ inline float3 operator*(float3 a, float3 b) { return make_float3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__host__ __device__ inline float3 operator/(float3 a, float s) { return make_float3(a.x / s, a.y / s, a.z / s); }
+__host__ __device__ inline float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ inline float3 cross3(float3 a, float3 b) { return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+__host__ __device__ inline float3 abs3(float3 a) { return make_float3(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+__host__ __device__ inline float len3(float3 a) { return sqrtf(dot3(a, a)); }
+__host__ __device__ inline float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+__host__ __device__ inline float4 qmul(float4 a, float4 b) {
+  return make_float4(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+                     a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+__host__ __device__ inline float4 qconj(float4 q) { return make_float4(-q.x, -q.y, -q.z, q.w); }
+// The reference's rotate (ref/math.ts:115-126): t = 2 u x v; v + t w + u x t
+__host__ __device__ inline float3 qrotate(float4 q, float3 v) {
+  float tx = (q.y * v.z - q.z * v.y) * 2.0f;
+  float ty = (q.z * v.x - q.x * v.z) * 2.0f;
+  float tz = (q.x * v.y - q.y * v.x) * 2.0f;
+  return make_float3(v.x + tx * q.w + (q.y * tz - q.z * ty), v.y + ty * q.w + (q.z * tx - q.x * tz), v.z + tz * q.w + (q.x * ty - q.y * tx));
+}
+// qsub (ref/math.ts:86-89): 2 vec(a b^-1), b^-1 = conj(b) / |b|^2
+__host__ __device__ inline float3 qsub(float4 a, float4 b) {
+  float l = (b.x * b.x + b.y * b.y + b.z * b.z) + b.w * b.w;
+  float4 inv = make_float4(-b.x / l, -b.y / l, -b.z / l, b.w / l);
+  float4 s = qmul(a, inv);
+  return make_float3(s.x * 2.0f, s.y * 2.0f, s.z * 2.0f);
+}
+// qaddv (ref/math.ts:109-113): normalize(a + (v, 0) a / 2)
+__host__ __device__ inline float4 qadd(float4 a, float3 v) {
+  float4 s = qmul(make_float4(v.x, v.y, v.z, 0.0f), a);
+  float4 q = make_float4(a.x + s.x * 0.5f, a.y + s.y * 0.5f, a.z + s.z * 0.5f, a.w + s.w * 0.5f);
+  float l = sqrtf((q.x * q.x + q.y * q.y + q.z * q.z) + q.w * q.w);
+  return make_float4(q.x / l, q.y / l, q.z / l, q.w / l);
+}
+// orthonormal (ref/math.ts:228-238): rows n, t1, t2
+__host__ __device__ inline void orthonormal(float3 n, float3& t1, float3& t2) {
+  float3 t = fabsf(n.x) > fabsf(n.z) ? make_float3(-n.y, n.x, 0.0f) : make_float3(0.0f, -n.z, n.y);
+  float l = sqrtf(dot3(t, t));
+  t1 = make_float3(t.x / l, t.y / l, t.z / l);
+  t2 = cross3(n, t1);
+}
+__host__ __device__ inline uint32_t hash32(uint32_t x) {  // avbd2d/gpu/layout.ts:107-115 (lowbias32)
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__host__ __device__ inline uint32_t pairHash(uint32_t a, uint32_t b) { return hash32((a * 0x9e3779b1u) ^ hash32(b)); }  // wgsl-collision.ts:344
+
+inline uint32_t grid_for(uint32_t n, uint32_t block) { return (n + block - 1) / block; }
+
+// Host launchers (avbd_collide.cu)
+void launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s);
+// Host launchers (avbd_solve.cu)
+int solve_grid_blocks(int device);
+cudaError_t launch_topology_solve(const DWorld& w, const StepParams& p, int blocks, cudaStream_t s);
+
+}  // namespace avbd

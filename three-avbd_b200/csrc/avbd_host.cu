@@ -1,0 +1,855 @@
+// Host side of the B200 AVBD backend: world storage, the step schedule and the C ABI (include/avbd.h).
+//
+// Mirrors GpuSolver3D (src/avbd3d/gpu/solver.ts): the host keeps what the CPU owns (body radii and
+// masses for the broadphase configuration, joint endpoints, the no-collide list) and uploads it
+// when it changes (uploadStatics, solver.ts:1263-1318); everything per step runs on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/avbd.h"
+#include "avbd_device.cuh"
+
+using namespace avbd;
+
+namespace {
+
+uint32_t pow2AtLeast(uint64_t n) {
+  uint64_t p = 2;
+  while (p < n) p <<= 1;
+  return (uint32_t)p;
+}
+
+// radii.ts:19-55 (selection, not sorting)
+double selectKth(std::vector<double>& a, int k) {
+  int lo = 0, hi = int(a.size()) - 1;
+  while (lo < hi) {
+    double pivot = a[k];
+    int i = lo, j = hi;
+    do {
+      while (a[i] < pivot) i++;
+      while (pivot < a[j]) j--;
+      if (i <= j) {
+        std::swap(a[i], a[j]);
+        i++;
+        j--;
+      }
+    } while (i <= j);
+    if (j < k) lo = i;
+    if (k < i) hi = j;
+  }
+  return a[k];
+}
+double largestSmall(std::vector<double> radii) {
+  const int n = int(radii.size());
+  double median = n > 0 ? selectKth(radii, n >> 1) : 1.0;
+  double maxSmall = 0.0;
+  for (int i = 0; i < n; i++)
+    if (radii[i] <= 2.0 * median) maxSmall = std::max(maxSmall, radii[i]);
+  if (n > 64) maxSmall = std::max(maxSmall, selectKth(radii, n - 64 - 1));
+  return maxSmall;
+}
+
+struct NoCollide {
+  uint32_t hi, lo, slot;
+  bool operator<(const NoCollide& o) const { return hi < o.hi || (hi == o.hi && lo < o.lo); }
+};
+
+}  // namespace
+
+struct avbd_world {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  avbd_params params{};
+  uint32_t bodyCap = 0, n = 0, jointCap = 0, nj = 0, pairCap = 0, tableSize = 0, hashSize = 0, incCap = 0, adjCap = 0;
+  uint32_t sortTiles = 0;
+  DWorld d{};
+  int solveBlocks = 0;
+  int cur = 0;
+  uint32_t stepCount = 0;
+  bool fixedColors = false;
+  // host mirrors
+  std::vector<float> radius;
+  std::vector<char> dynamic;
+  std::vector<avbd_joint_info> info;
+  std::vector<NoCollide> nocollide;
+  bool staticsDirty = true;
+  float threshold = 0.0f, cellSize = 1.0f;
+  uint32_t nLarge = 0, nNoCollide = 0, anyDynamicLarge = 0;
+  uint32_t staticsWords = 0;
+  // counters of the last step, copied back asynchronously
+  uint32_t* hCounters = nullptr;
+  cudaEvent_t countersReady = nullptr;
+  bool countersInFlight = false;
+  bool timing = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  float lastCollisionMs = 0.0f, lastSolveMs = 0.0f;
+  std::vector<void*> allocations;
+};
+
+namespace {
+
+int fail(avbd_world* w, int code, const std::string& msg) {
+  if (w) w->error = msg;
+  return code;
+}
+
+#define CUDA_TRY(w, call)                                                                    \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) return fail(w, AVBD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(avbd_world* w, T** p, size_t count) {
+  void* ptr = nullptr;
+  cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) return e;
+  w->allocations.push_back(ptr);
+  *p = static_cast<T*>(ptr);
+  return cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), w->stream);
+}
+void dfree(avbd_world* w, void* p) {
+  if (!p) return;
+  auto it = std::find(w->allocations.begin(), w->allocations.end(), p);
+  if (it != w->allocations.end()) w->allocations.erase(it);
+  cudaFree(p);
+}
+
+// Pair-dependent storage (pairs, both manifold/contact buffers, hash, adjacency and incidence
+// lists). On growth last step's buffer (1 - cur) is carried over, so warm starts survive.
+int allocPairs(avbd_world* w, uint32_t cap) {
+  DWorld& d = w->d;
+  const uint32_t oldCap = w->pairCap;
+  const int prev = 1 - w->cur;
+  uint4* oldIds = d.mIds[prev];
+  float4* oldGeo = d.mGeo[prev];
+  float4 *oldRA = d.cRA[prev], *oldRB = d.cRB[prev], *oldPen = d.cPen[prev], *oldLam = d.cLam[prev];
+  uint4* keepIds[2] = {d.mIds[0], d.mIds[1]};
+  float4* keepGeo[2] = {d.mGeo[0], d.mGeo[1]};
+  float4* keepC[2][4] = {{d.cRA[0], d.cRB[0], d.cPen[0], d.cLam[0]}, {d.cRA[1], d.cRB[1], d.cPen[1], d.cLam[1]}};
+  dfree(w, d.pairs);
+  dfree(w, d.hash);
+  dfree(w, d.adjList);
+  dfree(w, d.incList);
+  w->pairCap = cap;
+  w->hashSize = pow2AtLeast(2ull * cap);
+  w->adjCap = 2u * (cap + w->jointCap);
+  w->incCap = 2u * (cap * MAX_CONTACTS + w->jointCap);
+  CUDA_TRY(w, dalloc(w, &d.pairs, cap));
+  CUDA_TRY(w, dalloc(w, &d.hash, w->hashSize));
+  CUDA_TRY(w, dalloc(w, &d.adjList, w->adjCap));
+  CUDA_TRY(w, dalloc(w, &d.incList, w->incCap));
+  for (int b = 0; b < 2; b++) {
+    CUDA_TRY(w, dalloc(w, &d.mIds[b], cap));
+    CUDA_TRY(w, dalloc(w, &d.mGeo[b], cap));
+    CUDA_TRY(w, dalloc(w, &d.cRA[b], size_t(cap) * MAX_CONTACTS));
+    CUDA_TRY(w, dalloc(w, &d.cRB[b], size_t(cap) * MAX_CONTACTS));
+    CUDA_TRY(w, dalloc(w, &d.cPen[b], size_t(cap) * MAX_CONTACTS));
+    CUDA_TRY(w, dalloc(w, &d.cLam[b], size_t(cap) * MAX_CONTACTS));
+  }
+  if (oldIds) {
+    size_t m = std::min(oldCap, cap);
+    CUDA_TRY(w, cudaMemcpyAsync(d.mIds[prev], oldIds, m * sizeof(uint4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(d.mGeo[prev], oldGeo, m * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(d.cRA[prev], oldRA, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(d.cRB[prev], oldRB, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(d.cPen[prev], oldPen, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(d.cLam[prev], oldLam, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+    for (int b = 0; b < 2; b++) {
+      dfree(w, keepIds[b]);
+      dfree(w, keepGeo[b]);
+      for (int k = 0; k < 4; k++) dfree(w, keepC[b][k]);
+    }
+  }
+  // the clears above run on the world's stream; host copies that follow use the default stream
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  return AVBD_OK;
+}
+
+int allocJoints(avbd_world* w, uint32_t cap) {
+  DWorld& d = w->d;
+  float4* oldJ = d.joint;
+  int4* oldI = d.jinfo;
+  float4* nj = nullptr;
+  int4* ni = nullptr;
+  CUDA_TRY(w, dalloc(w, &nj, size_t(cap) * JOINT_VEC4));
+  CUDA_TRY(w, dalloc(w, &ni, cap));
+  if (oldJ) {
+    CUDA_TRY(w, cudaMemcpyAsync(nj, oldJ, size_t(w->nj) * JOINT_VEC4 * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(ni, oldI, size_t(w->nj) * sizeof(int4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+    dfree(w, oldJ);
+    dfree(w, oldI);
+  }
+  d.joint = nj;
+  d.jinfo = ni;
+  w->jointCap = cap;
+  // adjacency and incidence lists are sized by the joint capacity too
+  dfree(w, d.adjList);
+  dfree(w, d.incList);
+  w->adjCap = 2u * (w->pairCap + w->jointCap);
+  w->incCap = 2u * (w->pairCap * MAX_CONTACTS + w->jointCap);
+  CUDA_TRY(w, dalloc(w, &d.adjList, w->adjCap));
+  CUDA_TRY(w, dalloc(w, &d.incList, w->incCap));
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  return AVBD_OK;
+}
+
+// uploadStatics (solver.ts:1263-1318): large bodies, cell size, sorted no-collide triples
+int uploadStatics(avbd_world* w) {
+  const uint32_t n = w->n;
+  std::vector<double> radii(n);
+  for (uint32_t i = 0; i < n; i++) radii[i] = w->radius[i];
+  double maxSmall = largestSmall(radii);
+  double minLarge = INFINITY;
+  for (uint32_t i = 0; i < n; i++)
+    if (radii[i] > maxSmall) minLarge = std::min(minLarge, radii[i]);
+  double threshold = std::isinf(minLarge) ? maxSmall * 1.5 : (maxSmall + minLarge) / 2;
+  w->threshold = float(threshold);
+  w->cellSize = float(std::max(2.0 * maxSmall * (1 + 1e-4), 1e-3));
+  std::vector<uint32_t> data;
+  w->anyDynamicLarge = 0;
+  for (uint32_t i = 0; i < n; i++)
+    if (w->radius[i] > w->threshold) {
+      data.push_back(i);
+      if (w->dynamic[i]) w->anyDynamicLarge = 1;
+    }
+  w->nLarge = uint32_t(data.size());
+  std::stable_sort(w->nocollide.begin(), w->nocollide.end());
+  for (auto& e : w->nocollide) {
+    data.push_back(e.hi);
+    data.push_back(e.lo);
+    data.push_back(e.slot);
+  }
+  w->nNoCollide = uint32_t(w->nocollide.size());
+  if (data.size() > w->staticsWords) {
+    dfree(w, w->d.large);
+    w->staticsWords = uint32_t(std::max<size_t>(data.size() * 2, 64));
+    CUDA_TRY(w, dalloc(w, &w->d.large, w->staticsWords));
+  }
+  if (!data.empty()) CUDA_TRY(w, cudaMemcpyAsync(w->d.large, data.data(), data.size() * 4, cudaMemcpyHostToDevice, w->stream));
+  // keep the upload's source alive until it lands (pageable copies are staged synchronously)
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  w->d.nocollide = w->d.large + w->nLarge;
+  w->staticsDirty = false;
+  return AVBD_OK;
+}
+
+StepParams makeParams(avbd_world* w) {
+  StepParams p{};
+  const avbd_params& a = w->params;
+  p.dt = a.dt;
+  p.gravity = a.gravity;
+  p.alpha = a.alpha;
+  p.betaLin = a.beta_lin;
+  p.betaAng = a.beta_ang;
+  p.gamma = a.gamma;
+  p.margin = a.contact_margin;
+  p.flags = a.flags;
+  p.iterations = a.iterations;
+  p.upx = a.up[0];
+  p.upy = a.up[1];
+  p.upz = a.up[2];
+  p.cellSize = w->cellSize;
+  p.largeThreshold = w->threshold;
+  p.tableMask = w->tableSize - 1;
+  p.nLarge = w->nLarge;
+  p.nNoCollide = w->nNoCollide;
+  p.anyDynamicLarge = w->anyDynamicLarge;
+  p.n = w->n;
+  p.nj = w->nj;
+  p.pairCap = w->pairCap;
+  p.hashMask = w->hashSize - 1;
+  p.incCap = w->incCap;
+  p.adjCap = w->adjCap;
+  p.step = w->stepCount;
+  p.fixedColors = w->fixedColors ? 1u : 0u;
+  p.colorCap = MAX_COLORS;
+  p.cur = w->cur;
+  return p;
+}
+
+// Storage grows past 80 % use or on overflow, to twice the demand (solver.ts:2362-2377).
+int adaptCapacity(avbd_world* w, bool wait) {
+  if (!w->countersInFlight) return AVBD_OK;
+  if (!wait && cudaEventQuery(w->countersReady) != cudaSuccess) return AVBD_OK;
+  CUDA_TRY(w, cudaEventSynchronize(w->countersReady));
+  w->countersInFlight = false;
+  const uint32_t* c = w->hCounters;
+  uint32_t demand = c[C_PAIRS];
+  if ((c[C_OVERFLOW] & 1u) || uint64_t(demand) * 10 > uint64_t(w->pairCap) * 8) {
+    uint64_t want = std::max<uint64_t>(2ull * demand, uint64_t(w->pairCap) * 5 / 4);
+    want = std::min<uint64_t>(want, 1ull << 26);
+    if (want > w->pairCap) {
+      CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+      int r = allocPairs(w, uint32_t(want));
+      if (r) return r;
+    }
+  }
+  return AVBD_OK;
+}
+
+void copyBodiesIn(avbd_world* w, uint32_t first, const avbd_body* b, uint32_t n, cudaMemcpyKind kind) {
+  float4* fields[10] = {w->d.pos, w->d.rot, w->d.ipos, w->d.irot, w->d.size, w->d.moment, w->d.ypos, w->d.yrot, w->d.vel, w->d.avel};
+  for (int f = 0; f < 10; f++)
+    cudaMemcpy2DAsync(fields[f] + first, sizeof(float4), reinterpret_cast<const char*>(b) + f * sizeof(float4), sizeof(avbd_body), sizeof(float4), n, kind,
+                      w->stream);
+}
+void copyBodiesOut(avbd_world* w, avbd_body* b, uint32_t n) {
+  float4* fields[10] = {w->d.pos, w->d.rot, w->d.ipos, w->d.irot, w->d.size, w->d.moment, w->d.ypos, w->d.yrot, w->d.vel, w->d.avel};
+  for (int f = 0; f < 10; f++)
+    cudaMemcpy2DAsync(reinterpret_cast<char*>(b) + f * sizeof(float4), sizeof(avbd_body), fields[f], sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToHost,
+                      w->stream);
+}
+
+bool finite(float x) { return std::isfinite(x); }
+
+}  // namespace
+
+extern "C" {
+
+int avbd_abi_version(void) { return AVBD_ABI_VERSION; }
+
+int avbd_device_info(int device, char* name, size_t cap, int* sms) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return AVBD_ERR_NO_DEVICE;
+  if (name && cap) {
+    std::strncpy(name, prop.name, cap - 1);
+    name[cap - 1] = 0;
+  }
+  if (sms) *sms = prop.multiProcessorCount;
+  return AVBD_OK;
+}
+
+int avbd_default_params(avbd_params* p) {
+  if (!p) return AVBD_ERR_INVALID;
+  p->dt = 1.0f / 60.0f;
+  p->gravity = -10.0f;
+  p->alpha = 0.99f;
+  p->beta_lin = 10000.0f;
+  p->beta_ang = 100.0f;
+  p->gamma = 0.999f;
+  p->contact_margin = 0.01f;
+  p->iterations = 10;
+  p->flags = 0;
+  p->up[0] = 0.0f;
+  p->up[1] = 0.0f;
+  p->up[2] = 1.0f;
+  return AVBD_OK;
+}
+
+int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
+  if (!out) return AVBD_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return AVBD_ERR_NO_DEVICE;
+  avbd_world* w = new avbd_world();
+  w->device = cfg ? cfg->device : 0;
+  if (w->device < 0 || w->device >= count) {
+    delete w;
+    return AVBD_ERR_INVALID;
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, w->device);
+  if (prop.major < 10) {
+    delete w;
+    return AVBD_ERR_NO_DEVICE;
+  }
+  cudaSetDevice(w->device);
+  avbd_default_params(&w->params);
+  w->bodyCap = cfg && cfg->body_capacity ? cfg->body_capacity : 1024;
+  w->jointCap = cfg && cfg->joint_capacity ? cfg->joint_capacity : 256;
+  uint32_t pairCap = cfg && cfg->pair_capacity ? cfg->pair_capacity : std::max<uint32_t>(65536, 8 * w->bodyCap);
+  auto bad = [&](int code) {
+    avbd_world_destroy(w);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(AVBD_ERR_CUDA);
+  DWorld& d = w->d;
+  const uint32_t B = w->bodyCap;
+  w->tableSize = pow2AtLeast(2ull * B);
+  w->sortTiles = (B + 2047) / 2048;
+  w->solveBlocks = solve_grid_blocks(w->device);
+  bool ok = true;
+  auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
+  for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel}) A(dalloc(w, f, B));
+  A(dalloc(w, &d.filters, B));
+  A(dalloc(w, &d.keyA, B));
+  A(dalloc(w, &d.keyB, B));
+  A(dalloc(w, &d.valA, B));
+  A(dalloc(w, &d.valB, B));
+  A(dalloc(w, &d.radixHist, size_t(256) * w->sortTiles));
+  A(dalloc(w, &d.cell, B));
+  A(dalloc(w, &d.cellStart, w->tableSize));
+  A(dalloc(w, &d.cellEnd, w->tableSize));
+  A(dalloc(w, &d.adjStart, B + 1));
+  A(dalloc(w, &d.adjFill, B + 1));
+  A(dalloc(w, &d.colorA, B));
+  A(dalloc(w, &d.colorB, B));
+  A(dalloc(w, &d.colorHist, size_t(MAX_COLORS) * w->solveBlocks + 1));
+  A(dalloc(w, &d.colorStart, MAX_COLORS + 1));
+  A(dalloc(w, &d.colorBodies, B));
+  A(dalloc(w, &d.fixedColor, B));
+  A(dalloc(w, &d.incStart, B + 1));
+  A(dalloc(w, &d.scanScratch, w->solveBlocks + 1));
+  A(dalloc(w, &d.counters, COUNTER_WORDS));
+  A(dalloc(w, &d.barrier, 2));
+  if (!ok) return bad(AVBD_ERR_CUDA);
+  // every body in every group, colliding with every group; colours start unset
+  A(cudaMemsetAsync(d.filters, 0xff, size_t(B) * sizeof(uint2), w->stream));
+  A(cudaStreamSynchronize(w->stream));
+  {
+    std::vector<uint32_t> none(B, NO_COLOR);
+    A(cudaMemcpy(d.colorA, none.data(), size_t(B) * 4, cudaMemcpyHostToDevice));
+  }
+  if (!ok) return bad(AVBD_ERR_CUDA);
+  w->pairCap = 0;
+  if (allocPairs(w, pairCap) != AVBD_OK) return bad(AVBD_ERR_CUDA);
+  if (allocJoints(w, w->jointCap) != AVBD_OK) return bad(AVBD_ERR_CUDA);
+  if (uploadStatics(w) != AVBD_OK) return bad(AVBD_ERR_CUDA);
+  if (cudaMallocHost(&w->hCounters, COUNTER_WORDS * sizeof(uint32_t)) != cudaSuccess) return bad(AVBD_ERR_CUDA);
+  std::memset(w->hCounters, 0, COUNTER_WORDS * sizeof(uint32_t));
+  if (cudaEventCreateWithFlags(&w->countersReady, cudaEventDisableTiming) != cudaSuccess) return bad(AVBD_ERR_CUDA);
+  for (auto& e : w->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bad(AVBD_ERR_CUDA);
+  if (cudaStreamSynchronize(w->stream) != cudaSuccess) return bad(AVBD_ERR_CUDA);
+  *out = w;
+  return AVBD_OK;
+}
+
+int avbd_world_destroy(avbd_world* w) {
+  if (!w) return AVBD_OK;
+  cudaSetDevice(w->device);
+  if (w->stream) cudaStreamSynchronize(w->stream);
+  for (void* p : w->allocations) cudaFree(p);
+  w->allocations.clear();
+  if (w->hCounters) cudaFreeHost(w->hCounters);
+  if (w->countersReady) cudaEventDestroy(w->countersReady);
+  for (auto& e : w->ev)
+    if (e) cudaEventDestroy(e);
+  if (w->stream) cudaStreamDestroy(w->stream);
+  delete w;
+  return AVBD_OK;
+}
+
+const char* avbd_last_error(const avbd_world* w) { return w ? w->error.c_str() : "no world"; }
+
+int avbd_set_params(avbd_world* w, const avbd_params* p) {
+  if (!w || !p) return AVBD_ERR_INVALID;
+  if (!(p->dt > 0.0f) || !finite(p->dt) || !finite(p->gravity) || !finite(p->alpha) || !finite(p->gamma) || p->iterations < 0 ||
+      !(p->contact_margin >= 0.0f) || !finite(p->contact_margin))
+    return fail(w, AVBD_ERR_INVALID, "invalid params (dt > 0, finite values, iterations >= 0, contact_margin >= 0)");
+  w->params = *p;
+  return AVBD_OK;
+}
+
+int avbd_get_params(const avbd_world* w, avbd_params* p) {
+  if (!w || !p) return AVBD_ERR_INVALID;
+  *p = w->params;
+  return AVBD_OK;
+}
+
+static int checkBodies(avbd_world* w, const avbd_body* b, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) {
+    const float* f = reinterpret_cast<const float*>(b + i);
+    for (int k = 0; k < 40; k++)
+      if (!finite(f[k])) return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + ": non-finite value");
+    if (b[i].mass < 0.0f || b[i].radius < 0.0f) return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + ": negative mass or radius");
+  }
+  return AVBD_OK;
+}
+
+int avbd_add_bodies(avbd_world* w, const avbd_body* bodies, uint32_t n, uint32_t* first) {
+  if (!w || (!bodies && n)) return AVBD_ERR_INVALID;
+  if (uint64_t(w->n) + n > w->bodyCap) return fail(w, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(w->bodyCap) + " reached");
+  int r = checkBodies(w, bodies, n);
+  if (r) return r;
+  uint32_t at = w->n;
+  if (first) *first = at;
+  if (n == 0) return AVBD_OK;
+  return avbd_write_bodies(w, at, bodies, n, 0) == AVBD_OK ? AVBD_OK : AVBD_ERR_CUDA;
+}
+
+int avbd_write_bodies(avbd_world* w, uint32_t first, const avbd_body* bodies, uint32_t n, int keep_contacts) {
+  if (!w || (!bodies && n)) return AVBD_ERR_INVALID;
+  if (uint64_t(first) + n > w->bodyCap || first > w->n) return fail(w, AVBD_ERR_INVALID, "body range outside the world");
+  int r = checkBodies(w, bodies, n);
+  if (r) return r;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  std::vector<avbd_body> copy(bodies, bodies + n);
+  for (auto& b : copy) {
+    uint32_t flags = uint32_t(b.flags) & 6u;
+    b.flags = float(keep_contacts ? flags : (flags | 1u));
+  }
+  copyBodiesIn(w, first, copy.data(), n, cudaMemcpyHostToDevice);
+  if (!keep_contacts) {
+    std::vector<uint32_t> none(n, NO_COLOR);
+    CUDA_TRY(w, cudaMemcpyAsync(w->d.colorA + first, none.data(), size_t(n) * 4, cudaMemcpyHostToDevice, w->stream));
+  }
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (w->radius.size() < first + n) {
+    w->radius.resize(first + n);
+    w->dynamic.resize(first + n);
+  }
+  for (uint32_t i = 0; i < n; i++) {
+    if (w->radius[first + i] != bodies[i].radius || w->dynamic[first + i] != (bodies[i].mass > 0.0f)) w->staticsDirty = true;
+    w->radius[first + i] = bodies[i].radius;
+    w->dynamic[first + i] = bodies[i].mass > 0.0f;
+  }
+  if (first + n > w->n) {
+    w->n = first + n;
+    w->staticsDirty = true;
+  }
+  return AVBD_OK;
+}
+
+static int checkJoints(avbd_world* w, const avbd_joint* j, const avbd_joint_info* info, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) {
+    const avbd_joint_info& in = info[i];
+    if (in.type != AVBD_T_JOINT && in.type != AVBD_T_SPRING && in.type != AVBD_T_NONE)
+      return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": unknown type");
+    if (in.b < 0 || uint32_t(in.b) >= w->n || in.a < -1 || (in.a >= 0 && uint32_t(in.a) >= w->n) || in.a == in.b)
+      return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": bodies must be distinct indices below the body count (a may be -1)");
+    if (in.type == AVBD_T_SPRING && in.a < 0) return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": a spring joins two bodies");
+    const float* f = reinterpret_cast<const float*>(j + i);
+    for (int k = 0; k < 40; k++)
+      if (std::isnan(f[k])) return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": NaN");
+  }
+  return AVBD_OK;
+}
+
+int avbd_write_joints(avbd_world* w, uint32_t first, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n) {
+  if (!w || (n && (!joints || !info))) return AVBD_ERR_INVALID;
+  if (uint64_t(first) + n > w->nj) return fail(w, AVBD_ERR_INVALID, "joint range outside the world's slots");
+  int r = checkJoints(w, joints, info, n);
+  if (r) return r;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(first) * JOINT_VEC4, joints, size_t(n) * sizeof(avbd_joint), cudaMemcpyHostToDevice));
+  CUDA_TRY(w, cudaMemcpy(w->d.jinfo + first, info, size_t(n) * sizeof(int4), cudaMemcpyHostToDevice));
+  for (uint32_t i = 0; i < n; i++) w->info[first + i] = info[i];
+  return AVBD_OK;
+}
+
+int avbd_add_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* first) {
+  if (!w || (n && (!joints || !info))) return AVBD_ERR_INVALID;
+  int r = checkJoints(w, joints, info, n);
+  if (r) return r;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (uint64_t(w->nj) + n > w->jointCap) {
+    uint64_t cap = std::max<uint64_t>(uint64_t(w->nj) + n + 256, uint64_t(w->jointCap) * 2);
+    r = allocJoints(w, uint32_t(cap));
+    if (r) return r;
+  }
+  uint32_t at = w->nj;
+  if (first) *first = at;
+  w->nj += n;
+  w->info.resize(w->nj);
+  r = avbd_write_joints(w, at, joints, info, n);
+  if (r) {
+    w->nj -= n;
+    return r;
+  }
+  for (uint32_t i = 0; i < n; i++)
+    if (info[i].a >= 0 && info[i].type != AVBD_T_NONE) {
+      uint32_t a = uint32_t(info[i].a), b = uint32_t(info[i].b);
+      w->nocollide.push_back({std::max(a, b), std::min(a, b), at + i});
+    }
+  w->staticsDirty = true;
+  return AVBD_OK;
+}
+
+int avbd_release_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
+  if (!w || (n && !slots)) return AVBD_ERR_INVALID;
+  for (uint32_t i = 0; i < n; i++)
+    if (slots[i] >= w->nj) return fail(w, AVBD_ERR_INVALID, "joint slot " + std::to_string(slots[i]) + " out of range");
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  const float zeros[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t i = 0; i < n; i++) {
+    float* rec = reinterpret_cast<float*>(w->d.joint + size_t(slots[i]) * JOINT_VEC4);
+    CUDA_TRY(w, cudaMemcpy(rec, zeros, 8 * sizeof(float), cudaMemcpyHostToDevice));        // penalties and stiffnesses
+    CUDA_TRY(w, cudaMemcpy(rec + 8, zeros, 3 * sizeof(float), cudaMemcpyHostToDevice));    // lam_lin (fracture kept)
+    CUDA_TRY(w, cudaMemcpy(rec + 12, zeros, 3 * sizeof(float), cudaMemcpyHostToDevice));   // lam_ang (torque arm kept)
+  }
+  return AVBD_OK;
+}
+
+int avbd_add_ignore_pairs(avbd_world* w, const uint32_t* ab, uint32_t n) {
+  if (!w || (n && !ab)) return AVBD_ERR_INVALID;
+  for (uint32_t i = 0; i < n; i++)
+    if (ab[2 * i] >= w->n || ab[2 * i + 1] >= w->n || ab[2 * i] == ab[2 * i + 1]) return fail(w, AVBD_ERR_INVALID, "ignore pair out of range");
+  for (uint32_t i = 0; i < n; i++) w->nocollide.push_back({std::max(ab[2 * i], ab[2 * i + 1]), std::min(ab[2 * i], ab[2 * i + 1]), 0xffffffffu});
+  w->staticsDirty = true;
+  return AVBD_OK;
+}
+
+int avbd_set_filters(avbd_world* w, uint32_t first, const uint32_t* gm, uint32_t n) {
+  if (!w || (n && !gm) || uint64_t(first) + n > w->n) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  CUDA_TRY(w, cudaMemcpy(w->d.filters + first, gm, size_t(n) * sizeof(uint2), cudaMemcpyHostToDevice));
+  return AVBD_OK;
+}
+
+int avbd_seed_contacts(avbd_world* w, const avbd_manifold* m, uint32_t nm, const avbd_contact* c, uint32_t nc) {
+  if (!w || (nm && !m) || (nc && !c)) return AVBD_ERR_INVALID;
+  for (uint32_t i = 0; i < nm; i++) {
+    if (m[i].count > MAX_CONTACTS || uint64_t(m[i].first) + m[i].count > nc || m[i].a >= w->n || m[i].b >= w->n)
+      return fail(w, AVBD_ERR_INVALID, "manifold " + std::to_string(i) + ": bad bodies or contact range");
+  }
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (nm > w->pairCap) {
+    int r = allocPairs(w, pow2AtLeast(nm));
+    if (r) return r;
+  }
+  const int prev = 1 - w->cur;
+  std::vector<uint4> ids(nm);
+  std::vector<float4> geo(nm);
+  std::vector<float4> ra(size_t(nm) * MAX_CONTACTS), rb(ra.size()), pen(ra.size()), lam(ra.size());
+  for (uint32_t i = 0; i < nm; i++) {
+    ids[i] = make_uint4(m[i].a, m[i].b, i * MAX_CONTACTS, m[i].count);
+    geo[i] = make_float4(m[i].normal[0], m[i].normal[1], m[i].normal[2], m[i].friction);
+    for (uint32_t k = 0; k < m[i].count; k++) {
+      const avbd_contact& s = c[m[i].first + k];
+      size_t o = size_t(i) * MAX_CONTACTS + k;
+      uint32_t key = s.key;
+      float keyf;
+      std::memcpy(&keyf, &key, 4);
+      ra[o] = make_float4(s.r_a[0], s.r_a[1], s.r_a[2], keyf);
+      rb[o] = make_float4(s.r_b[0], s.r_b[1], s.r_b[2], s.c0_n);
+      pen[o] = make_float4(s.pen[0], s.pen[1], s.pen[2], s.c0_t1);
+      lam[o] = make_float4(s.lam[0], s.lam[1], s.lam[2], s.c0_t2);
+    }
+  }
+  DWorld& d = w->d;
+  if (nm) {
+    CUDA_TRY(w, cudaMemcpy(d.mIds[prev], ids.data(), nm * sizeof(uint4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(d.mGeo[prev], geo.data(), nm * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(d.cRA[prev], ra.data(), ra.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(d.cRB[prev], rb.data(), rb.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(d.cPen[prev], pen.data(), pen.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(d.cLam[prev], lam.data(), lam.size() * sizeof(float4), cudaMemcpyHostToDevice));
+  }
+  uint32_t pairs = nm;
+  CUDA_TRY(w, cudaMemcpy(d.counters + C_PAIRS, &pairs, 4, cudaMemcpyHostToDevice));
+  w->countersInFlight = false;
+  return AVBD_OK;
+}
+
+int avbd_set_fixed_colors(avbd_world* w, const uint32_t* colors, uint32_t n) {
+  if (!w) return AVBD_ERR_INVALID;
+  if (!colors) {
+    w->fixedColors = false;
+    return AVBD_OK;
+  }
+  if (n < w->n) return fail(w, AVBD_ERR_INVALID, "one colour per body is needed");
+  for (uint32_t i = 0; i < w->n; i++)
+    if (colors[i] != NO_COLOR && colors[i] >= uint32_t(MAX_COLORS)) return fail(w, AVBD_ERR_INVALID, "colours are below 64 (or 255: none)");
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  CUDA_TRY(w, cudaMemcpy(w->d.fixedColor, colors, size_t(w->n) * 4, cudaMemcpyHostToDevice));
+  w->fixedColors = true;
+  return AVBD_OK;
+}
+
+int avbd_step(avbd_world* w, int n) {
+  if (!w || n < 0) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  for (int s = 0; s < n; s++) {
+    int r = adaptCapacity(w, false);
+    if (r) return r;
+    if (w->staticsDirty) {
+      r = uploadStatics(w);
+      if (r) return r;
+    }
+    w->stepCount++;
+    StepParams p = makeParams(w);
+    if (w->timing) cudaEventRecord(w->ev[0], w->stream);
+    launch_collision(w->d, p, w->tableSize, w->stream);
+    if (w->timing) cudaEventRecord(w->ev[1], w->stream);
+    CUDA_TRY(w, cudaGetLastError());
+    CUDA_TRY(w, launch_topology_solve(w->d, p, w->solveBlocks, w->stream));
+    if (w->timing) cudaEventRecord(w->ev[2], w->stream);
+    CUDA_TRY(w, cudaMemcpyAsync(w->hCounters, w->d.counters, COUNTER_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, w->stream));
+    CUDA_TRY(w, cudaEventRecord(w->countersReady, w->stream));
+    w->countersInFlight = true;
+    w->cur = 1 - w->cur;
+  }
+  return AVBD_OK;
+}
+
+int avbd_synchronize(avbd_world* w) {
+  if (!w) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (w->countersInFlight) {
+    CUDA_TRY(w, cudaEventSynchronize(w->countersReady));
+    w->countersInFlight = false;
+    if (w->hCounters[C_ERROR]) return fail(w, AVBD_ERR_TIMEOUT, "the step gave up: error bits " + std::to_string(w->hCounters[C_ERROR]));
+  }
+  if (w->timing) {
+    cudaEventElapsedTime(&w->lastCollisionMs, w->ev[0], w->ev[1]);
+    cudaEventElapsedTime(&w->lastSolveMs, w->ev[1], w->ev[2]);
+  }
+  return AVBD_OK;
+}
+
+int avbd_read_bodies(avbd_world* w, avbd_body* dst, uint32_t cap, uint32_t* n) {
+  if (!w) return AVBD_ERR_INVALID;
+  if (n) *n = w->n;
+  uint32_t k = std::min(cap, w->n);
+  if (k && !dst) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  if (k) copyBodiesOut(w, dst, k);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  return AVBD_OK;
+}
+
+int avbd_read_bodies_async(avbd_world* w, avbd_body* dst, uint32_t cap) {
+  if (!w) return AVBD_ERR_INVALID;
+  uint32_t k = std::min(cap, w->n);
+  if (k && !dst) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  if (k) copyBodiesOut(w, dst, k);
+  CUDA_TRY(w, cudaGetLastError());
+  return AVBD_OK;
+}
+
+int avbd_read_joints(avbd_world* w, avbd_joint* dst, avbd_joint_info* info, uint32_t cap, uint32_t* n) {
+  if (!w) return AVBD_ERR_INVALID;
+  if (n) *n = w->nj;
+  uint32_t k = std::min(cap, w->nj);
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (k && dst) CUDA_TRY(w, cudaMemcpy(dst, w->d.joint, size_t(k) * sizeof(avbd_joint), cudaMemcpyDeviceToHost));
+  if (k && info) std::memcpy(info, w->info.data(), size_t(k) * sizeof(avbd_joint_info));
+  return AVBD_OK;
+}
+
+int avbd_read_counters(avbd_world* w, avbd_counters* out) {
+  if (!w || !out) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  uint32_t c[COUNTER_WORDS];
+  CUDA_TRY(w, cudaMemcpy(c, w->d.counters, sizeof(c), cudaMemcpyDeviceToHost));
+  std::memset(out, 0, sizeof(*out));
+  out->pairs = c[C_PAIRS];
+  out->contacts = c[C_CONTACTS];
+  out->manifolds = c[C_MANIFOLDS];
+  out->overflow = c[C_OVERFLOW];
+  out->clashes = c[C_CLASHES];
+  out->colors = c[C_COLORS];
+  out->rounds = c[C_ROUNDS];
+  out->error = c[C_ERROR];
+  out->steps = w->stepCount;
+  out->pair_capacity = w->pairCap;
+  return AVBD_OK;
+}
+
+int avbd_read_contacts(avbd_world* w, avbd_manifold* mout, uint32_t mcap, uint32_t* nm, avbd_contact* cout, uint32_t ccap, uint32_t* nc) {
+  if (!w) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  uint32_t pairs = 0;
+  CUDA_TRY(w, cudaMemcpy(&pairs, w->d.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost));
+  pairs = std::min(pairs, w->pairCap);
+  const int last = 1 - w->cur;
+  std::vector<uint4> ids(pairs);
+  std::vector<float4> geo(pairs);
+  if (pairs) {
+    CUDA_TRY(w, cudaMemcpy(ids.data(), w->d.mIds[last], pairs * sizeof(uint4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, cudaMemcpy(geo.data(), w->d.mGeo[last], pairs * sizeof(float4), cudaMemcpyDeviceToHost));
+  }
+  std::vector<float4> ra, rb, pen, lam;
+  if (pairs) {
+    size_t k = size_t(pairs) * MAX_CONTACTS;
+    ra.resize(k);
+    rb.resize(k);
+    pen.resize(k);
+    lam.resize(k);
+    CUDA_TRY(w, cudaMemcpy(ra.data(), w->d.cRA[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, cudaMemcpy(rb.data(), w->d.cRB[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, cudaMemcpy(pen.data(), w->d.cPen[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, cudaMemcpy(lam.data(), w->d.cLam[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
+  }
+  uint32_t mi = 0, ci = 0;
+  for (uint32_t p = 0; p < pairs; p++) {
+    uint32_t count = ids[p].w & 15u;
+    if (!count) continue;
+    if (mout && mi < mcap) {
+      avbd_manifold& m = mout[mi];
+      m.a = ids[p].x;
+      m.b = ids[p].y;
+      m.first = ci;
+      m.count = count;
+      m.normal[0] = geo[p].x;
+      m.normal[1] = geo[p].y;
+      m.normal[2] = geo[p].z;
+      m.friction = geo[p].w;
+    }
+    for (uint32_t k = 0; k < count; k++) {
+      if (cout && ci + k < ccap) {
+        size_t o = size_t(p) * MAX_CONTACTS + k;
+        avbd_contact& c = cout[ci + k];
+        c.r_a[0] = ra[o].x; c.r_a[1] = ra[o].y; c.r_a[2] = ra[o].z;
+        std::memcpy(&c.key, &ra[o].w, 4);
+        c.r_b[0] = rb[o].x; c.r_b[1] = rb[o].y; c.r_b[2] = rb[o].z; c.c0_n = rb[o].w;
+        c.pen[0] = pen[o].x; c.pen[1] = pen[o].y; c.pen[2] = pen[o].z; c.c0_t1 = pen[o].w;
+        c.lam[0] = lam[o].x; c.lam[1] = lam[o].y; c.lam[2] = lam[o].z; c.c0_t2 = lam[o].w;
+      }
+    }
+    mi++;
+    ci += count;
+  }
+  if (nm) *nm = mi;
+  if (nc) *nc = ci;
+  return AVBD_OK;
+}
+
+int avbd_read_pairs(avbd_world* w, uint32_t* dst, uint32_t cap, uint32_t* n) {
+  if (!w) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  uint32_t pairs = 0;
+  CUDA_TRY(w, cudaMemcpy(&pairs, w->d.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost));
+  pairs = std::min(pairs, w->pairCap);
+  if (n) *n = pairs;
+  uint32_t k = std::min(cap, pairs);
+  if (k && dst) CUDA_TRY(w, cudaMemcpy(dst, w->d.pairs, size_t(k) * sizeof(uint2), cudaMemcpyDeviceToHost));
+  return AVBD_OK;
+}
+
+int avbd_read_colors(avbd_world* w, uint32_t* dst, uint32_t cap, uint32_t* n) {
+  if (!w) return AVBD_ERR_INVALID;
+  if (n) *n = w->n;
+  uint32_t k = std::min(cap, w->n);
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (k && dst) CUDA_TRY(w, cudaMemcpy(dst, w->d.colorA, size_t(k) * 4, cudaMemcpyDeviceToHost));
+  return AVBD_OK;
+}
+
+int avbd_enable_timing(avbd_world* w, int enable) {
+  if (!w) return AVBD_ERR_INVALID;
+  w->timing = enable != 0;
+  return AVBD_OK;
+}
+
+int avbd_last_timing(avbd_world* w, float* coll, float* solve) {
+  if (!w) return AVBD_ERR_INVALID;
+  if (coll) *coll = w->lastCollisionMs;
+  if (solve) *solve = w->lastSolveMs;
+  return AVBD_OK;
+}
+
+}  // extern "C"
