@@ -1,0 +1,300 @@
+"""Benchmark of the B200 AVBD step: body-steps/s on the 100k-body drop pile.
+
+A step is one full AVBD step (broadphase, narrowphase, adjacency, colouring, warm starts, 10
+iterations of primal + dual, velocities) of one world. The timed region is steps 1..K of the pile's
+rollout from its starting lattice (600 steps by default: the whole workload), on a fresh world
+after W warm-up steps on another one. Between timed steps a 256 MiB buffer is cleared on the
+world's stream so every step starts with a cold L2 (inside the timed region).
+
+Single world: replicas only. With --gpus N (one process per GPU under torchrun) every rank runs its
+own 100k world; `value` is all ranks' body-steps over the slowest rank's time.
+
+--impl reference times the reference's CPU algorithm (the oracle port, GPU-mode rules, all host
+threads) on a bounded sample of the same workload: the same generator at 2000 bodies, its whole
+rollout.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'three-avbd_b200'))
+
+METRIC = 'body-steps/s @100k boxes'
+UNIT = 'body-steps/s'
+PILE_BODIES = 100_000
+SAMPLE_BODIES = 2_000
+ROLLOUT = 600
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_config(n_bodies: int, steps: int) -> dict:
+    return {
+        'workload': f'drop pile: {n_bodies} bodies (70% boxes half-extents U[0.25,0.75], 30% spheres r U[0.2,0.6], density U[0.5,2], '
+                    f'friction U[0.3,0.8]) on a jittered 10-layer lattice, random orientations, speed U[0,1]; static ground box; '
+                    f'dt 1/60, 10 iterations, g -9.81; timed steps 1..{steps} of the rollout',
+        'bodies': n_bodies,
+        'iterations': 10,
+        'dt': 1 / 60,
+        'rollout_steps': ROLLOUT,
+        'seed': 1,
+        'spatial_sort': 'morton',
+        'l2': '256 MiB memset between timed steps, inside the timed region',
+    }
+
+
+def alg_bytes(s) -> float:
+    """Algorithmic (minimum) bytes of one topology+solve launch, from the step's own counters:
+    B_topo + B_warm + I (B_primal + B_dual) + B_vel with N dynamic bodies, M manifolds, P points,
+    A adjacency entries, P2 (dynamic body, point) incidences, J = 0 joints:
+      B_topo = 24 M + 16 A + 32 N, B_warm = 144 N, B_primal = 140 N + 92 A + 64 P2,
+      B_dual = 144 M + 92 P, B_vel = 88 N."""
+    N, M, P, A, P2 = float(s['dynamic_bodies']), float(s['manifolds']), float(s['contacts']), float(s['adjacency']), float(s['incidences'])
+    I = 10.0
+    return 24 * M + 16 * A + 32 * N + 144 * N + I * (140 * N + 92 * A + 64 * P2 + 144 * M + 92 * P) + 88 * N
+
+
+def measured_peak() -> tuple[float, str]:
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        return float(json.load(open(path))['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.device}', f'--query-gpu={self.QUERY}', '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ''
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for l in getattr(self, 'lines', []):
+            f = [x.strip() for x in l.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower() == 'active':
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': smax or None, 'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_reference(n_bodies: int, steps: int, threads: int) -> dict:
+    """The oracle (the reference's algorithm, GPU-mode rules) on the sampled pile's rollout."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    from avbd_b200.scenes import drop_pile
+    from oracle import Oracle, set_threads
+    used = set_threads(threads)
+    scene = drop_pile(n_bodies, seed=1)
+    o = Oracle(scene)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step_gpu()
+    dt = time.perf_counter() - t0
+    value = n_bodies * steps / dt
+    return {'value': value, 'unit': UNIT, 'cores': used, 'kind': 'port', 'seconds': dt,
+            'sample': f'drop pile generator at {n_bodies} bodies (same lattice, distributions and seed), steps 1..{steps} of its rollout, '
+                      f'C++ oracle in double (GPU-mode rules), {used} OpenMP threads'}
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    steps = min(args.steps, ROLLOUT)
+    ref = cpu_reference(SAMPLE_BODIES, steps, os.cpu_count() or 1)
+    line = {
+        'metric': METRIC, 'value': ref['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': steps, 'warmup': 0,
+        'ms_per_step': 1000 * ref['seconds'] / steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic', 'impl': 'reference', 'config': workload_config(SAMPLE_BODIES, steps),
+        'cpu_baseline': {'value': ref['value'], 'unit': UNIT, 'cores': ref['cores'], 'kind': 'port', 'sample': ref['sample']},
+        'e2e': {'value': ref['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=ROLLOUT)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='cuda', choices=['cuda', 'reference'])
+    ap.add_argument('--bodies', type=int, default=PILE_BODIES)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get('RANK', '0'))
+    world_size = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import avbd_b200
+    from avbd_b200.scenes import drop_pile
+
+    torch.cuda.set_device(local)
+    if world_size > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+
+    def barrier():
+        if world_size > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    scene = drop_pile(args.bodies, seed=1)
+    n_dyn = scene.dynamic_count
+
+    def fresh():
+        return avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
+
+    # Warm-up on its own world (module load, first touch), then a fresh world for the timed rollout
+    warm = fresh()
+    warm.step(args.warmup)
+    warm.synchronize()
+    warm.destroy()
+
+    w = fresh()
+    w.enable_step_stats(args.steps)
+    stream = torch.cuda.ExternalStream(w.stream, device=local)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                w.step(1)
+                flush.zero_()
+            end.record(stream)
+        w.synchronize()
+        barrier()
+    ms = start.elapsed_time(end)
+    stats = w.read_step_stats()
+    counters = w.read_counters()
+    if counters['error'] or counters['overflow']:
+        print(f'warning: counters {counters}', file=sys.stderr)
+    w.destroy()
+
+    t = torch.tensor([ms], dtype=torch.float64, device=f'cuda:{local}')
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world_size * n_dyn * args.steps / (ms_max / 1000.0)
+
+    # Roofline of the dominant kernel (the cooperative topology+solve launch), over the timed steps
+    solve_ms = float(stats['solve_ms'].sum())
+    coll_ms = float(stats['collision_ms'].sum())
+    bytes_alg = float(sum(alg_bytes(s) for s in stats))
+    achieved = bytes_alg / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else 0.0
+    peak, peak_kind = measured_peak()
+    traffic = None
+    prof = os.path.join(ROOT, 'profiles', 'topology_solve_traffic.json')
+    if os.path.exists(prof):
+        try:
+            tp = json.load(open(prof))
+            # dram bytes per algorithmic byte in the captured launch, applied to this run's launches
+            traffic = tp['dram_bytes'] / tp['alg_bytes'] * bytes_alg / len(stats)
+        except Exception:
+            traffic = None
+
+    # End to end through the public API with host buffers: each step uploads the bodies from pinned
+    # host memory, steps, and reads the bodies back (World.read's path), then waits for them.
+    e2e = None
+    if not args.no_e2e:
+        w2 = fresh()
+        host = torch.empty(w2.body_count * 160, dtype=torch.uint8).pin_memory()
+        host_np = host.numpy().view(avbd_b200.BODY_DTYPE)
+        w2.read_bodies_into(host_np)
+        s2 = torch.cuda.ExternalStream(w2.stream, device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        with torch.cuda.stream(s2):
+            e0.record(s2)
+            for _ in range(args.steps):
+                w2.write_bodies_async(host_np)
+                w2.step(1)
+                w2.read_bodies_into(host_np, sync=True)
+            e1.record(s2)
+        w2.synchronize()
+        barrier()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
+        if world_size > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        nbytes = w2.body_count * 160
+        e2e = {'value': world_size * n_dyn * args.steps / (float(te.item()) / 1000.0), 'unit': UNIT, 'h2d_bytes_per_step': nbytes,
+               'd2h_bytes_per_step': nbytes}
+        w2.destroy()
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        ref = cpu_reference(SAMPLE_BODIES, ROLLOUT, os.cpu_count() or 1)
+        cpu = {k: ref[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+
+    if rank == 0:
+        name = avbd_b200.device_info(local)
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world_size, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps), parallelism=f'replicas x{world_size}'),
+            'roofline': {'bound': 'hbm', 'kernel': 'k_topology_solve', 'achieved': achieved, 'peak': peak, 'peak_kind': peak_kind, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / max(len(stats), 1)},
+            'phases_ms_per_step': {'collision': coll_ms / max(len(stats), 1), 'topology_solve': solve_ms / max(len(stats), 1)},
+            'pile_last_step': {k: int(stats[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors', 'dynamic_bodies')} if len(stats) else None,
+            'gpu_launches': int(stats['launches'].sum()),
+            'clocks': clocks.summary(),
+            'e2e': e2e,
+            'cpu_baseline': cpu,
+            'device': name[0] if name else None,
+        }
+        print(json.dumps(line), flush=True)
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

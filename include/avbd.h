@@ -196,10 +196,24 @@ int avbd_read_counters(avbd_world* world, avbd_counters* counters);
 /* Asynchronous pose readback into caller memory (pinned for overlap): World.read (world.ts:2102-2224). */
 int avbd_read_bodies_async(avbd_world* world, avbd_body* dst, uint32_t cap);
 
-/* Device-side timing of the last `avbd_step` call's kernels, per phase (ms): collision,
- * topology + solve (profileNextStep, gpu/solver.ts:1951-1953). Requires enable != 0 before stepping. */
-int avbd_enable_timing(avbd_world* world, int enable);
-int avbd_last_timing(avbd_world* world, float* collision_ms, float* solve_ms);
+/* Per-step statistics (profileNextStep / readCounters, gpu/solver.ts:1951-1953, 2305-2309): with
+ * avbd_enable_step_stats(world, capacity) each step records device times of its two phases and a
+ * snapshot of its counters into a ring of `capacity` entries, without host synchronisation;
+ * avbd_read_step_stats returns them oldest first. capacity 0 turns it off. */
+typedef struct avbd_step_stats {
+  float collision_ms, solve_ms;  /* broadphase + narrowphase; topology + warm start + iterations + velocities */
+  uint32_t pairs, contacts, manifolds, adjacency, incidences, dynamic_bodies, colors, rounds, launches, error;
+} avbd_step_stats;
+int avbd_enable_step_stats(avbd_world* world, uint32_t capacity);
+int avbd_read_step_stats(avbd_world* world, avbd_step_stats* dst, uint32_t cap, uint32_t* n);
+
+/* The world's CUDA stream (cudaStream_t) for callers that order their own device work with its steps. */
+int avbd_world_stream(avbd_world* world, void** stream);
+
+/* Pose/velocity update from caller memory (pinned for overlap), enqueued on the world's stream
+ * without validation or synchronisation: shapes, masses and radii must be unchanged (use
+ * avbd_write_bodies for those). Keeps the bodies' contact history. */
+int avbd_write_bodies_async(avbd_world* world, uint32_t first, const avbd_body* bodies, uint32_t n);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,9 @@
 #include <memory>
 #include <unordered_map>
 #include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace orc {
 
@@ -900,12 +903,6 @@ template <class Ign> std::vector<std::pair<uint32_t, uint32_t>> gpuPairs(const s
   auto key = [](int64_t x, int64_t y, int64_t z) { return (uint64_t(x & 0x1fffff) << 42) | (uint64_t(y & 0x1fffff) << 21) | uint64_t(z & 0x1fffff); };
   for (int i = 0; i < n; i++) if (!large[i]) { auto c = cellOf(i); grid[key(c[0], c[1], c[2])].push_back(i); }
   std::vector<std::pair<uint32_t, uint32_t>> out;
-  auto emit = [&](int p, int j) {
-    if (!pairTest32(B[p], B[j])) return;
-    uint32_t a = std::max(p, j), b = std::min(p, j);
-    if (ignored(a, b)) return;
-    out.push_back({a, b});
-  };
   // Which body probes (findPairs / findFixedLarge ownership, wgsl-collision.ts:243-323)
   auto prober = [&](int i, int j) -> int {
     bool di = B[i].mass > 0, dj = B[j].mass > 0;
@@ -918,23 +915,43 @@ template <class Ign> std::vector<std::pair<uint32_t, uint32_t>> gpuPairs(const s
     if (!large[fix] && large[dyn]) return fix;  // findFixedLarge
     return dyn;
   };
-  for (int i = 0; i < n; i++) {
-    if (large[i]) continue;
-    auto c = cellOf(i);
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
-          auto it = grid.find(key(c[0] + dx, c[1] + dy, c[2] + dz));
-          if (it == grid.end()) continue;
-          for (int j : it->second) if (j < i) emit(prober(i, j), prober(i, j) == i ? j : i);
-        }
-  }
-  for (int l : largeList)
-    for (int j = 0; j < n; j++) {
-      if (j == l || (large[j] && j > l)) continue;  // large-large once
-      int p = prober(l, j);
-      emit(p, p == l ? j : l);
+#pragma omp parallel
+  {
+    std::vector<std::pair<uint32_t, uint32_t>> local;
+    auto emit = [&](int p, int j) {
+      if (!pairTest32(B[p], B[j])) return;
+      uint32_t a = std::max(p, j), b = std::min(p, j);
+      if (ignored(a, b)) return;
+      local.push_back({a, b});
+    };
+#pragma omp for schedule(dynamic, 256)
+    for (int i = 0; i < n; i++) {
+      if (large[i]) continue;
+      auto c = cellOf(i);
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            auto it = grid.find(key(c[0] + dx, c[1] + dy, c[2] + dz));
+            if (it == grid.end()) continue;
+            for (int j : it->second)
+              if (j < i) {
+                int p = prober(i, j);
+                emit(p, p == i ? j : i);
+              }
+          }
     }
+#pragma omp for schedule(dynamic, 1)
+    for (int li = 0; li < int(largeList.size()); li++) {
+      int l = largeList[li];
+      for (int j = 0; j < n; j++) {
+        if (j == l || (large[j] && j > l)) continue;  // large-large once
+        int p = prober(l, j);
+        emit(p, p == l ? j : l);
+      }
+    }
+#pragma omp critical
+    out.insert(out.end(), local.begin(), local.end());
+  }
   std::sort(out.begin(), out.end());
   out.erase(std::unique(out.begin(), out.end()), out.end());
   return out;
@@ -1220,7 +1237,10 @@ template <class T> struct Solver {
       forces = std::move(kept);
     }
     auto pr = pairs();
-    for (auto& p : pr) {
+    std::vector<std::unique_ptr<Manifold<T>>> made(pr.size());
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long pi = 0; pi < long(pr.size()); pi++) {
+      auto& p = pr[pi];
       int a = int(p.first), b = int(p.second);
       Body<T>& A = bodies[a];
       Body<T>& B = bodies[b];
@@ -1275,8 +1295,10 @@ template <class T> struct Solver {
         c.penalty[0] = tmax(c.penalty[0], penaltyMin);
         m->contacts.push_back(c);
       }
-      addForce(std::move(m));
+      made[pi] = std::move(m);
     }
+    for (auto& m : made)
+      if (m) addForce(std::move(m));
     // Per-body summation order
     std::vector<std::vector<Force<T>*>> order(n);
     for (auto& up : forces) {
@@ -1289,10 +1311,11 @@ template <class T> struct Solver {
       std::unordered_map<Force<T>*, int> idx;
       int s = 0;
       for (auto& up : forces) idx[up.get()] = s++;
+#pragma omp parallel for schedule(dynamic, 256)
       for (int b = 0; b < n; b++) {
         std::stable_sort(order[b].begin(), order[b].end(), [&](Force<T>* x, Force<T>* y) {
           auto key = [&](Force<T>* f) -> std::pair<uint64_t, uint64_t> {
-            if (f->kind != K_MANIFOLD) return {0, uint64_t(idx[f])};
+            if (f->kind != K_MANIFOLD) return {0, uint64_t(idx.at(f))};
             int other = f->bodyA == b ? f->bodyB : f->bodyA;
             auto* m = static_cast<Manifold<T>*>(f);
             return {uint64_t(other + 2), uint64_t(m->contacts.empty() ? 0 : m->contacts[0].feature & ~STICK_BIT)};
@@ -1336,8 +1359,13 @@ template <class T> struct Solver {
 
     warmStartBodies(true);
     for (int it = 0; it < iterations; it++) {
-      for (int c = 0; c < ncol; c++) for (int b : buckets[c]) primal(b, true, &order[b]);
-      for (auto& f : forces) f->updateDual(alpha);
+      for (int c = 0; c < ncol; c++) {
+        const std::vector<int>& bucket = buckets[c];
+#pragma omp parallel for schedule(dynamic, 64)
+        for (long k = 0; k < long(bucket.size()); k++) primal(bucket[k], true, &order[bucket[k]]);
+      }
+#pragma omp parallel for schedule(dynamic, 256)
+      for (long f = 0; f < long(forces.size()); f++) forces[f]->updateDual(alpha);
     }
     velocities(true);
   }
@@ -1594,5 +1622,16 @@ void orc_color_graph(int n, const unsigned char* dynamic, const int* start, cons
 }
 
 unsigned orc_hash32(unsigned x) { return hash32(x); }
+
+// Host threads for the GPU-mode step (OpenMP); returns the count in use.
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
 
 }  // extern "C"

@@ -56,6 +56,8 @@ def lib():
         L.orc_narrowphase.argtypes = [P, I, I, I, D, D]
         L.orc_narrowphase.restype = I
         L.orc_color_graph.argtypes = [I, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(U), I, I, ctypes.POINTER(I)]
+        L.orc_set_threads.argtypes = [I]
+        L.orc_set_threads.restype = I
         L.orc_hash32.argtypes = [U]
         L.orc_hash32.restype = U
         _lib = L
@@ -210,6 +212,11 @@ class Oracle:
 
     def colors(self) -> np.ndarray:
         return self.bodies()[:, 42].astype(np.uint32)
+
+
+def set_threads(n: int) -> int:
+    """OpenMP threads of the GPU-mode step (0: keep); returns the count in use."""
+    return lib().orc_set_threads(n)
 
 
 def sequential_colors(scene) -> np.ndarray:

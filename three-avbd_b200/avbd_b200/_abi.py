@@ -50,6 +50,8 @@ CONTACT_DTYPE = np.dtype([
     ('r_a', '<f4', 3), ('key', '<u4'), ('r_b', '<f4', 3), ('c0_n', '<f4'), ('pen', '<f4', 3), ('c0_t1', '<f4'),
     ('lam', '<f4', 3), ('c0_t2', '<f4'),
 ])
+STEP_STATS_DTYPE = np.dtype([('collision_ms', '<f4'), ('solve_ms', '<f4')] + [(n, '<u4') for n in (
+    'pairs', 'contacts', 'manifolds', 'adjacency', 'incidences', 'dynamic_bodies', 'colors', 'rounds', 'launches', 'error')])
 assert BODY_DTYPE.itemsize == 160 and JOINT_DTYPE.itemsize == 160 and MANIFOLD_DTYPE.itemsize == 32 and CONTACT_DTYPE.itemsize == 64
 
 
@@ -101,8 +103,10 @@ SIGNATURES = {
     'avbd_read_colors': ([P, PU, U, PU], I),
     'avbd_read_counters': ([P, ctypes.POINTER(Counters)], I),
     'avbd_read_bodies_async': ([P, VP, U], I),
-    'avbd_enable_timing': ([P, I], I),
-    'avbd_last_timing': ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)], I),
+    'avbd_enable_step_stats': ([P, U], I),
+    'avbd_read_step_stats': ([P, VP, U, PU], I),
+    'avbd_world_stream': ([P, ctypes.POINTER(ctypes.c_void_p)], I),
+    'avbd_write_bodies_async': ([P, U, VP, U], I),
 }
 
 _lib = None

@@ -32,24 +32,26 @@ def finite(x: float) -> float:
 def pack_bodies(bodies, up=(0.0, 0.0, 1.0)) -> np.ndarray:
     """Scene bodies (f64) as device records (GpuSolver3D.pack, solver.ts:1176-1212)."""
     out = np.zeros(len(bodies), dtype=BODY_DTYPE)
-    for k, b in enumerate(bodies):
-        r = out[k]
-        r['pos'] = b.pos
-        r['friction'] = b.friction
-        r['rot'] = b.rot
-        r['initial_pos'] = b.initial_pos
-        r['flags'] = 1.0
-        r['initial_rot'] = b.initial_rot
-        r['size'] = b.size
-        r['mass'] = b.mass
-        r['moment'] = b.moment
-        r['radius'] = b.radius
-        r['inertial_pos'] = b.inertial_pos
-        r['inertial_rot'] = b.inertial_rot
-        r['vel'] = b.vel
-        r['prev_up_vel'] = b.prev_vel[0] * up[0] + b.prev_vel[1] * up[1] + b.prev_vel[2] * up[2]
-        r['ang_vel'] = b.ang_vel
-        r['shape'] = float(b.shape)
+    if not len(bodies):
+        return out
+    col = lambda name: np.array([getattr(b, name) for b in bodies], dtype=np.float64)
+    out['pos'] = col('pos')
+    out['friction'] = col('friction')
+    out['rot'] = col('rot')
+    out['initial_pos'] = col('initial_pos')
+    out['flags'] = 1.0
+    out['initial_rot'] = col('initial_rot')
+    out['size'] = col('size')
+    out['mass'] = col('mass')
+    out['moment'] = col('moment')
+    out['radius'] = col('radius')
+    out['inertial_pos'] = col('inertial_pos')
+    out['inertial_rot'] = col('inertial_rot')
+    out['vel'] = col('vel')
+    pv = col('prev_vel')
+    out['prev_up_vel'] = pv[:, 0] * up[0] + pv[:, 1] * up[1] + pv[:, 2] * up[2]
+    out['ang_vel'] = col('ang_vel')
+    out['shape'] = col('shape')
     return out
 
 
@@ -259,13 +261,27 @@ class CudaSolver3D:
     def synchronize(self):
         self._check(self.lib.avbd_synchronize(self.handle))
 
-    def enable_timing(self, on: bool = True):
-        self._check(self.lib.avbd_enable_timing(self.handle, 1 if on else 0))
+    def enable_step_stats(self, capacity: int):
+        """Record per-step device times and counters into a ring of `capacity` steps (no host syncs)."""
+        self._check(self.lib.avbd_enable_step_stats(self.handle, capacity))
 
-    def last_timing(self):
-        a, b = ctypes.c_float(), ctypes.c_float()
-        self._check(self.lib.avbd_last_timing(self.handle, ctypes.byref(a), ctypes.byref(b)))
-        return a.value, b.value
+    def read_step_stats(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_step_stats(self.handle, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=_abi.STEP_STATS_DTYPE)
+        self._check(self.lib.avbd_read_step_stats(self.handle, ptr(out), n.value, ctypes.byref(n)))
+        return out
+
+    @property
+    def stream(self) -> int:
+        """The world's cudaStream_t, for torch.cuda.ExternalStream."""
+        s = ctypes.c_void_p()
+        self._check(self.lib.avbd_world_stream(self.handle, ctypes.byref(s)))
+        return s.value or 0
+
+    def write_bodies_async(self, records: np.ndarray, first: int = 0):
+        """Pose/velocity upload from (pinned) host memory on the world's stream; shapes unchanged."""
+        self._check(self.lib.avbd_write_bodies_async(self.handle, first, ptr(records), len(records)))
 
     # --- readbacks ---
     @property

@@ -707,8 +707,9 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
 }
 
 // Host: the collision phase, enqueued on `s`.
-void launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s) {
+uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s) {
   const uint32_t n = p.n;
+  uint32_t launches = 3;  // begin, hash insert, narrowphase
   k_begin<<<1, 1, 0, s>>>(w, p);
   cudaMemsetAsync(w.hash, 0, (size_t(p.hashMask) + 1) * 4, s);
   k_hash_insert<<<GS_BLOCKS, 256, 0, s>>>(w, p);
@@ -727,13 +728,16 @@ void launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, 
       k_radix_hist<<<tiles, SORT_THREADS, 0, s>>>(kin, n, shift, w.radixHist, tiles);
       k_scan_single<<<1, 1024, 0, s>>>(w.radixHist, RADIX * tiles);
       k_radix_scatter<<<tiles, SORT_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, w.radixHist, tiles);
+      launches += 3;
       uint32_t* t = kin; kin = kout; kout = t;
       t = vin; vin = vout; vout = t;
     }
     k_cell_ranges<<<grid_for(n, 256), 256, 0, s>>>(kin, n, w.cellStart, w.cellEnd, p.tableMask + 1u);
     k_find_pairs<<<grid_for(n, 128), 128, 0, s>>>(w, p, vin);
+    launches += 3;  // cell keys, cell ranges, find pairs
   }
   k_narrowphase<<<GS_BLOCKS, 128, 0, s>>>(w, p);
+  return launches;
 }
 
 }  // namespace avbd

@@ -33,7 +33,7 @@ constexpr uint32_t OWNER_BIT = 0x80000000u;  // incidence entry: this body updat
 // Counter words (device memory)
 enum : int {
   C_PAIRS = 0, C_CONTACTS = 1, C_MANIFOLDS = 2, C_OVERFLOW = 3, C_CLASHES = 4, C_COLORS = 5, C_ROUNDS = 6, C_ERROR = 7,
-  C_PREV_PAIRS = 8, C_PENDING = 16,  // 16..16+2*MAX_ROUND_PAIRS: pending counts per round pair
+  C_PREV_PAIRS = 8, C_ADJ = 9, C_INC = 10, C_DYN = 11, C_PENDING = 16,  // 16..16+2*MAX_ROUND_PAIRS: pending counts per round pair
   COUNTER_WORDS = 128,
 };
 constexpr int MAX_ROUND_PAIRS = 32;
@@ -148,7 +148,7 @@ __host__ __device__ inline uint32_t pairHash(uint32_t a, uint32_t b) { return ha
 inline uint32_t grid_for(uint32_t n, uint32_t block) { return (n + block - 1) / block; }
 
 // Host launchers (avbd_collide.cu)
-void launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s);
+uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s);
 // Host launchers (avbd_solve.cu)
 int solve_grid_blocks(int device);
 cudaError_t launch_topology_solve(const DWorld& w, const StepParams& p, int blocks, cudaStream_t s);

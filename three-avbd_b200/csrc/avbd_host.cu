@@ -85,9 +85,12 @@ struct avbd_world {
   uint32_t* hCounters = nullptr;
   cudaEvent_t countersReady = nullptr;
   bool countersInFlight = false;
-  bool timing = false;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-  float lastCollisionMs = 0.0f, lastSolveMs = 0.0f;
+  // per-step statistics ring: 3 events and a counter snapshot per entry
+  uint32_t statsCap = 0, statsCount = 0;
+  std::vector<cudaEvent_t> statsEvents;
+  uint32_t* statsCounters = nullptr;  // device, statsCap * COUNTER_WORDS
+  std::vector<uint32_t> statsLaunches;
+  uint32_t launchesPerStep = 0;
   std::vector<void*> allocations;
 };
 
@@ -416,8 +419,6 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   if (cudaMallocHost(&w->hCounters, COUNTER_WORDS * sizeof(uint32_t)) != cudaSuccess) return bad(AVBD_ERR_CUDA);
   std::memset(w->hCounters, 0, COUNTER_WORDS * sizeof(uint32_t));
   if (cudaEventCreateWithFlags(&w->countersReady, cudaEventDisableTiming) != cudaSuccess) return bad(AVBD_ERR_CUDA);
-  for (auto& e : w->ev)
-    if (cudaEventCreate(&e) != cudaSuccess) return bad(AVBD_ERR_CUDA);
   if (cudaStreamSynchronize(w->stream) != cudaSuccess) return bad(AVBD_ERR_CUDA);
   *out = w;
   return AVBD_OK;
@@ -431,7 +432,7 @@ int avbd_world_destroy(avbd_world* w) {
   w->allocations.clear();
   if (w->hCounters) cudaFreeHost(w->hCounters);
   if (w->countersReady) cudaEventDestroy(w->countersReady);
-  for (auto& e : w->ev)
+  for (auto& e : w->statsEvents)
     if (e) cudaEventDestroy(e);
   if (w->stream) cudaStreamDestroy(w->stream);
   delete w;
@@ -674,12 +675,22 @@ int avbd_step(avbd_world* w, int n) {
     }
     w->stepCount++;
     StepParams p = makeParams(w);
-    if (w->timing) cudaEventRecord(w->ev[0], w->stream);
-    launch_collision(w->d, p, w->tableSize, w->stream);
-    if (w->timing) cudaEventRecord(w->ev[1], w->stream);
+    const uint32_t slot = w->statsCap ? w->statsCount % w->statsCap : 0;
+    cudaEvent_t* ev = w->statsCap ? &w->statsEvents[3 * slot] : nullptr;
+    if (ev) cudaEventRecord(ev[0], w->stream);
+    uint32_t launches = launch_collision(w->d, p, w->tableSize, w->stream);
+    if (ev) cudaEventRecord(ev[1], w->stream);
     CUDA_TRY(w, cudaGetLastError());
     CUDA_TRY(w, launch_topology_solve(w->d, p, w->solveBlocks, w->stream));
-    if (w->timing) cudaEventRecord(w->ev[2], w->stream);
+    launches += 1;
+    w->launchesPerStep = launches;
+    if (ev) {
+      cudaEventRecord(ev[2], w->stream);
+      CUDA_TRY(w, cudaMemcpyAsync(w->statsCounters + size_t(slot) * COUNTER_WORDS, w->d.counters, COUNTER_WORDS * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToDevice, w->stream));
+      w->statsLaunches[slot] = launches;
+      w->statsCount++;
+    }
     CUDA_TRY(w, cudaMemcpyAsync(w->hCounters, w->d.counters, COUNTER_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, w->stream));
     CUDA_TRY(w, cudaEventRecord(w->countersReady, w->stream));
     w->countersInFlight = true;
@@ -696,10 +707,6 @@ int avbd_synchronize(avbd_world* w) {
     CUDA_TRY(w, cudaEventSynchronize(w->countersReady));
     w->countersInFlight = false;
     if (w->hCounters[C_ERROR]) return fail(w, AVBD_ERR_TIMEOUT, "the step gave up: error bits " + std::to_string(w->hCounters[C_ERROR]));
-  }
-  if (w->timing) {
-    cudaEventElapsedTime(&w->lastCollisionMs, w->ev[0], w->ev[1]);
-    cudaEventElapsedTime(&w->lastSolveMs, w->ev[1], w->ev[2]);
   }
   return AVBD_OK;
 }
@@ -839,16 +846,68 @@ int avbd_read_colors(avbd_world* w, uint32_t* dst, uint32_t cap, uint32_t* n) {
   return AVBD_OK;
 }
 
-int avbd_enable_timing(avbd_world* w, int enable) {
+int avbd_enable_step_stats(avbd_world* w, uint32_t capacity) {
   if (!w) return AVBD_ERR_INVALID;
-  w->timing = enable != 0;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  for (auto& e : w->statsEvents) cudaEventDestroy(e);
+  w->statsEvents.clear();
+  dfree(w, w->statsCounters);
+  w->statsCounters = nullptr;
+  w->statsCap = capacity;
+  w->statsCount = 0;
+  w->statsLaunches.assign(capacity, 0);
+  if (!capacity) return AVBD_OK;
+  w->statsEvents.resize(size_t(capacity) * 3, nullptr);
+  for (auto& e : w->statsEvents) CUDA_TRY(w, cudaEventCreate(&e));
+  CUDA_TRY(w, dalloc(w, &w->statsCounters, size_t(capacity) * COUNTER_WORDS));
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   return AVBD_OK;
 }
 
-int avbd_last_timing(avbd_world* w, float* coll, float* solve) {
+int avbd_read_step_stats(avbd_world* w, avbd_step_stats* dst, uint32_t cap, uint32_t* n) {
   if (!w) return AVBD_ERR_INVALID;
-  if (coll) *coll = w->lastCollisionMs;
-  if (solve) *solve = w->lastSolveMs;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  uint32_t have = std::min(w->statsCount, w->statsCap);
+  if (n) *n = have;
+  if (!dst || !have) return AVBD_OK;
+  std::vector<uint32_t> c(size_t(w->statsCap) * COUNTER_WORDS);
+  CUDA_TRY(w, cudaMemcpy(c.data(), w->statsCounters, c.size() * 4, cudaMemcpyDeviceToHost));
+  uint32_t first = w->statsCount - have;
+  for (uint32_t k = 0; k < have && k < cap; k++) {
+    uint32_t slot = (first + k) % w->statsCap;
+    avbd_step_stats& s = dst[k];
+    cudaEvent_t* ev = &w->statsEvents[3 * slot];
+    s.collision_ms = s.solve_ms = 0.0f;
+    cudaEventElapsedTime(&s.collision_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&s.solve_ms, ev[1], ev[2]);
+    const uint32_t* q = &c[size_t(slot) * COUNTER_WORDS];
+    s.pairs = q[C_PAIRS];
+    s.contacts = q[C_CONTACTS];
+    s.manifolds = q[C_MANIFOLDS];
+    s.adjacency = q[C_ADJ];
+    s.incidences = q[C_INC];
+    s.dynamic_bodies = q[C_DYN];
+    s.colors = q[C_COLORS];
+    s.rounds = q[C_ROUNDS];
+    s.launches = w->statsLaunches[slot];
+    s.error = q[C_ERROR];
+  }
+  return AVBD_OK;
+}
+
+int avbd_world_stream(avbd_world* w, void** stream) {
+  if (!w || !stream) return AVBD_ERR_INVALID;
+  *stream = (void*)w->stream;
+  return AVBD_OK;
+}
+
+int avbd_write_bodies_async(avbd_world* w, uint32_t first, const avbd_body* bodies, uint32_t n) {
+  if (!w || (!bodies && n) || uint64_t(first) + n > w->n) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  if (n) copyBodiesIn(w, first, bodies, n, cudaMemcpyHostToDevice);
+  CUDA_TRY(w, cudaGetLastError());
   return AVBD_OK;
 }
 

@@ -562,6 +562,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
   }
   GSYNC
   if (!grid_scan(w.adjStart, n + 1, w.scanScratch, bar, ctr)) return;
+  if (tid == 0) ctr[C_ADJ] = w.adjStart[n];
   // B. fill (adjFill zeroed by the host), then each body's list sorted into its summation order
   for (uint32_t c = tid; c < ncons; c += T) {
     int ea, eb;
@@ -721,6 +722,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
   GSYNC
   if (!grid_scan(w.incStart, numDyn + 1, w.scanScratch, bar, ctr)) return;
   const uint32_t totalInc = ldv(&w.scanScratch[gridDim.x]);
+  if (tid == 0) {
+    ctr[C_INC] = totalInc;
+    ctr[C_DYN] = numDyn;
+  }
   if (totalInc > p.incCap) {
     if (tid == 0) atomicOr(&ctr[C_ERROR], ERR_INC_OVERFLOW);
     return;  // uniform: every block read the same total after the barrier
