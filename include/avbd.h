@@ -207,6 +207,10 @@ typedef struct avbd_step_stats {
 int avbd_enable_step_stats(avbd_world* world, uint32_t capacity);
 int avbd_read_step_stats(avbd_world* world, avbd_step_stats* dst, uint32_t cap, uint32_t* n);
 
+/* Device time (ms from the start of the topology+solve launch) at each of its grid barriers in the
+ * last step: the per-phase profile of the persistent kernel (profileNextStep's phases, gpu/solver.ts:2159-2172). */
+int avbd_read_phase_clocks(avbd_world* world, double* dst, uint32_t cap, uint32_t* n);
+
 /* The world's CUDA stream (cudaStream_t) for callers that order their own device work with its steps. */
 int avbd_world_stream(avbd_world* world, void** stream);
 

@@ -106,6 +106,7 @@ SIGNATURES = {
     'avbd_enable_step_stats': ([P, U], I),
     'avbd_read_step_stats': ([P, VP, U, PU], I),
     'avbd_world_stream': ([P, ctypes.POINTER(ctypes.c_void_p)], I),
+    'avbd_read_phase_clocks': ([P, ctypes.POINTER(ctypes.c_double), U, PU], I),
     'avbd_write_bodies_async': ([P, U, VP, U], I),
 }
 

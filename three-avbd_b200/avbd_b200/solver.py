@@ -272,6 +272,13 @@ class CudaSolver3D:
         self._check(self.lib.avbd_read_step_stats(self.handle, ptr(out), n.value, ctypes.byref(n)))
         return out
 
+    def read_phase_clocks(self) -> np.ndarray:
+        """Device time (ms) at each grid barrier of the last step's topology+solve launch."""
+        out = np.zeros(1024, dtype=np.float64)
+        n = ctypes.c_uint32()
+        self._check(self.lib.avbd_read_phase_clocks(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1024, ctypes.byref(n)))
+        return out[:n.value]
+
     @property
     def stream(self) -> int:
         """The world's cudaStream_t, for torch.cuda.ExternalStream."""

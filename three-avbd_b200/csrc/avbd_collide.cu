@@ -14,7 +14,7 @@ namespace cg = cooperative_groups;
 
 namespace avbd {
 
-constexpr int RADIX_BITS = 8, RADIX = 1 << RADIX_BITS, SORT_THREADS = 256, SORT_ITEMS = 8, SORT_TILE = SORT_THREADS * SORT_ITEMS;
+
 constexpr int GS_BLOCKS = 148 * 8;  // grid-stride kernels over device-side counts
 
 __device__ inline bool enabled(const DWorld& w, uint32_t i) {
@@ -86,103 +86,101 @@ __global__ void k_cell_keys(DWorld w, StepParams p) {
   w.valA[i] = i;
 }
 
-// --- stable LSD radix sort of (key, value) -----------------------------------------------------------
-// Per pass: per-tile digit histogram, one exclusive scan over (digit, tile), and a stable scatter
-// ranking each tile's keys with warp match + per-warp digit counts.
-__global__ void __launch_bounds__(SORT_THREADS) k_radix_hist(const uint32_t* keys, uint32_t n, int shift, uint32_t* hist, uint32_t tiles) {
-  __shared__ uint32_t counts[RADIX];
-  counts[threadIdx.x] = 0;
-  __syncthreads();
-  uint32_t base = blockIdx.x * SORT_TILE;
-  for (int r = 0; r < SORT_ITEMS; r++) {
-    uint32_t i = base + r * SORT_THREADS + threadIdx.x;
-    if (i < n) atomicAdd(&counts[(keys[i] >> shift) & (RADIX - 1)], 1u);
-  }
-  __syncthreads();
-  hist[threadIdx.x * tiles + blockIdx.x] = counts[threadIdx.x];
+// --- counting sort of bodies by cell hash (a single radix pass on the whole key) -------------------
+// Count (each body keeps its rank in its bucket), exclusive scan of the bucket counts, scatter. The
+// order of bodies within a bucket follows the atomics and changes nothing downstream: pairs are a
+// set, and every body sums its rows in a sorted order of its own.
+__global__ void k_bucket_count(const uint32_t* keys, uint32_t n, uint32_t* count, uint32_t* rank, uint32_t sentinel) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k = keys[i];
+  rank[i] = k == sentinel ? 0u : atomicAdd(&count[k], 1u);
 }
 
-// Exclusive scan of `len` words in place by one block of 1024 threads.
+// Exclusive scan, three kernels: block tiles of 4096 (totals out), the totals, the tiles' offsets.
+constexpr int SCAN_THREADS = 1024, SCAN_ITEMS = 4, SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+__device__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32_t* warpSums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warpSums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = warpSums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warpSums[lane] = t;
+  }
+  __syncthreads();
+  uint32_t r = x - v + (warp > 0 ? warpSums[warp - 1] : 0u);
+  __syncthreads();
+  return r;
+}
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(uint32_t* data, uint32_t len, uint32_t* totals) {
+  __shared__ uint32_t warpSums[32];
+  uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS], sum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < len ? data[base + k] : 0u;
+    sum += v[k];
+  }
+  uint32_t run = block_exclusive_scan_1024(sum, warpSums);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < len) data[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == SCAN_THREADS - 1) totals[blockIdx.x] = run;
+}
 __global__ void __launch_bounds__(1024) k_scan_single(uint32_t* data, uint32_t len) {
   __shared__ uint32_t warpSums[32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint32_t base = 0; base < len; base += 1024) {
     uint32_t i = base + threadIdx.x;
     uint32_t v = i < len ? data[i] : 0u;
-    uint32_t x = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) warpSums[warp] = x;
+    uint32_t ex = block_exclusive_scan_1024(v, warpSums) + carry;
+    if (i < len) data[i] = ex;
     __syncthreads();
-    if (warp == 0) {
-      uint32_t s = warpSums[lane];
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-        if (lane >= o) s += y;
-      }
-      warpSums[lane] = s;
-    }
-    __syncthreads();
-    uint32_t incl = x + (warp > 0 ? warpSums[warp - 1] : 0u) + carry;
-    if (i < len) data[i] = incl - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) carry = incl;
+    if (threadIdx.x == 1023) carry = ex + v;
     __syncthreads();
   }
 }
-
-__global__ void __launch_bounds__(SORT_THREADS) k_radix_scatter(const uint32_t* keysIn, const uint32_t* valsIn, uint32_t* keysOut, uint32_t* valsOut,
-                                                                uint32_t n, int shift, const uint32_t* hist, uint32_t tiles) {
-  __shared__ uint32_t running[RADIX];
-  __shared__ uint32_t warpCount[SORT_THREADS / 32][RADIX];
-  __shared__ uint32_t tileCount[RADIX];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  running[threadIdx.x] = hist[threadIdx.x * tiles + blockIdx.x];
-  uint32_t base = blockIdx.x * SORT_TILE;
-  for (int r = 0; r < SORT_ITEMS; r++) {
-    for (int k = 0; k < SORT_THREADS / 32; k++) warpCount[k][threadIdx.x] = 0;
-    __syncthreads();
-    uint32_t i = base + r * SORT_THREADS + threadIdx.x;
-    bool live = i < n;
-    uint32_t key = live ? keysIn[i] : 0u;
-    uint32_t digit = live ? (key >> shift) & (RADIX - 1) : 0xffffffffu;
-    uint32_t peers = __match_any_sync(0xffffffffu, digit);
-    uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-    if (live && rank == 0) warpCount[warp][digit] = __popc(peers);
-    __syncthreads();
-    {
-      uint32_t s = 0;
-      for (int k = 0; k < SORT_THREADS / 32; k++) {
-        uint32_t c = warpCount[k][threadIdx.x];
-        warpCount[k][threadIdx.x] = s;
-        s += c;
-      }
-      tileCount[threadIdx.x] = s;
-    }
-    __syncthreads();
-    if (live) {
-      uint32_t pos = running[digit] + warpCount[warp][digit] + rank;
-      keysOut[pos] = key;
-      valsOut[pos] = valsIn[i];
-    }
-    __syncthreads();
-    running[threadIdx.x] += tileCount[threadIdx.x];
-  }
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* data, uint32_t len, const uint32_t* totals) {
+  uint32_t add = totals[blockIdx.x];
+  uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++)
+    if (base + k < len) data[base + k] += add;
 }
 
-// --- cell ranges in the sorted order -------------------------------------------------------------------
-__global__ void k_cell_ranges(const uint32_t* keys, uint32_t n, uint32_t* start, uint32_t* end, uint32_t sentinel) {
+// cellEnd held the counts: make it start + count
+__global__ void k_bucket_finish(const uint32_t* start, uint32_t* end, uint32_t len) {
+  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h < len) end[h] += start[h];
+}
+
+// Bodies into bucket order, with each sorted slot's candidate record (position and radius, exact cell
+// and body with its dynamic bit) so a cell walk reads contiguous memory.
+__global__ void k_bucket_scatter(DWorld w, uint32_t n, uint32_t sentinel) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  uint32_t k = keys[i];
+  uint32_t k = w.keyA[i];
   if (k == sentinel) return;
-  if (i == 0 || keys[i - 1] != k) start[k] = i;
-  if (i == n - 1 || keys[i + 1] != k) end[k] = i + 1;
+  uint32_t slot = w.cellStart[k] + w.valB[i];
+  float4 pi = w.pos[i];
+  w.sortedPR[slot] = make_float4(pi.x, pi.y, pi.z, w.moment[i].w);
+  int4 c = w.cell[i];
+  w.sortedCell[slot] = make_int4(c.x, c.y, c.z, (int)(i | (w.size[i].w > 0.0f ? 0x80000000u : 0u)));
 }
 
 // --- pair tests (wgsl-collision.ts:150-234) ------------------------------------------------------------
@@ -294,45 +292,77 @@ __device__ inline void testPair(const DWorld& w, const StepParams& p, const Prob
   emitPair(w, p, a, b);
 }
 
-// findPairs + findFixedLarge (wgsl-collision.ts:242-323): a dynamic body probes the 27 cells around
-// it (same-level dynamic pairs belong to the higher index, fixed pairs to the mover) and the large
-// bodies; a small fixed body probes the large dynamic ones.
-__global__ void __launch_bounds__(128) k_find_pairs(DWorld w, StepParams p, const uint32_t* sortedVals) {
+// Which body's view a pair is tested from (findPairs / findFixedLarge ownership, wgsl-collision.ts:
+// 242-323): two small dynamic bodies from the higher index, small against large from the small one,
+// two large dynamic ones from the lower index, a fixed body's pair from the mover, except a small
+// fixed body against a large mover (findFixedLarge). The f32 tests round differently from either
+// side, so the GPU's own choice is kept.
+__device__ inline uint32_t proberOf(const DWorld& w, const StepParams& p, uint32_t i, uint32_t j) {
+  bool di = w.size[i].w > 0.0f, dj = w.size[j].w > 0.0f;
+  bool li = w.moment[i].w > p.largeThreshold, lj = w.moment[j].w > p.largeThreshold;
+  if (di && dj) {
+    if (!li && !lj) return max(i, j);
+    if (li != lj) return li ? j : i;
+    return min(i, j);
+  }
+  uint32_t dyn = di ? i : j, fix = di ? j : i;
+  bool lfix = di ? lj : li, ldyn = di ? li : lj;
+  if (!lfix && ldyn) return fix;
+  return dyn;
+}
+
+__device__ inline void testFromProber(const DWorld& w, const StepParams& p, const Probe& P, uint32_t j) {
+  uint32_t pr = proberOf(w, p, P.index, j);
+  if (pr == P.index) testPair(w, p, P, j);
+  else testPair(w, p, probeOf(w, pr), P.index);
+}
+
+// The grid walk: every small body (fixed ones too) visits its own cell (bodies of lower index) and
+// the 13 cells of its forward half-shell, so each small-small pair is visited once; cells are at
+// least twice the largest small radius, so this covers every overlap. Large bodies test against
+// everything (the large list), as the reference's do.
+__global__ void __launch_bounds__(128) k_find_pairs(DWorld w, StepParams p) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.n || !enabled(w, i)) return;
   bool dyn = w.size[i].w > 0.0f;
   bool small = w.moment[i].w <= p.largeThreshold;
-  if (!dyn) {
-    if (!small || p.anyDynamicLarge == 0u) return;
+  if (small) {
     Probe P = probeOf(w, i);
-    for (uint32_t k = 0; k < p.nLarge; k++) {
-      uint32_t l = w.large[k];
-      if (!enabled(w, l) || w.size[l].w <= 0.0f) continue;
-      testPair(w, p, P, l);
+    int4 c = w.cell[i];
+    for (int o = 0; o < 14; o++) {
+      // offset o = 0: the own cell; 1..13: (dx, dy, dz) > 0 in (z, y, x) order
+      int q = o == 0 ? 13 : 13 + o;
+      int4 cc = make_int4(c.x + q % 3 - 1, c.y + (q / 3) % 3 - 1, c.z + q / 9 - 1, 0);
+      uint32_t h = cellHash(cc, p.tableMask);
+      uint32_t end = w.cellEnd[h];
+      for (uint32_t k = w.cellStart[h]; k < end; k++) {
+        int4 cj = w.sortedCell[k];
+        uint32_t j = (uint32_t)cj.w & 0x7fffffffu;
+        bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
+        if (o == 0 && j >= i) continue;
+        if (!dyn && !dj) continue;
+        if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
+        float4 pr = w.sortedPR[k];
+        float3 d = P.pos - make_float3(pr.x, pr.y, pr.z);
+        float r = P.radius + pr.w;
+        if (dot3(d, d) > r * r) continue;  // the sphere test, the same in both views
+        testFromProber(w, p, P, j);
+      }
+    }
+    if (dyn || p.anyDynamicLarge) {
+      for (uint32_t k = 0; k < p.nLarge; k++) {
+        uint32_t l = w.large[k];
+        if (!dyn && (!enabled(w, l) || w.size[l].w <= 0.0f)) continue;
+        testPair(w, p, P, l);
+      }
     }
     return;
   }
+  if (!dyn) return;
   Probe P = probeOf(w, i);
-  if (small) {
-    int4 c = w.cell[i];
-    for (int oz = -1; oz <= 1; oz++)
-      for (int oy = -1; oy <= 1; oy++)
-        for (int ox = -1; ox <= 1; ox++) {
-          int4 cc = make_int4(c.x + ox, c.y + oy, c.z + oz, 0);
-          uint32_t h = cellHash(cc, p.tableMask);
-          uint32_t end = w.cellEnd[h];
-          for (uint32_t k = w.cellStart[h]; k < end; k++) {
-            uint32_t j = sortedVals[k];
-            if (j == i || (j > i && w.size[j].w > 0.0f)) continue;
-            int4 cj = w.cell[j];
-            if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
-            testPair(w, p, P, j);
-          }
-        }
-  }
   for (uint32_t k = 0; k < p.nLarge; k++) {
     uint32_t l = w.large[k];
-    if (l == i || (!small && l < i && w.size[l].w > 0.0f)) continue;
+    if (l == i || (l < i && w.size[l].w > 0.0f)) continue;
     testPair(w, p, P, l);
   }
 }
@@ -665,7 +695,7 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
       uint32_t stick = 0;
       int j = -1;
       for (uint32_t c = prevFirst; c < prevFirst + prevCount; c++) {
-        if ((__float_as_uint(w.cRA[prev][c].w) & ~STICK_BIT) == found.feature[i]) {
+        if ((__float_as_uint(w.cPt[prev][4 * c + K_RA].w) & ~STICK_BIT) == found.feature[i]) {
           j = int(c);
           break;
         }
@@ -673,7 +703,7 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
       if (j < 0 && matchNearest) {
         float bestDist = NEAREST_FRACTION * minSide;
         for (uint32_t c = prevFirst; c < prevFirst + prevCount; c++) {
-          float3 d = f3(w.cRA[prev][c]) - rA;
+          float3 d = f3(w.cPt[prev][4 * c + K_RA]) - rA;
           float dist = sqrtf(dot3(d, d));
           if (dist <= bestDist) {
             bestDist = dist;
@@ -682,13 +712,14 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
         }
       }
       if (j >= 0) {
-        float4 pra = w.cRA[prev][j];
-        pen = f3(w.cPen[prev][j]);
-        lam = f3(w.cLam[prev][j]);
+        const float4* q = w.cPt[prev] + 4 * j;
+        float4 pra = q[K_RA];
+        pen = f3(q[K_PEN]);
+        lam = f3(q[K_LAM]);
         stick = __float_as_uint(pra.w) & STICK_BIT;
         if (stick != 0u && !anySphere) {
           rA = f3(pra);
-          rB = f3(w.cRB[prev][j]);
+          rB = f3(q[K_RB]);
         }
       }
       float3 d = (qrotate(qA, rA) + cA) - (qrotate(qB, rB) + cB);
@@ -698,43 +729,37 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
                         fminf(fmaxf(pen.z * p.gamma, PENALTY_MIN), PENALTY_MAX));
       pen.x = fmaxf(pen.x, penaltyMin);
       uint32_t slot = pi * MAX_CONTACTS + i;
-      w.cRA[cur][slot] = make_float4(rA.x, rA.y, rA.z, __uint_as_float(found.feature[i] | stick));
-      w.cRB[cur][slot] = make_float4(rB.x, rB.y, rB.z, c0x);
-      w.cPen[cur][slot] = make_float4(pen.x, pen.y, pen.z, c0y);
-      w.cLam[cur][slot] = make_float4(lam.x, lam.y, lam.z, c0z);
+      float4* o = w.cPt[cur] + 4 * slot;
+      o[K_RA] = make_float4(rA.x, rA.y, rA.z, __uint_as_float(found.feature[i] | stick));
+      o[K_RB] = make_float4(rB.x, rB.y, rB.z, c0x);
+      o[K_PEN] = make_float4(pen.x, pen.y, pen.z, c0y);
+      o[K_LAM] = make_float4(lam.x, lam.y, lam.z, c0z);
     }
   }
 }
 
-// Host: the collision phase, enqueued on `s`.
+// Host: the collision phase, enqueued on `s`. Returns the number of kernels it launched.
 uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s) {
   const uint32_t n = p.n;
   uint32_t launches = 3;  // begin, hash insert, narrowphase
   k_begin<<<1, 1, 0, s>>>(w, p);
   cudaMemsetAsync(w.hash, 0, (size_t(p.hashMask) + 1) * 4, s);
   k_hash_insert<<<GS_BLOCKS, 256, 0, s>>>(w, p);
-  cudaMemsetAsync(w.cellStart, 0, size_t(tableSize) * 4, s);
-  cudaMemsetAsync(w.cellEnd, 0, size_t(tableSize) * 4, s);
   if (n > 0) {
+    const uint32_t sentinel = p.tableMask + 1u;
+    cudaMemsetAsync(w.cellStart, 0, size_t(tableSize) * 4, s);
     k_cell_keys<<<grid_for(n, 256), 256, 0, s>>>(w, p);
-    // Keys <= tableSize (the sentinel): as many 8-bit passes as those bits need
-    int bits = 1;
-    while ((1u << bits) <= tableSize) bits++;
-    int passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
-    uint32_t tiles = grid_for(n, SORT_TILE);
-    uint32_t *kin = w.keyA, *vin = w.valA, *kout = w.keyB, *vout = w.valB;
-    for (int pass = 0; pass < passes; pass++) {
-      int shift = pass * RADIX_BITS;
-      k_radix_hist<<<tiles, SORT_THREADS, 0, s>>>(kin, n, shift, w.radixHist, tiles);
-      k_scan_single<<<1, 1024, 0, s>>>(w.radixHist, RADIX * tiles);
-      k_radix_scatter<<<tiles, SORT_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, w.radixHist, tiles);
-      launches += 3;
-      uint32_t* t = kin; kin = kout; kout = t;
-      t = vin; vin = vout; vout = t;
-    }
-    k_cell_ranges<<<grid_for(n, 256), 256, 0, s>>>(kin, n, w.cellStart, w.cellEnd, p.tableMask + 1u);
-    k_find_pairs<<<grid_for(n, 128), 128, 0, s>>>(w, p, vin);
-    launches += 3;  // cell keys, cell ranges, find pairs
+    k_bucket_count<<<grid_for(n, 256), 256, 0, s>>>(w.keyA, n, w.cellStart, w.valB, sentinel);
+    // cellEnd = counts before the scan turns them into starts
+    cudaMemcpyAsync(w.cellEnd, w.cellStart, size_t(tableSize) * 4, cudaMemcpyDeviceToDevice, s);
+    uint32_t tiles = grid_for(tableSize, SCAN_TILE);
+    k_scan_tiles<<<tiles, SCAN_THREADS, 0, s>>>(w.cellStart, tableSize, w.radixHist);
+    k_scan_single<<<1, 1024, 0, s>>>(w.radixHist, tiles);
+    k_scan_add<<<tiles, SCAN_THREADS, 0, s>>>(w.cellStart, tableSize, w.radixHist);
+    k_bucket_finish<<<grid_for(tableSize, 256), 256, 0, s>>>(w.cellStart, w.cellEnd, tableSize);
+    k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(w, n, sentinel);
+    k_find_pairs<<<grid_for(n, 128), 128, 0, s>>>(w, p);
+    launches += 8;
   }
   k_narrowphase<<<GS_BLOCKS, 128, 0, s>>>(w, p);
   return launches;

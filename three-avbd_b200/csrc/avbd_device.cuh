@@ -29,6 +29,10 @@ constexpr uint32_t FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_START_AT_RES
 constexpr float REST_SPEED = 0.1f;
 constexpr float NEAREST_FRACTION = 0.05f;
 constexpr uint32_t OWNER_BIT = 0x80000000u;  // incidence entry: this body updates the constraint's dual
+constexpr int LANE_CLASSES = 6;                // 1, 2, 4, 8, 16, 32 lanes per body
+constexpr int BUCKETS = MAX_COLORS * LANE_CLASSES;
+constexpr int BUCKET_WORDS = 5 * BUCKETS;  // counts | starts + total | fill cursors | lane bases | lane totals (64)
+enum : int { K_RA = 0, K_RB = 1, K_PEN = 2, K_LAM = 3 };
 
 // Counter words (device memory)
 enum : int {
@@ -37,6 +41,7 @@ enum : int {
   COUNTER_WORDS = 128,
 };
 constexpr int MAX_ROUND_PAIRS = 32;
+constexpr int MAX_CLOCKS = 1023;  // barrier timestamps kept per step
 // Error bits
 constexpr uint32_t ERR_BARRIER_TIMEOUT = 1, ERR_ADJ_OVERFLOW = 2, ERR_INC_OVERFLOW = 4;
 
@@ -72,20 +77,27 @@ struct DWorld {
   uint32_t *keyA, *keyB, *valA, *valB, *radixHist;
   int4* cell;
   uint32_t *cellStart, *cellEnd;
+  float4* sortedPR;  // per sorted slot: position, bounding radius
+  int4* sortedCell;  // per sorted slot: cell x, y, z, body index | dynamic << 31
   uint2* pairs;
   // contact pairs and points, double-buffered (cur: this step, 1 - cur: last step)
   uint4* mIds[2];   // a, b, first (= 8 * slot), count | step << 4
   float4* mGeo[2];  // normal (B to A), friction
-  float4 *cRA[2], *cRB[2], *cPen[2], *cLam[2];
+  float4* cPt[2];   // 4 float4 per point (layout.ts:124-127): rA + key, rB + C0.n, pen + C0.t1, lam + C0.t2
   uint32_t* hash;   // last step's pairs: slot + 1, open addressing
   // topology
-  uint32_t *adjStart, *adjFill, *adjList;
+  uint32_t *adjStart, *adjFill;
+  uint4* adjList;  // per (body, constraint): sort key hi, key lo, constraint | rows << 28, other | dynamic << 31
   uint32_t *colorA, *colorB, *colorHist, *colorStart, *colorBodies, *fixedColor;
-  uint32_t *incStart, *incList;
+  uint32_t *incCount, *incStart;
+  uint2* incList;         // per incidence: constraint row (joint slot, or nj + point slot) | OWNER_BIT, partner body
+  uint32_t* bucket;       // BUCKET_WORDS: counts, starts (+ total), fill cursors, lane bases, lane totals per colour
+  float4 *dlin, *dang;    // per body: position and rotation change since x- (kept by the solve)
   uint32_t* scanScratch;
   // bookkeeping
   uint32_t* counters;
   uint32_t* barrier;  // [0] arrive count, [1] generation
+  unsigned long long* clocks;  // device time (ns) at each grid barrier of the last step, [0] = count
 };
 
 // --- vector / quaternion helpers (operation order of the reference's WGSL, wgsl layout.ts:307-340) ---

@@ -131,10 +131,10 @@ int allocPairs(avbd_world* w, uint32_t cap) {
   const int prev = 1 - w->cur;
   uint4* oldIds = d.mIds[prev];
   float4* oldGeo = d.mGeo[prev];
-  float4 *oldRA = d.cRA[prev], *oldRB = d.cRB[prev], *oldPen = d.cPen[prev], *oldLam = d.cLam[prev];
+  float4* oldPt = d.cPt[prev];
   uint4* keepIds[2] = {d.mIds[0], d.mIds[1]};
   float4* keepGeo[2] = {d.mGeo[0], d.mGeo[1]};
-  float4* keepC[2][4] = {{d.cRA[0], d.cRB[0], d.cPen[0], d.cLam[0]}, {d.cRA[1], d.cRB[1], d.cPen[1], d.cLam[1]}};
+  float4* keepPt[2] = {d.cPt[0], d.cPt[1]};
   dfree(w, d.pairs);
   dfree(w, d.hash);
   dfree(w, d.adjList);
@@ -150,24 +150,18 @@ int allocPairs(avbd_world* w, uint32_t cap) {
   for (int b = 0; b < 2; b++) {
     CUDA_TRY(w, dalloc(w, &d.mIds[b], cap));
     CUDA_TRY(w, dalloc(w, &d.mGeo[b], cap));
-    CUDA_TRY(w, dalloc(w, &d.cRA[b], size_t(cap) * MAX_CONTACTS));
-    CUDA_TRY(w, dalloc(w, &d.cRB[b], size_t(cap) * MAX_CONTACTS));
-    CUDA_TRY(w, dalloc(w, &d.cPen[b], size_t(cap) * MAX_CONTACTS));
-    CUDA_TRY(w, dalloc(w, &d.cLam[b], size_t(cap) * MAX_CONTACTS));
+    CUDA_TRY(w, dalloc(w, &d.cPt[b], size_t(cap) * MAX_CONTACTS * 4));
   }
   if (oldIds) {
     size_t m = std::min(oldCap, cap);
     CUDA_TRY(w, cudaMemcpyAsync(d.mIds[prev], oldIds, m * sizeof(uint4), cudaMemcpyDeviceToDevice, w->stream));
     CUDA_TRY(w, cudaMemcpyAsync(d.mGeo[prev], oldGeo, m * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
-    CUDA_TRY(w, cudaMemcpyAsync(d.cRA[prev], oldRA, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
-    CUDA_TRY(w, cudaMemcpyAsync(d.cRB[prev], oldRB, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
-    CUDA_TRY(w, cudaMemcpyAsync(d.cPen[prev], oldPen, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
-    CUDA_TRY(w, cudaMemcpyAsync(d.cLam[prev], oldLam, m * MAX_CONTACTS * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    CUDA_TRY(w, cudaMemcpyAsync(d.cPt[prev], oldPt, m * MAX_CONTACTS * 4 * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
     CUDA_TRY(w, cudaStreamSynchronize(w->stream));
     for (int b = 0; b < 2; b++) {
       dfree(w, keepIds[b]);
       dfree(w, keepGeo[b]);
-      for (int k = 0; k < 4; k++) dfree(w, keepC[b][k]);
+      dfree(w, keepPt[b]);
     }
   }
   // the clears above run on the world's stream; host copies that follow use the default stream
@@ -377,7 +371,7 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   DWorld& d = w->d;
   const uint32_t B = w->bodyCap;
   w->tableSize = pow2AtLeast(2ull * B);
-  w->sortTiles = (B + 2047) / 2048;
+  w->sortTiles = (B + 8191) / 8192;
   w->solveBlocks = solve_grid_blocks(w->device);
   bool ok = true;
   auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
@@ -387,8 +381,10 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.keyB, B));
   A(dalloc(w, &d.valA, B));
   A(dalloc(w, &d.valB, B));
-  A(dalloc(w, &d.radixHist, size_t(256) * w->sortTiles));
+  A(dalloc(w, &d.radixHist, size_t(w->tableSize) / 4096 + 2));
   A(dalloc(w, &d.cell, B));
+  A(dalloc(w, &d.sortedPR, B));
+  A(dalloc(w, &d.sortedCell, B));
   A(dalloc(w, &d.cellStart, w->tableSize));
   A(dalloc(w, &d.cellEnd, w->tableSize));
   A(dalloc(w, &d.adjStart, B + 1));
@@ -400,9 +396,14 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.colorBodies, B));
   A(dalloc(w, &d.fixedColor, B));
   A(dalloc(w, &d.incStart, B + 1));
+  A(dalloc(w, &d.incCount, B));
+  A(dalloc(w, &d.bucket, BUCKET_WORDS));
+  A(dalloc(w, &d.dlin, B));
+  A(dalloc(w, &d.dang, B));
   A(dalloc(w, &d.scanScratch, w->solveBlocks + 1));
   A(dalloc(w, &d.counters, COUNTER_WORDS));
   A(dalloc(w, &d.barrier, 2));
+  A(dalloc(w, &d.clocks, MAX_CLOCKS + 1));
   if (!ok) return bad(AVBD_ERR_CUDA);
   // every body in every group, colliding with every group; colours start unset
   A(cudaMemsetAsync(d.filters, 0xff, size_t(B) * sizeof(uint2), w->stream));
@@ -616,30 +617,18 @@ int avbd_seed_contacts(avbd_world* w, const avbd_manifold* m, uint32_t nm, const
   const int prev = 1 - w->cur;
   std::vector<uint4> ids(nm);
   std::vector<float4> geo(nm);
-  std::vector<float4> ra(size_t(nm) * MAX_CONTACTS), rb(ra.size()), pen(ra.size()), lam(ra.size());
+  std::vector<avbd_contact> pts(size_t(nm) * MAX_CONTACTS);
+  std::memset(pts.data(), 0, pts.size() * sizeof(avbd_contact));
   for (uint32_t i = 0; i < nm; i++) {
     ids[i] = make_uint4(m[i].a, m[i].b, i * MAX_CONTACTS, m[i].count);
     geo[i] = make_float4(m[i].normal[0], m[i].normal[1], m[i].normal[2], m[i].friction);
-    for (uint32_t k = 0; k < m[i].count; k++) {
-      const avbd_contact& s = c[m[i].first + k];
-      size_t o = size_t(i) * MAX_CONTACTS + k;
-      uint32_t key = s.key;
-      float keyf;
-      std::memcpy(&keyf, &key, 4);
-      ra[o] = make_float4(s.r_a[0], s.r_a[1], s.r_a[2], keyf);
-      rb[o] = make_float4(s.r_b[0], s.r_b[1], s.r_b[2], s.c0_n);
-      pen[o] = make_float4(s.pen[0], s.pen[1], s.pen[2], s.c0_t1);
-      lam[o] = make_float4(s.lam[0], s.lam[1], s.lam[2], s.c0_t2);
-    }
+    for (uint32_t k = 0; k < m[i].count; k++) pts[size_t(i) * MAX_CONTACTS + k] = c[m[i].first + k];
   }
   DWorld& d = w->d;
   if (nm) {
     CUDA_TRY(w, cudaMemcpy(d.mIds[prev], ids.data(), nm * sizeof(uint4), cudaMemcpyHostToDevice));
     CUDA_TRY(w, cudaMemcpy(d.mGeo[prev], geo.data(), nm * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(d.cRA[prev], ra.data(), ra.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(d.cRB[prev], rb.data(), rb.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(d.cPen[prev], pen.data(), pen.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(d.cLam[prev], lam.data(), lam.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(d.cPt[prev], pts.data(), pts.size() * sizeof(avbd_contact), cudaMemcpyHostToDevice));
   }
   uint32_t pairs = nm;
   CUDA_TRY(w, cudaMemcpy(d.counters + C_PAIRS, &pairs, 4, cudaMemcpyHostToDevice));
@@ -777,17 +766,10 @@ int avbd_read_contacts(avbd_world* w, avbd_manifold* mout, uint32_t mcap, uint32
     CUDA_TRY(w, cudaMemcpy(ids.data(), w->d.mIds[last], pairs * sizeof(uint4), cudaMemcpyDeviceToHost));
     CUDA_TRY(w, cudaMemcpy(geo.data(), w->d.mGeo[last], pairs * sizeof(float4), cudaMemcpyDeviceToHost));
   }
-  std::vector<float4> ra, rb, pen, lam;
+  std::vector<avbd_contact> pts;
   if (pairs) {
-    size_t k = size_t(pairs) * MAX_CONTACTS;
-    ra.resize(k);
-    rb.resize(k);
-    pen.resize(k);
-    lam.resize(k);
-    CUDA_TRY(w, cudaMemcpy(ra.data(), w->d.cRA[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(w, cudaMemcpy(rb.data(), w->d.cRB[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(w, cudaMemcpy(pen.data(), w->d.cPen[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(w, cudaMemcpy(lam.data(), w->d.cLam[last], k * sizeof(float4), cudaMemcpyDeviceToHost));
+    pts.resize(size_t(pairs) * MAX_CONTACTS);
+    CUDA_TRY(w, cudaMemcpy(pts.data(), w->d.cPt[last], pts.size() * sizeof(avbd_contact), cudaMemcpyDeviceToHost));
   }
   uint32_t mi = 0, ci = 0;
   for (uint32_t p = 0; p < pairs; p++) {
@@ -805,15 +787,7 @@ int avbd_read_contacts(avbd_world* w, avbd_manifold* mout, uint32_t mcap, uint32
       m.friction = geo[p].w;
     }
     for (uint32_t k = 0; k < count; k++) {
-      if (cout && ci + k < ccap) {
-        size_t o = size_t(p) * MAX_CONTACTS + k;
-        avbd_contact& c = cout[ci + k];
-        c.r_a[0] = ra[o].x; c.r_a[1] = ra[o].y; c.r_a[2] = ra[o].z;
-        std::memcpy(&c.key, &ra[o].w, 4);
-        c.r_b[0] = rb[o].x; c.r_b[1] = rb[o].y; c.r_b[2] = rb[o].z; c.c0_n = rb[o].w;
-        c.pen[0] = pen[o].x; c.pen[1] = pen[o].y; c.pen[2] = pen[o].z; c.c0_t1 = pen[o].w;
-        c.lam[0] = lam[o].x; c.lam[1] = lam[o].y; c.lam[2] = lam[o].z; c.c0_t2 = lam[o].w;
-      }
+      if (cout && ci + k < ccap) cout[ci + k] = pts[size_t(p) * MAX_CONTACTS + k];
     }
     mi++;
     ci += count;
@@ -894,6 +868,18 @@ int avbd_read_step_stats(avbd_world* w, avbd_step_stats* dst, uint32_t cap, uint
     s.launches = w->statsLaunches[slot];
     s.error = q[C_ERROR];
   }
+  return AVBD_OK;
+}
+
+int avbd_read_phase_clocks(avbd_world* w, double* dst, uint32_t cap, uint32_t* n) {
+  if (!w) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  std::vector<unsigned long long> ck(MAX_CLOCKS + 1);
+  CUDA_TRY(w, cudaMemcpy(ck.data(), w->d.clocks, ck.size() * 8, cudaMemcpyDeviceToHost));
+  uint32_t k = uint32_t(std::min<unsigned long long>(ck[0], MAX_CLOCKS));
+  if (n) *n = k;
+  for (uint32_t i = 0; i < k && i < cap && dst; i++) dst[i] = double(ck[1 + i] - ck[1]) * 1e-6;
   return AVBD_OK;
 }
 

@@ -26,32 +26,58 @@ constexpr long long BARRIER_CYCLES = 4000000000LL;  // about two seconds of SM c
 
 __device__ __forceinline__ uint32_t ldv(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 
-// Grid barrier (arrive counter + generation), bounded wait. Returns false when the step must stop.
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t atom_add_release_gpu(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier: a monotonic arrival counter (zeroed before the launch); the k-th barrier completes
+// when it reaches k x gridDim.x. Arrival is a release, the wait an acquire (PTX memory model), so
+// every block's writes before the barrier are visible to every block after it. The wait is bounded:
+// past the clock budget the block sets an error bit and returns false, and every other block
+// leaves at its next wait. The last block to arrive stamps the device time for the phase profile.
+__device__ unsigned long long* g_clocks;
+__shared__ uint32_t s_epoch;
 __device__ bool grid_sync(uint32_t* bar, uint32_t* counters) {
   __shared__ uint32_t s_abort;
   __syncthreads();
   if (threadIdx.x == 0) {
-    uint32_t gen = ldv(bar + 1);
+    uint32_t target = (++s_epoch) * gridDim.x;
     uint32_t ab = 0;
-    __threadfence();
-    uint32_t arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
+    uint32_t old = atom_add_release_gpu(bar, 1u);
+    if (old + 1u == target) {
+      unsigned long long* ck = g_clocks;
+      if (ck) {
+        unsigned long long k = ck[0];
+        if (k < (unsigned long long)MAX_CLOCKS) {
+          ck[1 + k] = globaltimer();
+          ck[0] = k + 1;
+        }
+      }
     } else {
       long long t0 = clock64();
-      while (ldv(bar + 1) == gen) {
+      while (ld_acquire_gpu(bar) < target) {
         if (ldv(&counters[C_ERROR]) & ERR_BARRIER_TIMEOUT) { ab = 1; break; }
         if (clock64() - t0 > BARRIER_CYCLES) {
           atomicOr(&counters[C_ERROR], ERR_BARRIER_TIMEOUT);
           ab = 1;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
-    __threadfence();
     s_abort = ab;
   }
   __syncthreads();
@@ -135,15 +161,18 @@ __device__ inline bool endpoints(const DWorld& w, const StepParams& p, uint32_t 
   return true;
 }
 
-// Summation order of a body's constraints (wgsl-topology.ts:116-125): joints by slot, then contact
-// pairs by (other body + 2, first point's feature key).
-__device__ inline unsigned long long adjKey(const DWorld& w, const StepParams& p, uint32_t b, uint32_t c) {
-  if (c < p.nj) return (unsigned long long)c;
+// An adjacency entry of body b for constraint c: its summation-order key (wgsl-topology.ts:116-125:
+// joints by slot, then contact pairs by (other body + 2, first point's feature key)), the constraint
+// with its row count, and the other body with its dynamic bit.
+__device__ inline uint4 adjEntry(const DWorld& w, const StepParams& p, uint32_t b, uint32_t c, int ea, int eb, uint32_t rows) {
+  int other = ea == (int)b ? eb : ea;
+  uint32_t o = other < 0 ? 0x7fffffffu : ((uint32_t)other | (dynBody(w, other) ? 0x80000000u : 0u));
+  if (c < p.nj) return make_uint4(0u, c, c | (rows << 28), o);
   uint4 ids = w.mIds[p.cur][c - p.nj];
-  uint32_t other = ids.x == b ? ids.y : ids.x;
-  uint32_t feature = __float_as_uint(w.cRA[p.cur][ids.z].w) & ~STICK_BIT;
-  return ((unsigned long long)(other + 2u) << 32) | feature;
+  uint32_t feature = __float_as_uint(w.cPt[p.cur][4 * ids.z + K_RA].w) & ~STICK_BIT;
+  return make_uint4((uint32_t)other + 2u, feature, c | (rows << 28), o);
 }
+__device__ inline bool entryLess(uint4 a, uint4 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); }
 
 // --- Jones-Plassmann (wgsl-topology.ts:157-262) ---------------------------------------------------------
 __device__ inline uint32_t priority(uint32_t i) { return hash32(i + 0x9e3779b9u); }
@@ -151,22 +180,10 @@ __device__ inline bool beats(uint32_t i, uint32_t j) {
   uint32_t pi = priority(i), pj = priority(j);
   return pi > pj || (pi == pj && i > j);
 }
-__device__ inline int neighbour(const DWorld& w, const StepParams& p, uint32_t b, uint32_t e) {
-  uint32_t c = w.adjList[e];
-  int ea, eb;
-  uint32_t cnt;
-  if (c < p.nj) {
-    int4 in = w.jinfo[c];
-    ea = in.y;
-    eb = in.z;
-  } else {
-    uint4 ids = w.mIds[p.cur][c - p.nj];
-    ea = (int)ids.x;
-    eb = (int)ids.y;
-  }
-  (void)cnt;
-  int other = ea == (int)b ? eb : ea;
-  return dynBody(w, other) ? other : -1;
+// A constraint's other body for the colouring: -1 unless it is dynamic (adjacency entry word w)
+__device__ inline int neighbour(const DWorld& w, const StepParams&, uint32_t, uint32_t e) {
+  uint32_t o = w.adjList[e].w;
+  return (o & 0x80000000u) ? int(o & 0x7fffffffu) : -1;
 }
 __device__ inline uint32_t smallestFree(const DWorld& w, const StepParams& p, uint32_t b, const uint32_t* src, bool skipPending) {
   uint32_t lo = 0, hi = 0;
@@ -185,63 +202,22 @@ __device__ inline uint32_t smallestFree(const DWorld& w, const StepParams& p, ui
   return MAX_COLORS;
 }
 
-// --- stable bucket scatter of one block's chunk (64 colours) ---------------------------------------------
-// Bodies of [lo, hi) go to colorBodies in index order within each colour, at the block's scanned
-// per-colour offsets colorHist[c * gridDim.x + blockIdx.x].
-__device__ void color_scatter_chunk(const DWorld& w, uint32_t lo, uint32_t hi) {
-  __shared__ uint32_t running[MAX_COLORS];
-  __shared__ uint32_t warpCount[SOLVE_THREADS / 32][MAX_COLORS];
-  __shared__ uint32_t tileCount[MAX_COLORS];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x < MAX_COLORS) running[threadIdx.x] = w.colorHist[threadIdx.x * gridDim.x + blockIdx.x];
-  for (uint32_t base = lo; base < hi; base += SOLVE_THREADS) {
-    for (int k = threadIdx.x; k < (SOLVE_THREADS / 32) * MAX_COLORS; k += SOLVE_THREADS) (&warpCount[0][0])[k] = 0;
-    __syncthreads();
-    uint32_t b = base + threadIdx.x;
-    bool live = b < hi && (w.colorB[b] != 0xffffffffu);
-    uint32_t col = live ? (w.colorA[b] & 0xffu) : 0xffffffffu;
-    uint32_t peers = __match_any_sync(0xffffffffu, col);
-    uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-    if (live && rank == 0) warpCount[warp][col] = __popc(peers);
-    __syncthreads();
-    if (threadIdx.x < MAX_COLORS) {
-      uint32_t s = 0;
-      for (int k = 0; k < SOLVE_THREADS / 32; k++) {
-        uint32_t c = warpCount[k][threadIdx.x];
-        warpCount[k][threadIdx.x] = s;
-        s += c;
-      }
-      tileCount[threadIdx.x] = s;
-    }
-    __syncthreads();
-    if (live) w.colorBodies[running[col] + warpCount[warp][col] + rank] = b;
-    __syncthreads();
-    if (threadIdx.x < MAX_COLORS) running[threadIdx.x] += tileCount[threadIdx.x];
-    __syncthreads();
-  }
-}
-
 // --- body poses -----------------------------------------------------------------------------------------
+// What a contact row needs of a body: its rotation (and step-start rotation, for rolling spheres) and
+// its displacement since x- (dlin, dang are kept by the solve, so a partner costs three loads and no
+// quaternion division).
 struct Pose {
-  float3 x, x0, dLin, dAng;
+  float3 x, dLin, dAng;
   float4 q, q0;
 };
-__device__ inline Pose loadPose(const DWorld& w, uint32_t i) {
+__device__ inline Pose partnerPose(const DWorld& w, uint32_t i) {
   Pose P;
-  float4 p = w.pos[i], q = w.rot[i], p0 = w.ipos[i], q0 = w.irot[i];
-  P.x = f3(p);
-  P.q = q;
-  P.x0 = f3(p0);
-  P.q0 = q0;
-  P.dLin = P.x - P.x0;
-  P.dAng = qsub(q, q0);
+  P.q = w.rot[i];
+  P.dLin = f3(w.dlin[i]);
+  P.dAng = f3(w.dang[i]);
+  P.x = make_float3(0.0f, 0.0f, 0.0f);
+  P.q0 = P.q;
   return P;
-}
-__device__ inline void setPose(Pose& P, float3 x, float4 q) {
-  P.x = x;
-  P.q = q;
-  P.dLin = x - P.x0;
-  P.dAng = qsub(q, P.q0);
 }
 
 // The Newton system of one body (wgsl-solve.ts:56-75): lin and ang symmetric (upper triangles),
@@ -445,99 +421,125 @@ __device__ inline void finishBody(const Acc& acc, float3& x, float4& q) {
   float A41 = v[12], A42 = v[13], A43 = v[14], A44 = v[6];
   float A51 = v[15], A52 = v[16], A53 = v[17], A54 = v[7], A55 = v[9];
   float A61 = v[18], A62 = v[19], A63 = v[20], A64 = v[8], A65 = v[10], A66 = v[11];
-  float D1 = A11;
-  float L21 = A21 / D1, L31 = A31 / D1, L41 = A41 / D1, L51 = A51 / D1, L61 = A61 / D1;
-  float D2 = fmaxf(A22 - L21 * L21 * D1, A22 * PIVOT_FLOOR);
-  float L32 = (A32 - L21 * L31 * D1) / D2;
-  float L42 = (A42 - L21 * L41 * D1) / D2;
-  float L52 = (A52 - L21 * L51 * D1) / D2;
-  float L62 = (A62 - L21 * L61 * D1) / D2;
-  float D3 = fmaxf(A33 - (L31 * L31 * D1 + L32 * L32 * D2), A33 * PIVOT_FLOOR);
-  float L43 = (A43 - L31 * L41 * D1 - L32 * L42 * D2) / D3;
-  float L53 = (A53 - L31 * L51 * D1 - L32 * L52 * D2) / D3;
-  float L63 = (A63 - L31 * L61 * D1 - L32 * L62 * D2) / D3;
-  float D4 = fmaxf(A44 - (L41 * L41 * D1 + L42 * L42 * D2 + L43 * L43 * D3), A44 * PIVOT_FLOOR);
-  float L54 = (A54 - L41 * L51 * D1 - L42 * L52 * D2 - L43 * L53 * D3) / D4;
-  float L64 = (A64 - L41 * L61 * D1 - L42 * L62 * D2 - L43 * L63 * D3) / D4;
-  float D5 = fmaxf(A55 - (L51 * L51 * D1 + L52 * L52 * D2 + L53 * L53 * D3 + L54 * L54 * D4), A55 * PIVOT_FLOOR);
-  float L65 = (A65 - L51 * L61 * D1 - L52 * L62 * D2 - L53 * L63 * D3 - L54 * L64 * D4) / D5;
-  float D6 = fmaxf(A66 - (L61 * L61 * D1 + L62 * L62 * D2 + L63 * L63 * D3 + L64 * L64 * D4 + L65 * L65 * D5), A66 * PIVOT_FLOOR);
+  // Each pivot is inverted once and multiplied (the reference divides; the results agree to rounding)
+  float D1 = A11, i1 = 1.0f / D1;
+  float L21 = A21 * i1, L31 = A31 * i1, L41 = A41 * i1, L51 = A51 * i1, L61 = A61 * i1;
+  float D2 = fmaxf(A22 - L21 * L21 * D1, A22 * PIVOT_FLOOR), i2 = 1.0f / D2;
+  float L32 = (A32 - L21 * L31 * D1) * i2;
+  float L42 = (A42 - L21 * L41 * D1) * i2;
+  float L52 = (A52 - L21 * L51 * D1) * i2;
+  float L62 = (A62 - L21 * L61 * D1) * i2;
+  float D3 = fmaxf(A33 - (L31 * L31 * D1 + L32 * L32 * D2), A33 * PIVOT_FLOOR), i3 = 1.0f / D3;
+  float L43 = (A43 - L31 * L41 * D1 - L32 * L42 * D2) * i3;
+  float L53 = (A53 - L31 * L51 * D1 - L32 * L52 * D2) * i3;
+  float L63 = (A63 - L31 * L61 * D1 - L32 * L62 * D2) * i3;
+  float D4 = fmaxf(A44 - (L41 * L41 * D1 + L42 * L42 * D2 + L43 * L43 * D3), A44 * PIVOT_FLOOR), i4 = 1.0f / D4;
+  float L54 = (A54 - L41 * L51 * D1 - L42 * L52 * D2 - L43 * L53 * D3) * i4;
+  float L64 = (A64 - L41 * L61 * D1 - L42 * L62 * D2 - L43 * L63 * D3) * i4;
+  float D5 = fmaxf(A55 - (L51 * L51 * D1 + L52 * L52 * D2 + L53 * L53 * D3 + L54 * L54 * D4), A55 * PIVOT_FLOOR), i5 = 1.0f / D5;
+  float L65 = (A65 - L51 * L61 * D1 - L52 * L62 * D2 - L53 * L63 * D3 - L54 * L64 * D4) * i5;
+  float D6 = fmaxf(A66 - (L61 * L61 * D1 + L62 * L62 * D2 + L63 * L63 * D3 + L64 * L64 * D4 + L65 * L65 * D5), A66 * PIVOT_FLOOR), i6 = 1.0f / D6;
   float y1 = v[21];
   float y2 = v[22] - L21 * y1;
   float y3 = v[23] - L31 * y1 - L32 * y2;
   float y4 = v[24] - L41 * y1 - L42 * y2 - L43 * y3;
   float y5 = v[25] - L51 * y1 - L52 * y2 - L53 * y3 - L54 * y4;
   float y6 = v[26] - L61 * y1 - L62 * y2 - L63 * y3 - L64 * y4 - L65 * y5;
-  float w3 = y6 / D6;
-  float w2 = y5 / D5 - L65 * w3;
-  float w1 = y4 / D4 - L54 * w2 - L64 * w3;
-  float v3 = y3 / D3 - L43 * w1 - L53 * w2 - L63 * w3;
-  float v2 = y2 / D2 - L32 * v3 - L42 * w1 - L52 * w2 - L62 * w3;
-  float v1 = y1 / D1 - L21 * v2 - L31 * v3 - L41 * w1 - L51 * w2 - L61 * w3;
+  float w3 = y6 * i6;
+  float w2 = y5 * i5 - L65 * w3;
+  float w1 = y4 * i4 - L54 * w2 - L64 * w3;
+  float v3 = y3 * i3 - L43 * w1 - L53 * w2 - L63 * w3;
+  float v2 = y2 * i2 - L32 * v3 - L42 * w1 - L52 * w2 - L62 * w3;
+  float v1 = y1 * i1 - L21 * v2 - L31 * v3 - L41 * w1 - L51 * w2 - L61 * w3;
   x = make_float3(x.x - v1, x.y - v2, x.z - v3);
   q = qadd(q, make_float3(-w1, -w2, -w3));
 }
 
-// One lane's share of one incidence: a joint, or a contact point of a pair.
-__device__ inline void accumulateIncidence(Acc& acc, const DWorld& w, const StepParams& p, uint32_t id, uint32_t i, const Pose& own) {
+// One contact row set (a point of a pair) from body i's side
+struct PointView {
+  float4 ra, rb, pen, lam;
+  float3 n, t1, t2;
+  float friction;
+  bool isA;
+  Pose other;
+};
+__device__ inline void loadPoint(const DWorld& w, const StepParams& p, uint32_t cs, uint32_t i, uint32_t partner, PointView& v) {
+  const float4* pt = w.cPt[p.cur] + 4 * cs;
+  v.ra = pt[K_RA];
+  v.rb = pt[K_RB];
+  v.pen = pt[K_PEN];
+  v.lam = pt[K_LAM];
+  float4 geo = w.mGeo[p.cur][cs / MAX_CONTACTS];
+  v.n = f3(geo);
+  v.friction = geo.w;
+  orthonormal(v.n, v.t1, v.t2);
+  v.isA = i > partner;  // a pair's A is its higher index
+  v.other = partnerPose(w, partner);
+  if ((__float_as_uint(v.ra.w) & ~STICK_BIT) == SPHERE_FEATURE) v.other.q0 = w.irot[partner];
+}
+
+__device__ inline void accumulateIncidence(Acc& acc, const DWorld& w, const StepParams& p, uint2 inc, uint32_t i, const Pose& own) {
+  uint32_t id = inc.x & ~OWNER_BIT;
   if (id < p.nj) {
     Bodies2 B{&w, i, &own};
     addJoint(acc, w, id, p.alpha, i, B);
     return;
   }
-  uint32_t cs = id - p.nj;
-  uint32_t m = cs / MAX_CONTACTS;
-  uint4 ids = w.mIds[p.cur][m];
-  float4 geo = w.mGeo[p.cur][m];
-  bool isA = ids.x == i;
-  Pose other = loadPose(w, isA ? ids.y : ids.x);
-  const Pose& A = isA ? own : other;
-  const Pose& B = isA ? other : own;
-  float3 n = f3(geo), t1, t2;
-  orthonormal(n, t1, t2);
+  PointView v;
+  loadPoint(w, p, id - p.nj, i, inc.y, v);
+  const Pose& A = v.isA ? own : v.other;
+  const Pose& B = v.isA ? v.other : own;
   ContactEval e;
-  evalContact(w.cRA[p.cur][cs], w.cRB[p.cur][cs], w.cPen[p.cur][cs], w.cLam[p.cur][cs], n, t1, t2, geo.w, A, B, p.alpha, e);
-  float4 pen = w.cPen[p.cur][cs];
-  float sg = isA ? 1.0f : -1.0f;
-  float3 r = isA ? e.rAW : e.rBW;
-  float3 l0 = n * sg, l1 = t1 * sg, l2 = t2 * sg;
-  addRow(acc, l0, cross3(r, l0), pen.x, e.F.x);
-  addRow(acc, l1, cross3(r, l1), pen.y, e.F.y);
-  addRow(acc, l2, cross3(r, l2), pen.z, e.F.z);
+  evalContact(v.ra, v.rb, v.pen, v.lam, v.n, v.t1, v.t2, v.friction, A, B, p.alpha, e);
+  float sg = v.isA ? 1.0f : -1.0f;
+  float3 r = v.isA ? e.rAW : e.rBW;
+  float3 l0 = v.n * sg, l1 = v.t1 * sg, l2 = v.t2 * sg;
+  addRow(acc, l0, cross3(r, l0), v.pen.x, e.F.x);
+  addRow(acc, l1, cross3(r, l1), v.pen.y, e.F.y);
+  addRow(acc, l2, cross3(r, l2), v.pen.z, e.F.z);
 }
 
 // The dual update of one owned incidence (wgsl-solve.ts:562-662)
-__device__ inline void dualIncidence(const DWorld& w, const StepParams& p, uint32_t id, uint32_t i, const Pose& own) {
+__device__ inline void dualIncidence(const DWorld& w, const StepParams& p, uint2 inc, uint32_t i, const Pose& own) {
+  uint32_t id = inc.x & ~OWNER_BIT;
   if (id < p.nj) {
     Bodies2 B{&w, i, &own};
     dualJoint(w, p, id, B);
     return;
   }
   uint32_t cs = id - p.nj;
-  uint32_t m = cs / MAX_CONTACTS;
-  uint4 ids = w.mIds[p.cur][m];
-  float4 geo = w.mGeo[p.cur][m];
-  bool isA = ids.x == i;
-  Pose other = loadPose(w, isA ? ids.y : ids.x);
-  const Pose& A = isA ? own : other;
-  const Pose& B = isA ? other : own;
-  float3 n = f3(geo), t1, t2;
-  orthonormal(n, t1, t2);
-  float4 ra = w.cRA[p.cur][cs], pen = w.cPen[p.cur][cs], lam = w.cLam[p.cur][cs];
+  PointView v;
+  loadPoint(w, p, cs, i, inc.y, v);
+  const Pose& A = v.isA ? own : v.other;
+  const Pose& B = v.isA ? v.other : own;
   ContactEval e;
-  evalContact(ra, w.cRB[p.cur][cs], pen, lam, n, t1, t2, geo.w, A, B, p.alpha, e);
-  w.cLam[p.cur][cs] = make_float4(e.F.x, e.F.y, e.F.z, lam.w);
+  evalContact(v.ra, v.rb, v.pen, v.lam, v.n, v.t1, v.t2, v.friction, A, B, p.alpha, e);
+  float4* pt = w.cPt[p.cur] + 4 * cs;
+  pt[K_LAM] = make_float4(e.F.x, e.F.y, e.F.z, v.lam.w);
+  float4 pen = v.pen;
   if (e.F.x < 0.0f) pen.x = fminf(pen.x + p.betaLin * fabsf(e.C.x), PENALTY_MAX);
   if (e.frictionScale <= e.bounds) {
     pen.y = fminf(pen.y + p.betaLin * fabsf(e.C.y), PENALTY_MAX);
     pen.z = fminf(pen.z + p.betaLin * fabsf(e.C.z), PENALTY_MAX);
     bool stick = sqrtf(e.C.y * e.C.y + e.C.z * e.C.z) < STICK_THRESH;
-    uint32_t key = __float_as_uint(ra.w);
+    uint32_t key = __float_as_uint(v.ra.w);
     uint32_t nk = (key & ~STICK_BIT) | (stick ? STICK_BIT : 0u);
-    if (nk != key) w.cRA[p.cur][cs].w = __uint_as_float(nk);
+    if (nk != key) pt[K_RA].w = __uint_as_float(nk);
   }
-  w.cPen[p.cur][cs] = pen;
+  pt[K_PEN] = pen;
 }
+
+// Lanes per body: about two rows a lane, a power of two up to a warp
+__device__ inline uint32_t laneClass(uint32_t rows) {
+  uint32_t want = (rows + 1u) >> 1;
+  uint32_t k = 0;
+  while (k < 5u && (1u << k) < want) k++;
+  return k;
+}
+
+// Bucket bookkeeping in w.bucket: counts | starts (+ total) | fill cursors | lane bases | lane totals
+constexpr int B_COUNT = 0, B_START = BUCKETS, B_FILL = 2 * BUCKETS + 1, B_LANE = 3 * BUCKETS + 1, B_LANE_TOTAL = 4 * BUCKETS + 1;
+static_assert(B_LANE_TOTAL + MAX_COLORS <= BUCKET_WORDS, "bucket words");
 
 // --- the kernel -----------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, StepParams p) {
@@ -548,6 +550,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
   uint32_t* bar = w.barrier;
 #define GSYNC \
   if (!grid_sync(bar, ctr)) return;
+  if (threadIdx.x == 0) s_epoch = 0;
+  if (tid == 0) {
+    g_clocks = w.clocks;
+    w.clocks[0] = 1;
+    w.clocks[1] = globaltimer();
+  }
   uint32_t npairs = ldv(&ctr[C_PAIRS]);
   if (npairs > p.pairCap) npairs = p.pairCap;
   const uint32_t ncons = nj + npairs;
@@ -563,29 +571,33 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
   GSYNC
   if (!grid_scan(w.adjStart, n + 1, w.scanScratch, bar, ctr)) return;
   if (tid == 0) ctr[C_ADJ] = w.adjStart[n];
-  // B. fill (adjFill zeroed by the host), then each body's list sorted into its summation order
+  // B. fill (adjFill zeroed by the host), then each body's list sorted into its summation order and
+  // its row count (a joint is one row, a pair one per point)
   for (uint32_t c = tid; c < ncons; c += T) {
     int ea, eb;
     uint32_t cnt;
     if (!endpoints(w, p, c, ea, eb, cnt)) continue;
-    if (dynBody(w, ea)) w.adjList[w.adjStart[ea] + atomicAdd(&w.adjFill[ea], 1u)] = c;
-    if (dynBody(w, eb)) w.adjList[w.adjStart[eb] + atomicAdd(&w.adjFill[eb], 1u)] = c;
+    if (dynBody(w, ea)) w.adjList[w.adjStart[ea] + atomicAdd(&w.adjFill[ea], 1u)] = adjEntry(w, p, (uint32_t)ea, c, ea, eb, cnt);
+    if (dynBody(w, eb)) w.adjList[w.adjStart[eb] + atomicAdd(&w.adjFill[eb], 1u)] = adjEntry(w, p, (uint32_t)eb, c, ea, eb, cnt);
   }
   GSYNC
   for (uint32_t b = tid; b < n; b += T) {
     uint32_t lo = w.adjStart[b], hi = w.adjStart[b + 1];
-    for (uint32_t i = lo + 1; i < hi; i++) {
-      uint32_t id = w.adjList[i];
-      unsigned long long key = adjKey(w, p, b, id);
+    uint32_t rows = 0;
+    for (uint32_t i = lo; i < hi; i++) {
+      uint4 ent = w.adjList[i];
+      rows += ent.z >> 28;
+      if (i == lo) continue;
       uint32_t j = i;
       while (j > lo) {
-        uint32_t prevId = w.adjList[j - 1];
-        if (!(key < adjKey(w, p, b, prevId))) break;
-        w.adjList[j] = prevId;
+        uint4 prev = w.adjList[j - 1];
+        if (!entryLess(ent, prev)) break;
+        w.adjList[j] = prev;
         j--;
       }
-      w.adjList[j] = id;
+      w.adjList[j] = ent;
     }
+    w.incCount[b] = rows;
   }
   GSYNC
 
@@ -665,67 +677,84 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
     if (tid == 0) ctr[C_ROUNDS] = 2u * r;
   }
 
-  // D. final colours (NO_COLOR -> cap - 1, pending kept and counted) and per-block histograms over
-  // contiguous chunks; colorB marks non-dynamic bodies (0xffffffff) for the scatter
-  const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
-  const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
+  // D. final colours (NO_COLOR -> cap - 1, pending kept and counted), and bodies counted into
+  // (colour, lane class) buckets, widest lane class first within a colour. The order of bodies in a
+  // bucket does not change any result (a colour's bodies share no row), so the scatter uses atomics.
+  __shared__ uint32_t s_hist[BUCKETS], s_base[BUCKETS];
   {
-    __shared__ uint32_t hist[MAX_COLORS];
-    if (threadIdx.x < MAX_COLORS) hist[threadIdx.x] = 0;
+    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
     __syncthreads();
     uint32_t clashes = 0, maxc = 0;
-    for (uint32_t b = lo + threadIdx.x; b < hi; b += SOLVE_THREADS) {
-      if (!dynBody(w, (int)b)) {
-        w.colorB[b] = 0xffffffffu;
-        continue;
-      }
+    for (uint32_t b = tid; b < n; b += T) {
+      if (!dynBody(w, (int)b)) continue;
       uint32_t s = w.colorA[b];
       uint32_t col = s & 0xffu;
       if (s & PENDING) clashes++;
       if (col == NO_COLOR || col >= (uint32_t)MAX_COLORS) col = cap - 1u;
       w.colorA[b] = col | (s & PENDING);
-      w.colorB[b] = 0;
-      atomicAdd(&hist[col], 1u);
       maxc = max(maxc, col + 1u);
+      atomicAdd(&s_hist[col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b]))], 1u);
     }
     if (clashes) atomicAdd(&ctr[C_CLASHES], clashes);
     if (maxc) atomicMax(&ctr[C_COLORS], maxc);
     __syncthreads();
-    if (threadIdx.x < MAX_COLORS) w.colorHist[threadIdx.x * gridDim.x + blockIdx.x] = hist[threadIdx.x];
+    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS)
+      if (s_hist[k]) atomicAdd(&w.bucket[B_COUNT + k], s_hist[k]);
   }
   GSYNC
   if (blockIdx.x == 0) {
-    uint32_t total = block_scan_range(w.colorHist, 0, MAX_COLORS * gridDim.x);
+    if (threadIdx.x < BUCKETS) w.bucket[B_START + threadIdx.x] = w.bucket[B_COUNT + threadIdx.x];
+    if (threadIdx.x + SOLVE_THREADS < BUCKETS) w.bucket[B_START + threadIdx.x + SOLVE_THREADS] = w.bucket[B_COUNT + threadIdx.x + SOLVE_THREADS];
     __syncthreads();
-    if (threadIdx.x < MAX_COLORS) w.colorStart[threadIdx.x] = w.colorHist[threadIdx.x * gridDim.x];
-    if (threadIdx.x == 0) w.colorStart[MAX_COLORS] = total;
-  }
-  GSYNC
-  color_scatter_chunk(w, lo, hi);
-  GSYNC
-
-  // E. incidence list: for each colour position s (body b = colorBodies[s]) its rows in order,
-  // joints as one entry, contact pairs as one entry per point; OWNER_BIT where b is the last of the
-  // constraint's dynamic bodies to move in an iteration
-  const uint32_t numDyn = ldv(&w.colorStart[MAX_COLORS]);
-  const uint32_t numColors = ldv(&ctr[C_COLORS]);
-  for (uint32_t s = tid; s < numDyn; s += T) {
-    uint32_t b = w.colorBodies[s];
-    uint32_t count = 0;
-    for (uint32_t e = w.adjStart[b]; e < w.adjStart[b + 1]; e++) {
-      uint32_t c = w.adjList[e];
-      count += c < nj ? 1u : (w.mIds[p.cur][c - nj].w & 15u);
+    uint32_t total = block_scan_range(w.bucket + B_START, 0, BUCKETS);
+    if (threadIdx.x == 0) w.bucket[B_START + BUCKETS] = total;
+    if (threadIdx.x < (uint32_t)MAX_COLORS) {
+      uint32_t c = threadIdx.x, lanes = 0;
+      for (int j = 0; j < LANE_CLASSES; j++) {
+        w.bucket[B_LANE + c * LANE_CLASSES + j] = lanes;
+        lanes += w.bucket[B_COUNT + c * LANE_CLASSES + j] * (32u >> j);
+      }
+      w.bucket[B_LANE_TOTAL + c] = lanes;
     }
-    w.incStart[s] = count;
+    __syncthreads();
+    if (threadIdx.x <= (uint32_t)MAX_COLORS) w.colorStart[threadIdx.x] = w.bucket[B_START + threadIdx.x * LANE_CLASSES];
   }
-  if (tid == 0) w.incStart[numDyn] = 0;
   GSYNC
-  if (!grid_scan(w.incStart, numDyn + 1, w.scanScratch, bar, ctr)) return;
-  const uint32_t totalInc = ldv(&w.scanScratch[gridDim.x]);
+  const uint32_t numDyn = ldv(&w.bucket[B_START + BUCKETS]);
+  const uint32_t numColors = ldv(&ctr[C_COLORS]);
+  {
+    // each block reserves one range per bucket for its bodies, then places them by shared counters
+    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
+    __syncthreads();
+    for (uint32_t b = tid; b < n; b += T) {
+      if (!dynBody(w, (int)b)) continue;
+      atomicAdd(&s_hist[(w.colorA[b] & 0xffu) * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b]))], 1u);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) {
+      s_base[k] = s_hist[k] ? w.bucket[B_START + k] + atomicAdd(&w.bucket[B_FILL + k], s_hist[k]) : 0u;
+      s_hist[k] = 0;
+    }
+    __syncthreads();
+    for (uint32_t b = tid; b < n; b += T) {
+      if (!dynBody(w, (int)b)) continue;
+      uint32_t bucket = (w.colorA[b] & 0xffu) * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b]));
+      uint32_t pos = s_base[bucket] + atomicAdd(&s_hist[bucket], 1u);
+      w.colorBodies[pos] = b;
+      w.incStart[pos] = w.incCount[b];
+    }
+  }
   if (tid == 0) {
-    ctr[C_INC] = totalInc;
+    w.incStart[numDyn] = 0;
     ctr[C_DYN] = numDyn;
   }
+  GSYNC
+
+  // E. incidence list: for each colour position s (body b = colorBodies[s]) its rows in summation
+  // order, with the partner body and OWNER_BIT where b is the last of the row's dynamic bodies to move
+  if (!grid_scan(w.incStart, numDyn + 1, w.scanScratch, bar, ctr)) return;
+  const uint32_t totalInc = ldv(&w.scanScratch[gridDim.x]);
+  if (tid == 0) ctr[C_INC] = totalInc;
   if (totalInc > p.incCap) {
     if (tid == 0) atomicOr(&ctr[C_ERROR], ERR_INC_OVERFLOW);
     return;  // uniform: every block read the same total after the barrier
@@ -735,30 +764,19 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
     uint32_t colB = w.colorA[b] & 0xffu;
     uint32_t out = w.incStart[s];
     for (uint32_t e = w.adjStart[b]; e < w.adjStart[b + 1]; e++) {
-      uint32_t c = w.adjList[e];
-      int ea, eb;
-      uint32_t cnt;
-      if (c < nj) {
-        int4 in = w.jinfo[c];
-        ea = in.y;
-        eb = in.z;
-        cnt = 1;
-      } else {
-        uint4 ids = w.mIds[p.cur][c - nj];
-        ea = (int)ids.x;
-        eb = (int)ids.y;
-        cnt = ids.w & 15u;
-      }
-      int other = ea == (int)b ? eb : ea;
+      uint4 ent = w.adjList[e];
+      uint32_t c = ent.z & 0x0fffffffu, cnt = ent.z >> 28;
       bool owner = true;
-      if (dynBody(w, other)) {
+      if (ent.w & 0x80000000u) {
+        uint32_t other = ent.w & 0x7fffffffu;
         uint32_t colO = w.colorA[other] & 0xffu;
-        owner = colO < colB || (colO == colB && (uint32_t)other < b);
+        owner = colO < colB || (colO == colB && other < b);
       }
       uint32_t flag = owner ? OWNER_BIT : 0u;
-      if (c < nj) w.incList[out++] = c | flag;
+      uint32_t partner = ent.w & 0x7fffffffu;
+      if (c < nj) w.incList[out++] = make_uint2(c | flag, partner);
       else
-        for (uint32_t k = 0; k < cnt; k++) w.incList[out++] = (nj + (c - nj) * MAX_CONTACTS + k) | flag;
+        for (uint32_t k = 0; k < cnt; k++) w.incList[out++] = make_uint2((nj + (c - nj) * MAX_CONTACTS + k) | flag, partner);
     }
   }
 
@@ -802,43 +820,70 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
     bool atRest = (p.flags & FLAG_START_AT_REST) != 0u && slow;
     w.ipos[i] = make_float4(pos.x, pos.y, pos.z, 0.0f);
     w.irot[i] = rot;
+    float3 x = f3(pos);
+    float4 q = rot;
     if (dynamic && !atRest) {
-      float3 x = f3(pos) + f3(vel) * dt + up * (g * (wgt * dt * dt));
-      w.pos[i] = make_float4(x.x, x.y, x.z, pos.w);
-      w.rot[i] = qadd(rot, av * dt);
+      x = f3(pos) + f3(vel) * dt + up * (g * (wgt * dt * dt));
+      q = qadd(rot, av * dt);
     }
     if (!dynamic && (vel.x != 0.0f || vel.y != 0.0f || vel.z != 0.0f || av.x != 0.0f || av.y != 0.0f || av.z != 0.0f)) {
-      float3 x = f3(pos) + f3(vel) * dt;
-      w.pos[i] = make_float4(x.x, x.y, x.z, pos.w);
-      w.rot[i] = qadd(rot, av * dt);
+      x = f3(pos) + f3(vel) * dt;
+      q = qadd(rot, av * dt);
     }
+    w.pos[i] = make_float4(x.x, x.y, x.z, pos.w);
+    w.rot[i] = q;
+    float3 dl = x - f3(pos), da = qsub(q, rot);
+    w.dlin[i] = make_float4(dl.x, dl.y, dl.z, 0.0f);
+    w.dang[i] = make_float4(da.x, da.y, da.z, 0.0f);
   }
   GSYNC
 
-  // G. iterations: each colour one sweep of its bodies, `lanes` threads per body
+  // G. iterations: per colour, each body's group of lanes (its lane class) accumulates its rows, the
+  // group sums in registers, the first lane solves, and every lane then updates the rows it owns.
+  // The colours' lane tables (lane bases, bucket starts, lane totals) are kept in shared memory.
+  __shared__ uint32_t s_lane[BUCKETS], s_start[BUCKETS], s_total[MAX_COLORS];
+  for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) {
+    s_lane[k] = w.bucket[B_LANE + k];
+    s_start[k] = w.bucket[B_START + k];
+  }
+  if (threadIdx.x < (uint32_t)MAX_COLORS) s_total[threadIdx.x] = w.bucket[B_LANE_TOTAL + threadIdx.x];
+  __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warpGlobal = tid >> 5, nwarps = T >> 5;
   const float dt2 = dt * dt;
   for (int it = 0; it < p.iterations; it++) {
     for (uint32_t c = 0; c < numColors; c++) {
-      const uint32_t s0 = w.colorStart[c], nb = w.colorStart[c + 1] - s0;
-      uint32_t L = 1;
-      while (L < 16u && nb * L * 2u <= T) L <<= 1;
-      const uint32_t groupsPerWarp = 32u / L;
-      const uint32_t sub = lane & (L - 1u), leader = lane & ~(L - 1u);
-      for (uint32_t base = warpGlobal * groupsPerWarp; base < nb; base += nwarps * groupsPerWarp) {
-        const uint32_t g = base + lane / L;
-        const bool active = g < nb;
+      const uint32_t laneTotal = s_total[c];
+      const uint32_t* laneBase = s_lane + c * LANE_CLASSES;
+      const uint32_t* bucketStart = s_start + c * LANE_CLASSES;
+      for (uint32_t base = warpGlobal * 32u; base < laneTotal; base += nwarps * 32u) {
+        const uint32_t lam = base + lane;
+        const bool active = lam < laneTotal;
+        uint32_t j = 0;
+        if (active)
+          while (j + 1 < (uint32_t)LANE_CLASSES && lam >= laneBase[j + 1]) j++;
+        const uint32_t L = active ? (32u >> j) : 1u;
+        const uint32_t local = active ? lam - laneBase[j] : 0u;
+        const uint32_t sub = local & (L - 1u);
+        const uint32_t leader = lane - sub;
         uint32_t body = 0, e0 = 0, e1 = 0;
         Pose own;
         Acc acc;
         accZero(acc);
+        float3 x0 = make_float3(0.0f, 0.0f, 0.0f);
         if (active) {
-          body = w.colorBodies[s0 + g];
-          e0 = w.incStart[s0 + g];
-          e1 = w.incStart[s0 + g + 1];
-          own = loadPose(w, body);
+          const uint32_t s = bucketStart[j] + (local >> (5u - j));
+          body = w.colorBodies[s];
+          e0 = w.incStart[s];
+          e1 = w.incStart[s + 1];
+          float4 pos = w.pos[body];
+          own.x = f3(pos);
+          own.q = w.rot[body];
+          own.q0 = w.irot[body];
+          own.dLin = f3(w.dlin[body]);
+          own.dAng = f3(w.dang[body]);
           if (sub == 0) {
+            x0 = f3(w.ipos[body]);
             float m = w.size[body].w / dt2;
             float3 I = f3(w.moment[body]) / dt2;
             acc.v[0] = m;
@@ -856,31 +901,38 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
             acc.v[25] = ra.y;
             acc.v[26] = ra.z;
           }
-          for (uint32_t e = e0 + sub; e < e1; e += L) accumulateIncidence(acc, w, p, w.incList[e] & ~OWNER_BIT, body, own);
+          for (uint32_t e = e0 + sub; e < e1; e += L) accumulateIncidence(acc, w, p, w.incList[e], body, own);
         }
-        for (uint32_t off = L >> 1; off > 0; off >>= 1) {
+        // butterfly over the group: as many rounds as the warp's widest group needs
+        const uint32_t Lmax = __reduce_max_sync(0xffffffffu, L);
+        for (uint32_t off = Lmax >> 1; off > 0; off >>= 1) {
+          const bool take = off < L;
 #pragma unroll
-          for (int k = 0; k < 27; k++) acc.v[k] += __shfl_xor_sync(0xffffffffu, acc.v[k], off);
+          for (int k = 0; k < 27; k++) {
+            float o = __shfl_xor_sync(0xffffffffu, acc.v[k], off);
+            if (take) acc.v[k] += o;
+          }
         }
-        float3 x = own.x;
+        float3 x = own.x, dl = own.dLin, da = own.dAng;
         float4 q = own.q;
         if (active && sub == 0) {
           finishBody(acc, x, q);
+          dl = x - x0;
+          da = qsub(q, own.q0);
           w.pos[body] = make_float4(x.x, x.y, x.z, w.pos[body].w);
           w.rot[body] = q;
+          w.dlin[body] = make_float4(dl.x, dl.y, dl.z, 0.0f);
+          w.dang[body] = make_float4(da.x, da.y, da.z, 0.0f);
         }
-        x.x = __shfl_sync(0xffffffffu, x.x, leader);
-        x.y = __shfl_sync(0xffffffffu, x.y, leader);
-        x.z = __shfl_sync(0xffffffffu, x.z, leader);
-        q.x = __shfl_sync(0xffffffffu, q.x, leader);
-        q.y = __shfl_sync(0xffffffffu, q.y, leader);
-        q.z = __shfl_sync(0xffffffffu, q.z, leader);
-        q.w = __shfl_sync(0xffffffffu, q.w, leader);
+        own.x = make_float3(__shfl_sync(0xffffffffu, x.x, leader), __shfl_sync(0xffffffffu, x.y, leader), __shfl_sync(0xffffffffu, x.z, leader));
+        own.q = make_float4(__shfl_sync(0xffffffffu, q.x, leader), __shfl_sync(0xffffffffu, q.y, leader), __shfl_sync(0xffffffffu, q.z, leader),
+                            __shfl_sync(0xffffffffu, q.w, leader));
+        own.dLin = make_float3(__shfl_sync(0xffffffffu, dl.x, leader), __shfl_sync(0xffffffffu, dl.y, leader), __shfl_sync(0xffffffffu, dl.z, leader));
+        own.dAng = make_float3(__shfl_sync(0xffffffffu, da.x, leader), __shfl_sync(0xffffffffu, da.y, leader), __shfl_sync(0xffffffffu, da.z, leader));
         if (active) {
-          setPose(own, x, q);
           for (uint32_t e = e0 + sub; e < e1; e += L) {
-            uint32_t id = w.incList[e];
-            if (id & OWNER_BIT) dualIncidence(w, p, id & ~OWNER_BIT, body, own);
+            uint2 inc = w.incList[e];
+            if (inc.x & OWNER_BIT) dualIncidence(w, p, inc, body, own);
           }
         }
       }
@@ -902,6 +954,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
       w.vel[i] = make_float4(vel.x, vel.y, vel.z, prevUp);
     }
   }
+  grid_sync(bar, ctr);
 #undef GSYNC
 }
 
@@ -917,6 +970,7 @@ cudaError_t launch_topology_solve(const DWorld& w, const StepParams& p, int bloc
   cudaMemsetAsync(w.barrier, 0, 2 * sizeof(uint32_t), s);
   cudaMemsetAsync(w.adjStart, 0, (size_t(p.n) + 1) * sizeof(uint32_t), s);
   cudaMemsetAsync(w.adjFill, 0, (size_t(p.n) + 1) * sizeof(uint32_t), s);
+  cudaMemsetAsync(w.bucket, 0, BUCKET_WORDS * sizeof(uint32_t), s);
   DWorld wc = w;
   StepParams pc = p;
   void* args[] = {&wc, &pc};
