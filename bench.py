@@ -9,6 +9,12 @@ world's stream so every step starts with a cold L2 (inside the timed region).
 Single world: replicas only. With --gpus N (one process per GPU under torchrun) every rank runs its
 own 100k world; `value` is all ranks' body-steps over the slowest rank's time.
 
+With --batched-worlds N (4096 by default, 0 to skip) the line also carries `batched`: world-steps/s of
+N small worlds (lognormal sizes, median 64 bodies, sigma 0.5, clipped to [16, 512]; stacks or piles on
+their own ground) stepped together by the batched entry points, against the same worlds stepped one by
+one through the single-world entry points (a sample of them), and the batched step end to end through
+host buffers.
+
 --impl reference times the reference's CPU algorithm (the oracle port, GPU-mode rules, all host
 threads) on a bounded sample of the same workload: the same generator at 2000 bodies, its whole
 rollout.
@@ -150,6 +156,100 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, dist) -> dict:
+    """world-steps/s of the batched workload, batched launch against per-world launches."""
+    import numpy as np
+    import avbd_b200
+    from avbd_b200.scenes import batched_worlds
+
+    scenes = batched_worlds(args.batched_worlds, seed=3 + rank)
+    n = sum(len(s.bodies) for s in scenes)
+    dyn = sum(s.dynamic_count for s in scenes)
+    b = avbd_b200.BatchSolver3D(len(scenes), n, 1, params=scenes[0].params, device=local)
+    for s in scenes:
+        b.add_scene(s)
+    tuning = b.tune(2)
+    b.step(args.warmup)
+    b.synchronize()
+    steps = args.batched_steps
+    stream = torch.cuda.ExternalStream(b.stream, device=local)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            b.step(1)
+            flush.zero_()
+        e1.record(stream)
+    b.synchronize()
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    errors = sum(1 for i in range(len(scenes)) if b.read_counters(i)['error'])
+    info = b.info()
+
+    # end to end: every step uploads all bodies from pinned host memory and reads them back
+    host = torch.empty(n * 160, dtype=torch.uint8).pin_memory()
+    host_np = host.numpy().view(avbd_b200.BODY_DTYPE)
+    b.read_all_bodies_into(host_np)
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            b.write_all_bodies_async(host_np)
+            b.step(1)
+            b.read_all_bodies_into(host_np, sync=True)
+        e1.record(stream)
+    b.synchronize()
+    barrier()
+    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
+    if world_size > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    b.destroy()
+
+    # per-world launches: a sample of the same worlds, each stepped through the single-world API
+    sample = scenes[::max(1, len(scenes) // args.plain_sample)][:args.plain_sample]
+    worlds = [avbd_b200.CudaSolver3D(s, device=local) for s in sample]
+    for w in worlds:
+        w.step(args.warmup)
+        w.synchronize()
+    plain_steps = max(1, min(steps, 30))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(plain_steps):
+        for w in worlds:
+            w.step(1)
+    for w in worlds:
+        w.synchronize()
+    plain_s = time.perf_counter() - t0
+    for w in worlds:
+        w.destroy()
+    value = world_size * len(scenes) * steps / (ms / 1000.0)
+    plain = len(sample) * plain_steps / plain_s
+    return {
+        'metric': 'world-steps/s', 'value': value, 'ms_per_step': ms / steps, 'steps': steps,
+        'body_steps_per_s': world_size * dyn * steps / (ms / 1000.0),
+        'per_world_launch': {'value': plain, 'unit': 'world-steps/s', 'sample_worlds': len(sample), 'steps': plain_steps,
+                             'how': 'each sampled world stepped through the single-world entry points in turn, wall clock'},
+        'speedup_vs_per_world_launch': value / world_size / plain,
+        'e2e': {'value': world_size * len(scenes) * steps / (float(te.item()) / 1000.0), 'unit': 'world-steps/s',
+                'h2d_bytes_per_step': n * 160, 'd2h_bytes_per_step': n * 160},
+        'worlds': len(scenes), 'bodies': n, 'dynamic_bodies': dyn, 'world_errors': errors,
+        'launch': {'collide_threads': info['collide_threads'], 'collide_blocks': info['collide_blocks'], 'solve_blocks': info['solve_blocks'],
+                   'graphs': bool(info['graphs'])},
+        'tuning_ms': {f"{c['collide_threads']}x{c['solve_blocks']}": round(c['ms_per_step'], 4) for c in tuning['candidates']},
+        'gpu_launches': 2 * steps,
+        'config': {'workload': f'{len(scenes)} worlds, bodies per world round(lognormal(median 64, sigma 0.5)) clipped to [16, 512]; '
+                               'half stacks of unit cubes, half piles of unit cubes and r 0.5 spheres, each on its own ground box; '
+                               f'dt 1/60, 10 iterations; timed steps {args.warmup + 1 + tuning["steps_taken"]}..'
+                               f'{args.warmup + tuning["steps_taken"] + steps} after tuning and warm-up',
+                   'seed': 3 + rank, 'l2': '256 MiB memset between timed steps, inside the timed region'},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -159,6 +259,10 @@ def main():
     ap.add_argument('--bodies', type=int, default=PILE_BODIES)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-graphs', action='store_true', help='launch each kernel directly instead of replaying the step graph')
+    ap.add_argument('--batched-worlds', type=int, default=4096, help='worlds of the batched workload (0: skip it)')
+    ap.add_argument('--batched-steps', type=int, default=300)
+    ap.add_argument('--plain-sample', type=int, default=64, help='worlds stepped one by one for the per-world comparison')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -190,7 +294,10 @@ def main():
     n_dyn = scene.dynamic_count
 
     def fresh():
-        return avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
+        w = avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
+        if args.no_graphs:
+            w.use_graphs(False)
+        return w
 
     # Warm-up on its own world (module load, first touch), then a fresh world for the timed rollout
     warm = fresh()
@@ -216,6 +323,7 @@ def main():
     ms = start.elapsed_time(end)
     stats = w.read_step_stats()
     counters = w.read_counters()
+    graphs = bool(counters['graphs'])
     if counters['error'] or counters['overflow']:
         print(f'warning: counters {counters}', file=sys.stderr)
     w.destroy()
@@ -270,6 +378,10 @@ def main():
                'd2h_bytes_per_step': nbytes}
         w2.destroy()
 
+    batched = None
+    if args.batched_worlds > 0:
+        batched = run_batched(args, local, rank, world_size, barrier, torch, dist)
+
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         ref = cpu_reference(SAMPLE_BODIES, ROLLOUT, os.cpu_count() or 1)
@@ -284,11 +396,14 @@ def main():
             'roofline': {'bound': 'hbm', 'kernel': 'k_topology_solve', 'achieved': achieved, 'peak': peak, 'peak_kind': peak_kind, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / max(len(stats), 1)},
             'phases_ms_per_step': {'collision': coll_ms / max(len(stats), 1), 'topology_solve': solve_ms / max(len(stats), 1)},
-            'pile_last_step': {k: int(stats[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors', 'dynamic_bodies')} if len(stats) else None,
+            'pile_last_step': dict({k: int(stats[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors', 'dynamic_bodies', 'adjacency', 'incidences')},
+                                   alg_bytes=alg_bytes(stats[-1])) if len(stats) else None,
             'gpu_launches': int(stats['launches'].sum()),
+            'cuda_graphs': graphs,
             'clocks': clocks.summary(),
             'e2e': e2e,
             'cpu_baseline': cpu,
+            'batched': batched,
             'device': name[0] if name else None,
         }
         print(json.dumps(line), flush=True)

@@ -133,7 +133,7 @@ typedef struct avbd_config {
 typedef struct avbd_counters {
   uint32_t pairs, contacts, manifolds, overflow; /* overflow: 1 pairs, 2 contacts, 4 manifolds */
   uint32_t clashes, colors, rounds, error;       /* error: nonzero after a bounded wait gave up */
-  uint32_t steps, pair_capacity, reserved0, reserved1;
+  uint32_t steps, pair_capacity, graphs, launches; /* graphs: steps replay a CUDA graph; launches: kernels per step */
 } avbd_counters;
 
 typedef struct avbd_world avbd_world;
@@ -197,9 +197,11 @@ int avbd_read_counters(avbd_world* world, avbd_counters* counters);
 int avbd_read_bodies_async(avbd_world* world, avbd_body* dst, uint32_t cap);
 
 /* Per-step statistics (profileNextStep / readCounters, gpu/solver.ts:1951-1953, 2305-2309): with
- * avbd_enable_step_stats(world, capacity) each step records device times of its two phases and a
- * snapshot of its counters into a ring of `capacity` entries, without host synchronisation;
- * avbd_read_step_stats returns them oldest first. capacity 0 turns it off. */
+ * avbd_enable_step_stats(world, capacity) each step writes the device-clock times of its two phases
+ * (collision: from the step's first kernel to the solve kernel's start; solve: the topology+solve
+ * kernel) and a snapshot of its counters into a device ring of `capacity` entries, inside the step
+ * (so it works under graph replay, without host synchronisation); avbd_read_step_stats returns the
+ * entries oldest first. capacity 0 turns it off. */
 typedef struct avbd_step_stats {
   float collision_ms, solve_ms;  /* broadphase + narrowphase; topology + warm start + iterations + velocities */
   uint32_t pairs, contacts, manifolds, adjacency, incidences, dynamic_bodies, colors, rounds, launches, error;
@@ -211,6 +213,14 @@ int avbd_read_step_stats(avbd_world* world, avbd_step_stats* dst, uint32_t cap, 
  * last step: the per-phase profile of the persistent kernel (profileNextStep's phases, gpu/solver.ts:2159-2172). */
 int avbd_read_phase_clocks(avbd_world* world, double* dst, uint32_t cap, uint32_t* n);
 
+/* Steps replay a captured CUDA graph (default on; per-step statistics launch directly). */
+int avbd_use_graphs(avbd_world* world, int enable);
+
+/* Blocks of the cooperative topology + solve launch (0: every co-resident block, the default). The
+ * lane groups a body's rows are summed in depend on the launch's thread count, so results differ in
+ * the last bits between launch shapes; one block reproduces a batched world's step bit for bit. */
+int avbd_set_solve_blocks(avbd_world* world, int blocks);
+
 /* The world's CUDA stream (cudaStream_t) for callers that order their own device work with its steps. */
 int avbd_world_stream(avbd_world* world, void** stream);
 
@@ -218,6 +228,76 @@ int avbd_world_stream(avbd_world* world, void** stream);
  * without validation or synchronisation: shapes, masses and radii must be unchanged (use
  * avbd_write_bodies for those). Keeps the bodies' contact history. */
 int avbd_write_bodies_async(avbd_world* world, uint32_t first, const avbd_body* bodies, uint32_t n);
+
+/* ---- Batched worlds ------------------------------------------------------------------------------
+ * No counterpart in the reference, which steps one world per GpuSolver3D (gpu/solver.ts:598). A batch
+ * holds many small independent worlds (1 to AVBD_BATCH_MAX_WORLD_BODIES bodies each) and steps them
+ * all with two launches per step, one block per world, captured in a CUDA graph. Each world runs
+ * exactly the single-world step (pair rule, narrowphase, warm start, Jones-Plassmann colouring,
+ * Gauss-Seidel solve, dual, velocities) on its own bodies; indices inside a world are local to it.
+ * The worlds share one avbd_params. Not thread-safe; one stream per batch. */
+typedef struct avbd_batch avbd_batch;
+
+#define AVBD_BATCH_MAX_WORLD_BODIES 4096u
+#define AVBD_BATCH_TUNE_CANDIDATES 8
+
+typedef struct avbd_batch_config {
+  uint32_t world_capacity; /* worlds */
+  uint32_t body_capacity;  /* bodies over all worlds */
+  uint32_t joint_capacity; /* joints over all worlds */
+  uint32_t pairs_per_body; /* a new world's pair slots per body (0: 6); grows per world as needed */
+  int32_t device;
+} avbd_batch_config;
+
+typedef struct avbd_batch_world {
+  uint32_t first_body, bodies, first_joint, joints, pair_capacity, fixed_colors;
+} avbd_batch_world;
+
+typedef struct avbd_batch_status {
+  uint32_t worlds, bodies, joints, steps;
+  uint64_t pair_slots;
+  uint32_t relayouts; /* times pair storage was laid out again for a world that outgrew it */
+  uint32_t collide_threads, collide_blocks, solve_blocks, graphs;
+} avbd_batch_status;
+
+/* The autotuner's measurements: per candidate launch shape its mean step time */
+typedef struct avbd_batch_tuning {
+  uint32_t candidates;
+  uint32_t candidate_threads[AVBD_BATCH_TUNE_CANDIDATES];
+  uint32_t candidate_solve_blocks[AVBD_BATCH_TUNE_CANDIDATES];
+  float candidate_ms[AVBD_BATCH_TUNE_CANDIDATES];
+  uint32_t collide_threads, solve_blocks; /* the choice */
+  float ms_per_step;
+  uint32_t steps_taken; /* tuning steps are real steps: the worlds advance by this many */
+} avbd_batch_tuning;
+
+int avbd_batch_create(const avbd_batch_config* config, avbd_batch** out);
+int avbd_batch_destroy(avbd_batch* batch);
+const char* avbd_batch_last_error(const avbd_batch* batch);
+int avbd_batch_set_params(avbd_batch* batch, const avbd_params* params);
+/* A new world from host records (as avbd_add_bodies + avbd_add_joints + avbd_add_ignore_pairs on a
+ * fresh world); joint and ignore-pair indices are local to the world. */
+int avbd_batch_add_world(avbd_batch* batch, const avbd_body* bodies, uint32_t n, const avbd_joint* joints, const avbd_joint_info* info,
+                         uint32_t n_joints, const uint32_t* ignore_pairs_ab, uint32_t n_ignore, uint32_t* index);
+/* A new world that continues a single world exactly: bodies, joints, filters, no-collide pairs, last
+ * step's contacts (warm starts), colour state and fixed colours are copied from it. */
+int avbd_batch_add_world_from(avbd_batch* batch, avbd_world* world, uint32_t* index);
+int avbd_batch_world_info(avbd_batch* batch, uint32_t world, avbd_batch_world* out);
+int avbd_batch_step(avbd_batch* batch, int n);
+int avbd_batch_synchronize(avbd_batch* batch);
+int avbd_batch_read_bodies(avbd_batch* batch, uint32_t world, avbd_body* dst, uint32_t cap, uint32_t* n);
+int avbd_batch_read_joints(avbd_batch* batch, uint32_t world, avbd_joint* dst, avbd_joint_info* info, uint32_t cap, uint32_t* n);
+int avbd_batch_read_colors(avbd_batch* batch, uint32_t world, uint32_t* dst, uint32_t cap, uint32_t* n);
+int avbd_batch_read_counters(avbd_batch* batch, uint32_t world, avbd_counters* counters);
+/* Every world's bodies in batch order (world w at its first_body), on the batch's stream */
+int avbd_batch_read_all_bodies_async(avbd_batch* batch, avbd_body* dst, uint32_t cap);
+int avbd_batch_write_all_bodies_async(avbd_batch* batch, const avbd_body* src, uint32_t n);
+int avbd_batch_use_graphs(avbd_batch* batch, int enable);
+int avbd_batch_stream(avbd_batch* batch, void** stream);
+/* Times each candidate launch shape (collision block size x solve blocks) over `steps` real steps
+ * and keeps the fastest. */
+int avbd_batch_tune(avbd_batch* batch, int steps, avbd_batch_tuning* out);
+int avbd_batch_info(avbd_batch* batch, avbd_batch_status* out);
 
 #ifdef __cplusplus
 }

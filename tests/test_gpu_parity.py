@@ -217,6 +217,24 @@ def test_determinism_bitwise(cuda_lib):
     assert np.array_equal(runs[0], runs[1])
 
 
+def test_graph_replay_matches_direct_launches(cuda_lib):
+    """A step replayed from a captured CUDA graph does exactly what the direct launches do."""
+    s = drop_pile(6000, seed=6, spacing=1.6, layers=6)
+    out = []
+    for graphs in (True, False):
+        w = avbd_b200.CudaSolver3D(s)
+        w.use_graphs(graphs)
+        w.enable_step_stats(64)
+        w.step(70)
+        c = w.read_counters()
+        assert c['graphs'] == (1 if graphs else 0) and c['error'] == 0
+        st = w.read_step_stats()
+        assert len(st) == 64 and np.all(st['solve_ms'] > 0) and st['manifolds'][-1] > 500
+        out.append(w.read_bodies().view(np.uint32).copy())
+        w.destroy()
+    assert np.array_equal(out[0], out[1])
+
+
 def test_pivot_floor_keeps_sliver_finite(cuda_lib):
     """tests-gpu/pivot.gpu.test.ts:15-40: a light sliver on its edge under PENALTY_MAX contacts stays finite."""
     s = Scene('sliver')

@@ -2,9 +2,10 @@
 
 `CudaSolver3D` mirrors the reference's `GpuSolver3D` over the C ABI in include/avbd.h
 (libavbd_cuda.so, built in-tree by three-avbd_b200/build.py); `scenes` builds the reference's
-demo scenes and the synthetic workloads.
+demo scenes and the synthetic workloads; `BatchSolver3D` steps many small worlds together.
 """
 
 from . import scenes  # noqa: F401
 from ._abi import AvbdError, BODY_DTYPE, CONTACT_DTYPE, INFO_DTYPE, JOINT_DTYPE, MANIFOLD_DTYPE, LIB_PATH, load  # noqa: F401
-from .solver import CudaSolver3D, device_info, pack_bodies, pack_force  # noqa: F401
+from .solver import CudaSolver3D, device_info, pack_bodies, pack_force, scene_records  # noqa: F401
+from .batch import BatchSolver3D  # noqa: F401

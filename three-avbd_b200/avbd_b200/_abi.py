@@ -67,10 +67,36 @@ class Config(ctypes.Structure):
 
 class Counters(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ('pairs', 'contacts', 'manifolds', 'overflow', 'clashes', 'colors', 'rounds', 'error', 'steps',
-                                                'pair_capacity', 'reserved0', 'reserved1')]
+                                                'pair_capacity', 'graphs', 'launches')]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if not n.startswith('reserved')}
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [('world_capacity', ctypes.c_uint32), ('body_capacity', ctypes.c_uint32), ('joint_capacity', ctypes.c_uint32),
+                ('pairs_per_body', ctypes.c_uint32), ('device', ctypes.c_int32)]
+
+
+class BatchWorld(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ('first_body', 'bodies', 'first_joint', 'joints', 'pair_capacity', 'fixed_colors')]
+
+
+class BatchStatus(ctypes.Structure):
+    _fields_ = [('worlds', ctypes.c_uint32), ('bodies', ctypes.c_uint32), ('joints', ctypes.c_uint32), ('steps', ctypes.c_uint32),
+                ('pair_slots', ctypes.c_uint64), ('relayouts', ctypes.c_uint32), ('collide_threads', ctypes.c_uint32),
+                ('collide_blocks', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32), ('graphs', ctypes.c_uint32)]
+
+
+TUNE_CANDIDATES = 8
+BATCH_MAX_WORLD_BODIES = 4096
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [('candidates', ctypes.c_uint32), ('candidate_threads', ctypes.c_uint32 * TUNE_CANDIDATES),
+                ('candidate_solve_blocks', ctypes.c_uint32 * TUNE_CANDIDATES), ('candidate_ms', ctypes.c_float * TUNE_CANDIDATES),
+                ('collide_threads', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32), ('ms_per_step', ctypes.c_float),
+                ('steps_taken', ctypes.c_uint32)]
 
 
 # Every function include/avbd.h declares, with its argument types (the C-ABI symbol table)
@@ -106,8 +132,29 @@ SIGNATURES = {
     'avbd_enable_step_stats': ([P, U], I),
     'avbd_read_step_stats': ([P, VP, U, PU], I),
     'avbd_world_stream': ([P, ctypes.POINTER(ctypes.c_void_p)], I),
+    'avbd_use_graphs': ([P, I], I),
+    'avbd_set_solve_blocks': ([P, I], I),
     'avbd_read_phase_clocks': ([P, ctypes.POINTER(ctypes.c_double), U, PU], I),
     'avbd_write_bodies_async': ([P, U, VP, U], I),
+    'avbd_batch_create': ([ctypes.POINTER(BatchConfig), ctypes.POINTER(P)], I),
+    'avbd_batch_destroy': ([P], I),
+    'avbd_batch_last_error': ([P], ctypes.c_char_p),
+    'avbd_batch_set_params': ([P, ctypes.POINTER(Params)], I),
+    'avbd_batch_add_world': ([P, VP, U, VP, VP, U, PU, U, PU], I),
+    'avbd_batch_add_world_from': ([P, P, PU], I),
+    'avbd_batch_world_info': ([P, U, ctypes.POINTER(BatchWorld)], I),
+    'avbd_batch_step': ([P, I], I),
+    'avbd_batch_synchronize': ([P], I),
+    'avbd_batch_read_bodies': ([P, U, VP, U, PU], I),
+    'avbd_batch_read_joints': ([P, U, VP, VP, U, PU], I),
+    'avbd_batch_read_colors': ([P, U, PU, U, PU], I),
+    'avbd_batch_read_counters': ([P, U, ctypes.POINTER(Counters)], I),
+    'avbd_batch_read_all_bodies_async': ([P, VP, U], I),
+    'avbd_batch_write_all_bodies_async': ([P, VP, U], I),
+    'avbd_batch_use_graphs': ([P, I], I),
+    'avbd_batch_stream': ([P, ctypes.POINTER(ctypes.c_void_p)], I),
+    'avbd_batch_tune': ([P, I, ctypes.POINTER(BatchTuning)], I),
+    'avbd_batch_info': ([P, ctypes.POINTER(BatchStatus)], I),
 }
 
 _lib = None

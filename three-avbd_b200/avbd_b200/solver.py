@@ -114,6 +114,40 @@ def morton_order(positions: np.ndarray) -> np.ndarray:
     return np.lexsort((np.arange(len(code)), code))
 
 
+def to_params(sp) -> Params:
+    """A scenes.Params (the reference's SolverParams + GPU flags) as the C record; a Params passes through."""
+    if isinstance(sp, Params):
+        return sp
+    flags = (_abi.FLAG_MATCH_NEAREST if sp.match_nearest else 0) | (_abi.FLAG_FACE_BIAS if sp.face_bias else 0) | \
+            (_abi.FLAG_START_AT_REST if sp.start_at_rest else 0) | (_abi.FLAG_MASS_PENALTY if sp.mass_penalty else 0)
+    p = Params(dt=sp.dt, gravity=sp.gravity, alpha=sp.alpha, beta_lin=sp.beta_lin, beta_ang=sp.beta_ang, gamma=sp.gamma,
+               contact_margin=sp.contact_margin, iterations=sp.iterations, flags=flags)
+    p.up[0], p.up[1], p.up[2] = 0.0, 0.0, 1.0
+    return p
+
+
+def scene_records(scene: Scene, order=None):
+    """A scene as C-ABI records: bodies (in `order`), joints and springs with their infos, and ignore
+    pairs, with body indices mapped through `order` (GpuSolver3D's refToGpu)."""
+    n = len(scene.bodies)
+    order = np.arange(n) if order is None else np.asarray(order)
+    gpu_index = np.empty(n, dtype=np.int64)
+    gpu_index[order] = np.arange(n)
+    bodies = pack_bodies([scene.bodies[i] for i in order])
+    recs, infos, ignores = [], [], []
+    for f in scene.forces:
+        if f.kind == 'ignore':
+            ignores.append((int(gpu_index[f.a]), int(gpu_index[f.b])))
+            continue
+        r, i = pack_force(f, scene.bodies)
+        i['a'] = int(gpu_index[f.a]) if f.a >= 0 else -1
+        i['b'] = int(gpu_index[f.b])
+        recs.append(r)
+        infos.append(i)
+    return (bodies, np.array(recs, dtype=JOINT_DTYPE), np.array(infos, dtype=INFO_DTYPE),
+            np.array(ignores, dtype=np.uint32).reshape(-1, 2))
+
+
 class CudaSolver3D:
     """One world on one B200. Mirrors GpuSolver3D's construction from a scene (`new GpuSolver3D(device,
     ref, {spatialSort})`): bodies and joints are uploaded in creation order (or Morton order with
@@ -139,21 +173,12 @@ class CudaSolver3D:
                 self.order = morton_order(np.array([b.pos for b in scene.bodies]))
                 self.gpu_index = np.empty(n, dtype=np.int64)
                 self.gpu_index[self.order] = np.arange(n)
-            self.add_bodies(pack_bodies([scene.bodies[i] for i in self.order]))
-            recs, infos, ignores = [], [], []
-            for f in scene.forces:
-                if f.kind == 'ignore':
-                    ignores.append((int(self.gpu_index[f.a]), int(self.gpu_index[f.b])))
-                    continue
-                r, i = pack_force(f, scene.bodies)
-                i['a'] = int(self.gpu_index[f.a]) if f.a >= 0 else -1
-                i['b'] = int(self.gpu_index[f.b])
-                recs.append(r)
-                infos.append(i)
-            if recs:
-                self.add_joints(np.array(recs, dtype=JOINT_DTYPE), np.array(infos, dtype=INFO_DTYPE))
-            if ignores:
-                self.add_ignore_pairs(np.array(ignores, dtype=np.uint32))
+            bodies, joints, infos, ignores = scene_records(scene, self.order)
+            self.add_bodies(bodies)
+            if len(joints):
+                self.add_joints(joints, infos)
+            if len(ignores):
+                self.add_ignore_pairs(ignores)
 
     # --- lifetime ---
     def destroy(self):
@@ -182,15 +207,7 @@ class CudaSolver3D:
     @params.setter
     def params(self, sp):
         """Accepts a scenes.Params (the reference's SolverParams + GPU flags) or a ctypes Params."""
-        if isinstance(sp, Params):
-            self._check(self.lib.avbd_set_params(self.handle, ctypes.byref(sp)))
-            return
-        flags = (_abi.FLAG_MATCH_NEAREST if sp.match_nearest else 0) | (_abi.FLAG_FACE_BIAS if sp.face_bias else 0) | \
-                (_abi.FLAG_START_AT_REST if sp.start_at_rest else 0) | (_abi.FLAG_MASS_PENALTY if sp.mass_penalty else 0)
-        p = Params(dt=sp.dt, gravity=sp.gravity, alpha=sp.alpha, beta_lin=sp.beta_lin, beta_ang=sp.beta_ang, gamma=sp.gamma,
-                   contact_margin=sp.contact_margin, iterations=sp.iterations, flags=flags)
-        p.up[0], p.up[1], p.up[2] = 0.0, 0.0, 1.0
-        self._check(self.lib.avbd_set_params(self.handle, ctypes.byref(p)))
+        self._check(self.lib.avbd_set_params(self.handle, ctypes.byref(to_params(sp))))
 
     # --- scene edits ---
     def add_bodies(self, records: np.ndarray) -> int:
@@ -260,6 +277,14 @@ class CudaSolver3D:
 
     def synchronize(self):
         self._check(self.lib.avbd_synchronize(self.handle))
+
+    def use_graphs(self, on: bool = True):
+        """Replay each step as a captured CUDA graph (default on)."""
+        self._check(self.lib.avbd_use_graphs(self.handle, 1 if on else 0))
+
+    def set_solve_blocks(self, blocks: int = 0):
+        """Blocks of the cooperative topology + solve launch (0: all co-resident ones)."""
+        self._check(self.lib.avbd_set_solve_blocks(self.handle, blocks))
 
     def enable_step_stats(self, capacity: int):
         """Record per-step device times and counters into a ring of `capacity` steps (no host syncs)."""

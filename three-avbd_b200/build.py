@@ -19,6 +19,7 @@ UNITS = {
     'avbd_collide.cu': ['--fmad=false'],
     'avbd_solve.cu': [],
     'avbd_host.cu': [],
+    'avbd_batch.cu': [],
 }
 
 
@@ -38,7 +39,7 @@ def _stale(out: str, deps: list) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')] + [os.path.join(HERE, '..', 'include', 'avbd.h')]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cuh', '.hpp'))] + [os.path.join(HERE, '..', 'include', 'avbd.h')]
     objs = []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)

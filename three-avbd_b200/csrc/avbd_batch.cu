@@ -1,0 +1,763 @@
+// Batched worlds: many small independent worlds stepped together, one block per world.
+//
+// The reference steps one world per GpuSolver3D (src/avbd3d/gpu/solver.ts:598) and has no batched
+// mode; a batch runs the same step, world by world, with every launch shared:
+//   - the worlds' records are concatenated (bodies, joints, pair slots, scratch), and a table of
+//     WorldDesc gives each world's slices; a world's indices are local to it;
+//   - one launch collides every world (all pairs of a world against the pair rule, then the
+//     narrowphase), one launch runs every world's topology, colouring and solve at block scope;
+//     blocks take worlds from a queue, largest first;
+//   - the step is captured in a CUDA graph per contact-buffer parity;
+//   - pair storage grows per world, as a world's does (gpu/solver.ts:2362-2377): the collision
+//     kernel flags a world past 80 % or overflowing, and the next step lays the batch out again.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "avbd_host.hpp"
+
+using namespace avbd;
+
+struct avbd_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  avbd_params params{};
+  uint32_t worldCap = 0, bodyCap = 0, jointCap = 0, pairsPerBody = 6;
+  uint32_t n = 0, nj = 0;  // bodies and joints used over all worlds
+  std::vector<WorldDesc> worlds;
+  std::vector<uint32_t> statics;  // every world's no-collide triples
+  DWorld d{};
+  WorldDesc* dWorlds = nullptr;
+  uint32_t *dOrder = nullptr, *dQueue = nullptr, *dStatus = nullptr;
+  uint32_t staticsAlloc = 0;
+  // pair-dependent storage: allocated entries and entries used by the worlds' slices
+  uint64_t pairAlloc = 0, hashAlloc = 0, adjAlloc = 0, incAlloc = 0;
+  uint64_t pairUsed = 0, hashUsed = 0, adjUsed = 0, incUsed = 0;
+  uint64_t pairReserve = 0;  // the first allocation: pairs_per_body slots for every body of the capacity
+  bool tableDirty = true;
+  int cur = 0;
+  uint32_t stepCount = 0;
+  // launch shape (the autotuner's choice)
+  int sms = 0, collideThreads = 128, collideBlocks = 0, solveBlocks = 0;
+  // status of the last step, copied back asynchronously
+  uint32_t* hStatus = nullptr;
+  cudaEvent_t statusReady = nullptr;
+  bool statusInFlight = false;
+  uint32_t relayouts = 0;
+  bool useGraphs = true;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  uint64_t graphGen[2] = {0, 0};
+  uint64_t configGen = 1;
+  std::vector<void*> allocations;
+};
+
+namespace {
+
+int bfail(avbd_batch* b, int code, const std::string& msg) {
+  if (b) b->error = msg;
+  return code;
+}
+
+#define BATCH_TRY(b, call)                                                                                   \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess) return bfail(b, AVBD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+cudaError_t balloc(avbd_batch* b, T** p, size_t count) {
+  void* ptr = nullptr;
+  cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) return e;
+  b->allocations.push_back(ptr);
+  *p = static_cast<T*>(ptr);
+  return cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), b->stream);
+}
+void bfree(avbd_batch* b, void* p) {
+  if (!p) return;
+  auto it = std::find(b->allocations.begin(), b->allocations.end(), p);
+  if (it != b->allocations.end()) b->allocations.erase(it);
+  cudaFree(p);
+}
+
+// A world's pair-dependent slice sizes from its pair capacity (the single world's rule, allocPairs)
+void sizeSlices(WorldDesc& w, uint32_t pairCap) {
+  w.pairCap = pairCap;
+  w.hashMask = pow2AtLeast(2ull * pairCap) - 1u;
+  w.adjCap = 2u * (pairCap + w.nj);
+  w.incCap = 2u * (pairCap * MAX_CONTACTS + w.nj);
+}
+
+// Reallocates the pair-dependent arrays for the worlds' current slices. Last step's manifolds and
+// contacts (buffer 1 - cur) move with their world; the rest is scratch.
+int layoutPairs(avbd_batch* b, const std::vector<WorldDesc>& old) {
+  uint64_t pairs = 0, hash = 0, adj = 0, inc = 0;
+  for (auto& w : b->worlds) {
+    w.pair = uint32_t(pairs);
+    w.hash = uint32_t(hash);
+    w.adj = uint32_t(adj);
+    w.inc = uint32_t(inc);
+    pairs += w.pairCap;
+    hash += w.hashMask + 1ull;
+    adj += w.adjCap;
+    inc += w.incCap;
+  }
+  if (pairs >= (1ull << 31) / MAX_CONTACTS || inc >= (1ull << 31) || adj >= (1ull << 31) || hash >= (1ull << 31))
+    return bfail(b, AVBD_ERR_CAPACITY, "batch pair storage past 2^31 entries");
+  b->pairUsed = pairs;
+  b->hashUsed = hash;
+  b->adjUsed = adj;
+  b->incUsed = inc;
+  DWorld& d = b->d;
+  const int prev = 1 - b->cur;
+  bool movePrev = false;
+  for (size_t i = 0; i < old.size() && !movePrev; i++) movePrev = old[i].pair != b->worlds[i].pair;
+  const bool grow = pairs > b->pairAlloc;
+  if (grow || movePrev) {
+    uint64_t cap = grow ? std::max<uint64_t>(std::max<uint64_t>(pairs, b->pairAlloc * 3 / 2), b->pairReserve) : b->pairAlloc;
+    uint4* ids[2] = {nullptr, nullptr};
+    float4* geo[2] = {nullptr, nullptr};
+    float4* pts[2] = {nullptr, nullptr};
+    for (int k = 0; k < 2; k++) {
+      BATCH_TRY(b, balloc(b, &ids[k], cap));
+      BATCH_TRY(b, balloc(b, &geo[k], cap));
+      BATCH_TRY(b, balloc(b, &pts[k], size_t(cap) * MAX_CONTACTS * 4));
+    }
+    if (d.mIds[prev] && !movePrev && !old.empty()) {
+      // worlds were only appended: the old slices keep their offsets
+      const WorldDesc& o = old.back();
+      size_t m = size_t(o.pair) + o.pairCap;
+      BATCH_TRY(b, cudaMemcpyAsync(ids[prev], d.mIds[prev], m * sizeof(uint4), cudaMemcpyDeviceToDevice, b->stream));
+      BATCH_TRY(b, cudaMemcpyAsync(geo[prev], d.mGeo[prev], m * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream));
+      BATCH_TRY(b, cudaMemcpyAsync(pts[prev], d.cPt[prev], m * MAX_CONTACTS * 4 * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream));
+      BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    } else if (d.mIds[prev]) {
+      for (size_t i = 0; i < old.size(); i++) {
+        const WorldDesc &o = old[i], &w = b->worlds[i];
+        size_t m = std::min(o.pairCap, w.pairCap);
+        BATCH_TRY(b, cudaMemcpyAsync(ids[prev] + w.pair, d.mIds[prev] + o.pair, m * sizeof(uint4), cudaMemcpyDeviceToDevice, b->stream));
+        BATCH_TRY(b, cudaMemcpyAsync(geo[prev] + w.pair, d.mGeo[prev] + o.pair, m * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream));
+        BATCH_TRY(b, cudaMemcpyAsync(pts[prev] + size_t(w.pair) * MAX_CONTACTS * 4, d.cPt[prev] + size_t(o.pair) * MAX_CONTACTS * 4,
+                                     m * MAX_CONTACTS * 4 * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream));
+      }
+      BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    }
+    for (int k = 0; k < 2; k++) {
+      bfree(b, d.mIds[k]);
+      bfree(b, d.mGeo[k]);
+      bfree(b, d.cPt[k]);
+      d.mIds[k] = ids[k];
+      d.mGeo[k] = geo[k];
+      d.cPt[k] = pts[k];
+    }
+    bfree(b, d.pairs);
+    BATCH_TRY(b, balloc(b, &d.pairs, cap));
+    b->pairAlloc = cap;
+  }
+  if (hash > b->hashAlloc) {
+    bfree(b, d.hash);
+    b->hashAlloc = std::max<uint64_t>(hash, b->hashAlloc * 3 / 2);
+    BATCH_TRY(b, balloc(b, &d.hash, b->hashAlloc));
+  }
+  if (adj > b->adjAlloc) {
+    bfree(b, d.adjList);
+    b->adjAlloc = std::max<uint64_t>(adj, b->adjAlloc * 3 / 2);
+    BATCH_TRY(b, balloc(b, &d.adjList, b->adjAlloc));
+  }
+  if (inc > b->incAlloc) {
+    bfree(b, d.incList);
+    b->incAlloc = std::max<uint64_t>(inc, b->incAlloc * 3 / 2);
+    BATCH_TRY(b, balloc(b, &d.incList, b->incAlloc));
+  }
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  b->tableDirty = true;
+  b->configGen++;
+  return AVBD_OK;
+}
+
+// The world table, the queue order (most bodies first) and every world's no-collide triples
+int uploadTable(avbd_batch* b) {
+  const uint32_t nw = uint32_t(b->worlds.size());
+  std::vector<uint32_t> order(nw);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+    const WorldDesc &a = b->worlds[x], &c = b->worlds[y];
+    return uint64_t(a.n) + a.nj > uint64_t(c.n) + c.nj;
+  });
+  if (b->statics.size() > b->staticsAlloc) {
+    bfree(b, b->d.nocollide);
+    b->staticsAlloc = uint32_t(std::max<size_t>(b->statics.size() * 2, 64));
+    BATCH_TRY(b, balloc(b, &b->d.nocollide, b->staticsAlloc));
+  }
+  if (nw) {
+    BATCH_TRY(b, cudaMemcpyAsync(b->dWorlds, b->worlds.data(), nw * sizeof(WorldDesc), cudaMemcpyHostToDevice, b->stream));
+    BATCH_TRY(b, cudaMemcpyAsync(b->dOrder, order.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+  }
+  if (!b->statics.empty())
+    BATCH_TRY(b, cudaMemcpyAsync(b->d.nocollide, b->statics.data(), b->statics.size() * 4, cudaMemcpyHostToDevice, b->stream));
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  b->tableDirty = false;
+  b->configGen++;
+  return AVBD_OK;
+}
+
+// Grows the pair capacity of every world that overflowed or passed 80 % in the last step
+int adaptBatch(avbd_batch* b, bool wait) {
+  if (!b->statusInFlight) return AVBD_OK;
+  if (!wait && cudaEventQuery(b->statusReady) != cudaSuccess) return AVBD_OK;
+  BATCH_TRY(b, cudaEventSynchronize(b->statusReady));
+  b->statusInFlight = false;
+  if (!(b->hStatus[0] & (BATCH_OVERFLOW | BATCH_NEAR_FULL))) return AVBD_OK;
+  const uint32_t nw = uint32_t(b->worlds.size());
+  std::vector<uint32_t> ctr(size_t(nw) * COUNTER_WORDS);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  BATCH_TRY(b, cudaMemcpy(ctr.data(), b->d.counters, ctr.size() * 4, cudaMemcpyDeviceToHost));
+  std::vector<WorldDesc> old = b->worlds;
+  bool any = false;
+  for (uint32_t i = 0; i < nw; i++) {
+    WorldDesc& w = b->worlds[i];
+    const uint32_t* c = ctr.data() + size_t(i) * COUNTER_WORDS;
+    uint32_t demand = c[C_PAIRS];
+    if ((c[C_OVERFLOW] & 1u) || uint64_t(demand) * 10 > uint64_t(w.pairCap) * 8) {
+      uint64_t want = std::min<uint64_t>(std::max<uint64_t>(2ull * demand, uint64_t(w.pairCap) * 5 / 4), 1ull << 24);
+      if (want > w.pairCap) {
+        sizeSlices(w, uint32_t(want));
+        any = true;
+      }
+    }
+  }
+  if (!any) return AVBD_OK;
+  b->relayouts++;
+  return layoutPairs(b, old);
+}
+
+void launchShape(avbd_batch* b) {
+  const int nw = int(std::max<size_t>(b->worlds.size(), 1));
+  int cper = std::max(1, batch_collide_blocks_per_sm(b->collideThreads));
+  b->collideBlocks = std::min(nw, b->sms * cper);
+  if (b->solveBlocks <= 0) b->solveBlocks = b->sms * std::max(1, batch_solve_blocks_per_sm());
+}
+
+BatchLaunch makeLaunch(avbd_batch* b) {
+  BatchLaunch L{};
+  L.base = b->d;
+  L.worlds = b->dWorlds;
+  L.order = b->dOrder;
+  L.nWorlds = uint32_t(b->worlds.size());
+  L.queue = b->dQueue;
+  L.status = b->dStatus;
+  StepParams& p = L.p;
+  const avbd_params& a = b->params;
+  p.dt = a.dt;
+  p.gravity = a.gravity;
+  p.alpha = a.alpha;
+  p.betaLin = a.beta_lin;
+  p.betaAng = a.beta_ang;
+  p.gamma = a.gamma;
+  p.margin = a.contact_margin;
+  p.flags = a.flags;
+  p.iterations = a.iterations;
+  p.upx = a.up[0];
+  p.upy = a.up[1];
+  p.upz = a.up[2];
+  p.step = b->stepCount;
+  p.colorCap = MAX_COLORS;
+  p.cur = b->cur;
+  return L;
+}
+
+cudaError_t enqueueStep(avbd_batch* b, const BatchLaunch& L) {
+  cudaMemsetAsync(b->dQueue, 0, 2 * sizeof(uint32_t), b->stream);
+  cudaMemsetAsync(b->dStatus, 0, 2 * sizeof(uint32_t), b->stream);
+  cudaError_t e = launch_batch_collision(L, b->collideBlocks, b->collideThreads, b->stream);
+  if (e != cudaSuccess) return e;
+  e = launch_batch_solve(L, std::min<int>(b->solveBlocks, int(L.nWorlds)), b->stream);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(b->hStatus, b->dStatus, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+}
+
+int checkWorld(avbd_batch* b, uint32_t world) {
+  if (!b) return AVBD_ERR_INVALID;
+  if (world >= b->worlds.size()) return bfail(b, AVBD_ERR_INVALID, "no world " + std::to_string(world) + " in the batch");
+  return AVBD_OK;
+}
+
+// A new world's slices: bodies and joints appended, pair slices sized from its body count
+int appendWorld(avbd_batch* b, uint32_t n, uint32_t nj, uint32_t pairCap, double threshold, const std::vector<NoCollide>& nocollide,
+                uint32_t flags, uint32_t* index) {
+  WorldDesc w{};
+  w.body = b->n;
+  w.n = n;
+  w.joint = b->nj;
+  w.nj = nj;
+  w.largeThreshold = float(threshold);
+  w.noCollide = uint32_t(b->statics.size());
+  w.nNoCollide = uint32_t(nocollide.size());
+  w.flags = flags;
+  sizeSlices(w, pairCap);
+  std::vector<WorldDesc> old = b->worlds;
+  b->worlds.push_back(w);
+  for (auto& e : nocollide) {
+    b->statics.push_back(e.hi);
+    b->statics.push_back(e.lo);
+    b->statics.push_back(e.slot);
+  }
+  int r = layoutPairs(b, old);
+  if (r) {
+    b->worlds.pop_back();
+    b->statics.resize(w.noCollide);
+    return r;
+  }
+  b->n += n;
+  b->nj += nj;
+  if (index) *index = uint32_t(b->worlds.size() - 1);
+  return AVBD_OK;
+}
+
+void bodiesIn(avbd_batch* b, uint32_t first, const avbd_body* src, uint32_t n, cudaMemcpyKind kind) {
+  float4* fields[10] = {b->d.pos, b->d.rot, b->d.ipos, b->d.irot, b->d.size, b->d.moment, b->d.ypos, b->d.yrot, b->d.vel, b->d.avel};
+  for (int f = 0; f < 10; f++)
+    cudaMemcpy2DAsync(fields[f] + first, sizeof(float4), reinterpret_cast<const char*>(src) + f * sizeof(float4), sizeof(avbd_body), sizeof(float4), n, kind,
+                      b->stream);
+}
+void bodiesOut(avbd_batch* b, uint32_t first, avbd_body* dst, uint32_t n) {
+  float4* fields[10] = {b->d.pos, b->d.rot, b->d.ipos, b->d.irot, b->d.size, b->d.moment, b->d.ypos, b->d.yrot, b->d.vel, b->d.avel};
+  for (int f = 0; f < 10; f++)
+    cudaMemcpy2DAsync(reinterpret_cast<char*>(dst) + f * sizeof(float4), sizeof(avbd_body), fields[f] + first, sizeof(float4), sizeof(float4), n,
+                      cudaMemcpyDeviceToHost, b->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int avbd_batch_create(const avbd_batch_config* cfg, avbd_batch** out) {
+  if (!out || !cfg) return AVBD_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->world_capacity == 0 || cfg->body_capacity == 0) return AVBD_ERR_INVALID;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return AVBD_ERR_NO_DEVICE;
+  if (cfg->device < 0 || cfg->device >= count) return AVBD_ERR_INVALID;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major < 10) return AVBD_ERR_NO_DEVICE;
+  cudaSetDevice(cfg->device);
+  avbd_batch* b = new avbd_batch();
+  b->device = cfg->device;
+  b->sms = prop.multiProcessorCount;
+  b->worldCap = cfg->world_capacity;
+  b->bodyCap = cfg->body_capacity;
+  b->jointCap = std::max<uint32_t>(cfg->joint_capacity, 1);
+  b->pairsPerBody = cfg->pairs_per_body ? cfg->pairs_per_body : 6;
+  b->pairReserve = uint64_t(b->pairsPerBody) * b->bodyCap;
+  avbd_default_params(&b->params);
+  auto bad = [&](int code) {
+    avbd_batch_destroy(b);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(AVBD_ERR_CUDA);
+  DWorld& d = b->d;
+  const size_t B = b->bodyCap, W = b->worldCap;
+  bool ok = true;
+  auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
+  for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel, &d.dlin, &d.dang, &d.aabb}) A(balloc(b, f, B));
+  A(balloc(b, &d.filters, B));
+  A(balloc(b, &d.cell, B));
+  A(balloc(b, &d.colorA, B));
+  A(balloc(b, &d.colorB, B));
+  A(balloc(b, &d.colorBodies, B));
+  A(balloc(b, &d.fixedColor, B));
+  A(balloc(b, &d.incCount, B));
+  A(balloc(b, &d.adjStart, B + W));
+  A(balloc(b, &d.adjFill, B + W));
+  A(balloc(b, &d.incStart, B + W));
+  A(balloc(b, &d.bucket, W * BUCKET_WORDS));
+  A(balloc(b, &d.colorStart, W * (MAX_COLORS + 1)));
+  A(balloc(b, &d.scanScratch, W * 2));
+  A(balloc(b, &d.counters, W * COUNTER_WORDS));
+  A(balloc(b, &d.joint, size_t(b->jointCap) * JOINT_VEC4));
+  A(balloc(b, &d.jinfo, b->jointCap));
+  A(balloc(b, &b->dWorlds, W));
+  A(balloc(b, &b->dOrder, W));
+  A(balloc(b, &b->dQueue, 2));
+  A(balloc(b, &b->dStatus, 2));
+  if (!ok) return bad(AVBD_ERR_CUDA);
+  A(cudaMemsetAsync(d.filters, 0xff, B * sizeof(uint2), b->stream));
+  A(cudaMallocHost(&b->hStatus, 2 * sizeof(uint32_t)));
+  A(cudaEventCreateWithFlags(&b->statusReady, cudaEventDisableTiming));
+  A(cudaStreamSynchronize(b->stream));
+  if (!ok) return bad(AVBD_ERR_CUDA);
+  std::memset(b->hStatus, 0, 2 * sizeof(uint32_t));
+  launchShape(b);
+  *out = b;
+  return AVBD_OK;
+}
+
+int avbd_batch_destroy(avbd_batch* b) {
+  if (!b) return AVBD_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (void* p : b->allocations) cudaFree(p);
+  b->allocations.clear();
+  for (auto& g : b->graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (b->hStatus) cudaFreeHost(b->hStatus);
+  if (b->statusReady) cudaEventDestroy(b->statusReady);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return AVBD_OK;
+}
+
+const char* avbd_batch_last_error(const avbd_batch* b) { return b ? b->error.c_str() : "no batch"; }
+
+int avbd_batch_set_params(avbd_batch* b, const avbd_params* p) {
+  if (!b || !p) return AVBD_ERR_INVALID;
+  if (!(p->dt > 0.0f) || p->iterations < 0 || !std::isfinite(p->gravity)) return bfail(b, AVBD_ERR_INVALID, "dt must be positive, iterations non-negative");
+  b->params = *p;
+  b->configGen++;
+  return AVBD_OK;
+}
+
+int avbd_batch_add_world(avbd_batch* b, const avbd_body* bodies, uint32_t n, const avbd_joint* joints, const avbd_joint_info* info, uint32_t nj,
+                         const uint32_t* ignore_ab, uint32_t n_ignore, uint32_t* index) {
+  if (!b || !bodies || (nj && (!joints || !info)) || (n_ignore && !ignore_ab)) return AVBD_ERR_INVALID;
+  if (n == 0 || n > BATCH_MAX_WORLD_BODIES)
+    return bfail(b, AVBD_ERR_INVALID, "a batched world holds 1 to " + std::to_string(BATCH_MAX_WORLD_BODIES) + " bodies");
+  if (b->worlds.size() >= b->worldCap) return bfail(b, AVBD_ERR_CAPACITY, "world capacity " + std::to_string(b->worldCap) + " reached");
+  if (uint64_t(b->n) + n > b->bodyCap) return bfail(b, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(b->bodyCap) + " reached");
+  if (uint64_t(b->nj) + nj > b->jointCap) return bfail(b, AVBD_ERR_CAPACITY, "joint capacity " + std::to_string(b->jointCap) + " reached");
+  std::string msg = bodyProblem(bodies, n);
+  if (msg.empty()) msg = jointProblem(joints, info, nj, n);
+  for (uint32_t i = 0; i < n_ignore && msg.empty(); i++)
+    if (ignore_ab[2 * i] >= n || ignore_ab[2 * i + 1] >= n || ignore_ab[2 * i] == ignore_ab[2 * i + 1]) msg = "ignore pair out of range";
+  if (!msg.empty()) return bfail(b, AVBD_ERR_INVALID, msg);
+  cudaSetDevice(b->device);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  std::vector<double> radii(n);
+  for (uint32_t i = 0; i < n; i++) radii[i] = bodies[i].radius;
+  std::vector<NoCollide> nocollide;
+  for (uint32_t i = 0; i < nj; i++)
+    if (info[i].a >= 0 && info[i].type != AVBD_T_NONE) {
+      uint32_t a = uint32_t(info[i].a), c = uint32_t(info[i].b);
+      nocollide.push_back({std::max(a, c), std::min(a, c), i});
+    }
+  for (uint32_t i = 0; i < n_ignore; i++)
+    nocollide.push_back({std::max(ignore_ab[2 * i], ignore_ab[2 * i + 1]), std::min(ignore_ab[2 * i], ignore_ab[2 * i + 1]), 0xffffffffu});
+  std::stable_sort(nocollide.begin(), nocollide.end());
+  const uint32_t first = b->n, firstJoint = b->nj;
+  int r = appendWorld(b, n, nj, std::max<uint32_t>(32, b->pairsPerBody * n), largeThreshold(radii), nocollide, 0u, index);
+  if (r) return r;
+  std::vector<avbd_body> copy(bodies, bodies + n);
+  for (auto& x : copy) x.flags = float((uint32_t(x.flags) & 6u) | 1u);  // new slots: no contact history
+  bodiesIn(b, first, copy.data(), n, cudaMemcpyHostToDevice);
+  std::vector<uint32_t> none(n, NO_COLOR);
+  BATCH_TRY(b, cudaMemcpyAsync(b->d.colorA + first, none.data(), size_t(n) * 4, cudaMemcpyHostToDevice, b->stream));
+  if (nj) {
+    BATCH_TRY(b, cudaMemcpyAsync(b->d.joint + size_t(firstJoint) * JOINT_VEC4, joints, size_t(nj) * sizeof(avbd_joint), cudaMemcpyHostToDevice, b->stream));
+    BATCH_TRY(b, cudaMemcpyAsync(b->d.jinfo + firstJoint, info, size_t(nj) * sizeof(int4), cudaMemcpyHostToDevice, b->stream));
+  }
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  return AVBD_OK;
+}
+
+int avbd_batch_add_world_from(avbd_batch* b, avbd_world* src, uint32_t* index) {
+  if (!b || !src) return AVBD_ERR_INVALID;
+  if (src->device != b->device) return bfail(b, AVBD_ERR_INVALID, "the world is on another device");
+  const uint32_t n = src->n, nj = src->nj;
+  if (n == 0 || n > BATCH_MAX_WORLD_BODIES)
+    return bfail(b, AVBD_ERR_INVALID, "a batched world holds 1 to " + std::to_string(BATCH_MAX_WORLD_BODIES) + " bodies");
+  if (b->worlds.size() >= b->worldCap) return bfail(b, AVBD_ERR_CAPACITY, "world capacity " + std::to_string(b->worldCap) + " reached");
+  if (uint64_t(b->n) + n > b->bodyCap) return bfail(b, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(b->bodyCap) + " reached");
+  if (uint64_t(b->nj) + nj > b->jointCap) return bfail(b, AVBD_ERR_CAPACITY, "joint capacity " + std::to_string(b->jointCap) + " reached");
+  cudaSetDevice(b->device);
+  if (avbd_synchronize(src) != AVBD_OK) return bfail(b, AVBD_ERR_CUDA, std::string("source world: ") + src->error);
+  if (src->staticsDirty && uploadStatics(src) != AVBD_OK) return bfail(b, AVBD_ERR_CUDA, std::string("source world: ") + src->error);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  // last step's contact pairs (the buffer the next step reads)
+  std::vector<uint32_t> ctr(COUNTER_WORDS);
+  BATCH_TRY(b, cudaMemcpy(ctr.data(), src->d.counters, COUNTER_WORDS * 4, cudaMemcpyDeviceToHost));
+  const uint32_t prevPairs = std::min(ctr[C_PAIRS], src->pairCap);
+  const uint32_t first = b->n, firstJoint = b->nj;
+  uint32_t pairCap = std::max<uint32_t>(std::max<uint32_t>(32, b->pairsPerBody * n), 2 * prevPairs);
+  int r = appendWorld(b, n, nj, pairCap, src->threshold, src->nocollide, src->fixedColors ? WORLD_FIXED_COLORS : 0u, index);
+  if (r) return r;
+  const WorldDesc& w = b->worlds.back();
+  const DWorld& s = src->d;
+  DWorld& d = b->d;
+  const float4* sf[10] = {s.pos, s.rot, s.ipos, s.irot, s.size, s.moment, s.ypos, s.yrot, s.vel, s.avel};
+  float4* df[10] = {d.pos, d.rot, d.ipos, d.irot, d.size, d.moment, d.ypos, d.yrot, d.vel, d.avel};
+  const cudaMemcpyKind DD = cudaMemcpyDeviceToDevice;
+  for (int f = 0; f < 10; f++) BATCH_TRY(b, cudaMemcpyAsync(df[f] + first, sf[f], size_t(n) * sizeof(float4), DD, b->stream));
+  BATCH_TRY(b, cudaMemcpyAsync(d.filters + first, s.filters, size_t(n) * sizeof(uint2), DD, b->stream));
+  BATCH_TRY(b, cudaMemcpyAsync(d.colorA + first, s.colorA, size_t(n) * 4, DD, b->stream));
+  BATCH_TRY(b, cudaMemcpyAsync(d.fixedColor + first, s.fixedColor, size_t(n) * 4, DD, b->stream));
+  if (nj) {
+    BATCH_TRY(b, cudaMemcpyAsync(d.joint + size_t(firstJoint) * JOINT_VEC4, s.joint, size_t(nj) * JOINT_VEC4 * sizeof(float4), DD, b->stream));
+    BATCH_TRY(b, cudaMemcpyAsync(d.jinfo + firstJoint, s.jinfo, size_t(nj) * sizeof(int4), DD, b->stream));
+  }
+  const size_t wi = b->worlds.size() - 1;
+  BATCH_TRY(b, cudaMemcpyAsync(d.counters + wi * COUNTER_WORDS, s.counters, COUNTER_WORDS * 4, DD, b->stream));
+  const int sp = 1 - src->cur, bp = 1 - b->cur;
+  if (prevPairs) {
+    BATCH_TRY(b, cudaMemcpyAsync(d.mIds[bp] + w.pair, s.mIds[sp], size_t(prevPairs) * sizeof(uint4), DD, b->stream));
+    BATCH_TRY(b, cudaMemcpyAsync(d.mGeo[bp] + w.pair, s.mGeo[sp], size_t(prevPairs) * sizeof(float4), DD, b->stream));
+    BATCH_TRY(b, cudaMemcpyAsync(d.cPt[bp] + size_t(w.pair) * MAX_CONTACTS * 4, s.cPt[sp], size_t(prevPairs) * MAX_CONTACTS * 4 * sizeof(float4), DD,
+                                 b->stream));
+  }
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  return AVBD_OK;
+}
+
+int avbd_batch_world_info(avbd_batch* b, uint32_t world, avbd_batch_world* out) {
+  int r = checkWorld(b, world);
+  if (r) return r;
+  if (!out) return AVBD_ERR_INVALID;
+  const WorldDesc& w = b->worlds[world];
+  out->first_body = w.body;
+  out->bodies = w.n;
+  out->first_joint = w.joint;
+  out->joints = w.nj;
+  out->pair_capacity = w.pairCap;
+  out->fixed_colors = (w.flags & WORLD_FIXED_COLORS) ? 1u : 0u;
+  return AVBD_OK;
+}
+
+int avbd_batch_step(avbd_batch* b, int steps) {
+  if (!b || steps < 0) return AVBD_ERR_INVALID;
+  if (b->worlds.empty()) return bfail(b, AVBD_ERR_INVALID, "the batch has no worlds");
+  cudaSetDevice(b->device);
+  for (int s = 0; s < steps; s++) {
+    int r = adaptBatch(b, false);
+    if (r) return r;
+    if (b->tableDirty) {
+      r = uploadTable(b);
+      if (r) return r;
+      launchShape(b);
+    }
+    b->stepCount++;
+    BatchLaunch L = makeLaunch(b);
+    bool launched = false;
+    if (b->useGraphs) {
+      const int c = b->cur;
+      if (!b->graph[c] || b->graphGen[c] != b->configGen) {
+        if (b->graph[c]) cudaGraphExecDestroy(b->graph[c]);
+        b->graph[c] = nullptr;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          cudaError_t le = enqueueStep(b, L);
+          e = cudaStreamEndCapture(b->stream, &g);
+          if (e == cudaSuccess && le == cudaSuccess) e = cudaGraphInstantiate(&b->graph[c], g, 0);
+          else if (e == cudaSuccess) e = le;
+          if (g) cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          b->useGraphs = false;
+          if (b->graph[c]) cudaGraphExecDestroy(b->graph[c]);
+          b->graph[c] = nullptr;
+        } else {
+          b->graphGen[c] = b->configGen;
+        }
+      }
+      if (b->graph[c]) {
+        BATCH_TRY(b, cudaGraphLaunch(b->graph[c], b->stream));
+        launched = true;
+      }
+    }
+    if (!launched) BATCH_TRY(b, enqueueStep(b, L));
+    BATCH_TRY(b, cudaEventRecord(b->statusReady, b->stream));
+    b->statusInFlight = true;
+    b->cur = 1 - b->cur;
+  }
+  return AVBD_OK;
+}
+
+int avbd_batch_synchronize(avbd_batch* b) {
+  if (!b) return AVBD_ERR_INVALID;
+  cudaSetDevice(b->device);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  if (b->statusInFlight && b->hStatus[1]) {
+    uint32_t bits = b->hStatus[1];
+    int r = adaptBatch(b, true);
+    if (r) return r;
+    return bfail(b, AVBD_ERR_TIMEOUT, "a world's step gave up: error bits " + std::to_string(bits));
+  }
+  return adaptBatch(b, true);
+}
+
+int avbd_batch_read_bodies(avbd_batch* b, uint32_t world, avbd_body* dst, uint32_t cap, uint32_t* n) {
+  int r = checkWorld(b, world);
+  if (r) return r;
+  const WorldDesc& w = b->worlds[world];
+  if (n) *n = w.n;
+  if (!dst) return AVBD_OK;
+  if (cap < w.n) return bfail(b, AVBD_ERR_CAPACITY, "destination holds fewer bodies than the world");
+  cudaSetDevice(b->device);
+  bodiesOut(b, w.body, dst, w.n);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  return AVBD_OK;
+}
+
+int avbd_batch_read_all_bodies_async(avbd_batch* b, avbd_body* dst, uint32_t cap) {
+  if (!b || !dst) return AVBD_ERR_INVALID;
+  if (cap < b->n) return bfail(b, AVBD_ERR_CAPACITY, "destination holds fewer bodies than the batch");
+  cudaSetDevice(b->device);
+  bodiesOut(b, 0, dst, b->n);
+  BATCH_TRY(b, cudaGetLastError());
+  return AVBD_OK;
+}
+
+int avbd_batch_write_all_bodies_async(avbd_batch* b, const avbd_body* src, uint32_t n) {
+  if (!b || !src) return AVBD_ERR_INVALID;
+  if (n != b->n) return bfail(b, AVBD_ERR_INVALID, "one record per body of the batch is needed");
+  cudaSetDevice(b->device);
+  bodiesIn(b, 0, src, n, cudaMemcpyHostToDevice);
+  BATCH_TRY(b, cudaGetLastError());
+  return AVBD_OK;
+}
+
+int avbd_batch_read_joints(avbd_batch* b, uint32_t world, avbd_joint* dst, avbd_joint_info* info, uint32_t cap, uint32_t* n) {
+  int r = checkWorld(b, world);
+  if (r) return r;
+  const WorldDesc& w = b->worlds[world];
+  if (n) *n = w.nj;
+  if (!dst && !info) return AVBD_OK;
+  if (cap < w.nj) return bfail(b, AVBD_ERR_CAPACITY, "destination holds fewer joints than the world");
+  cudaSetDevice(b->device);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  if (dst && w.nj)
+    BATCH_TRY(b, cudaMemcpy(dst, b->d.joint + size_t(w.joint) * JOINT_VEC4, size_t(w.nj) * sizeof(avbd_joint), cudaMemcpyDeviceToHost));
+  if (info && w.nj) BATCH_TRY(b, cudaMemcpy(info, b->d.jinfo + w.joint, size_t(w.nj) * sizeof(avbd_joint_info), cudaMemcpyDeviceToHost));
+  return AVBD_OK;
+}
+
+int avbd_batch_read_colors(avbd_batch* b, uint32_t world, uint32_t* dst, uint32_t cap, uint32_t* n) {
+  int r = checkWorld(b, world);
+  if (r) return r;
+  const WorldDesc& w = b->worlds[world];
+  if (n) *n = w.n;
+  if (!dst) return AVBD_OK;
+  if (cap < w.n) return bfail(b, AVBD_ERR_CAPACITY, "destination holds fewer entries than the world's bodies");
+  cudaSetDevice(b->device);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  BATCH_TRY(b, cudaMemcpy(dst, b->d.colorA + w.body, size_t(w.n) * 4, cudaMemcpyDeviceToHost));
+  return AVBD_OK;
+}
+
+int avbd_batch_read_counters(avbd_batch* b, uint32_t world, avbd_counters* out) {
+  int r = checkWorld(b, world);
+  if (r) return r;
+  if (!out) return AVBD_ERR_INVALID;
+  cudaSetDevice(b->device);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  uint32_t c[COUNTER_WORDS];
+  BATCH_TRY(b, cudaMemcpy(c, b->d.counters + size_t(world) * COUNTER_WORDS, sizeof(c), cudaMemcpyDeviceToHost));
+  std::memset(out, 0, sizeof(*out));
+  out->pairs = c[C_PAIRS];
+  out->contacts = c[C_CONTACTS];
+  out->manifolds = c[C_MANIFOLDS];
+  out->overflow = c[C_OVERFLOW];
+  out->clashes = c[C_CLASHES];
+  out->colors = c[C_COLORS];
+  out->rounds = c[C_ROUNDS];
+  out->error = c[C_ERROR];
+  out->steps = c[C_STEP];
+  out->pair_capacity = b->worlds[world].pairCap;
+  out->graphs = (b->useGraphs && b->graph[0] != nullptr) || (b->useGraphs && b->graph[1] != nullptr) ? 1u : 0u;
+  out->launches = 2;
+  return AVBD_OK;
+}
+
+int avbd_batch_use_graphs(avbd_batch* b, int enable) {
+  if (!b) return AVBD_ERR_INVALID;
+  b->useGraphs = enable != 0;
+  b->configGen++;
+  return AVBD_OK;
+}
+
+int avbd_batch_stream(avbd_batch* b, void** stream) {
+  if (!b || !stream) return AVBD_ERR_INVALID;
+  *stream = b->stream;
+  return AVBD_OK;
+}
+
+int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
+  if (!b || steps <= 0) return AVBD_ERR_INVALID;
+  if (b->worlds.empty()) return bfail(b, AVBD_ERR_INVALID, "the batch has no worlds");
+  cudaSetDevice(b->device);
+  int r = avbd_batch_synchronize(b);
+  if (r) return r;
+  const int threads[3] = {64, 128, 256};
+  const int solvePer = std::max(1, batch_solve_blocks_per_sm());
+  avbd_batch_tuning t{};
+  cudaEvent_t e0, e1;
+  BATCH_TRY(b, cudaEventCreate(&e0));
+  BATCH_TRY(b, cudaEventCreate(&e1));
+  float best = INFINITY;
+  int bestT = b->collideThreads, bestS = b->solveBlocks;
+  const bool graphs = b->useGraphs;
+  b->useGraphs = false;
+  uint32_t k = 0;
+  for (int ti = 0; ti < 3; ti++)
+    for (int sp = 1; sp <= solvePer && k < AVBD_BATCH_TUNE_CANDIDATES; sp++) {
+      b->collideThreads = threads[ti];
+      b->solveBlocks = b->sms * sp;
+      launchShape(b);
+      r = avbd_batch_step(b, 1);  // settle storage for this shape
+      if (!r) r = avbd_batch_synchronize(b);
+      if (r) break;
+      cudaEventRecord(e0, b->stream);
+      r = avbd_batch_step(b, steps);
+      cudaEventRecord(e1, b->stream);
+      if (!r) r = avbd_batch_synchronize(b);
+      if (r) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= float(steps);
+      t.candidate_threads[k] = uint32_t(threads[ti]);
+      t.candidate_solve_blocks[k] = uint32_t(b->solveBlocks);
+      t.candidate_ms[k] = ms;
+      k++;
+      if (ms < best) {
+        best = ms;
+        bestT = threads[ti];
+        bestS = b->solveBlocks;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->useGraphs = graphs;
+  b->collideThreads = bestT;
+  b->solveBlocks = bestS;
+  launchShape(b);
+  b->configGen++;
+  if (r) return r;
+  t.candidates = k;
+  t.collide_threads = uint32_t(bestT);
+  t.solve_blocks = uint32_t(bestS);
+  t.ms_per_step = best;
+  t.steps_taken = k * uint32_t(steps + 1);
+  if (out) *out = t;
+  return AVBD_OK;
+}
+
+int avbd_batch_info(avbd_batch* b, avbd_batch_status* out) {
+  if (!b || !out) return AVBD_ERR_INVALID;
+  out->worlds = uint32_t(b->worlds.size());
+  out->bodies = b->n;
+  out->joints = b->nj;
+  out->steps = b->stepCount;
+  out->pair_slots = b->pairUsed;
+  out->relayouts = b->relayouts;
+  out->collide_threads = uint32_t(b->collideThreads);
+  out->collide_blocks = uint32_t(b->collideBlocks);
+  out->solve_blocks = uint32_t(b->solveBlocks);
+  out->graphs = b->useGraphs ? 1u : 0u;
+  return AVBD_OK;
+}
+
+}  // extern "C"

@@ -22,11 +22,21 @@ __device__ inline bool enabled(const DWorld& w, uint32_t i) {
   return (f & 2u) == 0u;
 }
 
+__device__ inline float3 aabbOf(const DWorld& w, uint32_t i);
+
 // --- begin: rotate counters (wgsl-collision.ts:96-107) -------------------------------------------
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 __global__ void k_begin(DWorld w, StepParams p) {
+  w.clocks[CLOCK_T0] = gtimer();
   uint32_t* c = w.counters;
   uint32_t pairs = c[C_PAIRS];
   c[C_PREV_PAIRS] = pairs < p.pairCap ? pairs : p.pairCap;
+  c[C_STEP] += 1;  // steps since the world was made (the manifold's generation word)
   c[C_PAIRS] = 0;
   c[C_CONTACTS] = 0;
   c[C_MANIFOLDS] = 0;
@@ -181,6 +191,8 @@ __global__ void k_bucket_scatter(DWorld w, uint32_t n, uint32_t sentinel) {
   w.sortedPR[slot] = make_float4(pi.x, pi.y, pi.z, w.moment[i].w);
   int4 c = w.cell[i];
   w.sortedCell[slot] = make_int4(c.x, c.y, c.z, (int)(i | (w.size[i].w > 0.0f ? 0x80000000u : 0u)));
+  float3 a = aabbOf(w, i);
+  w.sortedAabb[slot] = make_float4(a.x, a.y, a.z, 0.0f);
 }
 
 // --- pair tests (wgsl-collision.ts:150-234) ------------------------------------------------------------
@@ -217,6 +229,8 @@ __device__ inline bool faceSeparated(const Shape& A, const Shape& B, float3 d) {
   }
   return false;
 }
+
+__device__ inline float3 aabbOf(const DWorld& w, uint32_t i) { return aabbHalf(shapeOf(w, i)); }
 
 struct Probe {
   uint32_t index;
@@ -346,6 +360,8 @@ __global__ void __launch_bounds__(128) k_find_pairs(DWorld w, StepParams p) {
         float3 d = P.pos - make_float3(pr.x, pr.y, pr.z);
         float r = P.radius + pr.w;
         if (dot3(d, d) > r * r) continue;  // the sphere test, the same in both views
+        float4 ab = w.sortedAabb[k];         // and the AABB test (its sums commute)
+        if (fabsf(d.x) > P.aabb.x + ab.x + 1e-4f || fabsf(d.y) > P.aabb.y + ab.y + 1e-4f || fabsf(d.z) > P.aabb.z + ab.z + 1e-4f) continue;
         testFromProber(w, p, P, j);
       }
     }
@@ -623,11 +639,9 @@ __device__ bool sphereBox(const Box& S, const Box& X, float4 qX, float3& onSpher
 
 // Contact pair p: manifold slot p with its points at 8p .. 8p+count-1, warm-started from last step's
 // pair (a, b) by feature key (wgsl-collision.ts:767-892).
-__global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
+__device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
   const int cur = p.cur, prev = 1 - cur;
-  uint32_t total = w.counters[C_PAIRS];
-  if (total > p.pairCap) total = p.pairCap;
-  for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < total; pi += gridDim.x * blockDim.x) {
+  {
     uint2 pr = w.pairs[pi];
     uint32_t a = pr.x, b = pr.y;
     Box A = makeBox(w, a), B = makeBox(w, b);
@@ -657,7 +671,7 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
     uint32_t count = found.count;
     float3 n = -sat.n;
     float fa = w.pos[a].w, fb = w.pos[b].w;
-    w.mIds[cur][pi] = make_uint4(a, b, pi * MAX_CONTACTS, count | (p.step << 4));
+    w.mIds[cur][pi] = make_uint4(a, b, pi * MAX_CONTACTS, count | (w.counters[C_STEP] << 4));
     w.mGeo[cur][pi] = make_float4(n.x, n.y, n.z, sqrtf(fa * fb));
     {
       cg::coalesced_group g = cg::coalesced_threads();
@@ -668,7 +682,7 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
         atomicAdd(&w.counters[C_MANIFOLDS], nonEmpty);
       }
     }
-    if (count == 0u) continue;
+    if (count == 0u) return;
     float3 t1, t2;
     orthonormal(n, t1, t2);
     bool anySphere = sphereA || sphereB;
@@ -737,6 +751,121 @@ __global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
     }
   }
 }
+
+__global__ void __launch_bounds__(128) k_narrowphase(DWorld w, StepParams p) {
+  uint32_t total = w.counters[C_PAIRS];
+  if (total > p.pairCap) total = p.pairCap;
+  for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < total; pi += gridDim.x * blockDim.x) narrowPair(w, p, pi);
+}
+
+// --- batched worlds: one block per world ------------------------------------------------------------------
+// A world of a batch holds at most a few hundred bodies: its pairs are found by testing every pair
+// of bodies against the broadphase rule (the same set the grid walk finds), then collided.
+__global__ void __launch_bounds__(256) k_batch_collide(BatchLaunch B) {
+  __shared__ uint32_t s_world;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_world = atomicAdd(&B.queue[0], 1u);
+    __syncthreads();
+    const uint32_t qi = s_world;
+    if (qi >= B.nWorlds) return;
+    const uint32_t wi = B.order[qi];
+    const WorldDesc d = B.worlds[wi];
+    const DWorld w = worldView(B.base, d, wi);
+    const StepParams p = worldParams(B.p, d);
+    uint32_t* c = w.counters;
+    const uint32_t prevPairs = min(c[C_PAIRS], d.pairCap);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      c[C_PREV_PAIRS] = prevPairs;
+      c[C_STEP] += 1;
+      c[C_PAIRS] = 0;
+      c[C_CONTACTS] = 0;
+      c[C_MANIFOLDS] = 0;
+      c[C_OVERFLOW] = 0;
+      c[C_CLASHES] = 0;
+      c[C_COLORS] = 0;
+      c[C_ROUNDS] = 0;
+      c[C_ERROR] = 0;
+      for (int k = 0; k < 2 * MAX_ROUND_PAIRS + 2; k++) c[C_PENDING + k] = 0;
+    }
+    for (uint32_t h = threadIdx.x; h <= d.hashMask; h += blockDim.x) w.hash[h] = 0u;
+    __syncthreads();
+    const int prev = 1 - p.cur;
+    for (uint32_t m = threadIdx.x; m < prevPairs; m += blockDim.x) {  // hashInsert, per world
+      uint4 ids = w.mIds[prev][m];
+      if ((ids.w & 15u) == 0u) continue;
+      if (w.ipos[ids.x].w != 0.0f || w.ipos[ids.y].w != 0.0f) continue;
+      uint32_t h = pairHash(ids.x, ids.y) & d.hashMask;
+      for (uint32_t probe = 0; probe <= d.hashMask; probe++) {
+        if (atomicCAS(&w.hash[h], 0u, m + 1u) == 0u) break;
+        h = (h + 1u) & d.hashMask;
+      }
+    }
+    __syncthreads();
+    // every pair (i > j): triangular index k -> (i, j)
+    const uint32_t n = d.n;
+    const uint32_t total = n * (n - 1u) / 2u;
+    for (uint32_t k = threadIdx.x; k < total; k += blockDim.x) {
+      uint32_t i = (uint32_t)((1.0f + sqrtf(1.0f + 8.0f * (float)k)) * 0.5f);
+      while (i * (i - 1u) / 2u > k) i--;
+      while ((i + 1u) * i / 2u <= k) i++;
+      uint32_t j = k - i * (i - 1u) / 2u;
+      if (!enabled(w, i) || !enabled(w, j)) continue;
+      bool di = w.size[i].w > 0.0f, dj = w.size[j].w > 0.0f;
+      if (!di && !dj) continue;
+      float4 pi4 = w.pos[i], pj4 = w.pos[j];
+      float3 dd = make_float3(pi4.x - pj4.x, pi4.y - pj4.y, pi4.z - pj4.z);
+      float r = w.moment[i].w + w.moment[j].w;
+      if (dot3(dd, dd) > r * r) continue;  // the sphere test: the same from either body's view
+      uint32_t pr = proberOf(w, p, i, j);
+      testPair(w, p, probeOf(w, pr), pr == i ? j : i);
+    }
+    __syncthreads();
+    const uint32_t found = c[C_PAIRS];
+    const uint32_t pairs = min(found, d.pairCap);
+    for (uint32_t pi = threadIdx.x; pi < pairs; pi += blockDim.x) narrowPair(w, p, pi);
+    if (threadIdx.x == 0) {
+      uint32_t bits = (c[C_OVERFLOW] & 1u) ? BATCH_OVERFLOW : 0u;
+      if (uint64_t(found) * 10u > uint64_t(d.pairCap) * 8u) bits |= BATCH_NEAR_FULL;
+      if (bits) atomicOr(&B.status[0], bits);
+    }
+  }
+}
+
+int batch_collide_blocks_per_sm(int threads) {
+  int perSm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_collide, threads, 0);
+  return perSm;
+}
+
+cudaError_t launch_batch_collision(const BatchLaunch& b, int blocks, int threads, cudaStream_t s) {
+  k_batch_collide<<<blocks, threads, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+// The step's statistics into the ring: phase times from the device clocks, then the counters
+__global__ void k_step_stats(DWorld w, uint32_t launches) {
+  if (threadIdx.x != 0 || !w.statsRing || !w.statsCap) return;
+  const uint32_t* c = w.counters;
+  uint32_t slot = c[C_STATS_NEXT] % w.statsCap;
+  uint32_t* o = w.statsRing + size_t(slot) * STAT_WORDS;
+  unsigned long long n = w.clocks[0], t0 = w.clocks[CLOCK_T0], t1 = w.clocks[1], t2 = n ? w.clocks[n] : t1;
+  o[0] = (uint32_t)(t1 - t0);
+  o[1] = (uint32_t)(t2 - t1);
+  o[2] = c[C_PAIRS];
+  o[3] = c[C_CONTACTS];
+  o[4] = c[C_MANIFOLDS];
+  o[5] = c[C_ADJ];
+  o[6] = c[C_INC];
+  o[7] = c[C_DYN];
+  o[8] = c[C_COLORS];
+  o[9] = c[C_ROUNDS];
+  o[10] = launches;
+  o[11] = c[C_ERROR];
+  w.counters[C_STATS_NEXT] = c[C_STATS_NEXT] + 1;
+}
+void launch_step_stats(const DWorld& w, uint32_t launches, cudaStream_t s) { k_step_stats<<<1, 32, 0, s>>>(w, launches); }
 
 // Host: the collision phase, enqueued on `s`. Returns the number of kernels it launched.
 uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s) {

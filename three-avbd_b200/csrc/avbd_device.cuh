@@ -37,11 +37,14 @@ enum : int { K_RA = 0, K_RB = 1, K_PEN = 2, K_LAM = 3 };
 // Counter words (device memory)
 enum : int {
   C_PAIRS = 0, C_CONTACTS = 1, C_MANIFOLDS = 2, C_OVERFLOW = 3, C_CLASHES = 4, C_COLORS = 5, C_ROUNDS = 6, C_ERROR = 7,
-  C_PREV_PAIRS = 8, C_ADJ = 9, C_INC = 10, C_DYN = 11, C_PENDING = 16,  // 16..16+2*MAX_ROUND_PAIRS: pending counts per round pair
+  C_PREV_PAIRS = 8, C_ADJ = 9, C_INC = 10, C_DYN = 11, C_STEP = 12, C_PENDING = 16,  // 16..16+2*MAX_ROUND_PAIRS: pending counts per round pair
   COUNTER_WORDS = 128,
 };
 constexpr int MAX_ROUND_PAIRS = 32;
 constexpr int MAX_CLOCKS = 1023;  // barrier timestamps kept per step
+constexpr int CLOCK_T0 = MAX_CLOCKS + 1, CLOCK_WORDS = MAX_CLOCKS + 2;
+constexpr int STAT_WORDS = 16;    // collision ns, solve ns, then counters (pairs, contacts, manifolds, adjacency, incidences, dynamic, colours, rounds, launches, error)
+constexpr int C_STATS_NEXT = 13;  // counter word: next ring entry
 // Error bits
 constexpr uint32_t ERR_BARRIER_TIMEOUT = 1, ERR_ADJ_OVERFLOW = 2, ERR_INC_OVERFLOW = 4;
 
@@ -79,6 +82,8 @@ struct DWorld {
   uint32_t *cellStart, *cellEnd;
   float4* sortedPR;  // per sorted slot: position, bounding radius
   int4* sortedCell;  // per sorted slot: cell x, y, z, body index | dynamic << 31
+  float4* aabb;      // per body: world AABB half extents (this step), then per sorted slot (sortedAabb)
+  float4* sortedAabb;
   uint2* pairs;
   // contact pairs and points, double-buffered (cur: this step, 1 - cur: last step)
   uint4* mIds[2];   // a, b, first (= 8 * slot), count | step << 4
@@ -97,8 +102,74 @@ struct DWorld {
   // bookkeeping
   uint32_t* counters;
   uint32_t* barrier;  // [0] arrive count, [1] generation
-  unsigned long long* clocks;  // device time (ns) at each grid barrier of the last step, [0] = count
+  unsigned long long* clocks;  // [0] count, [1..] device time (ns) at each grid barrier of the last step's solve, [CLOCK_T0] collision start
+  uint32_t* statsRing;          // per-step statistics ring (STAT_WORDS a step), or null
+  uint32_t statsCap;
 };
+
+// One world of a batch: where its slices start in the batch's concatenated arrays, and its sizes
+struct WorldDesc {
+  uint32_t body, n, joint, nj;          // bodies (the world's local indices start at `body`), joints
+  uint32_t pair, pairCap, hash, hashMask;
+  uint32_t adj, adjCap, inc, incCap;
+  float largeThreshold;                 // the world's broadphase classification (radii.ts)
+  uint32_t nNoCollide, noCollide;       // nNoCollide (hi, lo, slot) triples from word noCollide, world-local indices
+  uint32_t flags;                       // WORLD_FIXED_COLORS
+};
+constexpr uint32_t WORLD_FIXED_COLORS = 1u;
+
+// The view of world `wi` of a batch: every pointer moved to the world's slice
+__host__ __device__ inline DWorld worldView(const DWorld& b, const WorldDesc& d, uint32_t wi) {
+  DWorld v = b;
+  float4** bodyArrays[] = {&v.pos, &v.rot, &v.ipos, &v.irot, &v.size, &v.moment, &v.ypos, &v.yrot, &v.vel, &v.avel, &v.dlin, &v.dang, &v.aabb};
+  for (float4** a : bodyArrays) *a += d.body;
+  v.filters += d.body;
+  v.cell += d.body;
+  v.joint += size_t(d.joint) * JOINT_VEC4;
+  v.jinfo += d.joint;
+  v.nocollide = b.nocollide + d.noCollide;
+  v.pairs += d.pair;
+  for (int k = 0; k < 2; k++) {
+    v.mIds[k] += d.pair;
+    v.mGeo[k] += d.pair;
+    v.cPt[k] += size_t(d.pair) * MAX_CONTACTS * 4;
+  }
+  v.hash += d.hash;
+  v.adjStart += d.body + wi;
+  v.adjFill += d.body + wi;
+  v.adjList += d.adj;
+  v.colorA += d.body;
+  v.colorB += d.body;
+  v.colorBodies += d.body;
+  v.fixedColor += d.body;
+  v.incCount += d.body;
+  v.incStart += d.body + wi;
+  v.incList += d.inc;
+  v.bucket += size_t(wi) * BUCKET_WORDS;
+  v.colorStart += size_t(wi) * (MAX_COLORS + 1);
+  v.scanScratch += size_t(wi) * 2;
+  v.counters += size_t(wi) * COUNTER_WORDS;
+  v.clocks = nullptr;
+  v.statsRing = nullptr;
+  v.statsCap = 0;
+  return v;
+}
+
+// The step parameters of one world of a batch: the batch's shared ones with the world's sizes
+__host__ __device__ inline StepParams worldParams(const StepParams& shared, const WorldDesc& d) {
+  StepParams p = shared;
+  p.n = d.n;
+  p.nj = d.nj;
+  p.pairCap = d.pairCap;
+  p.hashMask = d.hashMask;
+  p.incCap = d.incCap;
+  p.adjCap = d.adjCap;
+  p.largeThreshold = d.largeThreshold;
+  p.nLarge = 0;
+  p.nNoCollide = d.nNoCollide;
+  p.fixedColors = (d.flags & WORLD_FIXED_COLORS) ? 1u : 0u;
+  return p;
+}
 
 // --- vector / quaternion helpers (operation order of the reference's WGSL, wgsl layout.ts:307-340) ---
 __host__ __device__ inline float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
@@ -161,6 +232,25 @@ inline uint32_t grid_for(uint32_t n, uint32_t block) { return (n + block - 1) / 
 
 // Host launchers (avbd_collide.cu)
 uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s);
+void launch_step_stats(const DWorld& w, uint32_t launches, cudaStream_t s);
+// Batched worlds: one block per world over a queue of world indices (largest first)
+struct BatchLaunch {
+  DWorld base;
+  const WorldDesc* worlds;
+  const uint32_t* order;  // world indices, largest first
+  uint32_t nWorlds;
+  uint32_t* queue;        // [0] collision queue, [1] solve queue (zeroed before the launches)
+  uint32_t* status;       // [0] storage bits (BATCH_*), [1] error bits of any world
+  StepParams p;           // shared parameters; per-world sizes come from the WorldDesc
+};
+constexpr uint32_t BATCH_OVERFLOW = 1u, BATCH_NEAR_FULL = 2u;
+cudaError_t launch_batch_collision(const BatchLaunch& b, int blocks, int threads, cudaStream_t s);
+cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, cudaStream_t s);
+int batch_collide_blocks_per_sm(int threads);
+int batch_solve_blocks_per_sm();
+constexpr int BATCH_SOLVE_THREADS = 256;  // the solve's block size (its shared tables assume it)
+constexpr uint32_t BATCH_MAX_WORLD_BODIES = 4096;
+
 // Host launchers (avbd_solve.cu)
 int solve_grid_blocks(int device);
 cudaError_t launch_topology_solve(const DWorld& w, const StepParams& p, int blocks, cudaStream_t s);

@@ -10,12 +10,11 @@
 #include <string>
 #include <vector>
 
-#include "../../include/avbd.h"
-#include "avbd_device.cuh"
+#include "avbd_host.hpp"
 
 using namespace avbd;
 
-namespace {
+namespace avbd {
 
 uint32_t pow2AtLeast(uint64_t n) {
   uint64_t p = 2;
@@ -53,46 +52,42 @@ double largestSmall(std::vector<double> radii) {
   return maxSmall;
 }
 
-struct NoCollide {
-  uint32_t hi, lo, slot;
-  bool operator<(const NoCollide& o) const { return hi < o.hi || (hi == o.hi && lo < o.lo); }
-};
 
-}  // namespace
+// Bodies above this bounding radius are "large" (tested against every body): halfway between the
+// largest small radius and the smallest large one (solver.ts uploadStatics, radii.ts)
+double largeThreshold(const std::vector<double>& radii) {
+  double maxSmall = largestSmall(radii);
+  double minLarge = INFINITY;
+  for (double r : radii)
+    if (r > maxSmall) minLarge = std::min(minLarge, r);
+  return std::isinf(minLarge) ? maxSmall * 1.5 : (maxSmall + minLarge) / 2;
+}
 
-struct avbd_world {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string error;
-  avbd_params params{};
-  uint32_t bodyCap = 0, n = 0, jointCap = 0, nj = 0, pairCap = 0, tableSize = 0, hashSize = 0, incCap = 0, adjCap = 0;
-  uint32_t sortTiles = 0;
-  DWorld d{};
-  int solveBlocks = 0;
-  int cur = 0;
-  uint32_t stepCount = 0;
-  bool fixedColors = false;
-  // host mirrors
-  std::vector<float> radius;
-  std::vector<char> dynamic;
-  std::vector<avbd_joint_info> info;
-  std::vector<NoCollide> nocollide;
-  bool staticsDirty = true;
-  float threshold = 0.0f, cellSize = 1.0f;
-  uint32_t nLarge = 0, nNoCollide = 0, anyDynamicLarge = 0;
-  uint32_t staticsWords = 0;
-  // counters of the last step, copied back asynchronously
-  uint32_t* hCounters = nullptr;
-  cudaEvent_t countersReady = nullptr;
-  bool countersInFlight = false;
-  // per-step statistics ring: 3 events and a counter snapshot per entry
-  uint32_t statsCap = 0, statsCount = 0;
-  std::vector<cudaEvent_t> statsEvents;
-  uint32_t* statsCounters = nullptr;  // device, statsCap * COUNTER_WORDS
-  std::vector<uint32_t> statsLaunches;
-  uint32_t launchesPerStep = 0;
-  std::vector<void*> allocations;
-};
+std::string bodyProblem(const avbd_body* b, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) {
+    const float* f = reinterpret_cast<const float*>(b + i);
+    for (int k = 0; k < 40; k++)
+      if (!std::isfinite(f[k])) return "body " + std::to_string(i) + ": non-finite value";
+    if (b[i].mass < 0.0f || b[i].radius < 0.0f) return "body " + std::to_string(i) + ": negative mass or radius";
+  }
+  return {};
+}
+
+std::string jointProblem(const avbd_joint* j, const avbd_joint_info* info, uint32_t n, uint32_t bodies) {
+  for (uint32_t i = 0; i < n; i++) {
+    const avbd_joint_info& in = info[i];
+    if (in.type != AVBD_T_JOINT && in.type != AVBD_T_SPRING && in.type != AVBD_T_NONE) return "joint " + std::to_string(i) + ": unknown type";
+    if (in.b < 0 || uint32_t(in.b) >= bodies || in.a < -1 || (in.a >= 0 && uint32_t(in.a) >= bodies) || in.a == in.b)
+      return "joint " + std::to_string(i) + ": bodies must be distinct indices below the body count (a may be -1)";
+    if (in.type == AVBD_T_SPRING && in.a < 0) return "joint " + std::to_string(i) + ": a spring joins two bodies";
+    const float* f = reinterpret_cast<const float*>(j + i);
+    for (int k = 0; k < 40; k++)
+      if (std::isnan(f[k])) return "joint " + std::to_string(i) + ": NaN";
+  }
+  return {};
+}
+
+}  // namespace avbd
 
 namespace {
 
@@ -140,6 +135,7 @@ int allocPairs(avbd_world* w, uint32_t cap) {
   dfree(w, d.adjList);
   dfree(w, d.incList);
   w->pairCap = cap;
+  w->configGen++;
   w->hashSize = pow2AtLeast(2ull * cap);
   w->adjCap = 2u * (cap + w->jointCap);
   w->incCap = 2u * (cap * MAX_CONTACTS + w->jointCap);
@@ -187,6 +183,7 @@ int allocJoints(avbd_world* w, uint32_t cap) {
   d.joint = nj;
   d.jinfo = ni;
   w->jointCap = cap;
+  w->configGen++;
   // adjacency and incidence lists are sized by the joint capacity too
   dfree(w, d.adjList);
   dfree(w, d.incList);
@@ -195,46 +192,6 @@ int allocJoints(avbd_world* w, uint32_t cap) {
   CUDA_TRY(w, dalloc(w, &d.adjList, w->adjCap));
   CUDA_TRY(w, dalloc(w, &d.incList, w->incCap));
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  return AVBD_OK;
-}
-
-// uploadStatics (solver.ts:1263-1318): large bodies, cell size, sorted no-collide triples
-int uploadStatics(avbd_world* w) {
-  const uint32_t n = w->n;
-  std::vector<double> radii(n);
-  for (uint32_t i = 0; i < n; i++) radii[i] = w->radius[i];
-  double maxSmall = largestSmall(radii);
-  double minLarge = INFINITY;
-  for (uint32_t i = 0; i < n; i++)
-    if (radii[i] > maxSmall) minLarge = std::min(minLarge, radii[i]);
-  double threshold = std::isinf(minLarge) ? maxSmall * 1.5 : (maxSmall + minLarge) / 2;
-  w->threshold = float(threshold);
-  w->cellSize = float(std::max(2.0 * maxSmall * (1 + 1e-4), 1e-3));
-  std::vector<uint32_t> data;
-  w->anyDynamicLarge = 0;
-  for (uint32_t i = 0; i < n; i++)
-    if (w->radius[i] > w->threshold) {
-      data.push_back(i);
-      if (w->dynamic[i]) w->anyDynamicLarge = 1;
-    }
-  w->nLarge = uint32_t(data.size());
-  std::stable_sort(w->nocollide.begin(), w->nocollide.end());
-  for (auto& e : w->nocollide) {
-    data.push_back(e.hi);
-    data.push_back(e.lo);
-    data.push_back(e.slot);
-  }
-  w->nNoCollide = uint32_t(w->nocollide.size());
-  if (data.size() > w->staticsWords) {
-    dfree(w, w->d.large);
-    w->staticsWords = uint32_t(std::max<size_t>(data.size() * 2, 64));
-    CUDA_TRY(w, dalloc(w, &w->d.large, w->staticsWords));
-  }
-  if (!data.empty()) CUDA_TRY(w, cudaMemcpyAsync(w->d.large, data.data(), data.size() * 4, cudaMemcpyHostToDevice, w->stream));
-  // keep the upload's source alive until it lands (pageable copies are staged synchronously)
-  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  w->d.nocollide = w->d.large + w->nLarge;
-  w->staticsDirty = false;
   return AVBD_OK;
 }
 
@@ -309,6 +266,47 @@ bool finite(float x) { return std::isfinite(x); }
 
 }  // namespace
 
+namespace avbd {
+
+// uploadStatics (solver.ts:1263-1318): large bodies, cell size, sorted no-collide triples
+int uploadStatics(avbd_world* w) {
+  const uint32_t n = w->n;
+  std::vector<double> radii(n);
+  for (uint32_t i = 0; i < n; i++) radii[i] = w->radius[i];
+  double maxSmall = largestSmall(radii);
+  w->threshold = float(largeThreshold(radii));
+  w->cellSize = float(std::max(2.0 * maxSmall * (1 + 1e-4), 1e-3));
+  std::vector<uint32_t> data;
+  w->anyDynamicLarge = 0;
+  for (uint32_t i = 0; i < n; i++)
+    if (w->radius[i] > w->threshold) {
+      data.push_back(i);
+      if (w->dynamic[i]) w->anyDynamicLarge = 1;
+    }
+  w->nLarge = uint32_t(data.size());
+  std::stable_sort(w->nocollide.begin(), w->nocollide.end());
+  for (auto& e : w->nocollide) {
+    data.push_back(e.hi);
+    data.push_back(e.lo);
+    data.push_back(e.slot);
+  }
+  w->nNoCollide = uint32_t(w->nocollide.size());
+  w->configGen++;
+  if (data.size() > w->staticsWords) {
+    dfree(w, w->d.large);
+    w->staticsWords = uint32_t(std::max<size_t>(data.size() * 2, 64));
+    CUDA_TRY(w, dalloc(w, &w->d.large, w->staticsWords));
+  }
+  if (!data.empty()) CUDA_TRY(w, cudaMemcpyAsync(w->d.large, data.data(), data.size() * 4, cudaMemcpyHostToDevice, w->stream));
+  // keep the upload's source alive until it lands (pageable copies are staged synchronously)
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  w->d.nocollide = w->d.large + w->nLarge;
+  w->staticsDirty = false;
+  return AVBD_OK;
+}
+
+}  // namespace avbd
+
 extern "C" {
 
 int avbd_abi_version(void) { return AVBD_ABI_VERSION; }
@@ -372,7 +370,7 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   const uint32_t B = w->bodyCap;
   w->tableSize = pow2AtLeast(2ull * B);
   w->sortTiles = (B + 8191) / 8192;
-  w->solveBlocks = solve_grid_blocks(w->device);
+  w->solveBlocks = w->maxSolveBlocks = solve_grid_blocks(w->device);
   bool ok = true;
   auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
   for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel}) A(dalloc(w, f, B));
@@ -385,6 +383,8 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.cell, B));
   A(dalloc(w, &d.sortedPR, B));
   A(dalloc(w, &d.sortedCell, B));
+  A(dalloc(w, &d.aabb, B));
+  A(dalloc(w, &d.sortedAabb, B));
   A(dalloc(w, &d.cellStart, w->tableSize));
   A(dalloc(w, &d.cellEnd, w->tableSize));
   A(dalloc(w, &d.adjStart, B + 1));
@@ -403,7 +403,7 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.scanScratch, w->solveBlocks + 1));
   A(dalloc(w, &d.counters, COUNTER_WORDS));
   A(dalloc(w, &d.barrier, 2));
-  A(dalloc(w, &d.clocks, MAX_CLOCKS + 1));
+  A(dalloc(w, &d.clocks, CLOCK_WORDS));
   if (!ok) return bad(AVBD_ERR_CUDA);
   // every body in every group, colliding with every group; colours start unset
   A(cudaMemsetAsync(d.filters, 0xff, size_t(B) * sizeof(uint2), w->stream));
@@ -432,9 +432,10 @@ int avbd_world_destroy(avbd_world* w) {
   for (void* p : w->allocations) cudaFree(p);
   w->allocations.clear();
   if (w->hCounters) cudaFreeHost(w->hCounters);
+  for (auto& g : w->graph)
+    if (g) cudaGraphExecDestroy(g);
   if (w->countersReady) cudaEventDestroy(w->countersReady);
-  for (auto& e : w->statsEvents)
-    if (e) cudaEventDestroy(e);
+
   if (w->stream) cudaStreamDestroy(w->stream);
   delete w;
   return AVBD_OK;
@@ -448,6 +449,7 @@ int avbd_set_params(avbd_world* w, const avbd_params* p) {
       !(p->contact_margin >= 0.0f) || !finite(p->contact_margin))
     return fail(w, AVBD_ERR_INVALID, "invalid params (dt > 0, finite values, iterations >= 0, contact_margin >= 0)");
   w->params = *p;
+  w->configGen++;
   return AVBD_OK;
 }
 
@@ -458,13 +460,8 @@ int avbd_get_params(const avbd_world* w, avbd_params* p) {
 }
 
 static int checkBodies(avbd_world* w, const avbd_body* b, uint32_t n) {
-  for (uint32_t i = 0; i < n; i++) {
-    const float* f = reinterpret_cast<const float*>(b + i);
-    for (int k = 0; k < 40; k++)
-      if (!finite(f[k])) return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + ": non-finite value");
-    if (b[i].mass < 0.0f || b[i].radius < 0.0f) return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + ": negative mass or radius");
-  }
-  return AVBD_OK;
+  std::string msg = bodyProblem(b, n);
+  return msg.empty() ? AVBD_OK : fail(w, AVBD_ERR_INVALID, msg);
 }
 
 int avbd_add_bodies(avbd_world* w, const avbd_body* bodies, uint32_t n, uint32_t* first) {
@@ -513,18 +510,8 @@ int avbd_write_bodies(avbd_world* w, uint32_t first, const avbd_body* bodies, ui
 }
 
 static int checkJoints(avbd_world* w, const avbd_joint* j, const avbd_joint_info* info, uint32_t n) {
-  for (uint32_t i = 0; i < n; i++) {
-    const avbd_joint_info& in = info[i];
-    if (in.type != AVBD_T_JOINT && in.type != AVBD_T_SPRING && in.type != AVBD_T_NONE)
-      return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": unknown type");
-    if (in.b < 0 || uint32_t(in.b) >= w->n || in.a < -1 || (in.a >= 0 && uint32_t(in.a) >= w->n) || in.a == in.b)
-      return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": bodies must be distinct indices below the body count (a may be -1)");
-    if (in.type == AVBD_T_SPRING && in.a < 0) return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": a spring joins two bodies");
-    const float* f = reinterpret_cast<const float*>(j + i);
-    for (int k = 0; k < 40; k++)
-      if (std::isnan(f[k])) return fail(w, AVBD_ERR_INVALID, "joint " + std::to_string(i) + ": NaN");
-  }
-  return AVBD_OK;
+  std::string msg = jointProblem(j, info, n, w->n);
+  return msg.empty() ? AVBD_OK : fail(w, AVBD_ERR_INVALID, msg);
 }
 
 int avbd_write_joints(avbd_world* w, uint32_t first, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n) {
@@ -638,6 +625,7 @@ int avbd_seed_contacts(avbd_world* w, const avbd_manifold* m, uint32_t nm, const
 
 int avbd_set_fixed_colors(avbd_world* w, const uint32_t* colors, uint32_t n) {
   if (!w) return AVBD_ERR_INVALID;
+  w->configGen++;
   if (!colors) {
     w->fixedColors = false;
     return AVBD_OK;
@@ -664,23 +652,51 @@ int avbd_step(avbd_world* w, int n) {
     }
     w->stepCount++;
     StepParams p = makeParams(w);
-    const uint32_t slot = w->statsCap ? w->statsCount % w->statsCap : 0;
-    cudaEvent_t* ev = w->statsCap ? &w->statsEvents[3 * slot] : nullptr;
-    if (ev) cudaEventRecord(ev[0], w->stream);
-    uint32_t launches = launch_collision(w->d, p, w->tableSize, w->stream);
-    if (ev) cudaEventRecord(ev[1], w->stream);
-    CUDA_TRY(w, cudaGetLastError());
-    CUDA_TRY(w, launch_topology_solve(w->d, p, w->solveBlocks, w->stream));
-    launches += 1;
-    w->launchesPerStep = launches;
-    if (ev) {
-      cudaEventRecord(ev[2], w->stream);
-      CUDA_TRY(w, cudaMemcpyAsync(w->statsCounters + size_t(slot) * COUNTER_WORDS, w->d.counters, COUNTER_WORDS * sizeof(uint32_t),
-                                  cudaMemcpyDeviceToDevice, w->stream));
-      w->statsLaunches[slot] = launches;
-      w->statsCount++;
+    auto enqueue = [&]() -> cudaError_t {
+      uint32_t launches = launch_collision(w->d, p, w->tableSize, w->stream) + 1;
+      cudaError_t le = launch_topology_solve(w->d, p, w->solveBlocks, w->stream);
+      if (w->statsCap) launch_step_stats(w->d, launches + 1, w->stream);
+      w->launchesPerStep = launches + (w->statsCap ? 1 : 0);
+      cudaMemcpyAsync(w->hCounters, w->d.counters, COUNTER_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, w->stream);
+      return le;
+    };
+    bool launched = false;
+    if (w->useGraphs) {
+      const int c = w->cur;
+      if (!w->graph[c] || w->graphGen[c] != w->configGen) {
+        if (w->graph[c]) cudaGraphExecDestroy(w->graph[c]);
+        w->graph[c] = nullptr;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          cudaError_t le = enqueue();
+          e = cudaStreamEndCapture(w->stream, &g);
+          if (e == cudaSuccess && le == cudaSuccess) e = cudaGraphInstantiate(&w->graph[c], g, 0);
+          else if (e == cudaSuccess) e = le;
+          if (g) cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess) {
+          // capture is not available here: launch directly from now on
+          cudaGetLastError();
+          w->useGraphs = false;
+          w->graphNote = std::string("graph capture failed: ") + cudaGetErrorString(e);
+          if (w->graph[c]) cudaGraphExecDestroy(w->graph[c]);
+          w->graph[c] = nullptr;
+        } else {
+          w->graphGen[c] = w->configGen;
+        }
+      }
+      if (w->graph[c]) {
+        CUDA_TRY(w, cudaGraphLaunch(w->graph[c], w->stream));
+        launched = true;
+      }
     }
-    CUDA_TRY(w, cudaMemcpyAsync(w->hCounters, w->d.counters, COUNTER_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, w->stream));
+    if (!launched) {
+      cudaError_t le = enqueue();
+      CUDA_TRY(w, cudaGetLastError());
+      CUDA_TRY(w, le);
+    }
+    if (w->statsCap) w->statsCount++;
     CUDA_TRY(w, cudaEventRecord(w->countersReady, w->stream));
     w->countersInFlight = true;
     w->cur = 1 - w->cur;
@@ -748,6 +764,8 @@ int avbd_read_counters(avbd_world* w, avbd_counters* out) {
   out->rounds = c[C_ROUNDS];
   out->error = c[C_ERROR];
   out->steps = w->stepCount;
+  out->graphs = w->useGraphs ? 1u : 0u;
+  out->launches = w->launchesPerStep;
   out->pair_capacity = w->pairCap;
   return AVBD_OK;
 }
@@ -824,17 +842,17 @@ int avbd_enable_step_stats(avbd_world* w, uint32_t capacity) {
   if (!w) return AVBD_ERR_INVALID;
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  for (auto& e : w->statsEvents) cudaEventDestroy(e);
-  w->statsEvents.clear();
-  dfree(w, w->statsCounters);
-  w->statsCounters = nullptr;
+  dfree(w, w->d.statsRing);
+  w->d.statsRing = nullptr;
+  w->d.statsCap = 0;
   w->statsCap = capacity;
   w->statsCount = 0;
-  w->statsLaunches.assign(capacity, 0);
+  w->configGen++;
   if (!capacity) return AVBD_OK;
-  w->statsEvents.resize(size_t(capacity) * 3, nullptr);
-  for (auto& e : w->statsEvents) CUDA_TRY(w, cudaEventCreate(&e));
-  CUDA_TRY(w, dalloc(w, &w->statsCounters, size_t(capacity) * COUNTER_WORDS));
+  CUDA_TRY(w, dalloc(w, &w->d.statsRing, size_t(capacity) * STAT_WORDS));
+  w->d.statsCap = capacity;
+  uint32_t zero = 0;
+  CUDA_TRY(w, cudaMemcpyAsync(w->d.counters + C_STATS_NEXT, &zero, 4, cudaMemcpyHostToDevice, w->stream));
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   return AVBD_OK;
 }
@@ -846,27 +864,24 @@ int avbd_read_step_stats(avbd_world* w, avbd_step_stats* dst, uint32_t cap, uint
   uint32_t have = std::min(w->statsCount, w->statsCap);
   if (n) *n = have;
   if (!dst || !have) return AVBD_OK;
-  std::vector<uint32_t> c(size_t(w->statsCap) * COUNTER_WORDS);
-  CUDA_TRY(w, cudaMemcpy(c.data(), w->statsCounters, c.size() * 4, cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> r(size_t(w->statsCap) * STAT_WORDS);
+  CUDA_TRY(w, cudaMemcpy(r.data(), w->d.statsRing, r.size() * 4, cudaMemcpyDeviceToHost));
   uint32_t first = w->statsCount - have;
   for (uint32_t k = 0; k < have && k < cap; k++) {
-    uint32_t slot = (first + k) % w->statsCap;
+    const uint32_t* q = &r[size_t((first + k) % w->statsCap) * STAT_WORDS];
     avbd_step_stats& s = dst[k];
-    cudaEvent_t* ev = &w->statsEvents[3 * slot];
-    s.collision_ms = s.solve_ms = 0.0f;
-    cudaEventElapsedTime(&s.collision_ms, ev[0], ev[1]);
-    cudaEventElapsedTime(&s.solve_ms, ev[1], ev[2]);
-    const uint32_t* q = &c[size_t(slot) * COUNTER_WORDS];
-    s.pairs = q[C_PAIRS];
-    s.contacts = q[C_CONTACTS];
-    s.manifolds = q[C_MANIFOLDS];
-    s.adjacency = q[C_ADJ];
-    s.incidences = q[C_INC];
-    s.dynamic_bodies = q[C_DYN];
-    s.colors = q[C_COLORS];
-    s.rounds = q[C_ROUNDS];
-    s.launches = w->statsLaunches[slot];
-    s.error = q[C_ERROR];
+    s.collision_ms = float(q[0] * 1e-6);
+    s.solve_ms = float(q[1] * 1e-6);
+    s.pairs = q[2];
+    s.contacts = q[3];
+    s.manifolds = q[4];
+    s.adjacency = q[5];
+    s.incidences = q[6];
+    s.dynamic_bodies = q[7];
+    s.colors = q[8];
+    s.rounds = q[9];
+    s.launches = q[10];
+    s.error = q[11];
   }
   return AVBD_OK;
 }
@@ -875,11 +890,26 @@ int avbd_read_phase_clocks(avbd_world* w, double* dst, uint32_t cap, uint32_t* n
   if (!w) return AVBD_ERR_INVALID;
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  std::vector<unsigned long long> ck(MAX_CLOCKS + 1);
+  std::vector<unsigned long long> ck(CLOCK_WORDS);
   CUDA_TRY(w, cudaMemcpy(ck.data(), w->d.clocks, ck.size() * 8, cudaMemcpyDeviceToHost));
   uint32_t k = uint32_t(std::min<unsigned long long>(ck[0], MAX_CLOCKS));
   if (n) *n = k;
   for (uint32_t i = 0; i < k && i < cap && dst; i++) dst[i] = double(ck[1 + i] - ck[1]) * 1e-6;
+  return AVBD_OK;
+}
+
+int avbd_use_graphs(avbd_world* w, int enable) {
+  if (!w) return AVBD_ERR_INVALID;
+  w->useGraphs = enable != 0;
+  w->configGen++;
+  return AVBD_OK;
+}
+
+int avbd_set_solve_blocks(avbd_world* w, int blocks) {
+  if (!w || blocks < 0) return AVBD_ERR_INVALID;
+  if (blocks > w->maxSolveBlocks) return fail(w, AVBD_ERR_INVALID, "at most " + std::to_string(w->maxSolveBlocks) + " co-resident solve blocks");
+  w->solveBlocks = blocks ? blocks : w->maxSolveBlocks;
+  w->configGen++;
   return AVBD_OK;
 }
 

@@ -1,0 +1,71 @@
+// Host-side state shared by the single-world and batched entry points (avbd_host.cu, avbd_batch.cu).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "avbd.h"
+#include "avbd_device.cuh"
+
+namespace avbd {
+
+uint32_t pow2AtLeast(uint64_t n);
+// The largest "small" bounding radius of a body set (radii.ts:19-55): the broadphase classification
+double largestSmall(std::vector<double> radii);
+double largeThreshold(const std::vector<double>& radii);
+// Why a set of records is invalid (empty: valid)
+std::string bodyProblem(const avbd_body* b, uint32_t n);
+std::string jointProblem(const avbd_joint* j, const avbd_joint_info* info, uint32_t n, uint32_t bodies);
+
+struct NoCollide {
+  uint32_t hi, lo, slot;
+  bool operator<(const NoCollide& o) const { return hi < o.hi || (hi == o.hi && lo < o.lo); }
+};
+
+}  // namespace avbd
+
+// One simulation world (GpuSolver3D's state, gpu/solver.ts:598-700)
+struct avbd_world {
+  using DWorld = avbd::DWorld;
+  using NoCollide = avbd::NoCollide;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  avbd_params params{};
+  uint32_t bodyCap = 0, n = 0, jointCap = 0, nj = 0, pairCap = 0, tableSize = 0, hashSize = 0, incCap = 0, adjCap = 0;
+  uint32_t sortTiles = 0;
+  DWorld d{};
+  int solveBlocks = 0, maxSolveBlocks = 0;  // the cooperative solve's grid (maxSolveBlocks: all co-resident)
+  int cur = 0;
+  uint32_t stepCount = 0;
+  bool fixedColors = false;
+  // host mirrors
+  std::vector<float> radius;
+  std::vector<char> dynamic;
+  std::vector<avbd_joint_info> info;
+  std::vector<NoCollide> nocollide;
+  bool staticsDirty = true;
+  float threshold = 0.0f, cellSize = 1.0f;
+  uint32_t nLarge = 0, nNoCollide = 0, anyDynamicLarge = 0;
+  uint32_t staticsWords = 0;
+  // counters of the last step, copied back asynchronously
+  uint32_t* hCounters = nullptr;
+  cudaEvent_t countersReady = nullptr;
+  bool countersInFlight = false;
+  // per-step statistics: a device ring written by the step itself (graph-compatible)
+  uint32_t statsCap = 0, statsCount = 0;
+  uint32_t launchesPerStep = 0;
+  // The step as two CUDA graphs (one per contact-buffer parity), rebuilt when anything baked into
+  // their launches changes (configGen)
+  bool useGraphs = true;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  uint64_t graphGen[2] = {0, 0};
+  uint64_t configGen = 1;
+  std::string graphNote;
+  std::vector<void*> allocations;
+};
+
+namespace avbd {
+// Uploads the world's large-body list and sorted no-collide triples when they changed
+int uploadStatics(avbd_world* w);
+}  // namespace avbd

@@ -118,21 +118,45 @@ __device__ uint32_t block_scan_range(uint32_t* data, uint32_t lo, uint32_t hi) {
   return s_carry;
 }
 
-// Exclusive scan of data[0, len) across the grid; scratch[gridDim.x] receives the total.
-__device__ bool grid_scan(uint32_t* data, uint32_t len, uint32_t* scratch, uint32_t* bar, uint32_t* counters) {
-  uint32_t chunk = (len + gridDim.x - 1) / gridDim.x;
-  uint32_t lo = min(len, blockIdx.x * chunk), hi = min(len, lo + chunk);
-  uint32_t total = block_scan_range(data, lo, hi);
-  if (threadIdx.x == 0) scratch[blockIdx.x] = total;
-  if (!grid_sync(bar, counters)) return false;
-  if (blockIdx.x == 0) {
-    uint32_t all = block_scan_range(scratch, 0, gridDim.x);
-    if (threadIdx.x == 0) scratch[gridDim.x] = all;
+// The two scopes the topology+solve code runs at: the whole grid (one large world, cooperative
+// launch, bounded grid barriers) or one block (one small world of a batch, __syncthreads).
+struct GridTeam {
+  uint32_t* bar;
+  uint32_t* ctr;
+  __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+  __device__ uint32_t size() const { return gridDim.x * blockDim.x; }
+  __device__ uint32_t block() const { return blockIdx.x; }
+  __device__ uint32_t blocks() const { return gridDim.x; }
+  __device__ bool sync() { return grid_sync(bar, ctr); }
+};
+struct BlockTeam {
+  __device__ uint32_t rank() const { return threadIdx.x; }
+  __device__ uint32_t size() const { return blockDim.x; }
+  __device__ uint32_t block() const { return 0; }
+  __device__ uint32_t blocks() const { return 1; }
+  __device__ bool sync() {
+    __syncthreads();
+    return true;
   }
-  if (!grid_sync(bar, counters)) return false;
-  uint32_t add = scratch[blockIdx.x];
-  for (uint32_t i = lo + threadIdx.x; i < hi; i += SOLVE_THREADS) data[i] += add;
-  return grid_sync(bar, counters);
+};
+
+// Exclusive scan of data[0, len) across the team; scratch[team.blocks()] receives the total.
+template <class Team>
+__device__ bool team_scan(uint32_t* data, uint32_t len, uint32_t* scratch, Team& team) {
+  const uint32_t nb = team.blocks(), bi = team.block();
+  uint32_t chunk = (len + nb - 1) / nb;
+  uint32_t lo = min(len, bi * chunk), hi = min(len, lo + chunk);
+  uint32_t total = block_scan_range(data, lo, hi);
+  if (threadIdx.x == 0) scratch[bi] = total;
+  if (!team.sync()) return false;
+  if (bi == 0) {
+    uint32_t all = block_scan_range(scratch, 0, nb);
+    if (threadIdx.x == 0) scratch[nb] = all;
+  }
+  if (!team.sync()) return false;
+  uint32_t add = scratch[bi];
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) data[i] += add;
+  return team.sync();
 }
 
 // --- constraint endpoints and activity (gpu/layout.ts:356-369) ----------------------------------------
@@ -529,33 +553,29 @@ __device__ inline void dualIncidence(const DWorld& w, const StepParams& p, uint2
   pt[K_PEN] = pen;
 }
 
-// Lanes per body: about two rows a lane, a power of two up to a warp
-__device__ inline uint32_t laneClass(uint32_t rows) {
-  uint32_t want = (rows + 1u) >> 1;
+// Lanes per body: `perLane` rows a lane (the colour's rows over the grid's threads, at least one, so a
+// colour fills the GPU about once), rounded up to a power of two lanes, up to a warp
+__device__ inline uint32_t laneClass(uint32_t rows, uint32_t perLane) {
+  uint32_t want = (rows + perLane - 1u) / perLane;
   uint32_t k = 0;
   while (k < 5u && (1u << k) < want) k++;
   return k;
 }
 
 // Bucket bookkeeping in w.bucket: counts | starts (+ total) | fill cursors | lane bases | lane totals
-constexpr int B_COUNT = 0, B_START = BUCKETS, B_FILL = 2 * BUCKETS + 1, B_LANE = 3 * BUCKETS + 1, B_LANE_TOTAL = 4 * BUCKETS + 1;
-static_assert(B_LANE_TOTAL + MAX_COLORS <= BUCKET_WORDS, "bucket words");
+constexpr int B_COUNT = 0, B_START = BUCKETS, B_FILL = 2 * BUCKETS + 1, B_LANE = 3 * BUCKETS + 1, B_LANE_TOTAL = 4 * BUCKETS + 1,
+              B_ROWS = B_LANE_TOTAL + MAX_COLORS;
+static_assert(B_ROWS + MAX_COLORS <= BUCKET_WORDS, "bucket words");
 
 // --- the kernel -----------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, StepParams p) {
-  const uint32_t T = gridDim.x * blockDim.x;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+template <class Team>
+__device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) {
+  const uint32_t T = team.size();
+  const uint32_t tid = team.rank();
   const uint32_t n = p.n, nj = p.nj;
   uint32_t* ctr = w.counters;
-  uint32_t* bar = w.barrier;
 #define GSYNC \
-  if (!grid_sync(bar, ctr)) return;
-  if (threadIdx.x == 0) s_epoch = 0;
-  if (tid == 0) {
-    g_clocks = w.clocks;
-    w.clocks[0] = 1;
-    w.clocks[1] = globaltimer();
-  }
+  if (!team.sync()) return;
   uint32_t npairs = ldv(&ctr[C_PAIRS]);
   if (npairs > p.pairCap) npairs = p.pairCap;
   const uint32_t ncons = nj + npairs;
@@ -569,7 +589,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
     if (dynBody(w, eb)) atomicAdd(&w.adjStart[eb], 1u);
   }
   GSYNC
-  if (!grid_scan(w.adjStart, n + 1, w.scanScratch, bar, ctr)) return;
+  if (!team_scan(w.adjStart, n + 1, w.scanScratch, team)) return;
   if (tid == 0) ctr[C_ADJ] = w.adjStart[n];
   // B. fill (adjFill zeroed by the host), then each body's list sorted into its summation order and
   // its row count (a joint is one row, a pair one per point)
@@ -680,7 +700,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
   // D. final colours (NO_COLOR -> cap - 1, pending kept and counted), and bodies counted into
   // (colour, lane class) buckets, widest lane class first within a colour. The order of bodies in a
   // bucket does not change any result (a colour's bodies share no row), so the scatter uses atomics.
-  __shared__ uint32_t s_hist[BUCKETS], s_base[BUCKETS];
+  __shared__ uint32_t s_hist[BUCKETS], s_base[BUCKETS], s_perLane[MAX_COLORS];
   {
     for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
     __syncthreads();
@@ -693,16 +713,30 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
       if (col == NO_COLOR || col >= (uint32_t)MAX_COLORS) col = cap - 1u;
       w.colorA[b] = col | (s & PENDING);
       maxc = max(maxc, col + 1u);
-      atomicAdd(&s_hist[col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b]))], 1u);
+      atomicAdd(&s_hist[col], w.incCount[b] + 1u);  // the colour's rows (+1: the body's own inertia)
     }
     if (clashes) atomicAdd(&ctr[C_CLASHES], clashes);
     if (maxc) atomicMax(&ctr[C_COLORS], maxc);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < (uint32_t)MAX_COLORS; k += SOLVE_THREADS)
+      if (s_hist[k]) atomicAdd(&w.bucket[B_ROWS + k], s_hist[k]);
+  }
+  GSYNC
+  {
+    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
+    if (threadIdx.x < (uint32_t)MAX_COLORS) s_perLane[threadIdx.x] = max(1u, (w.bucket[B_ROWS + threadIdx.x] + T - 1u) / T);
+    __syncthreads();
+    for (uint32_t b = tid; b < n; b += T) {
+      if (!dynBody(w, (int)b)) continue;
+      uint32_t col = w.colorA[b] & 0xffu;
+      atomicAdd(&s_hist[col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b], s_perLane[col]))], 1u);
+    }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS)
       if (s_hist[k]) atomicAdd(&w.bucket[B_COUNT + k], s_hist[k]);
   }
   GSYNC
-  if (blockIdx.x == 0) {
+  if (team.block() == 0) {
     if (threadIdx.x < BUCKETS) w.bucket[B_START + threadIdx.x] = w.bucket[B_COUNT + threadIdx.x];
     if (threadIdx.x + SOLVE_THREADS < BUCKETS) w.bucket[B_START + threadIdx.x + SOLVE_THREADS] = w.bucket[B_COUNT + threadIdx.x + SOLVE_THREADS];
     __syncthreads();
@@ -728,7 +762,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
     __syncthreads();
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
-      atomicAdd(&s_hist[(w.colorA[b] & 0xffu) * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b]))], 1u);
+      uint32_t col = w.colorA[b] & 0xffu;
+      atomicAdd(&s_hist[col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b], s_perLane[col]))], 1u);
     }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) {
@@ -738,7 +773,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
     __syncthreads();
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
-      uint32_t bucket = (w.colorA[b] & 0xffu) * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b]));
+      uint32_t col = w.colorA[b] & 0xffu;
+      uint32_t bucket = col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b], s_perLane[col]));
       uint32_t pos = s_base[bucket] + atomicAdd(&s_hist[bucket], 1u);
       w.colorBodies[pos] = b;
       w.incStart[pos] = w.incCount[b];
@@ -752,8 +788,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
 
   // E. incidence list: for each colour position s (body b = colorBodies[s]) its rows in summation
   // order, with the partner body and OWNER_BIT where b is the last of the row's dynamic bodies to move
-  if (!grid_scan(w.incStart, numDyn + 1, w.scanScratch, bar, ctr)) return;
-  const uint32_t totalInc = ldv(&w.scanScratch[gridDim.x]);
+  if (!team_scan(w.incStart, numDyn + 1, w.scanScratch, team)) return;
+  const uint32_t totalInc = ldv(&w.scanScratch[team.blocks()]);
   if (tid == 0) ctr[C_INC] = totalInc;
   if (totalInc > p.incCap) {
     if (tid == 0) atomicOr(&ctr[C_ERROR], ERR_INC_OVERFLOW);
@@ -954,8 +990,59 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, S
       w.vel[i] = make_float4(vel.x, vel.y, vel.z, prevUp);
     }
   }
-  grid_sync(bar, ctr);
+  team.sync();
 #undef GSYNC
+}
+
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_topology_solve(DWorld w, StepParams p) {
+  if (threadIdx.x == 0) s_epoch = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    g_clocks = w.clocks;
+    w.clocks[0] = 1;
+    w.clocks[1] = globaltimer();
+  }
+  GridTeam team{w.barrier, w.counters};
+  topologySolve(w, p, team);
+}
+
+// Batched worlds: each block takes worlds from the queue (largest first) and runs the same
+// topology + solve code for one world at block scope.
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_batch_solve(BatchLaunch B) {
+  __shared__ uint32_t s_world;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_world = atomicAdd(&B.queue[1], 1u);
+    __syncthreads();
+    const uint32_t qi = s_world;
+    if (qi >= B.nWorlds) return;
+    const uint32_t wi = B.order[qi];
+    const WorldDesc d = B.worlds[wi];
+    const DWorld w = worldView(B.base, d, wi);
+    const StepParams p = worldParams(B.p, d);
+    for (uint32_t i = threadIdx.x; i <= d.n; i += SOLVE_THREADS) {
+      w.adjStart[i] = 0u;
+      w.adjFill[i] = 0u;
+    }
+    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKET_WORDS; k += SOLVE_THREADS) w.bucket[k] = 0u;
+    __syncthreads();
+    BlockTeam team;
+    topologySolve(w, p, team);
+    __syncthreads();
+    if (threadIdx.x == 0 && w.counters[C_ERROR]) atomicOr(&B.status[1], w.counters[C_ERROR]);
+  }
+}
+
+static_assert(BATCH_SOLVE_THREADS == SOLVE_THREADS, "one solve block size");
+
+int batch_solve_blocks_per_sm() {
+  int perSm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve, SOLVE_THREADS, 0);
+  return perSm;
+}
+
+cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, cudaStream_t s) {
+  k_batch_solve<<<blocks, SOLVE_THREADS, 0, s>>>(b);
+  return cudaGetLastError();
 }
 
 int solve_grid_blocks(int device) {
