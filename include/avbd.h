@@ -229,6 +229,23 @@ int avbd_world_stream(avbd_world* world, void** stream);
  * avbd_write_bodies for those). Keeps the bodies' contact history. */
 int avbd_write_bodies_async(avbd_world* world, uint32_t first, const avbd_body* bodies, uint32_t n);
 
+/* Broadphase without allocation. No counterpart in the reference. The step's candidate pairs
+ * (the rule of the step's broadphase: groups/mask, bounding spheres, AABBs + 1e-4, face separation)
+ * of n <= AVBD_NOALLOC_MAX_BODIES host body records, found in one block with every intermediate array
+ * in one fixed device array of AVBD_NOALLOC_SCRATCH_BYTES; it allocates no device or pinned memory.
+ * For callers that cannot allocate (a thread querying pairs while steps run on other streams, since
+ * cudaMalloc/cudaFree synchronise the device; hosts whose allocator owns all device memory).
+ * groups_mask: 2 words per body (groups, mask) or NULL (all collide). Writes up to cap (a, b) pairs,
+ * a > b, in no particular order, to pairs_ab and the number found to *count; returns
+ * AVBD_ERR_CAPACITY when n is past the maximum or more pairs were found than cap or
+ * AVBD_NOALLOC_MAX_PAIRS. Runs on `stream` (a cudaStream_t, NULL: the default stream) of the current
+ * device and waits for it. All calls share the fixed array: calls whose GPU work overlaps race. */
+#define AVBD_NOALLOC_MAX_BODIES 4096u
+#define AVBD_NOALLOC_MAX_PAIRS 32768u
+#define AVBD_NOALLOC_SCRATCH_BYTES 1065472u
+int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, const uint32_t* groups_mask, uint32_t* pairs_ab, uint32_t cap, uint32_t* count,
+                            void* stream);
+
 /* ---- Batched worlds ------------------------------------------------------------------------------
  * No counterpart in the reference, which steps one world per GpuSolver3D (gpu/solver.ts:598). A batch
  * holds many small independent worlds (1 to AVBD_BATCH_MAX_WORLD_BODIES bodies each) and steps them

@@ -88,6 +88,8 @@ class BatchStatus(ctypes.Structure):
                 ('collide_blocks', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32), ('graphs', ctypes.c_uint32)]
 
 
+NOALLOC_MAX_BODIES = 4096
+NOALLOC_MAX_PAIRS = 32768
 TUNE_CANDIDATES = 8
 BATCH_MAX_WORLD_BODIES = 4096
 
@@ -136,6 +138,7 @@ SIGNATURES = {
     'avbd_set_solve_blocks': ([P, I], I),
     'avbd_read_phase_clocks': ([P, ctypes.POINTER(ctypes.c_double), U, PU], I),
     'avbd_write_bodies_async': ([P, U, VP, U], I),
+    'avbd_find_pairs_noalloc': ([VP, U, PU, PU, U, PU, VP], I),
     'avbd_batch_create': ([ctypes.POINTER(BatchConfig), ctypes.POINTER(P)], I),
     'avbd_batch_destroy': ([P], I),
     'avbd_batch_last_error': ([P], ctypes.c_char_p),

@@ -383,6 +383,27 @@ class CudaSolver3D:
         return out
 
 
+def find_pairs_noalloc(bodies: np.ndarray, groups_mask: np.ndarray | None = None, cap: int = _abi.NOALLOC_MAX_PAIRS,
+                       stream: int = 0) -> np.ndarray:
+    """The step's candidate pairs of up to 4096 bodies (host records) through avbd_find_pairs_noalloc,
+    which allocates nothing: its scratch is one fixed device array shared by every call, so calls must
+    not overlap on the GPU. Returns an (k, 2) array of (a, b), a > b, in no particular order."""
+    lib = _abi.load()
+    bodies = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+    if len(bodies) > _abi.NOALLOC_MAX_BODIES:
+        raise AvbdError(_abi.AVBD_ERR_CAPACITY, f'avbd_find_pairs_noalloc takes at most {_abi.NOALLOC_MAX_BODIES} bodies, got {len(bodies)}')
+    gm = None if groups_mask is None else np.ascontiguousarray(groups_mask, dtype=np.uint32).reshape(-1)
+    out = np.zeros(2 * max(cap, 1), dtype=np.uint32)
+    count = ctypes.c_uint32()
+    code = lib.avbd_find_pairs_noalloc(ptr(bodies), len(bodies), uptr(gm) if gm is not None else None, uptr(out), cap, ctypes.byref(count),
+                                       ctypes.c_void_p(stream))
+    if code != _abi.AVBD_OK:
+        if code == _abi.AVBD_ERR_CAPACITY:
+            raise AvbdError(code, f'{count.value} pairs found, more than the {min(cap, _abi.NOALLOC_MAX_PAIRS)} that fit')
+        raise AvbdError(code, 'avbd_find_pairs_noalloc failed')
+    return out[:2 * count.value].reshape(-1, 2)
+
+
 def device_info(device: int = 0):
     lib = _abi.load()
     name = ctypes.create_string_buffer(256)

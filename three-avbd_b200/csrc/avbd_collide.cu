@@ -8,7 +8,11 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 
+#include <mutex>
+#include <vector>
+
 #include "avbd_device.cuh"
+#include "avbd_host.hpp"
 
 namespace cg = cooperative_groups;
 
@@ -895,3 +899,225 @@ uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSi
 }
 
 }  // namespace avbd
+
+// --- broadphase without allocation -------------------------------------------------------------------
+// No counterpart in the reference. avbd_find_pairs_noalloc runs the step's broadphase (cell keys,
+// counting sort, half-shell walk, large bodies against all; the pair rule of k_find_pairs) over up
+// to NOALLOC_MAX_BODIES bodies given as host records, in ONE block, with every intermediate array in
+// the file-scope device array below. Callers that cannot allocate device memory use it: a render or
+// input thread that queries candidate pairs between steps (cudaMalloc and cudaFree synchronise the
+// whole device, so they would stall the steps in flight on other streams), and hosts that hand all
+// device memory to their own allocator. Every call shares the one array: calls whose GPU work
+// overlaps (two streams, two host threads) race on it and their results are undefined.
+namespace avbd {
+
+constexpr uint32_t NOALLOC_MAX_BODIES = AVBD_NOALLOC_MAX_BODIES;
+constexpr uint32_t NOALLOC_MAX_PAIRS = AVBD_NOALLOC_MAX_PAIRS;
+constexpr uint32_t NOALLOC_TABLE = 2 * NOALLOC_MAX_BODIES;  // cell hash buckets (a power of two)
+constexpr uint32_t NOALLOC_THREADS = 1024;
+static_assert((NOALLOC_TABLE & (NOALLOC_TABLE - 1)) == 0 && NOALLOC_TABLE % NOALLOC_THREADS == 0, "table");
+
+// Byte offsets of the scratch arrays (each a multiple of 256)
+struct NoAllocLayout {
+  static constexpr size_t B = NOALLOC_MAX_BODIES, T = NOALLOC_TABLE;
+  static constexpr size_t POS = 0, ROT = POS + 16 * B, IPOS = ROT + 16 * B, SIZE = IPOS + 16 * B, MOMENT = SIZE + 16 * B, AVEL = MOMENT + 16 * B,
+                          FILTERS = AVEL + 16 * B, CELL = FILTERS + 8 * B, KEY = CELL + 16 * B, RANK = KEY + 4 * B, START = RANK + 4 * B,
+                          END = START + 4 * T, SPR = END + 4 * T, SCELL = SPR + 16 * B, SAABB = SCELL + 16 * B, LARGE = SAABB + 16 * B,
+                          PAIRS = LARGE + 4 * B, COUNTERS = PAIRS + 8 * size_t(NOALLOC_MAX_PAIRS), BYTES = COUNTERS + 4 * COUNTER_WORDS;
+};
+static_assert(NoAllocLayout::BYTES == AVBD_NOALLOC_SCRATCH_BYTES, "the header states the scratch size");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::BYTES];
+
+// One block: counts into buckets, scans them, scatters the candidate records, walks the cells.
+// What must start at zero (the bucket counts and the pair counters) is cleared here, every call.
+__global__ void __launch_bounds__(NOALLOC_THREADS) k_find_pairs_noalloc(DWorld w, StepParams p, uint32_t* key, uint32_t* rank) {
+  const uint32_t n = p.n, T = NOALLOC_TABLE, sentinel = T;
+  __shared__ uint32_t s_warp[NOALLOC_THREADS / 32];
+  for (uint32_t h = threadIdx.x; h < T; h += blockDim.x) w.cellStart[h] = 0u;
+  if (threadIdx.x == 0) {
+    w.counters[C_PAIRS] = 0u;
+    w.counters[C_OVERFLOW] = 0u;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {  // k_cell_keys + k_bucket_count
+    bool small = enabled(w, i) && w.moment[i].w <= p.largeThreshold;
+    int4 c = cellOf(f3(w.pos[i]), p.cellSize);
+    w.cell[i] = c;
+    uint32_t k = small ? cellHash(c, p.tableMask) : sentinel;
+    key[i] = k;
+    if (k != sentinel) rank[i] = atomicAdd(&w.cellStart[k], 1u);
+  }
+  __syncthreads();
+  {  // exclusive scan of the bucket counts: each thread owns T / threads consecutive buckets
+    constexpr uint32_t PER = NOALLOC_TABLE / NOALLOC_THREADS;
+    const uint32_t base = threadIdx.x * PER, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t v[PER], sum = 0;
+    for (uint32_t k = 0; k < PER; k++) {
+      v[k] = w.cellStart[base + k];
+      sum += v[k];
+    }
+    uint32_t x = sum;
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (uint32_t k = 0; k < warp; k++) before += s_warp[k];
+    uint32_t run = before + x - sum;
+    for (uint32_t k = 0; k < PER; k++) {
+      w.cellStart[base + k] = run;
+      w.cellEnd[base + k] = run + v[k];
+      run += v[k];
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {  // k_bucket_scatter
+    uint32_t k = key[i];
+    if (k == sentinel) continue;
+    uint32_t slot = w.cellStart[k] + rank[i];
+    float4 pi = w.pos[i];
+    w.sortedPR[slot] = make_float4(pi.x, pi.y, pi.z, w.moment[i].w);
+    int4 c = w.cell[i];
+    w.sortedCell[slot] = make_int4(c.x, c.y, c.z, (int)(i | (w.size[i].w > 0.0f ? 0x80000000u : 0u)));
+    float3 a = aabbOf(w, i);
+    w.sortedAabb[slot] = make_float4(a.x, a.y, a.z, 0.0f);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {  // the walk of k_find_pairs, body i
+    if (!enabled(w, i)) continue;
+    bool dyn = w.size[i].w > 0.0f;
+    Probe P = probeOf(w, i);
+    if (w.moment[i].w <= p.largeThreshold) {
+      int4 c = w.cell[i];
+      for (int o = 0; o < 14; o++) {
+        int q = o == 0 ? 13 : 13 + o;
+        int4 cc = make_int4(c.x + q % 3 - 1, c.y + (q / 3) % 3 - 1, c.z + q / 9 - 1, 0);
+        uint32_t h = cellHash(cc, p.tableMask);
+        uint32_t end = w.cellEnd[h];
+        for (uint32_t k = w.cellStart[h]; k < end; k++) {
+          int4 cj = w.sortedCell[k];
+          uint32_t j = (uint32_t)cj.w & 0x7fffffffu;
+          bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
+          if (o == 0 && j >= i) continue;
+          if (!dyn && !dj) continue;
+          if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
+          float4 pr = w.sortedPR[k];
+          float3 d = P.pos - make_float3(pr.x, pr.y, pr.z);
+          float r = P.radius + pr.w;
+          if (dot3(d, d) > r * r) continue;
+          float4 ab = w.sortedAabb[k];
+          if (fabsf(d.x) > P.aabb.x + ab.x + 1e-4f || fabsf(d.y) > P.aabb.y + ab.y + 1e-4f || fabsf(d.z) > P.aabb.z + ab.z + 1e-4f) continue;
+          testFromProber(w, p, P, j);
+        }
+      }
+      if (dyn || p.anyDynamicLarge) {
+        for (uint32_t k = 0; k < p.nLarge; k++) {
+          uint32_t l = w.large[k];
+          if (!dyn && (!enabled(w, l) || w.size[l].w <= 0.0f)) continue;
+          testPair(w, p, P, l);
+        }
+      }
+    } else if (dyn) {
+      for (uint32_t k = 0; k < p.nLarge; k++) {
+        uint32_t l = w.large[k];
+        if (l == i || (l < i && w.size[l].w > 0.0f)) continue;
+        testPair(w, p, P, l);
+      }
+    }
+  }
+}
+
+namespace {
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[64] = {};
+}  // namespace
+
+}  // namespace avbd
+
+extern "C" int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, const uint32_t* groups_mask, uint32_t* pairs_ab, uint32_t cap,
+                                       uint32_t* count, void* stream) {
+  using namespace avbd;
+  using L = NoAllocLayout;
+  if (count) *count = 0;
+  if ((n && !bodies) || (cap && !pairs_ab) || !count) return AVBD_ERR_INVALID;
+  if (n > NOALLOC_MAX_BODIES) return AVBD_ERR_CAPACITY;  // at most AVBD_NOALLOC_MAX_BODIES bodies
+  if (!bodyProblem(bodies, n).empty()) return AVBD_ERR_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return AVBD_ERR_NO_DEVICE;
+  unsigned char* base = nullptr;
+  {
+    // once per device, with that device current: the scratch array's address on it
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      void* ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return AVBD_ERR_CUDA;
+      g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    base = g_noalloc_ptr[dev];
+  }
+  if (n == 0) return AVBD_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the broadphase configuration of uploadStatics (solver.ts:1263-1318), from the radii
+  std::vector<double> radii(n);
+  for (uint32_t i = 0; i < n; i++) radii[i] = bodies[i].radius;
+  const double maxSmall = largestSmall(radii);
+  const float threshold = float(largeThreshold(radii));
+  std::vector<uint32_t> large;
+  uint32_t anyDynamicLarge = 0;
+  for (uint32_t i = 0; i < n; i++)
+    if (bodies[i].radius > threshold) {
+      large.push_back(i);
+      if (bodies[i].mass > 0.0f) anyDynamicLarge = 1;
+    }
+  DWorld w{};
+  w.pos = reinterpret_cast<float4*>(base + L::POS);
+  w.rot = reinterpret_cast<float4*>(base + L::ROT);
+  w.ipos = reinterpret_cast<float4*>(base + L::IPOS);
+  w.size = reinterpret_cast<float4*>(base + L::SIZE);
+  w.moment = reinterpret_cast<float4*>(base + L::MOMENT);
+  w.avel = reinterpret_cast<float4*>(base + L::AVEL);
+  w.filters = reinterpret_cast<uint2*>(base + L::FILTERS);
+  w.cell = reinterpret_cast<int4*>(base + L::CELL);
+  w.cellStart = reinterpret_cast<uint32_t*>(base + L::START);
+  w.cellEnd = reinterpret_cast<uint32_t*>(base + L::END);
+  w.sortedPR = reinterpret_cast<float4*>(base + L::SPR);
+  w.sortedCell = reinterpret_cast<int4*>(base + L::SCELL);
+  w.sortedAabb = reinterpret_cast<float4*>(base + L::SAABB);
+  w.large = reinterpret_cast<uint32_t*>(base + L::LARGE);
+  w.pairs = reinterpret_cast<uint2*>(base + L::PAIRS);
+  w.counters = reinterpret_cast<uint32_t*>(base + L::COUNTERS);
+  StepParams p{};
+  p.n = n;
+  p.largeThreshold = threshold;
+  p.cellSize = float(std::max(2.0 * maxSmall * (1 + 1e-4), 1e-3));
+  p.tableMask = NOALLOC_TABLE - 1u;
+  p.nLarge = uint32_t(large.size());
+  p.anyDynamicLarge = anyDynamicLarge;
+  p.pairCap = NOALLOC_MAX_PAIRS;
+  p.nNoCollide = 0;
+  // the record fields the pair rule reads, strided out of the host records
+  const size_t fieldIndex[6] = {0, 1, 2, 4, 5, 9};
+  float4* fields[6] = {w.pos, w.rot, w.ipos, w.size, w.moment, w.avel};
+  for (int f = 0; f < 6; f++)
+    if (cudaMemcpy2DAsync(fields[f], sizeof(float4), reinterpret_cast<const char*>(bodies) + fieldIndex[f] * sizeof(float4), sizeof(avbd_body), sizeof(float4),
+                          n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return AVBD_ERR_CUDA;
+  cudaError_t e = groups_mask ? cudaMemcpyAsync(w.filters, groups_mask, size_t(n) * sizeof(uint2), cudaMemcpyHostToDevice, s)
+                              : cudaMemsetAsync(w.filters, 0xff, size_t(n) * sizeof(uint2), s);
+  if (e != cudaSuccess) return AVBD_ERR_CUDA;
+  if (!large.empty() && cudaMemcpyAsync(w.large, large.data(), large.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return AVBD_ERR_CUDA;
+  k_find_pairs_noalloc<<<1, NOALLOC_THREADS, 0, s>>>(w, p, reinterpret_cast<uint32_t*>(base + L::KEY), reinterpret_cast<uint32_t*>(base + L::RANK));
+  if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
+  uint32_t found = 0;
+  if (cudaMemcpyAsync(&found, w.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return AVBD_ERR_CUDA;
+  // the host sources above must outlive their copies, and the count is needed below
+  if (cudaStreamSynchronize(s) != cudaSuccess) return AVBD_ERR_CUDA;
+  *count = found;
+  const uint32_t k = std::min(std::min(found, cap), NOALLOC_MAX_PAIRS);
+  if (k && (cudaMemcpyAsync(pairs_ab, w.pairs, size_t(k) * sizeof(uint2), cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess))
+    return AVBD_ERR_CUDA;
+  return found > NOALLOC_MAX_PAIRS || found > cap ? AVBD_ERR_CAPACITY : AVBD_OK;
+}
