@@ -37,6 +37,7 @@ METRIC = 'body-steps/s @100k boxes'
 UNIT = 'body-steps/s'
 PILE_BODIES = 100_000
 SAMPLE_BODIES = 2_000
+PILE_SPACING = 2.7
 ROLLOUT = 600
 L2_FLUSH_BYTES = 256 << 20
 
@@ -257,6 +258,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='cuda', choices=['cuda', 'reference'])
     ap.add_argument('--bodies', type=int, default=PILE_BODIES)
+    ap.add_argument('--spacing', type=float, default=PILE_SPACING,
+                    help='lattice spacing of the pile (1.15: bodies start touching, the dense case the profiles capture)')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-graphs', action='store_true', help='launch each kernel directly instead of replaying the step graph')
@@ -290,7 +293,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    scene = drop_pile(args.bodies, seed=1)
+    scene = drop_pile(args.bodies, seed=1, spacing=args.spacing)
     n_dyn = scene.dynamic_count
 
     def fresh():
@@ -392,7 +395,7 @@ def main():
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world_size, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
-            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps), parallelism=f'replicas x{world_size}'),
+            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps), parallelism=f'replicas x{world_size}', spacing=args.spacing),
             'roofline': {'bound': 'hbm', 'kernel': 'k_topology_solve', 'achieved': achieved, 'peak': peak, 'peak_kind': peak_kind, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / max(len(stats), 1)},
             'phases_ms_per_step': {'collision': coll_ms / max(len(stats), 1), 'topology_solve': solve_ms / max(len(stats), 1)},

@@ -29,6 +29,8 @@ constexpr uint32_t FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_START_AT_RES
 constexpr float REST_SPEED = 0.1f;
 constexpr float NEAREST_FRACTION = 0.05f;
 constexpr uint32_t OWNER_BIT = 0x80000000u;  // incidence entry: this body updates the constraint's dual
+// incidence partner word: index | PARTNER_DYNAMIC | PARTNER_EARLIER (its colour comes first in the sweep)
+constexpr uint32_t PARTNER_DYNAMIC = 0x80000000u, PARTNER_EARLIER = 0x40000000u, PARTNER_MASK = 0x3fffffffu;
 constexpr int LANE_CLASSES = 6;                // 1, 2, 4, 8, 16, 32 lanes per body
 constexpr int BUCKETS = MAX_COLORS * LANE_CLASSES;
 constexpr int BUCKET_WORDS = 5 * BUCKETS;  // counts | starts + total | fill cursors | lane bases | lane totals (64)
@@ -46,7 +48,7 @@ constexpr int CLOCK_T0 = MAX_CLOCKS + 1, CLOCK_WORDS = MAX_CLOCKS + 2;
 constexpr int STAT_WORDS = 16;    // collision ns, solve ns, then counters (pairs, contacts, manifolds, adjacency, incidences, dynamic, colours, rounds, launches, error)
 constexpr int C_STATS_NEXT = 13;  // counter word: next ring entry
 // Error bits
-constexpr uint32_t ERR_BARRIER_TIMEOUT = 1, ERR_ADJ_OVERFLOW = 2, ERR_INC_OVERFLOW = 4;
+constexpr uint32_t ERR_BARRIER_TIMEOUT = 1, ERR_ADJ_OVERFLOW = 2, ERR_INC_OVERFLOW = 4, ERR_DEPENDENCY_TIMEOUT = 8;
 
 // Joint record words (layout.ts:84-110), as float4 slots
 enum : int { J_PEN_LIN = 0, J_PEN_ANG = 1, J_LAM_LIN = 2, J_LAM_ANG = 3, J_C0_LIN = 4, J_C0_ANG = 5, J_RA = 6, J_RB = 7, J_REST = 8, J_REST_START = 9, JOINT_VEC4 = 10 };
@@ -95,7 +97,9 @@ struct DWorld {
   uint4* adjList;  // per (body, constraint): sort key hi, key lo, constraint | rows << 28, other | dynamic << 31
   uint32_t *colorA, *colorB, *colorHist, *colorStart, *colorBodies, *fixedColor;
   uint32_t *incCount, *incStart;
-  uint2* incList;         // per incidence: constraint row (joint slot, or nj + point slot) | OWNER_BIT, partner body
+  uint2* incList;         // per incidence: constraint row (joint slot, or nj + point slot) | OWNER_BIT, partner word
+  uint32_t* done;         // per body: iterations finished in this step's dataflow sweep
+  uint4* laneTable;       // per lane of the dataflow sweep: body, first row, row end, L | sub << 8
   uint32_t* bucket;       // BUCKET_WORDS: counts, starts (+ total), fill cursors, lane bases, lane totals per colour
   float4 *dlin, *dang;    // per body: position and rotation change since x- (kept by the solve)
   uint32_t* scanScratch;
@@ -142,6 +146,8 @@ __host__ __device__ inline DWorld worldView(const DWorld& b, const WorldDesc& d,
   v.colorB += d.body;
   v.colorBodies += d.body;
   v.fixedColor += d.body;
+  v.done = nullptr;
+  v.laneTable = nullptr;
   v.incCount += d.body;
   v.incStart += d.body + wi;
   v.incList += d.inc;

@@ -134,6 +134,7 @@ int allocPairs(avbd_world* w, uint32_t cap) {
   dfree(w, d.hash);
   dfree(w, d.adjList);
   dfree(w, d.incList);
+  dfree(w, d.laneTable);
   w->pairCap = cap;
   w->configGen++;
   w->hashSize = pow2AtLeast(2ull * cap);
@@ -143,6 +144,7 @@ int allocPairs(avbd_world* w, uint32_t cap) {
   CUDA_TRY(w, dalloc(w, &d.hash, w->hashSize));
   CUDA_TRY(w, dalloc(w, &d.adjList, w->adjCap));
   CUDA_TRY(w, dalloc(w, &d.incList, w->incCap));
+  CUDA_TRY(w, dalloc(w, &d.laneTable, w->incCap));
   for (int b = 0; b < 2; b++) {
     CUDA_TRY(w, dalloc(w, &d.mIds[b], cap));
     CUDA_TRY(w, dalloc(w, &d.mGeo[b], cap));
@@ -187,10 +189,12 @@ int allocJoints(avbd_world* w, uint32_t cap) {
   // adjacency and incidence lists are sized by the joint capacity too
   dfree(w, d.adjList);
   dfree(w, d.incList);
+  dfree(w, d.laneTable);
   w->adjCap = 2u * (w->pairCap + w->jointCap);
   w->incCap = 2u * (w->pairCap * MAX_CONTACTS + w->jointCap);
   CUDA_TRY(w, dalloc(w, &d.adjList, w->adjCap));
   CUDA_TRY(w, dalloc(w, &d.incList, w->incCap));
+  CUDA_TRY(w, dalloc(w, &d.laneTable, w->incCap));
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   return AVBD_OK;
 }
@@ -359,6 +363,10 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   cudaSetDevice(w->device);
   avbd_default_params(&w->params);
   w->bodyCap = cfg && cfg->body_capacity ? cfg->body_capacity : 1024;
+  if (w->bodyCap > (1u << 30)) {  // body indices share a word with two flag bits in the incidence list
+    delete w;
+    return AVBD_ERR_INVALID;
+  }
   w->jointCap = cfg && cfg->joint_capacity ? cfg->joint_capacity : 256;
   uint32_t pairCap = cfg && cfg->pair_capacity ? cfg->pair_capacity : std::max<uint32_t>(65536, 8 * w->bodyCap);
   auto bad = [&](int code) {
@@ -400,6 +408,7 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.bucket, BUCKET_WORDS));
   A(dalloc(w, &d.dlin, B));
   A(dalloc(w, &d.dang, B));
+  A(dalloc(w, &d.done, B));
   A(dalloc(w, &d.scanScratch, w->solveBlocks + 1));
   A(dalloc(w, &d.counters, COUNTER_WORDS));
   A(dalloc(w, &d.barrier, 2));

@@ -69,7 +69,7 @@ __device__ bool grid_sync(uint32_t* bar, uint32_t* counters) {
     } else {
       long long t0 = clock64();
       while (ld_acquire_gpu(bar) < target) {
-        if (ldv(&counters[C_ERROR]) & ERR_BARRIER_TIMEOUT) { ab = 1; break; }
+        if (ldv(&counters[C_ERROR]) & (ERR_BARRIER_TIMEOUT | ERR_DEPENDENCY_TIMEOUT)) { ab = 1; break; }
         if (clock64() - t0 > BARRIER_CYCLES) {
           atomicOr(&counters[C_ERROR], ERR_BARRIER_TIMEOUT);
           ab = 1;
@@ -121,6 +121,7 @@ __device__ uint32_t block_scan_range(uint32_t* data, uint32_t lo, uint32_t hi) {
 // The two scopes the topology+solve code runs at: the whole grid (one large world, cooperative
 // launch, bounded grid barriers) or one block (one small world of a batch, __syncthreads).
 struct GridTeam {
+  static constexpr bool kDataflow = true;  // colour passes as a dataflow sweep (no grid barrier per colour)
   uint32_t* bar;
   uint32_t* ctr;
   __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -130,6 +131,7 @@ struct GridTeam {
   __device__ bool sync() { return grid_sync(bar, ctr); }
 };
 struct BlockTeam {
+  static constexpr bool kDataflow = false;  // a block's __syncthreads per colour costs little
   __device__ uint32_t rank() const { return threadIdx.x; }
   __device__ uint32_t size() const { return blockDim.x; }
   __device__ uint32_t block() const { return 0; }
@@ -510,7 +512,7 @@ __device__ inline void accumulateIncidence(Acc& acc, const DWorld& w, const Step
     return;
   }
   PointView v;
-  loadPoint(w, p, id - p.nj, i, inc.y, v);
+  loadPoint(w, p, id - p.nj, i, inc.y & PARTNER_MASK, v);
   const Pose& A = v.isA ? own : v.other;
   const Pose& B = v.isA ? v.other : own;
   ContactEval e;
@@ -533,7 +535,7 @@ __device__ inline void dualIncidence(const DWorld& w, const StepParams& p, uint2
   }
   uint32_t cs = id - p.nj;
   PointView v;
-  loadPoint(w, p, cs, i, inc.y, v);
+  loadPoint(w, p, cs, i, inc.y & PARTNER_MASK, v);
   const Pose& A = v.isA ? own : v.other;
   const Pose& B = v.isA ? v.other : own;
   ContactEval e;
@@ -566,6 +568,167 @@ __device__ inline uint32_t laneClass(uint32_t rows, uint32_t perLane) {
 constexpr int B_COUNT = 0, B_START = BUCKETS, B_FILL = 2 * BUCKETS + 1, B_LANE = 3 * BUCKETS + 1, B_LANE_TOTAL = 4 * BUCKETS + 1,
               B_ROWS = B_LANE_TOTAL + MAX_COLORS;
 static_assert(B_ROWS + MAX_COLORS <= BUCKET_WORDS, "bucket words");
+
+// Waits until body b has finished `need` iterations (its done count, published with release
+// semantics after its pose and owned rows are written). Bounded: past the clock budget, or once any
+// wait of the launch gave up, it returns false.
+__device__ inline bool waitDone(const DWorld& w, uint32_t b, uint32_t need) {
+  if (ld_acquire_gpu(w.done + b) >= need) return true;
+  const long long t0 = clock64();
+  for (uint32_t n = 1;; n++) {
+    if (n > 64u) __nanosleep(32);
+    if (ld_acquire_gpu(w.done + b) >= need) return true;
+    if ((n & 15u) == 0u) {
+      if (ldv(&w.counters[C_ERROR]) & ERR_DEPENDENCY_TIMEOUT) return false;
+      if (clock64() - t0 > BARRIER_CYCLES) {
+        atomicOr(&w.counters[C_ERROR], ERR_DEPENDENCY_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// What one lane does in a chunk: its group's body, its first row (the group's rows are dealt
+// round-robin to the group's L lanes), the end of the body's rows, and its place in the group.
+struct LaneJob {
+  bool active;
+  uint32_t body, e, e1, L, sub;
+};
+__device__ __forceinline__ LaneJob jobFromEntry(uint4 t, bool active) {
+  LaneJob J;
+  J.active = active;
+  J.body = t.x;
+  J.e = t.y;
+  J.e1 = t.z;
+  J.L = active ? (t.w & 0xffu) : 1u;
+  J.sub = active ? (t.w >> 8) : 0u;
+  return J;
+}
+
+// Lane `base + lane` of colour c's lane space, from the colour's bucket tables: bucket j of the
+// colour holds bodies of 32 >> j lanes each.
+__device__ __forceinline__ LaneJob laneJob(const DWorld& w, uint32_t c, uint32_t base, const uint32_t* s_lane, const uint32_t* s_start,
+                                           const uint32_t* s_total) {
+  const uint32_t lam = base + (threadIdx.x & 31u);
+  const uint32_t* laneBase = s_lane + c * LANE_CLASSES;
+  LaneJob J;
+  J.active = lam < s_total[c];
+  uint32_t j = 0;
+  if (J.active)
+    while (j + 1 < (uint32_t)LANE_CLASSES && lam >= laneBase[j + 1]) j++;
+  J.L = J.active ? (32u >> j) : 1u;
+  const uint32_t local = J.active ? lam - laneBase[j] : 0u;
+  J.sub = local & (J.L - 1u);
+  J.body = J.e = J.e1 = 0;
+  if (J.active) {
+    const uint32_t s = s_start[c * LANE_CLASSES + j] + (local >> (5u - j));
+    J.body = w.colorBodies[s];
+    J.e = w.incStart[s] + J.sub;
+    J.e1 = w.incStart[s + 1];
+  }
+  return J;
+}
+
+// One 32-lane chunk: each group of lanes (one body) accumulates its rows, sums them by butterfly, its
+// first lane solves and writes the pose, and the lanes update the rows the body owns. With kWait the
+// chunk first waits for the bodies it reads and afterwards publishes its bodies' iteration count;
+// false: a wait gave up (warp-uniform).
+template <bool kWait>
+__device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p, const LaneJob& J, uint32_t it) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const float dt2 = p.dt * p.dt;
+  const bool active = J.active;
+  const uint32_t L = J.L, sub = J.sub, body = J.body, e1 = J.e1;
+  const uint32_t leader = lane - sub;
+  if constexpr (kWait) {
+    bool ok = true;
+    if (active) {
+      ok = waitDone(w, body, it);
+      for (uint32_t e = J.e; e < e1 && ok; e += L) {
+        const uint2 inc = w.incList[e];
+        // a partner of the same colour (only where the colour cap forced a clash) is not waited for
+        // within the iteration: the colour-by-colour sweep runs such pairs side by side too
+        if (inc.y & PARTNER_DYNAMIC) ok = waitDone(w, inc.y & PARTNER_MASK, it + ((inc.y & PARTNER_EARLIER) ? 1u : 0u));
+      }
+    }
+    if (__any_sync(0xffffffffu, !ok)) return false;
+  }
+  Pose own;
+  Acc acc;
+  accZero(acc);
+  float3 x0 = make_float3(0.0f, 0.0f, 0.0f);
+  if (active) {
+    float4 pos = w.pos[body];
+    own.x = f3(pos);
+    own.q = w.rot[body];
+    own.q0 = w.irot[body];
+    own.dLin = f3(w.dlin[body]);
+    own.dAng = f3(w.dang[body]);
+    if (sub == 0) {
+      x0 = f3(w.ipos[body]);
+      float m = w.size[body].w / dt2;
+      float3 I = f3(w.moment[body]) / dt2;
+      acc.v[0] = m;
+      acc.v[3] = m;
+      acc.v[5] = m;
+      acc.v[6] = I.x;
+      acc.v[9] = I.y;
+      acc.v[11] = I.z;
+      float3 rl = (own.x - f3(w.ypos[body])) * m;
+      float3 ra = I * qsub(own.q, w.yrot[body]);
+      acc.v[21] = rl.x;
+      acc.v[22] = rl.y;
+      acc.v[23] = rl.z;
+      acc.v[24] = ra.x;
+      acc.v[25] = ra.y;
+      acc.v[26] = ra.z;
+    }
+    for (uint32_t e = J.e; e < e1; e += L) accumulateIncidence(acc, w, p, w.incList[e], body, own);
+  }
+  // butterfly over the group: as many rounds as the warp's widest group needs
+  const uint32_t Lmax = __reduce_max_sync(0xffffffffu, L);
+  for (uint32_t off = Lmax >> 1; off > 0; off >>= 1) {
+    const bool take = off < L;
+#pragma unroll
+    for (int k = 0; k < 27; k++) {
+      float o = __shfl_xor_sync(0xffffffffu, acc.v[k], off);
+      if (take) acc.v[k] += o;
+    }
+  }
+  float3 x = own.x, dl = own.dLin, da = own.dAng;
+  float4 q = own.q;
+  if (active && sub == 0) {
+    finishBody(acc, x, q);
+    dl = x - x0;
+    da = qsub(q, own.q0);
+    w.pos[body] = make_float4(x.x, x.y, x.z, w.pos[body].w);
+    w.rot[body] = q;
+    w.dlin[body] = make_float4(dl.x, dl.y, dl.z, 0.0f);
+    w.dang[body] = make_float4(da.x, da.y, da.z, 0.0f);
+  }
+  own.x = make_float3(__shfl_sync(0xffffffffu, x.x, leader), __shfl_sync(0xffffffffu, x.y, leader), __shfl_sync(0xffffffffu, x.z, leader));
+  own.q = make_float4(__shfl_sync(0xffffffffu, q.x, leader), __shfl_sync(0xffffffffu, q.y, leader), __shfl_sync(0xffffffffu, q.z, leader),
+                      __shfl_sync(0xffffffffu, q.w, leader));
+  own.dLin = make_float3(__shfl_sync(0xffffffffu, dl.x, leader), __shfl_sync(0xffffffffu, dl.y, leader), __shfl_sync(0xffffffffu, dl.z, leader));
+  own.dAng = make_float3(__shfl_sync(0xffffffffu, da.x, leader), __shfl_sync(0xffffffffu, da.y, leader), __shfl_sync(0xffffffffu, da.z, leader));
+  if (active) {
+    for (uint32_t e = J.e; e < e1; e += L) {
+      uint2 inc = w.incList[e];
+      if (inc.x & OWNER_BIT) dualIncidence(w, p, inc, body, own);
+    }
+  }
+  if constexpr (kWait) {
+    // the group's writes (the leader's pose, every lane's rows) are ordered before the leader's
+    // release by the warp barrier, as the grid barrier orders a block's writes before its arrival
+    __syncwarp();
+    if (active && sub == 0) st_release_gpu(w.done + body, it + 1u);
+  }
+  return true;
+}
 
 // --- the kernel -----------------------------------------------------------------------------------------------
 template <class Team>
@@ -802,17 +965,45 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     for (uint32_t e = w.adjStart[b]; e < w.adjStart[b + 1]; e++) {
       uint4 ent = w.adjList[e];
       uint32_t c = ent.z & 0x0fffffffu, cnt = ent.z >> 28;
-      bool owner = true;
+      bool owner = true, earlier = false;
       if (ent.w & 0x80000000u) {
         uint32_t other = ent.w & 0x7fffffffu;
         uint32_t colO = w.colorA[other] & 0xffu;
-        owner = colO < colB || (colO == colB && other < b);
+        earlier = colO < colB;
+        owner = earlier || (colO == colB && other < b);
       }
       uint32_t flag = owner ? OWNER_BIT : 0u;
-      uint32_t partner = ent.w & 0x7fffffffu;
+      uint32_t partner = ent.w | (earlier ? PARTNER_EARLIER : 0u);
       if (c < nj) w.incList[out++] = make_uint2(c | flag, partner);
       else
         for (uint32_t k = 0; k < cnt; k++) w.incList[out++] = make_uint2((nj + (c - nj) * MAX_CONTACTS + k) | flag, partner);
+    }
+  }
+  if constexpr (Team::kDataflow) {
+    // the lane table of the dataflow sweep: per colour, its lanes in lane-space order, each with its
+    // body, first row, the body's row end and (L, sub)
+    __shared__ uint32_t s_colOff[MAX_COLORS + 1];
+    if (threadIdx.x == 0) {
+      uint32_t lanes = 0;
+      for (uint32_t c = 0; c <= (uint32_t)MAX_COLORS; c++) {
+        s_colOff[c] = lanes;
+        if (c < (uint32_t)MAX_COLORS) lanes += w.bucket[B_LANE_TOTAL + c];
+      }
+    }
+    __syncthreads();
+    if (s_colOff[MAX_COLORS] > p.incCap) {
+      if (tid == 0) atomicOr(&ctr[C_ERROR], ERR_INC_OVERFLOW);
+      return;  // uniform: every block sums the same totals
+    }
+    for (uint32_t s = tid; s < numDyn; s += T) {
+      const uint32_t b = w.colorBodies[s];
+      const uint32_t col = w.colorA[b] & 0xffu;
+      const uint32_t k = laneClass(w.incCount[b], s_perLane[col]);
+      const uint32_t bucket = col * LANE_CLASSES + (LANE_CLASSES - 1u - k);
+      const uint32_t L = 1u << k;
+      const uint32_t first = s_colOff[col] + w.bucket[B_LANE + bucket] + (s - w.bucket[B_START + bucket]) * L;
+      const uint32_t e0 = w.incStart[s], e1 = w.incStart[s + 1];
+      for (uint32_t q = 0; q < L; q++) w.laneTable[first + q] = make_uint4(b, e0 + q, e1, L | (q << 8));
     }
   }
 
@@ -842,6 +1033,7 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   const float dt = p.dt, g = p.gravity;
   const float3 up = make_float3(p.upx, p.upy, p.upz);
   for (uint32_t i = tid; i < n; i += T) {
+    if constexpr (Team::kDataflow) w.done[i] = 0u;
     if (!enabledBody(w, i)) continue;
     float4 pos = w.pos[i], rot = w.rot[i], vel = w.vel[i];
     float3 av = f3(w.avel[i]);
@@ -877,102 +1069,62 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   // G. iterations: per colour, each body's group of lanes (its lane class) accumulates its rows, the
   // group sums in registers, the first lane solves, and every lane then updates the rows it owns.
   // The colours' lane tables (lane bases, bucket starts, lane totals) are kept in shared memory.
-  __shared__ uint32_t s_lane[BUCKETS], s_start[BUCKETS], s_total[MAX_COLORS];
+  __shared__ uint32_t s_lane[BUCKETS], s_start[BUCKETS], s_total[MAX_COLORS], s_chunk[MAX_COLORS + 1], s_laneOff[MAX_COLORS + 1];
   for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) {
     s_lane[k] = w.bucket[B_LANE + k];
     s_start[k] = w.bucket[B_START + k];
   }
   if (threadIdx.x < (uint32_t)MAX_COLORS) s_total[threadIdx.x] = w.bucket[B_LANE_TOTAL + threadIdx.x];
   __syncthreads();
-  const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warpGlobal = tid >> 5, nwarps = T >> 5;
-  const float dt2 = dt * dt;
-  for (int it = 0; it < p.iterations; it++) {
-    for (uint32_t c = 0; c < numColors; c++) {
-      const uint32_t laneTotal = s_total[c];
-      const uint32_t* laneBase = s_lane + c * LANE_CLASSES;
-      const uint32_t* bucketStart = s_start + c * LANE_CLASSES;
-      for (uint32_t base = warpGlobal * 32u; base < laneTotal; base += nwarps * 32u) {
-        const uint32_t lam = base + lane;
-        const bool active = lam < laneTotal;
-        uint32_t j = 0;
-        if (active)
-          while (j + 1 < (uint32_t)LANE_CLASSES && lam >= laneBase[j + 1]) j++;
-        const uint32_t L = active ? (32u >> j) : 1u;
-        const uint32_t local = active ? lam - laneBase[j] : 0u;
-        const uint32_t sub = local & (L - 1u);
-        const uint32_t leader = lane - sub;
-        uint32_t body = 0, e0 = 0, e1 = 0;
-        Pose own;
-        Acc acc;
-        accZero(acc);
-        float3 x0 = make_float3(0.0f, 0.0f, 0.0f);
-        if (active) {
-          const uint32_t s = bucketStart[j] + (local >> (5u - j));
-          body = w.colorBodies[s];
-          e0 = w.incStart[s];
-          e1 = w.incStart[s + 1];
-          float4 pos = w.pos[body];
-          own.x = f3(pos);
-          own.q = w.rot[body];
-          own.q0 = w.irot[body];
-          own.dLin = f3(w.dlin[body]);
-          own.dAng = f3(w.dang[body]);
-          if (sub == 0) {
-            x0 = f3(w.ipos[body]);
-            float m = w.size[body].w / dt2;
-            float3 I = f3(w.moment[body]) / dt2;
-            acc.v[0] = m;
-            acc.v[3] = m;
-            acc.v[5] = m;
-            acc.v[6] = I.x;
-            acc.v[9] = I.y;
-            acc.v[11] = I.z;
-            float3 rl = (own.x - f3(w.ypos[body])) * m;
-            float3 ra = I * qsub(own.q, w.yrot[body]);
-            acc.v[21] = rl.x;
-            acc.v[22] = rl.y;
-            acc.v[23] = rl.z;
-            acc.v[24] = ra.x;
-            acc.v[25] = ra.y;
-            acc.v[26] = ra.z;
-          }
-          for (uint32_t e = e0 + sub; e < e1; e += L) accumulateIncidence(acc, w, p, w.incList[e], body, own);
-        }
-        // butterfly over the group: as many rounds as the warp's widest group needs
-        const uint32_t Lmax = __reduce_max_sync(0xffffffffu, L);
-        for (uint32_t off = Lmax >> 1; off > 0; off >>= 1) {
-          const bool take = off < L;
-#pragma unroll
-          for (int k = 0; k < 27; k++) {
-            float o = __shfl_xor_sync(0xffffffffu, acc.v[k], off);
-            if (take) acc.v[k] += o;
-          }
-        }
-        float3 x = own.x, dl = own.dLin, da = own.dAng;
-        float4 q = own.q;
-        if (active && sub == 0) {
-          finishBody(acc, x, q);
-          dl = x - x0;
-          da = qsub(q, own.q0);
-          w.pos[body] = make_float4(x.x, x.y, x.z, w.pos[body].w);
-          w.rot[body] = q;
-          w.dlin[body] = make_float4(dl.x, dl.y, dl.z, 0.0f);
-          w.dang[body] = make_float4(da.x, da.y, da.z, 0.0f);
-        }
-        own.x = make_float3(__shfl_sync(0xffffffffu, x.x, leader), __shfl_sync(0xffffffffu, x.y, leader), __shfl_sync(0xffffffffu, x.z, leader));
-        own.q = make_float4(__shfl_sync(0xffffffffu, q.x, leader), __shfl_sync(0xffffffffu, q.y, leader), __shfl_sync(0xffffffffu, q.z, leader),
-                            __shfl_sync(0xffffffffu, q.w, leader));
-        own.dLin = make_float3(__shfl_sync(0xffffffffu, dl.x, leader), __shfl_sync(0xffffffffu, dl.y, leader), __shfl_sync(0xffffffffu, dl.z, leader));
-        own.dAng = make_float3(__shfl_sync(0xffffffffu, da.x, leader), __shfl_sync(0xffffffffu, da.y, leader), __shfl_sync(0xffffffffu, da.z, leader));
-        if (active) {
-          for (uint32_t e = e0 + sub; e < e1; e += L) {
-            uint2 inc = w.incList[e];
-            if (inc.x & OWNER_BIT) dualIncidence(w, p, inc, body, own);
-          }
-        }
+  if constexpr (Team::kDataflow) {
+    // Dataflow sweep: the iterations' colour passes as one ordered list of 32-lane chunks, dealt to
+    // the warps in turn. A chunk waits only for the bodies its rows touch (a body of an earlier colour
+    // to finish this iteration, one of a later colour the previous iteration; the body itself its
+    // previous iteration), so every read sees exactly what the colour-by-colour sweep reads, and the
+    // colours overlap instead of meeting at grid barriers. Every wait is on chunks earlier in the
+    // list, and each warp takes its chunks in list order, so the earliest unfinished chunk can
+    // always run.
+    if (threadIdx.x == 0) {
+      uint32_t acc = 0, lanes = 0;
+      for (uint32_t c = 0; c < numColors; c++) {
+        s_chunk[c] = acc;
+        s_laneOff[c] = lanes;
+        acc += (s_total[c] + 31u) / 32u;
+        lanes += s_total[c];
       }
-      GSYNC
+      s_chunk[numColors] = acc;
+      s_laneOff[numColors] = lanes;
+    }
+    __syncthreads();
+    const uint32_t perIter = s_chunk[numColors];
+    const uint32_t items = perIter * (uint32_t)max(p.iterations, 0);
+    // chunk k's lane entry, fetched one chunk ahead (the lane table is fixed for the step)
+    auto entryOf = [&](uint32_t k, bool& active) -> uint4 {
+      active = false;
+      if (k >= items) return make_uint4(0u, 0u, 0u, 1u);
+      const uint32_t r = k % perIter;
+      uint32_t c = 0;
+      while (s_chunk[c + 1] <= r) c++;
+      const uint32_t lam = (r - s_chunk[c]) * 32u + (threadIdx.x & 31u);
+      active = lam < s_total[c];
+      return active ? w.laneTable[s_laneOff[c] + lam] : make_uint4(0u, 0u, 0u, 1u);
+    };
+    bool nextActive;
+    uint4 next = entryOf(warpGlobal, nextActive);
+    for (uint32_t k = warpGlobal; k < items; k += nwarps) {
+      const LaneJob J = jobFromEntry(next, nextActive);
+      next = entryOf(k + nwarps, nextActive);
+      if (!solveLanes<true>(w, p, J, k / perIter)) break;
+    }
+    GSYNC
+  } else {
+    for (int it = 0; it < p.iterations; it++) {
+      for (uint32_t c = 0; c < numColors; c++) {
+        for (uint32_t base = warpGlobal * 32u; base < s_total[c]; base += nwarps * 32u)
+          solveLanes<false>(w, p, laneJob(w, c, base, s_lane, s_start, s_total), (uint32_t)it);
+        GSYNC
+      }
     }
   }
 
