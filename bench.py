@@ -251,6 +251,51 @@ def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, di
     }
 
 
+def run_hulls(args, local: int, rank: int, world_size: int, barrier, torch, dist) -> dict:
+    """Config 3: 20k convex hulls falling onto 1000 jointed chains of 50 boxes, 15 iterations."""
+    import avbd_b200
+    from avbd_b200.scenes import hulls_and_chains
+
+    scene = hulls_and_chains(args.hulls, args.chains, 50, seed=9 + rank)
+    w = avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
+    w.step(args.warmup)
+    w.synchronize()
+    steps = args.hull_steps
+    w.enable_step_stats(steps)
+    stream = torch.cuda.ExternalStream(w.stream, device=local)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            w.step(1)
+            flush.zero_()
+        e1.record(stream)
+    w.synchronize()
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    st = w.read_step_stats()
+    c = w.read_counters()
+    joints, _ = w.read_joints()
+    broken = int((joints['stiffness_lin'] == 0).sum())
+    dyn = scene.dynamic_count
+    w.destroy()
+    return {
+        'metric': 'body-steps/s', 'value': world_size * dyn * steps / (ms / 1000.0), 'ms_per_step': ms / steps, 'steps': steps,
+        'dynamic_bodies': dyn, 'hull_records': len(scene.hull_offsets), 'joints': len(joints), 'joints_broken': broken,
+        'phases_ms_per_step': {'collision': float(st['collision_ms'].mean()), 'topology_solve': float(st['solve_ms'].mean())},
+        'last_step': {k: int(st[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors')}, 'error': c['error'], 'overflow': c['overflow'],
+        'config': {'workload': f'{args.hulls} hulls (hull of 8-32 points on an ellipsoid, semi-axes U[0.3,1.0]; 512 distinct shapes) falling '
+                               f'onto {args.chains} chains of 50 boxes (0.2x0.2x0.5) with ball joints breaking at 1e4 N on pull, hung from static '
+                               f'anchors; static ground; dt 1/60, 15 iterations; timed steps {args.warmup + 1}..{args.warmup + steps}',
+                   'seed': 9 + rank, 'l2': '256 MiB memset between timed steps, inside the timed region'},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -266,6 +311,9 @@ def main():
     ap.add_argument('--batched-worlds', type=int, default=4096, help='worlds of the batched workload (0: skip it)')
     ap.add_argument('--batched-steps', type=int, default=300)
     ap.add_argument('--plain-sample', type=int, default=64, help='worlds stepped one by one for the per-world comparison')
+    ap.add_argument('--hull-steps', type=int, default=120, help='timed steps of the hulls-and-chains workload (0: skip it)')
+    ap.add_argument('--hulls', type=int, default=20000)
+    ap.add_argument('--chains', type=int, default=1000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -381,6 +429,10 @@ def main():
                'd2h_bytes_per_step': nbytes}
         w2.destroy()
 
+    hulls = None
+    if args.hull_steps > 0:
+        hulls = run_hulls(args, local, rank, world_size, barrier, torch, dist)
+
     batched = None
     if args.batched_worlds > 0:
         batched = run_batched(args, local, rank, world_size, barrier, torch, dist)
@@ -407,6 +459,7 @@ def main():
             'e2e': e2e,
             'cpu_baseline': cpu,
             'batched': batched,
+            'hulls': hulls,
             'device': name[0] if name else None,
         }
         print(json.dumps(line), flush=True)

@@ -43,6 +43,11 @@ enum {
 #define AVBD_SHAPE_BOX 0
 #define AVBD_SHAPE_SPHERE 1
 #define AVBD_SHAPE_SAIL 2
+/* A hull body's shape is AVBD_SHAPE_HULL + its hull's header offset (vec4s) in the world's hull
+ * buffer (layout.ts:150-151): the offset avbd_add_hull returns. */
+#define AVBD_SHAPE_HULL 3
+/* Most vertices a hull keeps (hull.ts:51); faces and edges at most 255 each. */
+#define AVBD_MAX_HULL_VERTICES 32
 /* Joint slot types (avbd_joint_info.type, layout.ts:153-154, avbd2d/gpu/layout.ts:74). */
 #define AVBD_T_NONE 0
 #define AVBD_T_JOINT 1
@@ -170,6 +175,32 @@ int avbd_release_joints(avbd_world* world, const uint32_t* slots, uint32_t n);
 int avbd_add_ignore_pairs(avbd_world* world, const uint32_t* pairs_ab, uint32_t n);
 /* setFilters (gpu/solver.ts): groups_mask[2i] = groups, [2i+1] = collides-with mask. */
 int avbd_set_filters(avbd_world* world, uint32_t first, const uint32_t* groups_mask, uint32_t n);
+
+/* Convex hulls (src/avbd3d/hull.ts, gpu/wgsl-hull.ts). A hull record is the reference's packed
+ * layout (gpu/solver.ts:313-338 packHull with its header at vec4 0), 4 words per vec4:
+ *   header: vertex start, vertex count, face start, face count | edge start, edge count, index start, 0
+ *   vertices (x, y, z as f32 bits), faces (normal + plane offset as f32 bits, then first index and
+ *   vertex count), vertex indices (4 a vec4), edges (vertex a, vertex b, face on each side),
+ * all in the body's principal frame. */
+typedef struct avbd_hull_props {
+  double volume;                   /* per unit density */
+  double moments[3];               /* principal moments per unit density */
+  double size[3];                  /* full widths of the vertex bounds (principal frame) */
+  double radius;                   /* farthest vertex from the centre of mass */
+  double center[3];                /* where the principal frame sits in the points' frame */
+  double rotation[4];              /* its rotation, x y z w */
+  uint32_t vertices, faces, edges; /* counts */
+} avbd_hull_props;
+/* convexHull(points) (hull.ts:60-75): the hull of n xyz points, simplified to
+ * AVBD_MAX_HULL_VERTICES by farthest-point sampling; AVBD_ERR_INVALID when the points span no
+ * volume. Host code (no device needed). *vec4s receives the record's size; with packed NULL only
+ * the size and props are returned. */
+int avbd_hull_build(const float* points, uint32_t n, uint32_t* packed, uint32_t cap_vec4s, uint32_t* vec4s, avbd_hull_props* props);
+/* The hull buffer's append (gpu/solver.ts:1390-1410, pinHull): copies one packed record (header at
+ * vec4 0) into the world's hull buffer; *offset receives its header offset (shape code - 3).
+ * Records are validated (counts, index ranges); a body naming an offset that is not a hull header
+ * is rejected by avbd_add_bodies / avbd_write_bodies. */
+int avbd_add_hull(avbd_world* world, const uint32_t* packed, uint32_t vec4s, uint32_t* offset);
 /* seedFrom's contact import (gpu/solver.ts:1320-1359): last step's manifolds and contacts, the
  * next step's warm-start source. manifold.first indexes `contacts`. */
 int avbd_seed_contacts(avbd_world* world, const avbd_manifold* manifolds, uint32_t n_manifolds, const avbd_contact* contacts,

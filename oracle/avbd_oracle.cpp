@@ -183,7 +183,7 @@ void solve6(const M3<T>& aLin, const M3<T>& aAng, const M3<T>& aCross, const V3<
 // ---------------------------------------------------------------------------------------------
 const double PENALTY_MIN = 1.0, PENALTY_MAX = 1e10, COLLISION_MARGIN = 0.01, STICK_THRESH = 1e-5;
 const uint32_t STICK_BIT = 0x80000000u, SPHERE_FEATURE = 3u << 24;
-const int SHAPE_BOX = 0, SHAPE_SPHERE = 1;
+const int SHAPE_BOX = 0, SHAPE_SPHERE = 1, SHAPE_HULL = 3;  // layout.ts:143-151 (a hull: SHAPE_HULL + header offset)
 const int MAX_COLORS = 64;
 const uint32_t NO_COLOR = 255, PENDING = 256;
 const double PIVOT_FLOOR = 1e-5;
@@ -457,14 +457,338 @@ template <class T> bool sphereBox(const OBB<T>& S, const OBB<T>& X, const Q4<T>&
   return true;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Convex hulls (src/avbd3d/gpu/wgsl-hull.ts), restated from the WGSL in its operation order. The
+// hull buffer is the reference's packed layout (gpu/solver.ts:313-338): 4 words per vec4; a body's
+// shape code is SHAPE_HULL + its header offset. A box takes part with its own topology.
+// ---------------------------------------------------------------------------------------------
+const uint32_t NO_HULL = 0xffffffffu;
+const int MAX_CLIP = 64;
+const uint32_t BOX_FACE_VERTS[24] = {1, 3, 7, 5, 0, 2, 6, 4, 2, 3, 7, 6, 0, 1, 5, 4, 4, 5, 7, 6, 0, 1, 3, 2};  // wgsl-hull.ts:37
+const uint32_t BOX_EDGES[12][4] = {{0, 1, 3, 5}, {2, 3, 2, 5}, {4, 5, 3, 4}, {6, 7, 2, 4}, {0, 2, 1, 5}, {1, 3, 0, 5},
+                                   {4, 6, 1, 4}, {5, 7, 0, 4}, {0, 4, 1, 3}, {1, 5, 0, 3}, {2, 6, 1, 2}, {3, 7, 0, 2}};  // :38-41
+
+template <class T> struct PolyShape {  // wgsl-hull.ts:27-33 (Poly)
+  V3<T> c, h;
+  Q4<T> q;
+  uint32_t hull = NO_HULL, vs = 0, nv = 8, fs = 0, nf = 6, es = 0, ne = 12, is = 0;
+  const uint32_t* buf = nullptr;
+};
+inline float wordf(const uint32_t* b, uint32_t word) {
+  float f;
+  std::memcpy(&f, b + word, 4);
+  return f;
+}
+template <class T> PolyShape<T> polyOf(const Body<T>& body, const uint32_t* buf) {  // wgsl-hull.ts:47-63
+  PolyShape<T> P;
+  P.c = body.pos;
+  P.q = body.rot;
+  P.h = scale3(body.size, T(0.5));
+  P.buf = buf;
+  if (body.shape >= SHAPE_HULL) {
+    uint32_t h = uint32_t(body.shape - SHAPE_HULL);
+    P.hull = h;
+    P.vs = buf[4 * h]; P.nv = buf[4 * h + 1]; P.fs = buf[4 * h + 2]; P.nf = buf[4 * h + 3];
+    P.es = buf[4 * h + 4]; P.ne = buf[4 * h + 5]; P.is = buf[4 * h + 6];
+  }
+  return P;
+}
+template <class T> V3<T> vertLocal(const PolyShape<T>& P, uint32_t v) {  // :65-70
+  if (P.hull == NO_HULL) return {(v & 1u) ? P.h[0] : -P.h[0], (v & 2u) ? P.h[1] : -P.h[1], (v & 4u) ? P.h[2] : -P.h[2]};
+  uint32_t o = 4 * (P.vs + v);
+  return {T(wordf(P.buf, o)), T(wordf(P.buf, o + 1)), T(wordf(P.buf, o + 2))};
+}
+template <class T> V3<T> vertOf(const PolyShape<T>& P, uint32_t v) { return add3(P.c, rotate(P.q, vertLocal(P, v))); }  // :72-74
+template <class T> V3<T> faceNormalLocal(const PolyShape<T>& P, uint32_t f) {  // :149-157
+  if (P.hull == NO_HULL) {
+    V3<T> n{0, 0, 0};
+    n[f / 2u] = (f & 1u) ? T(-1) : T(1);
+    return n;
+  }
+  uint32_t o = 4 * (P.fs + 2 * f);
+  return {T(wordf(P.buf, o)), T(wordf(P.buf, o + 1)), T(wordf(P.buf, o + 2))};
+}
+template <class T> Q4<T> facePlane(const PolyShape<T>& P, uint32_t f) {  // :77-92 (normal, offset)
+  V3<T> nl = faceNormalLocal(P, f);
+  T d = P.hull == NO_HULL ? P.h[f / 2u] : T(wordf(P.buf, 4 * (P.fs + 2 * f) + 3));
+  V3<T> n = rotate(P.q, nl);
+  return {n[0], n[1], n[2], d + dot(n, P.c)};
+}
+template <class T> V3<T> planeN(const Q4<T>& p) { return {p[0], p[1], p[2]}; }
+template <class T> uint32_t faceVertCount(const PolyShape<T>& P, uint32_t f) { return P.hull == NO_HULL ? 4u : P.buf[4 * (P.fs + 2 * f + 1) + 1]; }
+template <class T> uint32_t faceVert(const PolyShape<T>& P, uint32_t f, uint32_t j) {  // :99-103
+  if (P.hull == NO_HULL) return BOX_FACE_VERTS[f * 4 + j];
+  uint32_t k = P.buf[4 * (P.fs + 2 * f + 1)] + j;
+  return P.buf[4 * (P.is + k / 4) + k % 4];
+}
+template <class T> std::array<uint32_t, 4> edgeOf(const PolyShape<T>& P, uint32_t e) {  // :105-108
+  if (P.hull == NO_HULL) return {BOX_EDGES[e][0], BOX_EDGES[e][1], BOX_EDGES[e][2], BOX_EDGES[e][3]};
+  const uint32_t* q = P.buf + 4 * (P.es + e);
+  return {q[0], q[1], q[2], q[3]};
+}
+template <class T> V3<T> polySupport(const PolyShape<T>& P, const V3<T>& dir) {  // :110-121
+  V3<T> l = rotate(conjugate(P.q), dir);
+  if (P.hull == NO_HULL) return add3(P.c, rotate(P.q, V3<T>{l[0] >= 0 ? P.h[0] : -P.h[0], l[1] >= 0 ? P.h[1] : -P.h[1], l[2] >= 0 ? P.h[2] : -P.h[2]}));
+  T best = T(-3.4e38);
+  V3<T> at{0, 0, 0};
+  for (uint32_t v = 0; v < P.nv; v++) {
+    V3<T> p = vertLocal(P, v);
+    T s = dot(p, l);
+    if (s > best) { best = s; at = p; }
+  }
+  return add3(P.c, rotate(P.q, at));
+}
+template <class T> void queryFaces(const PolyShape<T>& A, const PolyShape<T>& B, T& sep, uint32_t& face) {  // :126-134
+  sep = T(-3.4e38);
+  face = 0;
+  for (uint32_t f = 0; f < A.nf; f++) {
+    Q4<T> p = facePlane(A, f);
+    T s = dot(planeN(p), polySupport(B, neg3(planeN(p)))) - p[3];
+    if (s > sep) { sep = s; face = f; }
+  }
+}
+template <class T> bool minkowskiFace(const V3<T>& a, const V3<T>& b, const V3<T>& c, const V3<T>& d) {  // :137-146
+  V3<T> bxa = cross(b, a), dxc = cross(d, c);
+  T cba = dot(c, bxa), dba = dot(d, bxa), adc = dot(a, dxc), bdc = dot(b, dxc);
+  return cba * dba < 0 && adc * bdc < 0 && cba * bdc > 0;
+}
+template <class T> struct EdgeQuery { T sep; uint32_t ea = 0, eb = 0; V3<T> n{}; bool valid = false; };
+template <class T> EdgeQuery<T> queryEdges(const PolyShape<T>& A, const PolyShape<T>& B) {  // :159-188
+  EdgeQuery<T> out;
+  out.sep = T(-3.4e38);
+  Q4<T> toB = qmul(conjugate(B.q), A.q);
+  for (uint32_t i = 0; i < A.ne; i++) {
+    auto ea = edgeOf(A, i);
+    V3<T> a = rotate(toB, faceNormalLocal(A, ea[2]));
+    V3<T> b = rotate(toB, faceNormalLocal(A, ea[3]));
+    for (uint32_t j = 0; j < B.ne; j++) {
+      auto eb = edgeOf(B, j);
+      if (!minkowskiFace(a, b, neg3(faceNormalLocal(B, eb[2])), neg3(faceNormalLocal(B, eb[3])))) continue;
+      V3<T> pa = vertOf(A, ea[0]), qa = vertOf(A, ea[1]), pb = vertOf(B, eb[0]), qb = vertOf(B, eb[1]);
+      V3<T> n = cross(sub3(qa, pa), sub3(qb, pb));
+      T l = length(n);
+      if (l < T(1e-5) * length(sub3(qa, pa)) * length(sub3(qb, pb))) continue;
+      n = div3(n, l);
+      if (dot(n, sub3(pa, A.c)) < 0) n = neg3(n);
+      T s = dot(n, sub3(pb, pa));
+      if (s > out.sep) { out.sep = s; out.ea = i; out.eb = j; out.n = n; out.valid = true; }
+    }
+  }
+  return out;
+}
+template <class T> int clipHull(const V3<T>* src, int n, V3<T>* dst, const V3<T>& pn, T offset) {  // :191-211
+  if (n == 0) return 0;
+  int count = 0;
+  V3<T> a = src[n - 1];
+  T da = dot(pn, a) - offset;
+  for (int i = 0; i < n; i++) {
+    V3<T> b = src[i];
+    T db = dot(pn, b) - offset;
+    if ((da <= T(PLANE_EPSILON)) != (db <= T(PLANE_EPSILON))) {
+      T t = 0;
+      if (std::fabs(da - db) > T(SAT_AXIS_EPSILON)) t = clampv(da / (da - db), T(0), T(1));
+      if (count < MAX_CLIP) dst[count++] = add3(a, scale3(sub3(b, a), t));
+    }
+    if (db <= T(PLANE_EPSILON) && count < MAX_CLIP) dst[count++] = b;
+    a = b;
+    da = db;
+  }
+  return count;
+}
+template <class T> Found<T> hullFaceContact(const PolyShape<T>& A, const PolyShape<T>& B, bool refIsA, uint32_t refFace) {  // :214-291
+  Found<T> found;
+  const PolyShape<T>& R = refIsA ? A : B;
+  const PolyShape<T>& I = refIsA ? B : A;
+  Q4<T> plane = facePlane(R, refFace);
+  V3<T> rn = planeN(plane);
+  uint32_t deepest = 0;
+  T low = T(3.4e38);
+  for (uint32_t v = 0; v < I.nv; v++) {
+    T d = dot(vertOf(I, v), rn);
+    if (d < low) { low = d; deepest = v; }
+  }
+  uint32_t inc = 0;
+  T least = T(3.4e38);
+  for (uint32_t f = 0; f < I.nf; f++) {
+    bool touches = false;
+    for (uint32_t j = 0; j < faceVertCount(I, f); j++)
+      if (faceVert(I, f, j) == deepest) { touches = true; break; }
+    if (!touches) continue;
+    T d = dot(planeN(facePlane(I, f)), rn);
+    if (d < least) { least = d; inc = f; }
+  }
+  V3<T> poly[MAX_CLIP], tmp[MAX_CLIP];
+  int n = int(std::min<uint32_t>(faceVertCount(I, inc), MAX_CLIP));
+  for (int j = 0; j < n; j++) poly[j] = vertOf(I, faceVert(I, inc, uint32_t(j)));
+  uint32_t k = faceVertCount(R, refFace);
+  V3<T> centre{0, 0, 0};
+  for (uint32_t j = 0; j < k; j++) centre = add3(centre, vertOf(R, faceVert(R, refFace, j)));
+  centre = div3(centre, T(k));
+  for (uint32_t j = 0; j < k && n > 0; j++) {
+    V3<T> v0 = vertOf(R, faceVert(R, refFace, j));
+    V3<T> v1 = vertOf(R, faceVert(R, refFace, (j + 1) % k));
+    V3<T> sd = cross(sub3(v1, v0), rn);
+    T l = length(sd);
+    if (l < T(SAT_AXIS_EPSILON)) continue;
+    sd = div3(sd, l);
+    if (dot(sd, sub3(centre, v0)) > 0) sd = neg3(sd);
+    n = clipHull(poly, n, tmp, sd, dot(sd, v0));
+    for (int m = 0; m < n; m++) poly[m] = tmp[m];
+  }
+  T depth[MAX_CLIP];
+  uint32_t index[MAX_CLIP];
+  bool chosen[MAX_CLIP] = {};
+  int keep = 0;
+  for (int m = 0; m < n; m++) {
+    T dist = dot(rn, poly[m]) - plane[3];
+    if (dist <= T(PLANE_EPSILON)) { tmp[keep] = poly[m]; depth[keep] = dist; index[keep] = uint32_t(m); keep++; }
+  }
+  uint32_t prefix = (uint32_t(refIsA ? AXIS_FACE_A : AXIS_FACE_B) << 24) | (std::min<uint32_t>(refFace, 255) << 16) | (std::min<uint32_t>(inc, 255) << 8);
+  for (int c = 0; c < std::min(keep, MAX_CONTACTS); c++) {
+    int pick = 0;
+    T bestScore = T(-3.4e38);
+    for (int m = 0; m < keep; m++) {
+      if (chosen[m]) continue;
+      T score = -depth[m];
+      if (c > 0) {
+        score = T(3.4e38);
+        for (int o = 0; o < keep; o++)
+          if (chosen[o]) score = tmin(score, dot(sub3(tmp[m], tmp[o]), sub3(tmp[m], tmp[o])));
+      }
+      if (score > bestScore) { bestScore = score; pick = m; }
+    }
+    chosen[pick] = true;
+    V3<T> p = tmp[pick];
+    V3<T> onRef = sub3(p, scale3(rn, depth[pick]));
+    addFound(found, refIsA ? onRef : p, refIsA ? p : onRef, prefix | std::min<uint32_t>(index[pick], 255));
+  }
+  if (found.count == 0) {
+    V3<T> nAB = refIsA ? rn : neg3(rn);
+    addFound(found, polySupport(A, nAB), polySupport(B, neg3(nAB)), prefix);
+  }
+  return found;
+}
+template <class T> Found<T> hullEdgeContact(const PolyShape<T>& A, const PolyShape<T>& B, const EdgeQuery<T>& q) {  // :293-315
+  Found<T> found;
+  auto ea = edgeOf(A, q.ea);
+  auto eb = edgeOf(B, q.eb);
+  V3<T> p0 = vertOf(A, ea[0]), q0 = vertOf(B, eb[0]);
+  V3<T> d1 = sub3(vertOf(A, ea[1]), p0), d2 = sub3(vertOf(B, eb[1]), q0);
+  V3<T> r = sub3(p0, q0);
+  T a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r), c = dot(d1, r), b = dot(d1, d2);
+  T denom = a * e - b * b;
+  T s = 0;
+  if (std::fabs(denom) > T(SAT_AXIS_EPSILON) * a * e) s = clampv((b * f - c * e) / denom, T(0), T(1));
+  T t = (b * s + f) / tmax(e, T(SAT_AXIS_EPSILON));
+  if (t < 0) { t = 0; s = clampv(-c / tmax(a, T(SAT_AXIS_EPSILON)), T(0), T(1)); }
+  else if (t > 1) { t = 1; s = clampv((b - c) / tmax(a, T(SAT_AXIS_EPSILON)), T(0), T(1)); }
+  addFound(found, add3(p0, scale3(d1, s)), add3(q0, scale3(d2, t)), (uint32_t(AXIS_EDGE) << 24) | (std::min<uint32_t>(q.ea, 255) << 8) | std::min<uint32_t>(q.eb, 255));
+  return found;
+}
+template <class T> Found<T> collidePoly(const PolyShape<T>& A, const PolyShape<T>& B, bool faceBias, Sat<T>& sat) {  // :318-341
+  Found<T> none;
+  T faSep, fbSep;
+  uint32_t faFace, fbFace;
+  queryFaces(A, B, faSep, faFace);
+  if (faSep > 0) return none;
+  queryFaces(B, A, fbSep, fbFace);
+  if (fbSep > 0) return none;
+  EdgeQuery<T> eq = queryEdges(A, B);
+  if (eq.valid && eq.sep > 0) return none;
+  T faceSep = tmax(faSep, fbSep);
+  bool edgeWins = eq.valid && eq.sep > T(0.95) * faceSep + T(0.01);
+  if (!faceBias) edgeWins = eq.valid && T(0.95) * eq.sep > faceSep + T(0.01);
+  if (edgeWins) {
+    sat.type = AXIS_EDGE; sat.ia = int(eq.ea); sat.ib = int(eq.eb); sat.sep = eq.sep; sat.n = eq.n; sat.valid = true;
+    return hullEdgeContact(A, B, eq);
+  }
+  if (fbSep > faSep) {
+    sat.type = AXIS_FACE_B; sat.ia = 0; sat.ib = int(fbFace); sat.sep = fbSep; sat.n = neg3(planeN(facePlane(B, fbFace))); sat.valid = true;
+    return hullFaceContact(A, B, false, fbFace);
+  }
+  sat.type = AXIS_FACE_A; sat.ia = int(faFace); sat.ib = 0; sat.sep = faSep; sat.n = planeN(facePlane(A, faFace)); sat.valid = true;
+  return hullFaceContact(A, B, true, faFace);
+}
+template <class T> V3<T> segmentPoint(const V3<T>& a, const V3<T>& b, const V3<T>& p) {  // :344-347
+  V3<T> d = sub3(b, a);
+  return add3(a, scale3(d, clampv(dot(sub3(p, a), d) / tmax(dot(d, d), T(1e-20)), T(0), T(1))));
+}
+// wgsl-hull.ts:350-405: n from the sphere towards X
+template <class T> bool sphereHull(const V3<T>& c, T r, const PolyShape<T>& X, V3<T>& onSphere, V3<T>& onHull, V3<T>& nOut) {
+  T deepest = T(-3.4e38);
+  uint32_t deepFace = 0;
+  for (uint32_t f = 0; f < X.nf; f++) {
+    T s = dot(planeN(facePlane(X, f)), c) - facePlane(X, f)[3];
+    if (s > deepest) { deepest = s; deepFace = f; }
+  }
+  if (deepest > r) return false;
+  if (deepest <= 0) {
+    V3<T> n = planeN(facePlane(X, deepFace));
+    nOut = neg3(n);
+    onHull = sub3(c, scale3(n, deepest));
+    onSphere = sub3(c, scale3(n, r));
+    return true;
+  }
+  V3<T> best{0, 0, 0};
+  T bestDist = T(3.4e38);
+  for (uint32_t f = 0; f < X.nf; f++) {
+    Q4<T> plane = facePlane(X, f);
+    T s = dot(planeN(plane), c) - plane[3];
+    if (s <= 0) continue;
+    V3<T> p = sub3(c, scale3(planeN(plane), s));
+    uint32_t k = faceVertCount(X, f);
+    V3<T> centre{0, 0, 0};
+    for (uint32_t j = 0; j < k; j++) centre = add3(centre, vertOf(X, faceVert(X, f, j)));
+    centre = div3(centre, T(k));
+    bool inside = true;
+    V3<T> edgeBest{0, 0, 0};
+    T edgeDist = T(3.4e38);
+    for (uint32_t j = 0; j < k; j++) {
+      V3<T> v0 = vertOf(X, faceVert(X, f, j));
+      V3<T> v1 = vertOf(X, faceVert(X, f, (j + 1) % k));
+      V3<T> side = cross(sub3(v1, v0), planeN(plane));
+      if (dot(side, sub3(centre, v0)) > 0) side = neg3(side);
+      if (dot(side, sub3(p, v0)) > 0) inside = false;
+      V3<T> q = segmentPoint(v0, v1, c);
+      T dq = dot(sub3(q, c), sub3(q, c));
+      if (dq < edgeDist) { edgeDist = dq; edgeBest = q; }
+    }
+    if (!inside) p = edgeBest;
+    T dist = length(sub3(p, c));
+    if (dist < bestDist) { bestDist = dist; best = p; }
+  }
+  if (bestDist > r) return false;
+  V3<T> n{0, 0, 1};
+  if (bestDist > 0) n = div3(sub3(c, best), bestDist);
+  nOut = neg3(n);
+  onHull = best;
+  onSphere = sub3(c, scale3(n, r));
+  return true;
+}
+
 // One pair's contacts (wgsl-collision.ts:767-811). Returns the manifold normal (B to A) in `normal`.
-template <class T> Found<T> narrowphase(const Body<T>& a, const Body<T>& b, bool faceBias, V3<T>& normal) {
+template <class T> Found<T> narrowphase(const Body<T>& a, const Body<T>& b, bool faceBias, V3<T>& normal, const uint32_t* hulls = nullptr) {
   OBB<T> A = makeOBB(a.pos, a.rot, a.size), B = makeOBB(b.pos, b.rot, b.size);
   Sat<T> sat;
   Found<T> found;
   bool sA = a.shape == SHAPE_SPHERE, sB = b.shape == SHAPE_SPHERE;
   if (sA && sB) {
     found = sphereSphere(A, B, sat);
+  } else if (hulls && (a.shape >= SHAPE_HULL || b.shape >= SHAPE_HULL)) {  // wgsl-collision.ts:781-796
+    if (sA || sB) {
+      V3<T> onS, onX, n;
+      if (sA) {
+        bool hit = sphereHull(A.c, A.h[0], polyOf(b, hulls), onS, onX, n);
+        sat.n = n;
+        if (hit) addFound(found, onS, onX, SPHERE_FEATURE);
+      } else {
+        bool hit = sphereHull(B.c, B.h[0], polyOf(a, hulls), onS, onX, n);
+        sat.n = neg3(n);
+        if (hit) addFound(found, onX, onS, SPHERE_FEATURE);
+      }
+    } else {
+      found = collidePoly(polyOf(a, hulls), polyOf(b, hulls), faceBias, sat);
+    }
   } else if (sA || sB) {
     V3<T> onS, onX, n;
     if (sA) {
@@ -1060,6 +1384,7 @@ template <class T> struct Solver {
   uint32_t flags = 0;
   T contactMargin = T(COLLISION_MARGIN);
   bool gpuMode = false;
+  std::vector<uint32_t> hulls;  // hull buffer (wgsl-hull.ts layout)
   std::vector<Body<T>> bodies;
   std::vector<std::unique_ptr<Force<T>>> forces;  // creation order
   // GPU mode: colour state, and the manifolds of the last step by pair (warm start)
@@ -1247,7 +1572,7 @@ template <class T> struct Solver {
       // The GPU's own arithmetic (f32) finds the contacts, so both sides solve one contact set
       Body<float> fA = toFloat(A), fB = toFloat(B);
       V3<float> nf;
-      Found<float> ff = narrowphase(fA, fB, (flags & FLAG_FACE_BIAS) != 0, nf);
+      Found<float> ff = narrowphase(fA, fB, (flags & FLAG_FACE_BIAS) != 0, nf, hulls.empty() ? nullptr : hulls.data());
       if (ff.count == 0) continue;
       V3<T> normal{T(nf[0]), T(nf[1]), T(nf[2])};
       auto m = std::make_unique<Manifold<T>>(this, a, b);
@@ -1598,7 +1923,7 @@ int orc_narrowphase(void* h, int a, int b, int faceBias, double* out, double* no
     const Body<T>& A = s.bodies[a];
     const Body<T>& B = s.bodies[b];
     V3<T> nrm;
-    Found<T> f = narrowphase(A, B, faceBias != 0, nrm);
+    Found<T> f = narrowphase(A, B, faceBias != 0, nrm, s.hulls.empty() ? nullptr : s.hulls.data());
     for (int i = 0; i < f.count; i++) {
       V3<T> rA = rotate(conjugate(A.rot), sub3(f.xA[i], A.pos));
       V3<T> rB = rotate(conjugate(B.rot), sub3(f.xB[i], B.pos));
@@ -1622,6 +1947,14 @@ void orc_color_graph(int n, const unsigned char* dynamic, const int* start, cons
 }
 
 unsigned orc_hash32(unsigned x) { return hash32(x); }
+
+// The hull buffer (gpu/solver.ts:313-338 layout, absolute offsets) the bodies' shape codes name
+void orc_set_hulls(void* h, const unsigned* words, int n) {
+  with(h, [&](auto& s) {
+    s.hulls.assign(words, words + n);
+    return 0;
+  });
+}
 
 // Host threads for the GPU-mode step (OpenMP); returns the count in use.
 int orc_set_threads(int n) {

@@ -60,6 +60,7 @@ def lib():
         L.orc_set_threads.restype = I
         L.orc_hash32.argtypes = [U]
         L.orc_hash32.restype = U
+        L.orc_set_hulls.argtypes = [P, ctypes.POINTER(U), I]
         _lib = L
     return _lib
 
@@ -111,8 +112,16 @@ class Oracle:
         arr = np.array([p.dt, p.gravity, p.iterations, p.alpha, p.beta_lin, p.beta_ang, p.gamma, p.contact_margin], dtype=np.float64)
         self.L.orc_set_params(self.h, _dp(arr), flags)
 
+    def set_hulls(self, words):
+        """The hull buffer the bodies' shape codes name (gpu/solver.ts:313-338 layout)."""
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        self._hulls = w
+        self.L.orc_set_hulls(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), len(w))
+
     def load(self, scene, flags: int = 0):
         self.set_params(scene.params, flags)
+        if len(getattr(scene, 'hull_words', [])):
+            self.set_hulls(scene.hull_words)
         for b in scene.bodies:
             self.L.orc_add_body(self.h, _dp(body_record(b)))
         for f in scene.forces:

@@ -114,12 +114,15 @@ def params_struct(p, flags: int = 0):
     return s
 
 
-def cuda_from_oracle(o: Oracle, params, flags: int = 0, seed: bool = True, **kw) -> avbd_b200.CudaSolver3D:
-    """A fresh CUDA world holding the oracle's state (`new GpuSolver3D(device, ref)` + `seedFrom(ref)`)."""
+def cuda_from_oracle(o: Oracle, params, flags: int = 0, seed: bool = True, hulls_from=None, **kw) -> avbd_b200.CudaSolver3D:
+    """A fresh CUDA world holding the oracle's state (`new GpuSolver3D(device, ref)` + `seedFrom(ref)`);
+    `hulls_from`: the scene whose hull buffer the bodies' shape codes name."""
     bodies = body_records(o)
     joints, info, ignores = joint_records(o)
     w = avbd_b200.CudaSolver3D(body_capacity=max(len(bodies), 1), joint_capacity=max(len(joints), 16), **kw)
     w.params = params_struct(params, flags)
+    if hulls_from is not None:
+        w.add_scene_hulls(hulls_from)
     w.add_bodies(bodies)
     if len(joints):
         w.add_joints(joints, info)

@@ -73,6 +73,16 @@ class Counters(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_ if not n.startswith('reserved')}
 
 
+class HullProps(ctypes.Structure):
+    _fields_ = [('volume', ctypes.c_double), ('moments', ctypes.c_double * 3), ('size', ctypes.c_double * 3), ('radius', ctypes.c_double),
+                ('center', ctypes.c_double * 3), ('rotation', ctypes.c_double * 4), ('vertices', ctypes.c_uint32), ('faces', ctypes.c_uint32),
+                ('edges', ctypes.c_uint32)]
+
+
+SHAPE_HULL = 3
+MAX_HULL_VERTICES = 32
+
+
 class BatchConfig(ctypes.Structure):
     _fields_ = [('world_capacity', ctypes.c_uint32), ('body_capacity', ctypes.c_uint32), ('joint_capacity', ctypes.c_uint32),
                 ('pairs_per_body', ctypes.c_uint32), ('device', ctypes.c_int32)]
@@ -138,6 +148,8 @@ SIGNATURES = {
     'avbd_set_solve_blocks': ([P, I], I),
     'avbd_read_phase_clocks': ([P, ctypes.POINTER(ctypes.c_double), U, PU], I),
     'avbd_write_bodies_async': ([P, U, VP, U], I),
+    'avbd_hull_build': ([VP, U, PU, U, PU, ctypes.POINTER(HullProps)], I),
+    'avbd_add_hull': ([P, PU, U, PU], I),
     'avbd_find_pairs_noalloc': ([VP, U, PU, PU, U, PU, VP], I),
     'avbd_batch_create': ([ctypes.POINTER(BatchConfig), ctypes.POINTER(P)], I),
     'avbd_batch_destroy': ([P], I),

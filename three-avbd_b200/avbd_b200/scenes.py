@@ -112,6 +112,8 @@ class Scene:
         self.bodies: list[Body] = []
         self.forces: list[Force] = []
         self.params = Params()
+        self.hull_words = np.zeros(0, dtype=np.uint32)  # hull buffer (gpu/solver.ts:313-338 layout)
+        self.hull_offsets: list[int] = []  # header offset of each hull record, in upload order
 
     # Rigid constructor (ref/body.ts:32-54)
     def box(self, size, density, friction, position, velocity=(0.0, 0.0, 0.0)) -> int:
@@ -134,6 +136,26 @@ class Scene:
         b.moment = [inertia, inertia, inertia]
         b.radius = float(r)
         b.shape = SHAPE_SPHERE
+        return i
+
+    def add_hull_shape(self, shape) -> int:
+        """Appends a hull record (a hulls.HullShape) to the scene's hull buffer; its header offset."""
+        from .hulls import relocate
+        at = len(self.hull_words) // 4
+        self.hull_words = np.concatenate([self.hull_words, relocate(shape.packed, at)])
+        self.hull_offsets.append(at)
+        return at
+
+    # A convex hull body (src/avbd3d/shapes.ts:58-70): principal frame at `position`, turned by `rotation`
+    def hull(self, shape, density, friction, position, rotation=(0.0, 0.0, 0.0, 1.0), velocity=(0.0, 0.0, 0.0), offset=None) -> int:
+        at = self.add_hull_shape(shape) if offset is None else int(offset)
+        i = self.box(list(shape.size), density, friction, position, velocity)
+        b = self.bodies[i]
+        b.rot = [float(x) for x in rotation]
+        b.mass = shape.volume * density if density > 0 else 0.0
+        b.moment = [m * max(density, 0.0) for m in shape.moments]
+        b.radius = float(shape.radius)
+        b.shape = SHAPE_HULL + at
         return i
 
     def joint(self, a, b, rA, rB, stiffness_lin=INF, stiffness_ang=0.0, fracture=INF) -> int:
@@ -477,4 +499,113 @@ def tumbling_world(rng: np.random.Generator, n: int = 64) -> Scene:
         b = s.box([0.8, 0.8, 0.8], 1, 0.5, p, v)
         s.bodies[b].rot = q[i].tolist()
         s.bodies[b].ang_vel = [rng.uniform(-3, 3) for _ in range(3)]
+    return s
+
+
+# --- convex hulls (config 3) ----------------------------------------------------------------------
+
+def ellipsoid_hull(rng: np.random.Generator, points: int | None = None):
+    """The hull of 8-32 points on an ellipsoid with semi-axes U[0.3, 1.0] (random orientation of the
+    points' frame): the reference's convexHull of them (src/avbd3d/hull.ts)."""
+    from .hulls import build_hull
+    while True:
+        k = int(points if points is not None else rng.integers(8, 33))
+        axes = rng.uniform(0.3, 1.0, 3)
+        d = rng.standard_normal((k, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        h = build_hull((d * axes).reshape(-1))
+        if h is not None:
+            return h
+
+
+def hull_pairs(count: int = 200, seed: int = 5) -> Scene:
+    """Overlapping pairs of a hull with a hull, a box or a sphere (either order), each pair far from
+    the others; no gravity and no iterations, so one step's contacts are the narrowphase's."""
+    rng = np.random.default_rng(seed)
+    s = Scene('hull pairs')
+    s.params.gravity = 0.0
+    s.params.iterations = 0
+    shapes = [ellipsoid_hull(rng) for _ in range(16)]
+    offsets = [s.add_hull_shape(h) for h in shapes]
+    for p in range(count):
+        base = np.array([(p % 20) * 10.0, (p // 20) * 10.0, 0.0])
+        kinds = [('hull', 'hull'), ('hull', 'box'), ('box', 'hull'), ('hull', 'sphere'), ('sphere', 'hull')][p % 5]
+        for k, kind in enumerate(kinds):
+            at = base if k == 0 else base + rng.uniform(-0.6, 0.6, 3)
+            q = rng.standard_normal(4)
+            q /= np.linalg.norm(q)
+            if kind == 'hull':
+                j = int(rng.integers(len(shapes)))
+                i = s.hull(shapes[j], 1.0, 0.5, at.tolist(), q.tolist(), offset=offsets[j])
+            elif kind == 'box':
+                i = s.box(rng.uniform(0.4, 1.6, 3).tolist(), 1.0, 0.5, at.tolist())
+                s.bodies[i].rot = q.tolist()
+            else:
+                i = s.sphere(float(rng.uniform(0.3, 0.8)), 1.0, 0.5, at.tolist())
+    return s
+
+
+def hull_pile(n: int = 300, seed: int = 7, spacing: float = 1.9, boxes: float = 0.2, spheres: float = 0.1, gravity: float = -9.81) -> Scene:
+    """Hulls (ellipsoid point hulls), with some boxes and spheres, dropped on a jittered lattice onto a
+    static ground box."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f'hull pile {n}')
+    s.params.gravity = gravity
+    side = max(1, int(math.ceil(math.sqrt(n / 4))))
+    s.box([side * spacing + 20.0, side * spacing + 20.0, 1.0], 0, 0.5, [0.0, 0.0, -0.5])
+    shapes = [ellipsoid_hull(rng) for _ in range(min(n, 64))]
+    offsets = [s.add_hull_shape(h) for h in shapes]
+    for i in range(n):
+        gx, gy, gz = i % side, (i // side) % side, i // (side * side)
+        p = [(gx - (side - 1) / 2) * spacing + rng.uniform(-0.05, 0.05), (gy - (side - 1) / 2) * spacing + rng.uniform(-0.05, 0.05),
+             1.2 + gz * spacing]
+        q = rng.standard_normal(4)
+        q /= np.linalg.norm(q)
+        u = rng.uniform()
+        if u < boxes:
+            k = s.box(rng.uniform(0.5, 1.2, 3).tolist(), 1.0, 0.5, p)
+            s.bodies[k].rot = q.tolist()
+        elif u < boxes + spheres:
+            s.sphere(float(rng.uniform(0.3, 0.6)), 1.0, 0.5, p)
+        else:
+            j = int(rng.integers(len(shapes)))
+            s.hull(shapes[j], float(rng.uniform(0.5, 2.0)), float(rng.uniform(0.3, 0.8)), p, q.tolist(), offset=offsets[j])
+    return s
+
+
+def hulls_and_chains(hulls: int = 20000, chains: int = 1000, links: int = 50, seed: int = 9, distinct: int = 512) -> Scene:
+    """Config 3: `hulls` hulls of 8-32 points on ellipsoids (semi-axes U[0.3, 1.0]) falling onto
+    `chains` chains of `links` boxes (0.2 x 0.2 x 0.5) joined by ball joints (break force 1e4 N on the
+    linear force: breakOnPull), each hung from a static anchor; static ground box. 15 iterations.
+    `distinct` hull shapes are built and shared."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f'hulls {hulls} + chains {chains}x{links}')
+    s.params.gravity = -9.81
+    s.params.iterations = 15
+    cside = int(math.ceil(math.sqrt(chains)))
+    cspacing = 3.2
+    extent = cside * cspacing
+    top = links * 0.5 + 6.0
+    s.box([extent + 20.0, extent + 20.0, 1.0], 0, 0.5, [0.0, 0.0, -0.5])
+    for c in range(chains):
+        x = (c % cside - (cside - 1) / 2) * cspacing
+        y = (c // cside - (cside - 1) / 2) * cspacing
+        anchor = s.box([0.4, 0.4, 0.2], 0, 0.5, [x, y, top + 0.1])
+        prev, prev_off = anchor, [0.0, 0.0, -0.1]
+        for k in range(links):
+            z = top - 0.25 - 0.5 * k
+            b = s.box([0.2, 0.2, 0.5], 1.0, 0.5, [x, y, z])
+            j = s.joint(prev, b, prev_off, [0.0, 0.0, 0.25], stiffness_lin=INF, stiffness_ang=0.0, fracture=1e4)
+            s.forces[j].fracture_linear = True
+            prev, prev_off = b, [0.0, 0.0, -0.25]
+    shapes = [ellipsoid_hull(rng) for _ in range(min(distinct, hulls))]
+    offsets = [s.add_hull_shape(h) for h in shapes]
+    hside = int(math.ceil(extent / 2.2))
+    for i in range(hulls):
+        gx, gy, gz = i % hside, (i // hside) % hside, i // (hside * hside)
+        p = [(gx - (hside - 1) / 2) * 2.2 + rng.uniform(-0.1, 0.1), (gy - (hside - 1) / 2) * 2.2 + rng.uniform(-0.1, 0.1), top + 2.5 + gz * 2.2]
+        q = rng.standard_normal(4)
+        q /= np.linalg.norm(q)
+        j = int(rng.integers(len(shapes)))
+        s.hull(shapes[j], 1.0, float(rng.uniform(0.3, 0.8)), p, q.tolist(), offset=offsets[j])
     return s

@@ -173,6 +173,7 @@ class CudaSolver3D:
                 self.order = morton_order(np.array([b.pos for b in scene.bodies]))
                 self.gpu_index = np.empty(n, dtype=np.int64)
                 self.gpu_index[self.order] = np.arange(n)
+            self.add_scene_hulls(scene)
             bodies, joints, infos, ignores = scene_records(scene, self.order)
             self.add_bodies(bodies)
             if len(joints):
@@ -210,6 +211,26 @@ class CudaSolver3D:
         self._check(self.lib.avbd_set_params(self.handle, ctypes.byref(to_params(sp))))
 
     # --- scene edits ---
+    def add_hull(self, packed: np.ndarray) -> int:
+        """A hull record (header at vec4 0) into the world's hull buffer; its header offset (shape - 3)."""
+        packed = np.ascontiguousarray(packed, dtype=np.uint32)
+        at = ctypes.c_uint32()
+        self._check(self.lib.avbd_add_hull(self.handle, uptr(packed), len(packed) // 4, ctypes.byref(at)))
+        return at.value
+
+    def add_scene_hulls(self, scene: Scene):
+        """The scene's hull buffer, record by record, at the same offsets (the scene packs from 0)."""
+        offs = list(getattr(scene, 'hull_offsets', []))
+        words = getattr(scene, 'hull_words', np.zeros(0, np.uint32))
+        for k, at in enumerate(offs):
+            end = offs[k + 1] if k + 1 < len(offs) else len(words) // 4
+            rec = words[4 * at:4 * end].copy()
+            for j in (0, 2, 4, 6):
+                rec[j] -= at
+            got = self.add_hull(rec)
+            if got != at:
+                raise AvbdError(_abi.AVBD_ERR_INVALID, f'hull record landed at {got}, the scene packed it at {at}')
+
     def add_bodies(self, records: np.ndarray) -> int:
         records = np.ascontiguousarray(records, dtype=BODY_DTYPE)
         first = ctypes.c_uint32()

@@ -20,6 +20,7 @@ UNITS = {
     'avbd_solve.cu': [],
     'avbd_host.cu': [],
     'avbd_batch.cu': [],
+    'avbd_hull.cu': [],
 }
 
 

@@ -430,6 +430,8 @@ int avbd_batch_add_world(avbd_batch* b, const avbd_body* bodies, uint32_t n, con
   if (uint64_t(b->n) + n > b->bodyCap) return bfail(b, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(b->bodyCap) + " reached");
   if (uint64_t(b->nj) + nj > b->jointCap) return bfail(b, AVBD_ERR_CAPACITY, "joint capacity " + std::to_string(b->jointCap) + " reached");
   std::string msg = bodyProblem(bodies, n);
+  for (uint32_t i = 0; i < n && msg.empty(); i++)
+    if (!(bodies[i].shape == 0.0f || bodies[i].shape == 1.0f || bodies[i].shape == 2.0f)) msg = "batched worlds hold boxes, spheres and sails";
   if (msg.empty()) msg = jointProblem(joints, info, nj, n);
   for (uint32_t i = 0; i < n_ignore && msg.empty(); i++)
     if (ignore_ab[2 * i] >= n || ignore_ab[2 * i + 1] >= n || ignore_ab[2 * i] == ignore_ab[2 * i + 1]) msg = "ignore pair out of range";
@@ -466,6 +468,7 @@ int avbd_batch_add_world(avbd_batch* b, const avbd_body* bodies, uint32_t n, con
 int avbd_batch_add_world_from(avbd_batch* b, avbd_world* src, uint32_t* index) {
   if (!b || !src) return AVBD_ERR_INVALID;
   if (src->device != b->device) return bfail(b, AVBD_ERR_INVALID, "the world is on another device");
+  if (!src->hullWords.empty()) return bfail(b, AVBD_ERR_INVALID, "batched worlds hold boxes, spheres and sails");
   const uint32_t n = src->n, nj = src->nj;
   if (n == 0 || n > BATCH_MAX_WORLD_BODIES)
     return bfail(b, AVBD_ERR_INVALID, "a batched world holds 1 to " + std::to_string(BATCH_MAX_WORLD_BODIES) + " bodies");

@@ -643,6 +643,408 @@ __device__ bool sphereBox(const Box& S, const Box& X, float4 qX, float3& onSpher
 
 // Contact pair p: manifold slot p with its points at 8p .. 8p+count-1, warm-started from last step's
 // pair (a, b) by feature key (wgsl-collision.ts:767-892).
+// --- convex hulls (wgsl-hull.ts) -------------------------------------------------------------------------
+// A pair with a hull on either side (the other a hull, a box or a sphere) collides here: SAT over
+// both shapes' face normals by support points and the edge pairs whose Gauss-map arcs cross
+// (queryFaces, queryEdges), then the incident face clipped by the reference face's side planes, or
+// the closest points of two edges. A box takes part as a hull of its own topology. These run one
+// thread per pair with their clip polygons in local memory, kept out of the box path (noinline).
+constexpr uint32_t NO_HULL = 0xffffffffu, MAX_CLIP = 64;
+constexpr float SHAPE_HULL_F = 3.0f;
+__constant__ uint8_t BOX_FACE_VERTS[24] = {1, 3, 7, 5, 0, 2, 6, 4, 2, 3, 7, 6, 0, 1, 5, 4, 4, 5, 7, 6, 0, 1, 3, 2};
+__constant__ uint8_t BOX_EDGES[12][4] = {{0, 1, 3, 5}, {2, 3, 2, 5}, {4, 5, 3, 4}, {6, 7, 2, 4}, {0, 2, 1, 5}, {1, 3, 0, 5},
+                                         {4, 6, 1, 4}, {5, 7, 0, 4}, {0, 4, 1, 3}, {1, 5, 0, 3}, {2, 6, 1, 2}, {3, 7, 0, 2}};
+
+struct Poly {
+  float3 c, h;
+  float4 q;
+  uint32_t hull, vs, nv, fs, nf, es, ne, is;
+};
+__device__ inline bool isHull(const DWorld& w, uint32_t i) { return w.avel[i].w >= SHAPE_HULL_F; }
+__device__ inline Poly polyOf(const DWorld& w, uint32_t i) {  // wgsl-hull.ts:47-63
+  Poly P;
+  P.c = f3(w.pos[i]);
+  P.q = w.rot[i];
+  P.h = f3(w.size[i]) * 0.5f;
+  P.hull = NO_HULL;
+  P.nv = 8u;
+  P.nf = 6u;
+  P.ne = 12u;
+  P.vs = P.fs = P.es = P.is = 0u;
+  if (isHull(w, i)) {
+    uint32_t h = (uint32_t)(w.avel[i].w - SHAPE_HULL_F + 0.5f);
+    uint4 h0 = w.hulls[h], h1 = w.hulls[h + 1u];
+    P.hull = h;
+    P.vs = h0.x;
+    P.nv = h0.y;
+    P.fs = h0.z;
+    P.nf = h0.w;
+    P.es = h1.x;
+    P.ne = h1.y;
+    P.is = h1.z;
+  }
+  return P;
+}
+__device__ inline float3 u4f3(uint4 u) { return make_float3(__uint_as_float(u.x), __uint_as_float(u.y), __uint_as_float(u.z)); }
+__device__ inline float3 vertLocal(const DWorld& w, const Poly& P, uint32_t v) {
+  if (P.hull == NO_HULL) return make_float3((v & 1u) ? P.h.x : -P.h.x, (v & 2u) ? P.h.y : -P.h.y, (v & 4u) ? P.h.z : -P.h.z);
+  return u4f3(w.hulls[P.vs + v]);
+}
+__device__ inline float3 vert(const DWorld& w, const Poly& P, uint32_t v) { return P.c + qrotate(P.q, vertLocal(w, P, v)); }
+__device__ inline float3 faceNormalLocal(const DWorld& w, const Poly& P, uint32_t f) {
+  if (P.hull == NO_HULL) {
+    float3 n = make_float3(0.0f, 0.0f, 0.0f);
+    float s = (f & 1u) ? -1.0f : 1.0f;
+    if (f / 2u == 0u) n.x = s;
+    else if (f / 2u == 1u) n.y = s;
+    else n.z = s;
+    return n;
+  }
+  return u4f3(w.hulls[P.fs + 2u * f]);
+}
+__device__ inline float4 facePlane(const DWorld& w, const Poly& P, uint32_t f) {  // wgsl-hull.ts:75-92
+  float3 nl;
+  float d;
+  if (P.hull == NO_HULL) {
+    nl = faceNormalLocal(w, P, f);
+    uint32_t k = f / 2u;
+    d = k == 0u ? P.h.x : (k == 1u ? P.h.y : P.h.z);
+  } else {
+    uint4 u = w.hulls[P.fs + 2u * f];
+    nl = u4f3(u);
+    d = __uint_as_float(u.w);
+  }
+  float3 n = qrotate(P.q, nl);
+  return make_float4(n.x, n.y, n.z, d + dot3(n, P.c));
+}
+__device__ inline uint32_t faceVertCount(const DWorld& w, const Poly& P, uint32_t f) { return P.hull == NO_HULL ? 4u : w.hulls[P.fs + 2u * f + 1u].y; }
+__device__ inline uint32_t faceVert(const DWorld& w, const Poly& P, uint32_t f, uint32_t j) {
+  if (P.hull == NO_HULL) return BOX_FACE_VERTS[f * 4u + j];
+  uint32_t k = w.hulls[P.fs + 2u * f + 1u].x + j;
+  uint4 q = w.hulls[P.is + k / 4u];
+  uint32_t m = k % 4u;
+  return m == 0u ? q.x : (m == 1u ? q.y : (m == 2u ? q.z : q.w));
+}
+__device__ inline uint4 edgeOf(const DWorld& w, const Poly& P, uint32_t e) {
+  if (P.hull == NO_HULL) return make_uint4(BOX_EDGES[e][0], BOX_EDGES[e][1], BOX_EDGES[e][2], BOX_EDGES[e][3]);
+  return w.hulls[P.es + e];
+}
+__device__ inline float3 polySupport(const DWorld& w, const Poly& P, float3 dir) {  // wgsl-hull.ts:104-115
+  float3 l = qrotate(qconj(P.q), dir);
+  if (P.hull == NO_HULL)
+    return P.c + qrotate(P.q, make_float3(l.x >= 0.0f ? P.h.x : -P.h.x, l.y >= 0.0f ? P.h.y : -P.h.y, l.z >= 0.0f ? P.h.z : -P.h.z));
+  float best = -3.4e38f;
+  float3 at = make_float3(0.0f, 0.0f, 0.0f);
+  for (uint32_t v = 0; v < P.nv; v++) {
+    float3 q = u4f3(w.hulls[P.vs + v]);
+    float s = dot3(q, l);
+    if (s > best) {
+      best = s;
+      at = q;
+    }
+  }
+  return P.c + qrotate(P.q, at);
+}
+// The face of A whose plane B sticks out of least (wgsl-hull.ts:120-128)
+__device__ inline void queryFaces(const DWorld& w, const Poly& A, const Poly& B, float& sep, uint32_t& face) {
+  sep = -3.4e38f;
+  face = 0u;
+  for (uint32_t f = 0; f < A.nf; f++) {
+    float4 pl = facePlane(w, A, f);
+    float3 n = make_float3(pl.x, pl.y, pl.z);
+    float s = dot3(n, polySupport(w, B, -n)) - pl.w;
+    if (s > sep) {
+      sep = s;
+      face = f;
+    }
+  }
+}
+__device__ inline bool minkowskiFace(float3 a, float3 b, float3 c, float3 d) {  // wgsl-hull.ts:131-142
+  float3 bxa = cross3(b, a), dxc = cross3(d, c);
+  float cba = dot3(c, bxa), dba = dot3(d, bxa), adc = dot3(a, dxc), bdc = dot3(b, dxc);
+  return cba * dba < 0.0f && adc * bdc < 0.0f && cba * bdc > 0.0f;
+}
+struct EdgeQuery {
+  float sep;
+  uint32_t ea, eb;
+  float3 n;
+  bool valid;
+};
+__device__ __noinline__ EdgeQuery queryEdges(const DWorld& w, const Poly& A, const Poly& B) {  // wgsl-hull.ts:155-183
+  EdgeQuery out;
+  out.sep = -3.4e38f;
+  out.ea = out.eb = 0u;
+  out.n = make_float3(0.0f, 0.0f, 0.0f);
+  out.valid = false;
+  float4 toB = qmul(qconj(B.q), A.q);
+  for (uint32_t i = 0; i < A.ne; i++) {
+    uint4 ea = edgeOf(w, A, i);
+    float3 a = qrotate(toB, faceNormalLocal(w, A, ea.z));
+    float3 b = qrotate(toB, faceNormalLocal(w, A, ea.w));
+    for (uint32_t j = 0; j < B.ne; j++) {
+      uint4 eb = edgeOf(w, B, j);
+      if (!minkowskiFace(a, b, -faceNormalLocal(w, B, eb.z), -faceNormalLocal(w, B, eb.w))) continue;
+      float3 pa = vert(w, A, ea.x), qa = vert(w, A, ea.y), pb = vert(w, B, eb.x), qb = vert(w, B, eb.y);
+      float3 n = cross3(qa - pa, qb - pb);
+      float l = len3(n);
+      if (l < 1e-5f * len3(qa - pa) * len3(qb - pb)) continue;
+      n = n / l;
+      if (dot3(n, pa - A.c) < 0.0f) n = -n;
+      float s = dot3(n, pb - pa);
+      if (s > out.sep) {
+        out.sep = s;
+        out.ea = i;
+        out.eb = j;
+        out.n = n;
+        out.valid = true;
+      }
+    }
+  }
+  return out;
+}
+__device__ inline uint32_t clipHull(const float3* src, uint32_t n, float3* dst, float3 pn, float offset) {  // wgsl-hull.ts:186-204
+  if (n == 0u) return 0u;
+  uint32_t count = 0;
+  float3 a = src[n - 1u];
+  float da = dot3(pn, a) - offset;
+  for (uint32_t i = 0; i < n; i++) {
+    float3 b = src[i];
+    float db = dot3(pn, b) - offset;
+    if ((da <= PLANE_EPSILON) != (db <= PLANE_EPSILON)) {
+      float t = 0.0f;
+      if (fabsf(da - db) > SAT_AXIS_EPSILON) t = fminf(fmaxf(da / (da - db), 0.0f), 1.0f);
+      if (count < MAX_CLIP) dst[count++] = a + (b - a) * t;
+    }
+    if (db <= PLANE_EPSILON && count < MAX_CLIP) dst[count++] = b;
+    a = b;
+    da = db;
+  }
+  return count;
+}
+// Face contact (wgsl-hull.ts:207-291): the other shape's face clipped to the reference face
+__device__ __noinline__ void hullFaceContact(const DWorld& w, const Poly& A, const Poly& B, bool refIsA, uint32_t refFace, Found& found) {
+  const Poly& R = refIsA ? A : B;
+  const Poly& I = refIsA ? B : A;
+  float4 plane = facePlane(w, R, refFace);
+  float3 rn = make_float3(plane.x, plane.y, plane.z);
+  uint32_t deepest = 0;
+  float low = 3.4e38f;
+  for (uint32_t v = 0; v < I.nv; v++) {
+    float d = dot3(vert(w, I, v), rn);
+    if (d < low) {
+      low = d;
+      deepest = v;
+    }
+  }
+  uint32_t inc = 0;
+  float least = 3.4e38f;
+  for (uint32_t f = 0; f < I.nf; f++) {
+    bool touches = false;
+    uint32_t cnt = faceVertCount(w, I, f);
+    for (uint32_t j = 0; j < cnt; j++)
+      if (faceVert(w, I, f, j) == deepest) {
+        touches = true;
+        break;
+      }
+    if (!touches) continue;
+    float4 pf = facePlane(w, I, f);
+    float d = dot3(make_float3(pf.x, pf.y, pf.z), rn);
+    if (d < least) {
+      least = d;
+      inc = f;
+    }
+  }
+  float3 poly[MAX_CLIP], tmp[MAX_CLIP];
+  uint32_t n = min(faceVertCount(w, I, inc), MAX_CLIP);
+  for (uint32_t j = 0; j < n; j++) poly[j] = vert(w, I, faceVert(w, I, inc, j));
+  const uint32_t k = faceVertCount(w, R, refFace);
+  float3 centre = make_float3(0.0f, 0.0f, 0.0f);
+  for (uint32_t j = 0; j < k; j++) centre = centre + vert(w, R, faceVert(w, R, refFace, j));
+  centre = centre / (float)k;
+  for (uint32_t j = 0; j < k && n > 0u; j++) {
+    float3 v0 = vert(w, R, faceVert(w, R, refFace, j));
+    float3 v1 = vert(w, R, faceVert(w, R, refFace, (j + 1u) % k));
+    float3 sd = cross3(v1 - v0, rn);
+    float l = len3(sd);
+    if (l < SAT_AXIS_EPSILON) continue;
+    sd = sd / l;
+    if (dot3(sd, centre - v0) > 0.0f) sd = -sd;
+    n = clipHull(poly, n, tmp, sd, dot3(sd, v0));
+    for (uint32_t m = 0; m < n; m++) poly[m] = tmp[m];
+  }
+  float depth[MAX_CLIP];
+  uint32_t index[MAX_CLIP];
+  bool chosen[MAX_CLIP];
+  uint32_t keep = 0;
+  for (uint32_t m = 0; m < n; m++) {
+    float dist = dot3(rn, poly[m]) - plane.w;
+    if (dist <= PLANE_EPSILON) {
+      tmp[keep] = poly[m];
+      depth[keep] = dist;
+      index[keep] = m;
+      chosen[keep] = false;
+      keep++;
+    }
+  }
+  const uint32_t prefix = ((refIsA ? AXIS_FACE_A : AXIS_FACE_B) << 24) | (min(refFace, 255u) << 16) | (min(inc, 255u) << 8);
+  for (uint32_t c = 0; c < min(keep, (uint32_t)MAX_CONTACTS); c++) {
+    uint32_t pick = 0;
+    float bestScore = -3.4e38f;
+    for (uint32_t m = 0; m < keep; m++) {
+      if (chosen[m]) continue;
+      float score = -depth[m];
+      if (c > 0u) {
+        score = 3.4e38f;
+        for (uint32_t o = 0; o < keep; o++)
+          if (chosen[o]) score = fminf(score, dot3(tmp[m] - tmp[o], tmp[m] - tmp[o]));
+      }
+      if (score > bestScore) {
+        bestScore = score;
+        pick = m;
+      }
+    }
+    chosen[pick] = true;
+    float3 pp = tmp[pick];
+    float3 onRef = pp - rn * depth[pick];
+    addFound(found, refIsA ? onRef : pp, refIsA ? pp : onRef, prefix | min(index[pick], 255u));
+  }
+  if (found.count == 0u) {
+    float3 nAB = refIsA ? rn : -rn;
+    addFound(found, polySupport(w, A, nAB), polySupport(w, B, -nAB), prefix);
+  }
+}
+// Edge contact (wgsl-hull.ts:293-315): closest points of the two edges
+__device__ inline void hullEdgeContact(const DWorld& w, const Poly& A, const Poly& B, const EdgeQuery& q, Found& found) {
+  uint4 ea = edgeOf(w, A, q.ea), eb = edgeOf(w, B, q.eb);
+  float3 p0 = vert(w, A, ea.x), q0 = vert(w, B, eb.x);
+  float3 d1 = vert(w, A, ea.y) - p0, d2 = vert(w, B, eb.y) - q0;
+  float3 r = p0 - q0;
+  float a = dot3(d1, d1), e = dot3(d2, d2), f = dot3(d2, r), c = dot3(d1, r), b = dot3(d1, d2);
+  float denom = a * e - b * b;
+  float s = 0.0f;
+  if (fabsf(denom) > SAT_AXIS_EPSILON * a * e) s = fminf(fmaxf((b * f - c * e) / denom, 0.0f), 1.0f);
+  float t = (b * s + f) / fmaxf(e, SAT_AXIS_EPSILON);
+  if (t < 0.0f) {
+    t = 0.0f;
+    s = fminf(fmaxf(-c / fmaxf(a, SAT_AXIS_EPSILON), 0.0f), 1.0f);
+  } else if (t > 1.0f) {
+    t = 1.0f;
+    s = fminf(fmaxf((b - c) / fmaxf(a, SAT_AXIS_EPSILON), 0.0f), 1.0f);
+  }
+  addFound(found, p0 + d1 * s, q0 + d2 * t, (AXIS_EDGE << 24) | (min(q.ea, 255u) << 8) | min(q.eb, 255u));
+}
+// collidePoly (wgsl-hull.ts:318-341): sat.n from A towards B
+__device__ __noinline__ void collidePoly(const DWorld& w, const Poly& A, const Poly& B, bool faceBias, Sat& sat, Found& found) {
+  float faSep, fbSep;
+  uint32_t faFace, fbFace;
+  queryFaces(w, A, B, faSep, faFace);
+  if (faSep > 0.0f) return;
+  queryFaces(w, B, A, fbSep, fbFace);
+  if (fbSep > 0.0f) return;
+  EdgeQuery eq = queryEdges(w, A, B);
+  if (eq.valid && eq.sep > 0.0f) return;
+  float faceSep = fmaxf(faSep, fbSep);
+  bool edgeWins = eq.valid && eq.sep > 0.95f * faceSep + 0.01f;
+  if (!faceBias) edgeWins = eq.valid && 0.95f * eq.sep > faceSep + 0.01f;
+  if (edgeWins) {
+    sat.kind = AXIS_EDGE;
+    sat.ia = eq.ea;
+    sat.ib = eq.eb;
+    sat.sep = eq.sep;
+    sat.n = eq.n;
+    sat.valid = true;
+    hullEdgeContact(w, A, B, eq, found);
+    return;
+  }
+  if (fbSep > faSep) {
+    float4 pl = facePlane(w, B, fbFace);
+    sat.kind = AXIS_FACE_B;
+    sat.ia = 0u;
+    sat.ib = fbFace;
+    sat.sep = fbSep;
+    sat.n = -make_float3(pl.x, pl.y, pl.z);
+    sat.valid = true;
+    hullFaceContact(w, A, B, false, fbFace, found);
+    return;
+  }
+  float4 pl = facePlane(w, A, faFace);
+  sat.kind = AXIS_FACE_A;
+  sat.ia = faFace;
+  sat.ib = 0u;
+  sat.sep = faSep;
+  sat.n = make_float3(pl.x, pl.y, pl.z);
+  sat.valid = true;
+  hullFaceContact(w, A, B, true, faFace, found);
+}
+__device__ inline float3 segmentPoint(float3 a, float3 b, float3 p) {  // wgsl-hull.ts:344-347
+  float3 d = b - a;
+  return a + d * fminf(fmaxf(dot3(p - a, d) / fmaxf(dot3(d, d), 1e-20f), 0.0f), 1.0f);
+}
+// Sphere (centre c, radius r) against hull X (wgsl-hull.ts:350-405): n from the sphere towards X
+__device__ __noinline__ bool sphereHull(const DWorld& w, float3 c, float r, const Poly& X, float3& onSphere, float3& onHull, float3& nOut) {
+  float deepest = -3.4e38f;
+  uint32_t deepFace = 0;
+  for (uint32_t f = 0; f < X.nf; f++) {
+    float4 pl = facePlane(w, X, f);
+    float s = dot3(make_float3(pl.x, pl.y, pl.z), c) - pl.w;
+    if (s > deepest) {
+      deepest = s;
+      deepFace = f;
+    }
+  }
+  if (deepest > r) return false;
+  if (deepest <= 0.0f) {
+    float4 pl = facePlane(w, X, deepFace);
+    float3 n = make_float3(pl.x, pl.y, pl.z);
+    nOut = -n;
+    onHull = c - n * deepest;
+    onSphere = c - n * r;
+    return true;
+  }
+  float3 best = make_float3(0.0f, 0.0f, 0.0f);
+  float bestDist = 3.4e38f;
+  for (uint32_t f = 0; f < X.nf; f++) {
+    float4 pl = facePlane(w, X, f);
+    float3 pn = make_float3(pl.x, pl.y, pl.z);
+    float s = dot3(pn, c) - pl.w;
+    if (s <= 0.0f) continue;
+    float3 pp = c - pn * s;
+    uint32_t k = faceVertCount(w, X, f);
+    float3 centre = make_float3(0.0f, 0.0f, 0.0f);
+    for (uint32_t j = 0; j < k; j++) centre = centre + vert(w, X, faceVert(w, X, f, j));
+    centre = centre / (float)k;
+    bool inside = true;
+    float3 edgeBest = make_float3(0.0f, 0.0f, 0.0f);
+    float edgeDist = 3.4e38f;
+    for (uint32_t j = 0; j < k; j++) {
+      float3 v0 = vert(w, X, faceVert(w, X, f, j));
+      float3 v1 = vert(w, X, faceVert(w, X, f, (j + 1u) % k));
+      float3 side = cross3(v1 - v0, pn);
+      if (dot3(side, centre - v0) > 0.0f) side = -side;
+      if (dot3(side, pp - v0) > 0.0f) inside = false;
+      float3 q = segmentPoint(v0, v1, c);
+      float dq = dot3(q - c, q - c);
+      if (dq < edgeDist) {
+        edgeDist = dq;
+        edgeBest = q;
+      }
+    }
+    if (!inside) pp = edgeBest;
+    float dist = len3(pp - c);
+    if (dist < bestDist) {
+      bestDist = dist;
+      best = pp;
+    }
+  }
+  if (bestDist > r) return false;
+  float3 n = make_float3(0.0f, 0.0f, 1.0f);
+  if (bestDist > 0.0f) n = (c - best) / bestDist;
+  nOut = -n;
+  onHull = best;
+  onSphere = c - n * r;
+  return true;
+}
+
 __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
   const int cur = p.cur, prev = 1 - cur;
   {
@@ -658,6 +1060,21 @@ __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
     float4 qA = w.rot[a], qB = w.rot[b];
     if (sphereA && sphereB) {
       sphereSphere(A, B, sat, found);
+    } else if (w.hulls && (isHull(w, a) || isHull(w, b))) {
+      if (sphereA || sphereB) {
+        float3 onS, onX, nn;
+        if (sphereA) {
+          bool hit = sphereHull(w, A.c, A.h.x, polyOf(w, b), onS, onX, nn);
+          sat.n = nn;
+          if (hit) addFound(found, onS, onX, SPHERE_FEATURE);
+        } else {
+          bool hit = sphereHull(w, B.c, B.h.x, polyOf(w, a), onS, onX, nn);
+          sat.n = -nn;
+          if (hit) addFound(found, onX, onS, SPHERE_FEATURE);
+        }
+      } else {
+        collidePoly(w, polyOf(w, a), polyOf(w, b), (p.flags & FLAG_FACE_BIAS) != 0u, sat, found);
+      }
     } else if (sphereA || sphereB) {
       float3 onS, onX, nn;
       if (sphereA) {

@@ -73,6 +73,7 @@ struct DWorld {
   // bodies (SoA, capacity bodyCap)
   float4 *pos, *rot, *ipos, *irot, *size, *moment, *ypos, *yrot, *vel, *avel;
   uint2* filters;
+  uint4* hulls;  // hull records (wgsl-hull.ts layout), or null when the world has none
   // joints: JOINT_VEC4 float4 per slot, AoS (a joint row reads the whole record)
   float4* joint;
   int4* jinfo;

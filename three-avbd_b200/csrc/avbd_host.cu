@@ -470,7 +470,48 @@ int avbd_get_params(const avbd_world* w, avbd_params* p) {
 
 static int checkBodies(avbd_world* w, const avbd_body* b, uint32_t n) {
   std::string msg = bodyProblem(b, n);
-  return msg.empty() ? AVBD_OK : fail(w, AVBD_ERR_INVALID, msg);
+  if (!msg.empty()) return fail(w, AVBD_ERR_INVALID, msg);
+  // a shape code is a box, sphere or sail, or SHAPE_HULL + the header offset of a hull of this world
+  for (uint32_t i = 0; i < n; i++) {
+    float s = b[i].shape;
+    if (s == 0.0f || s == 1.0f || s == 2.0f) continue;
+    float h = s - float(AVBD_SHAPE_HULL);
+    if (!(h >= 0.0f) || h != std::floor(h) || !w->hullStarts.count(uint32_t(h)))
+      return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + ": shape " + std::to_string(s) + " is no box, sphere, sail or hull of this world");
+  }
+  return AVBD_OK;
+}
+
+// A packed hull record (header at vec4 0): counts within the narrowphase's limits, every block and
+// index inside the record, finite planes and vertices
+static std::string hullProblem(const uint32_t* u, uint32_t vec4s) {
+  if (vec4s < 2) return "a hull record holds at least its header";
+  const uint32_t vs = u[0], nv = u[1], fs = u[2], nf = u[3], es = u[4], ne = u[5], is = u[6];
+  if (nv < 4 || nv > AVBD_MAX_HULL_VERTICES || nf < 4 || nf > 255 || ne < 6 || ne > 255) return "hull counts out of range";
+  auto inside = [&](uint64_t start, uint64_t count) { return start >= 2 && start + count <= vec4s; };
+  if (!inside(vs, nv) || !inside(fs, 2ull * nf) || !inside(es, ne) || !(is >= 2 && is < vec4s)) return "hull blocks outside the record";
+  auto finite = [&](uint32_t word) {
+    float f;
+    std::memcpy(&f, &u[word], 4);
+    return std::isfinite(f);
+  };
+  for (uint32_t v = 0; v < nv; v++)
+    for (int k = 0; k < 3; k++)
+      if (!finite((vs + v) * 4 + k)) return "hull vertex not finite";
+  for (uint32_t f = 0; f < nf; f++) {
+    const uint32_t o = (fs + 2 * f) * 4;
+    for (int k = 0; k < 4; k++)
+      if (!finite(o + k)) return "hull face plane not finite";
+    const uint32_t first = u[o + 4], count = u[o + 5];
+    if (count < 3 || count > nv || uint64_t(is) * 4 + first + count > uint64_t(vec4s) * 4) return "hull face indices outside the record";
+    for (uint32_t j = 0; j < count; j++)
+      if (u[is * 4 + first + j] >= nv) return "hull face vertex out of range";
+  }
+  for (uint32_t e = 0; e < ne; e++) {
+    const uint32_t* q = u + (es + e) * 4;
+    if (q[0] >= nv || q[1] >= nv || q[2] >= nf || q[3] >= nf) return "hull edge out of range";
+  }
+  return {};
 }
 
 int avbd_add_bodies(avbd_world* w, const avbd_body* bodies, uint32_t n, uint32_t* first) {
@@ -919,6 +960,39 @@ int avbd_set_solve_blocks(avbd_world* w, int blocks) {
   if (blocks > w->maxSolveBlocks) return fail(w, AVBD_ERR_INVALID, "at most " + std::to_string(w->maxSolveBlocks) + " co-resident solve blocks");
   w->solveBlocks = blocks ? blocks : w->maxSolveBlocks;
   w->configGen++;
+  return AVBD_OK;
+}
+
+int avbd_add_hull(avbd_world* w, const uint32_t* packed, uint32_t vec4s, uint32_t* offset) {
+  if (!w || !packed || !offset) return AVBD_ERR_INVALID;
+  std::string msg = hullProblem(packed, vec4s);
+  if (!msg.empty()) return fail(w, AVBD_ERR_INVALID, msg);
+  const uint32_t at = uint32_t(w->hullWords.size() / 4);
+  if (uint64_t(at) + vec4s + AVBD_SHAPE_HULL >= (1ull << 24)) return fail(w, AVBD_ERR_CAPACITY, "hull buffer beyond 2^24 vec4s (f32 shape codes)");
+  std::vector<uint32_t> rec(packed, packed + size_t(vec4s) * 4);
+  for (int k : {0, 2, 4, 6}) rec[k] += at;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  w->hullWords.insert(w->hullWords.end(), rec.begin(), rec.end());
+  const uint32_t total = uint32_t(w->hullWords.size() / 4);
+  if (total > w->hullCapVec4) {
+    uint32_t cap = std::max<uint32_t>(4096, std::max(total, 2 * w->hullCapVec4));
+    uint4* fresh = nullptr;
+    cudaError_t e = dalloc(w, &fresh, cap);
+    if (e != cudaSuccess) {
+      w->hullWords.resize(size_t(at) * 4);
+      return fail(w, AVBD_ERR_CUDA, std::string("hull buffer: ") + cudaGetErrorString(e));
+    }
+    dfree(w, w->d.hulls);
+    w->d.hulls = fresh;
+    w->hullCapVec4 = cap;
+    w->configGen++;  // the step graphs hold the buffer's address
+    CUDA_TRY(w, cudaMemcpy(w->d.hulls, w->hullWords.data(), w->hullWords.size() * 4, cudaMemcpyHostToDevice));
+  } else {
+    CUDA_TRY(w, cudaMemcpy(w->d.hulls + at, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
+  }
+  w->hullStarts.insert(at);
+  *offset = at;
   return AVBD_OK;
 }
 

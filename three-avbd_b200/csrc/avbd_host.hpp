@@ -1,6 +1,7 @@
 // Host-side state shared by the single-world and batched entry points (avbd_host.cu, avbd_batch.cu).
 #pragma once
 #include <cstdint>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -63,6 +64,10 @@ struct avbd_world {
   uint64_t configGen = 1;
   std::string graphNote;
   std::vector<void*> allocations;
+  // hull buffer: host copy of every record (wgsl-hull.ts layout), header offsets, device capacity
+  std::vector<uint32_t> hullWords;
+  std::set<uint32_t> hullStarts;
+  uint32_t hullCapVec4 = 0;
 };
 
 namespace avbd {
