@@ -49,6 +49,7 @@ __global__ void k_begin(DWorld w, StepParams p) {
   c[C_COLORS] = 0;
   c[C_ROUNDS] = 0;
   c[C_ERROR] = 0;
+  c[C_HULL_PAIRS] = 0;
   for (int k = 0; k < 2 * MAX_ROUND_PAIRS + 2; k++) c[C_PENDING + k] = 0;
 }
 
@@ -1045,8 +1046,126 @@ __device__ __noinline__ bool sphereHull(const DWorld& w, float3 c, float r, cons
   return true;
 }
 
+
+// --- hull pairs, one warp per pair ---------------------------------------------------------------------
+// The SAT queries of collidePoly with the faces, and the edge pairs (i, j) in i-major order, dealt to
+// the lanes; each lane evaluates its candidates exactly as the sequential loops do, and a warp
+// reduction keeps the largest separation, the lowest index among equals: the candidate the
+// sequential loop's strict "greater" keeps. The contact itself is built by lane 0.
+__device__ inline void warpArgMax(float& v, uint32_t& i) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    float ov = __shfl_xor_sync(0xffffffffu, v, off);
+    uint32_t oi = __shfl_xor_sync(0xffffffffu, i, off);
+    if (ov > v || (ov == v && oi < i)) {
+      v = ov;
+      i = oi;
+    }
+  }
+}
+__device__ inline void queryFacesWarp(const DWorld& w, const Poly& A, const Poly& B, uint32_t lane, float& sep, uint32_t& face) {
+  float best = -3.4e38f;
+  uint32_t at = 0xffffffffu;
+  for (uint32_t f = lane; f < A.nf; f += 32u) {
+    float4 pl = facePlane(w, A, f);
+    float3 n = make_float3(pl.x, pl.y, pl.z);
+    float s = dot3(n, polySupport(w, B, -n)) - pl.w;
+    if (s > best) {  // lanes take ascending faces: the first of equals stays
+      best = s;
+      at = f;
+    }
+  }
+  warpArgMax(best, at);
+  sep = best;
+  face = at == 0xffffffffu ? 0u : at;
+}
+__device__ inline EdgeQuery queryEdgesWarp(const DWorld& w, const Poly& A, const Poly& B, uint32_t lane) {
+  const float4 toB = qmul(qconj(B.q), A.q);
+  const uint32_t total = A.ne * B.ne;
+  float best = -3.4e38f;
+  uint32_t at = 0xffffffffu;
+  float3 bestN = make_float3(0.0f, 0.0f, 0.0f);
+  for (uint32_t k = lane; k < total; k += 32u) {
+    const uint32_t i = k / B.ne, j = k - i * B.ne;
+    uint4 ea = edgeOf(w, A, i);
+    float3 a = qrotate(toB, faceNormalLocal(w, A, ea.z));
+    float3 b = qrotate(toB, faceNormalLocal(w, A, ea.w));
+    uint4 eb = edgeOf(w, B, j);
+    if (!minkowskiFace(a, b, -faceNormalLocal(w, B, eb.z), -faceNormalLocal(w, B, eb.w))) continue;
+    float3 pa = vert(w, A, ea.x), qa = vert(w, A, ea.y), pb = vert(w, B, eb.x), qb = vert(w, B, eb.y);
+    float3 n = cross3(qa - pa, qb - pb);
+    float l = len3(n);
+    if (l < 1e-5f * len3(qa - pa) * len3(qb - pb)) continue;
+    n = n / l;
+    if (dot3(n, pa - A.c) < 0.0f) n = -n;
+    float s = dot3(n, pb - pa);
+    if (s > best) {
+      best = s;
+      at = k;
+      bestN = n;
+    }
+  }
+  const uint32_t mine = at;
+  warpArgMax(best, at);
+  const uint32_t src = __ffs(__ballot_sync(0xffffffffu, mine == at && at != 0xffffffffu)) - 1u;
+  EdgeQuery out;
+  out.valid = at != 0xffffffffu;
+  out.sep = best;
+  out.ea = out.valid ? at / B.ne : 0u;
+  out.eb = out.valid ? at - out.ea * B.ne : 0u;
+  out.n = out.valid ? make_float3(__shfl_sync(0xffffffffu, bestN.x, src), __shfl_sync(0xffffffffu, bestN.y, src), __shfl_sync(0xffffffffu, bestN.z, src))
+                    : make_float3(0.0f, 0.0f, 0.0f);
+  return out;
+}
+// collidePoly (wgsl-hull.ts:318-341) with the queries spread over the warp; the result is lane 0's
+__device__ void collidePolyWarp(const DWorld& w, const Poly& A, const Poly& B, bool faceBias, uint32_t lane, Sat& sat, Found& found) {
+  float faSep, fbSep;
+  uint32_t faFace, fbFace;
+  queryFacesWarp(w, A, B, lane, faSep, faFace);
+  if (faSep > 0.0f) return;
+  queryFacesWarp(w, B, A, lane, fbSep, fbFace);
+  if (fbSep > 0.0f) return;
+  EdgeQuery eq = queryEdgesWarp(w, A, B, lane);
+  if (eq.valid && eq.sep > 0.0f) return;
+  if (lane != 0u) return;
+  float faceSep = fmaxf(faSep, fbSep);
+  bool edgeWins = eq.valid && eq.sep > 0.95f * faceSep + 0.01f;
+  if (!faceBias) edgeWins = eq.valid && 0.95f * eq.sep > faceSep + 0.01f;
+  if (edgeWins) {
+    sat.kind = AXIS_EDGE;
+    sat.ia = eq.ea;
+    sat.ib = eq.eb;
+    sat.sep = eq.sep;
+    sat.n = eq.n;
+    sat.valid = true;
+    hullEdgeContact(w, A, B, eq, found);
+    return;
+  }
+  if (fbSep > faSep) {
+    float4 pl = facePlane(w, B, fbFace);
+    sat.kind = AXIS_FACE_B;
+    sat.ia = 0u;
+    sat.ib = fbFace;
+    sat.sep = fbSep;
+    sat.n = -make_float3(pl.x, pl.y, pl.z);
+    sat.valid = true;
+    hullFaceContact(w, A, B, false, fbFace, found);
+    return;
+  }
+  float4 pl = facePlane(w, A, faFace);
+  sat.kind = AXIS_FACE_A;
+  sat.ia = faFace;
+  sat.ib = 0u;
+  sat.sep = faSep;
+  sat.n = make_float3(pl.x, pl.y, pl.z);
+  sat.valid = true;
+  hullFaceContact(w, A, B, true, faFace, found);
+}
+
+__device__ __forceinline__ void writeManifold(const DWorld& w, const StepParams& p, uint32_t pi, uint32_t a, uint32_t b, const Box& A, const Box& B, const Sat& sat,
+                              const Found& found, bool anySphere);
+
 __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
-  const int cur = p.cur, prev = 1 - cur;
   {
     uint2 pr = w.pairs[pi];
     uint32_t a = pr.x, b = pr.y;
@@ -1073,7 +1192,9 @@ __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
           if (hit) addFound(found, onX, onS, SPHERE_FEATURE);
         }
       } else {
-        collidePoly(w, polyOf(w, a), polyOf(w, b), (p.flags & FLAG_FACE_BIAS) != 0u, sat, found);
+        // hull against hull or box: one warp per pair (k_hull_narrowphase) writes this slot
+        w.hullPairs[atomicAdd(&w.counters[C_HULL_PAIRS], 1u)] = pi;
+        return;
       }
     } else if (sphereA || sphereB) {
       float3 onS, onX, nn;
@@ -1089,6 +1210,17 @@ __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
     } else {
       collideBoxes(A, B, (p.flags & FLAG_FACE_BIAS) != 0u, sat, found);
     }
+    writeManifold(w, p, pi, a, b, A, B, sat, found, sphereA || sphereB);
+  }
+}
+
+// Pair slot pi's manifold from its contacts: ids, normal and friction, and every point warm-started
+// from last step's point of the same feature (wgsl-collision.ts:812-900)
+__device__ __forceinline__ void writeManifold(const DWorld& w, const StepParams& p, uint32_t pi, uint32_t a, uint32_t b, const Box& A, const Box& B, const Sat& sat,
+                              const Found& found, bool anySphere) {
+  const int cur = p.cur, prev = 1 - cur;
+  {
+    float4 qA = w.rot[a], qB = w.rot[b];
     uint32_t count = found.count;
     float3 n = -sat.n;
     float fa = w.pos[a].w, fb = w.pos[b].w;
@@ -1106,7 +1238,6 @@ __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
     if (count == 0u) return;
     float3 t1, t2;
     orthonormal(n, t1, t2);
-    bool anySphere = sphereA || sphereB;
     uint32_t prevFirst = 0, prevCount = 0;
     int pm = hashFind(w, p, a, b);
     if (pm >= 0) {
@@ -1170,6 +1301,25 @@ __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
       o[K_PEN] = make_float4(pen.x, pen.y, pen.z, c0y);
       o[K_LAM] = make_float4(lam.x, lam.y, lam.z, c0z);
     }
+  }
+}
+
+// The deferred hull pairs, one warp each
+__global__ void __launch_bounds__(256) k_hull_narrowphase(DWorld w, StepParams p) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t total = w.counters[C_HULL_PAIRS];
+  for (uint32_t k = warp; k < total; k += nwarps) {
+    const uint32_t pi = w.hullPairs[k];
+    const uint2 pr = w.pairs[pi];
+    Sat sat;
+    sat.n = make_float3(0.0f, 0.0f, 0.0f);
+    sat.valid = false;
+    Found found;
+    found.count = 0;
+    collidePolyWarp(w, polyOf(w, pr.x), polyOf(w, pr.y), (p.flags & FLAG_FACE_BIAS) != 0u, lane, sat, found);
+    if (lane == 0u) writeManifold(w, p, pi, pr.x, pr.y, makeBox(w, pr.x), makeBox(w, pr.y), sat, found, false);
+    __syncwarp();
   }
 }
 
@@ -1312,6 +1462,10 @@ uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSi
     launches += 8;
   }
   k_narrowphase<<<GS_BLOCKS, 128, 0, s>>>(w, p);
+  if (w.hulls) {
+    k_hull_narrowphase<<<GS_BLOCKS, 256, 0, s>>>(w, p);
+    launches++;
+  }
   return launches;
 }
 

@@ -47,6 +47,7 @@ constexpr int MAX_CLOCKS = 1023;  // barrier timestamps kept per step
 constexpr int CLOCK_T0 = MAX_CLOCKS + 1, CLOCK_WORDS = MAX_CLOCKS + 2;
 constexpr int STAT_WORDS = 16;    // collision ns, solve ns, then counters (pairs, contacts, manifolds, adjacency, incidences, dynamic, colours, rounds, launches, error)
 constexpr int C_STATS_NEXT = 13;  // counter word: next ring entry
+constexpr int C_HULL_PAIRS = 14;  // counter word: pairs deferred to the warp-per-pair hull narrowphase
 // Error bits
 constexpr uint32_t ERR_BARRIER_TIMEOUT = 1, ERR_ADJ_OVERFLOW = 2, ERR_INC_OVERFLOW = 4, ERR_DEPENDENCY_TIMEOUT = 8;
 
@@ -74,6 +75,7 @@ struct DWorld {
   float4 *pos, *rot, *ipos, *irot, *size, *moment, *ypos, *yrot, *vel, *avel;
   uint2* filters;
   uint4* hulls;  // hull records (wgsl-hull.ts layout), or null when the world has none
+  uint32_t* hullPairs;  // pair slots whose narrowphase runs one warp per pair (hull against hull or box)
   // joints: JOINT_VEC4 float4 per slot, AoS (a joint row reads the whole record)
   float4* joint;
   int4* jinfo;

@@ -135,12 +135,14 @@ int allocPairs(avbd_world* w, uint32_t cap) {
   dfree(w, d.adjList);
   dfree(w, d.incList);
   dfree(w, d.laneTable);
+  dfree(w, d.hullPairs);
   w->pairCap = cap;
   w->configGen++;
   w->hashSize = pow2AtLeast(2ull * cap);
   w->adjCap = 2u * (cap + w->jointCap);
   w->incCap = 2u * (cap * MAX_CONTACTS + w->jointCap);
   CUDA_TRY(w, dalloc(w, &d.pairs, cap));
+  CUDA_TRY(w, dalloc(w, &d.hullPairs, cap));
   CUDA_TRY(w, dalloc(w, &d.hash, w->hashSize));
   CUDA_TRY(w, dalloc(w, &d.adjList, w->adjCap));
   CUDA_TRY(w, dalloc(w, &d.incList, w->incCap));
