@@ -25,11 +25,74 @@
 #include <map>
 #include <memory>
 #include <unordered_map>
+#include <tuple>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
+
+// ---------------------------------------------------------------------------------------------
+// Reverse-mode scalar for the FP64 CPU adjoint (test infrastructure): every operation on AD values
+// appends a node (two parents and their partial derivatives) to a tape; sweeping the tape backwards
+// gives the gradient of one output with respect to every input. Comparisons and selections act on
+// the values, so a derivative follows the branch the forward took.
+// ---------------------------------------------------------------------------------------------
+namespace orc {
+struct ADNode { int a, b; double da, db; };
+inline std::vector<ADNode>& adTape() {
+  static std::vector<ADNode> tape;
+  return tape;
+}
+struct AD {
+  double v = 0;
+  int i = -1;
+  AD() {}
+  AD(double x) : v(x) {}
+  static AD node(double v, int a, double da, int b = -1, double db = 0) {
+    AD r(v);
+    if (a < 0 && b < 0) return r;
+    adTape().push_back({a, b, da, db});
+    r.i = int(adTape().size()) - 1;
+    return r;
+  }
+  static AD input(double v) {
+    AD r(v);
+    adTape().push_back({-1, -1, 0, 0});
+    r.i = int(adTape().size()) - 1;
+    return r;
+  }
+  explicit operator double() const { return v; }
+  explicit operator float() const { return float(v); }
+  AD& operator+=(const AD& o);
+  AD& operator-=(const AD& o);
+  AD& operator*=(const AD& o);
+  AD& operator/=(const AD& o);
+};
+inline AD operator+(const AD& x, const AD& y) { return AD::node(x.v + y.v, x.i, 1.0, y.i, 1.0); }
+inline AD operator-(const AD& x, const AD& y) { return AD::node(x.v - y.v, x.i, 1.0, y.i, -1.0); }
+inline AD operator*(const AD& x, const AD& y) { return AD::node(x.v * y.v, x.i, y.v, y.i, x.v); }
+inline AD operator/(const AD& x, const AD& y) { return AD::node(x.v / y.v, x.i, 1.0 / y.v, y.i, -x.v / (y.v * y.v)); }
+inline AD operator-(const AD& x) { return AD::node(-x.v, x.i, -1.0); }
+inline AD& AD::operator+=(const AD& o) { return *this = *this + o; }
+inline AD& AD::operator-=(const AD& o) { return *this = *this - o; }
+inline AD& AD::operator*=(const AD& o) { return *this = *this * o; }
+inline AD& AD::operator/=(const AD& o) { return *this = *this / o; }
+inline bool operator<(const AD& x, const AD& y) { return x.v < y.v; }
+inline bool operator>(const AD& x, const AD& y) { return x.v > y.v; }
+inline bool operator<=(const AD& x, const AD& y) { return x.v <= y.v; }
+inline bool operator>=(const AD& x, const AD& y) { return x.v >= y.v; }
+inline bool operator==(const AD& x, const AD& y) { return x.v == y.v; }
+inline bool operator!=(const AD& x, const AD& y) { return x.v != y.v; }
+}  // namespace orc
+namespace std {
+inline orc::AD sqrt(const orc::AD& x) {
+  double r = std::sqrt(x.v);
+  return orc::AD::node(r, x.i, r > 0 ? 0.5 / r : 0.0);
+}
+inline orc::AD fabs(const orc::AD& x) { return orc::AD::node(std::fabs(x.v), x.i, x.v < 0 ? -1.0 : 1.0); }
+inline bool isfinite(const orc::AD& x) { return std::isfinite(x.v); }
+}  // namespace std
 namespace orc {
 
 // ---------------------------------------------------------------------------------------------
@@ -1699,6 +1762,282 @@ template <class T> struct Solver {
 }  // namespace orc
 
 // ---------------------------------------------------------------------------------------------
+// FP64 adjoint of the GPU-mode step with the contact structure frozen (test infrastructure).
+// A forward rollout of the oracle records, per step, its contact structure: the pairs, each pair's
+// normal (its basis), each point's body-frame anchors and the last-step point it warm-starts from,
+// and the colouring. The replay steps that structure again from any parameters (initial linear and
+// angular velocities, masses with moments in proportion, friction coefficients): C(x-) from the
+// poses, warm starts, the coloured primal sweeps, the duals (penalty ramps, friction cone) and the
+// velocities, as stepGpu does. Its gradient comes from the AD tape, one step at a time, from the
+// step-start states the replay keeps. Only boxes on static bodies and on each other (no joints).
+// ---------------------------------------------------------------------------------------------
+namespace orc {
+struct AdjPoint { double rA[3], rB[3]; int man, prev; };
+struct AdjMan { int a, b; double basis[9]; };
+struct AdjStep { std::vector<AdjMan> mans; std::vector<AdjPoint> pts; std::vector<int> color; int ncol = 0; };
+struct AdjProblem {
+  int n = 0;
+  std::vector<char> dynamic;
+  std::vector<double> pos, rot, prevVel, unitMoment, friction, mass, vel, angVel;  // initial state and nominal params
+  double dt, gravity, alpha, gamma, betaLin, margin;
+  int iterations;
+  std::vector<AdjStep> steps;
+  std::vector<double> target;  // 7 per body
+};
+template <class S> struct AdjState {
+  std::vector<V3<S>> pos, vel, angVel, initPos;
+  std::vector<Q4<S>> rot, initRot, inRot;
+  std::vector<V3<S>> inPos;
+  std::vector<S> prevVz;
+  std::vector<V3<S>> lam, pen;  // per point of the last step replayed
+};
+
+// One replayed step (stepGpu with the recorded structure; manifold.ts / wgsl-solve.ts maths)
+template <class S>
+void adjStep(const AdjProblem& P, const AdjStep& st, AdjState<S>& X, const std::vector<S>& mass, const std::vector<S>& mu) {
+  const int n = P.n;
+  const S dt(P.dt), g(P.gravity), alpha(P.alpha), gamma(P.gamma), beta(P.betaLin);
+  const size_t np = st.pts.size();
+  std::vector<V3<S>> lam(np), pen(np), C0(np);
+  std::vector<S> fr(st.mans.size());
+  for (size_t m = 0; m < st.mans.size(); m++) fr[m] = std::sqrt(mu[st.mans[m].a] * mu[st.mans[m].b]);
+  // points: warm starts from the recorded last-step point, C(x-) at the step-start poses
+  for (size_t k = 0; k < np; k++) {
+    const AdjPoint& q = st.pts[k];
+    const AdjMan& m = st.mans[q.man];
+    V3<S> l{S(0), S(0), S(0)}, pe{S(0), S(0), S(0)};
+    if (q.prev >= 0) { l = X.lam[q.prev]; pe = X.pen[q.prev]; }
+    for (int c = 0; c < 3; c++) {
+      lam[k][c] = l[c] * alpha * gamma;
+      pen[k][c] = clampv(pe[c] * gamma, S(PENALTY_MIN), S(PENALTY_MAX));
+    }
+    V3<S> rA{S(q.rA[0]), S(q.rA[1]), S(q.rA[2])}, rB{S(q.rB[0]), S(q.rB[1]), S(q.rB[2])};
+    V3<S> d = sub3(add3(rotate(X.rot[m.a], rA), X.pos[m.a]), add3(rotate(X.rot[m.b], rB), X.pos[m.b]));
+    for (int c = 0; c < 3; c++) C0[k][c] = S(m.basis[3 * c]) * d[0] + S(m.basis[3 * c + 1]) * d[1] + S(m.basis[3 * c + 2]) * d[2];
+    C0[k][0] = C0[k][0] + S(P.margin);
+  }
+  // warm start bodies (solver.ts:273-295, up = z)
+  for (int b = 0; b < n; b++) {
+    X.initPos[b] = X.pos[b];
+    X.initRot[b] = X.rot[b];
+    if (!P.dynamic[b]) continue;
+    X.inPos[b] = addScaled3(X.pos[b], X.vel[b], dt);
+    X.inPos[b][2] = X.inPos[b][2] + g * (dt * dt);
+    X.inRot[b] = qaddv(X.rot[b], scale3(X.angVel[b], dt));
+    S accelExt = (X.vel[b][2] - X.prevVz[b]) / dt * S(signv(P.gravity));
+    S wgt = clampv(accelExt / S(std::fabs(P.gravity)), S(0), S(1));
+    X.pos[b] = addScaled3(X.pos[b], X.vel[b], dt);
+    X.pos[b][2] = X.pos[b][2] + g * (wgt * dt * dt);
+    X.rot[b] = qaddv(X.rot[b], scale3(X.angVel[b], dt));
+  }
+  std::vector<std::vector<int>> touch(n);
+  for (size_t k = 0; k < np; k++) {
+    const AdjMan& m = st.mans[st.pts[k].man];
+    touch[m.a].push_back(int(k));
+    touch[m.b].push_back(int(k));
+  }
+  // C, F of point k at the current poses (manifold.ts:139-168)
+  auto evalPoint = [&](size_t k, V3<S>& C, V3<S>& F, S& fs, S& bd, V3<S>& rAW, V3<S>& rBW) {
+    const AdjPoint& q = st.pts[k];
+    const AdjMan& m = st.mans[q.man];
+    V3<S> rA{S(q.rA[0]), S(q.rA[1]), S(q.rA[2])}, rB{S(q.rB[0]), S(q.rB[1]), S(q.rB[2])};
+    rAW = rotate(X.rot[m.a], rA);
+    rBW = rotate(X.rot[m.b], rB);
+    V3<S> dAL = sub3(X.pos[m.a], X.initPos[m.a]), dAA = qsub(X.rot[m.a], X.initRot[m.a]);
+    V3<S> dBL = sub3(X.pos[m.b], X.initPos[m.b]), dBA = qsub(X.rot[m.b], X.initRot[m.b]);
+    for (int c = 0; c < 3; c++) {
+      V3<S> bk{S(m.basis[3 * c]), S(m.basis[3 * c + 1]), S(m.basis[3 * c + 2])};
+      S v = C0[k][c] * (S(1) - alpha);
+      v = v + dot(bk, dAL) - dot(bk, dBL) + dot(cross(rAW, bk), dAA) + dot(cross(rBW, neg3(bk)), dBA);
+      C[c] = v;
+      F[c] = pen[k][c] * v + lam[k][c];
+    }
+    F[0] = tmin(F[0], S(0));
+    bd = std::fabs(F[0]) * fr[q.man];
+    fs = std::sqrt(F[1] * F[1] + F[2] * F[2]);
+    if (fs > bd && fs > S(0)) {
+      F[1] = F[1] * (bd / fs);
+      F[2] = F[2] * (bd / fs);
+    }
+  };
+  std::vector<std::vector<int>> buckets(st.ncol);
+  for (int b = 0; b < n; b++)
+    if (P.dynamic[b] && st.color[b] >= 0 && st.color[b] < st.ncol) buckets[st.color[b]].push_back(b);
+  for (int it = 0; it < P.iterations; it++) {
+    for (int c = 0; c < st.ncol; c++) {
+      for (int b : buckets[c]) {
+        S mdt = mass[b] / (dt * dt);
+        V3<S> I{mass[b] * S(P.unitMoment[3 * b]) / (dt * dt), mass[b] * S(P.unitMoment[3 * b + 1]) / (dt * dt), mass[b] * S(P.unitMoment[3 * b + 2]) / (dt * dt)};
+        M3<S> hL = diagonal(mdt, mdt, mdt), hA = diagonal(I[0], I[1], I[2]), hC{};
+        for (auto& e : hC) e = S(0);
+        V3<S> gL = scale3(sub3(X.pos[b], X.inPos[b]), mdt);
+        V3<S> qd = qsub(X.rot[b], X.inRot[b]);
+        V3<S> gA{I[0] * qd[0], I[1] * qd[1], I[2] * qd[2]};
+        for (int k : touch[b]) {
+          const AdjMan& m = st.mans[st.pts[k].man];
+          V3<S> C, F, rAW, rBW;
+          S fs, bd;
+          evalPoint(size_t(k), C, F, fs, bd, rAW, rBW);
+          bool isA = b == m.a;
+          S sg = isA ? S(1) : S(-1);
+          V3<S> r = isA ? rAW : rBW;
+          for (int cc = 0; cc < 3; cc++) {
+            V3<S> l{S(m.basis[3 * cc]) * sg, S(m.basis[3 * cc + 1]) * sg, S(m.basis[3 * cc + 2]) * sg};
+            V3<S> a = cross(r, l);
+            S kk = pen[k][cc];
+            for (int i = 0; i < 3; i++)
+              for (int j = 0; j < 3; j++) {
+                hL[3 * i + j] = hL[3 * i + j] + kk * l[i] * l[j];
+                hA[3 * i + j] = hA[3 * i + j] + kk * a[i] * a[j];
+                hC[3 * i + j] = hC[3 * i + j] + kk * a[i] * l[j];
+              }
+            gL = addScaled3(gL, l, F[cc]);
+            gA = addScaled3(gA, a, F[cc]);
+          }
+        }
+        V3<S> dxL, dxA;
+        solve6(hL, hA, hC, neg3(gL), neg3(gA), dxL, dxA, S(PIVOT_FLOOR));
+        X.pos[b] = add3(X.pos[b], dxL);
+        X.rot[b] = qaddv(X.rot[b], dxA);
+      }
+    }
+    for (size_t k = 0; k < np; k++) {  // duals (manifold.ts:202-217)
+      V3<S> C, F, rAW, rBW;
+      S fs, bd;
+      evalPoint(k, C, F, fs, bd, rAW, rBW);
+      lam[k] = F;
+      if (F[0] < S(0)) pen[k][0] = tmin(pen[k][0] + beta * std::fabs(C[0]), S(PENALTY_MAX));
+      if (fs <= bd) {
+        pen[k][1] = tmin(pen[k][1] + beta * std::fabs(C[1]), S(PENALTY_MAX));
+        pen[k][2] = tmin(pen[k][2] + beta * std::fabs(C[2]), S(PENALTY_MAX));
+      }
+    }
+  }
+  for (int b = 0; b < n; b++) {  // velocities (solver.ts:328-334)
+    X.prevVz[b] = X.vel[b][2];
+    if (!P.dynamic[b]) continue;
+    X.vel[b] = div3(sub3(X.pos[b], X.initPos[b]), dt);
+    X.angVel[b] = div3(qsub(X.rot[b], X.initRot[b]), dt);
+  }
+  X.lam = lam;
+  X.pen = pen;
+}
+
+template <class S> void adjInit(const AdjProblem& P, const double* params, AdjState<S>& X, std::vector<S>& mass, std::vector<S>& mu, bool inputs) {
+  const int n = P.n;
+  auto in = [&](double v) { return inputs ? S(v) : S(v); };
+  X.pos.resize(n); X.vel.resize(n); X.angVel.resize(n); X.initPos.resize(n); X.inPos.resize(n);
+  X.rot.resize(n); X.initRot.resize(n); X.inRot.resize(n); X.prevVz.resize(n);
+  mass.resize(n); mu.resize(n);
+  for (int b = 0; b < n; b++) {
+    for (int k = 0; k < 3; k++) X.pos[b][k] = S(P.pos[3 * b + k]);
+    for (int k = 0; k < 4; k++) X.rot[b][k] = S(P.rot[4 * b + k]);
+    const double* q = params + 8 * b;
+    for (int k = 0; k < 3; k++) { X.vel[b][k] = in(q[k]); X.angVel[b][k] = in(q[3 + k]); }
+    mass[b] = in(q[6]);
+    mu[b] = in(q[7]);
+    X.prevVz[b] = S(P.prevVel[3 * b + 2]);
+  }
+  X.lam.clear();
+  X.pen.clear();
+}
+
+template <class S> S adjLoss(const AdjProblem& P, const AdjState<S>& X) {
+  S L(0);
+  for (int b = 0; b < P.n; b++) {
+    if (!P.dynamic[b]) continue;
+    for (int k = 0; k < 3; k++) { S d = X.pos[b][k] - S(P.target[7 * b + k]); L = L + d * d; }
+    for (int k = 0; k < 4; k++) { S d = X.rot[b][k] - S(P.target[7 * b + 3 + k]); L = L + d * d; }
+  }
+  return L;
+}
+
+// The gradient of the loss with respect to params (8 per body): forward replay keeping every step's
+// start state, then per step (last first) the step taped from its start state and swept backwards.
+inline double adjGradient(const AdjProblem& P, const double* params, double* grad) {
+  const int n = P.n, K = int(P.steps.size());
+  AdjState<double> X;
+  std::vector<double> mass, mu;
+  adjInit(P, params, X, mass, mu, false);
+  std::vector<AdjState<double>> starts;
+  starts.reserve(K);
+  for (int k = 0; k < K; k++) {
+    starts.push_back(X);
+    adjStep(P, P.steps[k], X, mass, mu);
+  }
+  double loss = adjLoss(P, X);
+  // cotangents of the state after step k (bodies; this step's points)
+  std::vector<V3<double>> gPos(n), gVel(n), gAng(n), gLam, gPen;
+  std::vector<Q4<double>> gRot(n);
+  std::vector<double> gPrevVz(n, 0.0);
+  for (int b = 0; b < n; b++) {
+    gPos[b] = {0, 0, 0}; gVel[b] = {0, 0, 0}; gAng[b] = {0, 0, 0}; gRot[b] = {0, 0, 0, 0};
+    if (!P.dynamic[b]) continue;
+    for (int c = 0; c < 3; c++) gPos[b][c] = 2 * (X.pos[b][c] - P.target[7 * b + c]);
+    for (int c = 0; c < 4; c++) gRot[b][c] = 2 * (X.rot[b][c] - P.target[7 * b + 3 + c]);
+  }
+  gLam.assign(X.lam.size(), V3<double>{0, 0, 0});
+  gPen.assign(X.pen.size(), V3<double>{0, 0, 0});
+  std::vector<double> gMass(n, 0.0), gMu(n, 0.0);
+  auto& tape = adTape();
+  for (int k = K - 1; k >= 0; k--) {
+    tape.clear();
+    const AdjState<double>& S0 = starts[k];
+    AdjState<AD> A;
+    auto V = [](const V3<double>& v) { return V3<AD>{AD::input(v[0]), AD::input(v[1]), AD::input(v[2])}; };
+    auto Q = [](const Q4<double>& q) { return Q4<AD>{AD::input(q[0]), AD::input(q[1]), AD::input(q[2]), AD::input(q[3])}; };
+    A.pos.resize(n); A.vel.resize(n); A.angVel.resize(n); A.rot.resize(n); A.prevVz.resize(n);
+    A.initPos.resize(n); A.initRot.resize(n); A.inPos.resize(n); A.inRot.resize(n);
+    for (int b = 0; b < n; b++) {
+      A.pos[b] = V(S0.pos[b]); A.vel[b] = V(S0.vel[b]); A.angVel[b] = V(S0.angVel[b]); A.rot[b] = Q(S0.rot[b]);
+      A.prevVz[b] = AD::input(S0.prevVz[b]);
+    }
+    for (auto& l : S0.lam) A.lam.push_back(V(l));
+    for (auto& p : S0.pen) A.pen.push_back(V(p));
+    std::vector<AD> am(n), au(n);
+    for (int b = 0; b < n; b++) { am[b] = AD::input(mass[b]); au[b] = AD::input(mu[b]); }
+    // input node ids, before the step replaces them
+    AdjState<AD> In = A;
+    adjStep(P, P.steps[k], A, am, au);
+    std::vector<double> adj(tape.size(), 0.0);
+    auto seedV = [&](const V3<AD>& v, const V3<double>& g) { for (int c = 0; c < 3; c++) if (v[c].i >= 0) adj[v[c].i] += g[c]; };
+    auto seedQ = [&](const Q4<AD>& v, const Q4<double>& g) { for (int c = 0; c < 4; c++) if (v[c].i >= 0) adj[v[c].i] += g[c]; };
+    for (int b = 0; b < n; b++) {
+      seedV(A.pos[b], gPos[b]); seedQ(A.rot[b], gRot[b]); seedV(A.vel[b], gVel[b]); seedV(A.angVel[b], gAng[b]);
+      if (A.prevVz[b].i >= 0) adj[A.prevVz[b].i] += gPrevVz[b];
+    }
+    for (size_t p = 0; p < A.lam.size(); p++) { seedV(A.lam[p], gLam[p]); seedV(A.pen[p], gPen[p]); }
+    for (int i = int(tape.size()) - 1; i >= 0; i--) {
+      const ADNode& nd = tape[i];
+      if (adj[i] == 0.0) continue;
+      if (nd.a >= 0) adj[nd.a] += nd.da * adj[i];
+      if (nd.b >= 0) adj[nd.b] += nd.db * adj[i];
+    }
+    auto getV = [&](const V3<AD>& v) { return V3<double>{v[0].i >= 0 ? adj[v[0].i] : 0, v[1].i >= 0 ? adj[v[1].i] : 0, v[2].i >= 0 ? adj[v[2].i] : 0}; };
+    auto getQ = [&](const Q4<AD>& v) { Q4<double> o; for (int c = 0; c < 4; c++) o[c] = v[c].i >= 0 ? adj[v[c].i] : 0; return o; };
+    for (int b = 0; b < n; b++) {
+      gPos[b] = getV(In.pos[b]); gVel[b] = getV(In.vel[b]); gAng[b] = getV(In.angVel[b]); gRot[b] = getQ(In.rot[b]);
+      gPrevVz[b] = In.prevVz[b].i >= 0 ? adj[In.prevVz[b].i] : 0;
+      gMass[b] += am[b].i >= 0 ? adj[am[b].i] : 0;
+      gMu[b] += au[b].i >= 0 ? adj[au[b].i] : 0;
+    }
+    gLam.resize(In.lam.size());
+    gPen.resize(In.pen.size());
+    for (size_t p = 0; p < In.lam.size(); p++) { gLam[p] = getV(In.lam[p]); gPen[p] = getV(In.pen[p]); }
+  }
+  tape.clear();
+  tape.shrink_to_fit();
+  for (int b = 0; b < n; b++) {
+    double* o = grad + 8 * b;
+    for (int c = 0; c < 3; c++) { o[c] = gVel[b][c]; o[3 + c] = gAng[b][c]; }
+    o[6] = gMass[b];
+    o[7] = gMu[b];
+  }
+  return loss;
+}
+}  // namespace orc
+
+// ---------------------------------------------------------------------------------------------
 // C interface for ctypes (tests, smoke, bench cpu_baseline)
 // ---------------------------------------------------------------------------------------------
 using namespace orc;
@@ -1947,6 +2286,94 @@ void orc_color_graph(int n, const unsigned char* dynamic, const int* start, cons
 }
 
 unsigned orc_hash32(unsigned x) { return hash32(x); }
+
+// Adjoint problems (FP64 handle): record `steps` GPU-mode steps of the solver's scene (boxes and
+// static bodies, no joints) from its current state; null if the scene has joints or is FP32.
+void* orc_adj_record(void* h, int steps) {
+  OrcHandle* o = static_cast<OrcHandle*>(h);
+  if (o->fp32) return nullptr;
+  Solver<double>& s = *o->d;
+  for (auto& f : s.forces)
+    if (f->kind == K_JOINT || f->kind == K_SPRING) return nullptr;
+  auto* P = new AdjProblem();
+  const int n = int(s.bodies.size());
+  P->n = n;
+  P->dt = s.dt; P->gravity = s.gravity; P->alpha = s.alpha; P->gamma = s.gamma; P->betaLin = s.betaLin; P->margin = s.contactMargin;
+  P->iterations = s.iterations;
+  for (auto& b : s.bodies) {
+    P->dynamic.push_back(b.mass > 0);
+    for (int k = 0; k < 3; k++) {
+      P->pos.push_back(b.pos[k]); P->prevVel.push_back(b.prevVel[k]); P->vel.push_back(b.vel[k]); P->angVel.push_back(b.angVel[k]);
+      P->unitMoment.push_back(b.mass > 0 ? b.moment[k] / b.mass : 0.0);
+    }
+    for (int k = 0; k < 4; k++) P->rot.push_back(b.rot[k]);
+    P->friction.push_back(b.friction);
+    P->mass.push_back(b.mass);
+  }
+  std::map<std::tuple<int, int, uint32_t>, int> prevIndex;
+  for (int k = 0; k < steps; k++) {
+    s.stepGpu(nullptr);
+    AdjStep st;
+    std::map<std::tuple<int, int, uint32_t>, int> index;
+    for (auto& f : s.forces) {
+      if (f->kind != K_MANIFOLD) continue;
+      auto* m = static_cast<Manifold<double>*>(f.get());
+      AdjMan am;
+      am.a = m->bodyA;
+      am.b = m->bodyB;
+      for (int c = 0; c < 9; c++) am.basis[c] = m->basis[c];
+      int mi = int(st.mans.size());
+      st.mans.push_back(am);
+      for (auto& c : m->contacts) {
+        AdjPoint p;
+        for (int q = 0; q < 3; q++) { p.rA[q] = c.rA[q]; p.rB[q] = c.rB[q]; }
+        p.man = mi;
+        uint32_t feature = c.feature & ~STICK_BIT;
+        auto it = prevIndex.find({am.a, am.b, feature});
+        p.prev = it == prevIndex.end() ? -1 : it->second;
+        index[{am.a, am.b, feature}] = int(st.pts.size());
+        st.pts.push_back(p);
+      }
+    }
+    for (auto& b : s.bodies) st.color.push_back(b.mass > 0 ? int(b.color & 0xffu) : -1);
+    st.ncol = s.lastColors;
+    P->steps.push_back(std::move(st));
+    prevIndex = std::move(index);
+  }
+  P->target.assign(size_t(7) * n, 0.0);
+  return P;
+}
+void orc_adj_destroy(void* a) { delete static_cast<AdjProblem*>(a); }
+int orc_adj_bodies(void* a) { return static_cast<AdjProblem*>(a)->n; }
+int orc_adj_points(void* a, int step) { return int(static_cast<AdjProblem*>(a)->steps[step].pts.size()); }
+// The recorded parameters: per body v0 (3), omega0 (3), mass, friction
+void orc_adj_nominal(void* a, double* params) {
+  auto* P = static_cast<AdjProblem*>(a);
+  for (int b = 0; b < P->n; b++) {
+    for (int k = 0; k < 3; k++) { params[8 * b + k] = P->vel[3 * b + k]; params[8 * b + 3 + k] = P->angVel[3 * b + k]; }
+    params[8 * b + 6] = P->mass[b];
+    params[8 * b + 7] = P->friction[b];
+  }
+}
+void orc_adj_set_target(void* a, const double* target) {
+  auto* P = static_cast<AdjProblem*>(a);
+  P->target.assign(target, target + size_t(7) * P->n);
+}
+// Replay with `params`; the loss, and the final poses (7 per body) into `final_state` if not null
+double orc_adj_loss(void* a, const double* params, double* final_state) {
+  auto* P = static_cast<AdjProblem*>(a);
+  AdjState<double> X;
+  std::vector<double> mass, mu;
+  adjInit(*P, params, X, mass, mu, false);
+  for (auto& st : P->steps) adjStep(*P, st, X, mass, mu);
+  if (final_state)
+    for (int b = 0; b < P->n; b++) {
+      for (int k = 0; k < 3; k++) final_state[7 * b + k] = X.pos[b][k];
+      for (int k = 0; k < 4; k++) final_state[7 * b + 3 + k] = X.rot[b][k];
+    }
+  return adjLoss(*P, X);
+}
+double orc_adj_gradient(void* a, const double* params, double* grad) { return adjGradient(*static_cast<AdjProblem*>(a), params, grad); }
 
 // The hull buffer (gpu/solver.ts:313-338 layout, absolute offsets) the bodies' shape codes name
 void orc_set_hulls(void* h, const unsigned* words, int n) {

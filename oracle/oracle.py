@@ -61,6 +61,19 @@ def lib():
         L.orc_hash32.argtypes = [U]
         L.orc_hash32.restype = U
         L.orc_set_hulls.argtypes = [P, ctypes.POINTER(U), I]
+        L.orc_adj_record.argtypes = [P, I]
+        L.orc_adj_record.restype = P
+        L.orc_adj_destroy.argtypes = [P]
+        L.orc_adj_bodies.argtypes = [P]
+        L.orc_adj_bodies.restype = I
+        L.orc_adj_points.argtypes = [P, I]
+        L.orc_adj_points.restype = I
+        L.orc_adj_nominal.argtypes = [P, D]
+        L.orc_adj_set_target.argtypes = [P, D]
+        L.orc_adj_loss.argtypes = [P, D, D]
+        L.orc_adj_loss.restype = ctypes.c_double
+        L.orc_adj_gradient.argtypes = [P, D, D]
+        L.orc_adj_gradient.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -222,6 +235,9 @@ class Oracle:
     def colors(self) -> np.ndarray:
         return self.bodies()[:, 42].astype(np.uint32)
 
+    def adjoint(self, steps: int) -> 'Adjoint':
+        return Adjoint(self, steps)
+
 
 def set_threads(n: int) -> int:
     """OpenMP threads of the GPU-mode step (0: keep); returns the count in use."""
@@ -251,3 +267,43 @@ def color_graph(n, dynamic, start, nbr, state, cap=64, max_rounds=64):
     L.orc_color_graph(n, dyn.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                       nb.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), s.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), cap, max_rounds, stats)
     return s, {'colors': stats[0], 'clashes': stats[1], 'rounds': stats[2]}
+
+
+class Adjoint:
+    """The FP64 adjoint of the GPU-mode step with the contact structure frozen: `Oracle.adjoint(steps)`
+    records that many steps of the oracle's scene (advancing it); `loss`/`gradient` replay them with
+    any parameters (8 per body: v0, omega0, mass, friction)."""
+
+    def __init__(self, oracle: 'Oracle', steps: int):
+        self.L = oracle.L
+        self.h = self.L.orc_adj_record(oracle.h, steps)
+        if not self.h:
+            raise ValueError('adjoint problems need the FP64 oracle and a scene without joints')
+        self.n = self.L.orc_adj_bodies(self.h)
+        self.steps = steps
+
+    def __del__(self):
+        if getattr(self, 'h', None):
+            self.L.orc_adj_destroy(self.h)
+            self.h = None
+
+    def nominal(self) -> np.ndarray:
+        out = np.zeros(8 * self.n)
+        self.L.orc_adj_nominal(self.h, _dp(out))
+        return out
+
+    def set_target(self, target: np.ndarray):
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+        self.L.orc_adj_set_target(self.h, _dp(t))
+
+    def loss(self, params: np.ndarray, final: bool = False):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        out = np.zeros(7 * self.n)
+        L = self.L.orc_adj_loss(self.h, _dp(p), _dp(out))
+        return (L, out.reshape(-1, 7)) if final else L
+
+    def gradient(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        g = np.zeros(8 * self.n)
+        L = self.L.orc_adj_gradient(self.h, _dp(p), _dp(g))
+        return L, g
