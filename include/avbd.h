@@ -277,6 +277,45 @@ int avbd_write_bodies_async(avbd_world* world, uint32_t first, const avbd_body* 
 int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, const uint32_t* groups_mask, uint32_t* pairs_ab, uint32_t cap, uint32_t* count,
                             void* stream);
 
+/* ---- Adjoint --------------------------------------------------------------------------------------
+ * No counterpart in the reference (it has no differentiation). Gradients of a pose loss
+ * L = sum over dynamic bodies of |x_T - x*|^2 + |q_T - q*|^2 after a recorded rollout, with respect
+ * to every body's initial linear and angular velocity, mass (moments in proportion) and friction
+ * coefficient, in double precision, for batched worlds of boxes on static bodies (no joints). The
+ * step is differentiated with its contact structure frozen from the recording: per step the pairs
+ * and their normal bases, each point's body-frame anchors and the last-step point it warm-starts
+ * from, and the colouring; everything else (C(x-), warm starts, inertial targets, the coloured
+ * primal solves, duals with penalty ramps and friction cone, velocities) is differentiated. The
+ * replay keeps a checkpoint every `checkpoint` steps and recomputes between them. A world holds at
+ * most 128 bodies and 2048 points a step. */
+typedef struct avbd_adjoint avbd_adjoint;
+typedef struct avbd_adjoint_desc {
+  uint32_t worlds, steps, iterations, checkpoint; /* checkpoint 0: every 10 steps */
+  double dt, gravity, alpha, gamma, beta_lin, contact_margin;
+  const uint32_t* world_first_body;    /* worlds + 1 */
+  const double* bodies;                /* 13 per body: pos3 rot4 prev_up_vel unit_moment3 dynamic friction */
+  const uint32_t* step_first_manifold; /* steps x (worlds + 1), global indices */
+  const uint32_t* step_first_point;    /* steps x (worlds + 1) */
+  const int32_t* manifold_bodies;      /* 2 per manifold, world-local (a > b) */
+  const double* manifold_basis;        /* 9 per manifold: rows n (B to A), t1, t2 */
+  const double* point_anchors;         /* 6 per point: rA, rB in body frames */
+  const int32_t* point_manifold;       /* global manifold index */
+  const int32_t* point_prev;           /* global index of the last step's point it warm-starts from, or -1 */
+  const int32_t* colors;               /* steps x bodies (-1: static) */
+  const int32_t* color_counts;         /* steps x worlds */
+  int32_t device;
+} avbd_adjoint_desc;
+int avbd_adjoint_create(const avbd_adjoint_desc* desc, avbd_adjoint** out);
+int avbd_adjoint_destroy(avbd_adjoint* adjoint);
+const char* avbd_adjoint_last_error(const avbd_adjoint* adjoint);
+/* target: 7 per body (pos, rot x y z w) */
+int avbd_adjoint_set_target(avbd_adjoint* adjoint, const double* target);
+/* params: 8 per body (v0 xyz, omega0 xyz, mass, friction); loss per world; final poses 7 per body (or NULL) */
+int avbd_adjoint_forward(avbd_adjoint* adjoint, const double* params, double* loss, double* final_pose);
+/* the reverse sweep, after a replay unless the last call was a forward with the same params: grad 8
+ * per body (as params), loss per world (or NULL) */
+int avbd_adjoint_backward(avbd_adjoint* adjoint, const double* params, double* grad, double* loss);
+
 /* ---- Batched worlds ------------------------------------------------------------------------------
  * No counterpart in the reference, which steps one world per GpuSolver3D (gpu/solver.ts:598). A batch
  * holds many small independent worlds (1 to AVBD_BATCH_MAX_WORLD_BODIES bodies each) and steps them

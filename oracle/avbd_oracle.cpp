@@ -2374,6 +2374,57 @@ double orc_adj_loss(void* a, const double* params, double* final_state) {
   return adjLoss(*P, X);
 }
 double orc_adj_gradient(void* a, const double* params, double* grad) { return adjGradient(*static_cast<AdjProblem*>(a), params, grad); }
+// The recorded structure as flat arrays (one world): totals first (out[0] manifolds, out[1] points)
+void orc_adj_sizes(void* a, int* out) {
+  auto* P = static_cast<AdjProblem*>(a);
+  int m = 0, p = 0;
+  for (auto& st : P->steps) { m += int(st.mans.size()); p += int(st.pts.size()); }
+  out[0] = m;
+  out[1] = p;
+}
+// bodies: 13 per body (pos3 rot4 prevVz unitMoment3 dynamic friction); stepMan/stepPt: steps + 1
+// firsts; manBodies 2, basis 9 per manifold; anchors 6, man, prev per point (indices over all steps);
+// colors: steps x bodies (-1 static); ncol: per step
+void orc_adj_export(void* a, double* bodies, int* stepMan, int* stepPt, int* manBodies, double* basis, double* anchors, int* ptMan, int* ptPrev,
+                    int* colors, int* ncol) {
+  auto* P = static_cast<AdjProblem*>(a);
+  for (int b = 0; b < P->n; b++) {
+    double* r = bodies + 13 * b;
+    for (int k = 0; k < 3; k++) { r[k] = P->pos[3 * b + k]; r[8 + k] = P->unitMoment[3 * b + k]; }
+    for (int k = 0; k < 4; k++) r[3 + k] = P->rot[4 * b + k];
+    r[7] = P->prevVel[3 * b + 2];
+    r[11] = P->dynamic[b] ? 1.0 : 0.0;
+    r[12] = P->friction[b];
+  }
+  int m = 0, p = 0, prevFirst = 0;
+  for (size_t s = 0; s < P->steps.size(); s++) {
+    const AdjStep& st = P->steps[s];
+    stepMan[s] = m;
+    stepPt[s] = p;
+    for (auto& am : st.mans) {
+      manBodies[2 * m] = am.a;
+      manBodies[2 * m + 1] = am.b;
+      for (int c = 0; c < 9; c++) basis[9 * m + c] = am.basis[c];
+      m++;
+    }
+    for (auto& q : st.pts) {
+      for (int k = 0; k < 3; k++) { anchors[6 * p + k] = q.rA[k]; anchors[6 * p + 3 + k] = q.rB[k]; }
+      ptMan[p] = stepMan[s] + q.man;
+      ptPrev[p] = q.prev < 0 ? -1 : prevFirst + q.prev;
+      p++;
+    }
+    prevFirst = stepPt[s];
+    for (int b = 0; b < P->n; b++) colors[s * P->n + b] = st.color[b];
+    ncol[s] = st.ncol;
+  }
+  stepMan[P->steps.size()] = m;
+  stepPt[P->steps.size()] = p;
+}
+double orc_adj_param(void* a, int which) {  // 0 dt 1 gravity 2 alpha 3 gamma 4 betaLin 5 margin 6 iterations
+  auto* P = static_cast<AdjProblem*>(a);
+  double v[7] = {P->dt, P->gravity, P->alpha, P->gamma, P->betaLin, P->margin, double(P->iterations)};
+  return v[which];
+}
 
 // The hull buffer (gpu/solver.ts:313-338 layout, absolute offsets) the bodies' shape codes name
 void orc_set_hulls(void* h, const unsigned* words, int n) {

@@ -74,6 +74,10 @@ def lib():
         L.orc_adj_loss.restype = ctypes.c_double
         L.orc_adj_gradient.argtypes = [P, D, D]
         L.orc_adj_gradient.restype = ctypes.c_double
+        L.orc_adj_sizes.argtypes = [P, ctypes.POINTER(I)]
+        L.orc_adj_export.argtypes = [P, D] + [ctypes.POINTER(I)] * 3 + [D, D] + [ctypes.POINTER(I)] * 4
+        L.orc_adj_param.argtypes = [P, I]
+        L.orc_adj_param.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -301,6 +305,23 @@ class Adjoint:
         out = np.zeros(7 * self.n)
         L = self.L.orc_adj_loss(self.h, _dp(p), _dp(out))
         return (L, out.reshape(-1, 7)) if final else L
+
+    def export(self) -> dict:
+        """The recorded structure as flat arrays (indices over all steps of this one world)."""
+        ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        sz = np.zeros(2, dtype=np.int32)
+        self.L.orc_adj_sizes(self.h, ip(sz))
+        nm, npts, n, K = int(sz[0]), int(sz[1]), self.n, self.steps
+        out = {'bodies': np.zeros(13 * n), 'step_man': np.zeros(K + 1, np.int32), 'step_pt': np.zeros(K + 1, np.int32),
+               'man_bodies': np.zeros(2 * max(nm, 1), np.int32), 'basis': np.zeros(9 * max(nm, 1)), 'anchors': np.zeros(6 * max(npts, 1)),
+               'pt_man': np.zeros(max(npts, 1), np.int32), 'pt_prev': np.zeros(max(npts, 1), np.int32), 'colors': np.zeros(K * n, np.int32),
+               'ncol': np.zeros(K, np.int32)}
+        self.L.orc_adj_export(self.h, _dp(out['bodies']), ip(out['step_man']), ip(out['step_pt']), ip(out['man_bodies']), _dp(out['basis']),
+                              _dp(out['anchors']), ip(out['pt_man']), ip(out['pt_prev']), ip(out['colors']), ip(out['ncol']))
+        out['params'] = {k: self.L.orc_adj_param(self.h, i) for i, k in enumerate(['dt', 'gravity', 'alpha', 'gamma', 'beta_lin', 'contact_margin',
+                                                                                     'iterations'])}
+        out['n'], out['steps'], out['manifolds'], out['points'] = n, K, nm, npts
+        return out
 
     def gradient(self, params: np.ndarray):
         p = np.ascontiguousarray(params, dtype=np.float64)

@@ -151,6 +151,12 @@ SIGNATURES = {
     'avbd_hull_build': ([VP, U, PU, U, PU, ctypes.POINTER(HullProps)], I),
     'avbd_add_hull': ([P, PU, U, PU], I),
     'avbd_find_pairs_noalloc': ([VP, U, PU, PU, U, PU, VP], I),
+    'avbd_adjoint_create': ([VP, ctypes.POINTER(P)], I),
+    'avbd_adjoint_destroy': ([P], I),
+    'avbd_adjoint_last_error': ([P], ctypes.c_char_p),
+    'avbd_adjoint_set_target': ([P, ctypes.POINTER(ctypes.c_double)], I),
+    'avbd_adjoint_forward': ([P] + [ctypes.POINTER(ctypes.c_double)] * 3, I),
+    'avbd_adjoint_backward': ([P] + [ctypes.POINTER(ctypes.c_double)] * 3, I),
     'avbd_batch_create': ([ctypes.POINTER(BatchConfig), ctypes.POINTER(P)], I),
     'avbd_batch_destroy': ([P], I),
     'avbd_batch_last_error': ([P], ctypes.c_char_p),

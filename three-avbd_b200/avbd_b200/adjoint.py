@@ -1,0 +1,129 @@
+"""The adjoint of the step (avbd_adjoint_* in include/avbd.h): gradients of a final-pose loss with
+respect to every body's initial velocities, mass and friction, for batched worlds, with the contact
+structure frozen from a recorded rollout.
+
+A recording is one world's structure as flat arrays (`bodies` 13 per body; per step its manifolds
+with their bases and points with their anchors and warm-start source; the colouring); `Adjoint`
+takes a list of them, one per world.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import AvbdError
+
+
+class AdjointDesc(ctypes.Structure):
+    _fields_ = [('worlds', ctypes.c_uint32), ('steps', ctypes.c_uint32), ('iterations', ctypes.c_uint32), ('checkpoint', ctypes.c_uint32),
+                ('dt', ctypes.c_double), ('gravity', ctypes.c_double), ('alpha', ctypes.c_double), ('gamma', ctypes.c_double),
+                ('beta_lin', ctypes.c_double), ('contact_margin', ctypes.c_double)] + \
+               [(n, ctypes.c_void_p) for n in ('world_first_body', 'bodies', 'step_first_manifold', 'step_first_point', 'manifold_bodies',
+                                               'manifold_basis', 'point_anchors', 'point_manifold', 'point_prev', 'colors', 'color_counts')] + \
+               [('device', ctypes.c_int32)]
+
+
+def combine(records: list) -> dict:
+    """World recordings (indices over their own steps) as one batch, step-major: step s holds every
+    world's manifolds and points of that step, world by world."""
+    W, K = len(records), records[0]['steps']
+    assert all(r['steps'] == K for r in records)
+    nbs = [r['n'] for r in records]
+    first_body = np.concatenate([[0], np.cumsum(nbs)]).astype(np.uint32)
+    bodies = np.concatenate([r['bodies'] for r in records])
+    step_man = np.zeros(K * (W + 1), np.uint32)
+    step_pt = np.zeros(K * (W + 1), np.uint32)
+    mb, basis, anchors, pt_man, pt_prev = [], [], [], [], []
+    m = p = 0
+    gpt = {}  # (world, step, local point) -> global point
+    for s in range(K):
+        for w, r in enumerate(records):
+            step_man[s * (W + 1) + w] = m
+            step_pt[s * (W + 1) + w] = p
+            m0, m1 = int(r['step_man'][s]), int(r['step_man'][s + 1])
+            p0, p1 = int(r['step_pt'][s]), int(r['step_pt'][s + 1])
+            mb.append(r['man_bodies'][2 * m0:2 * m1])
+            basis.append(r['basis'][9 * m0:9 * m1])
+            anchors.append(r['anchors'][6 * p0:6 * p1])
+            pt_man.append(r['pt_man'][p0:p1] - m0 + m)
+            prev = r['pt_prev'][p0:p1].copy()
+            if s > 0:
+                q0 = int(r['step_pt'][s - 1])
+                base = gpt[(w, s - 1)]
+                prev = np.where(prev >= 0, prev - q0 + base, -1)
+            pt_prev.append(prev)
+            gpt[(w, s)] = p
+            m += m1 - m0
+            p += p1 - p0
+        step_man[s * (W + 1) + W] = m
+        step_pt[s * (W + 1) + W] = p
+    colors = np.concatenate([np.concatenate([r['colors'][s * r['n']:(s + 1) * r['n']] for r in records]) for s in range(K)]).astype(np.int32)
+    ncol = np.array([[r['ncol'][s] for r in records] for s in range(K)], np.int32).reshape(-1)
+    cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0), dtype=dt)
+    return {'W': W, 'K': K, 'first_body': first_body, 'bodies': np.ascontiguousarray(bodies, np.float64), 'step_man': step_man, 'step_pt': step_pt,
+            'man_bodies': cat(mb, np.int32), 'basis': cat(basis, np.float64), 'anchors': cat(anchors, np.float64), 'pt_man': cat(pt_man, np.int32),
+            'pt_prev': cat(pt_prev, np.int32), 'colors': colors, 'ncol': ncol, 'params': records[0]['params'], 'nb': int(first_body[-1])}
+
+
+class Adjoint:
+    """Double-precision replay and reverse sweep on one B200 for a batch of recorded worlds."""
+
+    def __init__(self, records: list, checkpoint: int = 10, device: int = 0):
+        self.lib = _abi.load()
+        c = combine(records)
+        self._keep = c
+        P = c['params']
+        ptr = lambda a: a.ctypes.data if a.size else None
+        d = AdjointDesc(worlds=c['W'], steps=c['K'], iterations=int(P['iterations']), checkpoint=checkpoint, dt=P['dt'], gravity=P['gravity'],
+                        alpha=P['alpha'], gamma=P['gamma'], beta_lin=P['beta_lin'], contact_margin=P['contact_margin'],
+                        world_first_body=ptr(c['first_body']), bodies=ptr(c['bodies']), step_first_manifold=ptr(c['step_man']),
+                        step_first_point=ptr(c['step_pt']), manifold_bodies=ptr(c['man_bodies']), manifold_basis=ptr(c['basis']),
+                        point_anchors=ptr(c['anchors']), point_manifold=ptr(c['pt_man']), point_prev=ptr(c['pt_prev']), colors=ptr(c['colors']),
+                        color_counts=ptr(c['ncol']), device=device)
+        self.handle = ctypes.c_void_p()
+        code = self.lib.avbd_adjoint_create(ctypes.byref(d), ctypes.byref(self.handle))
+        if code != _abi.AVBD_OK:
+            raise AvbdError(code, 'avbd_adjoint_create failed')
+        self.worlds, self.bodies = c['W'], c['nb']
+        self.first_body = c['first_body']
+
+    def destroy(self):
+        if getattr(self, 'handle', None) and self.handle.value:
+            self.lib.avbd_adjoint_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def _check(self, code):
+        if code != _abi.AVBD_OK:
+            msg = self.lib.avbd_adjoint_last_error(self.handle)
+            raise AvbdError(code, msg.decode() if msg else '')
+
+    def set_target(self, target: np.ndarray):
+        t = np.ascontiguousarray(target, np.float64).reshape(-1)
+        self._check(self.lib.avbd_adjoint_set_target(self.handle, t.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def forward(self, params: np.ndarray):
+        """Loss per world and final poses (7 per body)."""
+        p = np.ascontiguousarray(params, np.float64).reshape(-1)
+        loss = np.zeros(self.worlds)
+        fin = np.zeros(7 * self.bodies)
+        D = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.avbd_adjoint_forward(self.handle, p.ctypes.data_as(D), loss.ctypes.data_as(D), fin.ctypes.data_as(D)))
+        return loss, fin.reshape(-1, 7)
+
+    def backward(self, params: np.ndarray):
+        """Loss per world and the gradient (8 per body: v0, omega0, mass, friction)."""
+        p = np.ascontiguousarray(params, np.float64).reshape(-1)
+        loss = np.zeros(self.worlds)
+        g = np.zeros(8 * self.bodies)
+        D = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.avbd_adjoint_backward(self.handle, p.ctypes.data_as(D), g.ctypes.data_as(D), loss.ctypes.data_as(D)))
+        return loss, g

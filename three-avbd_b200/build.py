@@ -21,6 +21,7 @@ UNITS = {
     'avbd_host.cu': [],
     'avbd_batch.cu': [],
     'avbd_hull.cu': [],
+    'avbd_adjoint.cu': [],
 }
 
 

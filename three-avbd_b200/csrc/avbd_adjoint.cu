@@ -1,0 +1,1166 @@
+// The adjoint of the step (batched worlds, double precision): gradients of a pose loss with respect
+// to every body's initial linear and angular velocity, mass and friction coefficient.
+//
+// The step is differentiated with its contact structure frozen from a recorded rollout: per step,
+// the pairs with their normals, each point's body-frame anchors and the last-step point it warm-
+// starts from, and the colouring. Everything else is differentiated: C(x-) from the poses, the warm
+// starts, the inertial targets and the accelerated warm-start guess, the coloured Gauss-Seidel
+// primal solves (6x6 LDLT), the duals (lambda, penalty ramps, friction cone) and the velocities.
+// The replay forward keeps the state every `checkpoint` steps; the reverse pass recomputes a
+// segment from its checkpoint, then each step with per-iteration snapshots, and sweeps the step
+// backwards: velocities, then per iteration the duals and the colours in reverse, then the warm
+// starts. One block per world; a thread per body (primal) or per point (duals, warm starts).
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "avbd.h"
+#include "avbd_adjoint_math.cuh"
+
+using namespace avbd::adj;
+
+namespace {
+
+constexpr int ADJ_THREADS = 128;     // bodies of a world at most
+constexpr int ADJ_MAX_POINTS = 2048;  // points of a world in one step at most
+constexpr double PEN_MIN = 1.0, PEN_MAX = 1e10, PIVOT = 1e-5;
+
+struct AdjDev {
+  int W, K, I, ck;
+  double dt, g, alpha, gamma, beta, margin;
+  const int* bodyFirst;  // W + 1
+  const D3* pos0;
+  const D4* rot0;
+  const double* prevVz0;
+  const D3* unitMoment;
+  const int* dynamic;
+  const double* fricStatic;
+  const int* manFirst;  // K x (W + 1), global manifold index
+  const int* ptFirst;   // K x (W + 1)
+  const int2* manAB;    // world-local bodies
+  const D3* basis;      // 3 rows per manifold
+  const D3* rA;
+  const D3* rB;
+  const int* ptMan;   // global manifold index
+  const int* ptPrev;  // global index into the previous step's points, or -1
+  const int* color;   // K x bodies (-1: static)
+  const int* ncol;    // K x W
+  int nb, maxPts;
+  // params (8 per body), target (7 per body)
+  const double* params;
+  const double* target;
+  // state (per body) and per-world point buffers
+  D3 *pos, *vel, *ang, *ipos, *ypos;
+  D4 *rot, *irot, *yrot;
+  double* pvz;
+  D3 *lam, *pen, *lamP, *penP, *C0;  // world w's points at w * maxPts
+  // checkpoints: every ck steps, the body state and the last step's points
+  D3 *ckPos, *ckVel, *ckAng, *ckLam, *ckPen;
+  D4* ckRot;
+  double* ckPvz;
+  // segment: the start state of each step of a segment
+  D3 *sgPos, *sgVel, *sgAng, *sgLam, *sgPen;
+  D4* sgRot;
+  double* sgPvz;
+  // per step of a segment: its per-iteration snapshots (I + 1), start poses, inertial targets, C0
+  D3 *snPos, *snLam, *snPen;
+  D4* snRot;
+  D3 *stIpos, *stYpos, *stC0;
+  D4 *stIrot, *stYrot;
+  // cotangents
+  D3 *gPos, *gVel, *gAng, *gIpos, *gYpos;
+  D4 *gRot, *gIrot, *gYrot;
+  double *gPvz, *gMass, *gMu;
+  D3 *gLam, *gPen, *gLamP, *gPenP, *gC0;
+  double* loss;  // per world
+  double* finalPose;
+};
+
+__device__ inline void atomicAdd3(D3* a, D3 v) {
+  atomicAdd(&a->x, v.x);
+  atomicAdd(&a->y, v.y);
+  atomicAdd(&a->z, v.z);
+}
+__device__ inline void atomicAdd4(D4* a, D4 v) {
+  atomicAdd(&a->x, v.x);
+  atomicAdd(&a->y, v.y);
+  atomicAdd(&a->z, v.z);
+  atomicAdd(&a->w, v.w);
+}
+
+// The world's view of step s: its manifolds, points and incidence (CSR in shared memory)
+struct StepView {
+  int m0, m1, p0, p1, b0, nb, ncol;
+  const int* color;
+};
+__device__ inline StepView viewOf(const AdjDev& D, int s, int w) {
+  StepView v;
+  v.m0 = D.manFirst[s * (D.W + 1) + w];
+  v.m1 = D.manFirst[s * (D.W + 1) + w + 1];
+  v.p0 = D.ptFirst[s * (D.W + 1) + w];
+  v.p1 = D.ptFirst[s * (D.W + 1) + w + 1];
+  v.b0 = D.bodyFirst[w];
+  v.nb = D.bodyFirst[w + 1] - v.b0;
+  v.ncol = D.ncol[s * D.W + w];
+  v.color = D.color + (size_t)s * D.nb + v.b0;
+  return v;
+}
+
+__shared__ int s_incStart[ADJ_THREADS + 1];
+__shared__ int s_inc[2 * ADJ_MAX_POINTS];
+
+__device__ void buildIncidence(const AdjDev& D, const StepView& v) {
+  for (int i = threadIdx.x; i <= v.nb; i += blockDim.x) s_incStart[i] = 0;
+  __syncthreads();
+  for (int k = v.p0 + threadIdx.x; k < v.p1; k += blockDim.x) {
+    int2 ab = D.manAB[D.ptMan[k]];
+    atomicAdd(&s_incStart[ab.x + 1], 1);
+    atomicAdd(&s_incStart[ab.y + 1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 0; i < v.nb; i++) s_incStart[i + 1] += s_incStart[i];
+  __syncthreads();
+  // fill in point order per body (a deterministic order: sequential per body)
+  if (threadIdx.x < v.nb) {
+    int b = threadIdx.x, o = s_incStart[b];
+    for (int k = v.p0; k < v.p1; k++) {
+      int2 ab = D.manAB[D.ptMan[k]];
+      if (ab.x == b || ab.y == b) s_inc[o++] = k;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ inline double mu(const AdjDev& D, int gb) { return D.dynamic[gb] ? D.params[8 * gb + 7] : D.fricStatic[gb]; }
+__device__ inline double mass(const AdjDev& D, int gb) { return D.params[8 * gb + 6]; }
+
+// C, F of point k (manifold.ts:139-168 with the GPU's rules) at poses (xa, qa), (xb, qb) and the
+// step-start poses; lam, pen the point's current values
+struct PointEval {
+  D3 rAW, rBW, dAL, dAA, dBL, dBA, C, Fraw, F;
+  double fs, bd, fr;
+  bool clamped;
+};
+__device__ inline void evalPoint(const AdjDev& D, int k, D3 xa, D4 qa, D3 xa0, D4 qa0, D3 xb, D4 qb, D3 xb0, D4 qb0, D3 c0, D3 lam, D3 pen, double fr,
+                                 PointEval& e) {
+  const D3* B = D.basis + 3 * D.ptMan[k];
+  e.rAW = rotate(qa, D.rA[k]);
+  e.rBW = rotate(qb, D.rB[k]);
+  e.dAL = xa - xa0;
+  e.dAA = qsub(qa, qa0);
+  e.dBL = xb - xb0;
+  e.dBA = qsub(qb, qb0);
+  for (int c = 0; c < 3; c++) {
+    D3 bk = B[c];
+    double v = comp(c0, c) * (1.0 - D.alpha);
+    v = v + dot(bk, e.dAL) - dot(bk, e.dBL) + dot(cross(e.rAW, bk), e.dAA) + dot(cross(e.rBW, -bk), e.dBA);
+    setComp(e.C, c, v);
+    setComp(e.Fraw, c, comp(pen, c) * v + comp(lam, c));
+  }
+  e.F = e.Fraw;
+  e.F.x = fmin(e.F.x, 0.0);
+  e.fr = fr;
+  e.bd = fabs(e.F.x) * fr;
+  e.fs = sqrt(e.F.y * e.F.y + e.F.z * e.F.z);
+  e.clamped = e.fs > e.bd && e.fs > 0.0;
+  if (e.clamped) {
+    e.F.y = e.F.y * (e.bd / e.fs);
+    e.F.z = e.F.z * (e.bd / e.fs);
+  }
+}
+
+// The cotangents of (C, lam, pen, friction) from the cotangent of F
+__device__ inline void evalFVjp(const PointEval& e, D3 lam, D3 pen, D3 gF, D3& gC, D3& gLam, D3& gPen, double& gFr) {
+  D3 gRaw{0, 0, 0};
+  double gFx = gF.x;  // of the min'd normal force
+  if (e.clamped) {
+    double s = e.bd / e.fs;
+    double dotFR = gF.y * e.Fraw.y + gF.z * e.Fraw.z;
+    gRaw.y = s * gF.y - (e.bd / (e.fs * e.fs * e.fs)) * dotFR * e.Fraw.y;
+    gRaw.z = s * gF.z - (e.bd / (e.fs * e.fs * e.fs)) * dotFR * e.Fraw.z;
+    double gBd = dotFR / e.fs;
+    gFr += gBd * fabs(e.F.x);
+    gFx += gBd * e.fr * (e.F.x < 0.0 ? -1.0 : 1.0);
+  } else {
+    gRaw.y = gF.y;
+    gRaw.z = gF.z;
+  }
+  gRaw.x = e.Fraw.x < 0.0 ? gFx : 0.0;  // min(raw, 0)
+  for (int c = 0; c < 3; c++) {
+    double r = comp(gRaw, c);
+    setComp(gC, c, comp(gC, c) + comp(pen, c) * r);
+    setComp(gPen, c, comp(gPen, c) + comp(e.C, c) * r);
+    setComp(gLam, c, comp(gLam, c) + r);
+  }
+}
+
+// The cotangents of the poses, step-start poses and C0 from the cotangent of C
+__device__ inline void evalCVjp(const AdjDev& D, int k, D4 qa, D4 qa0, D4 qb, D4 qb0, const PointEval& e, D3 gC, D3& gXa, D4& gQa, D3& gXa0, D4& gQa0,
+                                D3& gXb, D4& gQb, D3& gXb0, D4& gQb0, D3& gC0) {
+  const D3* B = D.basis + 3 * D.ptMan[k];
+  D3 gdAL{0, 0, 0}, gdAA{0, 0, 0}, gdBL{0, 0, 0}, gdBA{0, 0, 0}, grA{0, 0, 0}, grB{0, 0, 0};
+  for (int c = 0; c < 3; c++) {
+    double g = comp(gC, c);
+    D3 bk = B[c];
+    setComp(gC0, c, comp(gC0, c) + g * (1.0 - D.alpha));
+    gdAL += bk * g;
+    gdBL -= bk * g;
+    gdAA += cross(e.rAW, bk) * g;
+    gdBA += cross(e.rBW, -bk) * g;
+    grA += cross(bk, e.dAA) * g;
+    grB += cross(-bk, e.dBA) * g;
+  }
+  gXa += gdAL;
+  gXa0 -= gdAL;
+  gXb += gdBL;
+  gXb0 -= gdBL;
+  qsubVjp(qa, qa0, gdAA, gQa, gQa0);
+  qsubVjp(qb, qb0, gdBA, gQb, gQb0);
+  gQa += rotateVjpQ(qa, D.rA[k], grA);
+  gQb += rotateVjpQ(qb, D.rB[k], grB);
+}
+
+// The 6x6 system of body gb (its inertia and its points' rows) at the current poses
+__device__ inline void buildSystem(const AdjDev& D, const StepView& v, int wpt, int gb, int lb, Sys6& S, D3& gl, D3& ga, const D3* P, const D4* Q,
+                                   const D3* lamCur, const D3* penCur) {
+  const double dt2 = D.dt * D.dt;
+  const double m = mass(D, gb) / dt2;
+  D3 Iu = D.unitMoment[gb];
+  D3 I = Iu * (mass(D, gb) / dt2);
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) S.A[i][j] = 0.0;
+  S.A[0][0] = S.A[1][1] = S.A[2][2] = m;
+  S.A[3][3] = I.x;
+  S.A[4][4] = I.y;
+  S.A[5][5] = I.z;
+  gl = (P[gb] - D.ypos[gb]) * m;
+  D3 qd = qsub(Q[gb], D.yrot[gb]);
+  ga = D3{I.x * qd.x, I.y * qd.y, I.z * qd.z};
+  for (int t = s_incStart[lb]; t < s_incStart[lb + 1]; t++) {
+    int k = s_inc[t];
+    int2 ab = D.manAB[D.ptMan[k]];
+    int a = v.b0 + ab.x, b = v.b0 + ab.y;
+    double fr = sqrt(mu(D, a) * mu(D, b));
+    PointEval e;
+    int lk = k - v.p0;
+    evalPoint(D, k, P[a], Q[a], D.ipos[a], D.irot[a], P[b], Q[b], D.ipos[b], D.irot[b], D.C0[wpt + lk], lamCur[wpt + lk], penCur[wpt + lk], fr, e);
+    bool isA = gb == a;
+    double sg = isA ? 1.0 : -1.0;
+    D3 r = isA ? e.rAW : e.rBW;
+    const D3* B = D.basis + 3 * D.ptMan[k];
+    for (int c = 0; c < 3; c++) {
+      D3 l = B[c] * sg;
+      D3 aa = cross(r, l);
+      double kk = comp(penCur[wpt + lk], c);
+      double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
+      for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) S.A[i][j] += kk * J[i] * J[j];
+      gl += l * comp(e.F, c);
+      ga += aa * comp(e.F, c);
+    }
+  }
+}
+
+// One step of the replay (the oracle's stepGpu with the recorded structure). With snapshots, the
+// poses after the warm start and after each iteration, and the points after each dual, are kept.
+__device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
+  const bool snapshots = slot >= 0;
+  const size_t snB = snapshots ? (size_t)slot * (D.I + 1) * D.nb : 0, snP = snapshots ? (size_t)slot * (D.I + 1) * D.W * D.maxPts : 0;
+  const StepView v = viewOf(D, s, w);
+  const int wpt = w * D.maxPts;
+  const int np = v.p1 - v.p0;
+  const double dt = D.dt;
+  buildIncidence(D, v);
+  // points: warm starts and C(x-)
+  for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+    int k = v.p0 + lk;
+    int pv = D.ptPrev[k];
+    D3 l{0, 0, 0}, pe{0, 0, 0};
+    if (pv >= 0) {
+      int plk = pv - D.ptFirst[(s - 1) * (D.W + 1) + w];
+      l = D.lamP[wpt + plk];
+      pe = D.penP[wpt + plk];
+    }
+    D3 lw = l * (D.alpha * D.gamma), pw;
+    for (int c = 0; c < 3; c++) setComp(pw, c, fmin(fmax(comp(pe, c) * D.gamma, PEN_MIN), PEN_MAX));
+    int2 ab = D.manAB[D.ptMan[k]];
+    int a = v.b0 + ab.x, b = v.b0 + ab.y;
+    D3 d = (rotate(D.rot[a], D.rA[k]) + D.pos[a]) - (rotate(D.rot[b], D.rB[k]) + D.pos[b]);
+    const D3* B = D.basis + 3 * D.ptMan[k];
+    D3 c0{dot(B[0], d) + D.margin, dot(B[1], d), dot(B[2], d)};
+    D.lam[wpt + lk] = lw;
+    D.pen[wpt + lk] = pw;
+    D.C0[wpt + lk] = c0;
+  }
+  __syncthreads();
+  // bodies: inertial targets and the warm-start guess (solver.ts:273-295, up = z)
+  if (threadIdx.x < v.nb) {
+    int gb = v.b0 + threadIdx.x;
+    D.ipos[gb] = D.pos[gb];
+    D.irot[gb] = D.rot[gb];
+    if (D.dynamic[gb]) {
+      D3 x = D.pos[gb], u = D.vel[gb];
+      D4 q = D.rot[gb];
+      D3 y = x + u * dt;
+      y.z = y.z + D.g * (dt * dt);
+      D.ypos[gb] = y;
+      D4 qt = qaddv(q, D.ang[gb] * dt);
+      D.yrot[gb] = qt;
+      double sgn = D.g < 0 ? -1.0 : (D.g > 0 ? 1.0 : 0.0);
+      double accelExt = (u.z - D.pvz[gb]) / dt * sgn;
+      double wgt = fmin(fmax(accelExt / fabs(D.g), 0.0), 1.0);
+      D3 xn = x + u * dt;
+      xn.z = xn.z + D.g * (wgt * dt * dt);
+      D.pos[gb] = xn;
+      D.rot[gb] = qt;
+    }
+    if (snapshots) {
+      D.snPos[snB + gb] = D.pos[gb];
+      D.snRot[snB + gb] = D.rot[gb];
+      D.stIpos[(size_t)slot * D.nb + gb] = D.ipos[gb];
+      D.stIrot[(size_t)slot * D.nb + gb] = D.irot[gb];
+      D.stYpos[(size_t)slot * D.nb + gb] = D.ypos[gb];
+      D.stYrot[(size_t)slot * D.nb + gb] = D.yrot[gb];
+    }
+  }
+  if (snapshots)
+    for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+      D.snLam[snP + wpt + lk] = D.lam[wpt + lk];
+      D.snPen[snP + wpt + lk] = D.pen[wpt + lk];
+      D.stC0[(size_t)slot * D.W * D.maxPts + wpt + lk] = D.C0[wpt + lk];
+    }
+  __syncthreads();
+  for (int it = 0; it < D.I; it++) {
+    for (int c = 0; c < v.ncol; c++) {
+      if (threadIdx.x < v.nb && v.color[threadIdx.x] == c) {
+        int lb = threadIdx.x, gb = v.b0 + lb;
+        Sys6 S;
+        D3 gl, ga;
+        buildSystem(D, v, wpt, gb, lb, S, gl, ga, D.pos, D.rot, D.lam, D.pen);
+        LDLT6 F;
+        factor6(S, F, PIVOT);
+        double rhs[6] = {gl.x, gl.y, gl.z, ga.x, ga.y, ga.z}, dx[6];
+        solve6(F, rhs, dx);
+        D.pos[gb] = D.pos[gb] - D3{dx[0], dx[1], dx[2]};
+        D.rot[gb] = qaddv(D.rot[gb], D3{-dx[3], -dx[4], -dx[5]});
+      }
+      __syncthreads();
+    }
+    // duals (manifold.ts:202-217)
+    for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+      int k = v.p0 + lk;
+      int2 ab = D.manAB[D.ptMan[k]];
+      int a = v.b0 + ab.x, b = v.b0 + ab.y;
+      PointEval e;
+      evalPoint(D, k, D.pos[a], D.rot[a], D.ipos[a], D.irot[a], D.pos[b], D.rot[b], D.ipos[b], D.irot[b], D.C0[wpt + lk], D.lam[wpt + lk], D.pen[wpt + lk],
+                sqrt(mu(D, a) * mu(D, b)), e);
+      D3 pen = D.pen[wpt + lk];
+      if (e.F.x < 0.0) pen.x = fmin(pen.x + D.beta * fabs(e.C.x), PEN_MAX);
+      if (e.fs <= e.bd) {
+        pen.y = fmin(pen.y + D.beta * fabs(e.C.y), PEN_MAX);
+        pen.z = fmin(pen.z + D.beta * fabs(e.C.z), PEN_MAX);
+      }
+      D.lam[wpt + lk] = e.F;
+      D.pen[wpt + lk] = pen;
+    }
+    __syncthreads();
+    if (snapshots) {
+      if (threadIdx.x < v.nb) {
+        int gb = v.b0 + threadIdx.x;
+        D.snPos[snB + (size_t)(it + 1) * D.nb + gb] = D.pos[gb];
+        D.snRot[snB + (size_t)(it + 1) * D.nb + gb] = D.rot[gb];
+      }
+      for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+        D.snLam[snP + (size_t)(it + 1) * D.W * D.maxPts + wpt + lk] = D.lam[wpt + lk];
+        D.snPen[snP + (size_t)(it + 1) * D.W * D.maxPts + wpt + lk] = D.pen[wpt + lk];
+      }
+      __syncthreads();
+    }
+  }
+  // velocities (solver.ts:328-334)
+  if (threadIdx.x < v.nb) {
+    int gb = v.b0 + threadIdx.x;
+    D.pvz[gb] = D.vel[gb].z;
+    if (D.dynamic[gb]) {
+      D.vel[gb] = (D.pos[gb] - D.ipos[gb]) * (1.0 / dt);
+      D.ang[gb] = qsub(D.rot[gb], D.irot[gb]) * (1.0 / dt);
+    }
+  }
+  // this step's points become the last step's
+  for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+    D.lamP[wpt + lk] = D.lam[wpt + lk];
+    D.penP[wpt + lk] = D.pen[wpt + lk];
+  }
+  __syncthreads();
+}
+
+__device__ void loadInitial(const AdjDev& D, int w) {
+  const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
+  if (threadIdx.x < nb) {
+    int gb = b0 + threadIdx.x;
+    const double* q = D.params + 8 * gb;
+    D.pos[gb] = D.pos0[gb];
+    D.rot[gb] = D.rot0[gb];
+    D.vel[gb] = D.dynamic[gb] ? D3{q[0], q[1], q[2]} : D3{0, 0, 0};
+    D.ang[gb] = D.dynamic[gb] ? D3{q[3], q[4], q[5]} : D3{0, 0, 0};
+    D.pvz[gb] = D.prevVz0[gb];
+  }
+  __syncthreads();
+}
+
+// State copies: `bodies and last step's points` to/from a checkpoint or segment slot
+__device__ void saveState(const AdjDev& D, int w, int np, D3* P, D4* R, D3* V, D3* A, double* Z, D3* L, D3* N, size_t slot) {
+  const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
+  if (threadIdx.x < nb) {
+    int gb = b0 + threadIdx.x;
+    size_t o = slot * D.nb + gb;
+    P[o] = D.pos[gb];
+    R[o] = D.rot[gb];
+    V[o] = D.vel[gb];
+    A[o] = D.ang[gb];
+    Z[o] = D.pvz[gb];
+  }
+  for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+    size_t o = slot * D.W * D.maxPts + w * D.maxPts + lk;
+    L[o] = D.lamP[w * D.maxPts + lk];
+    N[o] = D.penP[w * D.maxPts + lk];
+  }
+  __syncthreads();
+}
+__device__ void loadState(const AdjDev& D, int w, int np, const D3* P, const D4* R, const D3* V, const D3* A, const double* Z, const D3* L, const D3* N,
+                          size_t slot) {
+  const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
+  if (threadIdx.x < nb) {
+    int gb = b0 + threadIdx.x;
+    size_t o = slot * D.nb + gb;
+    D.pos[gb] = P[o];
+    D.rot[gb] = R[o];
+    D.vel[gb] = V[o];
+    D.ang[gb] = A[o];
+    D.pvz[gb] = Z[o];
+  }
+  for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+    size_t o = slot * D.W * D.maxPts + w * D.maxPts + lk;
+    D.lamP[w * D.maxPts + lk] = L[o];
+    D.penP[w * D.maxPts + lk] = N[o];
+  }
+  __syncthreads();
+}
+__device__ inline int pointsBefore(const AdjDev& D, int s, int w) {  // the last step's point count (step s's input)
+  if (s == 0) return 0;
+  return D.ptFirst[(s - 1) * (D.W + 1) + w + 1] - D.ptFirst[(s - 1) * (D.W + 1) + w];
+}
+
+__device__ void worldLoss(const AdjDev& D, int w) {
+  const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
+  __shared__ double s_loss[ADJ_THREADS];
+  double l = 0.0;
+  if (threadIdx.x < nb) {
+    int gb = b0 + threadIdx.x;
+    const double* t = D.target + 7 * gb;
+    D3 x = D.pos[gb];
+    D4 q = D.rot[gb];
+    if (D.dynamic[gb]) {
+      double d[7] = {x.x - t[0], x.y - t[1], x.z - t[2], q.x - t[3], q.y - t[4], q.z - t[5], q.w - t[6]};
+      for (int k = 0; k < 7; k++) l += d[k] * d[k];
+    }
+    if (D.finalPose) {
+      double* o = D.finalPose + 7 * gb;
+      o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = q.x; o[4] = q.y; o[5] = q.z; o[6] = q.w;
+    }
+  }
+  s_loss[threadIdx.x] = l;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < (int)blockDim.x; i++) s += s_loss[i];
+    D.loss[w] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_forward(AdjDev D) {
+  const int w = blockIdx.x;
+  loadInitial(D, w);
+  for (int s = 0; s < D.K; s++) {
+    if (s % D.ck == 0) saveState(D, w, pointsBefore(D, s, w), D.ckPos, D.ckRot, D.ckVel, D.ckAng, D.ckPvz, D.ckLam, D.ckPen, s / D.ck);
+    stepForward(D, s, w, -1);
+  }
+  worldLoss(D, w);
+}
+
+// --- reverse ------------------------------------------------------------------------------------------
+// Body gb's primal update at iteration it (poses read from the snapshots the sweep read): the
+// cotangent of its new pose is turned into cotangents of its old pose, of its partners' poses, of
+// its points' lambda and penalty, of the inertial targets, the step-start poses, its mass and the
+// friction coefficients.
+__device__ void primalVjp(const AdjDev& D, const StepView& v, int wpt, int it, int gb, int lb, int c) {
+  const double dt2 = D.dt * D.dt;
+  // the poses the update read: its own (iteration it - 1), partners of earlier colours (iteration it),
+  // of later colours (it - 1); the points' values after the dual of iteration it - 1
+  const size_t prevSn = (size_t)it * D.nb, curSn = (size_t)(it + 1) * D.nb;
+  const D3* lamIn = D.snLam + (size_t)it * D.W * D.maxPts;
+  const D3* penIn = D.snPen + (size_t)it * D.W * D.maxPts;
+  auto poseOf = [&](int b, D3& x, D4& q) {
+    if (!D.dynamic[b] || b == gb) {
+      x = D.snPos[prevSn + b];
+      q = D.snRot[prevSn + b];
+      return;
+    }
+    int cb = v.color[b - v.b0];
+    size_t o = cb < c ? curSn : prevSn;
+    x = D.snPos[o + b];
+    q = D.snRot[o + b];
+  };
+  // forward values
+  D3 x;
+  D4 q;
+  poseOf(gb, x, q);
+  const double m = mass(D, gb) / dt2;
+  const D3 Iu = D.unitMoment[gb];
+  const D3 I = Iu * (mass(D, gb) / dt2);
+  Sys6 S;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) S.A[i][j] = 0.0;
+  S.A[0][0] = S.A[1][1] = S.A[2][2] = m;
+  S.A[3][3] = I.x;
+  S.A[4][4] = I.y;
+  S.A[5][5] = I.z;
+  D3 gl = (x - D.ypos[gb]) * m;
+  D3 qd = qsub(q, D.yrot[gb]);
+  D3 ga = D3{I.x * qd.x, I.y * qd.y, I.z * qd.z};
+  const int t0 = s_incStart[lb], t1 = s_incStart[lb + 1];
+  for (int t = t0; t < t1; t++) {
+    int k = s_inc[t], lk = k - v.p0;
+    int2 ab = D.manAB[D.ptMan[k]];
+    int a = v.b0 + ab.x, b = v.b0 + ab.y;
+    D3 xa, xb;
+    D4 qa, qb;
+    poseOf(a, xa, qa);
+    poseOf(b, xb, qb);
+    PointEval e;
+    evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamIn[wpt + lk], penIn[wpt + lk],
+              sqrt(mu(D, a) * mu(D, b)), e);
+    bool isA = gb == a;
+    double sg = isA ? 1.0 : -1.0;
+    D3 r = isA ? e.rAW : e.rBW;
+    const D3* B = D.basis + 3 * D.ptMan[k];
+    for (int cc = 0; cc < 3; cc++) {
+      D3 l = B[cc] * sg;
+      D3 aa = cross(r, l);
+      double kk = comp(penIn[wpt + lk], cc);
+      double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
+      for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) S.A[i][j] += kk * J[i] * J[j];
+      gl += l * comp(e.F, cc);
+      ga += aa * comp(e.F, cc);
+    }
+  }
+  LDLT6 F;
+  factor6(S, F, PIVOT);
+  double rhs[6] = {gl.x, gl.y, gl.z, ga.x, ga.y, ga.z}, delta[6];
+  solve6(F, rhs, delta);
+  D3 dA{delta[3], delta[4], delta[5]};
+  // the new pose's cotangent: x' = x - delta_lin, q' = qaddv(q, -delta_ang)
+  D3 gXn = D.gPos[gb];
+  D4 gQn = D.gRot[gb];
+  D3 gX = gXn;
+  D4 gQ{0, 0, 0, 0};
+  D3 gV{0, 0, 0};
+  qaddvVjp(q, -dA, gQn, gQ, gV);
+  double gDelta[6] = {-gXn.x, -gXn.y, -gXn.z, -gV.x, -gV.y, -gV.z};
+  // the cotangent of g is w (H^-1 gDelta), that of H's lower triangle Hb (-w delta^T symmetrised,
+  // but through a floored pivot only to its diagonal entry)
+  double wv[6], Hb[6][6];
+  ldltVjp(S, F, PIVOT, rhs, delta, gDelta, wv, Hb);
+  D3 wl{wv[0], wv[1], wv[2]}, wa{wv[3], wv[4], wv[5]};
+  // inertia
+  gX += wl * m;
+  D3 gY = wl * (-m);
+  D3 gqd{I.x * wa.x, I.y * wa.y, I.z * wa.z};
+  D4 gYq{0, 0, 0, 0};
+  qsubVjp(q, D.yrot[gb], gqd, gQ, gYq);
+  double gM = 0.0;
+  {
+    // H_lin = m/dt2 I, H_ang = diag(m Iu/dt2); g_lin = (x - y) m/dt2, g_ang = (m Iu/dt2) qd
+    D3 xy = x - D.ypos[gb];
+    double dH = Hb[0][0] + Hb[1][1] + Hb[2][2];
+    double dHa = Hb[3][3] * Iu.x + Hb[4][4] * Iu.y + Hb[5][5] * Iu.z;
+    gM += (dH + dot(wl, xy) + dHa + wa.x * Iu.x * qd.x + wa.y * Iu.y * qd.y + wa.z * Iu.z * qd.z) / dt2;
+  }
+  D3 gIpos{0, 0, 0};
+  D4 gIrot{0, 0, 0, 0};
+  for (int t = t0; t < t1; t++) {
+    int k = s_inc[t], lk = k - v.p0;
+    int2 ab = D.manAB[D.ptMan[k]];
+    int a = v.b0 + ab.x, b = v.b0 + ab.y;
+    D3 xa, xb;
+    D4 qa, qb;
+    poseOf(a, xa, qa);
+    poseOf(b, xb, qb);
+    double fr = sqrt(mu(D, a) * mu(D, b));
+    PointEval e;
+    D3 lamv = lamIn[wpt + lk], penv = penIn[wpt + lk];
+    evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamv, penv, fr, e);
+    bool isA = gb == a;
+    double sg = isA ? 1.0 : -1.0;
+    D3 r = isA ? e.rAW : e.rBW;
+    const D3* B = D.basis + 3 * D.ptMan[k];
+    D3 gF{0, 0, 0}, gPen{0, 0, 0}, gr{0, 0, 0};
+    for (int cc = 0; cc < 3; cc++) {
+      D3 l = B[cc] * sg;
+      D3 aa = cross(r, l);
+      double kk = comp(penv, cc);
+      const double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
+      double wJ = dot(wl, l) + dot(wa, aa);
+      // H += k J J^T: k's cotangent sums Hb J_i J_j over the lower triangle; J's is k (Hb + Hb^T) J
+      double kb = 0.0, MJ[3] = {0.0, 0.0, 0.0};
+      for (int i = 0; i < 6; i++)
+        for (int j = 0; j <= i; j++) {
+          kb += Hb[i][j] * J[i] * J[j];
+          if (i >= 3) MJ[i - 3] += Hb[i][j] * J[j];
+          if (j >= 3) MJ[j - 3] += Hb[i][j] * J[i];
+        }
+      setComp(gF, cc, wJ);
+      setComp(gPen, cc, kb);
+      // cotangent of a (the angular Jacobian row): F_c w_a from g, k (Hb + Hb^T) J from H
+      D3 gAa = wa * comp(e.F, cc) + D3{MJ[0], MJ[1], MJ[2]} * kk;
+      gr += cross(l, gAa);
+    }
+    D3 gC{0, 0, 0}, gLam{0, 0, 0};
+    double gFr = 0.0;
+    evalFVjp(e, lamv, penv, gF, gC, gLam, gPen, gFr);
+    D3 gXa{0, 0, 0}, gXb{0, 0, 0}, gXa0{0, 0, 0}, gXb0{0, 0, 0}, gC0{0, 0, 0};
+    D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
+    evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
+    // the lever arm r = R(q_own) r_local
+    if (isA) gQa += rotateVjpQ(qa, D.rA[k], gr);
+    else gQb += rotateVjpQ(qb, D.rB[k], gr);
+    // own terms stay local; the partner's go to its current cotangent
+    if (isA) {
+      gX += gXa;
+      gQ += gQa;
+      gIpos += gXa0;
+      gIrot += gQa0;
+      if (D.dynamic[b]) {
+        atomicAdd3(&D.gPos[b], gXb);
+        atomicAdd4(&D.gRot[b], gQb);
+        atomicAdd3(&D.gIpos[b], gXb0);
+        atomicAdd4(&D.gIrot[b], gQb0);
+      }
+    } else {
+      gX += gXb;
+      gQ += gQb;
+      gIpos += gXb0;
+      gIrot += gQb0;
+      if (D.dynamic[a]) {
+        atomicAdd3(&D.gPos[a], gXa);
+        atomicAdd4(&D.gRot[a], gQa);
+        atomicAdd3(&D.gIpos[a], gXa0);
+        atomicAdd4(&D.gIrot[a], gQa0);
+      }
+    }
+    atomicAdd3(&D.gLam[wpt + lk], gLam);
+    atomicAdd3(&D.gPen[wpt + lk], gPen);
+    atomicAdd3(&D.gC0[wpt + lk], gC0);
+    if (gFr != 0.0 && fr > 0.0) {
+      double ma = mu(D, a), mb = mu(D, b);
+      if (D.dynamic[a]) atomicAdd(&D.gMu[a], gFr * mb / (2.0 * fr));
+      if (D.dynamic[b]) atomicAdd(&D.gMu[b], gFr * ma / (2.0 * fr));
+    }
+  }
+  D.gPos[gb] = gX;
+  D.gRot[gb] = gQ;
+  D.gYpos[gb] += gY;
+  D.gYrot[gb] += gYq;
+  D.gIpos[gb] += gIpos;
+  D.gIrot[gb] += gIrot;
+  D.gMass[gb] += gM;
+}
+
+// Point k's dual at iteration it: lambda' = F, the penalty ramps
+__device__ void dualVjp(const AdjDev& D, const StepView& v, int wpt, int it, int k) {
+  const int lk = k - v.p0;
+  const size_t sn = (size_t)(it + 1) * D.nb;
+  const D3* lamIn = D.snLam + (size_t)it * D.W * D.maxPts;
+  const D3* penIn = D.snPen + (size_t)it * D.W * D.maxPts;
+  int2 ab = D.manAB[D.ptMan[k]];
+  int a = v.b0 + ab.x, b = v.b0 + ab.y;
+  D3 xa = D.snPos[sn + a], xb = D.snPos[sn + b];
+  D4 qa = D.snRot[sn + a], qb = D.snRot[sn + b];
+  double fr = sqrt(mu(D, a) * mu(D, b));
+  D3 lamv = lamIn[wpt + lk], penv = penIn[wpt + lk];
+  PointEval e;
+  evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamv, penv, fr, e);
+  D3 gLamOut = D.gLam[wpt + lk], gPenOut = D.gPen[wpt + lk];
+  D3 gPen{0, 0, 0}, gC{0, 0, 0}, gLam{0, 0, 0};
+  // pen' = min(pen + beta |C|, MAX) where the ramp applies, else pen
+  auto ramp = [&](int c, bool on) {
+    double go = comp(gPenOut, c);
+    if (!on) {
+      setComp(gPen, c, comp(gPen, c) + go);
+      return;
+    }
+    double raw = comp(penv, c) + D.beta * fabs(comp(e.C, c));
+    if (raw < PEN_MAX) {
+      setComp(gPen, c, comp(gPen, c) + go);
+      setComp(gC, c, comp(gC, c) + go * D.beta * (comp(e.C, c) < 0.0 ? -1.0 : 1.0));
+    }
+  };
+  ramp(0, e.F.x < 0.0);
+  ramp(1, e.fs <= e.bd);
+  ramp(2, e.fs <= e.bd);
+  double gFr = 0.0;
+  evalFVjp(e, lamv, penv, gLamOut, gC, gLam, gPen, gFr);
+  D3 gXa{0, 0, 0}, gXb{0, 0, 0}, gXa0{0, 0, 0}, gXb0{0, 0, 0}, gC0{0, 0, 0};
+  D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
+  evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
+  if (D.dynamic[a]) {
+    atomicAdd3(&D.gPos[a], gXa);
+    atomicAdd4(&D.gRot[a], gQa);
+    atomicAdd3(&D.gIpos[a], gXa0);
+    atomicAdd4(&D.gIrot[a], gQa0);
+  }
+  if (D.dynamic[b]) {
+    atomicAdd3(&D.gPos[b], gXb);
+    atomicAdd4(&D.gRot[b], gQb);
+    atomicAdd3(&D.gIpos[b], gXb0);
+    atomicAdd4(&D.gIrot[b], gQb0);
+  }
+  D.gLam[wpt + lk] = gLam;  // the value before this dual
+  D.gPen[wpt + lk] = gPen;
+  D.gC0[wpt + lk] += gC0;
+  if (gFr != 0.0 && fr > 0.0) {
+    double ma = mu(D, a), mb = mu(D, b);
+    if (D.dynamic[a]) atomicAdd(&D.gMu[a], gFr * mb / (2.0 * fr));
+    if (D.dynamic[b]) atomicAdd(&D.gMu[b], gFr * ma / (2.0 * fr));
+  }
+}
+
+// Step s backwards. On entry its start state is in segment slot `slot` and loaded (pos.., lamP/
+// penP), and the cotangents of its outputs (the bodies' state, its points' lambda and penalty) are
+// in gPos.. and gLam/gPen; on exit gPos.. hold those of its inputs and gLamP/gPenP those of the last
+// step's points.
+__device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
+  // this step's stored intermediates in place of the working arrays
+  AdjDev D = D0;
+  D.ipos = D0.stIpos + slot * D0.nb;
+  D.irot = D0.stIrot + slot * D0.nb;
+  D.ypos = D0.stYpos + slot * D0.nb;
+  D.yrot = D0.stYrot + slot * D0.nb;
+  D.C0 = D0.stC0 + slot * D0.W * D0.maxPts;
+  D.snPos = D0.snPos + slot * (D0.I + 1) * D0.nb;
+  D.snRot = D0.snRot + slot * (D0.I + 1) * D0.nb;
+  D.snLam = D0.snLam + slot * (D0.I + 1) * D0.W * D0.maxPts;
+  D.snPen = D0.snPen + slot * (D0.I + 1) * D0.W * D0.maxPts;
+  const StepView v = viewOf(D, s, w);
+  const int wpt = w * D.maxPts;
+  const int np = v.p1 - v.p0;
+  const double dt = D.dt;
+  buildIncidence(D, v);
+  // velocities: v' = (x - x0)/dt, w' = qsub(q, q0)/dt, prevVz' = v_old.z
+  if (threadIdx.x < v.nb) {
+    int gb = v.b0 + threadIdx.x;
+    D3 gv = D.gVel[gb], gw = D.gAng[gb];
+    double gz = D.gPvz[gb];
+    D.gIpos[gb] = D3{0, 0, 0};
+    D.gIrot[gb] = D4{0, 0, 0, 0};
+    D.gYpos[gb] = D3{0, 0, 0};
+    D.gYrot[gb] = D4{0, 0, 0, 0};
+    if (D.dynamic[gb]) {
+      D4 q = D.snRot[(size_t)D.I * D.nb + gb];
+      D.gPos[gb] += gv * (1.0 / dt);
+      D.gIpos[gb] -= gv * (1.0 / dt);
+      D4 gq{0, 0, 0, 0}, gq0{0, 0, 0, 0};
+      qsubVjp(q, D.irot[gb], gw * (1.0 / dt), gq, gq0);
+      D.gRot[gb] += gq;
+      D.gIrot[gb] += gq0;
+    } else {
+      D.gPos[gb] = D3{0, 0, 0};
+      D.gRot[gb] = D4{0, 0, 0, 0};
+    }
+    D.gVel[gb] = D3{0, 0, gz};  // the input velocity feeds prevVz'
+    D.gAng[gb] = D3{0, 0, 0};
+    D.gPvz[gb] = 0.0;
+  }
+  for (int lk = threadIdx.x; lk < np; lk += blockDim.x) D.gC0[wpt + lk] = D3{0, 0, 0};
+  __syncthreads();
+  for (int it = D.I - 1; it >= 0; it--) {
+    for (int lk = threadIdx.x; lk < np; lk += blockDim.x) dualVjp(D, v, wpt, it, v.p0 + lk);
+    __syncthreads();
+    for (int c = v.ncol - 1; c >= 0; c--) {
+      if (threadIdx.x < v.nb && v.color[threadIdx.x] == c) primalVjp(D, v, wpt, it, v.b0 + threadIdx.x, threadIdx.x, c);
+      __syncthreads();
+    }
+  }
+  // points' warm starts and C(x-) (the start poses' cotangents gather in gIpos/gIrot)
+  const int prevFirst = s > 0 ? D.ptFirst[(s - 1) * (D.W + 1) + w] : 0;
+  for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
+    int k = v.p0 + lk;
+    int pv = D.ptPrev[k];
+    if (pv >= 0) {
+      int plk = pv - prevFirst;
+      D3 gl = D.gLam[wpt + lk], gp = D.gPen[wpt + lk];
+      D3 pe = D.sgPen[slot * D.W * D.maxPts + wpt + plk];
+      D3 gpp{0, 0, 0};
+      for (int c = 0; c < 3; c++) {
+        double x = comp(pe, c) * D.gamma;
+        if (x > PEN_MIN && x < PEN_MAX) setComp(gpp, c, comp(gp, c) * D.gamma);
+      }
+      atomicAdd3(&D.gLamP[wpt + plk], gl * (D.alpha * D.gamma));  // two points may warm-start from one
+      atomicAdd3(&D.gPenP[wpt + plk], gpp);
+    }
+    int2 ab = D.manAB[D.ptMan[k]];
+    int a = v.b0 + ab.x, b = v.b0 + ab.y;
+    const D3* B = D.basis + 3 * D.ptMan[k];
+    D3 gc0 = D.gC0[wpt + lk];
+    D3 gd = B[0] * gc0.x + B[1] * gc0.y + B[2] * gc0.z;
+    if (D.dynamic[a]) {
+      atomicAdd3(&D.gIpos[a], gd);
+      atomicAdd4(&D.gIrot[a], rotateVjpQ(D.irot[a], D.rA[k], gd));
+    }
+    if (D.dynamic[b]) {
+      atomicAdd3(&D.gIpos[b], -gd);
+      atomicAdd4(&D.gIrot[b], rotateVjpQ(D.irot[b], D.rB[k], -gd));
+    }
+  }
+  __syncthreads();
+  // bodies: the warm-start guess and the inertial targets (solver.ts:273-295)
+  if (threadIdx.x < v.nb) {
+    int gb = v.b0 + threadIdx.x;
+    if (D.dynamic[gb]) {
+      const size_t o = slot * D.nb + gb;
+      const D3 u = D.sgVel[o], om = D.sgAng[o];
+      const double pvz = D.sgPvz[o];
+      const D4 q0 = D.irot[gb];
+      D3 gxg = D.gPos[gb];  // the guess: the pose iteration 0 starts from
+      D4 gqg = D.gRot[gb];
+      D3 gY = D.gYpos[gb];
+      D4 gYq = D.gYrot[gb];
+      D3 gX0 = gxg + gY + D.gIpos[gb];
+      D4 gQ0 = D.gIrot[gb];
+      D3 gU = (gxg + gY) * dt;
+      double sgn = D.g < 0 ? -1.0 : (D.g > 0 ? 1.0 : 0.0);
+      double accelExt = (u.z - pvz) / dt * sgn;
+      double wgt = accelExt / fabs(D.g);
+      double gPvz = 0.0;
+      if (wgt > 0.0 && wgt < 1.0) {
+        double gW = gxg.z * D.g * dt * dt;
+        double gA = gW / fabs(D.g);
+        gU.z += gA * sgn / dt;
+        gPvz = -gA * sgn / dt;
+      }
+      D3 gOm{0, 0, 0};
+      qaddvVjp(q0, om * dt, D4{gqg.x + gYq.x, gqg.y + gYq.y, gqg.z + gYq.z, gqg.w + gYq.w}, gQ0, gOm);
+      D.gPos[gb] = gX0;
+      D.gRot[gb] = gQ0;
+      D.gVel[gb] += gU;
+      D.gAng[gb] = gOm * dt;
+      D.gPvz[gb] = gPvz;
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_backward(const AdjDev D) {
+  const int w = blockIdx.x;
+  const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
+  const int wpt = w * D.maxPts;
+  if (threadIdx.x < nb) {
+    int gb = b0 + threadIdx.x;
+    D.gVel[gb] = D.gAng[gb] = D3{0, 0, 0};
+    D.gPvz[gb] = 0.0;
+    D.gMass[gb] = D.gMu[gb] = 0.0;
+  }
+  for (int lk = threadIdx.x; lk < D.maxPts; lk += blockDim.x) {
+    D.gLam[wpt + lk] = D.gPen[wpt + lk] = D.gLamP[wpt + lk] = D.gPenP[wpt + lk] = D3{0, 0, 0};
+  }
+  __syncthreads();
+  const int segments = (D.K + D.ck - 1) / D.ck;
+  for (int sg = segments - 1; sg >= 0; sg--) {
+    const int s0 = sg * D.ck, s1 = min(D.K, s0 + D.ck);
+    loadState(D, w, pointsBefore(D, s0, w), D.ckPos, D.ckRot, D.ckVel, D.ckAng, D.ckPvz, D.ckLam, D.ckPen, sg);
+    for (int s = s0; s < s1; s++) {
+      saveState(D, w, pointsBefore(D, s, w), D.sgPos, D.sgRot, D.sgVel, D.sgAng, D.sgPvz, D.sgLam, D.sgPen, s - s0);
+      stepForward(D, s, w, s - s0);
+    }
+    if (sg == segments - 1) {
+      worldLoss(D, w);
+      if (threadIdx.x < nb) {  // the loss's cotangent: 2 (pose - target)
+        int gb = b0 + threadIdx.x;
+        const double* t = D.target + 7 * gb;
+        D3 x = D.pos[gb];
+        D4 q = D.rot[gb];
+        bool dyn = D.dynamic[gb];
+        D.gPos[gb] = dyn ? D3{2 * (x.x - t[0]), 2 * (x.y - t[1]), 2 * (x.z - t[2])} : D3{0, 0, 0};
+        D.gRot[gb] = dyn ? D4{2 * (q.x - t[3]), 2 * (q.y - t[4]), 2 * (q.z - t[5]), 2 * (q.w - t[6])} : D4{0, 0, 0, 0};
+      }
+      __syncthreads();
+    }
+    for (int s = s1 - 1; s >= s0; s--) {
+      stepBackward(D, s, w, s - s0);
+      // the last step's points' cotangents become the outputs' of step s - 1. They are copied, not
+      // swapped: the buffers stay fixed in the struct the step functions take by reference.
+      const int npv = pointsBefore(D, s, w);
+      for (int lk = threadIdx.x; lk < D.maxPts; lk += blockDim.x) {
+        const bool live = lk < npv;
+        D.gLam[wpt + lk] = live ? D.gLamP[wpt + lk] : D3{0, 0, 0};
+        D.gPen[wpt + lk] = live ? D.gPenP[wpt + lk] : D3{0, 0, 0};
+        D.gLamP[wpt + lk] = D.gPenP[wpt + lk] = D3{0, 0, 0};
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace
+
+struct avbd_adjoint {
+  int device = 0;
+  std::string error;
+  AdjDev d{};
+  std::vector<void*> allocations;
+  int W = 0, nb = 0;
+  bool forwardDone = false;  // the checkpoints hold the forward of lastParams
+  std::vector<double> lastParams;
+};
+
+namespace {
+
+int afail(avbd_adjoint* a, int code, const std::string& m) {
+  if (a) a->error = m;
+  return code;
+}
+template <class T>
+bool aalloc(avbd_adjoint* a, T** p, size_t n) {
+  void* ptr = nullptr;
+  if (cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return false;
+  cudaMemset(ptr, 0, std::max<size_t>(n, 1) * sizeof(T));
+  a->allocations.push_back(ptr);
+  *p = static_cast<T*>(ptr);
+  return true;
+}
+template <class T>
+bool aupload(avbd_adjoint* a, const T** dst, const T* src, size_t n) {
+  T* p = nullptr;
+  if (!aalloc(a, &p, n)) return false;
+  if (n && cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return false;
+  *dst = p;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int avbd_adjoint_create(const avbd_adjoint_desc* desc, avbd_adjoint** out) {
+  if (!desc || !out) return AVBD_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return AVBD_ERR_NO_DEVICE;
+  if (desc->device < 0 || desc->device >= count) return AVBD_ERR_INVALID;
+  const uint32_t W = desc->worlds, K = desc->steps;
+  if (W == 0 || K == 0 || !desc->world_first_body || !desc->bodies || !desc->step_first_manifold || !desc->step_first_point || !desc->colors ||
+      !desc->color_counts)
+    return AVBD_ERR_INVALID;
+  const uint32_t nb = desc->world_first_body[W];
+  for (uint32_t w = 0; w < W; w++)
+    if (desc->world_first_body[w + 1] < desc->world_first_body[w] || desc->world_first_body[w + 1] - desc->world_first_body[w] > ADJ_THREADS)
+      return AVBD_ERR_CAPACITY;  // a world holds at most 128 bodies
+  const uint32_t nm = desc->step_first_manifold[K * (W + 1) - 1], npts = desc->step_first_point[K * (W + 1) - 1];
+  int maxPts = 1;
+  for (uint32_t s = 0; s < K; s++)
+    for (uint32_t w = 0; w < W; w++) {
+      int c = int(desc->step_first_point[s * (W + 1) + w + 1]) - int(desc->step_first_point[s * (W + 1) + w]);
+      if (c < 0) return AVBD_ERR_INVALID;
+      maxPts = std::max(maxPts, c);
+    }
+  if (maxPts > ADJ_MAX_POINTS) return AVBD_ERR_CAPACITY;
+  // every index inside its own world and step: manifolds' bodies, points' manifolds and sources
+  for (uint32_t s = 0; s < K; s++)
+    for (uint32_t w = 0; w < W; w++) {
+      const uint32_t m0 = desc->step_first_manifold[s * (W + 1) + w], m1 = desc->step_first_manifold[s * (W + 1) + w + 1];
+      const uint32_t p0 = desc->step_first_point[s * (W + 1) + w], p1 = desc->step_first_point[s * (W + 1) + w + 1];
+      const int nbw = int(desc->world_first_body[w + 1] - desc->world_first_body[w]);
+      if (m1 < m0 || m1 > nm || p1 > npts) return AVBD_ERR_INVALID;
+      for (uint32_t m = m0; m < m1; m++) {
+        int a = desc->manifold_bodies[2 * m], b = desc->manifold_bodies[2 * m + 1];
+        if (a < 0 || b < 0 || a >= nbw || b >= nbw || a == b) return AVBD_ERR_INVALID;
+      }
+      for (uint32_t k = p0; k < p1; k++) {
+        int m = desc->point_manifold[k], pv = desc->point_prev[k];
+        if (m < int(m0) || m >= int(m1)) return AVBD_ERR_INVALID;
+        if (pv >= 0) {
+          if (s == 0) return AVBD_ERR_INVALID;
+          const int q0 = int(desc->step_first_point[(s - 1) * (W + 1) + w]), q1 = int(desc->step_first_point[(s - 1) * (W + 1) + w + 1]);
+          if (pv < q0 || pv >= q1) return AVBD_ERR_INVALID;
+        }
+      }
+      if (desc->color_counts[s * W + w] < 0 || desc->color_counts[s * W + w] > 64) return AVBD_ERR_INVALID;
+    }
+  cudaSetDevice(desc->device);
+  auto* a = new avbd_adjoint();
+  a->device = desc->device;
+  a->W = int(W);
+  a->nb = int(nb);
+  AdjDev& D = a->d;
+  D.W = int(W);
+  D.K = int(K);
+  D.I = int(desc->iterations);
+  D.ck = desc->checkpoint ? int(desc->checkpoint) : 10;
+  D.dt = desc->dt;
+  D.g = desc->gravity;
+  D.alpha = desc->alpha;
+  D.gamma = desc->gamma;
+  D.beta = desc->beta_lin;
+  D.margin = desc->contact_margin;
+  D.nb = int(nb);
+  D.maxPts = maxPts;
+  // host-side unpacking of the body records (13 doubles each)
+  std::vector<D3> pos0(nb), um(nb);
+  std::vector<D4> rot0(nb);
+  std::vector<double> pvz(nb), fs(nb);
+  std::vector<int> dyn(nb), fb(desc->world_first_body, desc->world_first_body + W + 1);
+  for (uint32_t b = 0; b < nb; b++) {
+    const double* r = desc->bodies + 13 * b;
+    pos0[b] = D3{r[0], r[1], r[2]};
+    rot0[b] = D4{r[3], r[4], r[5], r[6]};
+    pvz[b] = r[7];
+    um[b] = D3{r[8], r[9], r[10]};
+    dyn[b] = r[11] != 0.0;
+    fs[b] = r[12];
+  }
+  std::vector<int> mf(desc->step_first_manifold, desc->step_first_manifold + K * (W + 1));
+  std::vector<int> pf(desc->step_first_point, desc->step_first_point + K * (W + 1));
+  std::vector<int2> ab(nm);
+  std::vector<D3> basis(3 * size_t(nm)), ra(npts), rb(npts);
+  for (uint32_t m = 0; m < nm; m++) {
+    ab[m] = make_int2(desc->manifold_bodies[2 * m], desc->manifold_bodies[2 * m + 1]);
+    for (int c = 0; c < 3; c++) basis[3 * m + c] = D3{desc->manifold_basis[9 * m + 3 * c], desc->manifold_basis[9 * m + 3 * c + 1], desc->manifold_basis[9 * m + 3 * c + 2]};
+  }
+  for (uint32_t k = 0; k < npts; k++) {
+    const double* r = desc->point_anchors + 6 * k;
+    ra[k] = D3{r[0], r[1], r[2]};
+    rb[k] = D3{r[3], r[4], r[5]};
+  }
+  bool ok = aupload(a, &D.bodyFirst, fb.data(), fb.size()) && aupload(a, &D.pos0, pos0.data(), nb) && aupload(a, &D.rot0, rot0.data(), nb) &&
+            aupload(a, &D.prevVz0, pvz.data(), nb) && aupload(a, &D.unitMoment, um.data(), nb) && aupload(a, &D.dynamic, dyn.data(), nb) &&
+            aupload(a, &D.fricStatic, fs.data(), nb) && aupload(a, &D.manFirst, mf.data(), mf.size()) && aupload(a, &D.ptFirst, pf.data(), pf.size()) &&
+            aupload(a, &D.manAB, ab.data(), nm) && aupload(a, &D.basis, basis.data(), basis.size()) && aupload(a, &D.rA, ra.data(), npts) &&
+            aupload(a, &D.rB, rb.data(), npts) && aupload(a, &D.ptMan, desc->point_manifold, npts) && aupload(a, &D.ptPrev, desc->point_prev, npts) &&
+            aupload(a, &D.color, desc->colors, size_t(K) * nb) && aupload(a, &D.ncol, desc->color_counts, size_t(K) * W);
+  const size_t WP = size_t(W) * maxPts, segs = (K + D.ck - 1) / D.ck, I1 = size_t(D.I) + 1;
+  double* prm = nullptr;
+  double* tgt = nullptr;
+  ok = ok && aalloc(a, &prm, 8 * size_t(nb)) && aalloc(a, &tgt, 7 * size_t(nb));
+  D.params = prm;
+  D.target = tgt;
+  for (D3** p : {&D.pos, &D.vel, &D.ang, &D.ipos, &D.ypos, &D.gPos, &D.gVel, &D.gAng, &D.gIpos, &D.gYpos}) ok = ok && aalloc(a, p, nb);
+  for (D4** p : {&D.rot, &D.irot, &D.yrot, &D.gRot, &D.gIrot, &D.gYrot}) ok = ok && aalloc(a, p, nb);
+  for (double** p : {&D.pvz, &D.gPvz, &D.gMass, &D.gMu}) ok = ok && aalloc(a, p, nb);
+  for (D3** p : {&D.lam, &D.pen, &D.lamP, &D.penP, &D.C0, &D.gLam, &D.gPen, &D.gLamP, &D.gPenP, &D.gC0}) ok = ok && aalloc(a, p, WP);
+  ok = ok && aalloc(a, &D.ckPos, segs * nb) && aalloc(a, &D.ckVel, segs * nb) && aalloc(a, &D.ckAng, segs * nb) && aalloc(a, &D.ckRot, segs * nb) &&
+       aalloc(a, &D.ckPvz, segs * nb) && aalloc(a, &D.ckLam, segs * WP) && aalloc(a, &D.ckPen, segs * WP);
+  ok = ok && aalloc(a, &D.sgPos, size_t(D.ck) * nb) && aalloc(a, &D.sgVel, size_t(D.ck) * nb) && aalloc(a, &D.sgAng, size_t(D.ck) * nb) &&
+       aalloc(a, &D.sgRot, size_t(D.ck) * nb) && aalloc(a, &D.sgPvz, size_t(D.ck) * nb) && aalloc(a, &D.sgLam, size_t(D.ck) * WP) &&
+       aalloc(a, &D.sgPen, size_t(D.ck) * WP);
+  const size_t CK = size_t(D.ck);
+  ok = ok && aalloc(a, &D.snPos, CK * I1 * nb) && aalloc(a, &D.snRot, CK * I1 * nb) && aalloc(a, &D.snLam, CK * I1 * WP) && aalloc(a, &D.snPen, CK * I1 * WP);
+  ok = ok && aalloc(a, &D.stIpos, CK * nb) && aalloc(a, &D.stIrot, CK * nb) && aalloc(a, &D.stYpos, CK * nb) && aalloc(a, &D.stYrot, CK * nb) &&
+       aalloc(a, &D.stC0, CK * WP);
+  double* loss = nullptr;
+  double* fin = nullptr;
+  ok = ok && aalloc(a, &loss, W) && aalloc(a, &fin, 7 * size_t(nb));
+  D.loss = loss;
+  D.finalPose = fin;
+  if (!ok) {
+    avbd_adjoint_destroy(a);
+    return AVBD_ERR_CUDA;
+  }
+  *out = a;
+  return AVBD_OK;
+}
+
+int avbd_adjoint_destroy(avbd_adjoint* a) {
+  if (!a) return AVBD_OK;
+  cudaSetDevice(a->device);
+  cudaDeviceSynchronize();
+  for (void* p : a->allocations) cudaFree(p);
+  delete a;
+  return AVBD_OK;
+}
+
+const char* avbd_adjoint_last_error(const avbd_adjoint* a) { return a ? a->error.c_str() : "no adjoint"; }
+
+int avbd_adjoint_set_target(avbd_adjoint* a, const double* target) {
+  if (!a || !target) return AVBD_ERR_INVALID;
+  cudaSetDevice(a->device);
+  if (cudaMemcpy(const_cast<double*>(a->d.target), target, 7 * size_t(a->nb) * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return afail(a, AVBD_ERR_CUDA, "target upload");
+  return AVBD_OK;
+}
+
+static int adjParams(avbd_adjoint* a, const double* params) {
+  if (!params) return afail(a, AVBD_ERR_INVALID, "params");
+  for (int b = 0; b < a->nb; b++)
+    for (int k = 0; k < 8; k++)
+      if (!std::isfinite(params[8 * b + k])) return afail(a, AVBD_ERR_INVALID, "params not finite");
+  if (cudaMemcpy(const_cast<double*>(a->d.params), params, 8 * size_t(a->nb) * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return afail(a, AVBD_ERR_CUDA, "params upload");
+  return AVBD_OK;
+}
+
+int avbd_adjoint_forward(avbd_adjoint* a, const double* params, double* loss, double* final_pose) {
+  if (!a) return AVBD_ERR_INVALID;
+  cudaSetDevice(a->device);
+  int r = adjParams(a, params);
+  if (r) return r;
+  k_adj_forward<<<a->W, ADJ_THREADS>>>(a->d);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("replay launch: ") + cudaGetErrorString(e));
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, cudaGetErrorString(e));
+  if (loss) cudaMemcpy(loss, a->d.loss, sizeof(double) * a->W, cudaMemcpyDeviceToHost);
+  if (final_pose) cudaMemcpy(final_pose, a->d.finalPose, sizeof(double) * 7 * a->nb, cudaMemcpyDeviceToHost);
+  a->forwardDone = true;
+  a->lastParams.assign(params, params + 8 * size_t(a->nb));
+  return AVBD_OK;
+}
+
+int avbd_adjoint_backward(avbd_adjoint* a, const double* params, double* grad, double* loss) {
+  if (!a || !grad) return AVBD_ERR_INVALID;
+  cudaSetDevice(a->device);
+  if (a->forwardDone && (!params || std::memcmp(params, a->lastParams.data(), a->lastParams.size() * sizeof(double)) != 0)) a->forwardDone = false;
+  int r = adjParams(a, params);
+  if (r) return r;
+  if (!a->forwardDone) {  // the checkpoints come from a forward with these params
+    k_adj_forward<<<a->W, ADJ_THREADS>>>(a->d);
+    cudaError_t e0 = cudaGetLastError();
+    if (e0 != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("replay launch: ") + cudaGetErrorString(e0));
+  }
+  a->forwardDone = false;
+  k_adj_backward<<<a->W, ADJ_THREADS>>>(a->d);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("reverse launch: ") + cudaGetErrorString(e));
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, cudaGetErrorString(e));
+  std::vector<D3> gv(a->nb), ga(a->nb);
+  std::vector<double> gm(a->nb), gu(a->nb);
+  cudaMemcpy(gv.data(), a->d.gVel, sizeof(D3) * a->nb, cudaMemcpyDeviceToHost);
+  cudaMemcpy(ga.data(), a->d.gAng, sizeof(D3) * a->nb, cudaMemcpyDeviceToHost);
+  cudaMemcpy(gm.data(), a->d.gMass, sizeof(double) * a->nb, cudaMemcpyDeviceToHost);
+  cudaMemcpy(gu.data(), a->d.gMu, sizeof(double) * a->nb, cudaMemcpyDeviceToHost);
+  for (int b = 0; b < a->nb; b++) {
+    double* o = grad + 8 * b;
+    o[0] = gv[b].x; o[1] = gv[b].y; o[2] = gv[b].z;
+    o[3] = ga[b].x; o[4] = ga[b].y; o[5] = ga[b].z;
+    o[6] = gm[b];
+    o[7] = gu[b];
+  }
+  if (loss) cudaMemcpy(loss, a->d.loss, sizeof(double) * a->W, cudaMemcpyDeviceToHost);
+  return AVBD_OK;
+}
+
+}  // extern "C"
