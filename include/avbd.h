@@ -386,6 +386,34 @@ int avbd_batch_stream(avbd_batch* batch, void** stream);
 int avbd_batch_tune(avbd_batch* batch, int steps, avbd_batch_tuning* out);
 int avbd_batch_info(avbd_batch* batch, avbd_batch_status* out);
 
+/* ---- Recording a batched rollout for the adjoint -------------------------------------------------
+ * No counterpart in the reference. The next `steps` avbd_batch_step calls append their contact
+ * structure (per step the manifolds with their normal bases, each point's body-frame anchors and
+ * the last-step point it warm-started from, the colouring) to a device recording, three extra
+ * launches per step. The batch must hold boxes only, no joints, default contact rules and up = +z;
+ * the first recorded step must not warm-start from an earlier step (a fresh batch, or bodies
+ * written again with avbd_batch_write_all_bodies_async and flag 1). points_per_body (0: 8) sizes the
+ * recording: steps x bodies x points_per_body points. */
+int avbd_batch_record_start(avbd_batch* batch, uint32_t steps, uint32_t points_per_body);
+/* steps recorded so far, manifolds and points, problems (bits: 1 out of room, 2 warm start from before
+ * the recording, 4 sphere contacts, 8 more than 64 colours) */
+int avbd_batch_record_status(avbd_batch* batch, uint32_t* steps, uint64_t* manifolds, uint64_t* points, uint32_t* problems);
+/* An adjoint of the recorded rollout: it adopts the batch's finished recording (the batch then
+ * holds none) and starts from the bodies as they were when recording began; worlds, steps and the
+ * step parameters are the batch's. */
+int avbd_adjoint_create_from_batch(avbd_batch* batch, uint32_t checkpoint, avbd_adjoint** out);
+/* The parameters the recording ran with: 8 per body (v0 xyz, omega0 xyz, mass, friction); zero for
+ * an adjoint built from a host description */
+int avbd_adjoint_nominal(const avbd_adjoint* adjoint, double* params);
+/* The adjoint's recording in the avbd_adjoint_desc layout (all worlds, global indices; sizes from
+ * avbd_adjoint_info): what avbd_adjoint_create would take to build the same adjoint */
+int avbd_adjoint_read_recording(const avbd_adjoint* adjoint, double* bodies, int32_t* step_first_manifold, int32_t* step_first_point,
+                                int32_t* manifold_bodies, double* manifold_basis, double* point_anchors, int32_t* point_manifold, int32_t* point_prev,
+                                int32_t* colors, int32_t* color_counts);
+/* worlds, steps, bodies, the most points of one world in one step, manifolds and points recorded */
+int avbd_adjoint_info(const avbd_adjoint* adjoint, uint32_t* worlds, uint32_t* steps, uint32_t* bodies, uint32_t* max_points, uint64_t* manifolds,
+                      uint64_t* points);
+
 #ifdef __cplusplus
 }
 #endif

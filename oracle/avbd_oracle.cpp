@@ -2420,6 +2420,53 @@ void orc_adj_export(void* a, double* bodies, int* stepMan, int* stepPt, int* man
   stepMan[P->steps.size()] = m;
   stepPt[P->steps.size()] = p;
 }
+// The inverse of orc_adj_export: a problem from one world's recorded structure (indices over its
+// own steps) and nominal parameters (8 per body); params7: dt gravity alpha gamma betaLin margin iterations
+void* orc_adj_import(const double* params7, int n, int steps, const double* bodies, const double* nominal, const int* stepMan, const int* stepPt,
+                     const int* manBodies, const double* basis, const double* anchors, const int* ptMan, const int* ptPrev, const int* colors,
+                     const int* ncol) {
+  auto* P = new AdjProblem();
+  P->n = n;
+  P->dt = params7[0]; P->gravity = params7[1]; P->alpha = params7[2]; P->gamma = params7[3]; P->betaLin = params7[4]; P->margin = params7[5];
+  P->iterations = int(params7[6]);
+  for (int b = 0; b < n; b++) {
+    const double* r = bodies + 13 * b;
+    const double* q = nominal + 8 * b;
+    P->dynamic.push_back(r[11] != 0.0);
+    for (int k = 0; k < 3; k++) {
+      P->pos.push_back(r[k]);
+      P->prevVel.push_back(k == 2 ? r[7] : 0.0);
+      P->unitMoment.push_back(r[8 + k]);
+      P->vel.push_back(q[k]);
+      P->angVel.push_back(q[3 + k]);
+    }
+    for (int k = 0; k < 4; k++) P->rot.push_back(r[3 + k]);
+    P->mass.push_back(q[6]);
+    P->friction.push_back(r[11] != 0.0 ? q[7] : r[12]);
+  }
+  for (int s = 0; s < steps; s++) {
+    AdjStep st;
+    for (int m = stepMan[s]; m < stepMan[s + 1]; m++) {
+      AdjMan am;
+      am.a = manBodies[2 * m];
+      am.b = manBodies[2 * m + 1];
+      for (int c = 0; c < 9; c++) am.basis[c] = basis[9 * m + c];
+      st.mans.push_back(am);
+    }
+    for (int k = stepPt[s]; k < stepPt[s + 1]; k++) {
+      AdjPoint q;
+      for (int c = 0; c < 3; c++) { q.rA[c] = anchors[6 * k + c]; q.rB[c] = anchors[6 * k + 3 + c]; }
+      q.man = ptMan[k] - stepMan[s];
+      q.prev = ptPrev[k] < 0 ? -1 : ptPrev[k] - stepPt[s - 1];
+      st.pts.push_back(q);
+    }
+    st.color.assign(colors + size_t(s) * n, colors + size_t(s + 1) * n);
+    st.ncol = ncol[s];
+    P->steps.push_back(std::move(st));
+  }
+  P->target.assign(size_t(7) * n, 0.0);
+  return P;
+}
 double orc_adj_param(void* a, int which) {  // 0 dt 1 gravity 2 alpha 3 gamma 4 betaLin 5 margin 6 iterations
   auto* P = static_cast<AdjProblem*>(a);
   double v[7] = {P->dt, P->gravity, P->alpha, P->gamma, P->betaLin, P->margin, double(P->iterations)};

@@ -76,6 +76,8 @@ def lib():
         L.orc_adj_gradient.restype = ctypes.c_double
         L.orc_adj_sizes.argtypes = [P, ctypes.POINTER(I)]
         L.orc_adj_export.argtypes = [P, D] + [ctypes.POINTER(I)] * 3 + [D, D] + [ctypes.POINTER(I)] * 4
+        L.orc_adj_import.argtypes = [D, I, I, D, D] + [ctypes.POINTER(I)] * 3 + [D, D] + [ctypes.POINTER(I)] * 4
+        L.orc_adj_import.restype = P
         L.orc_adj_param.argtypes = [P, I]
         L.orc_adj_param.restype = ctypes.c_double
         _lib = L
@@ -285,6 +287,23 @@ class Adjoint:
             raise ValueError('adjoint problems need the FP64 oracle and a scene without joints')
         self.n = self.L.orc_adj_bodies(self.h)
         self.steps = steps
+
+    @classmethod
+    def from_record(cls, rec: dict, nominal: np.ndarray) -> 'Adjoint':
+        """A problem from one world's recorded structure in the export() layout (for instance the
+        GPU recording's world, split out) with its nominal parameters (8 per body)."""
+        self = cls.__new__(cls)
+        self.L = lib()
+        P = rec['params']
+        p7 = np.array([P['dt'], P['gravity'], P['alpha'], P['gamma'], P['beta_lin'], P['contact_margin'], P['iterations']], np.float64)
+        keep = [np.ascontiguousarray(rec[k], np.int32) for k in ('step_man', 'step_pt', 'man_bodies', 'pt_man', 'pt_prev', 'colors', 'ncol')]
+        dk = [np.ascontiguousarray(x, np.float64) for x in (rec['bodies'], nominal, rec['basis'], rec['anchors'])]
+        I = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        self.h = self.L.orc_adj_import(_dp(p7), int(rec['n']), int(rec['steps']), _dp(dk[0]), _dp(dk[1]), I(keep[0]), I(keep[1]), I(keep[2]),
+                                       _dp(dk[2]), _dp(dk[3]), I(keep[3]), I(keep[4]), I(keep[5]), I(keep[6]))
+        self.n = int(rec['n'])
+        self.steps = int(rec['steps'])
+        return self
 
     def __del__(self):
         if getattr(self, 'h', None):

@@ -47,3 +47,21 @@ def test_gradient_matches_central_differences():
         worst = max(worst, abs(fd - g[j]) / max(abs(fd), abs(g[j])))
     print(f'adjoint vs central differences: worst relative error {worst:.2e}')
     assert worst < 1e-3
+
+
+def test_split_inverts_combine():
+    """adjoint.split takes one world back out of a combined (batched) recording."""
+    from avbd_b200.adjoint import combine, split
+    recs = []
+    for w in range(3):
+        s = tumbling_world(np.random.default_rng(40 + w), 6 + 3 * w)
+        s.params.iterations = 2
+        recs.append(Oracle(s).adjoint(12).export())
+    c = combine(recs)
+    for w, r in enumerate(recs):
+        x = split(c, w, r['params'])
+        for k in ('bodies', 'step_man', 'step_pt', 'colors', 'ncol'):
+            assert np.array_equal(x[k], r[k]), k
+        nm, npts = r['manifolds'], r['points']
+        for k, n in (('man_bodies', 2 * nm), ('basis', 9 * nm), ('anchors', 6 * npts), ('pt_man', npts), ('pt_prev', npts)):
+            assert np.array_equal(x[k][:n], r[k][:n]), k

@@ -157,6 +157,13 @@ SIGNATURES = {
     'avbd_adjoint_set_target': ([P, ctypes.POINTER(ctypes.c_double)], I),
     'avbd_adjoint_forward': ([P] + [ctypes.POINTER(ctypes.c_double)] * 3, I),
     'avbd_adjoint_backward': ([P] + [ctypes.POINTER(ctypes.c_double)] * 3, I),
+    'avbd_adjoint_create_from_batch': ([P, ctypes.c_uint32, ctypes.POINTER(P)], I),
+    'avbd_adjoint_nominal': ([P, ctypes.POINTER(ctypes.c_double)], I),
+    'avbd_adjoint_read_recording': ([P] + [VP] * 10, I),
+    'avbd_adjoint_info': ([P] + [ctypes.POINTER(ctypes.c_uint32)] * 4 + [ctypes.POINTER(ctypes.c_uint64)] * 2, I),
+    'avbd_batch_record_start': ([P, ctypes.c_uint32, ctypes.c_uint32], I),
+    'avbd_batch_record_status': ([P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                  ctypes.POINTER(ctypes.c_uint32)], I),
     'avbd_batch_create': ([ctypes.POINTER(BatchConfig), ctypes.POINTER(P)], I),
     'avbd_batch_destroy': ([P], I),
     'avbd_batch_last_error': ([P], ctypes.c_char_p),

@@ -68,6 +68,42 @@ def combine(records: list) -> dict:
             'pt_prev': cat(pt_prev, np.int32), 'colors': colors, 'ncol': ncol, 'params': records[0]['params'], 'nb': int(first_body[-1])}
 
 
+def split(c: dict, w: int, params: dict) -> dict:
+    """World w of a combined recording as one world's recording (indices over its own steps): the
+    inverse of `combine` for one world."""
+    W, K = c['W'], c['K']
+    fb = c.get('first_body')
+    sm, sp = c['step_man'].reshape(K, W + 1), c['step_pt'].reshape(K, W + 1)
+    bodies_of = lambda arr, per: arr.reshape(K, -1)[:, b0 * per:b1 * per].reshape(-1)
+    if fb is None:
+        raise ValueError('the recording needs first_body')
+    b0, b1 = int(fb[w]), int(fb[w + 1])
+    n = b1 - b0
+    mb, basis, anchors, pt_man, pt_prev = [], [], [], [], []
+    step_man, step_pt = np.zeros(K + 1, np.int32), np.zeros(K + 1, np.int32)
+    m = p = 0
+    for s in range(K):
+        m0, m1, p0, p1 = int(sm[s, w]), int(sm[s, w + 1]), int(sp[s, w]), int(sp[s, w + 1])
+        step_man[s], step_pt[s] = m, p
+        mb.append(c['man_bodies'][2 * m0:2 * m1])
+        basis.append(c['basis'][9 * m0:9 * m1])
+        anchors.append(c['anchors'][6 * p0:6 * p1])
+        pt_man.append(c['pt_man'][p0:p1] - m0 + m)
+        prev = c['pt_prev'][p0:p1]
+        if s > 0:
+            prev = np.where(prev >= 0, prev - int(sp[s - 1, w]) + int(step_pt[s - 1]), -1)
+        pt_prev.append(prev)
+        m += m1 - m0
+        p += p1 - p0
+    step_man[K], step_pt[K] = m, p
+    cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0), dtype=dt)
+    return {'n': n, 'steps': K, 'bodies': c['bodies'][13 * b0:13 * b1].copy(), 'step_man': step_man, 'step_pt': step_pt,
+            'man_bodies': cat(mb, np.int32), 'basis': cat(basis, np.float64), 'anchors': cat(anchors, np.float64),
+            'pt_man': cat(pt_man, np.int32), 'pt_prev': cat(pt_prev, np.int32),
+            'colors': bodies_of(c['colors'], 1).astype(np.int32), 'ncol': c['ncol'].reshape(K, W)[:, w].astype(np.int32).copy(),
+            'params': params, 'manifolds': m, 'points': p}
+
+
 class Adjoint:
     """Double-precision replay and reverse sweep on one B200 for a batch of recorded worlds."""
 
@@ -89,6 +125,48 @@ class Adjoint:
             raise AvbdError(code, 'avbd_adjoint_create failed')
         self.worlds, self.bodies = c['W'], c['nb']
         self.first_body = c['first_body']
+
+    @classmethod
+    def from_batch(cls, batch, checkpoint: int = 10) -> 'Adjoint':
+        """The adjoint of a batch's finished recording (BatchSolver3D.record_start): the device
+        recording is adopted as is; the batch keeps its worlds but no longer the recording."""
+        self = cls.__new__(cls)
+        self.lib = _abi.load()
+        self._keep = None
+        self.handle = ctypes.c_void_p()
+        code = self.lib.avbd_adjoint_create_from_batch(batch.handle, checkpoint, ctypes.byref(self.handle))
+        if code != _abi.AVBD_OK:
+            msg = self.lib.avbd_batch_last_error(batch.handle)
+            raise AvbdError(code, 'avbd_adjoint_create_from_batch: ' + (msg.decode() if msg else ''))
+        info = self.info()
+        self.worlds, self.bodies = info['worlds'], info['bodies']
+        self.first_body = np.array([batch.world_info(w)['first_body'] for w in range(self.worlds)] + [self.bodies], np.uint32)
+        return self
+
+    def info(self) -> dict:
+        u = [ctypes.c_uint32() for _ in range(4)]
+        q = [ctypes.c_uint64() for _ in range(2)]
+        self._check(self.lib.avbd_adjoint_info(self.handle, *[ctypes.byref(x) for x in u + q]))
+        return dict(zip(('worlds', 'steps', 'bodies', 'max_points', 'manifolds', 'points'), [x.value for x in u + q]))
+
+    def read_recording(self) -> dict:
+        """The recording in the layout `combine` builds (all worlds, global indices)."""
+        info = self.info()
+        W, K, nb, nm, npts = info['worlds'], info['steps'], info['bodies'], info['manifolds'], info['points']
+        c = {'W': W, 'K': K, 'nb': nb, 'bodies': np.zeros(13 * nb), 'step_man': np.zeros(K * (W + 1), np.int32),
+             'step_pt': np.zeros(K * (W + 1), np.int32), 'man_bodies': np.zeros(2 * max(nm, 1), np.int32), 'basis': np.zeros(9 * max(nm, 1)),
+             'anchors': np.zeros(6 * max(npts, 1)), 'pt_man': np.zeros(max(npts, 1), np.int32), 'pt_prev': np.zeros(max(npts, 1), np.int32),
+             'colors': np.zeros(K * nb, np.int32), 'ncol': np.zeros(K * W, np.int32)}
+        keys = ('bodies', 'step_man', 'step_pt', 'man_bodies', 'basis', 'anchors', 'pt_man', 'pt_prev', 'colors', 'ncol')
+        self._check(self.lib.avbd_adjoint_read_recording(self.handle, *[c[k].ctypes.data for k in keys]))
+        c['first_body'] = self.first_body
+        return c
+
+    def nominal(self) -> np.ndarray:
+        """The parameters the recorded rollout ran with (8 per body: v0, omega0, mass, friction)."""
+        p = np.zeros(8 * self.bodies)
+        self._check(self.lib.avbd_adjoint_nominal(self.handle, p.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return p
 
     def destroy(self):
         if getattr(self, 'handle', None) and self.handle.value:

@@ -150,3 +150,13 @@ class BatchSolver3D:
 
     def write_all_bodies_async(self, records: np.ndarray):
         self._check(self.lib.avbd_batch_write_all_bodies_async(self.handle, ptr(records), len(records)))
+
+    def record_start(self, steps: int, points_per_body: int = 0):
+        """Record the contact structure of the next `steps` steps for the adjoint (Adjoint.from_batch)."""
+        self._check(self.lib.avbd_batch_record_start(self.handle, steps, points_per_body))
+
+    def record_status(self) -> dict:
+        st, pr = ctypes.c_uint32(), ctypes.c_uint32()
+        m, p = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self.lib.avbd_batch_record_status(self.handle, ctypes.byref(st), ctypes.byref(m), ctypes.byref(p), ctypes.byref(pr)))
+        return {'steps': st.value, 'manifolds': m.value, 'points': p.value, 'problems': pr.value}

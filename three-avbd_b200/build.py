@@ -22,6 +22,7 @@ UNITS = {
     'avbd_batch.cu': [],
     'avbd_hull.cu': [],
     'avbd_adjoint.cu': [],
+    'avbd_record.cu': [],
 }
 
 

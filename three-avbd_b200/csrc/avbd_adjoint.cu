@@ -17,6 +17,7 @@
 
 #include "avbd.h"
 #include "avbd_adjoint_math.cuh"
+#include "avbd_record.hpp"
 
 using namespace avbd::adj;
 
@@ -40,8 +41,7 @@ struct AdjDev {
   const int* ptFirst;   // K x (W + 1)
   const int2* manAB;    // world-local bodies
   const D3* basis;      // 3 rows per manifold
-  const D3* rA;
-  const D3* rB;
+  const D3* anchor;   // 2 per point: rA, rB in the bodies' frames
   const int* ptMan;   // global manifold index
   const int* ptPrev;  // global index into the previous step's points, or -1
   const int* color;   // K x bodies (-1: static)
@@ -146,8 +146,8 @@ struct PointEval {
 __device__ inline void evalPoint(const AdjDev& D, int k, D3 xa, D4 qa, D3 xa0, D4 qa0, D3 xb, D4 qb, D3 xb0, D4 qb0, D3 c0, D3 lam, D3 pen, double fr,
                                  PointEval& e) {
   const D3* B = D.basis + 3 * D.ptMan[k];
-  e.rAW = rotate(qa, D.rA[k]);
-  e.rBW = rotate(qb, D.rB[k]);
+  e.rAW = rotate(qa, D.anchor[2 * k]);
+  e.rBW = rotate(qb, D.anchor[2 * k + 1]);
   e.dAL = xa - xa0;
   e.dAA = qsub(qa, qa0);
   e.dBL = xb - xb0;
@@ -218,8 +218,8 @@ __device__ inline void evalCVjp(const AdjDev& D, int k, D4 qa, D4 qa0, D4 qb, D4
   gXb0 -= gdBL;
   qsubVjp(qa, qa0, gdAA, gQa, gQa0);
   qsubVjp(qb, qb0, gdBA, gQb, gQb0);
-  gQa += rotateVjpQ(qa, D.rA[k], grA);
-  gQb += rotateVjpQ(qb, D.rB[k], grB);
+  gQa += rotateVjpQ(qa, D.anchor[2 * k], grA);
+  gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], grB);
 }
 
 // The 6x6 system of body gb (its inertia and its points' rows) at the current poses
@@ -287,7 +287,7 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
     for (int c = 0; c < 3; c++) setComp(pw, c, fmin(fmax(comp(pe, c) * D.gamma, PEN_MIN), PEN_MAX));
     int2 ab = D.manAB[D.ptMan[k]];
     int a = v.b0 + ab.x, b = v.b0 + ab.y;
-    D3 d = (rotate(D.rot[a], D.rA[k]) + D.pos[a]) - (rotate(D.rot[b], D.rB[k]) + D.pos[b]);
+    D3 d = (rotate(D.rot[a], D.anchor[2 * k]) + D.pos[a]) - (rotate(D.rot[b], D.anchor[2 * k + 1]) + D.pos[b]);
     const D3* B = D.basis + 3 * D.ptMan[k];
     D3 c0{dot(B[0], d) + D.margin, dot(B[1], d), dot(B[2], d)};
     D.lam[wpt + lk] = lw;
@@ -636,8 +636,8 @@ __device__ void primalVjp(const AdjDev& D, const StepView& v, int wpt, int it, i
     D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
     evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
     // the lever arm r = R(q_own) r_local
-    if (isA) gQa += rotateVjpQ(qa, D.rA[k], gr);
-    else gQb += rotateVjpQ(qb, D.rB[k], gr);
+    if (isA) gQa += rotateVjpQ(qa, D.anchor[2 * k], gr);
+    else gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], gr);
     // own terms stay local; the partner's go to its current cotangent
     if (isA) {
       gX += gXa;
@@ -819,11 +819,11 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
     D3 gd = B[0] * gc0.x + B[1] * gc0.y + B[2] * gc0.z;
     if (D.dynamic[a]) {
       atomicAdd3(&D.gIpos[a], gd);
-      atomicAdd4(&D.gIrot[a], rotateVjpQ(D.irot[a], D.rA[k], gd));
+      atomicAdd4(&D.gIrot[a], rotateVjpQ(D.irot[a], D.anchor[2 * k], gd));
     }
     if (D.dynamic[b]) {
       atomicAdd3(&D.gIpos[b], -gd);
-      atomicAdd4(&D.gIrot[b], rotateVjpQ(D.irot[b], D.rB[k], -gd));
+      atomicAdd4(&D.gIrot[b], rotateVjpQ(D.irot[b], D.anchor[2 * k + 1], -gd));
     }
   }
   __syncthreads();
@@ -923,6 +923,8 @@ struct avbd_adjoint {
   AdjDev d{};
   std::vector<void*> allocations;
   int W = 0, nb = 0;
+  std::vector<double> nominal;        // 8 per body when built from a batch recording
+  uint64_t manifolds = 0, points = 0;
   bool forwardDone = false;  // the checkpoints hold the forward of lastParams
   std::vector<double> lastParams;
 };
@@ -949,6 +951,38 @@ bool aupload(avbd_adjoint* a, const T** dst, const T* src, size_t n) {
   if (n && cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return false;
   *dst = p;
   return true;
+}
+
+// The replay's working buffers, checkpoints, snapshots and cotangents (D's sizes set)
+bool adjAllocWork(avbd_adjoint* a) {
+  AdjDev& D = a->d;
+  const size_t W = size_t(D.W), K = size_t(D.K), nb = size_t(D.nb);
+  bool ok = true;
+  const size_t WP = W * size_t(D.maxPts), segs = (K + D.ck - 1) / D.ck, I1 = size_t(D.I) + 1;
+  double* prm = nullptr;
+  double* tgt = nullptr;
+  ok = ok && aalloc(a, &prm, 8 * size_t(nb)) && aalloc(a, &tgt, 7 * size_t(nb));
+  D.params = prm;
+  D.target = tgt;
+  for (D3** p : {&D.pos, &D.vel, &D.ang, &D.ipos, &D.ypos, &D.gPos, &D.gVel, &D.gAng, &D.gIpos, &D.gYpos}) ok = ok && aalloc(a, p, nb);
+  for (D4** p : {&D.rot, &D.irot, &D.yrot, &D.gRot, &D.gIrot, &D.gYrot}) ok = ok && aalloc(a, p, nb);
+  for (double** p : {&D.pvz, &D.gPvz, &D.gMass, &D.gMu}) ok = ok && aalloc(a, p, nb);
+  for (D3** p : {&D.lam, &D.pen, &D.lamP, &D.penP, &D.C0, &D.gLam, &D.gPen, &D.gLamP, &D.gPenP, &D.gC0}) ok = ok && aalloc(a, p, WP);
+  ok = ok && aalloc(a, &D.ckPos, segs * nb) && aalloc(a, &D.ckVel, segs * nb) && aalloc(a, &D.ckAng, segs * nb) && aalloc(a, &D.ckRot, segs * nb) &&
+       aalloc(a, &D.ckPvz, segs * nb) && aalloc(a, &D.ckLam, segs * WP) && aalloc(a, &D.ckPen, segs * WP);
+  ok = ok && aalloc(a, &D.sgPos, size_t(D.ck) * nb) && aalloc(a, &D.sgVel, size_t(D.ck) * nb) && aalloc(a, &D.sgAng, size_t(D.ck) * nb) &&
+       aalloc(a, &D.sgRot, size_t(D.ck) * nb) && aalloc(a, &D.sgPvz, size_t(D.ck) * nb) && aalloc(a, &D.sgLam, size_t(D.ck) * WP) &&
+       aalloc(a, &D.sgPen, size_t(D.ck) * WP);
+  const size_t CK = size_t(D.ck);
+  ok = ok && aalloc(a, &D.snPos, CK * I1 * nb) && aalloc(a, &D.snRot, CK * I1 * nb) && aalloc(a, &D.snLam, CK * I1 * WP) && aalloc(a, &D.snPen, CK * I1 * WP);
+  ok = ok && aalloc(a, &D.stIpos, CK * nb) && aalloc(a, &D.stIrot, CK * nb) && aalloc(a, &D.stYpos, CK * nb) && aalloc(a, &D.stYrot, CK * nb) &&
+       aalloc(a, &D.stC0, CK * WP);
+  double* loss = nullptr;
+  double* fin = nullptr;
+  ok = ok && aalloc(a, &loss, W) && aalloc(a, &fin, 7 * size_t(nb));
+  D.loss = loss;
+  D.finalPose = fin;
+  return ok;
 }
 
 }  // namespace
@@ -1005,6 +1039,8 @@ int avbd_adjoint_create(const avbd_adjoint_desc* desc, avbd_adjoint** out) {
   a->device = desc->device;
   a->W = int(W);
   a->nb = int(nb);
+  a->manifolds = nm;
+  a->points = npts;
   AdjDev& D = a->d;
   D.W = int(W);
   D.K = int(K);
@@ -1035,51 +1071,173 @@ int avbd_adjoint_create(const avbd_adjoint_desc* desc, avbd_adjoint** out) {
   std::vector<int> mf(desc->step_first_manifold, desc->step_first_manifold + K * (W + 1));
   std::vector<int> pf(desc->step_first_point, desc->step_first_point + K * (W + 1));
   std::vector<int2> ab(nm);
-  std::vector<D3> basis(3 * size_t(nm)), ra(npts), rb(npts);
+  std::vector<D3> basis(3 * size_t(nm)), anchors(2 * size_t(npts));
   for (uint32_t m = 0; m < nm; m++) {
     ab[m] = make_int2(desc->manifold_bodies[2 * m], desc->manifold_bodies[2 * m + 1]);
     for (int c = 0; c < 3; c++) basis[3 * m + c] = D3{desc->manifold_basis[9 * m + 3 * c], desc->manifold_basis[9 * m + 3 * c + 1], desc->manifold_basis[9 * m + 3 * c + 2]};
   }
   for (uint32_t k = 0; k < npts; k++) {
     const double* r = desc->point_anchors + 6 * k;
-    ra[k] = D3{r[0], r[1], r[2]};
-    rb[k] = D3{r[3], r[4], r[5]};
+    anchors[2 * k] = D3{r[0], r[1], r[2]};
+    anchors[2 * k + 1] = D3{r[3], r[4], r[5]};
   }
   bool ok = aupload(a, &D.bodyFirst, fb.data(), fb.size()) && aupload(a, &D.pos0, pos0.data(), nb) && aupload(a, &D.rot0, rot0.data(), nb) &&
             aupload(a, &D.prevVz0, pvz.data(), nb) && aupload(a, &D.unitMoment, um.data(), nb) && aupload(a, &D.dynamic, dyn.data(), nb) &&
             aupload(a, &D.fricStatic, fs.data(), nb) && aupload(a, &D.manFirst, mf.data(), mf.size()) && aupload(a, &D.ptFirst, pf.data(), pf.size()) &&
-            aupload(a, &D.manAB, ab.data(), nm) && aupload(a, &D.basis, basis.data(), basis.size()) && aupload(a, &D.rA, ra.data(), npts) &&
-            aupload(a, &D.rB, rb.data(), npts) && aupload(a, &D.ptMan, desc->point_manifold, npts) && aupload(a, &D.ptPrev, desc->point_prev, npts) &&
+            aupload(a, &D.manAB, ab.data(), nm) && aupload(a, &D.basis, basis.data(), basis.size()) && aupload(a, &D.anchor, anchors.data(), anchors.size()) && aupload(a, &D.ptMan, desc->point_manifold, npts) && aupload(a, &D.ptPrev, desc->point_prev, npts) &&
             aupload(a, &D.color, desc->colors, size_t(K) * nb) && aupload(a, &D.ncol, desc->color_counts, size_t(K) * W);
-  const size_t WP = size_t(W) * maxPts, segs = (K + D.ck - 1) / D.ck, I1 = size_t(D.I) + 1;
-  double* prm = nullptr;
-  double* tgt = nullptr;
-  ok = ok && aalloc(a, &prm, 8 * size_t(nb)) && aalloc(a, &tgt, 7 * size_t(nb));
-  D.params = prm;
-  D.target = tgt;
-  for (D3** p : {&D.pos, &D.vel, &D.ang, &D.ipos, &D.ypos, &D.gPos, &D.gVel, &D.gAng, &D.gIpos, &D.gYpos}) ok = ok && aalloc(a, p, nb);
-  for (D4** p : {&D.rot, &D.irot, &D.yrot, &D.gRot, &D.gIrot, &D.gYrot}) ok = ok && aalloc(a, p, nb);
-  for (double** p : {&D.pvz, &D.gPvz, &D.gMass, &D.gMu}) ok = ok && aalloc(a, p, nb);
-  for (D3** p : {&D.lam, &D.pen, &D.lamP, &D.penP, &D.C0, &D.gLam, &D.gPen, &D.gLamP, &D.gPenP, &D.gC0}) ok = ok && aalloc(a, p, WP);
-  ok = ok && aalloc(a, &D.ckPos, segs * nb) && aalloc(a, &D.ckVel, segs * nb) && aalloc(a, &D.ckAng, segs * nb) && aalloc(a, &D.ckRot, segs * nb) &&
-       aalloc(a, &D.ckPvz, segs * nb) && aalloc(a, &D.ckLam, segs * WP) && aalloc(a, &D.ckPen, segs * WP);
-  ok = ok && aalloc(a, &D.sgPos, size_t(D.ck) * nb) && aalloc(a, &D.sgVel, size_t(D.ck) * nb) && aalloc(a, &D.sgAng, size_t(D.ck) * nb) &&
-       aalloc(a, &D.sgRot, size_t(D.ck) * nb) && aalloc(a, &D.sgPvz, size_t(D.ck) * nb) && aalloc(a, &D.sgLam, size_t(D.ck) * WP) &&
-       aalloc(a, &D.sgPen, size_t(D.ck) * WP);
-  const size_t CK = size_t(D.ck);
-  ok = ok && aalloc(a, &D.snPos, CK * I1 * nb) && aalloc(a, &D.snRot, CK * I1 * nb) && aalloc(a, &D.snLam, CK * I1 * WP) && aalloc(a, &D.snPen, CK * I1 * WP);
-  ok = ok && aalloc(a, &D.stIpos, CK * nb) && aalloc(a, &D.stIrot, CK * nb) && aalloc(a, &D.stYpos, CK * nb) && aalloc(a, &D.stYrot, CK * nb) &&
-       aalloc(a, &D.stC0, CK * WP);
-  double* loss = nullptr;
-  double* fin = nullptr;
-  ok = ok && aalloc(a, &loss, W) && aalloc(a, &fin, 7 * size_t(nb));
-  D.loss = loss;
-  D.finalPose = fin;
+  ok = ok && adjAllocWork(a);
   if (!ok) {
     avbd_adjoint_destroy(a);
     return AVBD_ERR_CUDA;
   }
   *out = a;
+  return AVBD_OK;
+}
+
+int avbd_adjoint_create_from_batch(avbd_batch* batch, uint32_t checkpoint, avbd_adjoint** out) {
+  if (!batch || !out) return AVBD_ERR_INVALID;
+  *out = nullptr;
+  avbd::RecordingHandoff h;
+  std::string why;
+  int r = avbd::batch_take_recording(batch, h, why);
+  if (r) return r;
+  cudaSetDevice(h.device);
+  auto* a = new avbd_adjoint();
+  a->device = h.device;
+  a->allocations = h.mem;  // adopted: freed with the adjoint
+  const uint32_t W = h.W, nb = h.nb;
+  for (uint32_t w = 0; w < W; w++)
+    if (h.worldFirst[w + 1] - h.worldFirst[w] > uint32_t(ADJ_THREADS)) {
+      avbd_adjoint_destroy(a);
+      return AVBD_ERR_CAPACITY;  // a world holds at most 128 bodies
+    }
+  if (h.maxPts > uint32_t(ADJ_MAX_POINTS)) {
+    avbd_adjoint_destroy(a);
+    return AVBD_ERR_CAPACITY;
+  }
+  a->W = int(W);
+  a->nb = int(nb);
+  a->manifolds = h.manifolds;
+  a->points = h.points;
+  AdjDev& D = a->d;
+  D.W = int(W);
+  D.K = int(h.K);
+  D.I = h.params.iterations;
+  D.ck = checkpoint ? int(checkpoint) : 10;
+  D.dt = h.params.dt;
+  D.g = h.params.gravity;
+  D.alpha = h.params.alpha;
+  D.gamma = h.params.gamma;
+  D.beta = h.params.beta_lin;
+  D.margin = h.params.contact_margin;
+  D.nb = int(nb);
+  D.maxPts = std::max<int>(1, int(h.maxPts));
+  D.manFirst = h.manFirst;
+  D.ptFirst = h.ptFirst;
+  D.manAB = static_cast<const int2*>(h.manAB);
+  D.basis = reinterpret_cast<const D3*>(h.basis);
+  D.anchor = reinterpret_cast<const D3*>(h.anchors);
+  D.ptMan = h.ptMan;
+  D.ptPrev = h.ptPrev;
+  D.color = h.color;
+  D.ncol = h.ncol;
+  std::vector<D3> pos0(nb), um(nb);
+  std::vector<D4> rot0(nb);
+  std::vector<double> pvz(nb), fs(nb);
+  std::vector<int> dyn(nb), fb(h.worldFirst.begin(), h.worldFirst.end());
+  a->nominal.assign(8 * size_t(nb), 0.0);
+  for (uint32_t b = 0; b < nb; b++) {
+    const avbd_body& x = h.initial[b];
+    const bool d = x.mass > 0.0f;
+    pos0[b] = D3{x.pos[0], x.pos[1], x.pos[2]};
+    rot0[b] = D4{x.rot[0], x.rot[1], x.rot[2], x.rot[3]};
+    pvz[b] = x.prev_up_vel;
+    um[b] = d ? D3{double(x.moment[0]) / x.mass, double(x.moment[1]) / x.mass, double(x.moment[2]) / x.mass} : D3{0, 0, 0};
+    dyn[b] = d;
+    fs[b] = x.friction;
+    double* q = a->nominal.data() + 8 * size_t(b);
+    if (d) {
+      for (int k = 0; k < 3; k++) {
+        q[k] = x.vel[k];
+        q[3 + k] = x.ang_vel[k];
+      }
+      q[6] = x.mass;
+    }
+    q[7] = x.friction;
+  }
+  bool ok = aupload(a, &D.bodyFirst, fb.data(), fb.size()) && aupload(a, &D.pos0, pos0.data(), nb) && aupload(a, &D.rot0, rot0.data(), nb) &&
+            aupload(a, &D.prevVz0, pvz.data(), nb) && aupload(a, &D.unitMoment, um.data(), nb) && aupload(a, &D.dynamic, dyn.data(), nb) &&
+            aupload(a, &D.fricStatic, fs.data(), nb);
+  ok = ok && adjAllocWork(a);
+  if (!ok) {
+    avbd_adjoint_destroy(a);
+    return AVBD_ERR_CUDA;
+  }
+  *out = a;
+  return AVBD_OK;
+}
+
+int avbd_adjoint_nominal(const avbd_adjoint* a, double* params) {
+  if (!a || !params) return AVBD_ERR_INVALID;
+  if (a->nominal.empty()) std::memset(params, 0, sizeof(double) * 8 * size_t(a->nb));
+  else std::memcpy(params, a->nominal.data(), sizeof(double) * a->nominal.size());
+  return AVBD_OK;
+}
+
+int avbd_adjoint_info(const avbd_adjoint* a, uint32_t* worlds, uint32_t* steps, uint32_t* bodies, uint32_t* max_points, uint64_t* manifolds,
+                      uint64_t* points) {
+  if (!a) return AVBD_ERR_INVALID;
+  if (worlds) *worlds = uint32_t(a->W);
+  if (steps) *steps = uint32_t(a->d.K);
+  if (bodies) *bodies = uint32_t(a->nb);
+  if (max_points) *max_points = uint32_t(a->d.maxPts);
+  if (manifolds) *manifolds = a->manifolds;
+  if (points) *points = a->points;
+  return AVBD_OK;
+}
+
+int avbd_adjoint_read_recording(const avbd_adjoint* a, double* bodies, int32_t* step_first_manifold, int32_t* step_first_point, int32_t* manifold_bodies,
+                                double* manifold_basis, double* point_anchors, int32_t* point_manifold, int32_t* point_prev, int32_t* colors,
+                                int32_t* color_counts) {
+  if (!a || !bodies || !step_first_manifold || !step_first_point || !colors || !color_counts) return AVBD_ERR_INVALID;
+  if ((a->manifolds && (!manifold_bodies || !manifold_basis)) || (a->points && (!point_anchors || !point_manifold || !point_prev)))
+    return AVBD_ERR_INVALID;
+  cudaSetDevice(a->device);
+  if (cudaDeviceSynchronize() != cudaSuccess) return AVBD_ERR_CUDA;
+  const AdjDev& D = a->d;
+  const size_t nb = size_t(a->nb), K = size_t(D.K), W = size_t(D.W);
+  std::vector<D3> pos(nb), um(nb);
+  std::vector<D4> rot(nb);
+  std::vector<double> pvz(nb), fs(nb);
+  std::vector<int> dyn(nb);
+  bool ok = cudaMemcpy(pos.data(), D.pos0, nb * sizeof(D3), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(rot.data(), D.rot0, nb * sizeof(D4), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(pvz.data(), D.prevVz0, nb * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(um.data(), D.unitMoment, nb * sizeof(D3), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(dyn.data(), D.dynamic, nb * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(fs.data(), D.fricStatic, nb * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(step_first_manifold, D.manFirst, K * (W + 1) * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(step_first_point, D.ptFirst, K * (W + 1) * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(colors, D.color, K * nb * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            cudaMemcpy(color_counts, D.ncol, K * W * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (ok && a->manifolds)
+    ok = cudaMemcpy(manifold_bodies, D.manAB, a->manifolds * sizeof(int2), cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(manifold_basis, D.basis, a->manifolds * 3 * sizeof(D3), cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (ok && a->points)
+    ok = cudaMemcpy(point_anchors, D.anchor, a->points * 2 * sizeof(D3), cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(point_manifold, D.ptMan, a->points * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(point_prev, D.ptPrev, a->points * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (!ok) return AVBD_ERR_CUDA;
+  for (size_t b = 0; b < nb; b++) {
+    double* r = bodies + 13 * b;
+    r[0] = pos[b].x, r[1] = pos[b].y, r[2] = pos[b].z;
+    r[3] = rot[b].x, r[4] = rot[b].y, r[5] = rot[b].z, r[6] = rot[b].w;
+    r[7] = pvz[b];
+    r[8] = um[b].x, r[9] = um[b].y, r[10] = um[b].z;
+    r[11] = dyn[b] ? 1.0 : 0.0;
+    r[12] = fs[b];
+  }
   return AVBD_OK;
 }
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "avbd_host.hpp"
+#include "avbd_record.hpp"
 
 using namespace avbd;
 
@@ -53,6 +54,14 @@ struct avbd_batch {
   uint64_t graphGen[2] = {0, 0};
   uint64_t configGen = 1;
   std::vector<void*> allocations;
+  // the adjoint's recording (avbd_batch_record_start): steps still to append, its device arrays
+  struct Recording {
+    uint32_t K = 0, done = 0;
+    RecordDev d{};
+    std::vector<void*> mem;
+    std::vector<avbd_body> initial;
+    avbd_params params{};
+  } rec;
 };
 
 namespace {
@@ -331,7 +340,95 @@ void bodiesOut(avbd_batch* b, uint32_t first, avbd_body* dst, uint32_t n) {
                       cudaMemcpyDeviceToHost, b->stream);
 }
 
+void freeRecording(avbd_batch* b) {
+  for (void* p : b->rec.mem) cudaFree(p);
+  b->rec = avbd_batch::Recording{};
+}
+
+template <class T>
+bool recAlloc(avbd_batch* b, T** p, size_t count) {
+  void* ptr = nullptr;
+  if (cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) return false;
+  b->rec.mem.push_back(ptr);
+  *p = static_cast<T*>(ptr);
+  return cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), b->stream) == cudaSuccess;
+}
+
 }  // namespace
+
+static int takeRecording(avbd_batch* b, RecordingHandoff& out, std::string& why);
+
+int avbd::batch_take_recording(avbd_batch* b, RecordingHandoff& out, std::string& why) {
+  if (!b) return AVBD_ERR_INVALID;
+  int r = takeRecording(b, out, why);
+  if (r) b->error = why;
+  return r;
+}
+
+static int takeRecording(avbd_batch* b, RecordingHandoff& out, std::string& why) {
+  const auto& R = b->rec;
+  if (!R.K) {
+    why = "the batch holds no recording (avbd_batch_record_start)";
+    return AVBD_ERR_INVALID;
+  }
+  if (R.done < R.K) {
+    why = "the recording holds " + std::to_string(R.done) + " of its " + std::to_string(R.K) + " steps";
+    return AVBD_ERR_INVALID;
+  }
+  cudaSetDevice(b->device);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+    why = "the batch's stream failed";
+    return AVBD_ERR_CUDA;
+  }
+  uint32_t status[2] = {0, 0};
+  unsigned long long totals[2] = {0, 0};
+  if (cudaMemcpy(status, R.d.status, sizeof(status), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(totals, R.d.totals, sizeof(totals), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    why = "reading the recording's status failed";
+    return AVBD_ERR_CUDA;
+  }
+  if (status[0] & REC_CAPACITY) {
+    why = "the recording ran out of room: start it again with more points per body";
+    return AVBD_ERR_CAPACITY;
+  }
+  if (status[0] & REC_HISTORY) {
+    why = "a recorded step warm-started from contacts of a step before the recording (write the bodies again, or record from the first step)";
+    return AVBD_ERR_INVALID;
+  }
+  if (status[0] & REC_SPHERE) {
+    why = "the recording holds sphere contacts, which the adjoint does not differentiate";
+    return AVBD_ERR_INVALID;
+  }
+  if (status[0] & (REC_COLORS | REC_ORDER)) {
+    why = "the recording holds a step with more than 64 colours or a misordered pair";
+    return AVBD_ERR_INVALID;
+  }
+  out.device = b->device;
+  out.K = R.K;
+  out.W = R.d.W;
+  out.nb = R.d.nb;
+  out.maxPts = status[1];
+  out.manifolds = totals[0];
+  out.points = totals[1];
+  out.manFirst = R.d.manFirst;
+  out.ptFirst = R.d.ptFirst;
+  out.ptMan = R.d.ptMan;
+  out.ptPrev = R.d.ptPrev;
+  out.color = R.d.color;
+  out.ncol = R.d.ncol;
+  out.manAB = R.d.manAB;
+  out.basis = R.d.basis;
+  out.anchors = R.d.anchors;
+  out.worldFirst.clear();
+  for (auto& w : b->worlds) out.worldFirst.push_back(w.body);
+  out.worldFirst.push_back(b->n);
+  out.initial = R.initial;
+  out.params = R.params;
+  out.mem = R.mem;
+  b->rec.mem.clear();  // the receiver owns the device arrays now
+  b->rec = avbd_batch::Recording{};
+  return AVBD_OK;
+}
 
 extern "C" {
 
@@ -402,6 +499,7 @@ int avbd_batch_destroy(avbd_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (void* p : b->allocations) cudaFree(p);
   b->allocations.clear();
+  freeRecording(b);
   for (auto& g : b->graph)
     if (g) cudaGraphExecDestroy(g);
   if (b->hStatus) cudaFreeHost(b->hStatus);
@@ -427,6 +525,7 @@ int avbd_batch_add_world(avbd_batch* b, const avbd_body* bodies, uint32_t n, con
   if (n == 0 || n > BATCH_MAX_WORLD_BODIES)
     return bfail(b, AVBD_ERR_INVALID, "a batched world holds 1 to " + std::to_string(BATCH_MAX_WORLD_BODIES) + " bodies");
   if (b->worlds.size() >= b->worldCap) return bfail(b, AVBD_ERR_CAPACITY, "world capacity " + std::to_string(b->worldCap) + " reached");
+  if (b->rec.K) return bfail(b, AVBD_ERR_INVALID, "a recording is in progress: adopt it (avbd_adjoint_create_from_batch) before adding worlds");
   if (uint64_t(b->n) + n > b->bodyCap) return bfail(b, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(b->bodyCap) + " reached");
   if (uint64_t(b->nj) + nj > b->jointCap) return bfail(b, AVBD_ERR_CAPACITY, "joint capacity " + std::to_string(b->jointCap) + " reached");
   std::string msg = bodyProblem(bodies, n);
@@ -469,10 +568,12 @@ int avbd_batch_add_world_from(avbd_batch* b, avbd_world* src, uint32_t* index) {
   if (!b || !src) return AVBD_ERR_INVALID;
   if (src->device != b->device) return bfail(b, AVBD_ERR_INVALID, "the world is on another device");
   if (!src->hullWords.empty()) return bfail(b, AVBD_ERR_INVALID, "batched worlds hold boxes, spheres and sails");
+  if (b->rec.K) return bfail(b, AVBD_ERR_INVALID, "a recording is in progress: adopt it (avbd_adjoint_create_from_batch) before adding worlds");
   const uint32_t n = src->n, nj = src->nj;
   if (n == 0 || n > BATCH_MAX_WORLD_BODIES)
     return bfail(b, AVBD_ERR_INVALID, "a batched world holds 1 to " + std::to_string(BATCH_MAX_WORLD_BODIES) + " bodies");
   if (b->worlds.size() >= b->worldCap) return bfail(b, AVBD_ERR_CAPACITY, "world capacity " + std::to_string(b->worldCap) + " reached");
+  if (b->rec.K) return bfail(b, AVBD_ERR_INVALID, "a recording is in progress: adopt it (avbd_adjoint_create_from_batch) before adding worlds");
   if (uint64_t(b->n) + n > b->bodyCap) return bfail(b, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(b->bodyCap) + " reached");
   if (uint64_t(b->nj) + nj > b->jointCap) return bfail(b, AVBD_ERR_CAPACITY, "joint capacity " + std::to_string(b->jointCap) + " reached");
   cudaSetDevice(b->device);
@@ -572,6 +673,10 @@ int avbd_batch_step(avbd_batch* b, int steps) {
       }
     }
     if (!launched) BATCH_TRY(b, enqueueStep(b, L));
+    if (b->rec.done < b->rec.K) {
+      BATCH_TRY(b, launch_record_step(L, b->rec.d, b->rec.done, b->sms * 8, b->stream));
+      b->rec.done++;
+    }
     BATCH_TRY(b, cudaEventRecord(b->statusReady, b->stream));
     b->statusInFlight = true;
     b->cur = 1 - b->cur;
@@ -745,6 +850,67 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
   t.ms_per_step = best;
   t.steps_taken = k * uint32_t(steps + 1);
   if (out) *out = t;
+  return AVBD_OK;
+}
+
+int avbd_batch_record_start(avbd_batch* b, uint32_t steps, uint32_t points_per_body) {
+  if (!b || steps == 0) return AVBD_ERR_INVALID;
+  if (b->worlds.empty()) return bfail(b, AVBD_ERR_INVALID, "the batch has no worlds");
+  if (b->nj) return bfail(b, AVBD_ERR_INVALID, "the adjoint differentiates contacts only: the batch holds joints");
+  const avbd_params& P = b->params;
+  if (P.flags & (AVBD_FLAG_MATCH_NEAREST | AVBD_FLAG_MASS_PENALTY | AVBD_FLAG_START_AT_REST))
+    return bfail(b, AVBD_ERR_INVALID, "the adjoint follows the default contact rules: no nearest matching, mass penalty or start at rest");
+  if (P.up[0] != 0.0f || P.up[1] != 0.0f || P.up[2] != 1.0f) return bfail(b, AVBD_ERR_INVALID, "the adjoint needs up = +z");
+  cudaSetDevice(b->device);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  std::vector<avbd_body> bodies(b->n);
+  bodiesOut(b, 0, bodies.data(), b->n);
+  BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+  for (auto& x : bodies)
+    if (x.shape != float(AVBD_SHAPE_BOX)) return bfail(b, AVBD_ERR_INVALID, "the adjoint differentiates boxes only");
+  freeRecording(b);
+  const uint64_t ppb = points_per_body ? points_per_body : 8u;
+  const uint64_t ptCap = uint64_t(steps) * b->n * ppb, manCap = std::max<uint64_t>(ptCap / 2, 1);
+  if (ptCap >= (1ull << 31)) return bfail(b, AVBD_ERR_CAPACITY, "a recording holds fewer than 2^31 points");
+  auto& R = b->rec;
+  RecordDev& d = R.d;
+  d.K = steps;
+  d.W = uint32_t(b->worlds.size());
+  d.nb = b->n;
+  d.manCap = manCap;
+  d.ptCap = ptCap;
+  int2* ab = nullptr;
+  bool ok = recAlloc(b, &d.manFirst, size_t(steps) * (d.W + 1)) && recAlloc(b, &d.ptFirst, size_t(steps) * (d.W + 1)) &&
+            recAlloc(b, &d.manCount, d.W) && recAlloc(b, &d.ptCount, d.W) && recAlloc(b, &ab, manCap) && recAlloc(b, &d.basis, 9 * manCap) &&
+            recAlloc(b, &d.manSlot, manCap) && recAlloc(b, &d.manPt0, manCap) && recAlloc(b, &d.anchors, 6 * ptCap) &&
+            recAlloc(b, &d.ptMan, ptCap) && recAlloc(b, &d.ptPrev, ptCap) && recAlloc(b, &d.color, size_t(steps) * b->n) &&
+            recAlloc(b, &d.ncol, size_t(steps) * d.W) && recAlloc(b, &d.totals, 2) && recAlloc(b, &d.status, 2);
+  d.manAB = ab;
+  if (!ok) {
+    freeRecording(b);
+    return bfail(b, AVBD_ERR_CUDA, "device memory for the recording");
+  }
+  R.K = steps;
+  R.done = 0;
+  R.initial = std::move(bodies);
+  R.params = P;
+  return AVBD_OK;
+}
+
+int avbd_batch_record_status(avbd_batch* b, uint32_t* steps, uint64_t* manifolds, uint64_t* points, uint32_t* problems) {
+  if (!b) return AVBD_ERR_INVALID;
+  uint32_t status[2] = {0, 0};
+  unsigned long long totals[2] = {0, 0};
+  if (b->rec.K) {
+    cudaSetDevice(b->device);
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    BATCH_TRY(b, cudaMemcpy(status, b->rec.d.status, sizeof(status), cudaMemcpyDeviceToHost));
+    BATCH_TRY(b, cudaMemcpy(totals, b->rec.d.totals, sizeof(totals), cudaMemcpyDeviceToHost));
+  }
+  if (steps) *steps = b->rec.done;
+  if (manifolds) *manifolds = totals[0];
+  if (points) *points = totals[1];
+  if (problems) *problems = status[0];
   return AVBD_OK;
 }
 

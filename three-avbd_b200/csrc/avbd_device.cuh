@@ -260,6 +260,33 @@ int batch_solve_blocks_per_sm();
 constexpr int BATCH_SOLVE_THREADS = 256;  // the solve's block size (its shared tables assume it)
 constexpr uint32_t BATCH_MAX_WORLD_BODIES = 4096;
 
+// The contact structure of a batched rollout, recorded step by step for the adjoint (avbd_record.cu).
+// Step s of the recording holds every world's manifolds, then every world's points, world after
+// world; manFirst/ptFirst (K x (W + 1) global indices) give each world's range. Indices of bodies
+// are world-local, of manifolds and points global.
+struct RecordDev {
+  uint32_t K, W, nb;  // steps, worlds, bodies over all worlds
+  uint64_t manCap, ptCap;
+  int* manFirst;      // K x (W + 1)
+  int* ptFirst;       // K x (W + 1)
+  int* manCount;      // W: the step's manifolds and points per world (scratch)
+  int* ptCount;
+  int2* manAB;        // per manifold: bodies a > b
+  double* basis;      // 9 per manifold: n (B to A), t1, t2 as the solve builds them
+  int* manSlot;       // the world-local pair slot it was found in (ascending within a world's step)
+  int* manPt0;        // global index of its first point
+  double* anchors;    // 6 per point: rA, rB in the bodies' frames
+  int* ptMan;         // global manifold index
+  int* ptPrev;        // global index of the last step's point it warm-started from, or -1
+  int* color;         // K x nb: the body's colour, -1 for a static body
+  int* ncol;          // K x W: colours of the world's step
+  unsigned long long* totals;  // [0] manifolds, [1] points recorded so far
+  uint32_t* status;            // [0] REC_* bits, [1] most points of one world in one step
+};
+constexpr uint32_t REC_CAPACITY = 1u, REC_HISTORY = 2u, REC_SPHERE = 4u, REC_COLORS = 8u, REC_ORDER = 16u;
+// Appends step s (the step L just ran) to the recording
+cudaError_t launch_record_step(const BatchLaunch& L, const RecordDev& R, uint32_t s, int blocks, cudaStream_t st);
+
 // Host launchers (avbd_solve.cu)
 int solve_grid_blocks(int device);
 cudaError_t launch_topology_solve(const DWorld& w, const StepParams& p, int blocks, cudaStream_t s);
