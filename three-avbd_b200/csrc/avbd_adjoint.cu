@@ -107,27 +107,72 @@ __device__ inline StepView viewOf(const AdjDev& D, int s, int w) {
   return v;
 }
 
+constexpr int ADJ_MAX_COLORS = 64;
+constexpr int ADJ_GROUP = 16;  // bodies of one colour solved together, a thread each
+constexpr int ADJ_ROW = 27;    // an incidence's share of its body's system: H's lower triangle, g
+
+// The step's solve positions: its dynamic coloured bodies by colour, then by index; a colour's
+// bodies are positions s_colStart[c] .. s_colStart[c + 1], and their incidences (local point |
+// position << 16) are contiguous in s_inc, position p's at s_incStart[p] .. s_incStart[p + 1].
+__shared__ int s_colStart[ADJ_MAX_COLORS + 1];
+__shared__ int s_colBody[ADJ_THREADS];
+__shared__ int s_posOf[ADJ_THREADS];
+__shared__ int s_nSolved;
 __shared__ int s_incStart[ADJ_THREADS + 1];
 __shared__ int s_inc[2 * ADJ_MAX_POINTS];
+// Dynamic shared memory: a chunk of incidences, a row each (its share of the body's system, or its
+// own-body cotangents), then, in the reverse sweep, a group's bodies: step, cotangent of g, and for a
+// floored factorization the cotangents of H and L
+struct BodyVjp {
+  double delta[6], w[6], Hb[36], Lb[36];
+  int floored;
+};
+extern __shared__ __align__(16) double s_dyn[];
+constexpr size_t ADJ_SMEM_ROWS = sizeof(double) * ADJ_THREADS * ADJ_ROW;
+constexpr size_t ADJ_SMEM_FORWARD = ADJ_SMEM_ROWS, ADJ_SMEM_BACKWARD = ADJ_SMEM_ROWS + sizeof(BodyVjp) * ADJ_GROUP;
+__device__ inline double* rowOf(int i) { return s_dyn + size_t(i) * ADJ_ROW; }
+__device__ inline BodyVjp* bodyVjp() { return reinterpret_cast<BodyVjp*>(s_dyn + size_t(ADJ_THREADS) * ADJ_ROW); }
 
 __device__ void buildIncidence(const AdjDev& D, const StepView& v) {
-  for (int i = threadIdx.x; i <= v.nb; i += blockDim.x) s_incStart[i] = 0;
+  const int tid = threadIdx.x;
+  for (int i = tid; i <= ADJ_MAX_COLORS; i += blockDim.x) s_colStart[i] = 0;
   __syncthreads();
-  for (int k = v.p0 + threadIdx.x; k < v.p1; k += blockDim.x) {
-    int2 ab = D.manAB[D.ptMan[k]];
-    atomicAdd(&s_incStart[ab.x + 1], 1);
-    atomicAdd(&s_incStart[ab.y + 1], 1);
+  const int myColor = tid < v.nb ? v.color[tid] : -1;
+  const bool solved = myColor >= 0 && myColor < v.ncol;
+  if (solved) atomicAdd(&s_colStart[myColor + 1], 1);
+  __syncthreads();
+  if (tid == 0) {
+    for (int c = 0; c < ADJ_MAX_COLORS; c++) s_colStart[c + 1] += s_colStart[c];
+    s_nSolved = s_colStart[ADJ_MAX_COLORS];
   }
   __syncthreads();
-  if (threadIdx.x == 0)
-    for (int i = 0; i < v.nb; i++) s_incStart[i + 1] += s_incStart[i];
+  int myPos = -1;
+  if (solved) {
+    int r = 0;
+    for (int j = 0; j < tid; j++) r += v.color[j] == myColor;
+    myPos = s_colStart[myColor] + r;
+    s_colBody[myPos] = tid;
+  }
+  if (tid < v.nb) s_posOf[tid] = myPos;
+  for (int i = tid; i <= s_nSolved; i += blockDim.x) s_incStart[i] = 0;
   __syncthreads();
-  // fill in point order per body (a deterministic order: sequential per body)
-  if (threadIdx.x < v.nb) {
-    int b = threadIdx.x, o = s_incStart[b];
+  for (int k = v.p0 + tid; k < v.p1; k += blockDim.x) {
+    const int2 ab = D.manAB[D.ptMan[k]];
+    const int pa = s_posOf[ab.x], pb = s_posOf[ab.y];
+    if (pa >= 0) atomicAdd(&s_incStart[pa + 1], 1);
+    if (pb >= 0) atomicAdd(&s_incStart[pb + 1], 1);
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int i = 0; i < s_nSolved; i++) s_incStart[i + 1] += s_incStart[i];
+  __syncthreads();
+  // fill in point order per body (deterministic)
+  if (tid < s_nSolved) {
+    const int lb = s_colBody[tid];
+    int o = s_incStart[tid];
     for (int k = v.p0; k < v.p1; k++) {
-      int2 ab = D.manAB[D.ptMan[k]];
-      if (ab.x == b || ab.y == b) s_inc[o++] = k;
+      const int2 ab = D.manAB[D.ptMan[k]];
+      if (ab.x == lb || ab.y == lb) s_inc[o++] = (k - v.p0) | (tid << 16);
     }
   }
   __syncthreads();
@@ -222,45 +267,88 @@ __device__ inline void evalCVjp(const AdjDev& D, int k, D4 qa, D4 qa0, D4 qb, D4
   gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], grB);
 }
 
-// The 6x6 system of body gb (its inertia and its points' rows) at the current poses
-__device__ inline void buildSystem(const AdjDev& D, const StepView& v, int wpt, int gb, int lb, Sys6& S, D3& gl, D3& ga, const D3* P, const D4* Q,
-                                   const D3* lamCur, const D3* penCur) {
-  const double dt2 = D.dt * D.dt;
-  const double m = mass(D, gb) / dt2;
-  D3 Iu = D.unitMoment[gb];
-  D3 I = Iu * (mass(D, gb) / dt2);
-  for (int i = 0; i < 6; i++)
-    for (int j = 0; j < 6; j++) S.A[i][j] = 0.0;
-  S.A[0][0] = S.A[1][1] = S.A[2][2] = m;
-  S.A[3][3] = I.x;
-  S.A[4][4] = I.y;
-  S.A[5][5] = I.z;
-  gl = (P[gb] - D.ypos[gb]) * m;
-  D3 qd = qsub(Q[gb], D.yrot[gb]);
-  ga = D3{I.x * qd.x, I.y * qd.y, I.z * qd.z};
-  for (int t = s_incStart[lb]; t < s_incStart[lb + 1]; t++) {
-    int k = s_inc[t];
-    int2 ab = D.manAB[D.ptMan[k]];
-    int a = v.b0 + ab.x, b = v.b0 + ab.y;
-    double fr = sqrt(mu(D, a) * mu(D, b));
-    PointEval e;
-    int lk = k - v.p0;
-    evalPoint(D, k, P[a], Q[a], D.ipos[a], D.irot[a], P[b], Q[b], D.ipos[b], D.irot[b], D.C0[wpt + lk], lamCur[wpt + lk], penCur[wpt + lk], fr, e);
-    bool isA = gb == a;
-    double sg = isA ? 1.0 : -1.0;
-    D3 r = isA ? e.rAW : e.rBW;
-    const D3* B = D.basis + 3 * D.ptMan[k];
-    for (int c = 0; c < 3; c++) {
-      D3 l = B[c] * sg;
-      D3 aa = cross(r, l);
-      double kk = comp(penCur[wpt + lk], c);
-      double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
-      for (int i = 0; i < 6; i++)
-        for (int j = 0; j < 6; j++) S.A[i][j] += kk * J[i] * J[j];
-      gl += l * comp(e.F, c);
-      ga += aa * comp(e.F, c);
-    }
+// Incidence `entry`'s share of its body's system at the poses poseOf gives: H's lower triangle (21,
+// row-major) and g (6), into row
+template <class PoseOf>
+__device__ inline void incidenceRows(const AdjDev& D, const StepView& v, int wpt, int entry, const D3* lamCur, const D3* penCur, PoseOf poseOf,
+                                     double* row) {
+  const int lk = entry & 0xffff, k = v.p0 + lk;
+  const int gb = v.b0 + s_colBody[entry >> 16];
+  const int2 ab = D.manAB[D.ptMan[k]];
+  const int a = v.b0 + ab.x, b = v.b0 + ab.y;
+  D3 xa, xb;
+  D4 qa, qb;
+  poseOf(a, xa, qa);
+  poseOf(b, xb, qb);
+  PointEval e;
+  evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamCur[wpt + lk], penCur[wpt + lk],
+            sqrt(mu(D, a) * mu(D, b)), e);
+  const double sg = gb == a ? 1.0 : -1.0;
+  const D3 rr = gb == a ? e.rAW : e.rBW;
+  const D3* B = D.basis + 3 * D.ptMan[k];
+  double h[21], r[6];
+  for (int i = 0; i < 21; i++) h[i] = 0.0;
+  for (int i = 0; i < 6; i++) r[i] = 0.0;
+  for (int c = 0; c < 3; c++) {
+    const D3 l = B[c] * sg;
+    const D3 aa = cross(rr, l);
+    const double kk = comp(penCur[wpt + lk], c), F = comp(e.F, c);
+    const double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
+    int o = 0;
+    for (int i = 0; i < 6; i++)
+      for (int j = 0; j <= i; j++) h[o++] += kk * J[i] * J[j];
+    for (int i = 0; i < 6; i++) r[i] += J[i] * F;
   }
+  for (int i = 0; i < 21; i++) row[i] = h[i];
+  for (int i = 0; i < 6; i++) row[21 + i] = r[i];
+}
+
+// The bodies at positions g0..g1 (thread tid: position g0 + tid) sum their incidences' rows, a chunk
+// of incidences at a time (one per thread), in incidence order
+template <class PoseOf>
+__device__ inline void groupRows(const AdjDev& D, const StepView& v, int wpt, int g0, int g1, const D3* lamCur, const D3* penCur, PoseOf poseOf,
+                                 double* acc) {
+  const int tid = threadIdx.x;
+  for (int i = 0; i < ADJ_ROW; i++) acc[i] = 0.0;
+  const int i0 = s_incStart[g0], i1 = s_incStart[g1];
+  for (int ch = i0; ch < i1; ch += blockDim.x) {
+    if (ch + tid < i1) incidenceRows(D, v, wpt, s_inc[ch + tid], lamCur, penCur, poseOf, rowOf(tid));
+    __syncthreads();
+    if (tid < g1 - g0) {
+      const int p = g0 + tid;
+      const int u0 = max(s_incStart[p], ch), u1 = min(s_incStart[p + 1], ch + int(blockDim.x));
+      for (int u = u0; u < u1; u++)
+        for (int i = 0; i < ADJ_ROW; i++) acc[i] += rowOf(u - ch)[i];
+    }
+    __syncthreads();
+  }
+}
+
+// Body gb's system: its rows' sums and its inertia (solver.ts:300-318)
+template <class PoseOf>
+__device__ inline void bodySystem(const AdjDev& D, int gb, const double* acc, PoseOf poseOf, Sys6& S, double* g) {
+  int o = 0;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j <= i; j++) S.A[i][j] = acc[o++];
+  for (int i = 0; i < 6; i++) g[i] = acc[21 + i];
+  const double dt2 = D.dt * D.dt, m = mass(D, gb) / dt2;
+  const D3 I = D.unitMoment[gb] * m;
+  D3 x;
+  D4 q;
+  poseOf(gb, x, q);
+  S.A[0][0] += m;
+  S.A[1][1] += m;
+  S.A[2][2] += m;
+  S.A[3][3] += I.x;
+  S.A[4][4] += I.y;
+  S.A[5][5] += I.z;
+  const D3 gl = (x - D.ypos[gb]) * m, qd = qsub(q, D.yrot[gb]);
+  g[0] += gl.x;
+  g[1] += gl.y;
+  g[2] += gl.z;
+  g[3] += I.x * qd.x;
+  g[4] += I.y * qd.y;
+  g[5] += I.z * qd.z;
 }
 
 // One step of the replay (the oracle's stepGpu with the recorded structure). With snapshots, the
@@ -332,21 +420,29 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
       D.stC0[(size_t)slot * D.W * D.maxPts + wpt + lk] = D.C0[wpt + lk];
     }
   __syncthreads();
+  auto livePose = [&](int b, D3& x, D4& q) {
+    x = D.pos[b];
+    q = D.rot[b];
+  };
   for (int it = 0; it < D.I; it++) {
-    for (int c = 0; c < v.ncol; c++) {
-      if (threadIdx.x < v.nb && v.color[threadIdx.x] == c) {
-        int lb = threadIdx.x, gb = v.b0 + lb;
-        Sys6 S;
-        D3 gl, ga;
-        buildSystem(D, v, wpt, gb, lb, S, gl, ga, D.pos, D.rot, D.lam, D.pen);
-        LDLT6 F;
-        factor6(S, F, PIVOT);
-        double rhs[6] = {gl.x, gl.y, gl.z, ga.x, ga.y, ga.z}, dx[6];
-        solve6(F, rhs, dx);
-        D.pos[gb] = D.pos[gb] - D3{dx[0], dx[1], dx[2]};
-        D.rot[gb] = qaddv(D.rot[gb], D3{-dx[3], -dx[4], -dx[5]});
+    for (int c = 0; c < v.ncol; c++) {  // the colour's bodies in groups, a thread each
+      for (int g0 = s_colStart[c]; g0 < s_colStart[c + 1]; g0 += ADJ_GROUP) {
+        const int g1 = min(g0 + ADJ_GROUP, s_colStart[c + 1]);
+        double acc[ADJ_ROW];
+        groupRows(D, v, wpt, g0, g1, D.lam, D.pen, livePose, acc);
+        if (threadIdx.x < g1 - g0) {
+          const int gb = v.b0 + s_colBody[g0 + threadIdx.x];
+          Sys6 S;
+          double rhs[6], dx[6];
+          bodySystem(D, gb, acc, livePose, S, rhs);
+          LDLT6 F;
+          factor6(S, F, PIVOT);
+          solve6(F, rhs, dx);
+          D.pos[gb] = D.pos[gb] - D3{dx[0], dx[1], dx[2]};
+          D.rot[gb] = qaddv(D.rot[gb], D3{-dx[3], -dx[4], -dx[5]});
+        }
+        __syncthreads();
       }
-      __syncthreads();
     }
     // duals (manifold.ts:202-217)
     for (int lk = threadIdx.x; lk < np; lk += blockDim.x) {
@@ -492,192 +588,195 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_forward(AdjDev D) {
 }
 
 // --- reverse ------------------------------------------------------------------------------------------
-// Body gb's primal update at iteration it (poses read from the snapshots the sweep read): the
-// cotangent of its new pose is turned into cotangents of its old pose, of its partners' poses, of
-// its points' lambda and penalty, of the inertial targets, the step-start poses, its mass and the
-// friction coefficients.
-__device__ void primalVjp(const AdjDev& D, const StepView& v, int wpt, int it, int gb, int lb, int c) {
+// Incidence `entry` of a body in the reverse sweep (its body's step, cotangent of g and floored
+// reverse in the group's BodyVjp): the cotangents from its rows go to its partner's pose and step-start pose,
+// its point's lambda, penalty and C0 and the friction coefficients (atomically), and to its own
+// body's pose and step-start pose, returned in out (gX 3, gQ 4, gX0 3, gQ0 4).
+template <class PoseOf>
+__device__ inline void incidenceVjp(const AdjDev& D, const StepView& v, int wpt, int entry, int g0, const D3* lamIn, const D3* penIn, PoseOf poseOf,
+                                    double* out) {
+  const int lk = entry & 0xffff, k = v.p0 + lk, pos = entry >> 16;
+  const int gb = v.b0 + s_colBody[pos];
+  const BodyVjp& bv = bodyVjp()[pos - g0];
+  const D3 dL{bv.delta[0], bv.delta[1], bv.delta[2]}, dA{bv.delta[3], bv.delta[4], bv.delta[5]};
+  const D3 wl{bv.w[0], bv.w[1], bv.w[2]}, wa{bv.w[3], bv.w[4], bv.w[5]};
+  const int floored = bv.floored;
+  const int2 ab = D.manAB[D.ptMan[k]];
+  const int a = v.b0 + ab.x, b = v.b0 + ab.y;
+  D3 xa, xb;
+  D4 qa, qb;
+  poseOf(a, xa, qa);
+  poseOf(b, xb, qb);
+  const double fr = sqrt(mu(D, a) * mu(D, b));
+  PointEval e;
+  const D3 lamv = lamIn[wpt + lk], penv = penIn[wpt + lk];
+  evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamv, penv, fr, e);
+  const bool isA = gb == a;
+  const double sg = isA ? 1.0 : -1.0;
+  const D3 r = isA ? e.rAW : e.rBW;
+  const D3* B = D.basis + 3 * D.ptMan[k];
+  D3 gF{0, 0, 0}, gPen{0, 0, 0}, gr{0, 0, 0};
+  for (int cc = 0; cc < 3; cc++) {
+    const D3 l = B[cc] * sg;
+    const D3 aa = cross(r, l);
+    const double kk = comp(penv, cc);
+    const double wJ = dot(wl, l) + dot(wa, aa);
+    double kb;
+    D3 gAa;  // cotangent of a (the angular Jacobian row): F_c w_a from g, k (Hb + Hb^T) J from H
+    if (!floored) {  // Hb = -(w delta^T) symmetrised
+      const double dJ = dot(dL, l) + dot(dA, aa);
+      kb = -wJ * dJ;
+      gAa = wa * comp(e.F, cc) - (wa * dJ + dA * wJ) * kk;
+    } else {
+      const double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
+      double MJ[3] = {0.0, 0.0, 0.0};
+      kb = 0.0;
+      for (int i = 0; i < 6; i++)
+        for (int j = 0; j <= i; j++) {
+          const double hb = bv.Hb[6 * i + j];
+          kb += hb * J[i] * J[j];
+          if (i >= 3) MJ[i - 3] += hb * J[j];
+          if (j >= 3) MJ[j - 3] += hb * J[i];
+        }
+      gAa = wa * comp(e.F, cc) + D3{MJ[0], MJ[1], MJ[2]} * kk;
+    }
+    setComp(gF, cc, wJ);
+    setComp(gPen, cc, kb);
+    gr += cross(l, gAa);
+  }
+  D3 gC{0, 0, 0}, gLam{0, 0, 0};
+  double gFr = 0.0;
+  evalFVjp(e, lamv, penv, gF, gC, gLam, gPen, gFr);
+  D3 gXa{0, 0, 0}, gXb{0, 0, 0}, gXa0{0, 0, 0}, gXb0{0, 0, 0}, gC0{0, 0, 0};
+  D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
+  evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
+  // the lever arm r = R(q_own) r_local
+  if (isA) gQa += rotateVjpQ(qa, D.anchor[2 * k], gr);
+  else gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], gr);
+  const D3 oX = isA ? gXa : gXb, oX0 = isA ? gXa0 : gXb0;
+  const D4 oQ = isA ? gQa : gQb, oQ0 = isA ? gQa0 : gQb0;
+  const int other = isA ? b : a;
+  if (D.dynamic[other]) {
+    atomicAdd3(&D.gPos[other], isA ? gXb : gXa);
+    atomicAdd4(&D.gRot[other], isA ? gQb : gQa);
+    atomicAdd3(&D.gIpos[other], isA ? gXb0 : gXa0);
+    atomicAdd4(&D.gIrot[other], isA ? gQb0 : gQa0);
+  }
+  atomicAdd3(&D.gLam[wpt + lk], gLam);
+  atomicAdd3(&D.gPen[wpt + lk], gPen);
+  atomicAdd3(&D.gC0[wpt + lk], gC0);
+  if (gFr != 0.0 && fr > 0.0) {
+    double ma = mu(D, a), mb = mu(D, b);
+    if (D.dynamic[a]) atomicAdd(&D.gMu[a], gFr * mb / (2.0 * fr));
+    if (D.dynamic[b]) atomicAdd(&D.gMu[b], gFr * ma / (2.0 * fr));
+  }
+  out[0] = oX.x, out[1] = oX.y, out[2] = oX.z;
+  out[3] = oQ.x, out[4] = oQ.y, out[5] = oQ.z, out[6] = oQ.w;
+  out[7] = oX0.x, out[8] = oX0.y, out[9] = oX0.z;
+  out[10] = oQ0.x, out[11] = oQ0.y, out[12] = oQ0.z, out[13] = oQ0.w;
+}
+
+// The primal updates of colour c's bodies at positions g0..g1 at iteration it, reversed (poses read
+// from the snapshots the sweep read: partners of earlier colours at iteration it, the rest at
+// it - 1; the points' values after the dual of iteration it - 1). Thread tid < g1 - g0 owns body
+// position g0 + tid; the incidences are spread over all threads.
+__device__ void primalGroupVjp(const AdjDev& D, const StepView& v, int wpt, int it, int c, int g0, int g1) {
+  const int tid = threadIdx.x, nbg = g1 - g0;
   const double dt2 = D.dt * D.dt;
-  // the poses the update read: its own (iteration it - 1), partners of earlier colours (iteration it),
-  // of later colours (it - 1); the points' values after the dual of iteration it - 1
   const size_t prevSn = (size_t)it * D.nb, curSn = (size_t)(it + 1) * D.nb;
   const D3* lamIn = D.snLam + (size_t)it * D.W * D.maxPts;
   const D3* penIn = D.snPen + (size_t)it * D.W * D.maxPts;
   auto poseOf = [&](int b, D3& x, D4& q) {
-    if (!D.dynamic[b] || b == gb) {
-      x = D.snPos[prevSn + b];
-      q = D.snRot[prevSn + b];
-      return;
-    }
-    int cb = v.color[b - v.b0];
-    size_t o = cb < c ? curSn : prevSn;
+    const size_t o = D.dynamic[b] && v.color[b - v.b0] < c ? curSn : prevSn;
     x = D.snPos[o + b];
     q = D.snRot[o + b];
   };
-  // forward values
-  D3 x;
-  D4 q;
-  poseOf(gb, x, q);
-  const double m = mass(D, gb) / dt2;
-  const D3 Iu = D.unitMoment[gb];
-  const D3 I = Iu * (mass(D, gb) / dt2);
-  Sys6 S;
-  for (int i = 0; i < 6; i++)
-    for (int j = 0; j < 6; j++) S.A[i][j] = 0.0;
-  S.A[0][0] = S.A[1][1] = S.A[2][2] = m;
-  S.A[3][3] = I.x;
-  S.A[4][4] = I.y;
-  S.A[5][5] = I.z;
-  D3 gl = (x - D.ypos[gb]) * m;
-  D3 qd = qsub(q, D.yrot[gb]);
-  D3 ga = D3{I.x * qd.x, I.y * qd.y, I.z * qd.z};
-  const int t0 = s_incStart[lb], t1 = s_incStart[lb + 1];
-  for (int t = t0; t < t1; t++) {
-    int k = s_inc[t], lk = k - v.p0;
-    int2 ab = D.manAB[D.ptMan[k]];
-    int a = v.b0 + ab.x, b = v.b0 + ab.y;
-    D3 xa, xb;
-    D4 qa, qb;
-    poseOf(a, xa, qa);
-    poseOf(b, xb, qb);
-    PointEval e;
-    evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamIn[wpt + lk], penIn[wpt + lk],
-              sqrt(mu(D, a) * mu(D, b)), e);
-    bool isA = gb == a;
-    double sg = isA ? 1.0 : -1.0;
-    D3 r = isA ? e.rAW : e.rBW;
-    const D3* B = D.basis + 3 * D.ptMan[k];
-    for (int cc = 0; cc < 3; cc++) {
-      D3 l = B[cc] * sg;
-      D3 aa = cross(r, l);
-      double kk = comp(penIn[wpt + lk], cc);
-      double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
-      for (int i = 0; i < 6; i++)
-        for (int j = 0; j < 6; j++) S.A[i][j] += kk * J[i] * J[j];
-      gl += l * comp(e.F, cc);
-      ga += aa * comp(e.F, cc);
-    }
+  // the forward's systems and steps
+  double acc[ADJ_ROW];
+  groupRows(D, v, wpt, g0, g1, lamIn, penIn, poseOf, acc);
+  if (tid < nbg) {
+    const int gb = v.b0 + s_colBody[g0 + tid];
+    Sys6 S;
+    double rhs[6], delta[6];
+    bodySystem(D, gb, acc, poseOf, S, rhs);
+    LDLT6 F;
+    const int floored = factor6(S, F, PIVOT);
+    solve6(F, rhs, delta);
+    // the new pose's cotangent: x' = x - delta_lin, q' = qaddv(q, -delta_ang)
+    D3 x;
+    D4 q;
+    poseOf(gb, x, q);
+    const D3 gXn = D.gPos[gb];
+    const D4 gQn = D.gRot[gb];
+    D4 gQ{0, 0, 0, 0};
+    D3 gV{0, 0, 0};
+    qaddvVjp(q, D3{-delta[3], -delta[4], -delta[5]}, gQn, gQ, gV);
+    double gDelta[6] = {-gXn.x, -gXn.y, -gXn.z, -gV.x, -gV.y, -gV.z};
+    BodyVjp& bv = bodyVjp()[tid];
+    // the cotangent of g is w = H^-1 gDelta; that of H is -w delta^T symmetrised, or, through a
+    // floored pivot, Hb from the factorization's reverse
+    if (!floored) solve6(F, gDelta, bv.w);
+    else ldltVjpMasked(F, floored, PIVOT, rhs, delta, gDelta, bv.w, bv.Lb, bv.Hb);
+    for (int i = 0; i < 6; i++) bv.delta[i] = delta[i];
+    bv.floored = floored;
   }
-  LDLT6 F;
-  factor6(S, F, PIVOT);
-  double rhs[6] = {gl.x, gl.y, gl.z, ga.x, ga.y, ga.z}, delta[6];
-  solve6(F, rhs, delta);
-  D3 dA{delta[3], delta[4], delta[5]};
-  // the new pose's cotangent: x' = x - delta_lin, q' = qaddv(q, -delta_ang)
-  D3 gXn = D.gPos[gb];
-  D4 gQn = D.gRot[gb];
-  D3 gX = gXn;
-  D4 gQ{0, 0, 0, 0};
-  D3 gV{0, 0, 0};
-  qaddvVjp(q, -dA, gQn, gQ, gV);
-  double gDelta[6] = {-gXn.x, -gXn.y, -gXn.z, -gV.x, -gV.y, -gV.z};
-  // the cotangent of g is w (H^-1 gDelta), that of H's lower triangle Hb (-w delta^T symmetrised,
-  // but through a floored pivot only to its diagonal entry)
-  double wv[6], Hb[6][6];
-  ldltVjp(S, F, PIVOT, rhs, delta, gDelta, wv, Hb);
-  D3 wl{wv[0], wv[1], wv[2]}, wa{wv[3], wv[4], wv[5]};
-  // inertia
-  gX += wl * m;
-  D3 gY = wl * (-m);
-  D3 gqd{I.x * wa.x, I.y * wa.y, I.z * wa.z};
-  D4 gYq{0, 0, 0, 0};
-  qsubVjp(q, D.yrot[gb], gqd, gQ, gYq);
-  double gM = 0.0;
-  {
-    // H_lin = m/dt2 I, H_ang = diag(m Iu/dt2); g_lin = (x - y) m/dt2, g_ang = (m Iu/dt2) qd
-    D3 xy = x - D.ypos[gb];
-    double dH = Hb[0][0] + Hb[1][1] + Hb[2][2];
-    double dHa = Hb[3][3] * Iu.x + Hb[4][4] * Iu.y + Hb[5][5] * Iu.z;
-    gM += (dH + dot(wl, xy) + dHa + wa.x * Iu.x * qd.x + wa.y * Iu.y * qd.y + wa.z * Iu.z * qd.z) / dt2;
-  }
-  D3 gIpos{0, 0, 0};
-  D4 gIrot{0, 0, 0, 0};
-  for (int t = t0; t < t1; t++) {
-    int k = s_inc[t], lk = k - v.p0;
-    int2 ab = D.manAB[D.ptMan[k]];
-    int a = v.b0 + ab.x, b = v.b0 + ab.y;
-    D3 xa, xb;
-    D4 qa, qb;
-    poseOf(a, xa, qa);
-    poseOf(b, xb, qb);
-    double fr = sqrt(mu(D, a) * mu(D, b));
-    PointEval e;
-    D3 lamv = lamIn[wpt + lk], penv = penIn[wpt + lk];
-    evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamv, penv, fr, e);
-    bool isA = gb == a;
-    double sg = isA ? 1.0 : -1.0;
-    D3 r = isA ? e.rAW : e.rBW;
-    const D3* B = D.basis + 3 * D.ptMan[k];
-    D3 gF{0, 0, 0}, gPen{0, 0, 0}, gr{0, 0, 0};
-    for (int cc = 0; cc < 3; cc++) {
-      D3 l = B[cc] * sg;
-      D3 aa = cross(r, l);
-      double kk = comp(penv, cc);
-      const double J[6] = {l.x, l.y, l.z, aa.x, aa.y, aa.z};
-      double wJ = dot(wl, l) + dot(wa, aa);
-      // H += k J J^T: k's cotangent sums Hb J_i J_j over the lower triangle; J's is k (Hb + Hb^T) J
-      double kb = 0.0, MJ[3] = {0.0, 0.0, 0.0};
-      for (int i = 0; i < 6; i++)
-        for (int j = 0; j <= i; j++) {
-          kb += Hb[i][j] * J[i] * J[j];
-          if (i >= 3) MJ[i - 3] += Hb[i][j] * J[j];
-          if (j >= 3) MJ[j - 3] += Hb[i][j] * J[i];
-        }
-      setComp(gF, cc, wJ);
-      setComp(gPen, cc, kb);
-      // cotangent of a (the angular Jacobian row): F_c w_a from g, k (Hb + Hb^T) J from H
-      D3 gAa = wa * comp(e.F, cc) + D3{MJ[0], MJ[1], MJ[2]} * kk;
-      gr += cross(l, gAa);
+  __syncthreads();
+  // the incidences' cotangents; each body sums its own
+  double own[14];
+  for (int i = 0; i < 14; i++) own[i] = 0.0;
+  const int i0 = s_incStart[g0], i1 = s_incStart[g1];
+  for (int ch = i0; ch < i1; ch += blockDim.x) {
+    if (ch + tid < i1) incidenceVjp(D, v, wpt, s_inc[ch + tid], g0, lamIn, penIn, poseOf, rowOf(tid));
+    __syncthreads();
+    if (tid < nbg) {
+      const int p = g0 + tid;
+      const int u0 = max(s_incStart[p], ch), u1 = min(s_incStart[p + 1], ch + int(blockDim.x));
+      for (int u = u0; u < u1; u++)
+        for (int i = 0; i < 14; i++) own[i] += rowOf(u - ch)[i];
     }
-    D3 gC{0, 0, 0}, gLam{0, 0, 0};
-    double gFr = 0.0;
-    evalFVjp(e, lamv, penv, gF, gC, gLam, gPen, gFr);
-    D3 gXa{0, 0, 0}, gXb{0, 0, 0}, gXa0{0, 0, 0}, gXb0{0, 0, 0}, gC0{0, 0, 0};
-    D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
-    evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
-    // the lever arm r = R(q_own) r_local
-    if (isA) gQa += rotateVjpQ(qa, D.anchor[2 * k], gr);
-    else gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], gr);
-    // own terms stay local; the partner's go to its current cotangent
-    if (isA) {
-      gX += gXa;
-      gQ += gQa;
-      gIpos += gXa0;
-      gIrot += gQa0;
-      if (D.dynamic[b]) {
-        atomicAdd3(&D.gPos[b], gXb);
-        atomicAdd4(&D.gRot[b], gQb);
-        atomicAdd3(&D.gIpos[b], gXb0);
-        atomicAdd4(&D.gIrot[b], gQb0);
-      }
+    __syncthreads();
+  }
+  if (tid < nbg) {
+    const int gb = v.b0 + s_colBody[g0 + tid];
+    const BodyVjp& bv = bodyVjp()[tid];
+    D3 x;
+    D4 q;
+    poseOf(gb, x, q);
+    const double m = mass(D, gb) / dt2;
+    const D3 Iu = D.unitMoment[gb];
+    const D3 I = Iu * m;
+    const D3 gXn = D.gPos[gb];
+    const D4 gQn = D.gRot[gb];
+    D4 gQ{0, 0, 0, 0};
+    D3 gV{0, 0, 0};
+    qaddvVjp(q, D3{-bv.delta[3], -bv.delta[4], -bv.delta[5]}, gQn, gQ, gV);
+    const D3 wl{bv.w[0], bv.w[1], bv.w[2]}, wa{bv.w[3], bv.w[4], bv.w[5]};
+    // inertia: g_lin = (x - y) m, g_ang = I qsub(q, y_rot); H_lin = m, H_ang = I (m, I over dt^2)
+    const D3 gX = gXn + wl * m + D3{own[0], own[1], own[2]};
+    const D3 gY = wl * (-m);
+    const D3 gqd{I.x * wa.x, I.y * wa.y, I.z * wa.z};
+    D4 gYq{0, 0, 0, 0};
+    qsubVjp(q, D.yrot[gb], gqd, gQ, gYq);
+    const D3 xy = x - D.ypos[gb];
+    const D3 qd = qsub(q, D.yrot[gb]);
+    double dH, dHa;
+    if (!bv.floored) {
+      dH = -(bv.w[0] * bv.delta[0] + bv.w[1] * bv.delta[1] + bv.w[2] * bv.delta[2]);
+      dHa = -bv.w[3] * bv.delta[3] * Iu.x - bv.w[4] * bv.delta[4] * Iu.y - bv.w[5] * bv.delta[5] * Iu.z;
     } else {
-      gX += gXb;
-      gQ += gQb;
-      gIpos += gXb0;
-      gIrot += gQb0;
-      if (D.dynamic[a]) {
-        atomicAdd3(&D.gPos[a], gXa);
-        atomicAdd4(&D.gRot[a], gQa);
-        atomicAdd3(&D.gIpos[a], gXa0);
-        atomicAdd4(&D.gIrot[a], gQa0);
-      }
+      dH = bv.Hb[0] + bv.Hb[7] + bv.Hb[14];
+      dHa = bv.Hb[21] * Iu.x + bv.Hb[28] * Iu.y + bv.Hb[35] * Iu.z;
     }
-    atomicAdd3(&D.gLam[wpt + lk], gLam);
-    atomicAdd3(&D.gPen[wpt + lk], gPen);
-    atomicAdd3(&D.gC0[wpt + lk], gC0);
-    if (gFr != 0.0 && fr > 0.0) {
-      double ma = mu(D, a), mb = mu(D, b);
-      if (D.dynamic[a]) atomicAdd(&D.gMu[a], gFr * mb / (2.0 * fr));
-      if (D.dynamic[b]) atomicAdd(&D.gMu[b], gFr * ma / (2.0 * fr));
-    }
+    const double gM = (dH + dot(wl, xy) + dHa + wa.x * Iu.x * qd.x + wa.y * Iu.y * qd.y + wa.z * Iu.z * qd.z) / dt2;
+    D.gPos[gb] = gX;
+    D.gRot[gb] = gQ + D4{own[3], own[4], own[5], own[6]};
+    D.gYpos[gb] += gY;
+    D.gYrot[gb] += gYq;
+    D.gIpos[gb] += D3{own[7], own[8], own[9]};
+    D.gIrot[gb] += D4{own[10], own[11], own[12], own[13]};
+    D.gMass[gb] += gM;
   }
-  D.gPos[gb] = gX;
-  D.gRot[gb] = gQ;
-  D.gYpos[gb] += gY;
-  D.gYrot[gb] += gYq;
-  D.gIpos[gb] += gIpos;
-  D.gIrot[gb] += gIrot;
-  D.gMass[gb] += gM;
+  __syncthreads();
 }
 
 // Point k's dual at iteration it: lambda' = F, the penalty ramps
@@ -790,10 +889,8 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
   for (int it = D.I - 1; it >= 0; it--) {
     for (int lk = threadIdx.x; lk < np; lk += blockDim.x) dualVjp(D, v, wpt, it, v.p0 + lk);
     __syncthreads();
-    for (int c = v.ncol - 1; c >= 0; c--) {
-      if (threadIdx.x < v.nb && v.color[threadIdx.x] == c) primalVjp(D, v, wpt, it, v.b0 + threadIdx.x, threadIdx.x, c);
-      __syncthreads();
-    }
+    for (int c = v.ncol - 1; c >= 0; c--)  // the colour's bodies in groups (order within a colour is free)
+      for (int g0 = s_colStart[c]; g0 < s_colStart[c + 1]; g0 += ADJ_GROUP) primalGroupVjp(D, v, wpt, it, c, g0, min(g0 + ADJ_GROUP, s_colStart[c + 1]));
   }
   // points' warm starts and C(x-) (the start poses' cotangents gather in gIpos/gIrot)
   const int prevFirst = s > 0 ? D.ptFirst[(s - 1) * (D.W + 1) + w] : 0;
@@ -956,6 +1053,9 @@ bool aupload(avbd_adjoint* a, const T** dst, const T* src, size_t n) {
 // The replay's working buffers, checkpoints, snapshots and cotangents (D's sizes set)
 bool adjAllocWork(avbd_adjoint* a) {
   AdjDev& D = a->d;
+  if (cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ADJ_SMEM_FORWARD)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_adj_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ADJ_SMEM_BACKWARD)) != cudaSuccess)
+    return false;
   const size_t W = size_t(D.W), K = size_t(D.K), nb = size_t(D.nb);
   bool ok = true;
   const size_t WP = W * size_t(D.maxPts), segs = (K + D.ck - 1) / D.ck, I1 = size_t(D.I) + 1;
@@ -1275,7 +1375,7 @@ int avbd_adjoint_forward(avbd_adjoint* a, const double* params, double* loss, do
   cudaSetDevice(a->device);
   int r = adjParams(a, params);
   if (r) return r;
-  k_adj_forward<<<a->W, ADJ_THREADS>>>(a->d);
+  k_adj_forward<<<a->W, ADJ_THREADS, ADJ_SMEM_FORWARD>>>(a->d);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("replay launch: ") + cudaGetErrorString(e));
   e = cudaDeviceSynchronize();
@@ -1294,12 +1394,12 @@ int avbd_adjoint_backward(avbd_adjoint* a, const double* params, double* grad, d
   int r = adjParams(a, params);
   if (r) return r;
   if (!a->forwardDone) {  // the checkpoints come from a forward with these params
-    k_adj_forward<<<a->W, ADJ_THREADS>>>(a->d);
+    k_adj_forward<<<a->W, ADJ_THREADS, ADJ_SMEM_FORWARD>>>(a->d);
     cudaError_t e0 = cudaGetLastError();
     if (e0 != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("replay launch: ") + cudaGetErrorString(e0));
   }
   a->forwardDone = false;
-  k_adj_backward<<<a->W, ADJ_THREADS>>>(a->d);
+  k_adj_backward<<<a->W, ADJ_THREADS, ADJ_SMEM_BACKWARD>>>(a->d);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("reverse launch: ") + cudaGetErrorString(e));
   e = cudaDeviceSynchronize();

@@ -105,11 +105,16 @@ struct Sys6 {
 struct LDLT6 {
   double L[6][6], D[6];
 };
-__host__ __device__ inline void factor6(const Sys6& S, LDLT6& F, double floor) {
+// returns the mask of pivots the floor replaced
+__host__ __device__ inline int factor6(const Sys6& S, LDLT6& F, double floor) {
+  int floored = 0;
   for (int j = 0; j < 6; j++) {
     double d = S.A[j][j];
     for (int k = 0; k < j; k++) d -= F.L[j][k] * F.L[j][k] * F.D[k];
-    if (j > 0) d = fmax(d, S.A[j][j] * floor);
+    if (j > 0 && d < S.A[j][j] * floor) {
+      d = S.A[j][j] * floor;
+      floored |= 1 << j;
+    }
     F.D[j] = d;
     F.L[j][j] = 1.0;
     for (int i = j + 1; i < 6; i++) {
@@ -118,6 +123,7 @@ __host__ __device__ inline void factor6(const Sys6& S, LDLT6& F, double floor) {
       F.L[i][j] = s / d;
     }
   }
+  return floored;
 }
 __host__ __device__ inline void forwardSub6(const LDLT6& F, const double* b, double* y) {
   for (int i = 0; i < 6; i++) {
@@ -189,6 +195,57 @@ __host__ __device__ inline void ldltVjp(const Sys6& S, const LDLT6& F, double fl
       Ab[j][j] += db;
       for (int k = 0; k < j; k++) {
         Lb[j][k] -= db * 2.0 * F.L[j][k] * F.D[k];
+        Db[k] -= db * F.L[j][k] * F.L[j][k];
+      }
+    }
+  }
+}
+
+// ldltVjp with the floored pivots given by factor6's mask and its 6x6 work arrays (Lb, Hb: 36
+// doubles each, row-major) supplied by the caller, for instance in shared memory
+__host__ __device__ inline void ldltVjpMasked(const LDLT6& F, int floored, double floor, const double* b, const double* x, const double* xb, double* bb,
+                                              double* Lb, double* Hb) {
+  double y[6], yb[6], xbar[6], Db[6];
+  forwardSub6(F, b, y);
+  for (int i = 0; i < 6; i++) {
+    xbar[i] = xb[i];
+    Db[i] = 0.0;
+  }
+  for (int i = 0; i < 36; i++) Lb[i] = Hb[i] = 0.0;
+  for (int i = 0; i < 6; i++) {
+    yb[i] = xbar[i] / F.D[i];
+    Db[i] -= xbar[i] * y[i] / (F.D[i] * F.D[i]);
+    for (int k = i + 1; k < 6; k++) {
+      Lb[6 * k + i] -= xbar[i] * x[k];
+      xbar[k] -= xbar[i] * F.L[k][i];
+    }
+  }
+  for (int i = 5; i >= 0; i--) {
+    bb[i] = yb[i];
+    for (int k = 0; k < i; k++) {
+      Lb[6 * i + k] -= yb[i] * y[k];
+      yb[k] -= yb[i] * F.L[i][k];
+    }
+  }
+  for (int j = 5; j >= 0; j--) {
+    const double d = F.D[j];
+    for (int i = j + 1; i < 6; i++) {
+      double sb = Lb[6 * i + j] / d;
+      Db[j] -= Lb[6 * i + j] * F.L[i][j] / d;
+      Hb[6 * i + j] += sb;
+      for (int k = 0; k < j; k++) {
+        Lb[6 * i + k] -= sb * F.L[j][k] * F.D[k];
+        Lb[6 * j + k] -= sb * F.L[i][k] * F.D[k];
+        Db[k] -= sb * F.L[i][k] * F.L[j][k];
+      }
+    }
+    const double db = Db[j];
+    if (floored & (1 << j)) {
+      Hb[6 * j + j] += db * floor;
+    } else {
+      Hb[6 * j + j] += db;
+      for (int k = 0; k < j; k++) {
+        Lb[6 * j + k] -= db * 2.0 * F.L[j][k] * F.D[k];
         Db[k] -= db * F.L[j][k] * F.L[j][k];
       }
     }
