@@ -287,7 +287,7 @@ int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, const uint32_t*
  * from, and the colouring; everything else (C(x-), warm starts, inertial targets, the coloured
  * primal solves, duals with penalty ramps and friction cone, velocities) is differentiated. The
  * replay keeps a checkpoint every `checkpoint` steps and recomputes between them. A world holds at
- * most 128 bodies and 2048 points a step. */
+ * most 128 bodies and 1024 points a step. */
 typedef struct avbd_adjoint avbd_adjoint;
 typedef struct avbd_adjoint_desc {
   uint32_t worlds, steps, iterations, checkpoint; /* checkpoint 0: every 10 steps */

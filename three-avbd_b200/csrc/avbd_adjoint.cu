@@ -24,8 +24,16 @@ using namespace avbd::adj;
 namespace {
 
 constexpr int ADJ_THREADS = 128;     // bodies of a world at most
-constexpr int ADJ_MAX_POINTS = 2048;  // points of a world in one step at most
+constexpr int ADJ_MAX_POINTS = 1024;  // points of a world in one step at most
+constexpr int ADJ_BLOCKS_PER_SM = 4;  // worlds in flight per SM: registers capped at 128 a thread
 constexpr double PEN_MIN = 1.0, PEN_MAX = 1e10, PIVOT = 1e-5;
+
+// A body's primal solve at one iteration, kept by the segment recompute for the reverse sweep: its
+// factorization (L's lower triangle, D, 1/D), right-hand side, step and floored pivots
+struct FactRec {
+  double L[15], D[6], invD[6], rhs[6], delta[6];
+  int floored;
+};
 
 struct AdjDev {
   int W, K, I, ck;
@@ -53,6 +61,7 @@ struct AdjDev {
   // state (per body) and per-world point buffers
   D3 *pos, *vel, *ang, *ipos, *ypos;
   D4 *rot, *irot, *yrot;
+  QInv *irotI, *yrotI;  // the step-start and inertial rotations prepared for qsub
   double* pvz;
   D3 *lam, *pen, *lamP, *penP, *C0;  // world w's points at w * maxPts
   // checkpoints: every ck steps, the body state and the last step's points
@@ -68,6 +77,7 @@ struct AdjDev {
   D4* snRot;
   D3 *stIpos, *stYpos, *stC0;
   D4 *stIrot, *stYrot;
+  FactRec* snFact;  // I x bodies per step
   // cotangents
   D3 *gPos, *gVel, *gAng, *gIpos, *gYpos;
   D4 *gRot, *gIrot, *gYrot;
@@ -188,15 +198,15 @@ struct PointEval {
   double fs, bd, fr;
   bool clamped;
 };
-__device__ inline void evalPoint(const AdjDev& D, int k, D3 xa, D4 qa, D3 xa0, D4 qa0, D3 xb, D4 qb, D3 xb0, D4 qb0, D3 c0, D3 lam, D3 pen, double fr,
+__device__ inline void evalPoint(const AdjDev& D, int k, D3 xa, D4 qa, D3 xa0, const QInv& qa0, D3 xb, D4 qb, D3 xb0, const QInv& qb0, D3 c0, D3 lam, D3 pen, double fr,
                                  PointEval& e) {
   const D3* B = D.basis + 3 * D.ptMan[k];
   e.rAW = rotate(qa, D.anchor[2 * k]);
   e.rBW = rotate(qb, D.anchor[2 * k + 1]);
   e.dAL = xa - xa0;
-  e.dAA = qsub(qa, qa0);
+  e.dAA = qsubI(qa, qa0);
   e.dBL = xb - xb0;
-  e.dBA = qsub(qb, qb0);
+  e.dBA = qsubI(qb, qb0);
   for (int c = 0; c < 3; c++) {
     D3 bk = B[c];
     double v = comp(c0, c) * (1.0 - D.alpha);
@@ -242,7 +252,7 @@ __device__ inline void evalFVjp(const PointEval& e, D3 lam, D3 pen, D3 gF, D3& g
 }
 
 // The cotangents of the poses, step-start poses and C0 from the cotangent of C
-__device__ inline void evalCVjp(const AdjDev& D, int k, D4 qa, D4 qa0, D4 qb, D4 qb0, const PointEval& e, D3 gC, D3& gXa, D4& gQa, D3& gXa0, D4& gQa0,
+__device__ inline void evalCVjp(const AdjDev& D, int k, D4 qa, D4 qa0, const QInv& ia0, D4 qb, D4 qb0, const QInv& ib0, const PointEval& e, D3 gC, D3& gXa, D4& gQa, D3& gXa0, D4& gQa0,
                                 D3& gXb, D4& gQb, D3& gXb0, D4& gQb0, D3& gC0) {
   const D3* B = D.basis + 3 * D.ptMan[k];
   D3 gdAL{0, 0, 0}, gdAA{0, 0, 0}, gdBL{0, 0, 0}, gdBA{0, 0, 0}, grA{0, 0, 0}, grB{0, 0, 0};
@@ -261,8 +271,8 @@ __device__ inline void evalCVjp(const AdjDev& D, int k, D4 qa, D4 qa0, D4 qb, D4
   gXa0 -= gdAL;
   gXb += gdBL;
   gXb0 -= gdBL;
-  qsubVjp(qa, qa0, gdAA, gQa, gQa0);
-  qsubVjp(qb, qb0, gdBA, gQb, gQb0);
+  qsubVjpI(qa, qa0, ia0, gdAA, gQa, gQa0);
+  qsubVjpI(qb, qb0, ib0, gdBA, gQb, gQb0);
   gQa += rotateVjpQ(qa, D.anchor[2 * k], grA);
   gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], grB);
 }
@@ -281,7 +291,7 @@ __device__ inline void incidenceRows(const AdjDev& D, const StepView& v, int wpt
   poseOf(a, xa, qa);
   poseOf(b, xb, qb);
   PointEval e;
-  evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamCur[wpt + lk], penCur[wpt + lk],
+  evalPoint(D, k, xa, qa, D.ipos[a], D.irotI[a], xb, qb, D.ipos[b], D.irotI[b], D.C0[wpt + lk], lamCur[wpt + lk], penCur[wpt + lk],
             sqrt(mu(D, a) * mu(D, b)), e);
   const double sg = gb == a ? 1.0 : -1.0;
   const D3 rr = gb == a ? e.rAW : e.rBW;
@@ -342,7 +352,7 @@ __device__ inline void bodySystem(const AdjDev& D, int gb, const double* acc, Po
   S.A[3][3] += I.x;
   S.A[4][4] += I.y;
   S.A[5][5] += I.z;
-  const D3 gl = (x - D.ypos[gb]) * m, qd = qsub(q, D.yrot[gb]);
+  const D3 gl = (x - D.ypos[gb]) * m, qd = qsubI(q, D.yrotI[gb]);
   g[0] += gl.x;
   g[1] += gl.y;
   g[2] += gl.z;
@@ -388,6 +398,7 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
     int gb = v.b0 + threadIdx.x;
     D.ipos[gb] = D.pos[gb];
     D.irot[gb] = D.rot[gb];
+    D.irotI[gb] = qinv(D.rot[gb]);
     if (D.dynamic[gb]) {
       D3 x = D.pos[gb], u = D.vel[gb];
       D4 q = D.rot[gb];
@@ -396,6 +407,7 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
       D.ypos[gb] = y;
       D4 qt = qaddv(q, D.ang[gb] * dt);
       D.yrot[gb] = qt;
+      D.yrotI[gb] = qinv(qt);
       double sgn = D.g < 0 ? -1.0 : (D.g > 0 ? 1.0 : 0.0);
       double accelExt = (u.z - D.pvz[gb]) / dt * sgn;
       double wgt = fmin(fmax(accelExt / fabs(D.g), 0.0), 1.0);
@@ -436,10 +448,23 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
           double rhs[6], dx[6];
           bodySystem(D, gb, acc, livePose, S, rhs);
           LDLT6 F;
-          factor6(S, F, PIVOT);
+          const int floored = factor6(S, F, PIVOT);
           solve6(F, rhs, dx);
           D.pos[gb] = D.pos[gb] - D3{dx[0], dx[1], dx[2]};
           D.rot[gb] = qaddv(D.rot[gb], D3{-dx[3], -dx[4], -dx[5]});
+          if (snapshots) {
+            FactRec& fr = D.snFact[(size_t(slot) * D.I + it) * D.nb + gb];
+            int o = 0;
+            for (int i = 1; i < 6; i++)
+              for (int j = 0; j < i; j++) fr.L[o++] = F.L[i][j];
+            for (int i = 0; i < 6; i++) {
+              fr.D[i] = F.D[i];
+              fr.invD[i] = F.invD[i];
+              fr.rhs[i] = rhs[i];
+              fr.delta[i] = dx[i];
+            }
+            fr.floored = floored;
+          }
         }
         __syncthreads();
       }
@@ -450,7 +475,7 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
       int2 ab = D.manAB[D.ptMan[k]];
       int a = v.b0 + ab.x, b = v.b0 + ab.y;
       PointEval e;
-      evalPoint(D, k, D.pos[a], D.rot[a], D.ipos[a], D.irot[a], D.pos[b], D.rot[b], D.ipos[b], D.irot[b], D.C0[wpt + lk], D.lam[wpt + lk], D.pen[wpt + lk],
+      evalPoint(D, k, D.pos[a], D.rot[a], D.ipos[a], D.irotI[a], D.pos[b], D.rot[b], D.ipos[b], D.irotI[b], D.C0[wpt + lk], D.lam[wpt + lk], D.pen[wpt + lk],
                 sqrt(mu(D, a) * mu(D, b)), e);
       D3 pen = D.pen[wpt + lk];
       if (e.F.x < 0.0) pen.x = fmin(pen.x + D.beta * fabs(e.C.x), PEN_MAX);
@@ -577,7 +602,7 @@ __device__ void worldLoss(const AdjDev& D, int w) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_forward(AdjDev D) {
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_BLOCKS_PER_SM) k_adj_forward(AdjDev D) {
   const int w = blockIdx.x;
   loadInitial(D, w);
   for (int s = 0; s < D.K; s++) {
@@ -610,7 +635,7 @@ __device__ inline void incidenceVjp(const AdjDev& D, const StepView& v, int wpt,
   const double fr = sqrt(mu(D, a) * mu(D, b));
   PointEval e;
   const D3 lamv = lamIn[wpt + lk], penv = penIn[wpt + lk];
-  evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamv, penv, fr, e);
+  evalPoint(D, k, xa, qa, D.ipos[a], D.irotI[a], xb, qb, D.ipos[b], D.irotI[b], D.C0[wpt + lk], lamv, penv, fr, e);
   const bool isA = gb == a;
   const double sg = isA ? 1.0 : -1.0;
   const D3 r = isA ? e.rAW : e.rBW;
@@ -649,7 +674,7 @@ __device__ inline void incidenceVjp(const AdjDev& D, const StepView& v, int wpt,
   evalFVjp(e, lamv, penv, gF, gC, gLam, gPen, gFr);
   D3 gXa{0, 0, 0}, gXb{0, 0, 0}, gXa0{0, 0, 0}, gXb0{0, 0, 0}, gC0{0, 0, 0};
   D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
-  evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
+  evalCVjp(D, k, qa, D.irot[a], D.irotI[a], qb, D.irot[b], D.irotI[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
   // the lever arm r = R(q_own) r_local
   if (isA) gQa += rotateVjpQ(qa, D.anchor[2 * k], gr);
   else gQb += rotateVjpQ(qb, D.anchor[2 * k + 1], gr);
@@ -691,17 +716,22 @@ __device__ void primalGroupVjp(const AdjDev& D, const StepView& v, int wpt, int 
     x = D.snPos[o + b];
     q = D.snRot[o + b];
   };
-  // the forward's systems and steps
-  double acc[ADJ_ROW];
-  groupRows(D, v, wpt, g0, g1, lamIn, penIn, poseOf, acc);
   if (tid < nbg) {
     const int gb = v.b0 + s_colBody[g0 + tid];
-    Sys6 S;
-    double rhs[6], delta[6];
-    bodySystem(D, gb, acc, poseOf, S, rhs);
+    // the forward's factorization and step, as the segment recompute kept them
+    const FactRec& fr = D.snFact[size_t(it) * D.nb + gb];
     LDLT6 F;
-    const int floored = factor6(S, F, PIVOT);
-    solve6(F, rhs, delta);
+    double rhs[6], delta[6];
+    int o = 0;
+    for (int i = 0; i < 6; i++) {
+      for (int j = 0; j < i; j++) F.L[i][j] = fr.L[o++];
+      F.L[i][i] = 1.0;
+      F.D[i] = fr.D[i];
+      F.invD[i] = fr.invD[i];
+      rhs[i] = fr.rhs[i];
+      delta[i] = fr.delta[i];
+    }
+    const int floored = fr.floored;
     // the new pose's cotangent: x' = x - delta_lin, q' = qaddv(q, -delta_ang)
     D3 x;
     D4 q;
@@ -756,9 +786,9 @@ __device__ void primalGroupVjp(const AdjDev& D, const StepView& v, int wpt, int 
     const D3 gY = wl * (-m);
     const D3 gqd{I.x * wa.x, I.y * wa.y, I.z * wa.z};
     D4 gYq{0, 0, 0, 0};
-    qsubVjp(q, D.yrot[gb], gqd, gQ, gYq);
+    qsubVjpI(q, D.yrot[gb], D.yrotI[gb], gqd, gQ, gYq);
     const D3 xy = x - D.ypos[gb];
-    const D3 qd = qsub(q, D.yrot[gb]);
+    const D3 qd = qsubI(q, D.yrotI[gb]);
     double dH, dHa;
     if (!bv.floored) {
       dH = -(bv.w[0] * bv.delta[0] + bv.w[1] * bv.delta[1] + bv.w[2] * bv.delta[2]);
@@ -792,7 +822,7 @@ __device__ void dualVjp(const AdjDev& D, const StepView& v, int wpt, int it, int
   double fr = sqrt(mu(D, a) * mu(D, b));
   D3 lamv = lamIn[wpt + lk], penv = penIn[wpt + lk];
   PointEval e;
-  evalPoint(D, k, xa, qa, D.ipos[a], D.irot[a], xb, qb, D.ipos[b], D.irot[b], D.C0[wpt + lk], lamv, penv, fr, e);
+  evalPoint(D, k, xa, qa, D.ipos[a], D.irotI[a], xb, qb, D.ipos[b], D.irotI[b], D.C0[wpt + lk], lamv, penv, fr, e);
   D3 gLamOut = D.gLam[wpt + lk], gPenOut = D.gPen[wpt + lk];
   D3 gPen{0, 0, 0}, gC{0, 0, 0}, gLam{0, 0, 0};
   // pen' = min(pen + beta |C|, MAX) where the ramp applies, else pen
@@ -815,7 +845,7 @@ __device__ void dualVjp(const AdjDev& D, const StepView& v, int wpt, int it, int
   evalFVjp(e, lamv, penv, gLamOut, gC, gLam, gPen, gFr);
   D3 gXa{0, 0, 0}, gXb{0, 0, 0}, gXa0{0, 0, 0}, gXb0{0, 0, 0}, gC0{0, 0, 0};
   D4 gQa{0, 0, 0, 0}, gQb{0, 0, 0, 0}, gQa0{0, 0, 0, 0}, gQb0{0, 0, 0, 0};
-  evalCVjp(D, k, qa, D.irot[a], qb, D.irot[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
+  evalCVjp(D, k, qa, D.irot[a], D.irotI[a], qb, D.irot[b], D.irotI[b], e, gC, gXa, gQa, gXa0, gQa0, gXb, gQb, gXb0, gQb0, gC0);
   if (D.dynamic[a]) {
     atomicAdd3(&D.gPos[a], gXa);
     atomicAdd4(&D.gRot[a], gQa);
@@ -854,10 +884,16 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
   D.snRot = D0.snRot + slot * (D0.I + 1) * D0.nb;
   D.snLam = D0.snLam + slot * (D0.I + 1) * D0.W * D0.maxPts;
   D.snPen = D0.snPen + slot * (D0.I + 1) * D0.W * D0.maxPts;
+  D.snFact = D0.snFact + slot * D0.I * D0.nb;
   const StepView v = viewOf(D, s, w);
   const int wpt = w * D.maxPts;
   const int np = v.p1 - v.p0;
   const double dt = D.dt;
+  if (threadIdx.x < v.nb) {  // the stored step's rotations prepared for qsub
+    const int gb = v.b0 + threadIdx.x;
+    D.irotI[gb] = qinv(D.irot[gb]);
+    if (D.dynamic[gb]) D.yrotI[gb] = qinv(D.yrot[gb]);
+  }
   buildIncidence(D, v);
   // velocities: v' = (x - x0)/dt, w' = qsub(q, q0)/dt, prevVz' = v_old.z
   if (threadIdx.x < v.nb) {
@@ -961,7 +997,7 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_backward(const AdjDev D) {
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_BLOCKS_PER_SM) k_adj_backward(const AdjDev D) {
   const int w = blockIdx.x;
   const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
   const int wpt = w * D.maxPts;
@@ -1053,8 +1089,11 @@ bool aupload(avbd_adjoint* a, const T** dst, const T* src, size_t n) {
 // The replay's working buffers, checkpoints, snapshots and cotangents (D's sizes set)
 bool adjAllocWork(avbd_adjoint* a) {
   AdjDev& D = a->d;
+  // shared memory sized for the blocks of several worlds on one SM
   if (cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ADJ_SMEM_FORWARD)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_adj_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ADJ_SMEM_BACKWARD)) != cudaSuccess)
+      cudaFuncSetAttribute(k_adj_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ADJ_SMEM_BACKWARD)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_adj_forward, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
+      cudaFuncSetAttribute(k_adj_backward, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
     return false;
   const size_t W = size_t(D.W), K = size_t(D.K), nb = size_t(D.nb);
   bool ok = true;
@@ -1066,6 +1105,7 @@ bool adjAllocWork(avbd_adjoint* a) {
   D.target = tgt;
   for (D3** p : {&D.pos, &D.vel, &D.ang, &D.ipos, &D.ypos, &D.gPos, &D.gVel, &D.gAng, &D.gIpos, &D.gYpos}) ok = ok && aalloc(a, p, nb);
   for (D4** p : {&D.rot, &D.irot, &D.yrot, &D.gRot, &D.gIrot, &D.gYrot}) ok = ok && aalloc(a, p, nb);
+  ok = ok && aalloc(a, &D.irotI, nb) && aalloc(a, &D.yrotI, nb);
   for (double** p : {&D.pvz, &D.gPvz, &D.gMass, &D.gMu}) ok = ok && aalloc(a, p, nb);
   for (D3** p : {&D.lam, &D.pen, &D.lamP, &D.penP, &D.C0, &D.gLam, &D.gPen, &D.gLamP, &D.gPenP, &D.gC0}) ok = ok && aalloc(a, p, WP);
   ok = ok && aalloc(a, &D.ckPos, segs * nb) && aalloc(a, &D.ckVel, segs * nb) && aalloc(a, &D.ckAng, segs * nb) && aalloc(a, &D.ckRot, segs * nb) &&
@@ -1075,6 +1115,7 @@ bool adjAllocWork(avbd_adjoint* a) {
        aalloc(a, &D.sgPen, size_t(D.ck) * WP);
   const size_t CK = size_t(D.ck);
   ok = ok && aalloc(a, &D.snPos, CK * I1 * nb) && aalloc(a, &D.snRot, CK * I1 * nb) && aalloc(a, &D.snLam, CK * I1 * WP) && aalloc(a, &D.snPen, CK * I1 * WP);
+  ok = ok && aalloc(a, &D.snFact, CK * size_t(std::max(D.I, 1)) * nb);
   ok = ok && aalloc(a, &D.stIpos, CK * nb) && aalloc(a, &D.stIrot, CK * nb) && aalloc(a, &D.stYpos, CK * nb) && aalloc(a, &D.stYrot, CK * nb) &&
        aalloc(a, &D.stC0, CK * WP);
   double* loss = nullptr;

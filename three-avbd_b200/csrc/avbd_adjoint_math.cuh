@@ -77,12 +77,33 @@ __host__ __device__ inline void qsubVjp(D4 a, D4 b, D3 g, D4& ga, D4& gb) {
   double dl = -(dot4(ib, conj(b))) / (l * l);
   gb += cb + b * (2.0 * dl);
 }
+// A rotation prepared for qsub against it: conj(b) / |b|^2 and 1 / |b|^2 (one division)
+struct QInv {
+  D4 inv;
+  double il;
+};
+__host__ __device__ inline QInv qinv(D4 b) {
+  const double il = 1.0 / ((b.x * b.x + b.y * b.y + b.z * b.z) + b.w * b.w);
+  return {D4{-b.x * il, -b.y * il, -b.z * il, b.w * il}, il};
+}
+__host__ __device__ inline D3 qsubI(D4 a, const QInv& bi) {
+  D4 s = qmul(a, bi.inv);
+  return {s.x * 2.0, s.y * 2.0, s.z * 2.0};
+}
+__host__ __device__ inline void qsubVjpI(D4 a, D4 b, const QInv& bi, D3 g, D4& ga, D4& gb) {
+  D4 sb{2.0 * g.x, 2.0 * g.y, 2.0 * g.z, 0.0};
+  ga += qmul(sb, conj(bi.inv));
+  D4 ib = qmul(conj(a), sb);
+  D4 cb = conj(ib) * bi.il;
+  double dl = -(dot4(ib, conj(b))) * (bi.il * bi.il);
+  gb += cb + b * (2.0 * dl);
+}
 // qaddv (ref/math.ts:109-113): normalize(a + (v, 0) a / 2)
 __host__ __device__ inline D4 qaddv(D4 a, D3 v) {
   D4 s = qmul(D4{v.x, v.y, v.z, 0.0}, a);
   D4 q{a.x + s.x * 0.5, a.y + s.y * 0.5, a.z + s.z * 0.5, a.w + s.w * 0.5};
-  double l = sqrt((q.x * q.x + q.y * q.y + q.z * q.z) + q.w * q.w);
-  return {q.x / l, q.y / l, q.z / l, q.w / l};
+  double il = 1.0 / sqrt((q.x * q.x + q.y * q.y + q.z * q.z) + q.w * q.w);
+  return {q.x * il, q.y * il, q.z * il, q.w * il};
 }
 __host__ __device__ inline void qaddvVjp(D4 a, D3 v, D4 g, D4& ga, D3& gv) {
   D4 V{v.x, v.y, v.z, 0.0};
@@ -103,7 +124,7 @@ struct Sys6 {
   double A[6][6];
 };
 struct LDLT6 {
-  double L[6][6], D[6];
+  double L[6][6], D[6], invD[6];
 };
 // returns the mask of pivots the floor replaced
 __host__ __device__ inline int factor6(const Sys6& S, LDLT6& F, double floor) {
@@ -116,11 +137,12 @@ __host__ __device__ inline int factor6(const Sys6& S, LDLT6& F, double floor) {
       floored |= 1 << j;
     }
     F.D[j] = d;
+    F.invD[j] = 1.0 / d;
     F.L[j][j] = 1.0;
     for (int i = j + 1; i < 6; i++) {
       double s = S.A[i][j];
       for (int k = 0; k < j; k++) s -= F.L[i][k] * F.L[j][k] * F.D[k];
-      F.L[i][j] = s / d;
+      F.L[i][j] = s * F.invD[j];
     }
   }
   return floored;
@@ -136,7 +158,7 @@ __host__ __device__ inline void solve6(const LDLT6& F, const double* b, double* 
   double y[6];
   forwardSub6(F, b, y);
   for (int i = 5; i >= 0; i--) {
-    double s = y[i] / F.D[i];
+    double s = y[i] * F.invD[i];
     for (int k = i + 1; k < 6; k++) s -= F.L[k][i] * x[k];
     x[i] = s;
   }
@@ -213,8 +235,8 @@ __host__ __device__ inline void ldltVjpMasked(const LDLT6& F, int floored, doubl
   }
   for (int i = 0; i < 36; i++) Lb[i] = Hb[i] = 0.0;
   for (int i = 0; i < 6; i++) {
-    yb[i] = xbar[i] / F.D[i];
-    Db[i] -= xbar[i] * y[i] / (F.D[i] * F.D[i]);
+    yb[i] = xbar[i] * F.invD[i];
+    Db[i] -= xbar[i] * y[i] * (F.invD[i] * F.invD[i]);
     for (int k = i + 1; k < 6; k++) {
       Lb[6 * k + i] -= xbar[i] * x[k];
       xbar[k] -= xbar[i] * F.L[k][i];
@@ -228,10 +250,10 @@ __host__ __device__ inline void ldltVjpMasked(const LDLT6& F, int floored, doubl
     }
   }
   for (int j = 5; j >= 0; j--) {
-    const double d = F.D[j];
+    const double id = F.invD[j];
     for (int i = j + 1; i < 6; i++) {
-      double sb = Lb[6 * i + j] / d;
-      Db[j] -= Lb[6 * i + j] * F.L[i][j] / d;
+      double sb = Lb[6 * i + j] * id;
+      Db[j] -= Lb[6 * i + j] * F.L[i][j] * id;
       Hb[6 * i + j] += sb;
       for (int k = 0; k < j; k++) {
         Lb[6 * i + k] -= sb * F.L[j][k] * F.D[k];
