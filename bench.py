@@ -296,6 +296,131 @@ def run_hulls(args, local: int, rank: int, world_size: int, barrier, torch, dist
     }
 
 
+def run_adjoint(args, local: int, rank: int, world_size: int, barrier, torch, dist) -> dict:
+    """Config 5: gradients of a final-pose loss over 1024 worlds of 64 tumbling boxes, 120 steps, 10
+    iterations, through the FP64 adjoint (checkpoint every 10 steps) of the recorded FP32 batched
+    rollout; the target comes from a seeded FP32 rollout with perturbed parameters. Reported: the FP32
+    forward (plain and recording), the adjoint's FP64 replay and reverse sweep, their ratios, and
+    central differences (h = 1e-6) of the replay along a random direction on 32 sampled worlds."""
+    import numpy as np
+    import avbd_b200
+    from avbd_b200.scenes import tumbling_world
+
+    W, NB, K = args.adjoint_worlds, 64, args.adjoint_steps
+    seed = 500 + rank
+    scenes = [tumbling_world(np.random.default_rng(seed * 100003 + w), NB) for w in range(W)]
+    n = sum(len(s.bodies) for s in scenes)
+    b = avbd_b200.BatchSolver3D(W, n, params=scenes[0].params, device=local)
+    for s in scenes:
+        b.add_scene(s)
+    nominal = np.zeros(n, avbd_b200.BODY_DTYPE)
+    b.read_all_bodies_into(nominal)
+    nominal['flags'] = 1.0  # written again: no contact history
+    dyn = nominal['mass'] > 0
+    stream = torch.cuda.ExternalStream(b.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def batch_ms(record: bool) -> float:
+        b.write_all_bodies_async(nominal)
+        b.synchronize()
+        if record:
+            b.record_start(K)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            b.step(K)
+            e1.record(stream)
+        b.synchronize()
+        return e0.elapsed_time(e1)
+
+    # the target: the FP32 rollout with perturbed parameters
+    rng = np.random.default_rng(seed)
+    pert = nominal.copy()
+    pert['vel'][dyn] += rng.normal(0, 0.2, (int(dyn.sum()), 3)).astype(np.float32)
+    pert['ang_vel'][dyn] += rng.normal(0, 0.5, (int(dyn.sum()), 3)).astype(np.float32)
+    scale = rng.uniform(0.9, 1.1, int(dyn.sum())).astype(np.float32)
+    pert['mass'][dyn] *= scale
+    pert['moment'][dyn] *= scale[:, None]
+    pert['friction'][dyn] *= rng.uniform(0.9, 1.1, int(dyn.sum())).astype(np.float32)
+    b.write_all_bodies_async(pert)
+    b.synchronize()
+    b.step(K)
+    b.synchronize()
+    final = np.zeros(n, avbd_b200.BODY_DTYPE)
+    b.read_all_bodies_into(final)
+    target = np.concatenate([final['pos'], final['rot']], axis=1).astype(np.float64).reshape(-1)
+    batch_ms(False)  # warm-up (graphs)
+    fwd_plain = batch_ms(False)
+    fwd_rec = batch_ms(True)
+    rec = b.record_status()
+    adj = avbd_b200.Adjoint.from_batch(b, checkpoint=10)
+    info = adj.info()
+    adj.set_target(target)
+    p0 = adj.nominal()
+    adj.forward(p0)  # warm-up
+    adj.backward(p0)
+    dev = torch.cuda.current_stream(local)
+    barrier()
+    e0.record(dev)
+    loss, _ = adj.forward(p0)
+    e1.record(dev)
+    torch.cuda.synchronize(local)
+    replay = e0.elapsed_time(e1)
+    e0.record(dev)
+    loss_b, grad = adj.backward(p0)
+    e1.record(dev)
+    torch.cuda.synchronize(local)
+    backward = e0.elapsed_time(e1)
+    barrier()
+    ms = torch.tensor([fwd_rec, replay, backward], dtype=torch.float64, device=f'cuda:{local}')
+    if world_size > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    fwd_rec, replay, backward = (float(x) for x in ms.tolist())
+    # central differences of the replay along a random direction, 32 sampled worlds
+    fb = adj.first_body.astype(np.int64)
+    d = rng.normal(0, 1, p0.shape)
+    d[6::8] *= 0.1
+    d[7::8] *= 0.05
+    d[np.repeat(~dyn, 8)] = 0.0
+    # (a world whose loss has a kink within the step along d, a contact switching between sticking and
+    # sliding or between touching and separating, shows as central differences at h and 2h that
+    # disagree; such worlds are counted apart)
+    h = 1e-6
+    fd = {}
+    for hh in (h, 2 * h):
+        lp, _ = adj.forward(p0 + hh * d)
+        lm, _ = adj.forward(p0 - hh * d)
+        fd[hh] = (lp - lm) / (2 * hh)
+    sample = rng.choice(W, size=min(32, W), replace=False)
+    rel, rel_all, kinks = [], [], 0
+    for w in sample:
+        a0, a1 = 8 * fb[w], 8 * fb[w + 1]
+        an = float(grad[a0:a1] @ d[a0:a1])
+        err = abs(fd[h][w] - an) / max(abs(an), 1e-12)
+        rel_all.append(err)
+        if abs(fd[h][w] - fd[2 * h][w]) > 1e-3 * max(abs(fd[h][w]), 1e-12):
+            kinks += 1
+        else:
+            rel.append(err)
+    adj.destroy()
+    b.destroy()
+    return {
+        'metric': 'adjoint/forward time ratio', 'value': (replay + backward) / fwd_rec, 'unit': 'x', 'higher_is_better': False,
+        'forward_fp32_ms': fwd_plain, 'forward_fp32_recording_ms': fwd_rec, 'replay_fp64_ms': replay, 'reverse_fp64_ms': backward,
+        'ratio_reverse_to_forward': backward / fwd_rec, 'ratio_replay_plus_reverse_to_forward': (replay + backward) / fwd_rec,
+        'loss_mean': float(np.mean(loss_b)), 'gradient_finite': bool(np.isfinite(grad).all()),
+        'fd_check': {'worlds': len(sample), 'h': h, 'direction': 'random per world (v0, omega0 unit scale; mass 0.1; friction 0.05)',
+                     'smooth_worlds': len(rel), 'max_rel_err_smooth': float(max(rel)) if rel else None,
+                     'median_rel_err': float(np.median(rel_all)), 'max_rel_err_all': float(max(rel_all)),
+                     'worlds_with_kink_within_2h': kinks},
+        'recording': {'manifolds': rec['manifolds'], 'points': rec['points'], 'max_points_per_world_step': info['max_points']},
+        'config': {'workload': f'{W} worlds x {NB} boxes (0.8 m, density 1, friction 0.5) tumbling onto a static ground; dt 1/60, '
+                               f'10 iterations, {K} steps; FP32 forward, FP64 adjoint with a checkpoint every 10 steps; gradients of the '
+                               'squared final-pose distance to a target w.r.t. v0, omega0, mass and friction of every body',
+                   'seed': seed, 'target': 'FP32 rollout with v0 + N(0,0.2), omega0 + N(0,0.5), mass and friction x U(0.9,1.1)',
+                   'timing': 'CUDA events on the launching stream; the replay and reverse read GBs of snapshots (inputs larger than L2)'},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -314,6 +439,8 @@ def main():
     ap.add_argument('--hull-steps', type=int, default=120, help='timed steps of the hulls-and-chains workload (0: skip it)')
     ap.add_argument('--hulls', type=int, default=20000)
     ap.add_argument('--chains', type=int, default=1000)
+    ap.add_argument('--adjoint-worlds', type=int, default=1024, help='worlds of the differentiated batch (0: skip it)')
+    ap.add_argument('--adjoint-steps', type=int, default=120)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -437,6 +564,10 @@ def main():
     if args.batched_worlds > 0:
         batched = run_batched(args, local, rank, world_size, barrier, torch, dist)
 
+    adjoint = None
+    if args.adjoint_worlds > 0:
+        adjoint = run_adjoint(args, local, rank, world_size, barrier, torch, dist)
+
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         ref = cpu_reference(SAMPLE_BODIES, ROLLOUT, os.cpu_count() or 1)
@@ -460,6 +591,7 @@ def main():
             'cpu_baseline': cpu,
             'batched': batched,
             'hulls': hulls,
+            'adjoint': adjoint,
             'device': name[0] if name else None,
         }
         print(json.dumps(line), flush=True)
