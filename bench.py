@@ -157,13 +157,14 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, dist) -> dict:
+def run_batched(args, R, torch) -> dict:
     """world-steps/s of the batched workload, batched launch against per-world launches."""
     import numpy as np
     import avbd_b200
     from avbd_b200.scenes import batched_worlds
 
-    scenes = batched_worlds(args.batched_worlds, seed=3 + rank)
+    local, barrier = R.local, R.barrier
+    scenes = batched_worlds(args.batched_worlds, seed=R.seed(3))
     n = sum(len(s.bodies) for s in scenes)
     dyn = sum(s.dynamic_count for s in scenes)
     b = avbd_b200.BatchSolver3D(len(scenes), n, 1, params=scenes[0].params, device=local)
@@ -185,10 +186,7 @@ def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, di
         e1.record(stream)
     b.synchronize()
     barrier()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms, = R.max([e0.elapsed_time(e1)])
     errors = sum(1 for i in range(len(scenes)) if b.read_counters(i)['error'])
     info = b.info()
 
@@ -206,9 +204,7 @@ def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, di
         e1.record(stream)
     b.synchronize()
     barrier()
-    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
-    if world_size > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    te, = R.max([e0.elapsed_time(e1)])
     b.destroy()
 
     # per-world launches: a sample of the same worlds, each stepped through the single-world API
@@ -228,15 +224,15 @@ def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, di
     plain_s = time.perf_counter() - t0
     for w in worlds:
         w.destroy()
-    value = world_size * len(scenes) * steps / (ms / 1000.0)
+    value = R.rate(len(scenes) * steps, ms)
     plain = len(sample) * plain_steps / plain_s
     return {
         'metric': 'world-steps/s', 'value': value, 'ms_per_step': ms / steps, 'steps': steps,
-        'body_steps_per_s': world_size * dyn * steps / (ms / 1000.0),
+        'body_steps_per_s': R.rate(dyn * steps, ms),
         'per_world_launch': {'value': plain, 'unit': 'world-steps/s', 'sample_worlds': len(sample), 'steps': plain_steps,
                              'how': 'each sampled world stepped through the single-world entry points in turn, wall clock'},
-        'speedup_vs_per_world_launch': value / world_size / plain,
-        'e2e': {'value': world_size * len(scenes) * steps / (float(te.item()) / 1000.0), 'unit': 'world-steps/s',
+        'speedup_vs_per_world_launch': value / R.world_size / plain,
+        'e2e': {'value': R.rate(len(scenes) * steps, te), 'unit': 'world-steps/s',
                 'h2d_bytes_per_step': n * 160, 'd2h_bytes_per_step': n * 160},
         'worlds': len(scenes), 'bodies': n, 'dynamic_bodies': dyn, 'world_errors': errors,
         'launch': {'collide_threads': info['collide_threads'], 'collide_blocks': info['collide_blocks'], 'solve_blocks': info['solve_blocks'],
@@ -247,16 +243,17 @@ def run_batched(args, local: int, rank: int, world_size: int, barrier, torch, di
                                'half stacks of unit cubes, half piles of unit cubes and r 0.5 spheres, each on its own ground box; '
                                f'dt 1/60, 10 iterations; timed steps {args.warmup + 1 + tuning["steps_taken"]}..'
                                f'{args.warmup + tuning["steps_taken"] + steps} after tuning and warm-up',
-                   'seed': 3 + rank, 'l2': '256 MiB memset between timed steps, inside the timed region'},
+                   'seed': R.seed(3), 'l2': '256 MiB memset between timed steps, inside the timed region'},
     }
 
 
-def run_hulls(args, local: int, rank: int, world_size: int, barrier, torch, dist) -> dict:
+def run_hulls(args, R, torch) -> dict:
     """Config 3: 20k convex hulls falling onto 1000 jointed chains of 50 boxes, 15 iterations."""
     import avbd_b200
     from avbd_b200.scenes import hulls_and_chains
 
-    scene = hulls_and_chains(args.hulls, args.chains, 50, seed=9 + rank)
+    local, barrier = R.local, R.barrier
+    scene = hulls_and_chains(args.hulls, args.chains, 50, seed=R.seed(9))
     w = avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
     w.step(args.warmup)
     w.synchronize()
@@ -274,10 +271,7 @@ def run_hulls(args, local: int, rank: int, world_size: int, barrier, torch, dist
         e1.record(stream)
     w.synchronize()
     barrier()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms, = R.max([e0.elapsed_time(e1)])
     st = w.read_step_stats()
     c = w.read_counters()
     joints, _ = w.read_joints()
@@ -285,18 +279,18 @@ def run_hulls(args, local: int, rank: int, world_size: int, barrier, torch, dist
     dyn = scene.dynamic_count
     w.destroy()
     return {
-        'metric': 'body-steps/s', 'value': world_size * dyn * steps / (ms / 1000.0), 'ms_per_step': ms / steps, 'steps': steps,
+        'metric': 'body-steps/s', 'value': R.rate(dyn * steps, ms), 'ms_per_step': ms / steps, 'steps': steps,
         'dynamic_bodies': dyn, 'hull_records': len(scene.hull_offsets), 'joints': len(joints), 'joints_broken': broken,
         'phases_ms_per_step': {'collision': float(st['collision_ms'].mean()), 'topology_solve': float(st['solve_ms'].mean())},
         'last_step': {k: int(st[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors')}, 'error': c['error'], 'overflow': c['overflow'],
         'config': {'workload': f'{args.hulls} hulls (hull of 8-32 points on an ellipsoid, semi-axes U[0.3,1.0]; 512 distinct shapes) falling '
                                f'onto {args.chains} chains of 50 boxes (0.2x0.2x0.5) with ball joints breaking at 1e4 N on pull, hung from static '
                                f'anchors; static ground; dt 1/60, 15 iterations; timed steps {args.warmup + 1}..{args.warmup + steps}',
-                   'seed': 9 + rank, 'l2': '256 MiB memset between timed steps, inside the timed region'},
+                   'seed': R.seed(9), 'l2': '256 MiB memset between timed steps, inside the timed region'},
     }
 
 
-def run_adjoint(args, local: int, rank: int, world_size: int, barrier, torch, dist) -> dict:
+def run_adjoint(args, R, torch) -> dict:
     """Config 5: gradients of a final-pose loss over 1024 worlds of 64 tumbling boxes, 120 steps, 10
     iterations, through the FP64 adjoint (checkpoint every 10 steps) of the recorded FP32 batched
     rollout; the target comes from a seeded FP32 rollout with perturbed parameters. Reported: the FP32
@@ -307,7 +301,8 @@ def run_adjoint(args, local: int, rank: int, world_size: int, barrier, torch, di
     from avbd_b200.scenes import tumbling_world
 
     W, NB, K = args.adjoint_worlds, 64, args.adjoint_steps
-    seed = 500 + rank
+    local, barrier = R.local, R.barrier
+    seed = R.seed(500)
     scenes = [tumbling_world(np.random.default_rng(seed * 100003 + w), NB) for w in range(W)]
     n = sum(len(s.bodies) for s in scenes)
     b = avbd_b200.BatchSolver3D(W, n, params=scenes[0].params, device=local)
@@ -371,10 +366,7 @@ def run_adjoint(args, local: int, rank: int, world_size: int, barrier, torch, di
     torch.cuda.synchronize(local)
     backward = e0.elapsed_time(e1)
     barrier()
-    ms = torch.tensor([fwd_rec, replay, backward], dtype=torch.float64, device=f'cuda:{local}')
-    if world_size > 1:
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    fwd_rec, replay, backward = (float(x) for x in ms.tolist())
+    fwd_rec, replay, backward = R.max([fwd_rec, replay, backward])
     # central differences of the replay along a random direction, 32 sampled worlds
     fb = adj.first_body.astype(np.int64)
     d = rng.normal(0, 1, p0.shape)
@@ -444,29 +436,18 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    rank = int(os.environ.get('RANK', '0'))
-    world_size = int(os.environ.get('WORLD_SIZE', '1'))
-    local = int(os.environ.get('LOCAL_RANK', '0'))
-
     if args.impl == 'reference':
-        run_reference(args, rank)
+        run_reference(args, int(os.environ.get('RANK', '0')))
         return
 
     import numpy as np
     import torch
-    import torch.distributed as dist
     import avbd_b200
+    from avbd_b200.replicas import Ranks
     from avbd_b200.scenes import drop_pile
 
-    torch.cuda.set_device(local)
-    if world_size > 1:
-        from datetime import timedelta
-        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
-
-    def barrier():
-        if world_size > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
+    R = Ranks.from_env('nccl', timeout_s=300)
+    rank, world_size, local, barrier = R.rank, R.world_size, R.local, R.barrier
 
     scene = drop_pile(args.bodies, seed=1, spacing=args.spacing)
     n_dyn = scene.dynamic_count
@@ -506,11 +487,8 @@ def main():
         print(f'warning: counters {counters}', file=sys.stderr)
     w.destroy()
 
-    t = torch.tensor([ms], dtype=torch.float64, device=f'cuda:{local}')
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world_size * n_dyn * args.steps / (ms_max / 1000.0)
+    ms_max, = R.max([ms])
+    value = R.rate(n_dyn * args.steps, ms_max)
 
     # Roofline of the dominant kernel (the cooperative topology+solve launch), over the timed steps
     solve_ms = float(stats['solve_ms'].sum())
@@ -548,25 +526,23 @@ def main():
             e1.record(s2)
         w2.synchronize()
         barrier()
-        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f'cuda:{local}')
-        if world_size > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te, = R.max([e0.elapsed_time(e1)])
         nbytes = w2.body_count * 160
-        e2e = {'value': world_size * n_dyn * args.steps / (float(te.item()) / 1000.0), 'unit': UNIT, 'h2d_bytes_per_step': nbytes,
+        e2e = {'value': R.rate(n_dyn * args.steps, te), 'unit': UNIT, 'h2d_bytes_per_step': nbytes,
                'd2h_bytes_per_step': nbytes}
         w2.destroy()
 
     hulls = None
     if args.hull_steps > 0:
-        hulls = run_hulls(args, local, rank, world_size, barrier, torch, dist)
+        hulls = run_hulls(args, R, torch)
 
     batched = None
     if args.batched_worlds > 0:
-        batched = run_batched(args, local, rank, world_size, barrier, torch, dist)
+        batched = run_batched(args, R, torch)
 
     adjoint = None
     if args.adjoint_worlds > 0:
-        adjoint = run_adjoint(args, local, rank, world_size, barrier, torch, dist)
+        adjoint = run_adjoint(args, R, torch)
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -595,8 +571,7 @@ def main():
             'device': name[0] if name else None,
         }
         print(json.dumps(line), flush=True)
-    if world_size > 1:
-        dist.destroy_process_group()
+    R.close()
 
 
 if __name__ == '__main__':
