@@ -175,6 +175,16 @@ int avbd_release_joints(avbd_world* world, const uint32_t* slots, uint32_t n);
 int avbd_add_ignore_pairs(avbd_world* world, const uint32_t* pairs_ab, uint32_t n);
 /* setFilters (gpu/solver.ts): groups_mask[2i] = groups, [2i+1] = collides-with mask. */
 int avbd_set_filters(avbd_world* world, uint32_t first, const uint32_t* groups_mask, uint32_t n);
+/* setBodyAux(indices, scales, linear?, angular?) (gpu/solver.ts:1814-1845; record layout.ts:33-46):
+ * per-slot gravity scale (default 1) and linear / angular damping rates in 1/s (default 0; a
+ * dynamic body's incoming velocities decay by exp(-rate dt) once per step, before its inertial
+ * target). linear and angular: both NULL (only the scales change) or both given. */
+int avbd_set_body_aux(avbd_world* world, const uint32_t* indices, uint32_t n, const float* scales, const float* linear, const float* angular);
+/* The aux records of slots first .. first + n - 1: 4 floats each (scale, linear, angular, 0). */
+int avbd_read_body_aux(avbd_world* world, uint32_t first, float* aux4, uint32_t n);
+/* setLifecycle(index, bits) (gpu/solver.ts:2069-2076): bits 2 disabled (the body takes no part),
+ * 4 cold (its joints start the next step without warm start); the slot loses its contact history. */
+int avbd_set_lifecycle(avbd_world* world, uint32_t index, uint32_t bits);
 
 /* Convex hulls (src/avbd3d/hull.ts, gpu/wgsl-hull.ts). A hull record is the reference's packed
  * layout (gpu/solver.ts:313-338 packHull with its header at vec4 0), 4 words per vec4:

@@ -265,6 +265,9 @@ template <class T> struct Body {
   int shape = SHAPE_BOX;
   uint32_t groups = 0xffffffffu, mask = 0xffffffffu;
   uint32_t color = NO_COLOR;  // GPU-mode colour state (colour | PENDING)
+  // GPU-mode body aux record (gpu/layout.ts:33-46): gravity scale, damping rates (1/s)
+  T gravityScale = 1, linDamp = 0, angDamp = 0;
+  uint32_t lifecycle = 0;  // GPU-mode lifecycle bits (layout.ts:17-19): 4 cold
   std::vector<Force<T>*> forces;
 };
 
@@ -1052,6 +1055,15 @@ template <class T> struct Joint : Force<T> {
     Solver<T>& s = *this->solver;
     C0Lin = evaluateLin();
     C0Ang = evaluateAng();
+    const bool cold = (this->bodyA >= 0 && (s.bodies[this->bodyA].lifecycle & 4u)) || (s.bodies[this->bodyB].lifecycle & 4u);
+    if (cold) {  // a cold body's joints start afresh (wgsl-solve.ts:247-253)
+      for (int i = 0; i < 3; i++) {
+        lambdaLin[i] = lambdaAng[i] = T(0);
+        penaltyLin[i] = tmin(T(PENALTY_MIN), stiffnessLin);
+        penaltyAng[i] = tmin(T(PENALTY_MIN), stiffnessAng);
+      }
+      return !broken;
+    }
     for (int i = 0; i < 3; i++) {
       lambdaLin[i] = lambdaLin[i] * s.alpha * s.gamma;
       lambdaAng[i] = lambdaAng[i] * s.alpha * s.gamma;
@@ -1505,12 +1517,19 @@ template <class T> struct Solver {
     for (int b = n - 1; b >= 0; b--) {
       Body<T>& body = bodies[b];
       bool dynamic = body.mass > 0;
+      // GPU mode: the body's aux record (wgsl-solve.ts:9-20, 297-305) and lifecycle bits consumed
+      const T g = gpu ? gravity * body.gravityScale : gravity;
+      if (gpu) body.lifecycle = 0;
+      if (gpu && dynamic && (body.linDamp > 0 || body.angDamp > 0)) {
+        body.vel = scale3(body.vel, T(std::exp(-double(body.linDamp) * double(dt))));
+        body.angVel = scale3(body.angVel, T(std::exp(-double(body.angDamp) * double(dt))));
+      }
       body.inertialPos = addScaled3(body.pos, body.vel, dt);
-      if (dynamic) body.inertialPos[2] += gravity * (dt * dt);
+      if (dynamic) body.inertialPos[2] += g * (dt * dt);
       body.inertialRot = qaddv(body.rot, scale3(body.angVel, dt));
       V3<T> accel = div3(sub3(body.vel, body.prevVel), dt);
-      T accelExt = accel[2] * signv(gravity);
-      T accelWeight = clampv(accelExt / std::fabs(gravity), T(0), T(1));
+      T accelExt = accel[2] * signv(g);
+      T accelWeight = clampv(accelExt / std::fabs(g), T(0), T(1));
       if (!std::isfinite(accelWeight)) accelWeight = 0;
       bool atRest = false;
       if (gpu && (flags & FLAG_START_AT_REST)) atRest = length(body.vel) + length(body.angVel) * body.radius < T(REST_SPEED);
@@ -1518,7 +1537,7 @@ template <class T> struct Solver {
       body.initRot = body.rot;
       if (dynamic && !atRest) {
         body.pos = addScaled3(body.pos, body.vel, dt);
-        body.pos[2] += gravity * (accelWeight * dt * dt);
+        body.pos[2] += g * (accelWeight * dt * dt);
         body.rot = qaddv(body.rot, scale3(body.angVel, dt));
       }
       if (gpu && !dynamic && (body.vel != V3<T>{0, 0, 0} || body.angVel != V3<T>{0, 0, 0})) {
@@ -2471,6 +2490,22 @@ double orc_adj_param(void* a, int which) {  // 0 dt 1 gravity 2 alpha 3 gamma 4 
   auto* P = static_cast<AdjProblem*>(a);
   double v[7] = {P->dt, P->gravity, P->alpha, P->gamma, P->betaLin, P->margin, double(P->iterations)};
   return v[which];
+}
+
+// GPU-mode body aux (gravity scale, damping rates) and lifecycle bits of body i
+void orc_set_body_aux(void* h, int i, double scale, double lin, double ang) {
+  with(h, [&](auto& s) {
+    s.bodies[i].gravityScale = scale;
+    s.bodies[i].linDamp = lin;
+    s.bodies[i].angDamp = ang;
+    return 0;
+  });
+}
+void orc_set_lifecycle(void* h, int i, unsigned bits) {
+  with(h, [&](auto& s) {
+    s.bodies[i].lifecycle = bits;
+    return 0;
+  });
 }
 
 // The hull buffer (gpu/solver.ts:313-338 layout, absolute offsets) the bodies' shape codes name

@@ -61,6 +61,8 @@ def lib():
         L.orc_hash32.argtypes = [U]
         L.orc_hash32.restype = U
         L.orc_set_hulls.argtypes = [P, ctypes.POINTER(U), I]
+        L.orc_set_body_aux.argtypes = [P, I, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_set_lifecycle.argtypes = [P, I, U]
         L.orc_adj_record.argtypes = [P, I]
         L.orc_adj_record.restype = P
         L.orc_adj_destroy.argtypes = [P]
@@ -130,6 +132,14 @@ class Oracle:
     def set_params(self, p, flags: int = 0):
         arr = np.array([p.dt, p.gravity, p.iterations, p.alpha, p.beta_lin, p.beta_ang, p.gamma, p.contact_margin], dtype=np.float64)
         self.L.orc_set_params(self.h, _dp(arr), flags)
+
+    def set_body_aux(self, i: int, scale: float, linear: float = 0.0, angular: float = 0.0):
+        """GPU-mode aux record of body i: gravity scale and damping rates (1/s)."""
+        self.L.orc_set_body_aux(self.h, i, scale, linear, angular)
+
+    def set_lifecycle(self, i: int, bits: int):
+        """GPU-mode lifecycle bits of body i (4: cold, its joints start the next step afresh)."""
+        self.L.orc_set_lifecycle(self.h, i, bits)
 
     def set_hulls(self, words):
         """The hull buffer the bodies' shape codes name (gpu/solver.ts:313-338 layout)."""

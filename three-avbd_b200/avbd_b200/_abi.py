@@ -157,6 +157,9 @@ SIGNATURES = {
     'avbd_adjoint_set_target': ([P, ctypes.POINTER(ctypes.c_double)], I),
     'avbd_adjoint_forward': ([P] + [ctypes.POINTER(ctypes.c_double)] * 3, I),
     'avbd_adjoint_backward': ([P] + [ctypes.POINTER(ctypes.c_double)] * 3, I),
+    'avbd_set_body_aux': ([P, VP, U, VP, VP, VP], I),
+    'avbd_read_body_aux': ([P, U, VP, U], I),
+    'avbd_set_lifecycle': ([P, U, U], I),
     'avbd_adjoint_create_from_batch': ([P, ctypes.c_uint32, ctypes.POINTER(P)], I),
     'avbd_adjoint_nominal': ([P, ctypes.POINTER(ctypes.c_double)], I),
     'avbd_adjoint_read_recording': ([P] + [VP] * 10, I),

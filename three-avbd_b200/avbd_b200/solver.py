@@ -265,6 +265,25 @@ class CudaSolver3D:
         g = np.ascontiguousarray(groups_mask, dtype=np.uint32).reshape(-1, 2)
         self._check(self.lib.avbd_set_filters(self.handle, first, uptr(g), len(g)))
 
+    def set_body_aux(self, indices, scales, linear=None, angular=None):
+        """setBodyAux: per-slot gravity scale and (both or neither) linear / angular damping rates."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint32)
+        sc = np.ascontiguousarray(scales, dtype=np.float32)
+        lin = None if linear is None else np.ascontiguousarray(linear, dtype=np.float32)
+        ang = None if angular is None else np.ascontiguousarray(angular, dtype=np.float32)
+        p = lambda a: a.ctypes.data if a is not None else None
+        self._check(self.lib.avbd_set_body_aux(self.handle, p(idx), len(idx), p(sc), p(lin), p(ang)))
+
+    def read_body_aux(self, first: int = 0, n: int | None = None) -> np.ndarray:
+        n = self.body_count - first if n is None else n
+        out = np.zeros((n, 4), np.float32)
+        self._check(self.lib.avbd_read_body_aux(self.handle, first, out.ctypes.data, n))
+        return out
+
+    def set_lifecycle(self, index: int, bits: int):
+        """setLifecycle: 2 disabled, 4 cold (joints start afresh); the slot loses its contact history."""
+        self._check(self.lib.avbd_set_lifecycle(self.handle, index, bits))
+
     def seed_contacts(self, manifolds: np.ndarray, contacts: np.ndarray):
         m = np.ascontiguousarray(manifolds, dtype=MANIFOLD_DTYPE)
         c = np.ascontiguousarray(contacts, dtype=CONTACT_DTYPE)

@@ -32,6 +32,7 @@ struct avbd_batch {
   std::vector<WorldDesc> worlds;
   std::vector<uint32_t> statics;  // every world's no-collide triples
   DWorld d{};
+  float4* staging = nullptr;  // body records for host transfers (10 float4 a body, capacity)
   WorldDesc* dWorlds = nullptr;
   uint32_t *dOrder = nullptr, *dQueue = nullptr, *dStatus = nullptr;
   uint32_t staticsAlloc = 0;
@@ -328,16 +329,19 @@ int appendWorld(avbd_batch* b, uint32_t n, uint32_t nj, uint32_t pairCap, double
 }
 
 void bodiesIn(avbd_batch* b, uint32_t first, const avbd_body* src, uint32_t n, cudaMemcpyKind kind) {
+  if (kind == cudaMemcpyHostToDevice && b->staging) {  // one contiguous transfer, then a scatter
+    cudaMemcpyAsync(b->staging, src, size_t(n) * sizeof(avbd_body), cudaMemcpyHostToDevice, b->stream);
+    unpackBodies(b->d, b->staging, first, n, b->stream);
+    return;
+  }
   float4* fields[10] = {b->d.pos, b->d.rot, b->d.ipos, b->d.irot, b->d.size, b->d.moment, b->d.ypos, b->d.yrot, b->d.vel, b->d.avel};
   for (int f = 0; f < 10; f++)
     cudaMemcpy2DAsync(fields[f] + first, sizeof(float4), reinterpret_cast<const char*>(src) + f * sizeof(float4), sizeof(avbd_body), sizeof(float4), n, kind,
                       b->stream);
 }
 void bodiesOut(avbd_batch* b, uint32_t first, avbd_body* dst, uint32_t n) {
-  float4* fields[10] = {b->d.pos, b->d.rot, b->d.ipos, b->d.irot, b->d.size, b->d.moment, b->d.ypos, b->d.yrot, b->d.vel, b->d.avel};
-  for (int f = 0; f < 10; f++)
-    cudaMemcpy2DAsync(reinterpret_cast<char*>(dst) + f * sizeof(float4), sizeof(avbd_body), fields[f] + first, sizeof(float4), sizeof(float4), n,
-                      cudaMemcpyDeviceToHost, b->stream);
+  packBodies(b->d, b->staging, first, n, b->stream);  // a gather into records, then one contiguous transfer
+  cudaMemcpyAsync(dst, b->staging, size_t(n) * sizeof(avbd_body), cudaMemcpyDeviceToHost, b->stream);
 }
 
 void freeRecording(avbd_batch* b) {
@@ -462,6 +466,7 @@ int avbd_batch_create(const avbd_batch_config* cfg, avbd_batch** out) {
   auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
   for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel, &d.dlin, &d.dang, &d.aabb}) A(balloc(b, f, B));
   A(balloc(b, &d.filters, B));
+  A(balloc(b, &b->staging, size_t(B) * 10));
   A(balloc(b, &d.cell, B));
   A(balloc(b, &d.colorA, B));
   A(balloc(b, &d.colorB, B));

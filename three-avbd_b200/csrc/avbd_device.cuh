@@ -73,6 +73,7 @@ struct StepParams {
 struct DWorld {
   // bodies (SoA, capacity bodyCap)
   float4 *pos, *rot, *ipos, *irot, *size, *moment, *ypos, *yrot, *vel, *avel;
+  float4* aux;  // per body: gravity scale, linear and angular damping rates (1/s), 0; null: 1, 0, 0, 0
   uint2* filters;
   uint4* hulls;  // hull records (wgsl-hull.ts layout), or null when the world has none
   uint32_t* hullPairs;  // pair slots whose narrowphase runs one warp per pair (hull against hull or box)
@@ -131,6 +132,7 @@ __host__ __device__ inline DWorld worldView(const DWorld& b, const WorldDesc& d,
   float4** bodyArrays[] = {&v.pos, &v.rot, &v.ipos, &v.irot, &v.size, &v.moment, &v.ypos, &v.yrot, &v.vel, &v.avel, &v.dlin, &v.dang, &v.aabb};
   for (float4** a : bodyArrays) *a += d.body;
   v.filters += d.body;
+  if (v.aux) v.aux += d.body;
   v.cell += d.body;
   v.joint += size_t(d.joint) * JOINT_VEC4;
   v.jinfo += d.joint;

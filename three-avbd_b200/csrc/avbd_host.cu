@@ -256,16 +256,19 @@ int adaptCapacity(avbd_world* w, bool wait) {
 }
 
 void copyBodiesIn(avbd_world* w, uint32_t first, const avbd_body* b, uint32_t n, cudaMemcpyKind kind) {
+  if (kind == cudaMemcpyHostToDevice && w->staging) {  // one contiguous transfer, then a scatter
+    cudaMemcpyAsync(w->staging, b, size_t(n) * sizeof(avbd_body), cudaMemcpyHostToDevice, w->stream);
+    unpackBodies(w->d, w->staging, first, n, w->stream);
+    return;
+  }
   float4* fields[10] = {w->d.pos, w->d.rot, w->d.ipos, w->d.irot, w->d.size, w->d.moment, w->d.ypos, w->d.yrot, w->d.vel, w->d.avel};
   for (int f = 0; f < 10; f++)
     cudaMemcpy2DAsync(fields[f] + first, sizeof(float4), reinterpret_cast<const char*>(b) + f * sizeof(float4), sizeof(avbd_body), sizeof(float4), n, kind,
                       w->stream);
 }
 void copyBodiesOut(avbd_world* w, avbd_body* b, uint32_t n) {
-  float4* fields[10] = {w->d.pos, w->d.rot, w->d.ipos, w->d.irot, w->d.size, w->d.moment, w->d.ypos, w->d.yrot, w->d.vel, w->d.avel};
-  for (int f = 0; f < 10; f++)
-    cudaMemcpy2DAsync(reinterpret_cast<char*>(b) + f * sizeof(float4), sizeof(avbd_body), fields[f], sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToHost,
-                      w->stream);
+  packBodies(w->d, w->staging, 0, n, w->stream);  // a gather into records, then one contiguous transfer
+  cudaMemcpyAsync(b, w->staging, size_t(n) * sizeof(avbd_body), cudaMemcpyDeviceToHost, w->stream);
 }
 
 bool finite(float x) { return std::isfinite(x); }
@@ -273,6 +276,39 @@ bool finite(float x) { return std::isfinite(x); }
 }  // namespace
 
 namespace avbd {
+
+// Body records between the device's field arrays and a contiguous staging array of records, so that
+// a host copy is one contiguous transfer (a strided 2D copy moves one 16-byte field per row)
+__device__ inline float4* bodyField(const DWorld& d, uint32_t f) {
+  switch (f) {
+    case 0: return d.pos;
+    case 1: return d.rot;
+    case 2: return d.ipos;
+    case 3: return d.irot;
+    case 4: return d.size;
+    case 5: return d.moment;
+    case 6: return d.ypos;
+    case 7: return d.yrot;
+    case 8: return d.vel;
+    default: return d.avel;
+  }
+}
+static_assert(sizeof(avbd_body) == 10 * sizeof(float4), "a body record is its ten device fields in order");
+__global__ void k_pack_bodies(DWorld d, float4* out, uint32_t first, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 10u * n) out[i] = bodyField(d, i % 10u)[first + i / 10u];
+}
+__global__ void k_unpack_bodies(DWorld d, const float4* in, uint32_t first, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 10u * n) bodyField(d, i % 10u)[first + i / 10u] = in[i];
+}
+void packBodies(const DWorld& d, float4* staging, uint32_t first, uint32_t n, cudaStream_t s) {
+  if (n) k_pack_bodies<<<grid_for(10u * n, 256), 256, 0, s>>>(d, staging, first, n);
+}
+void unpackBodies(const DWorld& d, const float4* staging, uint32_t first, uint32_t n, cudaStream_t s) {
+  if (n) k_unpack_bodies<<<grid_for(10u * n, 256), 256, 0, s>>>(d, staging, first, n);
+}
+
 
 // uploadStatics (solver.ts:1263-1318): large bodies, cell size, sorted no-collide triples
 int uploadStatics(avbd_world* w) {
@@ -384,6 +420,12 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   bool ok = true;
   auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
   for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel}) A(dalloc(w, f, B));
+  A(dalloc(w, &w->staging, size_t(B) * 10));
+  A(dalloc(w, &d.aux, B));
+  if (ok) {  // every slot at the default aux record: gravity scale 1, no damping
+    std::vector<float4> aux(B, make_float4(1.0f, 0.0f, 0.0f, 0.0f));
+    A(cudaMemcpy(d.aux, aux.data(), size_t(B) * sizeof(float4), cudaMemcpyHostToDevice));
+  }
   A(dalloc(w, &d.filters, B));
   A(dalloc(w, &d.keyA, B));
   A(dalloc(w, &d.keyB, B));
@@ -638,6 +680,53 @@ int avbd_set_filters(avbd_world* w, uint32_t first, const uint32_t* gm, uint32_t
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   CUDA_TRY(w, cudaMemcpy(w->d.filters + first, gm, size_t(n) * sizeof(uint2), cudaMemcpyHostToDevice));
+  return AVBD_OK;
+}
+
+int avbd_set_body_aux(avbd_world* w, const uint32_t* indices, uint32_t n, const float* scales, const float* linear, const float* angular) {
+  if (!w || (n && (!indices || !scales))) return AVBD_ERR_INVALID;
+  if ((linear == nullptr) != (angular == nullptr)) return fail(w, AVBD_ERR_INVALID, "pass both damping rate arrays or neither");
+  for (uint32_t k = 0; k < n; k++) {
+    if (indices[k] >= w->bodyCap) return fail(w, AVBD_ERR_INVALID, "slot " + std::to_string(indices[k]) + " is outside the body capacity");
+    if (!std::isfinite(scales[k])) return fail(w, AVBD_ERR_INVALID, "scales must be finite");
+    if (linear && !(std::isfinite(linear[k]) && linear[k] >= 0.0f && std::isfinite(angular[k]) && angular[k] >= 0.0f))
+      return fail(w, AVBD_ERR_INVALID, "damping rates must be finite and at least 0");
+  }
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  for (uint32_t k = 0; k < n; k++) {
+    // without rates only the gravity scale changes (setBodyAux writes the one word)
+    float4 rec;
+    if (linear) {
+      rec = make_float4(scales[k], linear[k], angular[k], 0.0f);
+    } else {
+      CUDA_TRY(w, cudaMemcpy(&rec, w->d.aux + indices[k], sizeof(float4), cudaMemcpyDeviceToHost));
+      rec.x = scales[k];
+    }
+    CUDA_TRY(w, cudaMemcpy(w->d.aux + indices[k], &rec, sizeof(float4), cudaMemcpyHostToDevice));
+  }
+  return AVBD_OK;
+}
+
+int avbd_read_body_aux(avbd_world* w, uint32_t first, float* aux4, uint32_t n) {
+  if (!w || (n && !aux4) || uint64_t(first) + n > w->bodyCap) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  CUDA_TRY(w, cudaMemcpy(aux4, w->d.aux + first, size_t(n) * sizeof(float4), cudaMemcpyDeviceToHost));
+  return AVBD_OK;
+}
+
+int avbd_set_lifecycle(avbd_world* w, uint32_t index, uint32_t bits) {
+  if (!w || index >= w->n || (bits & ~6u)) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  // the lifecycle word is the initial pose's w (layout.ts:17-19); a rewritten slot has no contact history
+  float4 ip;
+  CUDA_TRY(w, cudaMemcpy(&ip, w->d.ipos + index, sizeof(float4), cudaMemcpyDeviceToHost));
+  ip.w = float(1u | bits);
+  CUDA_TRY(w, cudaMemcpy(w->d.ipos + index, &ip, sizeof(float4), cudaMemcpyHostToDevice));
+  const uint32_t none = NO_COLOR;
+  CUDA_TRY(w, cudaMemcpy(w->d.colorA + index, &none, sizeof(uint32_t), cudaMemcpyHostToDevice));
   return AVBD_OK;
 }
 

@@ -18,6 +18,10 @@ double largeThreshold(const std::vector<double>& radii);
 std::string bodyProblem(const avbd_body* b, uint32_t n);
 std::string jointProblem(const avbd_joint* j, const avbd_joint_info* info, uint32_t n, uint32_t bodies);
 
+// Body records between the field arrays and a staging array of records (10 float4 a body), on `s`
+void packBodies(const DWorld& d, float4* staging, uint32_t first, uint32_t n, cudaStream_t s);
+void unpackBodies(const DWorld& d, const float4* staging, uint32_t first, uint32_t n, cudaStream_t s);
+
 struct NoCollide {
   uint32_t hi, lo, slot;
   bool operator<(const NoCollide& o) const { return hi < o.hi || (hi == o.hi && lo < o.lo); }
@@ -36,6 +40,7 @@ struct avbd_world {
   uint32_t bodyCap = 0, n = 0, jointCap = 0, nj = 0, pairCap = 0, tableSize = 0, hashSize = 0, incCap = 0, adjCap = 0;
   uint32_t sortTiles = 0;
   DWorld d{};
+  float4* staging = nullptr;  // body records for host transfers (10 float4 a body, capacity)
   int solveBlocks = 0, maxSolveBlocks = 0;  // the cooperative solve's grid (maxSolveBlocks: all co-resident)
   int cur = 0;
   uint32_t stepCount = 0;

@@ -163,6 +163,7 @@ __device__ bool team_scan(uint32_t* data, uint32_t len, uint32_t* scratch, Team&
 
 // --- constraint endpoints and activity (gpu/layout.ts:356-369) ----------------------------------------
 __device__ inline bool enabledBody(const DWorld& w, uint32_t i) { return ((uint32_t)w.ipos[i].w & 2u) == 0u; }
+__device__ inline bool coldBody(const DWorld& w, uint32_t i) { return ((uint32_t)w.ipos[i].w & 4u) != 0u; }  // layout.ts:31
 __device__ inline bool dynBody(const DWorld& w, int i) { return i >= 0 && w.size[i].w > 0.0f && enabledBody(w, (uint32_t)i); }
 
 // Endpoints of constraint c (joints first, then contact pair slots); false when it does not act.
@@ -1021,6 +1022,14 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     float4* o = w.joint + j * JOINT_VEC4;
     o[J_C0_LIN] = make_float4(cl.x, cl.y, cl.z, 0.0f);
     o[J_C0_ANG] = make_float4(ca.x, ca.y, ca.z, k[J_C0_ANG].w);
+    if ((a >= 0 && coldBody(w, (uint32_t)a)) || coldBody(w, (uint32_t)b)) {  // a cold body's joints start afresh (wgsl-solve.ts:247-253)
+      const float pl = fminf(PENALTY_MIN, k[J_PEN_LIN].w), pa = fminf(PENALTY_MIN, k[J_PEN_ANG].w);
+      o[J_LAM_LIN] = make_float4(0.0f, 0.0f, 0.0f, k[J_LAM_LIN].w);
+      o[J_LAM_ANG] = make_float4(0.0f, 0.0f, 0.0f, k[J_LAM_ANG].w);
+      o[J_PEN_LIN] = make_float4(pl, pl, pl, k[J_PEN_LIN].w);
+      o[J_PEN_ANG] = make_float4(pa, pa, pa, k[J_PEN_ANG].w);
+      continue;
+    }
     float decay = p.alpha * p.gamma;
     o[J_LAM_LIN] = make_float4(k[J_LAM_LIN].x * decay, k[J_LAM_LIN].y * decay, k[J_LAM_LIN].z * decay, k[J_LAM_LIN].w);
     o[J_LAM_ANG] = make_float4(k[J_LAM_ANG].x * decay, k[J_LAM_ANG].y * decay, k[J_LAM_ANG].z * decay, k[J_LAM_ANG].w);
@@ -1030,7 +1039,7 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     o[J_PEN_ANG] = make_float4(wp(pa.x, pa.w), wp(pa.y, pa.w), wp(pa.z, pa.w), pa.w);
   }
   GSYNC
-  const float dt = p.dt, g = p.gravity;
+  const float dt = p.dt, gWorld = p.gravity;
   const float3 up = make_float3(p.upx, p.upy, p.upz);
   for (uint32_t i = tid; i < n; i += T) {
     if constexpr (Team::kDataflow) w.done[i] = 0u;
@@ -1038,6 +1047,17 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     float4 pos = w.pos[i], rot = w.rot[i], vel = w.vel[i];
     float3 av = f3(w.avel[i]);
     bool dynamic = w.size[i].w > 0.0f;
+    // the body's aux record (wgsl-solve.ts:9-20, 297-305): gravity scale, and damping of the
+    // incoming velocities, stored so the next step's up-velocity history is this step's start
+    const float4 ax = w.aux ? w.aux[i] : make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+    const float g = gWorld * ax.x;
+    if (dynamic && (ax.y > 0.0f || ax.z > 0.0f)) {
+      const float kl = expf(-ax.y * dt), ka = expf(-ax.z * dt);
+      vel = make_float4(vel.x * kl, vel.y * kl, vel.z * kl, vel.w);
+      av = av * ka;
+      w.vel[i] = vel;
+      w.avel[i] = make_float4(av.x, av.y, av.z, w.avel[i].w);
+    }
     float3 y = f3(pos) + f3(vel) * dt;
     if (dynamic) y = y + up * (g * (dt * dt));
     w.ypos[i] = make_float4(y.x, y.y, y.z, w.ypos[i].w);
