@@ -211,6 +211,13 @@ int avbd_hull_build(const float* points, uint32_t n, uint32_t* packed, uint32_t 
  * Records are validated (counts, index ranges); a body naming an offset that is not a hull header
  * is rejected by avbd_add_bodies / avbd_write_bodies. */
 int avbd_add_hull(avbd_world* world, const uint32_t* packed, uint32_t vec4s, uint32_t* offset);
+/* releaseHull (gpu/solver.ts:1408-1414, unpinHull :1448-1454): the record's run goes to the free list
+ * (merged with free neighbours) and the next avbd_add_hull that fits reuses it. Refused while a
+ * body's shape names the record. Reference counting per shape stays with the caller. */
+int avbd_release_hull(avbd_world* world, uint32_t offset);
+/* The hull buffer: top (vec4s in use or freed), device capacity and the largest free run; an
+ * adaptive world grows, so a hull always fits (canPinHull, :1421-1432). */
+int avbd_hull_storage(const avbd_world* world, uint32_t* top, uint32_t* capacity, uint32_t* largest_free);
 /* seedFrom's contact import (gpu/solver.ts:1320-1359): last step's manifolds and contacts, the
  * next step's warm-start source. manifold.first indexes `contacts`. */
 int avbd_seed_contacts(avbd_world* world, const avbd_manifold* manifolds, uint32_t n_manifolds, const avbd_contact* contacts,

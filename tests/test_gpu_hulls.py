@@ -103,3 +103,36 @@ def test_hull_records_are_validated(cuda_lib):
     body['shape'] = 3 + at
     w.add_bodies(body)
     w.destroy()
+
+
+def test_hull_release_and_reuse(cuda_lib):
+    """releaseHull / unpinHull (gpu/solver.ts:1408-1454): a released record's run is reused by the
+    next hull that fits; a record a body names is not released; bodies keep colliding."""
+    s = hull_pile(10, seed=1)
+    offs = list(s.hull_offsets) + [len(s.hull_words) // 4]
+    recs = [s.hull_words[4 * offs[k]:4 * offs[k + 1]].copy() for k in range(len(offs) - 1)]
+    for r, o in zip(recs, offs):
+        r[[0, 2, 4, 6]] -= np.uint32(o)  # each record with its header at vec4 0
+    big = max(range(len(recs)), key=lambda k: len(recs[k]))
+    small = min(range(len(recs)), key=lambda k: len(recs[k]))
+    w = avbd_b200.CudaSolver3D(body_capacity=64)
+    a = w.add_hull(recs[big])
+    b = w.add_hull(recs[small])
+    body = avbd_b200.pack_bodies([s.bodies[1]])
+    body['shape'] = 3 + b
+    w.add_bodies(body)
+    with pytest.raises(avbd_b200.AvbdError):
+        w.release_hull(b)  # a body names it
+    w.release_hull(a)
+    st = w.hull_storage()
+    assert st['largest_free'] == len(recs[big]) // 4
+    c = w.add_hull(recs[small])
+    assert c == a  # first fit: the released run
+    assert w.hull_storage()['largest_free'] == (len(recs[big]) - len(recs[small])) // 4
+    body['shape'] = 3 + c
+    w.add_bodies(body)
+    w.step(5)
+    assert w.read_counters()['error'] == 0
+    with pytest.raises(avbd_b200.AvbdError):
+        w.release_hull(a + 1)  # not a record
+    w.destroy()

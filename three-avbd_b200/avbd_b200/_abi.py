@@ -160,6 +160,8 @@ SIGNATURES = {
     'avbd_set_body_aux': ([P, VP, U, VP, VP, VP], I),
     'avbd_read_body_aux': ([P, U, VP, U], I),
     'avbd_set_lifecycle': ([P, U, U], I),
+    'avbd_release_hull': ([P, U], I),
+    'avbd_hull_storage': ([P, ctypes.POINTER(U), ctypes.POINTER(U), ctypes.POINTER(U)], I),
     'avbd_adjoint_create_from_batch': ([P, ctypes.c_uint32, ctypes.POINTER(P)], I),
     'avbd_adjoint_nominal': ([P, ctypes.POINTER(ctypes.c_double)], I),
     'avbd_adjoint_read_recording': ([P] + [VP] * 10, I),

@@ -218,6 +218,15 @@ class CudaSolver3D:
         self._check(self.lib.avbd_add_hull(self.handle, uptr(packed), len(packed) // 4, ctypes.byref(at)))
         return at.value
 
+    def release_hull(self, offset: int):
+        """The record's run goes free for a later add_hull (refused while a body uses it)."""
+        self._check(self.lib.avbd_release_hull(self.handle, offset))
+
+    def hull_storage(self) -> dict:
+        t, c, f = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.lib.avbd_hull_storage(self.handle, ctypes.byref(t), ctypes.byref(c), ctypes.byref(f)))
+        return {'top': t.value, 'capacity': c.value, 'largest_free': f.value}
+
     def add_scene_hulls(self, scene: Scene):
         """The scene's hull buffer, record by record, at the same offsets (the scene packs from 0)."""
         offs = list(getattr(scene, 'hull_offsets', []))

@@ -1058,13 +1058,25 @@ int avbd_add_hull(avbd_world* w, const uint32_t* packed, uint32_t vec4s, uint32_
   if (!w || !packed || !offset) return AVBD_ERR_INVALID;
   std::string msg = hullProblem(packed, vec4s);
   if (!msg.empty()) return fail(w, AVBD_ERR_INVALID, msg);
-  const uint32_t at = uint32_t(w->hullWords.size() / 4);
+  // the first released run that fits (as acquireHull takes a free block, gpu/solver.ts:1389-1399), else the top
+  uint32_t at = uint32_t(w->hullWords.size() / 4);
+  bool reused = false;
+  for (auto it = w->hullFree.begin(); it != w->hullFree.end(); ++it)
+    if (it->second >= vec4s) {
+      at = it->first;
+      const uint32_t rest = it->second - vec4s;
+      w->hullFree.erase(it);
+      if (rest) w->hullFree[at + vec4s] = rest;
+      reused = true;
+      break;
+    }
   if (uint64_t(at) + vec4s + AVBD_SHAPE_HULL >= (1ull << 24)) return fail(w, AVBD_ERR_CAPACITY, "hull buffer beyond 2^24 vec4s (f32 shape codes)");
   std::vector<uint32_t> rec(packed, packed + size_t(vec4s) * 4);
   for (int k : {0, 2, 4, 6}) rec[k] += at;
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  w->hullWords.insert(w->hullWords.end(), rec.begin(), rec.end());
+  if (reused) std::copy(rec.begin(), rec.end(), w->hullWords.begin() + size_t(at) * 4);
+  else w->hullWords.insert(w->hullWords.end(), rec.begin(), rec.end());
   const uint32_t total = uint32_t(w->hullWords.size() / 4);
   if (total > w->hullCapVec4) {
     uint32_t cap = std::max<uint32_t>(4096, std::max(total, 2 * w->hullCapVec4));
@@ -1083,7 +1095,52 @@ int avbd_add_hull(avbd_world* w, const uint32_t* packed, uint32_t vec4s, uint32_
     CUDA_TRY(w, cudaMemcpy(w->d.hulls + at, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
   }
   w->hullStarts.insert(at);
+  w->hullSize[at] = vec4s;
   *offset = at;
+  return AVBD_OK;
+}
+
+int avbd_release_hull(avbd_world* w, uint32_t offset) {
+  if (!w) return AVBD_ERR_INVALID;
+  if (!w->hullStarts.count(offset)) return fail(w, AVBD_ERR_INVALID, "no hull record at offset " + std::to_string(offset));
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  // a record some body still names stays (its shape code would point into whatever reuses the run)
+  std::vector<float4> avel(w->n);
+  if (w->n) CUDA_TRY(w, cudaMemcpy(avel.data(), w->d.avel, size_t(w->n) * sizeof(float4), cudaMemcpyDeviceToHost));
+  const float code = float(AVBD_SHAPE_HULL + offset);
+  for (uint32_t i = 0; i < w->n; i++)
+    if (avel[i].w == code) return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + " uses the hull at offset " + std::to_string(offset));
+  const uint32_t size = w->hullSize[offset];
+  w->hullStarts.erase(offset);
+  w->hullSize.erase(offset);
+  // free run, merged with its neighbours (releaseHull / mergeFree, gpu/solver.ts:1408-1414)
+  uint32_t start = offset, len = size;
+  auto next = w->hullFree.find(offset + size);
+  if (next != w->hullFree.end()) {
+    len += next->second;
+    w->hullFree.erase(next);
+  }
+  auto prev = w->hullFree.lower_bound(offset);
+  if (prev != w->hullFree.begin()) {
+    --prev;
+    if (prev->first + prev->second == offset) {
+      start = prev->first;
+      len += prev->second;
+      w->hullFree.erase(prev);
+    }
+  }
+  w->hullFree[start] = len;
+  return AVBD_OK;
+}
+
+int avbd_hull_storage(const avbd_world* w, uint32_t* top, uint32_t* capacity, uint32_t* largest_free) {
+  if (!w) return AVBD_ERR_INVALID;
+  uint32_t big = 0;
+  for (auto& f : w->hullFree) big = std::max(big, f.second);
+  if (top) *top = uint32_t(w->hullWords.size() / 4);
+  if (capacity) *capacity = w->hullCapVec4;
+  if (largest_free) *largest_free = big;
   return AVBD_OK;
 }
 

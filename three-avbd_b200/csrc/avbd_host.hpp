@@ -1,6 +1,7 @@
 // Host-side state shared by the single-world and batched entry points (avbd_host.cu, avbd_batch.cu).
 #pragma once
 #include <cstdint>
+#include <map>
 #include <set>
 #include <string>
 #include <vector>
@@ -72,6 +73,8 @@ struct avbd_world {
   // hull buffer: host copy of every record (wgsl-hull.ts layout), header offsets, device capacity
   std::vector<uint32_t> hullWords;
   std::set<uint32_t> hullStarts;
+  std::map<uint32_t, uint32_t> hullSize;  // header offset -> vec4s of each resident record
+  std::map<uint32_t, uint32_t> hullFree;  // released runs: offset -> vec4s (merged with neighbours)
   uint32_t hullCapVec4 = 0;
 };
 
