@@ -124,13 +124,19 @@ class ClockSampler:
         return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': smax or None, 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_reference(n_bodies: int, steps: int, threads: int) -> dict:
-    """The oracle (the reference's algorithm, GPU-mode rules) on the sampled pile's rollout."""
+def cpu_reference(n_bodies: int, steps: int, threads: int, warmup: int = 0) -> dict:
+    """The oracle (the reference's algorithm, GPU-mode rules) on the sampled pile's rollout: `warmup`
+    untimed steps on one instance (threads and caches), then steps 1..`steps` of a fresh one."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     from avbd_b200.scenes import drop_pile
     from oracle import Oracle, set_threads
     used = set_threads(threads)
     scene = drop_pile(n_bodies, seed=1)
+    if warmup > 0:
+        warm = Oracle(scene)
+        for _ in range(warmup):
+            warm.step_gpu()
+        del warm
     o = Oracle(scene)
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -146,9 +152,10 @@ def run_reference(args, rank: int):
     if rank != 0:
         return
     steps = min(args.steps, ROLLOUT)
-    ref = cpu_reference(SAMPLE_BODIES, steps, os.cpu_count() or 1)
+    warmup = max(args.warmup, 3)
+    ref = cpu_reference(SAMPLE_BODIES, steps, os.cpu_count() or 1, warmup)
     line = {
-        'metric': METRIC, 'value': ref['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': steps, 'warmup': 0,
+        'metric': METRIC, 'value': ref['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': steps, 'warmup': warmup,
         'ms_per_step': 1000 * ref['seconds'] / steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic', 'impl': 'reference', 'config': workload_config(SAMPLE_BODIES, steps),
         'cpu_baseline': {'value': ref['value'], 'unit': UNIT, 'cores': ref['cores'], 'kind': 'port', 'sample': ref['sample']},
