@@ -636,8 +636,11 @@ __device__ __forceinline__ LaneJob laneJob(const DWorld& w, uint32_t c, uint32_t
 
 // One 32-lane chunk: each group of lanes (one body) accumulates its rows, sums them by butterfly, its
 // first lane solves and writes the pose, and the lanes update the rows the body owns. With kWait the
-// chunk first waits for the bodies it reads and afterwards publishes its bodies' iteration count;
-// false: a wait gave up (warp-uniform).
+// chunk waits for the partner bodies it reads and afterwards publishes its bodies' iteration count;
+// false: a wait gave up (warp-uniform). With kWait the caller runs a chunk on the same warp in every
+// iteration, so the chunk's own bodies were last written by this warp (ordered by its __syncwarp)
+// and need no wait: their state is loaded first, alongside the first row's incidence, and only the
+// partners' counts are awaited.
 template <bool kWait>
 __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p, const LaneJob& J, uint32_t it) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -645,19 +648,8 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
   const bool active = J.active;
   const uint32_t L = J.L, sub = J.sub, body = J.body, e1 = J.e1;
   const uint32_t leader = lane - sub;
-  if constexpr (kWait) {
-    bool ok = true;
-    if (active) {
-      ok = waitDone(w, body, it);
-      for (uint32_t e = J.e; e < e1 && ok; e += L) {
-        const uint2 inc = w.incList[e];
-        // a partner of the same colour (only where the colour cap forced a clash) is not waited for
-        // within the iteration: the colour-by-colour sweep runs such pairs side by side too
-        if (inc.y & PARTNER_DYNAMIC) ok = waitDone(w, inc.y & PARTNER_MASK, it + ((inc.y & PARTNER_EARLIER) ? 1u : 0u));
-      }
-    }
-    if (__any_sync(0xffffffffu, !ok)) return false;
-  }
+  // the incidence list is fixed for the step: the lane's first row is read before any wait
+  const uint2 inc0 = kWait && active && J.e < e1 ? w.incList[J.e] : make_uint2(0u, 0u);
   Pose own;
   Acc acc;
   accZero(acc);
@@ -688,8 +680,20 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
       acc.v[25] = ra.y;
       acc.v[26] = ra.z;
     }
-    for (uint32_t e = J.e; e < e1; e += L) accumulateIncidence(acc, w, p, w.incList[e], body, own);
   }
+  if constexpr (kWait) {
+    bool ok = true;
+    if (active)
+      for (uint32_t e = J.e; e < e1 && ok; e += L) {
+        const uint2 inc = e == J.e ? inc0 : w.incList[e];
+        // a partner of the same colour (only where the colour cap forced a clash) is not waited for
+        // within the iteration: the colour-by-colour sweep runs such pairs side by side too
+        if (inc.y & PARTNER_DYNAMIC) ok = waitDone(w, inc.y & PARTNER_MASK, it + ((inc.y & PARTNER_EARLIER) ? 1u : 0u));
+      }
+    if (__any_sync(0xffffffffu, !ok)) return false;
+  }
+  if (active)
+    for (uint32_t e = J.e; e < e1; e += L) accumulateIncidence(acc, w, p, kWait && e == J.e ? inc0 : w.incList[e], body, own);
   // butterfly over the group: as many rounds as the warp's widest group needs
   const uint32_t Lmax = __reduce_max_sync(0xffffffffu, L);
   for (uint32_t off = Lmax >> 1; off > 0; off >>= 1) {
@@ -1098,12 +1102,12 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   __syncthreads();
   const uint32_t warpGlobal = tid >> 5, nwarps = T >> 5;
   if constexpr (Team::kDataflow) {
-    // Dataflow sweep: the iterations' colour passes as one ordered list of 32-lane chunks, dealt to
-    // the warps in turn. A chunk waits only for the bodies its rows touch (a body of an earlier colour
-    // to finish this iteration, one of a later colour the previous iteration; the body itself its
-    // previous iteration), so every read sees exactly what the colour-by-colour sweep reads, and the
-    // colours overlap instead of meeting at grid barriers. Every wait is on chunks earlier in the
-    // list, and each warp takes its chunks in list order, so the earliest unfinished chunk can
+    // Dataflow sweep: the iterations' colour passes as one ordered list of 32-lane chunks. A chunk
+    // waits only for the partner bodies its rows touch (a body of an earlier colour to finish this
+    // iteration, one of a later colour the previous iteration; the body itself ran its previous
+    // iteration on the same warp), so every read sees exactly what the colour-by-colour sweep reads,
+    // and the colours overlap instead of meeting at grid barriers. Every wait is on chunks earlier in
+    // the list, and each warp takes its chunks in list order, so the earliest unfinished chunk can
     // always run.
     if (threadIdx.x == 0) {
       uint32_t acc = 0, lanes = 0;
@@ -1117,13 +1121,16 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
       s_laneOff[numColors] = lanes;
     }
     __syncthreads();
+    // Chunk r of every iteration runs on warp r mod (warps): a warp takes its chunks iteration by
+    // iteration, in list order, and a body's group of lanes stays on one warp for the whole sweep.
     const uint32_t perIter = s_chunk[numColors];
-    const uint32_t items = perIter * (uint32_t)max(p.iterations, 0);
-    // chunk k's lane entry, fetched one chunk ahead (the lane table is fixed for the step)
-    auto entryOf = [&](uint32_t k, bool& active) -> uint4 {
+    const uint32_t mine = warpGlobal < perIter ? (perIter - warpGlobal + nwarps - 1u) / nwarps : 0u;
+    const uint32_t items = mine * (uint32_t)max(p.iterations, 0);
+    // the warp's j-th chunk's lane entry, fetched one chunk ahead (the lane table is fixed for the step)
+    auto entryOf = [&](uint32_t j, bool& active) -> uint4 {
       active = false;
-      if (k >= items) return make_uint4(0u, 0u, 0u, 1u);
-      const uint32_t r = k % perIter;
+      if (j >= items) return make_uint4(0u, 0u, 0u, 1u);
+      const uint32_t r = warpGlobal + (j % mine) * nwarps;
       uint32_t c = 0;
       while (s_chunk[c + 1] <= r) c++;
       const uint32_t lam = (r - s_chunk[c]) * 32u + (threadIdx.x & 31u);
@@ -1131,11 +1138,11 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
       return active ? w.laneTable[s_laneOff[c] + lam] : make_uint4(0u, 0u, 0u, 1u);
     };
     bool nextActive;
-    uint4 next = entryOf(warpGlobal, nextActive);
-    for (uint32_t k = warpGlobal; k < items; k += nwarps) {
+    uint4 next = entryOf(0u, nextActive);
+    for (uint32_t j = 0; j < items; j++) {
       const LaneJob J = jobFromEntry(next, nextActive);
-      next = entryOf(k + nwarps, nextActive);
-      if (!solveLanes<true>(w, p, J, k / perIter)) break;
+      next = entryOf(j + 1u, nextActive);
+      if (!solveLanes<true>(w, p, J, j / mine)) break;
     }
     GSYNC
   } else {
