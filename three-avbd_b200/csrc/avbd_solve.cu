@@ -722,7 +722,7 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
   own.dAng = make_float3(__shfl_sync(0xffffffffu, da.x, leader), __shfl_sync(0xffffffffu, da.y, leader), __shfl_sync(0xffffffffu, da.z, leader));
   if (active) {
     for (uint32_t e = J.e; e < e1; e += L) {
-      uint2 inc = w.incList[e];
+      const uint2 inc = kWait && e == J.e ? inc0 : w.incList[e];
       if (inc.x & OWNER_BIT) dualIncidence(w, p, inc, body, own);
     }
   }
