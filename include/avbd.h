@@ -171,6 +171,15 @@ int avbd_add_joints(avbd_world* world, const avbd_joint* joints, const avbd_join
 int avbd_write_joints(avbd_world* world, uint32_t first, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n);
 /* releaseJoints (world.ts) / disableConstraint (gpu/solver.ts:1941-1947): slot stops acting. */
 int avbd_release_joints(avbd_world* world, const uint32_t* slots, uint32_t n);
+/* appendWorldJoint(b, anchorWorld, anchorBody) with the 'legacy' policy (gpu/solver.ts:1592-1623):
+ * appends a joint holding body b's point anchor_body (body frame) at the world point anchor_world:
+ * hard linear rows, no angular rows (the body turns freely about the point), never breaking, torque
+ * arm |size|^2 of the body. *slot receives its slot. ('inertial-hard' needs the reference's native
+ * sensor shaders and has no counterpart.) */
+int avbd_add_world_joint(avbd_world* world, uint32_t body, const float anchor_world[3], const float anchor_body[3], uint32_t* slot);
+/* setWorldAnchor(slot, p) (gpu/solver.ts:1937-1939): the slot's r_a (a world joint's world point)
+ * becomes p from the next step on. */
+int avbd_set_world_anchor(avbd_world* world, uint32_t slot, const float p[3]);
 /* IgnoreCollision pairs (ref/forces.ts:384-390; no-collide table gpu/no-collide.ts). */
 int avbd_add_ignore_pairs(avbd_world* world, const uint32_t* pairs_ab, uint32_t n);
 /* setFilters (gpu/solver.ts): groups_mask[2i] = groups, [2i+1] = collides-with mask. */
@@ -271,6 +280,33 @@ int avbd_set_solve_blocks(avbd_world* world, int blocks);
 
 /* The world's CUDA stream (cudaStream_t) for callers that order their own device work with its steps. */
 int avbd_world_stream(avbd_world* world, void** stream);
+
+/* Device views of the world's storage for CUDA consumers on its device, as the reference hands its
+ * buffers to ContactWatch, Pusher and BodyMover (bodyBuffer, contactStorage / contactStorages(),
+ * gpu/solver.ts:638-650; world.ts:854-862). Read or write them in stream order with the world's
+ * steps (avbd_world_stream). Body arrays stay where they are for the world's lifetime (the body
+ * capacity is fixed at creation); contact arrays move when pair storage grows (at a step, after 80 %
+ * use or an overflow bit), so query them again after each step. */
+typedef struct avbd_body_view {
+  void* fields[10];   /* one float4 array per row of the avbd_body record, in record order:
+                         pos + friction, rot, initial pos + flags, initial rot, size + mass,
+                         moment + radius, inertial pos, inertial rot, vel + prev up vel, ang vel + shape */
+  uint32_t count;     /* bodies in use */
+  uint32_t capacity;  /* length of each array */
+} avbd_body_view;
+int avbd_body_storage(avbd_world* world, avbd_body_view* out);
+
+typedef struct avbd_contact_view {
+  const void* pairs;         /* uint4 per pair slot: a, b, first point slot (8 x slot), count | step << 4; count 0: no manifold */
+  const void* normals;       /* float4 per pair slot: normal (B to A), friction */
+  const void* points;        /* avbd_contact per point slot: pair slot p's points at 8p .. 8p + count - 1 */
+  const uint32_t* counters;  /* the world's device counter words */
+  uint32_t count_word;       /* counters[count_word]: pair slots this storage holds */
+  uint32_t pair_capacity;    /* pair slots (points: 8 x) */
+} avbd_contact_view;
+/* which 0: the storage the last step wrote (contactStorage); 1: the one the step before wrote, which
+ * the next step overwrites (the other entry of contactStorages()). */
+int avbd_contact_storage(avbd_world* world, uint32_t which, avbd_contact_view* out);
 
 /* Pose/velocity update from caller memory (pinned for overlap), enqueued on the world's stream
  * without validation or synchronisation: shapes, masses and radii must be unchanged (use

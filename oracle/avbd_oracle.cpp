@@ -2208,6 +2208,16 @@ void orc_set_joint(void* h, int i, const double* r) {
   });
 }
 
+// setWorldAnchor (gpu/solver.ts:1937-1939): joint i's rA (the world point of a joint with no body A)
+void orc_set_joint_anchor(void* h, int i, const double* p) {
+  with(h, [&](auto& s) {
+    using T = std::decay_t<decltype(s.dt)>;
+    auto* j = static_cast<Joint<T>*>(s.forces[i].get());
+    for (int k = 0; k < 3; k++) j->rA[k] = T(p[k]);
+    return 0;
+  });
+}
+
 // Manifolds in force order. Manifold record (8 doubles): force index, a, b, count, normal3,
 // friction. Contact record (17): feature, stick, rA3, rB3, C0 3, pen3, lam3.
 int orc_manifold_count(void* h) {

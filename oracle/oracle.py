@@ -45,6 +45,7 @@ def lib():
         L.orc_force_count.argtypes = [P]
         L.orc_get_force.argtypes = [P, I, D]
         L.orc_set_joint.argtypes = [P, I, D]
+        L.orc_set_joint_anchor.argtypes = [P, I, D]
         L.orc_manifold_count.argtypes = [P]
         L.orc_contact_count.argtypes = [P]
         L.orc_get_manifolds.argtypes = [P, D, D]
@@ -206,6 +207,11 @@ class Oracle:
     def set_joint(self, i, rec):
         rec = np.ascontiguousarray(rec, dtype=np.float64)
         self.L.orc_set_joint(self.h, i, _dp(rec))
+
+    def set_joint_anchor(self, i, p):
+        """setWorldAnchor: joint i's rA (its world point when it has no body A)."""
+        q = np.ascontiguousarray(p, dtype=np.float64)
+        self.L.orc_set_joint_anchor(self.h, i, _dp(q))
 
     def manifolds(self):
         nm = self.L.orc_manifold_count(self.h)

@@ -170,3 +170,29 @@ def test_hash32_matches_reference_priorities():
         return x
     for v in [0, 1, 2, 12345, 0x9e3779b9, 0xFFFFFFFF]:
         assert L.orc_hash32(v) == ref(v)
+
+
+def test_world_joint_holds_and_follows_its_anchor():
+    """A joint with no body A (forces.ts:150-155: its rA is a world point) holds a pendulum's end at
+    that point, and moving the point (setWorldAnchor, gpu/solver.ts:1937-1939) is what the next
+    step's C0 measures from."""
+    import math
+    s = Scene('world joint')
+    a = s.box([1.0, 0.5, 0.5], 1.0, 0.5, [0.5, 0.0, 5.0])
+    s.bodies[a].vel = [0.0, 1.0, 0.0]
+    s.joint(-1, a, [0.0, 0.0, 5.0], [-0.5, 0.0, 0.0], math.inf, 0.0)
+    o = Oracle(s)
+    o.step(60)
+    b = o.bodies()[0]
+    x, q = b[0:3], b[3:7]
+    u, w = q[:3], q[3]
+    v = np.array([-0.5, 0.0, 0.0])
+    end = x + v + 2.0 * w * np.cross(u, v) + 2.0 * np.cross(u, np.cross(u, v))
+    assert np.linalg.norm(end - np.array([0.0, 0.0, 5.0])) < 1e-2
+    assert np.linalg.norm(x - np.array([0.0, 0.0, 5.0])) > 0.45  # it swung, and hangs by its end
+    moved = np.array([0.3, 0.0, 5.2])
+    o.set_joint_anchor(0, moved)
+    assert np.array_equal(o.force(0)[39:42], moved)
+    o.step()
+    # C0 = anchor - end at the step's start (forces.ts:186-203)
+    assert np.abs(o.force(0)[15:18] - (moved - end)).max() < 1e-9

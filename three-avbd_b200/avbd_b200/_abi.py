@@ -83,6 +83,15 @@ SHAPE_HULL = 3
 MAX_HULL_VERTICES = 32
 
 
+class BodyView(ctypes.Structure):
+    _fields_ = [('fields', ctypes.c_void_p * 10), ('count', ctypes.c_uint32), ('capacity', ctypes.c_uint32)]
+
+
+class ContactView(ctypes.Structure):
+    _fields_ = [('pairs', ctypes.c_void_p), ('normals', ctypes.c_void_p), ('points', ctypes.c_void_p), ('counters', ctypes.c_void_p),
+                ('count_word', ctypes.c_uint32), ('pair_capacity', ctypes.c_uint32)]
+
+
 class BatchConfig(ctypes.Structure):
     _fields_ = [('world_capacity', ctypes.c_uint32), ('body_capacity', ctypes.c_uint32), ('joint_capacity', ctypes.c_uint32),
                 ('pairs_per_body', ctypes.c_uint32), ('device', ctypes.c_int32)]
@@ -128,6 +137,10 @@ SIGNATURES = {
     'avbd_add_joints': ([P, VP, VP, U, PU], I),
     'avbd_write_joints': ([P, U, VP, VP, U], I),
     'avbd_release_joints': ([P, PU, U], I),
+    'avbd_add_world_joint': ([P, U, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), PU], I),
+    'avbd_set_world_anchor': ([P, U, ctypes.POINTER(ctypes.c_float)], I),
+    'avbd_body_storage': ([P, ctypes.POINTER(BodyView)], I),
+    'avbd_contact_storage': ([P, U, ctypes.POINTER(ContactView)], I),
     'avbd_add_ignore_pairs': ([P, PU, U], I),
     'avbd_set_filters': ([P, U, PU, U], I),
     'avbd_seed_contacts': ([P, VP, U, VP, U], I),

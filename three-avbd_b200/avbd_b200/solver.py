@@ -266,6 +266,36 @@ class CudaSolver3D:
         s = np.ascontiguousarray(slots, dtype=np.uint32)
         self._check(self.lib.avbd_release_joints(self.handle, uptr(s), len(s)))
 
+    def append_world_joint(self, body: int, anchor_world, anchor_body) -> int:
+        """appendWorldJoint(b, anchorWorld, anchorBody), 'legacy' policy: holds the body's point
+        `anchor_body` (body frame) at the world point `anchor_world`, free to turn; returns its slot."""
+        aw = (ctypes.c_float * 3)(*[float(x) for x in anchor_world])
+        ab = (ctypes.c_float * 3)(*[float(x) for x in anchor_body])
+        slot = ctypes.c_uint32()
+        self._check(self.lib.avbd_add_world_joint(self.handle, int(body), aw, ab, ctypes.byref(slot)))
+        return slot.value
+
+    def set_world_anchor(self, slot: int, p):
+        """setWorldAnchor(slot, p): the joint's world point (r_a) from the next step on."""
+        q = (ctypes.c_float * 3)(*[float(x) for x in p])
+        self._check(self.lib.avbd_set_world_anchor(self.handle, int(slot), q))
+
+    def body_storage(self) -> dict:
+        """bodyBuffer: device addresses of the ten float4 field arrays (avbd_body record rows, in
+        order), the bodies in use and the arrays' length."""
+        v = _abi.BodyView()
+        self._check(self.lib.avbd_body_storage(self.handle, ctypes.byref(v)))
+        return {'fields': [int(f or 0) for f in v.fields], 'count': v.count, 'capacity': v.capacity}
+
+    def contact_storage(self, which: int = 0) -> dict:
+        """contactStorage (which 0: what the last step wrote) / contactStorages() (which 1: the step
+        before's): device addresses of the pair words, normals and points, the counters and the word
+        holding the pair-slot count, and the pair-slot capacity."""
+        v = _abi.ContactView()
+        self._check(self.lib.avbd_contact_storage(self.handle, int(which), ctypes.byref(v)))
+        return {'pairs': int(v.pairs or 0), 'normals': int(v.normals or 0), 'points': int(v.points or 0), 'counters': int(v.counters or 0),
+                'count_word': v.count_word, 'pair_capacity': v.pair_capacity}
+
     def add_ignore_pairs(self, pairs: np.ndarray):
         p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)
         self._check(self.lib.avbd_add_ignore_pairs(self.handle, uptr(p), len(p)))

@@ -1158,4 +1158,69 @@ int avbd_write_bodies_async(avbd_world* w, uint32_t first, const avbd_body* bodi
   return AVBD_OK;
 }
 
+// appendWorldJoint, 'legacy' policy (gpu/solver.ts:1592-1623): the record of freshJoint (:132-138)
+// with a hard linear stiffness, the world point in r_a, the body point in r_b and the torque arm of
+// the body's size; no angular stiffness, so the joint holds the point and leaves the turn free.
+int avbd_add_world_joint(avbd_world* w, uint32_t body, const float anchor_world[3], const float anchor_body[3], uint32_t* slot) {
+  if (!w || !anchor_world || !anchor_body) return AVBD_ERR_INVALID;
+  if (body >= w->n) return fail(w, AVBD_ERR_INVALID, "appendWorldJoint: body " + std::to_string(body) + " is not a body of the world");
+  for (int k = 0; k < 3; k++)
+    if (!std::isfinite(anchor_world[k]) || !std::isfinite(anchor_body[k]))
+      return fail(w, AVBD_ERR_INVALID, "appendWorldJoint: anchors need three finite f32 numbers");
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  float4 size;
+  CUDA_TRY(w, cudaMemcpy(&size, w->d.size + body, sizeof(float4), cudaMemcpyDeviceToHost));
+  const float arm = size.x * size.x + size.y * size.y + size.z * size.z;
+  if (!std::isfinite(arm)) return fail(w, AVBD_ERR_INVALID, "appendWorldJoint: torque arm must be finite as f32");
+  avbd_joint j{};
+  j.stiffness_lin = AVBD_BIG;
+  j.fracture = AVBD_BIG;
+  j.yield_force = AVBD_BIG;
+  j.break_bend = AVBD_BIG;
+  j.rest[3] = 1.0f;
+  j.rest_start[3] = 1.0f;
+  j.torque_arm = arm;
+  for (int k = 0; k < 3; k++) {
+    j.r_a[k] = anchor_world[k];
+    j.r_b[k] = anchor_body[k];
+  }
+  const avbd_joint_info info{AVBD_T_JOINT, -1, int32_t(body), 0};
+  return avbd_add_joints(w, &j, &info, 1, slot);
+}
+
+// setWorldAnchor (gpu/solver.ts:1937-1939): the slot's r_a, in place before the next step
+int avbd_set_world_anchor(avbd_world* w, uint32_t slot, const float p[3]) {
+  if (!w || !p) return AVBD_ERR_INVALID;
+  if (slot >= w->nj) return fail(w, AVBD_ERR_INVALID, "setWorldAnchor: joint slot " + std::to_string(slot) + " out of range");
+  for (int k = 0; k < 3; k++)
+    if (!std::isfinite(p[k])) return fail(w, AVBD_ERR_INVALID, "setWorldAnchor: the anchor needs three finite f32 numbers");
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  float* rec = reinterpret_cast<float*>(w->d.joint + size_t(slot) * JOINT_VEC4 + J_RA);
+  CUDA_TRY(w, cudaMemcpy(rec, p, 3 * sizeof(float), cudaMemcpyHostToDevice));
+  return AVBD_OK;
+}
+
+int avbd_body_storage(avbd_world* w, avbd_body_view* out) {
+  if (!w || !out) return AVBD_ERR_INVALID;
+  float4* const fields[10] = {w->d.pos, w->d.rot, w->d.ipos, w->d.irot, w->d.size, w->d.moment, w->d.ypos, w->d.yrot, w->d.vel, w->d.avel};
+  for (int f = 0; f < 10; f++) out->fields[f] = fields[f];
+  out->count = w->n;
+  out->capacity = w->bodyCap;
+  return AVBD_OK;
+}
+
+int avbd_contact_storage(avbd_world* w, uint32_t which, avbd_contact_view* out) {
+  if (!w || !out || which > 1u) return AVBD_ERR_INVALID;
+  const int buf = which == 0u ? 1 - w->cur : w->cur;  // avbd_step flips cur after each step
+  out->pairs = w->d.mIds[buf];
+  out->normals = w->d.mGeo[buf];
+  out->points = w->d.cPt[buf];
+  out->counters = w->d.counters;
+  out->count_word = which == 0u ? uint32_t(C_PAIRS) : uint32_t(C_PREV_PAIRS);
+  out->pair_capacity = w->pairCap;
+  return AVBD_OK;
+}
+
 }  // extern "C"
