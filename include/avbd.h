@@ -169,8 +169,16 @@ int avbd_write_bodies(avbd_world* world, uint32_t first, const avbd_body* bodies
 int avbd_add_joints(avbd_world* world, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* first);
 /* seedFrom's joint rewrite (gpu/solver.ts:1330-1331). */
 int avbd_write_joints(avbd_world* world, uint32_t first, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n);
-/* releaseJoints (world.ts) / disableConstraint (gpu/solver.ts:1941-1947): slot stops acting. */
+/* appendJoints / appendSprings through appendConstraints (gpu/solver.ts:1709-1738): released slots
+ * are taken first (lowest first), then new slots at the end; slots[k] receives joint k's slot. */
+int avbd_append_joints(avbd_world* world, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* slots);
+/* releaseJoints (gpu/solver.ts:1745-1771): each slot in range and not yet released stops acting (record
+ * zeroed, info AVBD_T_NONE with bodies -1), its two bodies collide again, and the slot goes to the
+ * free list that avbd_append_joints takes from. Slots out of range or already released are ignored. */
 int avbd_release_joints(avbd_world* world, const uint32_t* slots, uint32_t n);
+/* disableConstraint (gpu/solver.ts:1941-1947): penalties, stiffnesses and multipliers zeroed
+ * (fracture and torque arm kept); the slot stays taken. */
+int avbd_disable_joints(avbd_world* world, const uint32_t* slots, uint32_t n);
 /* appendWorldJoint(b, anchorWorld, anchorBody) with the 'legacy' policy (gpu/solver.ts:1592-1623):
  * appends a joint holding body b's point anchor_body (body frame) at the world point anchor_world:
  * hard linear rows, no angular rows (the body turns freely about the point), never breaking, torque

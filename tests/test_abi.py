@@ -46,6 +46,8 @@ def test_defaults_and_invalid_arguments_without_a_device():
     assert lib.avbd_world_destroy(None) == 0
     assert lib.avbd_step(None, 1) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_add_world_joint(None, 0, None, None, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_append_joints(None, None, None, 0, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_disable_joints(None, None, 0) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_set_world_anchor(None, 0, None) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_body_storage(None, None) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_contact_storage(None, 0, None) == _abi.AVBD_ERR_INVALID

@@ -1,6 +1,7 @@
 """World joints (appendWorldJoint / setWorldAnchor, gpu/solver.ts:1592-1623, 1937-1939) against the
-FP64 oracle, and the device storage views (bodyBuffer, contactStorage / contactStorages(),
-gpu/solver.ts:638-650) read back through torch and compared with the synchronous readbacks."""
+FP64 oracle; joint slots released and reused (releaseJoints, appendConstraints, :1709-1771); and the
+device storage views (bodyBuffer, contactStorage / contactStorages(), :638-650) read back through
+torch and compared with the synchronous readbacks."""
 
 import math
 
@@ -8,7 +9,9 @@ import numpy as np
 import pytest
 
 import avbd_b200
+from avbd_b200 import _abi
 from avbd_b200.scenes import Scene, demo_scene
+from avbd_b200.solver import pack_force
 from oracle import Oracle
 from _util import cuda_from_oracle, joint_records, oracle_sequential_colors, pose_diff
 
@@ -159,3 +162,64 @@ def test_storage_views_match_readbacks(cuda_lib):
     for x, y in zip(before, last):
         assert x[:2] == y[:2] and np.array_equal(x[2], y[2]) and np.array_equal(x[3], y[3])
     w.destroy()
+
+
+def _row(joined):
+    """Four overlapping boxes in a row, weightless; `joined` lists the (a, b) pairs held by joints."""
+    s = Scene('row')
+    s.params.gravity = 0.0
+    for i in range(4):
+        s.box([1.05, 1.0, 1.0], 1.0, 0.5, [float(i), 0.0, 5.0])
+    for a, b in joined:
+        s.joint(a, b, [0.5, 0.0, 0.0], [-0.5, 0.0, 0.0], math.inf, math.inf)
+    return s
+
+
+def test_released_slots_collide_again_and_are_reused(cuda_lib):
+    w = avbd_b200.CudaSolver3D(_row([(0, 1), (1, 2), (2, 3)]))
+    w.step()
+    pairs = {tuple(sorted(p)) for p in w.read_pairs().tolist()}
+    assert not pairs & {(0, 1), (1, 2), (2, 3)}  # joined neighbours do not collide
+    w.release_joints([1, 1, 99])  # repeats and slots out of range are ignored
+    w.release_joints([1])         # so is a slot already released
+    recs, info = w.read_joints()
+    assert (int(info[1]['type']), int(info[1]['a']), int(info[1]['b'])) == (_abi.T_NONE, -1, -1)
+    assert not recs[1].tobytes().strip(b'\0')
+    w.step()
+    pairs = {tuple(sorted(p)) for p in w.read_pairs().tolist()}
+    assert (1, 2) in pairs and not pairs & {(0, 1), (2, 3)}
+    # the next append takes the freed slot, then new ones; its pair stops colliding
+    s = _row([(0, 2), (1, 3)])
+    recs_new = np.array([pack_force(f, s.bodies)[0] for f in s.forces])
+    info_new = np.array([pack_force(f, s.bodies)[1] for f in s.forces])
+    slots = w.append_joints(recs_new, info_new)
+    assert slots.tolist() == [1, 3]
+    w.step()
+    pairs = {tuple(sorted(p)) for p in w.read_pairs().tolist()}
+    assert (1, 2) in pairs
+    assert w.read_counters()['error'] == 0
+    w.destroy()
+
+
+def test_reused_slot_steps_as_a_fresh_world(cuda_lib):
+    """Releasing a slot and appending into it gives the world built with that joint in the slot."""
+    a = avbd_b200.CudaSolver3D(_row([(0, 1), (1, 2), (2, 3)]))
+    a.release_joints([1])
+    s = _row([(1, 3)])
+    slot = a.append_joints(np.array([pack_force(s.forces[0], s.bodies)[0]]), np.array([pack_force(s.forces[0], s.bodies)[1]]))
+    assert slot.tolist() == [1]
+    b = avbd_b200.CudaSolver3D(_row([(0, 1), (1, 3), (2, 3)]))
+    ra, ia = a.read_joints()
+    rb, ib = b.read_joints()
+    assert ra.tobytes() == rb.tobytes() and ia.tobytes() == ib.tobytes()
+    for w in (a, b):
+        w.step(20)
+    assert a.read_bodies().tobytes() == b.read_bodies().tobytes()
+    assert a.read_joints()[0].tobytes() == b.read_joints()[0].tobytes()
+    # disableConstraint keeps the slot taken
+    a.disable_joints([1])
+    recs, info = a.read_joints()
+    assert int(info[1]['type']) == _abi.T_JOINT and recs[1]['stiffness_lin'] == 0.0
+    assert a.append_joints(np.array([pack_force(s.forces[0], s.bodies)[0]]), np.array([pack_force(s.forces[0], s.bodies)[1]])).tolist() == [3]
+    a.destroy()
+    b.destroy()

@@ -137,6 +137,8 @@ SIGNATURES = {
     'avbd_add_joints': ([P, VP, VP, U, PU], I),
     'avbd_write_joints': ([P, U, VP, VP, U], I),
     'avbd_release_joints': ([P, PU, U], I),
+    'avbd_append_joints': ([P, VP, VP, U, PU], I),
+    'avbd_disable_joints': ([P, PU, U], I),
     'avbd_add_world_joint': ([P, U, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), PU], I),
     'avbd_set_world_anchor': ([P, U, ctypes.POINTER(ctypes.c_float)], I),
     'avbd_body_storage': ([P, ctypes.POINTER(BodyView)], I),

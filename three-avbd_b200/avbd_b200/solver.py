@@ -262,9 +262,23 @@ class CudaSolver3D:
         info = np.ascontiguousarray(info, dtype=INFO_DTYPE)
         self._check(self.lib.avbd_write_joints(self.handle, first, ptr(records), ptr(info), len(records)))
 
+    def append_joints(self, records: np.ndarray, info: np.ndarray) -> np.ndarray:
+        """appendJoints / appendSprings: released slots first (lowest first), then new ones; the slots."""
+        records = np.ascontiguousarray(records, dtype=JOINT_DTYPE)
+        info = np.ascontiguousarray(info, dtype=INFO_DTYPE)
+        slots = np.zeros(len(records), dtype=np.uint32)
+        self._check(self.lib.avbd_append_joints(self.handle, ptr(records), ptr(info), len(records), uptr(slots)))
+        return slots
+
     def release_joints(self, slots):
+        """releaseJoints: the slots stop acting, their bodies collide again, the slots are reused."""
         s = np.ascontiguousarray(slots, dtype=np.uint32)
         self._check(self.lib.avbd_release_joints(self.handle, uptr(s), len(s)))
+
+    def disable_joints(self, slots):
+        """disableConstraint: penalties, stiffnesses and multipliers zeroed; the slots stay taken."""
+        s = np.ascontiguousarray(slots, dtype=np.uint32)
+        self._check(self.lib.avbd_disable_joints(self.handle, uptr(s), len(s)))
 
     def append_world_joint(self, body: int, anchor_world, anchor_body) -> int:
         """appendWorldJoint(b, anchorWorld, anchorBody), 'legacy' policy: holds the body's point

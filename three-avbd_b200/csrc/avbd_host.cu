@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -650,7 +651,83 @@ int avbd_add_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint_in
   return AVBD_OK;
 }
 
+// appendConstraints (gpu/solver.ts:1709-1738): released slots first, lowest first, then new slots
+// at the end; each record and info written, each joint's pair kept out of the broadphase
+int avbd_append_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* slots) {
+  if (!w || (n && (!joints || !info || !slots))) return AVBD_ERR_INVALID;
+  int r = checkJoints(w, joints, info, n);
+  if (r) return r;
+  if (!n) return AVBD_OK;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  std::sort(w->freeSlots.begin(), w->freeSlots.end(), std::greater<uint32_t>());
+  const uint32_t reused = std::min<uint32_t>(n, uint32_t(w->freeSlots.size()));
+  const uint32_t fresh = n - reused;
+  if (uint64_t(w->nj) + fresh > w->jointCap) {
+    const uint64_t cap = std::max<uint64_t>(uint64_t(w->nj) + fresh + 256, uint64_t(w->jointCap) * 2);
+    r = allocJoints(w, uint32_t(cap));
+    if (r) return r;
+  }
+  for (uint32_t k = 0; k < reused; k++) {
+    slots[k] = w->freeSlots.back();
+    w->freeSlots.pop_back();
+  }
+  for (uint32_t k = 0; k < fresh; k++) slots[reused + k] = w->nj + k;
+  w->nj += fresh;
+  w->info.resize(w->nj);
+  for (uint32_t k = 0; k < n;) {  // one copy per run of consecutive slots
+    uint32_t e = k + 1;
+    while (e < n && slots[e] == slots[e - 1] + 1) e++;
+    CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(slots[k]) * JOINT_VEC4, joints + k, size_t(e - k) * sizeof(avbd_joint), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(w->d.jinfo + slots[k], info + k, size_t(e - k) * sizeof(int4), cudaMemcpyHostToDevice));
+    k = e;
+  }
+  for (uint32_t k = 0; k < n; k++) {
+    w->info[slots[k]] = info[k];
+    if (info[k].a >= 0 && info[k].type != AVBD_T_NONE) {
+      const uint32_t a = uint32_t(info[k].a), b = uint32_t(info[k].b);
+      w->nocollide.push_back({std::max(a, b), std::min(a, b), slots[k]});
+    }
+  }
+  w->staticsDirty = true;
+  return AVBD_OK;
+}
+
+// releaseJoints (gpu/solver.ts:1745-1771): slots in range and not yet released stop acting, their
+// records zeroed and their info T_NONE; their pairs collide again (their no-collide entries go, so a
+// reused slot keeps only its new pair's); the slots go to the free list
 int avbd_release_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
+  if (!w || (n && !slots)) return AVBD_ERR_INVALID;
+  std::vector<uint32_t> order;
+  for (uint32_t i = 0; i < n; i++)
+    if (slots[i] < w->nj && w->info[slots[i]].type != AVBD_T_NONE) order.push_back(slots[i]);
+  std::sort(order.begin(), order.end());
+  order.erase(std::unique(order.begin(), order.end()), order.end());
+  if (order.empty()) return AVBD_OK;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  const avbd_joint_info none{AVBD_T_NONE, -1, -1, 0};
+  for (size_t k = 0; k < order.size();) {
+    size_t e = k + 1;
+    while (e < order.size() && order[e] == order[e - 1] + 1) e++;
+    const std::vector<avbd_joint> zeros(e - k);
+    const std::vector<avbd_joint_info> infos(e - k, none);
+    CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(order[k]) * JOINT_VEC4, zeros.data(), zeros.size() * sizeof(avbd_joint), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, cudaMemcpy(w->d.jinfo + order[k], infos.data(), infos.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    k = e;
+  }
+  for (uint32_t s : order) {
+    w->info[s] = none;
+    w->freeSlots.push_back(s);
+  }
+  w->nocollide.erase(std::remove_if(w->nocollide.begin(), w->nocollide.end(),
+                                    [&](const NoCollide& c) { return c.slot != 0xffffffffu && std::binary_search(order.begin(), order.end(), c.slot); }),
+                     w->nocollide.end());
+  w->staticsDirty = true;
+  return AVBD_OK;
+}
+
+int avbd_disable_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
   if (!w || (n && !slots)) return AVBD_ERR_INVALID;
   for (uint32_t i = 0; i < n; i++)
     if (slots[i] >= w->nj) return fail(w, AVBD_ERR_INVALID, "joint slot " + std::to_string(slots[i]) + " out of range");
@@ -1186,7 +1263,10 @@ int avbd_add_world_joint(avbd_world* w, uint32_t body, const float anchor_world[
     j.r_b[k] = anchor_body[k];
   }
   const avbd_joint_info info{AVBD_T_JOINT, -1, int32_t(body), 0};
-  return avbd_add_joints(w, &j, &info, 1, slot);
+  uint32_t at = 0;
+  const int r = avbd_append_joints(w, &j, &info, 1, &at);
+  if (!r && slot) *slot = at;
+  return r;
 }
 
 // setWorldAnchor (gpu/solver.ts:1937-1939): the slot's r_a, in place before the next step

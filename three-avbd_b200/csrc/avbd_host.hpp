@@ -50,6 +50,7 @@ struct avbd_world {
   std::vector<float> radius;
   std::vector<char> dynamic;
   std::vector<avbd_joint_info> info;
+  std::vector<uint32_t> freeSlots;  // released joint slots, taken again by avbd_append_joints
   std::vector<NoCollide> nocollide;
   bool staticsDirty = true;
   float threshold = 0.0f, cellSize = 1.0f;
