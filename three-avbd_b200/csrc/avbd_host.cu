@@ -619,6 +619,10 @@ int avbd_write_joints(avbd_world* w, uint32_t first, const avbd_joint* joints, c
   CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(first) * JOINT_VEC4, joints, size_t(n) * sizeof(avbd_joint), cudaMemcpyHostToDevice));
   CUDA_TRY(w, cudaMemcpy(w->d.jinfo + first, info, size_t(n) * sizeof(int4), cudaMemcpyHostToDevice));
   for (uint32_t i = 0; i < n; i++) w->info[first + i] = info[i];
+  // a released slot rewritten with a live joint is taken again
+  w->freeSlots.erase(std::remove_if(w->freeSlots.begin(), w->freeSlots.end(),
+                                    [&](uint32_t s) { return s >= first && s - first < n && w->info[s].type != AVBD_T_NONE; }),
+                     w->freeSlots.end());
   return AVBD_OK;
 }
 
