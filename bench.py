@@ -374,6 +374,9 @@ def run_adjoint(args, R, torch) -> dict:
     backward = e0.elapsed_time(e1)
     barrier()
     fwd_rec, replay, backward = R.max([fwd_rec, replay, backward])
+    # the whole job's per-world losses and gradients on every rank (one all-gather each)
+    losses_all = R.all_gather(np.asarray(loss_b, dtype=np.float64))
+    grads_all = R.all_gather(np.asarray(grad, dtype=np.float64))
     # central differences of the replay along a random direction, 32 sampled worlds
     fb = adj.first_body.astype(np.int64)
     d = rng.normal(0, 1, p0.shape)
@@ -406,7 +409,8 @@ def run_adjoint(args, R, torch) -> dict:
         'metric': 'adjoint/forward time ratio', 'value': (replay + backward) / fwd_rec, 'unit': 'x', 'higher_is_better': False,
         'forward_fp32_ms': fwd_plain, 'forward_fp32_recording_ms': fwd_rec, 'replay_fp64_ms': replay, 'reverse_fp64_ms': backward,
         'ratio_reverse_to_forward': backward / fwd_rec, 'ratio_replay_plus_reverse_to_forward': (replay + backward) / fwd_rec,
-        'loss_mean': float(np.mean(loss_b)), 'gradient_finite': bool(np.isfinite(grad).all()),
+        'loss_mean': float(np.mean(losses_all)), 'gradient_finite': bool(np.isfinite(grads_all).all()),
+        'gathered': {'worlds': int(losses_all.size), 'gradient_values': int(grads_all.size)},
         'fd_check': {'worlds': len(sample), 'h': h, 'direction': 'random per world (v0, omega0 unit scale; mass 0.1; friction 0.05)',
                      'smooth_worlds': len(rel), 'max_rel_err_smooth': float(max(rel)) if rel else None,
                      'median_rel_err': float(np.median(rel_all)), 'max_rel_err_all': float(max(rel_all)),

@@ -22,7 +22,8 @@ def _rank_main(rank: int, world: int, port: int, out):
     try:
         R.barrier()
         mx = R.max([1.5 + rank, 10.0 - rank, 3.0])
-        out.put((rank, R.world_size, mx, R.seed(500), R.rate(1000.0, mx[0])))
+        g = R.all_gather([float(rank), rank + 0.5, -1.0])
+        out.put((rank, R.world_size, mx, R.seed(500), R.rate(1000.0, mx[0]), g.tolist()))
         R.barrier()
     finally:
         R.close()
@@ -39,11 +40,12 @@ def test_two_ranks_reduce_timings_and_rates():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, world, mx, seed, rate in res:
+    for rank, world, mx, seed, rate, g in res:
         assert world == 2
         assert mx == [2.5, 10.0, 3.0]          # every rank sees the slowest rank's times
         assert seed == 500 + rank              # replicas draw their own inputs
         assert rate == pytest.approx(2 * 1000.0 / 2.5e-3)  # all ranks' units over the slowest time
+        assert g == [[0.0, 0.5, -1.0], [1.0, 1.5, -1.0]]     # every rank's values, in rank order
 
 
 def test_one_rank_without_environment():
@@ -53,5 +55,6 @@ def test_one_rank_without_environment():
     R = Ranks.from_env('gloo')
     assert (R.rank, R.world_size, R.dist) == (0, 1, None)
     assert R.max([4.0, 2.0]) == [4.0, 2.0]
+    assert R.all_gather([1.0, 2.0]).tolist() == [[1.0, 2.0]]
     R.barrier()
     R.close()

@@ -3,9 +3,10 @@ barrier, the maximum over ranks of per-rank device times, per-rank seeds and who
 
 A single world does not shard (every colour is a Gauss-Seidel pass over the whole world and contacts
 cross any cut), so N GPUs run replicas: each rank steps its own world or its own batch of worlds,
-and no collective touches the simulation data. The only collectives are the barrier and the
-reduction of the timings, so that a whole-job rate divides all ranks' work by the slowest rank's
-time. NCCL on GPUs; gloo serves the same calls on CPU processes (the tests)."""
+and no collective touches the simulation data while it steps. The collectives are the barrier, the
+reduction of the timings (a whole-job rate divides all ranks' work by the slowest rank's time), and,
+after a differentiated rollout, one all-gather of every rank's per-world losses and gradients. NCCL
+on GPUs; gloo serves the same calls on CPU processes (the tests)."""
 
 from __future__ import annotations
 
@@ -53,6 +54,21 @@ class Ranks:
         if self.dist is not None:
             self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return [float(x) for x in t.tolist()]
+
+    def all_gather(self, values) -> 'np.ndarray':
+        """Every rank's `values` (the same shape and dtype on each rank), stacked in rank order:
+        shape (world_size, *values.shape), on every rank. One all-gather."""
+        import numpy as np
+        a = np.ascontiguousarray(values)
+        if self.dist is None:
+            return a[None].copy()
+        import torch
+        t = torch.from_numpy(a.copy())
+        if self.device is not None:
+            t = t.to(self.device)
+        out = [torch.empty_like(t) for _ in range(self.world_size)]
+        self.dist.all_gather(out, t)
+        return torch.stack(out).cpu().numpy()
 
     def seed(self, base: int) -> int:
         """A rank's own seed for its replica's synthetic inputs."""
