@@ -1,7 +1,7 @@
 // CPU oracle for the 3D AVBD step: TEST INFRASTRUCTURE ONLY.
 //
 // A C++ restatement of three-avbd's CPU reference (src/avbd3d/ref/*.ts), templated on the
-// floating type. It is the checker the CUDA backend is compared against; nothing in the product
+// floating type. The CUDA backend is compared against it in the tests; nothing in the product
 // links, includes or calls it. Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
 // leg load it (through ctypes).
 //
