@@ -148,6 +148,23 @@ def cpu_reference(n_bodies: int, steps: int, threads: int, warmup: int = 0) -> d
                       f'C++ oracle in double (GPU-mode rules), {used} OpenMP threads'}
 
 
+def cpu_upstream(n_bodies: int, steps: int) -> dict:
+    """The oracle in the reference CPU solver's own order (ref/solver.ts:137-223: all-pairs
+    broadphase, bodies and forces newest first, one Gauss-Seidel pass) on one thread, steps
+    1..`steps` of the sampled pile's rollout."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    from avbd_b200.scenes import drop_pile
+    from oracle import Oracle, set_threads
+    used = set_threads(1)
+    o = Oracle(drop_pile(n_bodies, seed=1))
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return {'value': n_bodies * steps / dt, 'unit': UNIT, 'cores': used, 'seconds': dt,
+            'sample': f'drop pile generator at {n_bodies} bodies, steps 1..{steps}, C++ oracle in double in the reference '
+                      'CPU solver\'s order (upstream mode), 1 thread'}
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -559,6 +576,8 @@ def main():
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         ref = cpu_reference(SAMPLE_BODIES, ROLLOUT, os.cpu_count() or 1)
         cpu = {k: ref[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        up = cpu_upstream(SAMPLE_BODIES, ROLLOUT)
+        cpu['upstream_order_1_thread'] = {k: up[k] for k in ('value', 'unit', 'cores', 'sample')}
 
     if rank == 0:
         name = avbd_b200.device_info(local)
