@@ -39,6 +39,7 @@ PILE_BODIES = 100_000
 SAMPLE_BODIES = 2_000
 PILE_SPACING = 2.7
 ROLLOUT = 600
+NOMINAL_HBM_GBS = 7700.0  # HGX B200 HBM3e, for context beside the measured copy bandwidth
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -586,7 +587,8 @@ def main():
             'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
             'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps), parallelism=f'replicas x{world_size}', spacing=args.spacing),
             'roofline': {'bound': 'hbm', 'kernel': 'k_topology_solve', 'achieved': achieved, 'peak': peak, 'peak_kind': peak_kind, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / max(len(stats), 1)},
+                         'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / max(len(stats), 1),
+                         'peak_nominal': NOMINAL_HBM_GBS, 'frac_nominal': achieved / NOMINAL_HBM_GBS},
             'phases_ms_per_step': {'collision': coll_ms / max(len(stats), 1), 'topology_solve': solve_ms / max(len(stats), 1)},
             'pile_last_step': dict({k: int(stats[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors', 'dynamic_bodies', 'adjacency', 'incidences')},
                                    alg_bytes=alg_bytes(stats[-1])) if len(stats) else None,
