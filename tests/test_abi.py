@@ -62,5 +62,15 @@ def test_create_fails_loudly_without_a_b200():
         has_gpu = False
     if has_gpu:
         pytest.skip('a GPU is present')
-    with pytest.raises(avbd_b200.AvbdError):
+    with pytest.raises(avbd_b200.DeviceError):
         avbd_b200.CudaSolver3D(avbd_b200.scenes.demo_scene('Ground'))
+
+
+def test_statuses_map_to_the_reference_errors():
+    e = _abi.error(_abi.AVBD_ERR_CAPACITY, 'body capacity 4 reached')
+    assert isinstance(e, avbd_b200.StorageCapacityError) and isinstance(e, avbd_b200.AvbdError) and e.code == _abi.AVBD_ERR_CAPACITY
+    assert isinstance(_abi.error(_abi.AVBD_ERR_NO_DEVICE, ''), avbd_b200.DeviceError)
+    assert isinstance(_abi.error(_abi.AVBD_ERR_CUDA, ''), avbd_b200.DeviceError)
+    assert isinstance(_abi.error(_abi.AVBD_ERR_TIMEOUT, ''), avbd_b200.DeviceTimeout)
+    e = _abi.error(_abi.AVBD_ERR_INVALID, 'joint 0: NaN')
+    assert type(e) is avbd_b200.AvbdError and 'joint 0: NaN' in str(e)

@@ -225,9 +225,30 @@ def load(path: str = LIB_PATH):
 
 
 class AvbdError(RuntimeError):
+    """A negative status of the C ABI (the reference throws `Error` before any state change)."""
+
     def __init__(self, code: int, message: str):
         super().__init__(f'avbd error {code}: {message}')
         self.code = code
+
+
+class StorageCapacityError(AvbdError):
+    """AVBD_ERR_CAPACITY: a fixed capacity would be passed (src/lib/storage-budget.ts:32-42)."""
+
+
+class DeviceError(AvbdError):
+    """AVBD_ERR_CUDA / AVBD_ERR_NO_DEVICE: the device failed or is missing (World's gpuError, world.ts:874-877)."""
+
+
+class DeviceTimeout(AvbdError):
+    """AVBD_ERR_TIMEOUT: a bounded device wait gave up; the step's results are not valid."""
+
+
+def error(code: int, message: str) -> AvbdError:
+    """The exception for a C-ABI status."""
+    kind = {AVBD_ERR_CAPACITY: StorageCapacityError, AVBD_ERR_CUDA: DeviceError, AVBD_ERR_NO_DEVICE: DeviceError,
+            AVBD_ERR_TIMEOUT: DeviceTimeout}.get(code, AvbdError)
+    return kind(code, message)
 
 
 def ptr(a: np.ndarray):

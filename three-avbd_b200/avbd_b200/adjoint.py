@@ -14,7 +14,6 @@ import ctypes
 import numpy as np
 
 from . import _abi
-from ._abi import AvbdError
 
 
 class AdjointDesc(ctypes.Structure):
@@ -122,7 +121,7 @@ class Adjoint:
         self.handle = ctypes.c_void_p()
         code = self.lib.avbd_adjoint_create(ctypes.byref(d), ctypes.byref(self.handle))
         if code != _abi.AVBD_OK:
-            raise AvbdError(code, 'avbd_adjoint_create failed')
+            raise _abi.error(code, 'avbd_adjoint_create failed')
         self.worlds, self.bodies = c['W'], c['nb']
         self.first_body = c['first_body']
 
@@ -137,7 +136,7 @@ class Adjoint:
         code = self.lib.avbd_adjoint_create_from_batch(batch.handle, checkpoint, ctypes.byref(self.handle))
         if code != _abi.AVBD_OK:
             msg = self.lib.avbd_batch_last_error(batch.handle)
-            raise AvbdError(code, 'avbd_adjoint_create_from_batch: ' + (msg.decode() if msg else ''))
+            raise _abi.error(code, 'avbd_adjoint_create_from_batch: ' + (msg.decode() if msg else ''))
         info = self.info()
         self.worlds, self.bodies = info['worlds'], info['bodies']
         self.first_body = np.array([batch.world_info(w)['first_body'] for w in range(self.worlds)] + [self.bodies], np.uint32)
@@ -182,7 +181,7 @@ class Adjoint:
     def _check(self, code):
         if code != _abi.AVBD_OK:
             msg = self.lib.avbd_adjoint_last_error(self.handle)
-            raise AvbdError(code, msg.decode() if msg else '')
+            raise _abi.error(code, msg.decode() if msg else '')
 
     def set_target(self, target: np.ndarray):
         t = np.ascontiguousarray(target, np.float64).reshape(-1)

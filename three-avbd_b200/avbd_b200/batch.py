@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 
 from . import _abi
-from ._abi import BODY_DTYPE, INFO_DTYPE, JOINT_DTYPE, AvbdError, BatchConfig, BatchStatus, BatchTuning, BatchWorld, Counters, ptr, uptr
+from ._abi import BODY_DTYPE, INFO_DTYPE, JOINT_DTYPE, BatchConfig, BatchStatus, BatchTuning, BatchWorld, Counters, ptr, uptr
 from .scenes import Scene
 from .solver import CudaSolver3D, scene_records, to_params
 
@@ -29,7 +29,7 @@ class BatchSolver3D:
         self.handle = ctypes.c_void_p()
         code = self.lib.avbd_batch_create(ctypes.byref(cfg), ctypes.byref(self.handle))
         if code != _abi.AVBD_OK:
-            raise AvbdError(code, 'avbd_batch_create failed (a B200 with the CUDA library is required; there is no CPU fallback)')
+            raise _abi.error(code, 'avbd_batch_create failed (a B200 with the CUDA library is required; there is no CPU fallback)')
         if params is not None:
             self.set_params(params)
 
@@ -47,7 +47,7 @@ class BatchSolver3D:
     def _check(self, code: int):
         if code != _abi.AVBD_OK:
             msg = self.lib.avbd_batch_last_error(self.handle)
-            raise AvbdError(code, msg.decode() if msg else '')
+            raise _abi.error(code, msg.decode() if msg else '')
 
     def set_params(self, sp):
         self._check(self.lib.avbd_batch_set_params(self.handle, ctypes.byref(to_params(sp))))

@@ -163,7 +163,7 @@ class CudaSolver3D:
         self.handle = ctypes.c_void_p()
         code = self.lib.avbd_world_create(ctypes.byref(cfg), ctypes.byref(self.handle))
         if code != _abi.AVBD_OK:
-            raise AvbdError(code, 'avbd_world_create failed (a B200 with the CUDA library is required; there is no CPU fallback)')
+            raise _abi.error(code, 'avbd_world_create failed (a B200 with the CUDA library is required; there is no CPU fallback)')
         self.order = np.arange(n)
         self.gpu_index = np.arange(n)
         self.fixed_colors = None
@@ -196,7 +196,7 @@ class CudaSolver3D:
     def _check(self, code: int):
         if code != _abi.AVBD_OK:
             msg = self.lib.avbd_last_error(self.handle)
-            raise AvbdError(code, msg.decode() if msg else '')
+            raise _abi.error(code, msg.decode() if msg else '')
 
     # --- params (GpuParams3D) ---
     @property
@@ -484,7 +484,7 @@ def find_pairs_noalloc(bodies: np.ndarray, groups_mask: np.ndarray | None = None
     lib = _abi.load()
     bodies = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
     if len(bodies) > _abi.NOALLOC_MAX_BODIES:
-        raise AvbdError(_abi.AVBD_ERR_CAPACITY, f'avbd_find_pairs_noalloc takes at most {_abi.NOALLOC_MAX_BODIES} bodies, got {len(bodies)}')
+        raise _abi.error(_abi.AVBD_ERR_CAPACITY, f'avbd_find_pairs_noalloc takes at most {_abi.NOALLOC_MAX_BODIES} bodies, got {len(bodies)}')
     gm = None if groups_mask is None else np.ascontiguousarray(groups_mask, dtype=np.uint32).reshape(-1)
     out = np.zeros(2 * max(cap, 1), dtype=np.uint32)
     count = ctypes.c_uint32()
@@ -492,8 +492,8 @@ def find_pairs_noalloc(bodies: np.ndarray, groups_mask: np.ndarray | None = None
                                        ctypes.c_void_p(stream))
     if code != _abi.AVBD_OK:
         if code == _abi.AVBD_ERR_CAPACITY:
-            raise AvbdError(code, f'{count.value} pairs found, more than the {min(cap, _abi.NOALLOC_MAX_PAIRS)} that fit')
-        raise AvbdError(code, 'avbd_find_pairs_noalloc failed')
+            raise _abi.error(code, f'{count.value} pairs found, more than the {min(cap, _abi.NOALLOC_MAX_PAIRS)} that fit')
+        raise _abi.error(code, 'avbd_find_pairs_noalloc failed')
     return out[:2 * count.value].reshape(-1, 2)
 
 
