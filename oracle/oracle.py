@@ -183,7 +183,16 @@ class Oracle:
     def body_count(self):
         return self.L.orc_body_count(self.h)
 
+    def _body_index(self, i):
+        if not 0 <= i < self.body_count:
+            raise IndexError(f'body {i} of {self.body_count}')
+
+    def _joint_index(self, i):
+        if not 0 <= i < self.force_count or int(self.force(i)[0]) != K_JOINT:
+            raise IndexError(f'force {i} is not a joint')
+
     def body(self, i) -> np.ndarray:
+        self._body_index(i)
         r = np.zeros(BODY_REC)
         self.L.orc_get_body(self.h, i, _dp(r))
         return r
@@ -192,6 +201,7 @@ class Oracle:
         return np.stack([self.body(i) for i in range(self.body_count)]) if self.body_count else np.zeros((0, BODY_REC))
 
     def set_body(self, i, rec):
+        self._body_index(i)
         rec = np.ascontiguousarray(rec, dtype=np.float64)
         self.L.orc_set_body(self.h, i, _dp(rec))
 
@@ -200,16 +210,20 @@ class Oracle:
         return self.L.orc_force_count(self.h)
 
     def force(self, i) -> np.ndarray:
+        if not 0 <= i < self.force_count:
+            raise IndexError(f'force {i} of {self.force_count}')
         r = np.zeros(FORCE_REC)
         self.L.orc_get_force(self.h, i, _dp(r))
         return r
 
     def set_joint(self, i, rec):
+        self._joint_index(i)
         rec = np.ascontiguousarray(rec, dtype=np.float64)
         self.L.orc_set_joint(self.h, i, _dp(rec))
 
     def set_joint_anchor(self, i, p):
         """setWorldAnchor: joint i's rA (its world point when it has no body A)."""
+        self._joint_index(i)
         q = np.ascontiguousarray(p, dtype=np.float64)
         self.L.orc_set_joint_anchor(self.h, i, _dp(q))
 
