@@ -286,6 +286,13 @@ int avbd_use_graphs(avbd_world* world, int enable);
  * the last bits between launch shapes; one block reproduces a batched world's step bit for bit. */
 int avbd_set_solve_blocks(avbd_world* world, int blocks);
 
+/* The broadphase's classification of bodies by bounding radius (gpu/radii.ts largestSmall, and
+ * uploadStatics, gpu/solver.ts:1263-1318): the largest radius still small (at most 2 x the median,
+ * or, past 64 larger bodies, the largest left), which sizes the grid cells (2 x it), and the radius
+ * above which a body is "large" and tested against every body (halfway to the smallest large one).
+ * Host code (no device needed). */
+int avbd_broadphase_radii(const double* radii, uint32_t n, double* largest_small, double* large_threshold);
+
 /* The world's CUDA stream (cudaStream_t) for callers that order their own device work with its steps. */
 int avbd_world_stream(avbd_world* world, void** stream);
 

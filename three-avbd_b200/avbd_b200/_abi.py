@@ -137,6 +137,7 @@ SIGNATURES = {
     'avbd_add_joints': ([P, VP, VP, U, PU], I),
     'avbd_write_joints': ([P, U, VP, VP, U], I),
     'avbd_release_joints': ([P, PU, U], I),
+    'avbd_broadphase_radii': ([ctypes.POINTER(ctypes.c_double), U, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], I),
     'avbd_append_joints': ([P, VP, VP, U, PU], I),
     'avbd_disable_joints': ([P, PU, U], I),
     'avbd_add_world_joint': ([P, U, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), PU], I),

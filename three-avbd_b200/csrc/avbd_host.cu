@@ -1225,6 +1225,16 @@ int avbd_hull_storage(const avbd_world* w, uint32_t* top, uint32_t* capacity, ui
   return AVBD_OK;
 }
 
+int avbd_broadphase_radii(const double* radii, uint32_t n, double* largest_small, double* large_threshold) {
+  if (n && !radii) return AVBD_ERR_INVALID;
+  std::vector<double> r(radii, radii + n);
+  for (double x : r)
+    if (!std::isfinite(x) || x < 0.0) return AVBD_ERR_INVALID;
+  if (largest_small) *largest_small = largestSmall(r);
+  if (large_threshold) *large_threshold = largeThreshold(r);
+  return AVBD_OK;
+}
+
 int avbd_world_stream(avbd_world* w, void** stream) {
   if (!w || !stream) return AVBD_ERR_INVALID;
   *stream = (void*)w->stream;
