@@ -195,7 +195,9 @@ int avbd_set_filters(avbd_world* world, uint32_t first, const uint32_t* groups_m
 /* setBodyAux(indices, scales, linear?, angular?) (gpu/solver.ts:1814-1845; record layout.ts:33-46):
  * per-slot gravity scale (default 1) and linear / angular damping rates in 1/s (default 0; a
  * dynamic body's incoming velocities decay by exp(-rate dt) once per step, before its inertial
- * target). linear and angular: both NULL (only the scales change) or both given. */
+ * target). linear and angular: both given, or both NULL, when a lone slot (no consecutive
+ * neighbour in `indices`) keeps its rates and a run of consecutive slots gets the default rates, as
+ * setBodyAux writes whole records for runs (:1826-1845). */
 int avbd_set_body_aux(avbd_world* world, const uint32_t* indices, uint32_t n, const float* scales, const float* linear, const float* angular);
 /* The aux records of slots first .. first + n - 1: 4 floats each (scale, linear, angular, 0). */
 int avbd_read_body_aux(avbd_world* world, uint32_t first, float* aux4, uint32_t n);

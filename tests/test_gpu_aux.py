@@ -80,3 +80,17 @@ def test_cold_body_joints_start_afresh(cuda_lib):
     with pytest.raises(avbd_b200.AvbdError):
         w.set_lifecycle(3, 1)  # only the disabled and cold bits
     w.destroy()
+
+
+def test_runs_without_rates_take_the_default_rates(cuda_lib):
+    """setBodyAux without rates (gpu/solver.ts:1826-1845): a lone slot changes only its gravity
+    scale; a run of consecutive slots gets whole records with the default rates (0)."""
+    w = avbd_b200.CudaSolver3D(demo_scene('Stack'))
+    w.set_body_aux([1, 2, 3, 5], [0.5] * 4, [1.0] * 4, [2.0] * 4)
+    w.set_body_aux([1, 2, 5], [0.25, 0.75, 3.0])
+    aux = w.read_body_aux()
+    assert np.allclose(aux[1], [0.25, 0.0, 0.0, 0.0]) and np.allclose(aux[2], [0.75, 0.0, 0.0, 0.0])
+    assert np.allclose(aux[3], [0.5, 1.0, 2.0, 0.0])
+    assert np.allclose(aux[5], [3.0, 1.0, 2.0, 0.0])
+    assert np.allclose(aux[4], [1.0, 0.0, 0.0, 0.0])  # untouched: the defaults
+    w.destroy()

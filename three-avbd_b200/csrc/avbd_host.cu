@@ -775,16 +775,23 @@ int avbd_set_body_aux(avbd_world* w, const uint32_t* indices, uint32_t n, const 
   }
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  for (uint32_t k = 0; k < n; k++) {
-    // without rates only the gravity scale changes (setBodyAux writes the one word)
-    float4 rec;
-    if (linear) {
-      rec = make_float4(scales[k], linear[k], angular[k], 0.0f);
-    } else {
+  // As setBodyAux writes them (gpu/solver.ts:1826-1845): a lone slot without rates changes only its
+  // gravity scale; otherwise each run of consecutive slots gets whole records, with the default
+  // rates (0) where none are given
+  for (uint32_t k = 0; k < n;) {
+    uint32_t e = k + 1;
+    while (e < n && indices[e] == indices[e - 1] + 1) e++;
+    if (e - k == 1 && !linear) {
+      float4 rec;
       CUDA_TRY(w, cudaMemcpy(&rec, w->d.aux + indices[k], sizeof(float4), cudaMemcpyDeviceToHost));
       rec.x = scales[k];
+      CUDA_TRY(w, cudaMemcpy(w->d.aux + indices[k], &rec, sizeof(float4), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float4> run(e - k);
+      for (uint32_t i = k; i < e; i++) run[i - k] = make_float4(scales[i], linear ? linear[i] : 0.0f, linear ? angular[i] : 0.0f, 0.0f);
+      CUDA_TRY(w, cudaMemcpy(w->d.aux + indices[k], run.data(), run.size() * sizeof(float4), cudaMemcpyHostToDevice));
     }
-    CUDA_TRY(w, cudaMemcpy(w->d.aux + indices[k], &rec, sizeof(float4), cudaMemcpyHostToDevice));
+    k = e;
   }
   return AVBD_OK;
 }
