@@ -192,6 +192,8 @@ int avbd_set_world_anchor(avbd_world* world, uint32_t slot, const float p[3]);
 int avbd_add_ignore_pairs(avbd_world* world, const uint32_t* pairs_ab, uint32_t n);
 /* setFilters (gpu/solver.ts): groups_mask[2i] = groups, [2i+1] = collides-with mask. */
 int avbd_set_filters(avbd_world* world, uint32_t first, const uint32_t* groups_mask, uint32_t n);
+/* setFilters(indices, groups, collidesWith) (gpu/solver.ts:1791-1801) for any list of slots. */
+int avbd_set_filters_at(avbd_world* world, const uint32_t* indices, const uint32_t* groups, const uint32_t* collides_with, uint32_t n);
 /* setBodyAux(indices, scales, linear?, angular?) (gpu/solver.ts:1814-1845; record layout.ts:33-46):
  * per-slot gravity scale (default 1) and linear / angular damping rates in 1/s (default 0; a
  * dynamic body's incoming velocities decay by exp(-rate dt) once per step, before its inertial

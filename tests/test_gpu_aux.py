@@ -94,3 +94,26 @@ def test_runs_without_rates_take_the_default_rates(cuda_lib):
     assert np.allclose(aux[5], [3.0, 1.0, 2.0, 0.0])
     assert np.allclose(aux[4], [1.0, 0.0, 0.0, 0.0])  # untouched: the defaults
     w.destroy()
+
+
+def test_filters_by_slot_list_equal_filters_by_range(cuda_lib):
+    """setFilters(indices, groups, collidesWith) (gpu/solver.ts:1791-1801) over a list of slots in any
+    order (runs and scattered slots) writes what a contiguous write of the same values writes."""
+    scene = demo_scene('Pyramid')
+    n = len(scene.bodies)
+    rng = np.random.default_rng(4)
+    groups = rng.integers(1, 4, n).astype(np.uint32)
+    masks = np.where(rng.uniform(size=n) < 0.5, 0xFFFFFFFF, 0xFFFFFFFE).astype(np.uint32)
+    a, b, c = (avbd_b200.CudaSolver3D(scene) for _ in range(3))
+    a.set_filters(0, np.stack([groups, masks], axis=1))
+    order = np.concatenate([np.arange(0, 10), 10 + rng.permutation(n - 10)])
+    b.set_filters_at(order, groups[order], masks[order])
+    for w in (a, b, c):
+        w.step(5)
+    pairs = [{tuple(p) for p in w.read_pairs().tolist()} for w in (a, b, c)]
+    assert pairs[0] == pairs[1] and pairs[0] != pairs[2]
+    assert a.read_bodies().tobytes() == b.read_bodies().tobytes()
+    with pytest.raises(avbd_b200.AvbdError):
+        b.set_filters_at([n], [1], [1])
+    for w in (a, b, c):
+        w.destroy()

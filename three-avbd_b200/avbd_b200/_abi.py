@@ -146,6 +146,7 @@ SIGNATURES = {
     'avbd_contact_storage': ([P, U, ctypes.POINTER(ContactView)], I),
     'avbd_add_ignore_pairs': ([P, PU, U], I),
     'avbd_set_filters': ([P, U, PU, U], I),
+    'avbd_set_filters_at': ([P, PU, PU, PU, U], I),
     'avbd_seed_contacts': ([P, VP, U, VP, U], I),
     'avbd_set_fixed_colors': ([P, PU, U], I),
     'avbd_step': ([P, I], I),

@@ -314,6 +314,13 @@ class CudaSolver3D:
         p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)
         self._check(self.lib.avbd_add_ignore_pairs(self.handle, uptr(p), len(p)))
 
+    def set_filters_at(self, indices, groups, collides_with):
+        """setFilters(indices, groups, collidesWith): any list of slots."""
+        i = np.ascontiguousarray(indices, dtype=np.uint32)
+        g = np.ascontiguousarray(np.asarray(groups, dtype=np.int64) & 0xFFFFFFFF, dtype=np.uint32)
+        m = np.ascontiguousarray(np.asarray(collides_with, dtype=np.int64) & 0xFFFFFFFF, dtype=np.uint32)
+        self._check(self.lib.avbd_set_filters_at(self.handle, uptr(i), uptr(g), uptr(m), len(i)))
+
     def set_filters(self, first: int, groups_mask: np.ndarray):
         g = np.ascontiguousarray(groups_mask, dtype=np.uint32).reshape(-1, 2)
         self._check(self.lib.avbd_set_filters(self.handle, first, uptr(g), len(g)))

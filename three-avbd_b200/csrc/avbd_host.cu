@@ -756,6 +756,25 @@ int avbd_add_ignore_pairs(avbd_world* w, const uint32_t* ab, uint32_t n) {
   return AVBD_OK;
 }
 
+// setFilters(indices, groups, collidesWith) (gpu/solver.ts:1791-1801): one write per run of
+// consecutive slots
+int avbd_set_filters_at(avbd_world* w, const uint32_t* indices, const uint32_t* groups, const uint32_t* collides_with, uint32_t n) {
+  if (!w || (n && (!indices || !groups || !collides_with))) return AVBD_ERR_INVALID;
+  for (uint32_t k = 0; k < n; k++)
+    if (indices[k] >= w->n) return fail(w, AVBD_ERR_INVALID, "setFilters: slot " + std::to_string(indices[k]) + " is not a body of the world");
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  for (uint32_t k = 0; k < n;) {
+    uint32_t e = k + 1;
+    while (e < n && indices[e] == indices[e - 1] + 1) e++;
+    std::vector<uint2> run(e - k);
+    for (uint32_t i = k; i < e; i++) run[i - k] = make_uint2(groups[i], collides_with[i]);
+    CUDA_TRY(w, cudaMemcpy(w->d.filters + indices[k], run.data(), run.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    k = e;
+  }
+  return AVBD_OK;
+}
+
 int avbd_set_filters(avbd_world* w, uint32_t first, const uint32_t* gm, uint32_t n) {
   if (!w || (n && !gm) || uint64_t(first) + n > w->n) return AVBD_ERR_INVALID;
   cudaSetDevice(w->device);
