@@ -824,7 +824,8 @@ int avbd_read_body_aux(avbd_world* w, uint32_t first, float* aux4, uint32_t n) {
 }
 
 int avbd_set_lifecycle(avbd_world* w, uint32_t index, uint32_t bits) {
-  if (!w || index >= w->n || (bits & ~6u)) return AVBD_ERR_INVALID;
+  if (!w) return AVBD_ERR_INVALID;
+  if (index >= w->n || (bits & ~6u)) return fail(w, AVBD_ERR_INVALID, "Invalid body lifecycle flags/index");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   // the lifecycle word is the initial pose's w (layout.ts:17-19); a rewritten slot has no contact history
