@@ -776,7 +776,8 @@ int avbd_set_filters_at(avbd_world* w, const uint32_t* indices, const uint32_t* 
 }
 
 int avbd_set_filters(avbd_world* w, uint32_t first, const uint32_t* gm, uint32_t n) {
-  if (!w || (n && !gm) || uint64_t(first) + n > w->n) return AVBD_ERR_INVALID;
+  if (!w || (n && !gm)) return AVBD_ERR_INVALID;
+  if (uint64_t(first) + n > w->n) return fail(w, AVBD_ERR_INVALID, "setFilters: slots outside the world's bodies");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   CUDA_TRY(w, cudaMemcpy(w->d.filters + first, gm, size_t(n) * sizeof(uint2), cudaMemcpyHostToDevice));
@@ -816,7 +817,8 @@ int avbd_set_body_aux(avbd_world* w, const uint32_t* indices, uint32_t n, const 
 }
 
 int avbd_read_body_aux(avbd_world* w, uint32_t first, float* aux4, uint32_t n) {
-  if (!w || (n && !aux4) || uint64_t(first) + n > w->bodyCap) return AVBD_ERR_INVALID;
+  if (!w || (n && !aux4)) return AVBD_ERR_INVALID;
+  if (uint64_t(first) + n > w->bodyCap) return fail(w, AVBD_ERR_INVALID, "aux records outside the body capacity");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   CUDA_TRY(w, cudaMemcpy(aux4, w->d.aux + first, size_t(n) * sizeof(float4), cudaMemcpyDeviceToHost));
