@@ -165,6 +165,9 @@ int avbd_add_bodies(avbd_world* world, const avbd_body* bodies, uint32_t n, uint
 /* rewriteBodies / patchBody (gpu/solver.ts:1113-1139): overwrite bodies [first, first+n);
  * keep_contacts != 0 keeps their contact history (seedFrom), else the slots start fresh. */
 int avbd_write_bodies(avbd_world* world, uint32_t first, const avbd_body* bodies, uint32_t n, int keep_contacts);
+/* rewriteBodies(indices, bodies) (gpu/solver.ts:1774-1784) for any list of existing slots: every
+ * record is checked before any is written; each slot starts afresh. */
+int avbd_write_bodies_at(avbd_world* world, const uint32_t* indices, const avbd_body* bodies, uint32_t n);
 /* appendJoints / appendSprings (gpu/solver.ts:1484-1533): appends slots; *first = first slot. */
 int avbd_add_joints(avbd_world* world, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* first);
 /* seedFrom's joint rewrite (gpu/solver.ts:1330-1331). */

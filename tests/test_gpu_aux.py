@@ -117,3 +117,32 @@ def test_filters_by_slot_list_equal_filters_by_range(cuda_lib):
         b.set_filters_at([n], [1], [1])
     for w in (a, b, c):
         w.destroy()
+
+
+def test_rewrite_bodies_by_slot_list_equals_range_writes(cuda_lib):
+    """rewriteBodies(indices, bodies) (gpu/solver.ts:1774-1784): a list of slots in runs writes what
+    range writes of the same records write; a bad record refuses the whole call."""
+    scene = demo_scene('Pyramid')
+    a, b = avbd_b200.CudaSolver3D(scene), avbd_b200.CudaSolver3D(scene)
+    for w in (a, b):
+        w.step(20)
+    recs = a.read_bodies()
+    idx = np.array([3, 4, 5, 6, 9, 20, 21])
+    new = recs[idx].copy()
+    new['pos'][:, 2] += 0.5
+    new['vel'][:, 0] = 1.0
+    a.write_bodies(3, new[:4])
+    a.write_bodies(9, new[4:5])
+    a.write_bodies(20, new[5:])
+    b.write_bodies_at(idx, new)
+    for w in (a, b):
+        w.step(10)
+    assert a.read_bodies().tobytes() == b.read_bodies().tobytes()
+    bad = new.copy()
+    bad['pos'][3, 0] = np.nan
+    before = b.read_bodies().tobytes()
+    with pytest.raises(avbd_b200.AvbdError):
+        b.write_bodies_at(idx, bad)
+    assert b.read_bodies().tobytes() == before
+    for w in (a, b):
+        w.destroy()

@@ -134,6 +134,7 @@ SIGNATURES = {
     'avbd_default_params': ([ctypes.POINTER(Params)], I),
     'avbd_add_bodies': ([P, VP, U, PU], I),
     'avbd_write_bodies': ([P, U, VP, U, I], I),
+    'avbd_write_bodies_at': ([P, PU, VP, U], I),
     'avbd_add_joints': ([P, VP, VP, U, PU], I),
     'avbd_write_joints': ([P, U, VP, VP, U], I),
     'avbd_release_joints': ([P, PU, U], I),

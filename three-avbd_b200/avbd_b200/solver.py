@@ -250,6 +250,12 @@ class CudaSolver3D:
         records = np.ascontiguousarray(records, dtype=BODY_DTYPE)
         self._check(self.lib.avbd_write_bodies(self.handle, first, ptr(records), len(records), 1 if keep_contacts else 0))
 
+    def write_bodies_at(self, indices, records: np.ndarray):
+        """rewriteBodies(indices, bodies): any existing slots, each starting afresh."""
+        i = np.ascontiguousarray(indices, dtype=np.uint32)
+        records = np.ascontiguousarray(records, dtype=BODY_DTYPE)
+        self._check(self.lib.avbd_write_bodies_at(self.handle, uptr(i), ptr(records), len(i)))
+
     def add_joints(self, records: np.ndarray, info: np.ndarray) -> int:
         records = np.ascontiguousarray(records, dtype=JOINT_DTYPE)
         info = np.ascontiguousarray(info, dtype=INFO_DTYPE)

@@ -604,6 +604,24 @@ int avbd_write_bodies(avbd_world* w, uint32_t first, const avbd_body* bodies, ui
   return AVBD_OK;
 }
 
+// rewriteBodies(indices, bodies) (gpu/solver.ts:1774-1784): every record checked first, then one
+// write per run of consecutive slots, each slot starting afresh (no contact history, no colour)
+int avbd_write_bodies_at(avbd_world* w, const uint32_t* indices, const avbd_body* bodies, uint32_t n) {
+  if (!w || (n && (!indices || !bodies))) return AVBD_ERR_INVALID;
+  for (uint32_t k = 0; k < n; k++)
+    if (indices[k] >= w->n) return fail(w, AVBD_ERR_INVALID, "rewriteBodies: slot " + std::to_string(indices[k]) + " is not a body of the world");
+  int r = checkBodies(w, bodies, n);
+  if (r) return r;
+  for (uint32_t k = 0; k < n;) {
+    uint32_t e = k + 1;
+    while (e < n && indices[e] == indices[e - 1] + 1) e++;
+    r = avbd_write_bodies(w, indices[k], bodies + k, e - k, 0);
+    if (r) return r;
+    k = e;
+  }
+  return AVBD_OK;
+}
+
 static int checkJoints(avbd_world* w, const avbd_joint* j, const avbd_joint_info* info, uint32_t n) {
   std::string msg = jointProblem(j, info, n, w->n);
   return msg.empty() ? AVBD_OK : fail(w, AVBD_ERR_INVALID, msg);
