@@ -56,3 +56,22 @@ def test_workload_config_names_the_pile():
 def test_cpu_baselines_on_a_tiny_sample(fn):
     r = bench.cpu_reference(60, 5, 2) if fn == 'cpu_reference' else bench.cpu_upstream(60, 5)
     assert r['value'] > 0 and r['unit'] == bench.UNIT and r['cores'] >= 1 and '60 bodies' in r['sample']
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` prints the contract's line on rank 0, nothing on other ranks."""
+    import subprocess
+    env = dict(os.environ, RANK='0', WORLD_SIZE='1')
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--steps', '3', '--warmup', '3'],
+                         capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for key in ('metric', 'value', 'unit', 'n_gpus', 'steps', 'warmup', 'ms_per_step', 'higher_is_better', 'scaling', 'vs_baseline', 'dtype',
+                'data', 'config', 'impl', 'cpu_baseline', 'e2e'):
+        assert key in line, key
+    assert line['impl'] == 'reference' and line['metric'] == bench.METRIC and line['steps'] == 3 and line['warmup'] == 3
+    assert line['e2e']['h2d_bytes_per_step'] == 0 and line['cpu_baseline']['value'] == line['value']
+    env = dict(os.environ, RANK='1', WORLD_SIZE='2')
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--steps', '3', '--warmup', '3'],
+                         capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+    assert out.returncode == 0 and out.stdout.strip() == ''
