@@ -341,11 +341,16 @@ int avbd_write_bodies_async(avbd_world* world, uint32_t first, const avbd_body* 
  * in one fixed device array of AVBD_NOALLOC_SCRATCH_BYTES; it allocates no device or pinned memory.
  * For callers that cannot allocate (a thread querying pairs while steps run on other streams, since
  * cudaMalloc/cudaFree synchronise the device; hosts whose allocator owns all device memory).
- * groups_mask: 2 words per body (groups, mask) or NULL (all collide). Writes up to cap (a, b) pairs,
- * a > b, in no particular order, to pairs_ab and the number found to *count; returns
- * AVBD_ERR_CAPACITY when n is past the maximum or more pairs were found than cap or
- * AVBD_NOALLOC_MAX_PAIRS. Runs on `stream` (a cudaStream_t, NULL: the default stream) of the current
- * device and waits for it. All calls share the fixed array: calls whose GPU work overlaps race. */
+ * groups_mask: NULL (all collide) or 2 x n words, (groups, mask) per body; the buffer must hold all
+ * 2 x n words. Shapes: boxes, spheres and sails (a hull's shape code is refused with
+ * AVBD_ERR_INVALID: this call has no hull buffer). Writes up to cap (a, b) pairs, a > b, in no
+ * particular order, to pairs_ab and the number found to *count; returns AVBD_ERR_CAPACITY when n is
+ * past the maximum (*count 0) or more pairs were found than cap or AVBD_NOALLOC_MAX_PAIRS (*count:
+ * all that were found). Runs on `stream` (a cudaStream_t, NULL: the default stream) of the current
+ * device and waits for it. Every call looks up the fixed array's device address on the current
+ * device; the first call on a device also loads the library's device code there, so make it before
+ * any stream capture on that device. All calls share the fixed array and each clears what it counts
+ * in: calls whose GPU work overlaps (two host threads, two streams) race on it. */
 #define AVBD_NOALLOC_MAX_BODIES 4096u
 #define AVBD_NOALLOC_MAX_PAIRS 32768u
 #define AVBD_NOALLOC_SCRATCH_BYTES 1065472u

@@ -2,12 +2,15 @@
 array) against the world's own broadphase: the pair list a world's step finds for the same bodies
 (avbd_step, then avbd_read_pairs). Collected last; passes alone in a fresh process too."""
 
+import ctypes
+
 import numpy as np
 import pytest
 
 import avbd_b200
-from avbd_b200 import CudaSolver3D, find_pairs_noalloc, scene_records
-from avbd_b200.scenes import drop_pile, small_world
+from avbd_b200 import CudaSolver3D, _abi, find_pairs_noalloc, scene_records
+from avbd_b200._abi import ptr, uptr
+from avbd_b200.scenes import Scene, drop_pile, small_world
 
 pytestmark = pytest.mark.gpu
 
@@ -60,4 +63,48 @@ def test_noalloc_rejects_past_its_limits(cuda_lib):
     with pytest.raises(avbd_b200.AvbdError, match='more than the 10'):
         find_pairs_noalloc(scene_records(dense)[0], cap=10)
     # and the next call is whole again
+    assert _as_set(find_pairs_noalloc(scene_records(dense)[0])) == _world_pairs(dense)
+
+
+def _sphere_lattice(side: int = 16, spacing: float = 0.6, r: float = 0.61) -> Scene:
+    """side^3 spheres whose neighbours up to two lattice steps away overlap: 57372 pairs at 16^3."""
+    s = Scene('sphere lattice')
+    for i in range(side):
+        for j in range(side):
+            for k in range(side):
+                s.sphere(r, 1, 0.5, [i * spacing, j * spacing, 5 + k * spacing])
+    return s
+
+
+def _call(lib, bodies, gm, cap):
+    out = np.zeros(2 * max(cap, 1), dtype=np.uint32)
+    count = ctypes.c_uint32(12345)
+    code = lib.avbd_find_pairs_noalloc(ptr(bodies), len(bodies), uptr(gm) if gm is not None else None, uptr(out), cap, ctypes.byref(count), None)
+    return code, count.value, out
+
+
+def test_noalloc_c_limits(cuda_lib):
+    """The C entry point's own refusals, called directly (the Python guard bypassed): past the body
+    maximum (*count 0), past the pair maximum with a larger cap (*count = every pair found), and a
+    hull shape code (no hull buffer to read it against)."""
+    lib = cuda_lib
+    big = scene_records(drop_pile(_abi.NOALLOC_MAX_BODIES + 1, seed=3, spacing=2.0, layers=4))[0]
+    code, count, _ = _call(lib, big, None, 1024)
+    assert code == _abi.AVBD_ERR_CAPACITY and count == 0
+    lattice = _sphere_lattice()
+    recs = scene_records(lattice)[0]
+    assert len(recs) == _abi.NOALLOC_MAX_BODIES
+    code, count, out = _call(lib, recs, None, 65536)
+    want = _world_pairs(lattice)
+    assert code == _abi.AVBD_ERR_CAPACITY and count == len(want) > _abi.NOALLOC_MAX_PAIRS
+    kept = _as_set(out[:2 * _abi.NOALLOC_MAX_PAIRS].reshape(-1, 2))
+    assert len(kept) == _abi.NOALLOC_MAX_PAIRS and kept <= want  # the pairs that fit are real ones
+    hull = recs[:8].copy()
+    hull['shape'][3] = 3.0
+    code, count, _ = _call(lib, hull, None, 1024)
+    assert code == _abi.AVBD_ERR_INVALID and count == 0
+    with pytest.raises(avbd_b200.AvbdError, match='groups_mask holds'):
+        find_pairs_noalloc(recs[:8], np.ones(8, dtype=np.uint32))
+    # and a whole call afterwards
+    dense, _ = _cases()[0]
     assert _as_set(find_pairs_noalloc(scene_records(dense)[0])) == _world_pairs(dense)

@@ -499,6 +499,8 @@ def find_pairs_noalloc(bodies: np.ndarray, groups_mask: np.ndarray | None = None
     if len(bodies) > _abi.NOALLOC_MAX_BODIES:
         raise _abi.error(_abi.AVBD_ERR_CAPACITY, f'avbd_find_pairs_noalloc takes at most {_abi.NOALLOC_MAX_BODIES} bodies, got {len(bodies)}')
     gm = None if groups_mask is None else np.ascontiguousarray(groups_mask, dtype=np.uint32).reshape(-1)
+    if gm is not None and gm.size != 2 * len(bodies):
+        raise _abi.error(_abi.AVBD_ERR_INVALID, f'groups_mask holds {gm.size} words; (groups, mask) of {len(bodies)} bodies is {2 * len(bodies)}')
     out = np.zeros(2 * max(cap, 1), dtype=np.uint32)
     count = ctypes.c_uint32()
     code = lib.avbd_find_pairs_noalloc(ptr(bodies), len(bodies), uptr(gm) if gm is not None else None, uptr(out), cap, ctypes.byref(count),

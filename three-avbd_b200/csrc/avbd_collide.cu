@@ -1,5 +1,6 @@
 // Collision phase of the B200 AVBD step: last step's pairs into the warm-start hash, cell keys,
-// a stable LSD radix sort of (cell hash, body), cell ranges, pair emission, and the narrowphase.
+// a counting sort of the bodies on their cell hash (a one-digit radix sort, stable by body index),
+// cell ranges, pair emission, and the narrowphase.
 //
 // This file is compiled with --fmad=false: every product and sum is rounded on its own, in the
 // operation order of the reference's WGSL (src/avbd3d/gpu/wgsl-collision.ts), so the pair tests
@@ -8,7 +9,6 @@
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 
-#include <mutex>
 #include <vector>
 
 #include "avbd_device.cuh"
@@ -1601,11 +1601,6 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_find_pairs_noalloc(DWorld w
   }
 }
 
-namespace {
-std::mutex g_noalloc_mutex;
-unsigned char* g_noalloc_ptr[64] = {};
-}  // namespace
-
 }  // namespace avbd
 
 extern "C" int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, const uint32_t* groups_mask, uint32_t* pairs_ab, uint32_t cap,
@@ -1616,19 +1611,18 @@ extern "C" int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, cons
   if ((n && !bodies) || (cap && !pairs_ab) || !count) return AVBD_ERR_INVALID;
   if (n > NOALLOC_MAX_BODIES) return AVBD_ERR_CAPACITY;  // at most AVBD_NOALLOC_MAX_BODIES bodies
   if (!bodyProblem(bodies, n).empty()) return AVBD_ERR_INVALID;
+  // boxes, spheres and sails only: this call has no hull buffer to read a hull's shape code against
+  for (uint32_t i = 0; i < n; i++)
+    if (bodies[i].shape != 0.0f && bodies[i].shape != 1.0f && bodies[i].shape != 2.0f) return AVBD_ERR_INVALID;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return AVBD_ERR_NO_DEVICE;
-  unsigned char* base = nullptr;
-  {
-    // once per device, with that device current: the scratch array's address on it
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-      void* ptr = nullptr;
-      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return AVBD_ERR_CUDA;
-      g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
-    }
-    base = g_noalloc_ptr[dev];
-  }
+  if (cudaGetDevice(&dev) != cudaSuccess) return AVBD_ERR_NO_DEVICE;
+  // The scratch array's address on the current device, looked up on every call (no allocation): in
+  // host code g_noalloc_scratch names a host-side stand-in, and a context torn down and made again
+  // (cudaDeviceReset) may load the module at another address, so no address is kept between calls.
+  // The first call on a device loads the module there; make it before any stream capture.
+  void* scratch = nullptr;
+  if (cudaGetSymbolAddress(&scratch, g_noalloc_scratch) != cudaSuccess || !scratch) return AVBD_ERR_CUDA;
+  unsigned char* base = static_cast<unsigned char*>(scratch);
   if (n == 0) return AVBD_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the broadphase configuration of uploadStatics (solver.ts:1263-1318), from the radii
