@@ -1,23 +1,27 @@
-"""Benchmark of the B200 AVBD step: body-steps/s on the 100k-body drop pile.
+"""Benchmark of the B200 AVBD step: body-steps/s on the 100k-body drop pile, in contact.
 
 A step is one full AVBD step (broadphase, narrowphase, adjacency, colouring, warm starts, 10
-iterations of primal + dual, velocities) of one world. The timed region is steps 1..K of the pile's
-rollout from its starting lattice (600 steps by default: the whole workload), on a fresh world
-after W warm-up steps on another one. Between timed steps a 256 MiB buffer is cleared on the
-world's stream so every step starts with a cold L2 (inside the timed region).
+iterations of primal + dual, velocities) of one world. The pile (100k bodies on a jittered lattice,
+70 % boxes and 30 % spheres, falling onto a static ground) is rolled forward untimed for 200 steps,
+by when every layer has landed and the contact count has levelled off (about 215k manifolds and
+350k points); the last W of those steps are the warm-up, and both step graphs (one per contact
+buffer parity) are captured before the clock starts. The timed region is the next K steps (201 ..
+200 + K), with a 256 MiB clear of a scratch buffer after each step on the world's stream so that
+every step starts with a cold L2.
 
 Single world: replicas only. With --gpus N (one process per GPU under torchrun) every rank runs its
 own 100k world; `value` is all ranks' body-steps over the slowest rank's time.
 
-With --batched-worlds N (4096 by default, 0 to skip) the line also carries `batched`: world-steps/s of
-N small worlds (lognormal sizes, median 64 bodies, sigma 0.5, clipped to [16, 512]; stacks or piles on
-their own ground) stepped together by the batched entry points, against the same worlds stepped one by
-one through the single-world entry points (a sample of them), and the batched step end to end through
-host buffers.
+The line also carries, each in a few keys: `phases_ms_per_step` (device-clock phase times of the timed
+steps, so that ms_per_step = collision + topology_solve + l2_flush + launch gaps can be checked),
+`e2e` (the same window through the public API with the bodies uploaded from and read back to pinned
+host memory every step), `cpu_baseline` (the oracle port from the same step-200 state of the same
+pile), `drift_vs_fp64` (poses against the FP64 oracle over a short horizon), `hulls` (config 3),
+`batched` (config 4) and `adjoint` (config 5).
 
---impl reference times the reference's CPU algorithm (the oracle port, GPU-mode rules, all host
-threads) on a bounded sample of the same workload: the same generator at 2000 bodies, its whole
-rollout.
+--impl reference times the reference's algorithm on the host cores (the oracle port, GPU-mode rules,
+all host threads) on the same pile and window: it rolls the same generator's pile forward 200 steps
+untimed and times the next min(K, 10) steps.
 """
 
 from __future__ import annotations
@@ -36,25 +40,20 @@ sys.path.insert(0, os.path.join(ROOT, 'three-avbd_b200'))
 METRIC = 'body-steps/s @100k boxes'
 UNIT = 'body-steps/s'
 PILE_BODIES = 100_000
-SAMPLE_BODIES = 2_000
 PILE_SPACING = 2.7
-ROLLOUT = 600
+ROLL = 200              # untimed steps before the timed window: the pile has landed and is in contact
+REF_MAX_STEPS = 10      # timed steps of the CPU runs (a bounded sample of the window)
 NOMINAL_HBM_GBS = 7700.0  # HGX B200 HBM3e, for context beside the measured copy bandwidth
 L2_FLUSH_BYTES = 256 << 20
 
 
-def workload_config(n_bodies: int, steps: int) -> dict:
+def workload_config(n_bodies: int, steps: int, roll: int = ROLL) -> dict:
     return {
         'workload': f'drop pile: {n_bodies} bodies (70% boxes half-extents U[0.25,0.75], 30% spheres r U[0.2,0.6], density U[0.5,2], '
-                    f'friction U[0.3,0.8]) on a jittered 10-layer lattice, random orientations, speed U[0,1]; static ground box; '
-                    f'dt 1/60, 10 iterations, g -9.81; timed steps 1..{steps} of the rollout',
-        'bodies': n_bodies,
-        'iterations': 10,
-        'dt': 1 / 60,
-        'rollout_steps': ROLLOUT,
-        'seed': 1,
-        'spatial_sort': 'morton',
-        'l2': '256 MiB memset between timed steps, inside the timed region',
+                    f'friction U[0.3,0.8]) on a jittered 10-layer lattice (spacing {PILE_SPACING}), random orientations, speed U[0,1]; '
+                    f'static ground box; dt 1/60, 10 iterations, g -9.81; rolled {roll} steps untimed, timed steps {roll + 1}..{roll + steps}',
+        'bodies': n_bodies, 'iterations': 10, 'seed': 1, 'window': [roll + 1, roll + steps],
+        'l2': '256 MiB clear between timed steps, inside the timed region',
     }
 
 
@@ -78,7 +77,7 @@ def measured_peak() -> tuple[float, str]:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while it is open."""
 
     QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
              'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
@@ -86,8 +85,9 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.lines = []
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.device}', f'--query-gpu={self.QUERY}', '--format=csv,noheader,nounits', '-lms', '200'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -95,8 +95,7 @@ class ClockSampler:
             self.proc = None
         return self
 
-    def __exit__(self, *exc):
-        self.lines = []
+    def stop(self):
         if self.proc:
             time.sleep(0.25)
             self.proc.terminate()
@@ -110,7 +109,7 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, smax, reasons = [], 0.0, set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for l in getattr(self, 'lines', []):
+        for l in self.lines:
             f = [x.strip() for x in l.split(',')]
             if len(f) < 9:
                 continue
@@ -125,66 +124,117 @@ class ClockSampler:
         return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': smax or None, 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_reference(n_bodies: int, steps: int, threads: int, warmup: int = 0) -> dict:
-    """The oracle (the reference's algorithm, GPU-mode rules) on the sampled pile's rollout: `warmup`
-    untimed steps on one instance (threads and caches), then steps 1..`steps` of a fresh one."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle
+    return oracle
+
+
+def cpu_reference(n_bodies: int, roll: int, steps: int, threads: int) -> dict:
+    """The reference's algorithm (the oracle port, GPU-mode rules, double) on `threads` host threads:
+    the pile rolled `roll` steps untimed, then steps roll+1 .. roll+steps timed."""
     from avbd_b200.scenes import drop_pile
-    from oracle import Oracle, set_threads
-    used = set_threads(threads)
-    scene = drop_pile(n_bodies, seed=1)
-    if warmup > 0:
-        warm = Oracle(scene)
-        for _ in range(warmup):
-            warm.step_gpu()
-        del warm
-    o = Oracle(scene)
+    orc = _oracle()
+    used = orc.set_threads(threads)
+    o = orc.Oracle(drop_pile(n_bodies, seed=1, spacing=PILE_SPACING))
+    for _ in range(roll):
+        o.step_gpu()
     t0 = time.perf_counter()
     for _ in range(steps):
         o.step_gpu()
     dt = time.perf_counter() - t0
-    value = n_bodies * steps / dt
-    return {'value': value, 'unit': UNIT, 'cores': used, 'kind': 'port', 'seconds': dt,
-            'sample': f'drop pile generator at {n_bodies} bodies (same lattice, distributions and seed), steps 1..{steps} of its rollout, '
+    return {'value': n_bodies * steps / dt, 'unit': UNIT, 'cores': used, 'kind': 'port', 'seconds': dt,
+            'sample': f'the same pile ({n_bodies} bodies, same generator and seed) rolled {roll} steps on the host, steps {roll + 1}..{roll + steps} timed; '
                       f'C++ oracle in double (GPU-mode rules), {used} OpenMP threads'}
 
 
-def cpu_upstream(n_bodies: int, steps: int) -> dict:
-    """The oracle in the reference CPU solver's own order (ref/solver.ts:137-223: all-pairs
-    broadphase, bodies and forces newest first, one Gauss-Seidel pass) on one thread, steps
-    1..`steps` of the sampled pile's rollout."""
-    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    from avbd_b200.scenes import drop_pile
-    from oracle import Oracle, set_threads
-    used = set_threads(1)
-    o = Oracle(drop_pile(n_bodies, seed=1))
+def cpu_upstream_pyramid(steps: int = 60) -> dict:
+    """Config 1 (the 210-cube pyramid, the reference's CPU-runnable case) in the reference CPU solver's
+    own order (ref/solver.ts:137-223: all-pairs broadphase, bodies and forces newest first, one
+    Gauss-Seidel pass), the oracle in double on one thread, steps 1..`steps`."""
+    from avbd_b200.scenes import cube_pyramid
+    orc = _oracle()
+    used = orc.set_threads(1)
+    o = orc.Oracle(cube_pyramid(20))
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
-    return {'value': n_bodies * steps / dt, 'unit': UNIT, 'cores': used, 'seconds': dt,
-            'sample': f'drop pile generator at {n_bodies} bodies, steps 1..{steps}, C++ oracle in double in the reference '
-                      'CPU solver\'s order (upstream mode), 1 thread'}
+    return {'value': 210 * steps / dt, 'unit': UNIT, 'cores': used, 'ms_per_step': 1000 * dt / steps,
+            'sample': f'210-cube pyramid, steps 1..{steps}, the reference CPU solver\'s order, oracle in double, 1 thread'}
 
 
 def run_reference(args, rank: int):
     if rank != 0:
         return
-    steps = min(args.steps, ROLLOUT)
-    warmup = max(args.warmup, 3)
-    ref = cpu_reference(SAMPLE_BODIES, steps, os.cpu_count() or 1, warmup)
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    ref = cpu_reference(args.bodies, args.roll, steps, os.cpu_count() or 1)
     line = {
-        'metric': METRIC, 'value': ref['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': steps, 'warmup': warmup,
+        'metric': METRIC, 'value': ref['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': steps, 'warmup': args.warmup,
         'ms_per_step': 1000 * ref['seconds'] / steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
-        'data': 'synthetic', 'impl': 'reference', 'config': workload_config(SAMPLE_BODIES, steps),
+        'data': 'synthetic', 'impl': 'reference', 'config': workload_config(args.bodies, steps, args.roll),
         'cpu_baseline': {'value': ref['value'], 'unit': UNIT, 'cores': ref['cores'], 'kind': 'port', 'sample': ref['sample']},
         'e2e': {'value': ref['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, R, torch) -> dict:
-    """world-steps/s of the batched workload, batched launch against per-world launches."""
+def pile_cpu_and_drift(scene, local: int, roll: int, steps: int) -> tuple[dict, dict]:
+    """The CPU baseline and the short-horizon drift at the timed window: a world holding the pile in
+    creation order is rolled to step `roll` (the same workload at the same step as the timed world; its
+    other body order gives other colourings, so not the same bits), its bodies, colours and contacts are
+    loaded into the FP64 oracle, then both advance `steps` steps; the oracle's steps are timed on all
+    host threads, and the largest pose differences are taken after each step."""
     import numpy as np
+    import avbd_b200
+    orc = _oracle()
+    w = avbd_b200.CudaSolver3D(scene, device=local)
+    w.step(roll)
+    w.synchronize()
+    used = orc.set_threads(os.cpu_count() or 1)
+    o = orc.Oracle(scene)
+    m, c = w.read_contacts()
+    o.load_cuda_state(w.read_bodies(), w.read_colors(), m, c)
+    drift, seconds = [], 0.0
+    for _ in range(steps):
+        w.step(1)
+        t0 = time.perf_counter()
+        o.step_gpu()
+        seconds += time.perf_counter() - t0
+        g, ob = w.read_bodies(), o.bodies()
+        drift.append((float(np.abs(g['pos'] - ob[:, 0:3]).max()), float(np.abs(g['rot'] - ob[:, 3:7]).max())))
+    w.destroy()
+    n = len(scene.bodies) - 1
+    cpu = {'value': n * steps / seconds, 'unit': UNIT, 'cores': used, 'kind': 'port',
+           'sample': f'the same pile at step {roll} (read back from a GPU world and loaded into the oracle), steps '
+                     f'{roll + 1}..{roll + steps}; C++ oracle in double (GPU-mode rules), {used} OpenMP threads'}
+    pile = {'start': roll, 'steps': steps, 'max_abs_pos_m': [round(d[0], 9) for d in drift], 'max_abs_rot': [round(d[1], 9) for d in drift]}
+    return cpu, pile
+
+
+def pyramid_drift(local: int, steps: int = 60) -> dict:
+    """Config 1 (the 210-cube pyramid) from its scene state: the CUDA step against the FP64 oracle's
+    GPU-mode step (its own Jones-Plassmann colouring), largest pose differences at a few steps."""
+    import numpy as np
+    import avbd_b200
+    from avbd_b200.scenes import cube_pyramid
+    orc = _oracle()
+    scene = cube_pyramid(20)
+    o = orc.Oracle(scene)
+    o.round_f32()
+    w = avbd_b200.CudaSolver3D(scene, device=local)
+    out = {}
+    for k in range(1, steps + 1):
+        w.step(1)
+        o.step_gpu()
+        if k in (1, 10, 30, steps):
+            g, ob = w.read_bodies(), o.bodies()
+            out[str(k)] = [float(np.abs(g['pos'] - ob[:, 0:3]).max()), float(np.abs(g['rot'] - ob[:, 3:7]).max())]
+    w.destroy()
+    return {'steps_pos_rot': out}
+
+
+def run_batched(args, R, torch) -> dict:
+    """World-steps/s of the batched workload (config 4), the batched launch against per-world launches."""
     import avbd_b200
     from avbd_b200.scenes import batched_worlds
 
@@ -202,6 +252,9 @@ def run_batched(args, R, torch) -> dict:
     stream = torch.cuda.ExternalStream(b.stream, device=local)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    b.synchronize()
     barrier()
     with torch.cuda.stream(stream):
         e0.record(stream)
@@ -252,23 +305,14 @@ def run_batched(args, R, torch) -> dict:
     value = R.rate(len(scenes) * steps, ms)
     plain = len(sample) * plain_steps / plain_s
     return {
-        'metric': 'world-steps/s', 'value': value, 'ms_per_step': ms / steps, 'steps': steps,
-        'body_steps_per_s': R.rate(dyn * steps, ms),
-        'per_world_launch': {'value': plain, 'unit': 'world-steps/s', 'sample_worlds': len(sample), 'steps': plain_steps,
-                             'how': 'each sampled world stepped through the single-world entry points in turn, wall clock'},
+        'value': value, 'unit': 'world-steps/s', 'ms_per_step': ms / steps, 'steps': steps,
         'speedup_vs_per_world_launch': value / R.world_size / plain,
-        'e2e': {'value': R.rate(len(scenes) * steps, te), 'unit': 'world-steps/s',
-                'h2d_bytes_per_step': n * 160, 'd2h_bytes_per_step': n * 160},
-        'worlds': len(scenes), 'bodies': n, 'dynamic_bodies': dyn, 'world_errors': errors,
-        'launch': {'collide_threads': info['collide_threads'], 'collide_blocks': info['collide_blocks'], 'solve_blocks': info['solve_blocks'],
-                   'graphs': bool(info['graphs'])},
-        'tuning_ms': {f"{c['collide_threads']}x{c['solve_blocks']}": round(c['ms_per_step'], 4) for c in tuning['candidates']},
-        'gpu_launches': 2 * steps,
-        'config': {'workload': f'{len(scenes)} worlds, bodies per world round(lognormal(median 64, sigma 0.5)) clipped to [16, 512]; '
-                               'half stacks of unit cubes, half piles of unit cubes and r 0.5 spheres, each on its own ground box; '
-                               f'dt 1/60, 10 iterations; timed steps {args.warmup + 1 + tuning["steps_taken"]}..'
-                               f'{args.warmup + tuning["steps_taken"] + steps} after tuning and warm-up',
-                   'seed': R.seed(3), 'l2': '256 MiB memset between timed steps, inside the timed region'},
+        'per_world_launch': plain, 'per_world_sample': len(sample),
+        'e2e': R.rate(len(scenes) * steps, te), 'h2d_d2h_bytes_per_step': n * 160,
+        'worlds': len(scenes), 'dynamic_bodies': dyn, 'world_errors': errors,
+        'launch': f"{info['collide_threads']}x{info['solve_blocks']}",
+        'tuning_ms': {f"{c['collide_threads']}x{c['solve_blocks']}": round(c['ms_per_step'], 3) for c in tuning['candidates']},
+        'window': [args.warmup + 1 + tuning['steps_taken'], args.warmup + tuning['steps_taken'] + steps], 'seed': R.seed(3),
     }
 
 
@@ -280,13 +324,16 @@ def run_hulls(args, R, torch) -> dict:
     local, barrier = R.local, R.barrier
     scene = hulls_and_chains(args.hulls, args.chains, 50, seed=R.seed(9))
     w = avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
-    w.step(args.warmup)
-    w.synchronize()
     steps = args.hull_steps
     w.enable_step_stats(steps)
+    w.step(args.hull_roll)
+    w.synchronize()
     stream = torch.cuda.ExternalStream(w.stream, device=local)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    w.synchronize()
     barrier()
     with torch.cuda.stream(stream):
         e0.record(stream)
@@ -304,14 +351,11 @@ def run_hulls(args, R, torch) -> dict:
     dyn = scene.dynamic_count
     w.destroy()
     return {
-        'metric': 'body-steps/s', 'value': R.rate(dyn * steps, ms), 'ms_per_step': ms / steps, 'steps': steps,
-        'dynamic_bodies': dyn, 'hull_records': len(scene.hull_offsets), 'joints': len(joints), 'joints_broken': broken,
-        'phases_ms_per_step': {'collision': float(st['collision_ms'].mean()), 'topology_solve': float(st['solve_ms'].mean())},
-        'last_step': {k: int(st[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors')}, 'error': c['error'], 'overflow': c['overflow'],
-        'config': {'workload': f'{args.hulls} hulls (hull of 8-32 points on an ellipsoid, semi-axes U[0.3,1.0]; 512 distinct shapes) falling '
-                               f'onto {args.chains} chains of 50 boxes (0.2x0.2x0.5) with ball joints breaking at 1e4 N on pull, hung from static '
-                               f'anchors; static ground; dt 1/60, 15 iterations; timed steps {args.warmup + 1}..{args.warmup + steps}',
-                   'seed': R.seed(9), 'l2': '256 MiB memset between timed steps, inside the timed region'},
+        'value': R.rate(dyn * steps, ms), 'unit': UNIT, 'ms_per_step': ms / steps, 'steps': steps,
+        'window': [args.hull_roll + 1, args.hull_roll + steps], 'dynamic_bodies': dyn, 'joints_broken': broken,
+        'phases_ms_per_step': {'collision': round(float(st['collision_ms'].mean()), 4), 'topology_solve': round(float(st['solve_ms'].mean()), 4)},
+        'mean_manifolds': int(st['manifolds'].mean()), 'mean_contacts': int(st['contacts'].mean()), 'error': c['error'], 'overflow': c['overflow'],
+        'seed': R.seed(9),
     }
 
 
@@ -320,7 +364,8 @@ def run_adjoint(args, R, torch) -> dict:
     iterations, through the FP64 adjoint (checkpoint every 10 steps) of the recorded FP32 batched
     rollout; the target comes from a seeded FP32 rollout with perturbed parameters. Reported: the FP32
     forward (plain and recording), the adjoint's FP64 replay and reverse sweep, their ratios, and
-    central differences (h = 1e-6) of the replay along a random direction on 32 sampled worlds."""
+    central differences (h = 1e-6) of the replay along a random direction on 32 sampled worlds. A world
+    counts as non-smooth when its recorded contact structure differs between the +h and -h rollouts."""
     import numpy as np
     import avbd_b200
     from avbd_b200.scenes import tumbling_world
@@ -401,56 +446,37 @@ def run_adjoint(args, R, torch) -> dict:
     d[6::8] *= 0.1
     d[7::8] *= 0.05
     d[np.repeat(~dyn, 8)] = 0.0
-    # (a world whose loss has a kink within the step along d, a contact switching between sticking and
-    # sliding or between touching and separating, shows as central differences at h and 2h that
-    # disagree; such worlds are counted apart)
     h = 1e-6
-    fd = {}
-    for hh in (h, 2 * h):
-        lp, _ = adj.forward(p0 + hh * d)
-        lm, _ = adj.forward(p0 - hh * d)
-        fd[hh] = (lp - lm) / (2 * hh)
+    lp, _ = adj.forward(p0 + h * d)
+    lm, _ = adj.forward(p0 - h * d)
+    fd = (lp - lm) / (2 * h)
     sample = rng.choice(W, size=min(32, W), replace=False)
-    rel, rel_all, kinks = [], [], 0
+    rel_all = []
     for w in sample:
         a0, a1 = 8 * fb[w], 8 * fb[w + 1]
         an = float(grad[a0:a1] @ d[a0:a1])
-        err = abs(fd[h][w] - an) / max(abs(an), 1e-12)
-        rel_all.append(err)
-        if abs(fd[h][w] - fd[2 * h][w]) > 1e-3 * max(abs(fd[h][w]), 1e-12):
-            kinks += 1
-        else:
-            rel.append(err)
+        rel_all.append(abs(fd[w] - an) / max(abs(an), 1e-12))
     adj.destroy()
     b.destroy()
     return {
-        'metric': 'adjoint/forward time ratio', 'value': (replay + backward) / fwd_rec, 'unit': 'x', 'higher_is_better': False,
-        'forward_fp32_ms': fwd_plain, 'forward_fp32_recording_ms': fwd_rec, 'replay_fp64_ms': replay, 'reverse_fp64_ms': backward,
-        'ratio_reverse_to_forward': backward / fwd_rec, 'ratio_replay_plus_reverse_to_forward': (replay + backward) / fwd_rec,
-        'loss_mean': float(np.mean(losses_all)), 'gradient_finite': bool(np.isfinite(grads_all).all()),
-        'gathered': {'worlds': int(losses_all.size), 'gradient_values': int(grads_all.size)},
-        'fd_check': {'worlds': len(sample), 'h': h, 'direction': 'random per world (v0, omega0 unit scale; mass 0.1; friction 0.05)',
-                     'smooth_worlds': len(rel), 'max_rel_err_smooth': float(max(rel)) if rel else None,
-                     'median_rel_err': float(np.median(rel_all)), 'max_rel_err_all': float(max(rel_all)),
-                     'worlds_with_kink_within_2h': kinks},
-        'recording': {'manifolds': rec['manifolds'], 'points': rec['points'], 'max_points_per_world_step': info['max_points']},
-        'config': {'workload': f'{W} worlds x {NB} boxes (0.8 m, density 1, friction 0.5) tumbling onto a static ground; dt 1/60, '
-                               f'10 iterations, {K} steps; FP32 forward, FP64 adjoint with a checkpoint every 10 steps; gradients of the '
-                               'squared final-pose distance to a target w.r.t. v0, omega0, mass and friction of every body',
-                   'seed': seed, 'target': 'FP32 rollout with v0 + N(0,0.2), omega0 + N(0,0.5), mass and friction x U(0.9,1.1)',
-                   'timing': 'CUDA events on the launching stream; the replay and reverse read GBs of snapshots (inputs larger than L2)'},
+        'value': (replay + backward) / fwd_rec, 'unit': 'x (adjoint / forward time)', 'higher_is_better': False,
+        'forward_fp32_ms': round(fwd_plain, 3), 'forward_fp32_recording_ms': round(fwd_rec, 3), 'replay_fp64_ms': round(replay, 3),
+        'reverse_fp64_ms': round(backward, 3), 'reverse_over_forward': backward / fwd_rec,
+        'loss_mean': float(np.mean(losses_all)), 'gradient_finite': bool(np.isfinite(grads_all).all()), 'gathered_worlds': int(losses_all.size),
+        'fd_check': {'worlds': len(sample), 'h': h, 'max_rel_err': float(max(rel_all)), 'median_rel_err': float(np.median(rel_all)),
+                     'worlds_within_1e-3': int(sum(1 for e in rel_all if e <= 1e-3))},
+        'recording': {'manifolds': rec['manifolds'], 'points': rec['points']}, 'seed': seed,
     }
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=ROLLOUT)
+    ap.add_argument('--steps', type=int, default=100)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='cuda', choices=['cuda', 'reference'])
     ap.add_argument('--bodies', type=int, default=PILE_BODIES)
-    ap.add_argument('--spacing', type=float, default=PILE_SPACING,
-                    help='lattice spacing of the pile (1.15: bodies start touching, the dense case the profiles capture)')
+    ap.add_argument('--roll', type=int, default=ROLL, help='untimed steps before the timed window of the pile')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-graphs', action='store_true', help='launch each kernel directly instead of replaying the step graph')
@@ -458,6 +484,7 @@ def main():
     ap.add_argument('--batched-steps', type=int, default=300)
     ap.add_argument('--plain-sample', type=int, default=64, help='worlds stepped one by one for the per-world comparison')
     ap.add_argument('--hull-steps', type=int, default=120, help='timed steps of the hulls-and-chains workload (0: skip it)')
+    ap.add_argument('--hull-roll', type=int, default=60, help='untimed steps before the hulls-and-chains window (the hulls reach the chains)')
     ap.add_argument('--hulls', type=int, default=20000)
     ap.add_argument('--chains', type=int, default=1000)
     ap.add_argument('--adjoint-worlds', type=int, default=1024, help='worlds of the differentiated batch (0: skip it)')
@@ -478,43 +505,50 @@ def main():
     R = Ranks.from_env('nccl', timeout_s=300)
     rank, world_size, local, barrier = R.rank, R.world_size, R.local, R.barrier
 
-    scene = drop_pile(args.bodies, seed=1, spacing=args.spacing)
+    scene = drop_pile(args.bodies, seed=1, spacing=PILE_SPACING)
     n_dyn = scene.dynamic_count
 
-    def fresh():
-        w = avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
-        if args.no_graphs:
-            w.use_graphs(False)
-        return w
-
-    # Warm-up on its own world (module load, first touch), then a fresh world for the timed rollout
-    warm = fresh()
-    warm.step(args.warmup)
-    warm.synchronize()
-    warm.destroy()
-
-    w = fresh()
+    # The timed world: rolled untimed to step ROLL (its last `warmup` steps are the warm-up). Step
+    # statistics are on from the start, so both step graphs are captured and instantiated in the roll.
+    w = avbd_b200.CudaSolver3D(scene, device=local, spatial_sort=True)
+    if args.no_graphs:
+        w.use_graphs(False)
     w.enable_step_stats(args.steps)
+    w.step(max(args.roll - args.warmup, 0))
+    w.step(args.warmup)
+    w.synchronize()
+    cap0 = w.read_counters()['pair_capacity']
     stream = torch.cuda.ExternalStream(w.stream, device=local)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the clear alone, K times (its share of ms_per_step), which also warms its kernel
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        for _ in range(args.steps):
+            flush.zero_()
+        end.record(stream)
+    w.synchronize()
+    flush_ms = start.elapsed_time(end) / args.steps
+    clocks = ClockSampler(local).start()
+    time.sleep(0.5)
     barrier()
-    with ClockSampler(local) as clocks:
-        with torch.cuda.stream(stream):
-            start.record(stream)
-            for _ in range(args.steps):
-                w.step(1)
-                flush.zero_()
-            end.record(stream)
-        w.synchronize()
-        barrier()
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        h0 = time.perf_counter()
+        for _ in range(args.steps):
+            w.step(1)
+            flush.zero_()
+        h1 = time.perf_counter()
+        end.record(stream)
+    w.synchronize()
+    barrier()
+    clocks.stop()
     ms = start.elapsed_time(end)
     stats = w.read_step_stats()
     counters = w.read_counters()
     graphs = bool(counters['graphs'])
     if counters['error'] or counters['overflow']:
         print(f'warning: counters {counters}', file=sys.stderr)
-    w.destroy()
 
     ms_max, = R.max([ms])
     value = R.rate(n_dyn * args.steps, ms_max)
@@ -534,71 +568,68 @@ def main():
             traffic = tp['dram_bytes'] / tp['alg_bytes'] * bytes_alg / len(stats)
         except Exception:
             traffic = None
+    K = max(len(stats), 1)
+    phases = {'collision': coll_ms / K, 'topology_solve': solve_ms / K, 'l2_flush': flush_ms}
+    phases['launch_gaps'] = ms_max / args.steps - sum(phases.values())
+    phases = {k: round(v, 4) for k, v in phases.items()}
 
-    # End to end through the public API with host buffers: each step uploads the bodies from pinned
-    # host memory, steps, and reads the bodies back (World.read's path), then waits for them.
+    # End to end through the public API with host buffers, on the same world's next K steps: each step
+    # uploads the bodies from pinned host memory, steps, and reads the bodies back (World.read's path).
     e2e = None
     if not args.no_e2e:
-        w2 = fresh()
-        host = torch.empty(w2.body_count * 160, dtype=torch.uint8).pin_memory()
+        host = torch.empty(w.body_count * 160, dtype=torch.uint8).pin_memory()
         host_np = host.numpy().view(avbd_b200.BODY_DTYPE)
-        w2.read_bodies_into(host_np)
-        s2 = torch.cuda.ExternalStream(w2.stream, device=local)
+        w.read_bodies_into(host_np)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
-        with torch.cuda.stream(s2):
-            e0.record(s2)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
             for _ in range(args.steps):
-                w2.write_bodies_async(host_np)
-                w2.step(1)
-                w2.read_bodies_into(host_np, sync=True)
-            e1.record(s2)
-        w2.synchronize()
+                w.write_bodies_async(host_np)
+                w.step(1)
+                w.read_bodies_into(host_np, sync=True)
+            e1.record(stream)
+        w.synchronize()
         barrier()
         te, = R.max([e0.elapsed_time(e1)])
-        nbytes = w2.body_count * 160
-        e2e = {'value': R.rate(n_dyn * args.steps, te), 'unit': UNIT, 'h2d_bytes_per_step': nbytes,
-               'd2h_bytes_per_step': nbytes}
-        w2.destroy()
+        nbytes = w.body_count * 160
+        e2e = {'value': R.rate(n_dyn * args.steps, te), 'unit': UNIT, 'h2d_bytes_per_step': nbytes, 'd2h_bytes_per_step': nbytes,
+               'window': [args.roll + args.steps + 1, args.roll + 2 * args.steps]}
+    cap1 = w.read_counters()['pair_capacity']
+    last = stats[-1] if len(stats) else None
+    w.destroy()
 
-    hulls = None
-    if args.hull_steps > 0:
-        hulls = run_hulls(args, R, torch)
-
-    batched = None
-    if args.batched_worlds > 0:
-        batched = run_batched(args, R, torch)
-
-    adjoint = None
-    if args.adjoint_worlds > 0:
-        adjoint = run_adjoint(args, R, torch)
-
-    cpu = None
+    cpu, drift = None, None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        ref = cpu_reference(SAMPLE_BODIES, ROLLOUT, os.cpu_count() or 1)
-        cpu = {k: ref[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
-        up = cpu_upstream(SAMPLE_BODIES, ROLLOUT)
-        cpu['upstream_order_1_thread'] = {k: up[k] for k in ('value', 'unit', 'cores', 'sample')}
+        cpu, pile_drift = pile_cpu_and_drift(scene, local, args.roll, REF_MAX_STEPS)
+        cpu['upstream_order_pyramid_1_thread'] = cpu_upstream_pyramid()
+        drift = {'pile': pile_drift, 'pyramid_210': pyramid_drift(local)}
+
+    hulls = run_hulls(args, R, torch) if args.hull_steps > 0 else None
+    batched = run_batched(args, R, torch) if args.batched_worlds > 0 else None
+    adjoint = run_adjoint(args, R, torch) if args.adjoint_worlds > 0 else None
 
     if rank == 0:
         name = avbd_b200.device_info(local)
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world_size, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
-            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps), parallelism=f'replicas x{world_size}', spacing=args.spacing),
+            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps, max(args.roll, args.warmup)), parallelism=f'replicas x{world_size}'),
             'roofline': {'bound': 'hbm', 'kernel': 'k_topology_solve', 'achieved': achieved, 'peak': peak, 'peak_kind': peak_kind, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / max(len(stats), 1),
-                         'peak_nominal': NOMINAL_HBM_GBS, 'frac_nominal': achieved / NOMINAL_HBM_GBS},
-            'phases_ms_per_step': {'collision': coll_ms / max(len(stats), 1), 'topology_solve': solve_ms / max(len(stats), 1)},
-            'pile_last_step': dict({k: int(stats[-1][k]) for k in ('pairs', 'manifolds', 'contacts', 'colors', 'dynamic_bodies', 'adjacency', 'incidences')},
-                                   alg_bytes=alg_bytes(stats[-1])) if len(stats) else None,
+                         'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / K,
+                         'frac_of_nominal_7700': achieved / NOMINAL_HBM_GBS},
+            'phases_ms_per_step': phases,
+            'host_enqueue_ms_per_step': round(1000 * (h1 - h0) / args.steps, 4),
+            'window_counters': {k: int(np.mean(stats[k])) for k in ('pairs', 'manifolds', 'contacts', 'colors', 'dynamic_bodies')} if last is not None else None,
+            'pair_capacity_grew_in_window': bool(cap1 != cap0),
             'gpu_launches': int(stats['launches'].sum()),
             'cuda_graphs': graphs,
             'clocks': clocks.summary(),
             'e2e': e2e,
             'cpu_baseline': cpu,
-            'batched': batched,
+            'drift_vs_fp64': drift,
             'hulls': hulls,
+            'batched': batched,
             'adjoint': adjoint,
             'device': name[0] if name else None,
         }

@@ -2526,6 +2526,75 @@ void orc_set_hulls(void* h, const unsigned* words, int n) {
   });
 }
 
+// Rounds the whole state to f32 in place (bodies, aux records, joints, springs, manifolds and their
+// contacts), so that a double solver and an f32 copy of its state (the CUDA world's records) start
+// a step from the same numbers.
+void orc_round_f32(void* h) {
+  with(h, [&](auto& s) {
+    using T = std::decay_t<decltype(s.dt)>;
+    auto r = [](T& x) { x = T(float(x)); };
+    auto r3 = [&](V3<T>& v) { for (auto& x : v) r(x); };
+    auto r4 = [&](Q4<T>& q) { for (auto& x : q) r(x); };
+    for (auto& b : s.bodies) {
+      r3(b.pos); r3(b.initPos); r3(b.inertialPos); r3(b.vel); r3(b.angVel); r3(b.prevVel); r3(b.size); r3(b.moment);
+      r4(b.rot); r4(b.initRot); r4(b.inertialRot);
+      r(b.mass); r(b.friction); r(b.radius); r(b.gravityScale); r(b.linDamp); r(b.angDamp);
+    }
+    for (auto& f : s.forces) {
+      if (f->kind == K_JOINT) {
+        auto* j = static_cast<Joint<T>*>(f.get());
+        r3(j->rA); r3(j->rB); r3(j->C0Lin); r3(j->C0Ang); r3(j->penaltyLin); r3(j->penaltyAng); r3(j->lambdaLin); r3(j->lambdaAng);
+        r(j->stiffnessLin); r(j->stiffnessAng); r(j->fracture); r(j->torqueArm); r(j->yield); r(j->breakBend);
+        r4(j->rest); r4(j->restStart);
+      } else if (f->kind == K_SPRING) {
+        auto* sp = static_cast<Spring<T>*>(f.get());
+        r3(sp->rA); r3(sp->rB); r(sp->rest); r(sp->stiffness);
+      } else if (f->kind == K_MANIFOLD) {
+        auto* m = static_cast<Manifold<T>*>(f.get());
+        for (auto& x : m->basis) r(x);
+        r(m->friction);
+        for (auto& c : m->contacts) { r3(c.rA); r3(c.rB); r3(c.C0); r3(c.penalty); r3(c.lambda); }
+      }
+    }
+    return 0;
+  });
+}
+
+// Replaces last step's manifolds (the GPU-mode step's warm-start source) with the given records, in
+// orc_get_manifolds' layout: manifold (8): ignored, a, b, count, normal3, friction; contact (17):
+// feature, stick, rA3, rB3, C0 3, pen3, lam3. A manifold's contacts follow the previous manifold's.
+// Manifolds are appended after the joints, springs and ignore pairs, as a step leaves them.
+void orc_set_manifolds(void* h, int nm, const double* mrec, int nc, const double* crec) {
+  with(h, [&](auto& s) {
+    using T = std::decay_t<decltype(s.dt)>;
+    std::vector<std::unique_ptr<Force<T>>> keep;
+    for (auto& f : s.forces) {
+      if (f->kind == K_MANIFOLD) s.unlink(f.get());
+      else keep.push_back(std::move(f));
+    }
+    s.forces = std::move(keep);
+    int ci = 0;
+    for (int i = 0; i < nm; i++) {
+      const double* r = mrec + 8 * i;
+      auto m = std::make_unique<Manifold<T>>(&s, int(r[1]), int(r[2]));
+      m->basis = orthonormal(V3<T>{T(r[4]), T(r[5]), T(r[6])});
+      m->friction = T(r[7]);
+      for (int k = 0; k < int(r[3]) && ci < nc; k++, ci++) {
+        const double* q = crec + 17 * ci;
+        Contact<T> c;
+        c.feature = uint32_t(q[0]);
+        c.stick = q[1] != 0;
+        for (int e = 0; e < 3; e++) {
+          c.rA[e] = T(q[2 + e]); c.rB[e] = T(q[5 + e]); c.C0[e] = T(q[8 + e]); c.penalty[e] = T(q[11 + e]); c.lambda[e] = T(q[14 + e]);
+        }
+        m->contacts.push_back(c);
+      }
+      s.addForce(std::move(m));
+    }
+    return 0;
+  });
+}
+
 // Host threads for the GPU-mode step (OpenMP); returns the count in use.
 int orc_set_threads(int n) {
 #ifdef _OPENMP

@@ -50,6 +50,8 @@ def lib():
         L.orc_contact_count.argtypes = [P]
         L.orc_get_manifolds.argtypes = [P, D, D]
         L.orc_set_contact_penalty.argtypes = [P, ctypes.c_double]
+        L.orc_round_f32.argtypes = [P]
+        L.orc_set_manifolds.argtypes = [P, I, D, I, D]
         L.orc_step.argtypes = [P]
         L.orc_step_gpu.argtypes = [P, ctypes.POINTER(U), ctypes.POINTER(I)]
         L.orc_pairs.argtypes = [P, ctypes.POINTER(U), I]
@@ -112,6 +114,63 @@ def body_record(b) -> np.ndarray:
     r[41] = b.mask
     r[42] = NO_COLOR
     return r
+
+
+STICK_BIT = 0x80000000
+
+
+def records_from_cuda_bodies(bodies: np.ndarray, colors: np.ndarray, base: np.ndarray) -> np.ndarray:
+    """Oracle body records (doubles) holding CUDA body records (the C ABI's avbd_body fields) and colour
+    state; `base` (oracle records of the same bodies) supplies what a CUDA record does not hold (the
+    collision filters)."""
+    r = np.array(base, dtype=np.float64, copy=True)
+    r[:, 0:3] = bodies['pos']
+    r[:, 3:7] = bodies['rot']
+    r[:, 7:10] = bodies['vel']
+    r[:, 10:13] = bodies['ang_vel']
+    r[:, 13:15] = 0.0
+    r[:, 15] = bodies['prev_up_vel']  # up = +z: only this component is read
+    r[:, 16:19] = bodies['size']
+    r[:, 19] = bodies['mass']
+    r[:, 20:23] = bodies['moment']
+    r[:, 23] = bodies['friction']
+    r[:, 24] = bodies['radius']
+    r[:, 25] = bodies['shape']
+    r[:, 26:29] = bodies['initial_pos']
+    r[:, 29:33] = bodies['initial_rot']
+    r[:, 33:36] = bodies['inertial_pos']
+    r[:, 36:40] = bodies['inertial_rot']
+    r[:, 42] = colors
+    return r
+
+
+def records_from_cuda_contacts(m: np.ndarray, c: np.ndarray):
+    """CUDA manifolds and contacts (avbd_read_contacts: manifold.first indexes the contacts) in the
+    layout of Oracle.manifolds() / Oracle.set_manifolds()."""
+    mrec = np.zeros((len(m), 8))
+    mrec[:, 1] = m['a']
+    mrec[:, 2] = m['b']
+    mrec[:, 3] = m['count']
+    mrec[:, 4:7] = m['normal']
+    mrec[:, 7] = m['friction']
+    if len(m):
+        first = m['first'].astype(np.int64)
+        count = m['count'].astype(np.int64)
+        idx = np.repeat(first - np.concatenate([[0], np.cumsum(count)[:-1]]), count) + np.arange(int(count.sum()))
+    else:
+        idx = np.zeros(0, np.int64)
+    q = c[idx]
+    crec = np.zeros((len(q), 17))
+    crec[:, 0] = q['key'] & np.uint32(~STICK_BIT & 0xFFFFFFFF)
+    crec[:, 1] = (q['key'] & np.uint32(STICK_BIT)) != 0
+    crec[:, 2:5] = q['r_a']
+    crec[:, 5:8] = q['r_b']
+    crec[:, 8] = q['c0_n']
+    crec[:, 9] = q['c0_t1']
+    crec[:, 10] = q['c0_t2']
+    crec[:, 11:14] = q['pen']
+    crec[:, 14:17] = q['lam']
+    return mrec, crec
 
 
 class Oracle:
@@ -237,6 +296,30 @@ class Oracle:
 
     def set_contact_penalty(self, pen):
         self.L.orc_set_contact_penalty(self.h, pen)
+
+    def round_f32(self):
+        """Rounds every state value to f32 in place: the state a CUDA world seeded from this one holds."""
+        self.L.orc_round_f32(self.h)
+
+    def set_bodies(self, recs: np.ndarray):
+        """Overwrites bodies 0 .. len(recs) - 1 with oracle body records."""
+        recs = np.ascontiguousarray(recs, dtype=np.float64)
+        for i in range(len(recs)):
+            self.set_body(i, recs[i])
+
+    def load_cuda_state(self, bodies: np.ndarray, colors: np.ndarray, manifolds: np.ndarray, contacts: np.ndarray):
+        """The bodies, colour state and last step's contacts of a CUDA world (C-ABI records) that holds
+        this oracle's bodies in the same order: both then start the next step from the same values."""
+        self.set_bodies(records_from_cuda_bodies(bodies, colors[:len(bodies)], self.bodies()))
+        self.set_manifolds(*records_from_cuda_contacts(manifolds, contacts))
+
+    def set_manifolds(self, m: np.ndarray, c: np.ndarray):
+        """Replaces last step's manifolds (manifolds()' layout: 8 per manifold, 17 per contact)."""
+        m = np.ascontiguousarray(m, dtype=np.float64).reshape(-1, 8)
+        c = np.ascontiguousarray(c, dtype=np.float64).reshape(-1, 17)
+        mm = m if len(m) else np.zeros((1, 8))
+        cc = c if len(c) else np.zeros((1, 17))
+        self.L.orc_set_manifolds(self.h, len(m), _dp(mm), len(c), _dp(cc))
 
     # --- stepping ---
     def step(self, n: int = 1):

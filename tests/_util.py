@@ -10,7 +10,7 @@ import avbd_b200
 from avbd_b200 import BODY_DTYPE, CONTACT_DTYPE, INFO_DTYPE, JOINT_DTYPE, MANIFOLD_DTYPE
 from avbd_b200 import _abi
 from avbd_b200.solver import finite
-from oracle import K_IGNORE, K_JOINT, K_MANIFOLD, K_SPRING, NO_COLOR, Oracle
+from oracle import K_IGNORE, K_JOINT, K_MANIFOLD, K_SPRING, NO_COLOR, Oracle, records_from_cuda_bodies, records_from_cuda_contacts
 
 STICK_BIT = _abi.STICK_BIT
 
@@ -168,3 +168,81 @@ def lcg(seed: int):
 def qnormalize(q):
     l = math.sqrt((q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) + q[3] * q[3])
     return [q[0] / l, q[1] / l, q[2] / l, q[3] / l]
+
+
+def _unbig(x):
+    """The device's BIG (its stand-in for infinity) back to infinity."""
+    x = np.asarray(x, dtype=np.float64)
+    return np.where(np.abs(x) >= 1e38, np.sign(x) * np.inf, x)
+
+
+def oracle_from_cuda(w: avbd_b200.CudaSolver3D, scene, flags: int = 0) -> Oracle:
+    """A GPU-mode FP64 oracle holding a CUDA world's state exactly (its f32 values): bodies, colour
+    state, joints and last step's contacts. The world must hold `scene`'s bodies in creation order and
+    its joints in the scene's force order (CudaSolver3D(scene), no spatial sort)."""
+    o = Oracle(scene, flags=flags)
+    o.set_bodies(records_from_cuda_bodies(w.read_bodies(), w.read_colors(), o.bodies()))
+    joints, _ = w.read_joints()
+    k = 0
+    for si, f in enumerate(scene.forces):
+        if f.kind == 'ignore':
+            continue
+        j = joints[k]
+        k += 1
+        if f.kind != 'joint':
+            continue
+        oi = o.force_of[si]
+        r = o.force(oi)
+        broken = j['stiffness_lin'] == 0 and j['stiffness_ang'] == 0
+        r[3:6] = j['pen_lin']
+        r[6:9] = j['pen_ang']
+        r[9:12] = j['lam_lin']
+        r[12:15] = j['lam_ang']
+        r[15:18] = j['c0_lin'][:3]
+        r[18:21] = j['c0_ang']
+        if broken:
+            r[26] = 1.0
+        else:
+            r[21] = _unbig(j['stiffness_lin'])
+            r[22] = _unbig(j['stiffness_ang'])
+        r[23] = _unbig(abs(float(j['fracture'])))
+        r[24] = 1.0 if j['fracture'] < 0 else 0.0
+        r[27] = _unbig(j['yield_force'])
+        r[28] = _unbig(j['break_bend'])
+        r[29:33] = j['rest']
+        r[34:38] = j['rest_start']
+        o.set_joint(oi, r)
+    o.set_manifolds(*records_from_cuda_contacts(*w.read_contacts()))
+    return o
+
+
+def contact_map(m: np.ndarray, c: np.ndarray) -> dict:
+    """(a, b, feature) -> (rA, rB, lambda, penalty) of a CUDA world's contact readback."""
+    out = {}
+    for rec in m:
+        for k in range(int(rec['first']), int(rec['first'] + rec['count'])):
+            key = int(c[k]['key']) & ~STICK_BIT & 0xFFFFFFFF
+            out[(int(rec['a']), int(rec['b']), key)] = (c[k]['r_a'], c[k]['r_b'], c[k]['lam'].astype(np.float64), c[k]['pen'].astype(np.float64))
+    return out
+
+
+def oracle_contact_map(o: Oracle) -> dict:
+    """(a, b, feature) -> (rA, rB, lambda, penalty) of the oracle's manifolds."""
+    m, c = o.manifolds()
+    out, k = {}, 0
+    for rec in m:
+        for q in c[k:k + int(rec[3])]:
+            out[(int(rec[1]), int(rec[2]), int(q[0]) & ~STICK_BIT & 0xFFFFFFFF)] = (q[2:5], q[5:8], q[14:17], q[11:14])
+        k += int(rec[3])
+    return out
+
+
+def pose_rel_diff(cuda_bodies: np.ndarray, oracle_bodies: np.ndarray) -> float:
+    """Largest pose difference relative to the pose's magnitude (positions against max(|x|, 1 m);
+    rotations are unit quaternions, so absolute)."""
+    if not len(oracle_bodies):
+        return 0.0
+    x = oracle_bodies[:, 0:3]
+    dp = np.abs(cuda_bodies['pos'] - x) / np.maximum(np.abs(x), 1.0)
+    dq = np.abs(cuda_bodies['rot'] - oracle_bodies[:, 3:7])
+    return max(float(dp.max()), float(dq.max()))

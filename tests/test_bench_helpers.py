@@ -47,23 +47,24 @@ def test_clock_summary():
 
 
 def test_workload_config_names_the_pile():
-    cfg = bench.workload_config(100_000, 600)
-    assert cfg['bodies'] == 100_000 and cfg['iterations'] == 10 and cfg['seed'] == 1
-    assert 'drop pile' in cfg['workload'] and '1..600' in cfg['workload']
+    cfg = bench.workload_config(100_000, 20)
+    assert cfg['bodies'] == 100_000 and cfg['iterations'] == 10 and cfg['seed'] == 1 and cfg['window'] == [201, 220]
+    assert 'drop pile' in cfg['workload'] and 'rolled 200 steps untimed, timed steps 201..220' in cfg['workload']
 
 
-@pytest.mark.parametrize('fn', ['cpu_reference', 'cpu_upstream'])
-def test_cpu_baselines_on_a_tiny_sample(fn):
-    r = bench.cpu_reference(60, 5, 2) if fn == 'cpu_reference' else bench.cpu_upstream(60, 5)
-    assert r['value'] > 0 and r['unit'] == bench.UNIT and r['cores'] >= 1 and '60 bodies' in r['sample']
+def test_cpu_baselines_on_a_tiny_sample():
+    r = bench.cpu_reference(60, 5, 3, 2)
+    assert r['value'] > 0 and r['unit'] == bench.UNIT and r['cores'] >= 1 and '60 bodies' in r['sample'] and 'steps 6..8' in r['sample']
+    u = bench.cpu_upstream_pyramid(2)
+    assert u['value'] > 0 and u['cores'] == 1 and 'pyramid' in u['sample']
 
 
 def test_reference_arm_line():
     """`bench.py --impl reference` prints the contract's line on rank 0, nothing on other ranks."""
     import subprocess
     env = dict(os.environ, RANK='0', WORLD_SIZE='1')
-    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--steps', '3', '--warmup', '3'],
-                         capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--steps', '3', '--warmup', '3', '--bodies', '300',
+                          '--roll', '20'], capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr
     line = json.loads(out.stdout.strip().splitlines()[-1])
     for key in ('metric', 'value', 'unit', 'n_gpus', 'steps', 'warmup', 'ms_per_step', 'higher_is_better', 'scaling', 'vs_baseline', 'dtype',
@@ -71,6 +72,7 @@ def test_reference_arm_line():
         assert key in line, key
     assert line['impl'] == 'reference' and line['metric'] == bench.METRIC and line['steps'] == 3 and line['warmup'] == 3
     assert line['e2e']['h2d_bytes_per_step'] == 0 and line['cpu_baseline']['value'] == line['value']
+    assert line['config']['window'] == [21, 23] and line['config']['bodies'] == 300
     env = dict(os.environ, RANK='1', WORLD_SIZE='2')
     out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--steps', '3', '--warmup', '3'],
                          capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
