@@ -233,13 +233,28 @@ def pyramid_drift(local: int, steps: int = 60) -> dict:
     return {'steps_pos_rot': out}
 
 
+def job_share(R, scenes):
+    """This rank's worlds of one batched job (all ranks build the same job from one seed): the
+    partition by Σ(N_w · degree), and the indices of this rank's share."""
+    import numpy as np
+    from avbd_b200.replicas import partition_worlds, world_cost
+    if R.world_size == 1:
+        return np.arange(len(scenes))
+    costs = [world_cost(np.array([b.pos for b in s.bodies]), np.array([b.radius for b in s.bodies]), np.array([b.mass > 0 for b in s.bodies]),
+                        sum(1 for f in s.forces if f.kind != 'ignore')) for s in scenes]
+    return partition_worlds(costs, R.world_size)[R.rank]
+
+
 def run_batched(args, R, torch) -> dict:
-    """World-steps/s of the batched workload (config 4), the batched launch against per-world launches."""
+    """World-steps/s of the batched workload (config 4), the batched launch against per-world launches.
+    On N ranks one job of N x the worlds is split over them (weak scaling)."""
     import avbd_b200
     from avbd_b200.scenes import batched_worlds
 
     local, barrier = R.local, R.barrier
-    scenes = batched_worlds(args.batched_worlds, seed=R.seed(3))
+    job = batched_worlds(args.batched_worlds * R.world_size, seed=3)
+    mine = job_share(R, job)
+    scenes = [job[i] for i in mine]
     n = sum(len(s.bodies) for s in scenes)
     dyn = sum(s.dynamic_count for s in scenes)
     b = avbd_b200.BatchSolver3D(len(scenes), n, 1, params=scenes[0].params, device=local)
@@ -302,17 +317,17 @@ def run_batched(args, R, torch) -> dict:
     plain_s = time.perf_counter() - t0
     for w in worlds:
         w.destroy()
-    value = R.rate(len(scenes) * steps, ms)
+    value = len(job) * steps / (ms / 1000.0)
     plain = len(sample) * plain_steps / plain_s
     return {
         'value': value, 'unit': 'world-steps/s', 'ms_per_step': ms / steps, 'steps': steps,
         'speedup_vs_per_world_launch': value / R.world_size / plain,
         'per_world_launch': plain, 'per_world_sample': len(sample),
-        'e2e': R.rate(len(scenes) * steps, te), 'h2d_d2h_bytes_per_step': n * 160,
-        'worlds': len(scenes), 'dynamic_bodies': dyn, 'world_errors': errors,
-        'launch': f"{info['collide_threads']}x{info['solve_blocks']}",
-        'tuning_ms': {f"{c['collide_threads']}x{c['solve_blocks']}": round(c['ms_per_step'], 3) for c in tuning['candidates']},
-        'window': [args.warmup + 1 + tuning['steps_taken'], args.warmup + tuning['steps_taken'] + steps], 'seed': R.seed(3),
+        'e2e': len(job) * steps / (te / 1000.0), 'h2d_d2h_bytes_per_step': n * 160,
+        'worlds': len(job), 'worlds_this_rank': len(scenes), 'dynamic_bodies': dyn, 'world_errors': errors,
+        'launch': f"{tuning['collide_threads']}x{tuning['solve_blocks']}x{tuning['rows_per_lane']}",
+        'tuning_ms': {f"{c['collide_threads']}x{c['solve_blocks']}x{c['rows_per_lane']}": round(c['ms_per_step'], 3) for c in tuning['candidates']},
+        'window': [args.warmup + 1 + tuning['steps_taken'], args.warmup + tuning['steps_taken'] + steps], 'seed': 3,
     }
 
 
@@ -370,10 +385,14 @@ def run_adjoint(args, R, torch) -> dict:
     import avbd_b200
     from avbd_b200.scenes import tumbling_world
 
-    W, NB, K = args.adjoint_worlds, 64, args.adjoint_steps
+    NB, K = 64, args.adjoint_steps
     local, barrier = R.local, R.barrier
-    seed = R.seed(500)
-    scenes = [tumbling_world(np.random.default_rng(seed * 100003 + w), NB) for w in range(W)]
+    seed = 500
+    # one job of world_size x the worlds, split over the ranks
+    job = [tumbling_world(np.random.default_rng(seed * 100003 + w), NB) for w in range(args.adjoint_worlds * R.world_size)]
+    mine = job_share(R, job)
+    scenes = [job[i] for i in mine]
+    W = len(scenes)
     n = sum(len(s.bodies) for s in scenes)
     b = avbd_b200.BatchSolver3D(W, n, params=scenes[0].params, device=local)
     for s in scenes:
@@ -398,7 +417,7 @@ def run_adjoint(args, R, torch) -> dict:
         return e0.elapsed_time(e1)
 
     # the target: the FP32 rollout with perturbed parameters
-    rng = np.random.default_rng(seed)
+    rng = np.random.default_rng(seed + R.rank)
     pert = nominal.copy()
     pert['vel'][dyn] += rng.normal(0, 0.2, (int(dyn.sum()), 3)).astype(np.float32)
     pert['ang_vel'][dyn] += rng.normal(0, 0.5, (int(dyn.sum()), 3)).astype(np.float32)
@@ -437,9 +456,9 @@ def run_adjoint(args, R, torch) -> dict:
     backward = e0.elapsed_time(e1)
     barrier()
     fwd_rec, replay, backward = R.max([fwd_rec, replay, backward])
-    # the whole job's per-world losses and gradients on every rank (one all-gather each)
-    losses_all = R.all_gather(np.asarray(loss_b, dtype=np.float64))
-    grads_all = R.all_gather(np.asarray(grad, dtype=np.float64))
+    # the whole job's per-world losses and gradients in job order on every rank (one reduction each)
+    losses_all = R.gather_worlds(mine, np.asarray(loss_b, dtype=np.float64), len(job))
+    grads_all = R.gather_worlds(mine, np.asarray(grad, dtype=np.float64).reshape(W, -1), len(job))
     # central differences of the replay along a random direction, 32 sampled worlds
     fb = adj.first_body.astype(np.int64)
     d = rng.normal(0, 1, p0.shape)
@@ -521,7 +540,10 @@ def main():
     stream = torch.cuda.ExternalStream(w.stream, device=local)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f'cuda:{local}')
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # the clear alone, K times (its share of ms_per_step), which also warms its kernel
+    # the clear alone, K times (its share of ms_per_step), after one untimed clear that loads its kernel
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    w.synchronize()
     with torch.cuda.stream(stream):
         start.record(stream)
         for _ in range(args.steps):

@@ -55,6 +55,10 @@ enum {
 /* GPU-only rules (gpu/solver.ts:174-231; the reference's parity tests turn every one off). */
 #define AVBD_FLAG_MATCH_NEAREST 1u
 #define AVBD_FLAG_FACE_BIAS 2u
+/* reuseContacts (gpu/solver.ts:181, wgsl-collision.ts:20-44, 706-753): a pair keeps last step's contact
+ * points (C(x-) evaluated again, warm starts as usual) when neither body moved more than 2 mm or turned
+ * more than 0.002 rad since the step that generated them; its narrowphase is skipped. */
+#define AVBD_FLAG_REUSE_CONTACTS 4u
 #define AVBD_FLAG_START_AT_REST 8u
 #define AVBD_FLAG_MASS_PENALTY 16u
 /* Contact key bit: static friction held last step (layout.ts:130). */
@@ -76,7 +80,7 @@ typedef struct avbd_body {
   float size[3], mass;     /* full widths; mass 0 = static */
   float moment[3], radius; /* principal moments; bounding radius */
   float inertial_pos[3];   /* inertial target y */
-  float moved_step;        /* reserved (contact reuse bookkeeping) */
+  float moved_step;        /* u32 bits: the step the body last moved past the contact-reuse tolerances */
   float inertial_rot[4];
   float vel[3], prev_up_vel; /* velocity; last step's velocity along up */
   float ang_vel[3], shape;   /* angular velocity; AVBD_SHAPE_* */
@@ -157,8 +161,13 @@ const char* avbd_last_error(const avbd_world* world);
 /* params (GpuParams3D, gpu/solver.ts:163-231). */
 int avbd_set_params(avbd_world* world, const avbd_params* params);
 int avbd_get_params(const avbd_world* world, avbd_params* params);
-/* Defaults of the reference's SolverParams with every GPU-only rule off and up = +z. */
+/* Defaults of the reference's SolverParams with every GPU-only rule off and up = +z (the reference's
+ * parity setting, avbd3d-gpu.gpu.test.ts:47-52). */
 int avbd_default_params(avbd_params* params);
+/* gpuParams3D() (gpu/solver.ts:216-230), what a World runs with: the reference's SolverParams, every
+ * GPU-only rule on (matchNearest, faceBias, reuseContacts, startAtRest, massPenalty), contact margin
+ * 0.01 and up = +y. */
+int avbd_world_params(avbd_params* params);
 
 /* addBodies (gpu/solver.ts:1469-1481): appends; *first = index of the first. */
 int avbd_add_bodies(avbd_world* world, const avbd_body* bodies, uint32_t n, uint32_t* first);
@@ -252,6 +261,20 @@ int avbd_set_fixed_colors(avbd_world* world, const uint32_t* colors, uint32_t n)
 
 /* step() (gpu/solver.ts:2112-2295): n steps, enqueued on the world's stream (asynchronous). */
 int avbd_step(avbd_world* world, int n);
+/* step(options) (GpuStepOptions, gpu/solver.ts:42-50). reuse_manifolds != 0: the step detects no pair
+ * and keeps every manifold of the step before (normals, anchors, keys), evaluating C(x-) again and
+ * warm-starting as usual, for substeps after a detecting step; it applies only while last step's
+ * manifolds are valid (a step ran and no body, joint, filter, lifecycle or contact write came since),
+ * else the step detects as usual. NULL options: avbd_step. */
+typedef struct avbd_step_options {
+  uint32_t reuse_manifolds;
+} avbd_step_options;
+int avbd_step_with(avbd_world* world, int n, const avbd_step_options* options);
+/* Contact-reuse state: per body its reference pose (8 floats: x y z 0 and rotation x y z w; a zero
+ * rotation: none yet; the step it last moved is the body record's moved_step word, as u32 bits), and
+ * per manifold (avbd_read_contacts' order) the step whose narrowphase generated its points. */
+int avbd_read_reuse_state(avbd_world* world, float* ref_poses, uint32_t body_cap, uint32_t* n_bodies, uint32_t* generations, uint32_t manifold_cap,
+                          uint32_t* n_manifolds);
 /* Waits for the world's stream; reports a device error or a bounded wait that gave up. */
 int avbd_synchronize(avbd_world* world);
 
@@ -357,6 +380,71 @@ int avbd_write_bodies_async(avbd_world* world, uint32_t first, const avbd_body* 
 int avbd_find_pairs_noalloc(const avbd_body* bodies, uint32_t n, const uint32_t* groups_mask, uint32_t* pairs_ab, uint32_t cap, uint32_t* count,
                             void* stream);
 
+/* ---- Around the step: impulses, contact events, raycasts -------------------------------------------
+ * The passes a World runs beside the solver (world.ts:1736-1738 and its queries), on the world's
+ * device state and stream. */
+
+/* Pusher.apply (src/lib/push.ts:103-131): impulses on bodies before the next step. Per pushed body (each
+ * slot at most once: sum a body's pushes first, as addImpulse does): lin the whole linear impulse (N s),
+ * off_lin the part of it applied at points, moment those parts' moment about the world origin plus any
+ * angular impulse. A dynamic, enabled body's velocity gains lin / mass and its angular velocity
+ * I^-1 (moment - x cross off_lin) taken in its principal frame, at the pose the device holds; static and
+ * disabled bodies are left alone. Waits for the world's stream. */
+typedef struct avbd_push {
+  uint32_t body;
+  float lin[3];
+  float off_lin[3];
+  float moment[3];
+} avbd_push;
+int avbd_apply_pushes(avbd_world* world, const avbd_push* pushes, uint32_t n);
+
+/* ContactWatch (src/lib/contacts.ts:129-267): after each step (avbd_contact_watch_run), the touching
+ * pairs with a reporting body go into this step's set; a pair missing from last step's set began
+ * touching (where: its points' mean on body a; how hard: |sum of its normal multipliers| dt; the normal
+ * from b to a), and one of last step's set missing from this step's ended. Bodies are reported by
+ * lifetime IDs (1 .. 2^31 - 1) set per slot, so events survive slot reuse. Events accumulate on the
+ * device until avbd_contact_watch_read; past `capacity` they are counted as dropped; a step with more
+ * touching pairs than a set holds (2 x `pairs`, a power of two) sets `full`, and that step's events
+ * are unreliable. The watch reads the world's storage: destroy it before the world. */
+#define AVBD_CONTACT_BEGIN 1u
+#define AVBD_CONTACT_END 2u
+typedef struct avbd_contact_event {
+  uint32_t kind, a, b, step; /* AVBD_CONTACT_*, lifetime IDs of the pair's bodies (a's slot > b's), the step */
+  float point[3], impulse;   /* a begin's point and normal impulse */
+  float normal[3], pad;      /* a begin's normal (b to a) */
+} avbd_contact_event;
+typedef struct avbd_contact_watch avbd_contact_watch;
+int avbd_contact_watch_create(avbd_world* world, uint32_t pairs, uint32_t capacity, avbd_contact_watch** out);
+int avbd_contact_watch_destroy(avbd_contact_watch* watch);
+const char* avbd_contact_watch_last_error(const avbd_contact_watch* watch);
+/* setWatched(indices, ids, on): slot indices[k] reports (on[k] != 0) under lifetime ID ids[k] */
+int avbd_contact_watch_set(avbd_contact_watch* watch, const uint32_t* indices, const uint32_t* ids, const uint32_t* on, uint32_t n);
+/* run(storage, pairs, step, dt): after a step, enqueued on the world's stream */
+int avbd_contact_watch_run(avbd_contact_watch* watch, uint32_t step, float dt);
+/* read(): the events since the last read, in step order (within a step as the device wrote them), and
+ * clears them; *n the events held, *dropped those past the capacity, *full whether a set overflowed */
+int avbd_contact_watch_read(avbd_contact_watch* watch, avbd_contact_event* dst, uint32_t cap, uint32_t* n, uint32_t* dropped, uint32_t* full);
+
+/* Raycaster.cast (src/lib/raycast.ts:170-251): the nearest hit of each ray among the world's bodies
+ * (boxes and sails by their faces, spheres, hulls by their face planes) at the poses the device holds,
+ * skipping disabled bodies, bodies whose groups miss `mask`, and the `ignore` slots. A hit at the same
+ * distance as another goes to the lower slot. direction is normalised here (a zero direction stays
+ * zero); max_distance caps the hit distance (values past 3e38: no cap). A ray starting inside a body
+ * hits it at distance 0 with the normal against the ray. hit.body -1 (distance -1): no hit. */
+#define AVBD_RAY_MAX 65535u
+#define AVBD_RAY_MAX_IGNORED 16u
+typedef struct avbd_ray {
+  float origin[3], max_distance;
+  float direction[3], pad;
+} avbd_ray;
+typedef struct avbd_ray_hit {
+  int32_t body;
+  float distance;
+  float point[3];  /* origin + direction * distance */
+  float normal[3]; /* world axes */
+} avbd_ray_hit;
+int avbd_raycast(avbd_world* world, const avbd_ray* rays, uint32_t n, const uint32_t* ignore, uint32_t n_ignore, uint32_t mask, avbd_ray_hit* hits);
+
 /* ---- Adjoint --------------------------------------------------------------------------------------
  * No counterpart in the reference (it has no differentiation). Gradients of a pose loss
  * L = sum over dynamic bodies of |x_T - x*|^2 + |q_T - q*|^2 after a recorded rollout, with respect
@@ -406,7 +494,7 @@ int avbd_adjoint_backward(avbd_adjoint* adjoint, const double* params, double* g
 typedef struct avbd_batch avbd_batch;
 
 #define AVBD_BATCH_MAX_WORLD_BODIES 4096u
-#define AVBD_BATCH_TUNE_CANDIDATES 8
+#define AVBD_BATCH_TUNE_CANDIDATES 16
 
 typedef struct avbd_batch_config {
   uint32_t world_capacity; /* worlds */
@@ -427,13 +515,15 @@ typedef struct avbd_batch_status {
   uint32_t collide_threads, collide_blocks, solve_blocks, graphs;
 } avbd_batch_status;
 
-/* The autotuner's measurements: per candidate launch shape its mean step time */
+/* The autotuner's measurements: per candidate launch shape (collision block size, solve blocks, and
+ * bodies per warp as the least rows a lane of a body's group takes: 1, or 4) its mean step time */
 typedef struct avbd_batch_tuning {
   uint32_t candidates;
   uint32_t candidate_threads[AVBD_BATCH_TUNE_CANDIDATES];
   uint32_t candidate_solve_blocks[AVBD_BATCH_TUNE_CANDIDATES];
+  uint32_t candidate_rows_per_lane[AVBD_BATCH_TUNE_CANDIDATES];
   float candidate_ms[AVBD_BATCH_TUNE_CANDIDATES];
-  uint32_t collide_threads, solve_blocks; /* the choice */
+  uint32_t collide_threads, solve_blocks, rows_per_lane; /* the choice */
   float ms_per_step;
   uint32_t steps_taken; /* tuning steps are real steps: the worlds advance by this many */
 } avbd_batch_tuning;
@@ -461,8 +551,8 @@ int avbd_batch_read_all_bodies_async(avbd_batch* batch, avbd_body* dst, uint32_t
 int avbd_batch_write_all_bodies_async(avbd_batch* batch, const avbd_body* src, uint32_t n);
 int avbd_batch_use_graphs(avbd_batch* batch, int enable);
 int avbd_batch_stream(avbd_batch* batch, void** stream);
-/* Times each candidate launch shape (collision block size x solve blocks) over `steps` real steps
- * and keeps the fastest. */
+/* Times each candidate launch shape (collision block size x solve blocks x rows per lane) over `steps`
+ * real steps and keeps the fastest. */
 int avbd_batch_tune(avbd_batch* batch, int steps, avbd_batch_tuning* out);
 int avbd_batch_info(avbd_batch* batch, avbd_batch_status* out);
 

@@ -251,7 +251,9 @@ const int MAX_COLORS = 64;
 const uint32_t NO_COLOR = 255, PENDING = 256;
 const double PIVOT_FLOOR = 1e-5;
 const double NEAREST_FRACTION = 0.05;
-enum { FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_START_AT_REST = 8, FLAG_MASS_PENALTY = 16 };
+enum { FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_REUSE_CONTACTS = 4, FLAG_START_AT_REST = 8, FLAG_MASS_PENALTY = 16 };
+// Contact reuse tolerances (gpu/layout.ts:174-175)
+const float REUSE_LIN_TOL = 0.002f, REUSE_ANG_TOL = 0.002f;
 const double REST_SPEED = 0.1;
 
 template <class T> struct Solver;
@@ -268,6 +270,11 @@ template <class T> struct Body {
   // GPU-mode body aux record (gpu/layout.ts:33-46): gravity scale, damping rates (1/s)
   T gravityScale = 1, linDamp = 0, angDamp = 0;
   uint32_t lifecycle = 0;  // GPU-mode lifecycle bits (layout.ts:17-19): 4 cold
+  // GPU-mode contact reuse (wgsl-collision.ts:20-44): the reference pose (f32, as the device keeps
+  // it; a zero rotation: none yet) and the step at which the body last moved past the tolerances
+  V3<float> refPos{0, 0, 0};
+  Q4<float> refRot{0, 0, 0, 0};
+  uint32_t movedStep = 0;
   std::vector<Force<T>*> forces;
 };
 
@@ -882,6 +889,7 @@ template <class T> struct Manifold : Force<T> {
   std::vector<Contact<T>> contacts;
   M3<T> basis{};
   T friction = 0;
+  uint32_t generated = 0;  // GPU mode: the step whose narrowphase made its contact points
   // GPU mode: which rule set, and the manifold of the same pair last step (warm start)
   Manifold(Solver<T>* s, int a, int b) : Force<T>(s, a, b, K_MANIFOLD) {}
 
@@ -1464,6 +1472,7 @@ template <class T> struct Solver {
   std::vector<std::unique_ptr<Force<T>>> forces;  // creation order
   // GPU mode: colour state, and the manifolds of the last step by pair (warm start)
   int lastColors = 0, lastClashes = 0, lastRounds = 0;
+  uint32_t stepCounter = 0;  // GPU-mode steps taken (the device's step word: manifold generations, moved steps)
 
   void unlink(Force<T>* f) {
     for (int bi : {f->bodyA, f->bodyB}) {
@@ -1620,17 +1629,71 @@ template <class T> struct Solver {
   // feature) → JP colouring (or `fixedColors`) → warm starts → iterations sweeping colours →
   // velocities. Joints keep the creation order; each body sums its joints by slot, then its
   // contacts by (other body, first feature) (wgsl-topology.ts:116-153).
-  void stepGpu(const uint32_t* fixedColors) {
+  // updateRefs (wgsl-collision.ts:28-43) in f32, in the device's operation order, so that both
+  // decide alike: a body without a reference, or moved or turned past the tolerance since its
+  // reference, takes its pose as the new reference and stamps the step.
+  void updateRefs() {
+    for (auto& b : bodies) {
+      V3<float> p{float(b.pos[0]), float(b.pos[1]), float(b.pos[2])};
+      Q4<float> q{float(b.rot[0]), float(b.rot[1]), float(b.rot[2]), float(b.rot[3])};
+      const Q4<float>& r = b.refRot;
+      bool moved = ((r[0] * r[0] + r[1] * r[1]) + r[2] * r[2]) + r[3] * r[3] == 0.0f || length(sub3(p, b.refPos)) > REUSE_LIN_TOL ||
+                   length(qsub(q, r)) > REUSE_ANG_TOL;
+      if (moved) {
+        b.refPos = p;
+        b.refRot = q;
+        b.movedStep = stepCounter;
+      }
+    }
+  }
+  // A manifold's least normal penalty (wgsl-collision.ts contactPenaltyMin)
+  T contactPenaltyMin(const Body<T>& A, const Body<T>& B) const {
+    if (!(flags & FLAG_MASS_PENALTY)) return T(PENALTY_MIN);
+    T mA = A.mass <= 0 ? T(3.4e38) : A.mass, mB = B.mass <= 0 ? T(3.4e38) : B.mass;
+    return clampv(tmin(mA, mB) / (dt * dt), T(PENALTY_MIN), T(PENALTY_MAX));
+  }
+  // copyContacts (wgsl-collision.ts:721-753): last step's manifold of a pair kept, its points'
+  // C(x-) evaluated at the current poses and their multipliers and penalties warm-started
+  std::unique_ptr<Manifold<T>> copyContacts(int a, int b, const Manifold<T>& prev) {
+    Body<T>& A = bodies[a];
+    Body<T>& B = bodies[b];
+    auto m = std::make_unique<Manifold<T>>(this, a, b);
+    m->basis = prev.basis;
+    m->friction = prev.friction;
+    m->generated = prev.generated;
+    const T penaltyMin = contactPenaltyMin(A, B);
+    for (const Contact<T>& o : prev.contacts) {
+      Contact<T> c = o;
+      V3<T> d = sub3(add3(rotate(A.rot, c.rA), A.pos), add3(rotate(B.rot, c.rB), B.pos));
+      c.C0 = V3<T>{dot(V3<T>{m->basis[0], m->basis[1], m->basis[2]}, d) + contactMargin, dot(V3<T>{m->basis[3], m->basis[4], m->basis[5]}, d),
+                   dot(V3<T>{m->basis[6], m->basis[7], m->basis[8]}, d)};
+      for (int k = 0; k < 3; k++) {
+        c.lambda[k] = c.lambda[k] * alpha * gamma;
+        c.penalty[k] = clampv(c.penalty[k] * gamma, T(PENALTY_MIN), T(PENALTY_MAX));
+      }
+      c.penalty[0] = tmax(c.penalty[0], penaltyMin);
+      m->contacts.push_back(c);
+    }
+    return m;
+  }
+
+  // reuseManifolds: every manifold of last step is kept (copyContacts) and no pair is detected
+  // (the substep option of GpuSolver3D.step, gpu/solver.ts:2121-2188).
+  void stepGpu(const uint32_t* fixedColors, bool reuseManifolds = false) {
     gpuMode = true;
+    stepCounter++;
+    if (flags & FLAG_REUSE_CONTACTS) updateRefs();
     int n = int(bodies.size());
     // Last step's manifolds by pair
     std::map<std::pair<int, int>, std::vector<Contact<T>>> prev;
+    std::map<std::pair<int, int>, std::unique_ptr<Force<T>>> prevMan;
     std::vector<std::unique_ptr<Force<T>>> keep;
     for (auto& f : forces) {
       if (f->kind == K_MANIFOLD) {
         auto* m = static_cast<Manifold<T>*>(f.get());
         prev[{m->bodyA, m->bodyB}] = m->contacts;
         unlink(m);
+        prevMan[{m->bodyA, m->bodyB}] = std::move(f);
       } else keep.push_back(std::move(f));
     }
     forces = std::move(keep);
@@ -1643,7 +1706,11 @@ template <class T> struct Solver {
       }
       forces = std::move(kept);
     }
-    auto pr = pairs();
+    std::vector<std::pair<uint32_t, uint32_t>> pr;
+    if (reuseManifolds)
+      for (auto& kv : prevMan) pr.push_back({uint32_t(kv.first.first), uint32_t(kv.first.second)});
+    else
+      pr = pairs();
     std::vector<std::unique_ptr<Manifold<T>>> made(pr.size());
 #pragma omp parallel for schedule(dynamic, 64)
     for (long pi = 0; pi < long(pr.size()); pi++) {
@@ -1651,6 +1718,18 @@ template <class T> struct Solver {
       int a = int(p.first), b = int(p.second);
       Body<T>& A = bodies[a];
       Body<T>& B = bodies[b];
+      {
+        // reuseContacts (wgsl-collision.ts:706-717): last step's points of a pair generated no
+        // earlier than either body's last move; every manifold under reuseManifolds
+        auto pm = prevMan.find({a, b});
+        if (pm != prevMan.end()) {
+          const auto& old = *static_cast<const Manifold<T>*>(pm->second.get());
+          if (reuseManifolds || ((flags & FLAG_REUSE_CONTACTS) && !old.contacts.empty() && old.generated >= std::max(A.movedStep, B.movedStep))) {
+            made[pi] = copyContacts(a, b, old);
+            continue;
+          }
+        }
+      }
       // The GPU's own arithmetic (f32) finds the contacts, so both sides solve one contact set
       Body<float> fA = toFloat(A), fB = toFloat(B);
       V3<float> nf;
@@ -1660,6 +1739,7 @@ template <class T> struct Solver {
       auto m = std::make_unique<Manifold<T>>(this, a, b);
       m->friction = std::sqrt(A.friction * B.friction);
       m->basis = orthonormal(normal);
+      m->generated = stepCounter;
       auto it = prev.find({a, b});
       const std::vector<Contact<T>>* old = it == prev.end() ? nullptr : &it->second;
       bool anySphere = A.shape == SHAPE_SPHERE || B.shape == SHAPE_SPHERE;
@@ -2269,6 +2349,63 @@ void orc_step_gpu(void* h, const unsigned* fixed_colors, int* stats) {
   with(h, [&](auto& s) {
     s.stepGpu(fixed_colors);
     if (stats) { stats[0] = s.lastColors; stats[1] = s.lastClashes; stats[2] = s.lastRounds; }
+    return 0;
+  });
+}
+
+// The GPU-mode step with manifold reuse (the step option reuseManifolds): last step's manifolds are
+// all kept and no pair is detected.
+void orc_step_gpu_reuse(void* h, const unsigned* fixed_colors, int* stats) {
+  with(h, [&](auto& s) {
+    s.stepGpu(fixed_colors, true);
+    if (stats) { stats[0] = s.lastColors; stats[1] = s.lastClashes; stats[2] = s.lastRounds; }
+    return 0;
+  });
+}
+
+// Contact-reuse state (GPU mode): the step counter, per body its reference pose (8 floats: pos,
+// 0, rot) and the step it last moved, per manifold (force order, as orc_get_manifolds) the step
+// that generated its points. Any pointer may be NULL.
+void orc_get_reuse(void* h, unsigned* step, float* refs, unsigned* moved, unsigned* generated) {
+  with(h, [&](auto& s) {
+    using T = std::decay_t<decltype(s.dt)>;
+    if (step) *step = s.stepCounter;
+    for (size_t i = 0; i < s.bodies.size(); i++) {
+      const auto& b = s.bodies[i];
+      if (refs) {
+        for (int k = 0; k < 3; k++) refs[8 * i + k] = b.refPos[k];
+        refs[8 * i + 3] = 0.0f;
+        for (int k = 0; k < 4; k++) refs[8 * i + 4 + k] = b.refRot[k];
+      }
+      if (moved) moved[i] = b.movedStep;
+    }
+    int mi = 0;
+    for (auto& f : s.forces)
+      if (f->kind == K_MANIFOLD) {
+        if (generated) generated[mi] = static_cast<Manifold<T>*>(f.get())->generated;
+        mi++;
+      }
+    return 0;
+  });
+}
+void orc_set_reuse(void* h, unsigned step, const float* refs, const unsigned* moved, const unsigned* generated) {
+  with(h, [&](auto& s) {
+    using T = std::decay_t<decltype(s.dt)>;
+    s.stepCounter = step;
+    for (size_t i = 0; i < s.bodies.size(); i++) {
+      auto& b = s.bodies[i];
+      if (refs) {
+        for (int k = 0; k < 3; k++) b.refPos[k] = refs[8 * i + k];
+        for (int k = 0; k < 4; k++) b.refRot[k] = refs[8 * i + 4 + k];
+      }
+      if (moved) b.movedStep = moved[i];
+    }
+    int mi = 0;
+    for (auto& f : s.forces)
+      if (f->kind == K_MANIFOLD) {
+        if (generated) static_cast<Manifold<T>*>(f.get())->generated = generated[mi];
+        mi++;
+      }
     return 0;
   });
 }

@@ -51,6 +51,10 @@ def lib():
         L.orc_get_manifolds.argtypes = [P, D, D]
         L.orc_set_contact_penalty.argtypes = [P, ctypes.c_double]
         L.orc_round_f32.argtypes = [P]
+        L.orc_step_gpu_reuse.argtypes = [P, ctypes.POINTER(U), ctypes.POINTER(I)]
+        F, PU = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(U)
+        L.orc_get_reuse.argtypes = [P, PU, F, PU, PU]
+        L.orc_set_reuse.argtypes = [P, U, F, PU, PU]
         L.orc_set_manifolds.argtypes = [P, I, D, I, D]
         L.orc_step.argtypes = [P]
         L.orc_step_gpu.argtypes = [P, ctypes.POINTER(U), ctypes.POINTER(I)]
@@ -326,14 +330,36 @@ class Oracle:
         for _ in range(n):
             self.L.orc_step(self.h)
 
-    def step_gpu(self, fixed_colors=None):
+    def step_gpu(self, fixed_colors=None, reuse_manifolds: bool = False):
+        """One GPU-mode step; reuse_manifolds: keep every manifold of last step, detect no pair (the
+        step option reuseManifolds)."""
         stats = (ctypes.c_int * 3)()
+        fn = self.L.orc_step_gpu_reuse if reuse_manifolds else self.L.orc_step_gpu
         if fixed_colors is None:
-            self.L.orc_step_gpu(self.h, None, stats)
+            fn(self.h, None, stats)
         else:
             fc = np.ascontiguousarray(fixed_colors, dtype=np.uint32)
-            self.L.orc_step_gpu(self.h, fc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), stats)
+            fn(self.h, fc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), stats)
         return {'colors': stats[0], 'clashes': stats[1], 'rounds': stats[2]}
+
+    def reuse_state(self) -> dict:
+        """Contact-reuse state: step counter, reference poses (n, 8), moved steps, manifold generations."""
+        n = self.body_count
+        nm = self.L.orc_manifold_count(self.h)
+        step = ctypes.c_uint()
+        refs = np.zeros((max(n, 1), 8), dtype=np.float32)
+        moved = np.zeros(max(n, 1), dtype=np.uint32)
+        gen = np.zeros(max(nm, 1), dtype=np.uint32)
+        F, PU = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint)
+        self.L.orc_get_reuse(self.h, ctypes.byref(step), refs.ctypes.data_as(F), moved.ctypes.data_as(PU), gen.ctypes.data_as(PU))
+        return {'step': step.value, 'refs': refs[:n], 'moved': moved[:n], 'generated': gen[:nm]}
+
+    def set_reuse_state(self, step: int, refs, moved, generated):
+        F, PU = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint)
+        refs = np.ascontiguousarray(refs, dtype=np.float32).reshape(-1, 8)
+        moved = np.ascontiguousarray(moved, dtype=np.uint32)
+        gen = np.ascontiguousarray(generated, dtype=np.uint32)
+        self.L.orc_set_reuse(self.h, int(step), refs.ctypes.data_as(F), moved.ctypes.data_as(PU), gen.ctypes.data_as(PU) if gen.size else None)
 
     def pairs(self) -> np.ndarray:
         cap = 1 << 16

@@ -51,6 +51,28 @@ def test_defaults_and_invalid_arguments_without_a_device():
     assert lib.avbd_set_world_anchor(None, 0, None) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_body_storage(None, None) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_contact_storage(None, 0, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_step_with(None, 1, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_read_reuse_state(None, None, 0, None, None, 0, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_apply_pushes(None, None, 0) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_contact_watch_create(None, 16, 16, None) == _abi.AVBD_ERR_INVALID
+    assert lib.avbd_contact_watch_destroy(None) == 0
+    assert lib.avbd_raycast(None, None, 0, None, 0, 0, None) == _abi.AVBD_ERR_INVALID
+
+
+def test_world_params_are_the_reference_production_defaults():
+    """avbd_world_params (gpuParams3D(), gpu/solver.ts:216-230): every GPU-only rule on, up = +y;
+    avbd_default_params keeps the parity setting (rules off, up = +z)."""
+    lib = avbd_b200.load()
+    p = _abi.Params()
+    assert lib.avbd_world_params(ctypes.byref(p)) == 0
+    rules = _abi.FLAG_MATCH_NEAREST | _abi.FLAG_FACE_BIAS | _abi.FLAG_REUSE_CONTACTS | _abi.FLAG_START_AT_REST | _abi.FLAG_MASS_PENALTY
+    assert p.flags == rules and tuple(p.up) == (0.0, 1.0, 0.0) and abs(p.contact_margin - 0.01) < 1e-9 and p.iterations == 10
+
+
+def test_query_record_layouts():
+    assert _abi.PUSH_DTYPE.itemsize == 40 and _abi.EVENT_DTYPE.itemsize == 48
+    assert _abi.RAY_DTYPE.itemsize == 32 and _abi.HIT_DTYPE.itemsize == 32
+    assert ctypes.sizeof(_abi.BatchTuning) == 4 + 4 * 16 * 4 + 4 * 5
 
 
 def test_create_fails_loudly_without_a_b200():

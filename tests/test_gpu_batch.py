@@ -167,7 +167,8 @@ def test_batch_tuner_and_host_buffers(cuda_lib):
     b = _batch_for(scenes)
     b.step(5)
     t = b.tune(2)
-    assert len(t['candidates']) >= 3 and all(c['ms_per_step'] > 0 for c in t['candidates'])
+    assert len(t['candidates']) >= 6 and all(c['ms_per_step'] > 0 for c in t['candidates'])
+    assert {c['rows_per_lane'] for c in t['candidates']} == {1, 4} and t['rows_per_lane'] in (1, 4)  # bodies per warp tuned too
     assert t['ms_per_step'] == min(c['ms_per_step'] for c in t['candidates'])
     info = b.info()
     assert info['collide_threads'] == t['collide_threads'] and info['solve_blocks'] == t['solve_blocks']

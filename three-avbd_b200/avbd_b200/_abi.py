@@ -25,7 +25,7 @@ AVBD_ERR_NO_DEVICE = -5
 
 SHAPE_BOX, SHAPE_SPHERE, SHAPE_SAIL = 0, 1, 2
 T_NONE, T_JOINT, T_SPRING = 0, 1, 2
-FLAG_MATCH_NEAREST, FLAG_FACE_BIAS, FLAG_START_AT_REST, FLAG_MASS_PENALTY = 1, 2, 8, 16
+FLAG_MATCH_NEAREST, FLAG_FACE_BIAS, FLAG_REUSE_CONTACTS, FLAG_START_AT_REST, FLAG_MASS_PENALTY = 1, 2, 4, 8, 16
 STICK_BIT = 0x80000000
 NO_COLOR = 255
 PENDING = 256
@@ -50,9 +50,17 @@ CONTACT_DTYPE = np.dtype([
     ('r_a', '<f4', 3), ('key', '<u4'), ('r_b', '<f4', 3), ('c0_n', '<f4'), ('pen', '<f4', 3), ('c0_t1', '<f4'),
     ('lam', '<f4', 3), ('c0_t2', '<f4'),
 ])
+PUSH_DTYPE = np.dtype([('body', '<u4'), ('lin', '<f4', 3), ('off_lin', '<f4', 3), ('moment', '<f4', 3)])
+EVENT_DTYPE = np.dtype([('kind', '<u4'), ('a', '<u4'), ('b', '<u4'), ('step', '<u4'), ('point', '<f4', 3), ('impulse', '<f4'),
+                        ('normal', '<f4', 3), ('pad', '<f4')])
+RAY_DTYPE = np.dtype([('origin', '<f4', 3), ('max_distance', '<f4'), ('direction', '<f4', 3), ('pad', '<f4')])
+HIT_DTYPE = np.dtype([('body', '<i4'), ('distance', '<f4'), ('point', '<f4', 3), ('normal', '<f4', 3)])
+CONTACT_BEGIN, CONTACT_END = 1, 2
+RAY_MAX, RAY_MAX_IGNORED = 65535, 16
 STEP_STATS_DTYPE = np.dtype([('collision_ms', '<f4'), ('solve_ms', '<f4')] + [(n, '<u4') for n in (
     'pairs', 'contacts', 'manifolds', 'adjacency', 'incidences', 'dynamic_bodies', 'colors', 'rounds', 'launches', 'error')])
 assert BODY_DTYPE.itemsize == 160 and JOINT_DTYPE.itemsize == 160 and MANIFOLD_DTYPE.itemsize == 32 and CONTACT_DTYPE.itemsize == 64
+assert PUSH_DTYPE.itemsize == 40 and EVENT_DTYPE.itemsize == 48 and RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 32
 
 
 class Params(ctypes.Structure):
@@ -97,6 +105,10 @@ class BatchConfig(ctypes.Structure):
                 ('pairs_per_body', ctypes.c_uint32), ('device', ctypes.c_int32)]
 
 
+class StepOptions(ctypes.Structure):
+    _fields_ = [('reuse_manifolds', ctypes.c_uint32)]
+
+
 class BatchWorld(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ('first_body', 'bodies', 'first_joint', 'joints', 'pair_capacity', 'fixed_colors')]
 
@@ -109,15 +121,15 @@ class BatchStatus(ctypes.Structure):
 
 NOALLOC_MAX_BODIES = 4096
 NOALLOC_MAX_PAIRS = 32768
-TUNE_CANDIDATES = 8
+TUNE_CANDIDATES = 16
 BATCH_MAX_WORLD_BODIES = 4096
 
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [('candidates', ctypes.c_uint32), ('candidate_threads', ctypes.c_uint32 * TUNE_CANDIDATES),
-                ('candidate_solve_blocks', ctypes.c_uint32 * TUNE_CANDIDATES), ('candidate_ms', ctypes.c_float * TUNE_CANDIDATES),
-                ('collide_threads', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32), ('ms_per_step', ctypes.c_float),
-                ('steps_taken', ctypes.c_uint32)]
+                ('candidate_solve_blocks', ctypes.c_uint32 * TUNE_CANDIDATES), ('candidate_rows_per_lane', ctypes.c_uint32 * TUNE_CANDIDATES),
+                ('candidate_ms', ctypes.c_float * TUNE_CANDIDATES), ('collide_threads', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32),
+                ('rows_per_lane', ctypes.c_uint32), ('ms_per_step', ctypes.c_float), ('steps_taken', ctypes.c_uint32)]
 
 
 # Every function include/avbd.h declares, with its argument types (the C-ABI symbol table)
@@ -132,6 +144,7 @@ SIGNATURES = {
     'avbd_set_params': ([P, ctypes.POINTER(Params)], I),
     'avbd_get_params': ([P, ctypes.POINTER(Params)], I),
     'avbd_default_params': ([ctypes.POINTER(Params)], I),
+    'avbd_world_params': ([ctypes.POINTER(Params)], I),
     'avbd_add_bodies': ([P, VP, U, PU], I),
     'avbd_write_bodies': ([P, U, VP, U, I], I),
     'avbd_write_bodies_at': ([P, PU, VP, U], I),
@@ -151,6 +164,16 @@ SIGNATURES = {
     'avbd_seed_contacts': ([P, VP, U, VP, U], I),
     'avbd_set_fixed_colors': ([P, PU, U], I),
     'avbd_step': ([P, I], I),
+    'avbd_step_with': ([P, I, ctypes.POINTER(StepOptions)], I),
+    'avbd_apply_pushes': ([P, VP, U], I),
+    'avbd_contact_watch_create': ([P, U, U, ctypes.POINTER(P)], I),
+    'avbd_contact_watch_destroy': ([P], I),
+    'avbd_contact_watch_last_error': ([P], ctypes.c_char_p),
+    'avbd_contact_watch_set': ([P, PU, PU, PU, U], I),
+    'avbd_contact_watch_run': ([P, U, ctypes.c_float], I),
+    'avbd_contact_watch_read': ([P, VP, U, PU, PU, PU], I),
+    'avbd_raycast': ([P, VP, U, PU, U, U, VP], I),
+    'avbd_read_reuse_state': ([P, ctypes.POINTER(ctypes.c_float), U, PU, PU, U, PU], I),
     'avbd_synchronize': ([P], I),
     'avbd_read_bodies': ([P, VP, U, PU], I),
     'avbd_read_joints': ([P, VP, VP, U, PU], I),

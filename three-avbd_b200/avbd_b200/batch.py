@@ -104,9 +104,9 @@ class BatchSolver3D:
         self._check(self.lib.avbd_batch_tune(self.handle, steps, ctypes.byref(t)))
         k = t.candidates
         return {'candidates': [{'collide_threads': t.candidate_threads[i], 'solve_blocks': t.candidate_solve_blocks[i],
-                                'ms_per_step': t.candidate_ms[i]} for i in range(k)],
-                'collide_threads': t.collide_threads, 'solve_blocks': t.solve_blocks, 'ms_per_step': t.ms_per_step,
-                'steps_taken': t.steps_taken}
+                                'rows_per_lane': t.candidate_rows_per_lane[i], 'ms_per_step': t.candidate_ms[i]} for i in range(k)],
+                'collide_threads': t.collide_threads, 'solve_blocks': t.solve_blocks, 'rows_per_lane': t.rows_per_lane,
+                'ms_per_step': t.ms_per_step, 'steps_taken': t.steps_taken}
 
     @property
     def stream(self) -> int:

@@ -378,8 +378,50 @@ class CudaSolver3D:
         return colors
 
     # --- stepping ---
-    def step(self, n: int = 1):
-        self._check(self.lib.avbd_step(self.handle, n))
+    def step(self, n: int = 1, reuse_manifolds: bool = False):
+        """step(options) (gpu/solver.ts:2112): n steps; reuse_manifolds keeps last step's manifolds
+        and detects no pair (substeps after a detecting step; applies while they are valid)."""
+        if reuse_manifolds:
+            opts = _abi.StepOptions(reuse_manifolds=1)
+            self._check(self.lib.avbd_step_with(self.handle, n, ctypes.byref(opts)))
+        else:
+            self._check(self.lib.avbd_step(self.handle, n))
+
+    # --- around the step: impulses, contact events, raycasts ---
+    def apply_pushes(self, pushes: np.ndarray):
+        """Pusher.apply (src/lib/push.ts:103-131): PUSH_DTYPE records (body, lin, off_lin, moment), one
+        per body, applied to the velocities now, before the next step."""
+        pushes = np.ascontiguousarray(pushes, dtype=_abi.PUSH_DTYPE)
+        self._check(self.lib.avbd_apply_pushes(self.handle, ptr(pushes), len(pushes)))
+
+    def contact_watch(self, pairs: int, capacity: int = 4096) -> 'ContactWatch':
+        """A ContactWatch (src/lib/contacts.ts) on this world's contacts."""
+        return ContactWatch(self, pairs, capacity)
+
+    def raycast(self, origins, directions, max_distance=None, ignore=(), mask: int = 0xFFFFFFFF) -> np.ndarray:
+        """Raycaster.cast (src/lib/raycast.ts:170-251): the nearest hit of each ray (HIT_DTYPE; body -1: none)."""
+        o = np.asarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.asarray(directions, dtype=np.float32).reshape(-1, 3)
+        rays = np.zeros(len(o), dtype=_abi.RAY_DTYPE)
+        rays['origin'] = o
+        rays['direction'] = d
+        rays['max_distance'] = 3.0e38 if max_distance is None else np.asarray(max_distance, dtype=np.float32)
+        ig = np.ascontiguousarray(ignore, dtype=np.uint32)
+        hits = np.zeros(len(o), dtype=_abi.HIT_DTYPE)
+        self._check(self.lib.avbd_raycast(self.handle, ptr(rays), len(rays), uptr(ig) if ig.size else None, ig.size, mask, ptr(hits)))
+        return hits
+
+    def read_reuse_state(self) -> dict:
+        """Contact-reuse state: reference poses (n, 8), moved steps (per body) and the generating step
+        of each manifold (avbd_read_contacts' order)."""
+        nb, nm = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.lib.avbd_read_reuse_state(self.handle, None, 0, ctypes.byref(nb), None, 0, ctypes.byref(nm)))
+        refs = np.zeros((max(nb.value, 1), 8), dtype=np.float32)
+        gen = np.zeros(max(nm.value, 1), dtype=np.uint32)
+        self._check(self.lib.avbd_read_reuse_state(self.handle, refs.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), nb.value, ctypes.byref(nb),
+                                                   uptr(gen), nm.value, ctypes.byref(nm)))
+        moved = self.read_bodies()['moved_step'].view(np.uint32).copy()
+        return {'refs': refs[:nb.value], 'moved': moved, 'generated': gen[:nm.value], 'step': self.read_counters()['steps']}
 
     def synchronize(self):
         self._check(self.lib.avbd_synchronize(self.handle))
@@ -487,6 +529,47 @@ class CudaSolver3D:
         out = np.zeros(n.value, dtype=np.uint32)
         self._check(self.lib.avbd_read_colors(self.handle, uptr(out), n.value, ctypes.byref(n)))
         return out
+
+
+class ContactWatch:
+    """ContactWatch (src/lib/contacts.ts:129-267) over the C ABI: begin and end events of the touching
+    pairs that have a reporting body, by lifetime IDs. Run it after each step; read drains the events."""
+
+    def __init__(self, world: CudaSolver3D, pairs: int, capacity: int = 4096):
+        self.world = world
+        self.lib = world.lib
+        h = ctypes.c_void_p()
+        world._check(self.lib.avbd_contact_watch_create(world.handle, pairs, capacity, ctypes.byref(h)))
+        self.handle = h
+        self.capacity = capacity
+
+    def _check(self, code: int):
+        if code != _abi.AVBD_OK:
+            msg = self.lib.avbd_contact_watch_last_error(self.handle)
+            raise _abi.error(code, msg.decode() if msg else 'contact watch error')
+
+    def set_watched(self, indices, ids, on):
+        i = np.ascontiguousarray(indices, dtype=np.uint32)
+        d = np.ascontiguousarray(ids, dtype=np.uint32)
+        o = np.ascontiguousarray(np.asarray(on, dtype=bool).astype(np.uint32))
+        if not (len(i) == len(d) == len(o)):
+            raise _abi.error(_abi.AVBD_ERR_INVALID, 'set_watched: indices, ids and on differ in length')
+        self._check(self.lib.avbd_contact_watch_set(self.handle, uptr(i), uptr(d), uptr(o), len(i)))
+
+    def run(self, step: int, dt: float):
+        self._check(self.lib.avbd_contact_watch_run(self.handle, step, dt))
+
+    def read(self):
+        """(events EVENT_DTYPE in step order, dropped, full)."""
+        out = np.zeros(self.capacity, dtype=_abi.EVENT_DTYPE)
+        n, dropped, full = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.lib.avbd_contact_watch_read(self.handle, ptr(out), self.capacity, ctypes.byref(n), ctypes.byref(dropped), ctypes.byref(full)))
+        return out[:n.value], dropped.value, bool(full.value)
+
+    def destroy(self):
+        if getattr(self, 'handle', None):
+            self.lib.avbd_contact_watch_destroy(self.handle)
+            self.handle = None
 
 
 def find_pairs_noalloc(bodies: np.ndarray, groups_mask: np.ndarray | None = None, cap: int = _abi.NOALLOC_MAX_PAIRS,

@@ -23,6 +23,7 @@ UNITS = {
     'avbd_hull.cu': [],
     'avbd_adjoint.cu': [],
     'avbd_record.cu': [],
+    'avbd_query.cu': [],
 }
 
 

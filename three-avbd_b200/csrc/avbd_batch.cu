@@ -45,6 +45,7 @@ struct avbd_batch {
   uint32_t stepCount = 0;
   // launch shape (the autotuner's choice)
   int sms = 0, collideThreads = 128, collideBlocks = 0, solveBlocks = 0;
+  uint32_t rowsPerLane = 1;  // the solve's least rows a lane (bodies per warp), chosen by the tuner
   // status of the last step, copied back asynchronously
   uint32_t* hStatus = nullptr;
   cudaEvent_t statusReady = nullptr;
@@ -276,6 +277,7 @@ BatchLaunch makeLaunch(avbd_batch* b) {
   p.upz = a.up[2];
   p.step = b->stepCount;
   p.colorCap = MAX_COLORS;
+  p.rowsPerLane = b->rowsPerLane;
   p.cur = b->cur;
   return L;
 }
@@ -464,7 +466,7 @@ int avbd_batch_create(const avbd_batch_config* cfg, avbd_batch** out) {
   const size_t B = b->bodyCap, W = b->worldCap;
   bool ok = true;
   auto A = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
-  for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel, &d.dlin, &d.dang, &d.aabb}) A(balloc(b, f, B));
+  for (float4** f : {&d.pos, &d.rot, &d.ipos, &d.irot, &d.size, &d.moment, &d.ypos, &d.yrot, &d.vel, &d.avel, &d.dlin, &d.dang, &d.ylin, &d.yang, &d.refPos, &d.refRot, &d.aabb}) A(balloc(b, f, B));
   A(balloc(b, &d.filters, B));
   A(balloc(b, &b->staging, size_t(B) * 10));
   A(balloc(b, &d.cell, B));
@@ -812,13 +814,17 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
   BATCH_TRY(b, cudaEventCreate(&e1));
   float best = INFINITY;
   int bestT = b->collideThreads, bestS = b->solveBlocks;
+  uint32_t bestR = b->rowsPerLane;
   const bool graphs = b->useGraphs;
   b->useGraphs = false;
   uint32_t k = 0;
+  const uint32_t rowsPerLane[2] = {1, 4};  // a body's rows over as many lanes as its colour allows, or 4 a lane at least
+  for (int ri = 0; ri < 2; ri++)
   for (int ti = 0; ti < 3; ti++)
     for (int sp = 1; sp <= solvePer && k < AVBD_BATCH_TUNE_CANDIDATES; sp++) {
       b->collideThreads = threads[ti];
       b->solveBlocks = b->sms * sp;
+      b->rowsPerLane = rowsPerLane[ri];
       launchShape(b);
       r = avbd_batch_step(b, 1);  // settle storage for this shape
       if (!r) r = avbd_batch_synchronize(b);
@@ -833,12 +839,14 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
       ms /= float(steps);
       t.candidate_threads[k] = uint32_t(threads[ti]);
       t.candidate_solve_blocks[k] = uint32_t(b->solveBlocks);
+      t.candidate_rows_per_lane[k] = rowsPerLane[ri];
       t.candidate_ms[k] = ms;
       k++;
       if (ms < best) {
         best = ms;
         bestT = threads[ti];
         bestS = b->solveBlocks;
+        bestR = rowsPerLane[ri];
       }
     }
   cudaEventDestroy(e0);
@@ -846,12 +854,14 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
   b->useGraphs = graphs;
   b->collideThreads = bestT;
   b->solveBlocks = bestS;
+  b->rowsPerLane = bestR;
   launchShape(b);
   b->configGen++;
   if (r) return r;
   t.candidates = k;
   t.collide_threads = uint32_t(bestT);
   t.solve_blocks = uint32_t(bestS);
+  t.rows_per_lane = bestR;
   t.ms_per_step = best;
   t.steps_taken = k * uint32_t(steps + 1);
   if (out) *out = t;
@@ -863,8 +873,8 @@ int avbd_batch_record_start(avbd_batch* b, uint32_t steps, uint32_t points_per_b
   if (b->worlds.empty()) return bfail(b, AVBD_ERR_INVALID, "the batch has no worlds");
   if (b->nj) return bfail(b, AVBD_ERR_INVALID, "the adjoint differentiates contacts only: the batch holds joints");
   const avbd_params& P = b->params;
-  if (P.flags & (AVBD_FLAG_MATCH_NEAREST | AVBD_FLAG_MASS_PENALTY | AVBD_FLAG_START_AT_REST))
-    return bfail(b, AVBD_ERR_INVALID, "the adjoint follows the default contact rules: no nearest matching, mass penalty or start at rest");
+  if (P.flags & (AVBD_FLAG_MATCH_NEAREST | AVBD_FLAG_MASS_PENALTY | AVBD_FLAG_START_AT_REST | AVBD_FLAG_REUSE_CONTACTS))
+    return bfail(b, AVBD_ERR_INVALID, "the adjoint follows the default contact rules: no nearest matching, mass penalty, start at rest or contact reuse");
   if (P.up[0] != 0.0f || P.up[1] != 0.0f || P.up[2] != 1.0f) return bfail(b, AVBD_ERR_INVALID, "the adjoint needs up = +z");
   cudaSetDevice(b->device);
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));

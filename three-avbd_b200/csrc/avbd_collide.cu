@@ -83,6 +83,112 @@ __device__ inline int hashFind(const DWorld& w, const StepParams& p, uint32_t a,
   return -1;
 }
 
+// --- contact reuse (wgsl-collision.ts:20-44, 706-762) -------------------------------------------------
+// updateRefs: a body without a reference pose, or moved or turned past the tolerance since it, takes
+// its pose (x-) as the new reference and stamps this step into its moved_step word (ypos.w)
+__device__ inline void updateRef(const DWorld& w, uint32_t i, uint32_t step) {
+  const float3 pos = f3(w.pos[i]);
+  const float4 rot = w.rot[i];
+  const float4 ref = w.refRot[i];
+  bool moved = ((ref.x * ref.x + ref.y * ref.y) + ref.z * ref.z) + ref.w * ref.w == 0.0f || len3(pos - f3(w.refPos[i])) > REUSE_LIN_TOL ||
+               len3(qsub(rot, ref)) > REUSE_ANG_TOL;
+  if (moved) {
+    w.refPos[i] = make_float4(pos.x, pos.y, pos.z, 0.0f);
+    w.refRot[i] = rot;
+    w.ypos[i].w = __uint_as_float(step);
+  }
+}
+__global__ void k_update_refs(DWorld w, StepParams p) {
+  const uint32_t step = w.counters[C_STEP];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x)
+    if (((uint32_t)w.ipos[i].w & 2u) == 0u) updateRef(w, i, step);
+}
+
+// A contact's least normal penalty (wgsl-collision.ts contactPenaltyMin): with FLAG_MASS_PENALTY the
+// lighter dynamic body's m/dt^2
+__device__ inline float contactPenaltyMin(const DWorld& w, const StepParams& p, uint32_t a, uint32_t b) {
+  if (!(p.flags & FLAG_MASS_PENALTY)) return PENALTY_MIN;
+  float mA = w.size[a].w <= 0.0f ? 3.4e38f : w.size[a].w;
+  float mB = w.size[b].w <= 0.0f ? 3.4e38f : w.size[b].w;
+  return fminf(fmaxf(fminf(mA, mB) / (p.dt * p.dt), PENALTY_MIN), PENALTY_MAX);
+}
+
+// Counts a manifold of `count` points into the step's counters, one atomic per coalesced group
+__device__ __forceinline__ void countManifold(const DWorld& w, uint32_t count) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t pts = cg::reduce(g, count, cg::plus<uint32_t>());
+  uint32_t nonEmpty = cg::reduce(g, count > 0u ? 1u : 0u, cg::plus<uint32_t>());
+  if (g.thread_rank() == 0) {
+    atomicAdd(&w.counters[C_CONTACTS], pts);
+    atomicAdd(&w.counters[C_MANIFOLDS], nonEmpty);
+  }
+}
+
+// copyContacts (wgsl-collision.ts:721-753): last step's manifold in slot pm kept as this step's
+// manifold in slot pi (ids with its generation step, normal, friction, points with their keys and
+// anchors), each point's C(x-) evaluated at the current poses and its multipliers and penalties
+// warm-started as a fresh point's are
+__device__ void copyContacts(const DWorld& w, const StepParams& p, uint32_t pi, uint32_t pm) {
+  const int cur = p.cur, prev = 1 - cur;
+  const uint4 ids = w.mIds[prev][pm];
+  const uint32_t a = ids.x, b = ids.y, count = min(ids.w & 15u, (uint32_t)MAX_CONTACTS);
+  const float4 geo = w.mGeo[prev][pm];
+  w.mIds[cur][pi] = make_uint4(a, b, pi * MAX_CONTACTS, ids.w);
+  w.mGeo[cur][pi] = geo;
+  countManifold(w, count);
+  const float3 n = f3(geo);
+  float3 t1, t2;
+  orthonormal(n, t1, t2);
+  const float3 cA = f3(w.pos[a]), cB = f3(w.pos[b]);
+  const float4 qA = w.rot[a], qB = w.rot[b];
+  const float penaltyMin = contactPenaltyMin(w, p, a, b);
+  for (uint32_t i = 0; i < count; i++) {
+    const float4* q = w.cPt[prev] + 4 * (size_t(ids.z) + i);
+    const float4 ra = q[K_RA], rb = q[K_RB];
+    float3 pen = f3(q[K_PEN]), lam = f3(q[K_LAM]);
+    const float3 d = (cA - cB) + (qrotate(qA, f3(ra)) - qrotate(qB, f3(rb)));
+    const float c0x = dot3(n, d) + p.margin, c0y = dot3(t1, d), c0z = dot3(t2, d);
+    lam = lam * p.alpha * p.gamma;
+    pen = make_float3(fminf(fmaxf(pen.x * p.gamma, PENALTY_MIN), PENALTY_MAX), fminf(fmaxf(pen.y * p.gamma, PENALTY_MIN), PENALTY_MAX),
+                      fminf(fmaxf(pen.z * p.gamma, PENALTY_MIN), PENALTY_MAX));
+    pen.x = fmaxf(pen.x, penaltyMin);
+    float4* o = w.cPt[cur] + 4 * (size_t(pi) * MAX_CONTACTS + i);
+    o[K_RA] = ra;
+    o[K_RB] = make_float4(rb.x, rb.y, rb.z, c0x);
+    o[K_PEN] = make_float4(pen.x, pen.y, pen.z, c0y);
+    o[K_LAM] = make_float4(lam.x, lam.y, lam.z, c0z);
+  }
+}
+
+// reuseContacts (wgsl-collision.ts:706-717): the pair keeps last step's points when they were
+// generated no earlier than either body's last move
+__device__ inline bool reusePair(const DWorld& w, const StepParams& p, uint32_t pi, uint32_t a, uint32_t b) {
+  const int pm = hashFind(w, p, a, b);
+  if (pm < 0) return false;
+  const uint32_t idw = w.mIds[1 - p.cur][pm].w;
+  const uint32_t moved = max(__float_as_uint(w.ypos[a].w), __float_as_uint(w.ypos[b].w));
+  if ((idw & 15u) == 0u || (idw >> 4) < moved) return false;
+  copyContacts(w, p, pi, (uint32_t)pm);
+  return true;
+}
+
+// reuseManifolds (wgsl-collision.ts:755-762): every pair slot of last step kept in the same slot,
+// its manifold copied; the step detects no pair
+__global__ void k_reuse_manifolds(DWorld w, StepParams p) {
+  const uint32_t total = w.counters[C_PREV_PAIRS];
+  const int prev = 1 - p.cur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[C_PAIRS] = total;
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
+    const uint4 ids = w.mIds[prev][m];
+    w.pairs[m] = make_uint2(ids.x, ids.y);
+    if ((ids.w & 15u) == 0u) {
+      w.mIds[p.cur][m] = make_uint4(ids.x, ids.y, m * MAX_CONTACTS, ids.w & ~15u);
+      continue;
+    }
+    copyContacts(w, p, m, m);
+  }
+}
+
 // --- grid keys: cellHash (wgsl-collision.ts:121-128), one level -----------------------------------
 __device__ inline int4 cellOf(float3 x, float size) {
   return make_int4((int)floorf(x.x / size), (int)floorf(x.y / size), (int)floorf(x.z / size), 0);
@@ -1175,6 +1281,7 @@ __device__ void narrowPair(const DWorld& w, const StepParams& p, uint32_t pi) {
     sat.valid = false;
     Found found;
     found.count = 0;
+    if ((p.flags & FLAG_REUSE_CONTACTS) && reusePair(w, p, pi, a, b)) return;
     bool sphereA = w.avel[a].w == SHAPE_SPHERE_F, sphereB = w.avel[b].w == SHAPE_SPHERE_F;
     float4 qA = w.rot[a], qB = w.rot[b];
     if (sphereA && sphereB) {
@@ -1226,15 +1333,7 @@ __device__ __forceinline__ void writeManifold(const DWorld& w, const StepParams&
     float fa = w.pos[a].w, fb = w.pos[b].w;
     w.mIds[cur][pi] = make_uint4(a, b, pi * MAX_CONTACTS, count | (w.counters[C_STEP] << 4));
     w.mGeo[cur][pi] = make_float4(n.x, n.y, n.z, sqrtf(fa * fb));
-    {
-      cg::coalesced_group g = cg::coalesced_threads();
-      uint32_t pts = cg::reduce(g, count, cg::plus<uint32_t>());
-      uint32_t nonEmpty = cg::reduce(g, count > 0u ? 1u : 0u, cg::plus<uint32_t>());
-      if (g.thread_rank() == 0) {
-        atomicAdd(&w.counters[C_CONTACTS], pts);
-        atomicAdd(&w.counters[C_MANIFOLDS], nonEmpty);
-      }
-    }
+    countManifold(w, count);
     if (count == 0u) return;
     float3 t1, t2;
     orthonormal(n, t1, t2);
@@ -1247,12 +1346,7 @@ __device__ __forceinline__ void writeManifold(const DWorld& w, const StepParams&
     }
     bool matchNearest = (p.flags & FLAG_MATCH_NEAREST) != 0u;
     float minSide = fminf(fminf(fminf(A.h.x, A.h.y), A.h.z), fminf(fminf(B.h.x, B.h.y), B.h.z)) * 2.0f;
-    float penaltyMin = PENALTY_MIN;
-    if (p.flags & FLAG_MASS_PENALTY) {
-      float mA = w.size[a].w <= 0.0f ? 3.4e38f : w.size[a].w;
-      float mB = w.size[b].w <= 0.0f ? 3.4e38f : w.size[b].w;
-      penaltyMin = fminf(fmaxf(fminf(mA, mB) / (p.dt * p.dt), PENALTY_MIN), PENALTY_MAX);
-    }
+    const float penaltyMin = contactPenaltyMin(w, p, a, b);
     float3 cA = A.c, cB = B.c;
     for (uint32_t i = 0; i < count; i++) {
       float3 rA = qrotate(qconj(qA), found.xA[i] - cA);
@@ -1288,7 +1382,8 @@ __device__ __forceinline__ void writeManifold(const DWorld& w, const StepParams&
           rB = f3(q[K_RB]);
         }
       }
-      float3 d = (qrotate(qA, rA) + cA) - (qrotate(qB, rB) + cB);
+      // the centres' difference first (exact for nearby bodies at any distance from the origin)
+      float3 d = (cA - cB) + (qrotate(qA, rA) - qrotate(qB, rB));
       float c0x = dot3(n, d) + p.margin, c0y = dot3(t1, d), c0z = dot3(t2, d);
       lam = lam * p.alpha * p.gamma;
       pen = make_float3(fminf(fmaxf(pen.x * p.gamma, PENALTY_MIN), PENALTY_MAX), fminf(fmaxf(pen.y * p.gamma, PENALTY_MIN), PENALTY_MAX),
@@ -1362,6 +1457,9 @@ __global__ void __launch_bounds__(256) k_batch_collide(BatchLaunch B) {
     }
     for (uint32_t h = threadIdx.x; h <= d.hashMask; h += blockDim.x) w.hash[h] = 0u;
     __syncthreads();
+    if (p.flags & FLAG_REUSE_CONTACTS)  // updateRefs, per world
+      for (uint32_t i = threadIdx.x; i < d.n; i += blockDim.x)
+        if (((uint32_t)w.ipos[i].w & 2u) == 0u) updateRef(w, i, c[C_STEP]);
     const int prev = 1 - p.cur;
     for (uint32_t m = threadIdx.x; m < prevPairs; m += blockDim.x) {  // hashInsert, per world
       uint4 ids = w.mIds[prev][m];
@@ -1439,10 +1537,19 @@ __global__ void k_step_stats(DWorld w, uint32_t launches) {
 void launch_step_stats(const DWorld& w, uint32_t launches, cudaStream_t s) { k_step_stats<<<1, 32, 0, s>>>(w, launches); }
 
 // Host: the collision phase, enqueued on `s`. Returns the number of kernels it launched.
-uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s) {
+uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, bool reuseManifolds, cudaStream_t s) {
   const uint32_t n = p.n;
-  uint32_t launches = 3;  // begin, hash insert, narrowphase
   k_begin<<<1, 1, 0, s>>>(w, p);
+  uint32_t launches = 1;
+  if ((p.flags & FLAG_REUSE_CONTACTS) && n > 0) {
+    k_update_refs<<<grid_for(n, 256), 256, 0, s>>>(w, p);
+    launches++;
+  }
+  if (reuseManifolds) {
+    k_reuse_manifolds<<<GS_BLOCKS, 128, 0, s>>>(w, p);
+    return launches + 1;
+  }
+  launches += 2;  // hash insert, narrowphase
   cudaMemsetAsync(w.hash, 0, (size_t(p.hashMask) + 1) * 4, s);
   k_hash_insert<<<GS_BLOCKS, 256, 0, s>>>(w, p);
   if (n > 0) {

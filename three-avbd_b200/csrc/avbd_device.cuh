@@ -25,7 +25,8 @@ constexpr int MAX_COLORS = 64;
 constexpr int MAX_CONTACTS = 8;
 constexpr float SHAPE_SPHERE_F = 1.0f;
 constexpr uint32_t T_NONE = 0, T_JOINT = 1, T_SPRING = 2;
-constexpr uint32_t FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_START_AT_REST = 8, FLAG_MASS_PENALTY = 16;
+constexpr uint32_t FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_REUSE_CONTACTS = 4, FLAG_START_AT_REST = 8, FLAG_MASS_PENALTY = 16;
+constexpr float REUSE_LIN_TOL = 0.002f, REUSE_ANG_TOL = 0.002f;  // gpu/layout.ts:174-175
 constexpr float REST_SPEED = 0.1f;
 constexpr float NEAREST_FRACTION = 0.05f;
 constexpr uint32_t OWNER_BIT = 0x80000000u;  // incidence entry: this body updates the constraint's dual
@@ -67,6 +68,7 @@ struct StepParams {
   uint32_t step;
   uint32_t fixedColors;  // colours come from the host (validation), no Jones-Plassmann
   uint32_t colorCap;
+  uint32_t rowsPerLane;  // the least rows a lane of a body's group takes (0, 1: as the colour's size asks)
   int cur;               // which manifold/contact buffers this step writes
 };
 
@@ -102,10 +104,18 @@ struct DWorld {
   uint32_t *colorA, *colorB, *colorHist, *colorStart, *colorBodies, *fixedColor;
   uint32_t *incCount, *incStart;
   uint2* incList;         // per incidence: constraint row (joint slot, or nj + point slot) | OWNER_BIT, partner word
-  uint32_t* done;         // per body: iterations finished in this step's dataflow sweep
+  uint32_t* done;         // per body: iterations finished in this step's dataflow sweep (pose and owned rows)
+  uint32_t* poseDone;     // per body: iterations whose pose is written (published before its owned rows)
   uint4* laneTable;       // per lane of the dataflow sweep: body, first row, row end, L | sub << 8
   uint32_t* bucket;       // BUCKET_WORDS: counts, starts (+ total), fill cursors, lane bases, lane totals per colour
-  float4 *dlin, *dang;    // per body: position and rotation change since x- (kept by the solve)
+  // Per body, the step's unknowns relative to x- (kept by the solve, precise at any distance from the
+  // origin, where an absolute f32 position rounds to its magnitude's ulp): dlin = x - x- and
+  // dang = (2 vec(r), r.w) with r the rotation since x- (q = r q-, so qsub(q, q-) = dang.xyz); and
+  // the inertial target y the same way: ylin = y - x-, yang = the rotation from q- to y's rotation.
+  float4 *dlin, *dang, *ylin, *yang;
+  // contact reuse (wgsl-collision.ts:20-44): per body its reference pose (zero rotation: none yet);
+  // the step it last moved past the tolerances is kept in ypos.w (the record's moved_step word)
+  float4 *refPos, *refRot;
   uint32_t* scanScratch;
   // bookkeeping
   uint32_t* counters;
@@ -129,7 +139,7 @@ constexpr uint32_t WORLD_FIXED_COLORS = 1u;
 // The view of world `wi` of a batch: every pointer moved to the world's slice
 __host__ __device__ inline DWorld worldView(const DWorld& b, const WorldDesc& d, uint32_t wi) {
   DWorld v = b;
-  float4** bodyArrays[] = {&v.pos, &v.rot, &v.ipos, &v.irot, &v.size, &v.moment, &v.ypos, &v.yrot, &v.vel, &v.avel, &v.dlin, &v.dang, &v.aabb};
+  float4** bodyArrays[] = {&v.pos, &v.rot, &v.ipos, &v.irot, &v.size, &v.moment, &v.ypos, &v.yrot, &v.vel, &v.avel, &v.dlin, &v.dang, &v.ylin, &v.yang, &v.refPos, &v.refRot, &v.aabb};
   for (float4** a : bodyArrays) *a += d.body;
   v.filters += d.body;
   if (v.aux) v.aux += d.body;
@@ -242,7 +252,7 @@ __host__ __device__ inline uint32_t pairHash(uint32_t a, uint32_t b) { return ha
 inline uint32_t grid_for(uint32_t n, uint32_t block) { return (n + block - 1) / block; }
 
 // Host launchers (avbd_collide.cu)
-uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, cudaStream_t s);
+uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSize, bool reuseManifolds, cudaStream_t s);
 void launch_step_stats(const DWorld& w, uint32_t launches, cudaStream_t s);
 // Batched worlds: one block per world over a queue of world indices (largest first)
 struct BatchLaunch {

@@ -382,6 +382,16 @@ int avbd_default_params(avbd_params* p) {
   return AVBD_OK;
 }
 
+int avbd_world_params(avbd_params* p) {
+  if (!p) return AVBD_ERR_INVALID;
+  avbd_default_params(p);
+  p->flags = AVBD_FLAG_MATCH_NEAREST | AVBD_FLAG_FACE_BIAS | AVBD_FLAG_REUSE_CONTACTS | AVBD_FLAG_START_AT_REST | AVBD_FLAG_MASS_PENALTY;
+  p->up[0] = 0.0f;
+  p->up[1] = 1.0f;
+  p->up[2] = 0.0f;
+  return AVBD_OK;
+}
+
 int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   if (!out) return AVBD_ERR_INVALID;
   *out = nullptr;
@@ -453,7 +463,12 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.bucket, BUCKET_WORDS));
   A(dalloc(w, &d.dlin, B));
   A(dalloc(w, &d.dang, B));
+  A(dalloc(w, &d.ylin, B));
+  A(dalloc(w, &d.yang, B));
+  A(dalloc(w, &d.refPos, B));
+  A(dalloc(w, &d.refRot, B));
   A(dalloc(w, &d.done, B));
+  A(dalloc(w, &d.poseDone, B));
   A(dalloc(w, &d.scanScratch, w->solveBlocks + 1));
   A(dalloc(w, &d.counters, COUNTER_WORDS));
   A(dalloc(w, &d.barrier, 2));
@@ -486,8 +501,9 @@ int avbd_world_destroy(avbd_world* w) {
   for (void* p : w->allocations) cudaFree(p);
   w->allocations.clear();
   if (w->hCounters) cudaFreeHost(w->hCounters);
-  for (auto& g : w->graph)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto& gk : w->graph)
+    for (auto& g : gk)
+      if (g) cudaGraphExecDestroy(g);
   if (w->countersReady) cudaEventDestroy(w->countersReady);
 
   if (w->stream) cudaStreamDestroy(w->stream);
@@ -561,6 +577,7 @@ static std::string hullProblem(const uint32_t* u, uint32_t vec4s) {
 
 int avbd_add_bodies(avbd_world* w, const avbd_body* bodies, uint32_t n, uint32_t* first) {
   if (!w || (!bodies && n)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (uint64_t(w->n) + n > w->bodyCap) return fail(w, AVBD_ERR_CAPACITY, "body capacity " + std::to_string(w->bodyCap) + " reached");
   int r = checkBodies(w, bodies, n);
   if (r) return r;
@@ -572,6 +589,7 @@ int avbd_add_bodies(avbd_world* w, const avbd_body* bodies, uint32_t n, uint32_t
 
 int avbd_write_bodies(avbd_world* w, uint32_t first, const avbd_body* bodies, uint32_t n, int keep_contacts) {
   if (!w || (!bodies && n)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (uint64_t(first) + n > w->bodyCap || first > w->n) return fail(w, AVBD_ERR_INVALID, "body range outside the world");
   int r = checkBodies(w, bodies, n);
   if (r) return r;
@@ -608,6 +626,7 @@ int avbd_write_bodies(avbd_world* w, uint32_t first, const avbd_body* bodies, ui
 // write per run of consecutive slots, each slot starting afresh (no contact history, no colour)
 int avbd_write_bodies_at(avbd_world* w, const uint32_t* indices, const avbd_body* bodies, uint32_t n) {
   if (!w || (n && (!indices || !bodies))) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   for (uint32_t k = 0; k < n; k++)
     if (indices[k] >= w->n) return fail(w, AVBD_ERR_INVALID, "rewriteBodies: slot " + std::to_string(indices[k]) + " is not a body of the world");
   int r = checkBodies(w, bodies, n);
@@ -629,6 +648,7 @@ static int checkJoints(avbd_world* w, const avbd_joint* j, const avbd_joint_info
 
 int avbd_write_joints(avbd_world* w, uint32_t first, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n) {
   if (!w || (n && (!joints || !info))) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (uint64_t(first) + n > w->nj) return fail(w, AVBD_ERR_INVALID, "joint range outside the world's slots");
   int r = checkJoints(w, joints, info, n);
   if (r) return r;
@@ -646,6 +666,7 @@ int avbd_write_joints(avbd_world* w, uint32_t first, const avbd_joint* joints, c
 
 int avbd_add_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* first) {
   if (!w || (n && (!joints || !info))) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   int r = checkJoints(w, joints, info, n);
   if (r) return r;
   cudaSetDevice(w->device);
@@ -677,6 +698,7 @@ int avbd_add_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint_in
 // at the end; each record and info written, each joint's pair kept out of the broadphase
 int avbd_append_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint_info* info, uint32_t n, uint32_t* slots) {
   if (!w || (n && (!joints || !info || !slots))) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   int r = checkJoints(w, joints, info, n);
   if (r) return r;
   if (!n) return AVBD_OK;
@@ -720,6 +742,7 @@ int avbd_append_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint
 // reused slot keeps only its new pair's); the slots go to the free list
 int avbd_release_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
   if (!w || (n && !slots)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   std::vector<uint32_t> order;
   for (uint32_t i = 0; i < n; i++)
     if (slots[i] < w->nj && w->info[slots[i]].type != AVBD_T_NONE) order.push_back(slots[i]);
@@ -751,6 +774,7 @@ int avbd_release_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
 
 int avbd_disable_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
   if (!w || (n && !slots)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   for (uint32_t i = 0; i < n; i++)
     if (slots[i] >= w->nj) return fail(w, AVBD_ERR_INVALID, "joint slot " + std::to_string(slots[i]) + " out of range");
   cudaSetDevice(w->device);
@@ -767,6 +791,7 @@ int avbd_disable_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
 
 int avbd_add_ignore_pairs(avbd_world* w, const uint32_t* ab, uint32_t n) {
   if (!w || (n && !ab)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   for (uint32_t i = 0; i < n; i++)
     if (ab[2 * i] >= w->n || ab[2 * i + 1] >= w->n || ab[2 * i] == ab[2 * i + 1]) return fail(w, AVBD_ERR_INVALID, "ignore pair out of range");
   for (uint32_t i = 0; i < n; i++) w->nocollide.push_back({std::max(ab[2 * i], ab[2 * i + 1]), std::min(ab[2 * i], ab[2 * i + 1]), 0xffffffffu});
@@ -778,6 +803,7 @@ int avbd_add_ignore_pairs(avbd_world* w, const uint32_t* ab, uint32_t n) {
 // consecutive slots
 int avbd_set_filters_at(avbd_world* w, const uint32_t* indices, const uint32_t* groups, const uint32_t* collides_with, uint32_t n) {
   if (!w || (n && (!indices || !groups || !collides_with))) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   for (uint32_t k = 0; k < n; k++)
     if (indices[k] >= w->n) return fail(w, AVBD_ERR_INVALID, "setFilters: slot " + std::to_string(indices[k]) + " is not a body of the world");
   cudaSetDevice(w->device);
@@ -795,6 +821,7 @@ int avbd_set_filters_at(avbd_world* w, const uint32_t* indices, const uint32_t* 
 
 int avbd_set_filters(avbd_world* w, uint32_t first, const uint32_t* gm, uint32_t n) {
   if (!w || (n && !gm)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (uint64_t(first) + n > w->n) return fail(w, AVBD_ERR_INVALID, "setFilters: slots outside the world's bodies");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
@@ -845,6 +872,7 @@ int avbd_read_body_aux(avbd_world* w, uint32_t first, float* aux4, uint32_t n) {
 
 int avbd_set_lifecycle(avbd_world* w, uint32_t index, uint32_t bits) {
   if (!w) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (index >= w->n || (bits & ~6u)) return fail(w, AVBD_ERR_INVALID, "Invalid body lifecycle flags/index");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
@@ -860,6 +888,7 @@ int avbd_set_lifecycle(avbd_world* w, uint32_t index, uint32_t bits) {
 
 int avbd_seed_contacts(avbd_world* w, const avbd_manifold* m, uint32_t nm, const avbd_contact* c, uint32_t nc) {
   if (!w || (nm && !m) || (nc && !c)) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   for (uint32_t i = 0; i < nm; i++) {
     if (m[i].count > MAX_CONTACTS || uint64_t(m[i].first) + m[i].count > nc || m[i].a >= w->n || m[i].b >= w->n)
       return fail(w, AVBD_ERR_INVALID, "manifold " + std::to_string(i) + ": bad bodies or contact range");
@@ -909,10 +938,14 @@ int avbd_set_fixed_colors(avbd_world* w, const uint32_t* colors, uint32_t n) {
   return AVBD_OK;
 }
 
-int avbd_step(avbd_world* w, int n) {
+int avbd_step(avbd_world* w, int n) { return avbd_step_with(w, n, nullptr); }
+
+int avbd_step_with(avbd_world* w, int n, const avbd_step_options* opts) {
   if (!w || n < 0) return AVBD_ERR_INVALID;
   cudaSetDevice(w->device);
   for (int s = 0; s < n; s++) {
+    // last step's manifolds are kept only while they are valid (gpu/solver.ts:2121)
+    const bool reuse = opts && opts->reuse_manifolds && w->manifoldsValid;
     int r = adaptCapacity(w, false);
     if (r) return r;
     if (w->staticsDirty) {
@@ -922,7 +955,7 @@ int avbd_step(avbd_world* w, int n) {
     w->stepCount++;
     StepParams p = makeParams(w);
     auto enqueue = [&]() -> cudaError_t {
-      uint32_t launches = launch_collision(w->d, p, w->tableSize, w->stream) + 1;
+      uint32_t launches = launch_collision(w->d, p, w->tableSize, reuse, w->stream) + 1;
       cudaError_t le = launch_topology_solve(w->d, p, w->solveBlocks, w->stream);
       if (w->statsCap) launch_step_stats(w->d, launches + 1, w->stream);
       w->launchesPerStep = launches + (w->statsCap ? 1 : 0);
@@ -932,15 +965,17 @@ int avbd_step(avbd_world* w, int n) {
     bool launched = false;
     if (w->useGraphs) {
       const int c = w->cur;
-      if (!w->graph[c] || w->graphGen[c] != w->configGen) {
-        if (w->graph[c]) cudaGraphExecDestroy(w->graph[c]);
-        w->graph[c] = nullptr;
+      cudaGraphExec_t& graph = w->graph[reuse ? 1 : 0][c];
+      uint64_t& graphGen = w->graphGen[reuse ? 1 : 0][c];
+      if (!graph || graphGen != w->configGen) {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
           cudaError_t le = enqueue();
           e = cudaStreamEndCapture(w->stream, &g);
-          if (e == cudaSuccess && le == cudaSuccess) e = cudaGraphInstantiate(&w->graph[c], g, 0);
+          if (e == cudaSuccess && le == cudaSuccess) e = cudaGraphInstantiate(&graph, g, 0);
           else if (e == cudaSuccess) e = le;
           if (g) cudaGraphDestroy(g);
         }
@@ -949,14 +984,14 @@ int avbd_step(avbd_world* w, int n) {
           cudaGetLastError();
           w->useGraphs = false;
           w->graphNote = std::string("graph capture failed: ") + cudaGetErrorString(e);
-          if (w->graph[c]) cudaGraphExecDestroy(w->graph[c]);
-          w->graph[c] = nullptr;
+          if (graph) cudaGraphExecDestroy(graph);
+          graph = nullptr;
         } else {
-          w->graphGen[c] = w->configGen;
+          graphGen = w->configGen;
         }
       }
-      if (w->graph[c]) {
-        CUDA_TRY(w, cudaGraphLaunch(w->graph[c], w->stream));
+      if (graph) {
+        CUDA_TRY(w, cudaGraphLaunch(graph, w->stream));
         launched = true;
       }
     }
@@ -969,7 +1004,40 @@ int avbd_step(avbd_world* w, int n) {
     CUDA_TRY(w, cudaEventRecord(w->countersReady, w->stream));
     w->countersInFlight = true;
     w->cur = 1 - w->cur;
+    w->manifoldsValid = true;
   }
+  return AVBD_OK;
+}
+
+int avbd_read_reuse_state(avbd_world* w, float* ref_poses, uint32_t body_cap, uint32_t* n_bodies, uint32_t* generations, uint32_t manifold_cap,
+                          uint32_t* n_manifolds) {
+  if (!w) return AVBD_ERR_INVALID;
+  cudaSetDevice(w->device);
+  CUDA_TRY(w, cudaStreamSynchronize(w->stream));
+  if (n_bodies) *n_bodies = w->n;
+  const uint32_t nb = std::min(body_cap, w->n);
+  if (nb && !ref_poses) return AVBD_ERR_INVALID;
+  if (nb) {
+    std::vector<float4> pos(nb), rot(nb);
+    CUDA_TRY(w, cudaMemcpy(pos.data(), w->d.refPos, nb * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, cudaMemcpy(rot.data(), w->d.refRot, nb * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nb; i++) {
+      std::memcpy(ref_poses + 8 * size_t(i), &pos[i], sizeof(float4));
+      std::memcpy(ref_poses + 8 * size_t(i) + 4, &rot[i], sizeof(float4));
+    }
+  }
+  uint32_t pairs = 0;
+  CUDA_TRY(w, cudaMemcpy(&pairs, w->d.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost));
+  pairs = std::min(pairs, w->pairCap);
+  std::vector<uint4> ids(pairs);
+  if (pairs) CUDA_TRY(w, cudaMemcpy(ids.data(), w->d.mIds[1 - w->cur], pairs * sizeof(uint4), cudaMemcpyDeviceToHost));
+  uint32_t mi = 0;
+  for (uint32_t p = 0; p < pairs; p++) {
+    if (!(ids[p].w & 15u)) continue;
+    if (generations && mi < manifold_cap) generations[mi] = ids[p].w >> 4;
+    mi++;
+  }
+  if (n_manifolds) *n_manifolds = mi;
   return AVBD_OK;
 }
 
@@ -1290,6 +1358,7 @@ int avbd_world_stream(avbd_world* w, void** stream) {
 
 int avbd_write_bodies_async(avbd_world* w, uint32_t first, const avbd_body* bodies, uint32_t n) {
   if (!w || (!bodies && n) || uint64_t(first) + n > w->n) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   cudaSetDevice(w->device);
   if (n) copyBodiesIn(w, first, bodies, n, cudaMemcpyHostToDevice);
   CUDA_TRY(w, cudaGetLastError());
@@ -1301,6 +1370,7 @@ int avbd_write_bodies_async(avbd_world* w, uint32_t first, const avbd_body* bodi
 // the body's size; no angular stiffness, so the joint holds the point and leaves the turn free.
 int avbd_add_world_joint(avbd_world* w, uint32_t body, const float anchor_world[3], const float anchor_body[3], uint32_t* slot) {
   if (!w || !anchor_world || !anchor_body) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (body >= w->n) return fail(w, AVBD_ERR_INVALID, "appendWorldJoint: body " + std::to_string(body) + " is not a body of the world");
   for (int k = 0; k < 3; k++)
     if (!std::isfinite(anchor_world[k]) || !std::isfinite(anchor_body[k]))
@@ -1333,6 +1403,7 @@ int avbd_add_world_joint(avbd_world* w, uint32_t body, const float anchor_world[
 // setWorldAnchor (gpu/solver.ts:1937-1939): the slot's r_a, in place before the next step
 int avbd_set_world_anchor(avbd_world* w, uint32_t slot, const float p[3]) {
   if (!w || !p) return AVBD_ERR_INVALID;
+  w->manifoldsValid = false;
   if (slot >= w->nj) return fail(w, AVBD_ERR_INVALID, "setWorldAnchor: joint slot " + std::to_string(slot) + " out of range");
   for (int k = 0; k < 3; k++)
     if (!std::isfinite(p[k])) return fail(w, AVBD_ERR_INVALID, "setWorldAnchor: the anchor needs three finite f32 numbers");

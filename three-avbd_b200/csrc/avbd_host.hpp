@@ -63,14 +63,22 @@ struct avbd_world {
   // per-step statistics: a device ring written by the step itself (graph-compatible)
   uint32_t statsCap = 0, statsCount = 0;
   uint32_t launchesPerStep = 0;
-  // The step as two CUDA graphs (one per contact-buffer parity), rebuilt when anything baked into
-  // their launches changes (configGen)
+  // The step as CUDA graphs, one per contact-buffer parity and per kind (detecting, or keeping last
+  // step's manifolds), rebuilt when anything baked into their launches changes (configGen)
   bool useGraphs = true;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  uint64_t graphGen[2] = {0, 0};
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  uint64_t graphGen[2][2] = {{0, 0}, {0, 0}};
+  // last step's manifolds may be kept by the next step (reuseManifolds): a step ran and nothing
+  // that changes bodies, joints, filters or contacts happened since (gpu/solver.ts manifoldsValid)
+  bool manifoldsValid = false;
   uint64_t configGen = 1;
   std::string graphNote;
   std::vector<void*> allocations;
+  // scratch of the queries around the step (avbd_query.cu), grown on demand: pushes, rays, the
+  // rays' nearest keys and their hits
+  float4 *pushBuf = nullptr, *rayBuf = nullptr, *rayHits = nullptr;
+  unsigned long long* rayBest = nullptr;
+  size_t pushCap = 0, rayCap = 0, rayBestCap = 0, rayHitsCap = 0;
   // hull buffer: host copy of every record (wgsl-hull.ts layout), header offsets, device capacity
   std::vector<uint32_t> hullWords;
   std::set<uint32_t> hullStarts;

@@ -232,19 +232,32 @@ __device__ inline uint32_t smallestFree(const DWorld& w, const StepParams& p, ui
 // --- body poses -----------------------------------------------------------------------------------------
 // What a contact row needs of a body: its rotation (and step-start rotation, for rolling spheres) and
 // its displacement since x- (dlin, dang are kept by the solve, so a partner costs three loads and no
-// quaternion division).
+// quaternion division). The solve's unknowns are the displacement from x- and the rotation r since
+// x- (q = r q-): both stay precise in f32 wherever the body is, where an absolute position rounds to
+// its magnitude's ulp (7.6e-6 m at 100 m) and a difference of two such positions carries that error
+// into every constraint value and multiplier. x0 is the step-start position; rw is r's w (its vector
+// part is dAng / 2).
 struct Pose {
-  float3 x, dLin, dAng;
+  float3 x0, dLin, dAng;
   float4 q, q0;
+  float rw;
 };
 __device__ inline Pose partnerPose(const DWorld& w, uint32_t i) {
   Pose P;
   P.q = w.rot[i];
   P.dLin = f3(w.dlin[i]);
   P.dAng = f3(w.dang[i]);
-  P.x = make_float3(0.0f, 0.0f, 0.0f);
+  P.x0 = make_float3(0.0f, 0.0f, 0.0f);
   P.q0 = P.q;
+  P.rw = 1.0f;
   return P;
+}
+// r of a body from its dang word, and the dang word of r
+__device__ __forceinline__ float4 relRot(float3 dAng, float rw) { return make_float4(dAng.x * 0.5f, dAng.y * 0.5f, dAng.z * 0.5f, rw); }
+__device__ __forceinline__ float4 dangWord(float4 r) { return make_float4(r.x * 2.0f, r.y * 2.0f, r.z * 2.0f, r.w); }
+__device__ __forceinline__ float4 qnormalize4(float4 q) {
+  float l = sqrtf((q.x * q.x + q.y * q.y + q.z * q.z) + q.w * q.w);
+  return make_float4(q.x / l, q.y / l, q.z / l, q.w / l);
 }
 
 // The Newton system of one body (wgsl-solve.ts:56-75): lin and ang symmetric (upper triangles),
@@ -295,16 +308,25 @@ __device__ inline void evalContact(float4 ra, float4 rb, float4 pen, float4 lam,
 }
 
 // --- joints and springs (wgsl-solve.ts:79-165, 562-635) --------------------------------------------------
-struct Bodies2 {  // poses of a joint's bodies; `own` is the body being solved (its pose in registers)
+// Poses of a joint's bodies; `own` is the body being solved (its pose in registers). A position is
+// base + disp: the step-start position and the displacement since (at the warm start, `atStart`:
+// the positions the step starts from, no displacement), so that two bodies' positions are
+// differenced as (base a - base b) + (disp a - disp b), which is exact to the displacements' precision.
+struct Bodies2 {
   const DWorld* w;
   uint32_t own;
   const Pose* ownPose;
-  __device__ inline float3 pos(int i) const { return (uint32_t)i == own ? ownPose->x : f3(w->pos[i]); }
+  bool atStart;
+  __device__ inline float3 base(int i) const { return atStart ? f3(w->pos[i]) : (uint32_t)i == own ? ownPose->x0 : f3(w->ipos[i]); }
+  __device__ inline float3 disp(int i) const {
+    return atStart ? make_float3(0.0f, 0.0f, 0.0f) : (uint32_t)i == own ? ownPose->dLin : f3(w->dlin[i]);
+  }
   __device__ inline float4 rot(int i) const { return (uint32_t)i == own ? ownPose->q : w->rot[i]; }
 };
 __device__ inline float3 jointLinC(const float4* k, int a, int b, const Bodies2& B) {
-  float3 anchorA = a < 0 ? f3(k[J_RA]) : qrotate(B.rot(a), f3(k[J_RA])) + B.pos(a);
-  return anchorA - (qrotate(B.rot(b), f3(k[J_RB])) + B.pos(b));
+  float3 rb = qrotate(B.rot(b), f3(k[J_RB]));
+  if (a < 0) return ((f3(k[J_RA]) - B.base(b)) - B.disp(b)) - rb;  // a world point against body b
+  return ((B.base(a) - B.base(b)) + (B.disp(a) - B.disp(b))) + (qrotate(B.rot(a), f3(k[J_RA])) - rb);
 }
 __device__ inline float3 jointAngC(const float4* k, int a, int b, const Bodies2& B) {
   float4 qb = B.rot(b);
@@ -331,7 +353,7 @@ __device__ void addJoint(Acc& acc, const DWorld& w, uint32_t j, float alpha, uin
   if ((uint32_t)info.x == T_SPRING) {
     float3 rAW = qrotate(B.rot(a), f3(k[J_RA]));
     float3 rBW = qrotate(B.rot(b), f3(k[J_RB]));
-    float3 d = (rAW + B.pos(a)) - (rBW + B.pos(b));
+    float3 d = ((B.base(a) - B.base(b)) + (B.disp(a) - B.disp(b))) + (rAW - rBW);
     float len = len3(d);
     if (len <= 1.0e-6f) return;
     float3 n = d / len;
@@ -441,8 +463,9 @@ __device__ void dualJoint(const DWorld& w, const StepParams& p, uint32_t j, cons
   }
 }
 
-// --- the 6x6 LDLT with pivot floor and the pose update (wgsl-solve.ts:504-558) ------------------------------
-__device__ inline void finishBody(const Acc& acc, float3& x, float4& q) {
+// --- the 6x6 LDLT with pivot floor (wgsl-solve.ts:504-558): the Newton step (dx, dtheta), which the
+// caller subtracts from the body's displacement and rotation -------------------------------------------------
+__device__ inline void finishBody(const Acc& acc, float3& dx, float3& dth) {
   const float* v = acc.v;
   float A11 = v[0], A21 = v[1], A22 = v[3], A31 = v[2], A32 = v[4], A33 = v[5];
   float A41 = v[12], A42 = v[13], A43 = v[14], A44 = v[6];
@@ -478,8 +501,8 @@ __device__ inline void finishBody(const Acc& acc, float3& x, float4& q) {
   float v3 = y3 * i3 - L43 * w1 - L53 * w2 - L63 * w3;
   float v2 = y2 * i2 - L32 * v3 - L42 * w1 - L52 * w2 - L62 * w3;
   float v1 = y1 * i1 - L21 * v2 - L31 * v3 - L41 * w1 - L51 * w2 - L61 * w3;
-  x = make_float3(x.x - v1, x.y - v2, x.z - v3);
-  q = qadd(q, make_float3(-w1, -w2, -w3));
+  dx = make_float3(v1, v2, v3);
+  dth = make_float3(w1, w2, w3);
 }
 
 // One contact row set (a point of a pair) from body i's side
@@ -508,7 +531,7 @@ __device__ inline void loadPoint(const DWorld& w, const StepParams& p, uint32_t 
 __device__ inline void accumulateIncidence(Acc& acc, const DWorld& w, const StepParams& p, uint2 inc, uint32_t i, const Pose& own) {
   uint32_t id = inc.x & ~OWNER_BIT;
   if (id < p.nj) {
-    Bodies2 B{&w, i, &own};
+    Bodies2 B{&w, i, &own, false};
     addJoint(acc, w, id, p.alpha, i, B);
     return;
   }
@@ -530,7 +553,7 @@ __device__ inline void accumulateIncidence(Acc& acc, const DWorld& w, const Step
 __device__ inline void dualIncidence(const DWorld& w, const StepParams& p, uint2 inc, uint32_t i, const Pose& own) {
   uint32_t id = inc.x & ~OWNER_BIT;
   if (id < p.nj) {
-    Bodies2 B{&w, i, &own};
+    Bodies2 B{&w, i, &own, false};
     dualJoint(w, p, id, B);
     return;
   }
@@ -570,15 +593,15 @@ constexpr int B_COUNT = 0, B_START = BUCKETS, B_FILL = 2 * BUCKETS + 1, B_LANE =
               B_ROWS = B_LANE_TOTAL + MAX_COLORS;
 static_assert(B_ROWS + MAX_COLORS <= BUCKET_WORDS, "bucket words");
 
-// Waits until body b has finished `need` iterations (its done count, published with release
-// semantics after its pose and owned rows are written). Bounded: past the clock budget, or once any
-// wait of the launch gave up, it returns false.
-__device__ inline bool waitDone(const DWorld& w, uint32_t b, uint32_t need) {
-  if (ld_acquire_gpu(w.done + b) >= need) return true;
+// Waits until a body's count (`flag`: its done or poseDone word, published with release semantics)
+// reaches `need`. Bounded: past the clock budget, or once any wait of the launch gave up, it returns
+// false.
+__device__ inline bool waitDone(const DWorld& w, const uint32_t* flag, uint32_t need) {
+  if (ld_acquire_gpu(flag) >= need) return true;
   const long long t0 = clock64();
   for (uint32_t n = 1;; n++) {
     if (n > 64u) __nanosleep(32);
-    if (ld_acquire_gpu(w.done + b) >= need) return true;
+    if (ld_acquire_gpu(flag) >= need) return true;
     if ((n & 15u) == 0u) {
       if (ldv(&w.counters[C_ERROR]) & ERR_DEPENDENCY_TIMEOUT) return false;
       if (clock64() - t0 > BARRIER_CYCLES) {
@@ -653,16 +676,15 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
   Pose own;
   Acc acc;
   accZero(acc);
-  float3 x0 = make_float3(0.0f, 0.0f, 0.0f);
   if (active) {
-    float4 pos = w.pos[body];
-    own.x = f3(pos);
+    own.x0 = f3(w.ipos[body]);
     own.q = w.rot[body];
     own.q0 = w.irot[body];
     own.dLin = f3(w.dlin[body]);
-    own.dAng = f3(w.dang[body]);
+    const float4 da = w.dang[body];
+    own.dAng = f3(da);
+    own.rw = da.w;
     if (sub == 0) {
-      x0 = f3(w.ipos[body]);
       float m = w.size[body].w / dt2;
       float3 I = f3(w.moment[body]) / dt2;
       acc.v[0] = m;
@@ -671,8 +693,9 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
       acc.v[6] = I.x;
       acc.v[9] = I.y;
       acc.v[11] = I.z;
-      float3 rl = (own.x - f3(w.ypos[body])) * m;
-      float3 ra = I * qsub(own.q, w.yrot[body]);
+      // M (x - y) and I qsub(q, y's rotation), both relative to x-: (dlin - ylin) and qsub(r, yang)
+      float3 rl = (own.dLin - f3(w.ylin[body])) * m;
+      float3 ra = I * qsub(relRot(own.dAng, own.rw), w.yang[body]);
       acc.v[21] = rl.x;
       acc.v[22] = rl.y;
       acc.v[23] = rl.z;
@@ -686,9 +709,15 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
     if (active)
       for (uint32_t e = J.e; e < e1 && ok; e += L) {
         const uint2 inc = e == J.e ? inc0 : w.incList[e];
-        // a partner of the same colour (only where the colour cap forced a clash) is not waited for
-        // within the iteration: the colour-by-colour sweep runs such pairs side by side too
-        if (inc.y & PARTNER_DYNAMIC) ok = waitDone(w, inc.y & PARTNER_MASK, it + ((inc.y & PARTNER_EARLIER) ? 1u : 0u));
+        // A partner of an earlier colour must have moved in this iteration: its pose is all this
+        // body reads of it (their shared rows are this body's to update). One of a later colour must
+        // have finished the previous iteration, pose and the rows it updates, these among them. A
+        // partner of the same colour (only where the colour cap forced a clash) is not waited for
+        // within the iteration: the colour-by-colour sweep runs such pairs side by side too.
+        if (inc.y & PARTNER_DYNAMIC) {
+          const uint32_t partner = inc.y & PARTNER_MASK;
+          ok = (inc.y & PARTNER_EARLIER) ? waitDone(w, w.poseDone + partner, it + 1u) : waitDone(w, w.done + partner, it);
+        }
       }
     if (__any_sync(0xffffffffu, !ok)) return false;
   }
@@ -704,18 +733,24 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
       if (take) acc.v[k] += o;
     }
   }
-  float3 x = own.x, dl = own.dLin, da = own.dAng;
+  float3 dl = own.dLin, da = own.dAng;
   float4 q = own.q;
   if (active && sub == 0) {
-    finishBody(acc, x, q);
-    dl = x - x0;
-    da = qsub(q, own.q0);
+    float3 dx, dth;
+    finishBody(acc, dx, dth);
+    dl = dl - dx;
+    const float4 r = qadd(relRot(own.dAng, own.rw), make_float3(-dth.x, -dth.y, -dth.z));
+    q = qnormalize4(qmul(r, own.q0));
+    const float4 dw = dangWord(r);
+    da = f3(dw);
+    const float3 x = own.x0 + dl;
     w.pos[body] = make_float4(x.x, x.y, x.z, w.pos[body].w);
     w.rot[body] = q;
     w.dlin[body] = make_float4(dl.x, dl.y, dl.z, 0.0f);
-    w.dang[body] = make_float4(da.x, da.y, da.z, 0.0f);
+    w.dang[body] = dw;
+    // the pose is final for this iteration: partners of later colours may read it now
+    if constexpr (kWait) st_release_gpu(w.poseDone + body, it + 1u);
   }
-  own.x = make_float3(__shfl_sync(0xffffffffu, x.x, leader), __shfl_sync(0xffffffffu, x.y, leader), __shfl_sync(0xffffffffu, x.z, leader));
   own.q = make_float4(__shfl_sync(0xffffffffu, q.x, leader), __shfl_sync(0xffffffffu, q.y, leader), __shfl_sync(0xffffffffu, q.z, leader),
                       __shfl_sync(0xffffffffu, q.w, leader));
   own.dLin = make_float3(__shfl_sync(0xffffffffu, dl.x, leader), __shfl_sync(0xffffffffu, dl.y, leader), __shfl_sync(0xffffffffu, dl.z, leader));
@@ -892,7 +927,7 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   GSYNC
   {
     for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
-    if (threadIdx.x < (uint32_t)MAX_COLORS) s_perLane[threadIdx.x] = max(1u, (w.bucket[B_ROWS + threadIdx.x] + T - 1u) / T);
+    if (threadIdx.x < (uint32_t)MAX_COLORS) s_perLane[threadIdx.x] = max(max(1u, p.rowsPerLane), (w.bucket[B_ROWS + threadIdx.x] + T - 1u) / T);
     __syncthreads();
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
@@ -1021,7 +1056,7 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     float4 k[JOINT_VEC4];
     loadJoint(w, j, k);
     Pose dummy;
-    Bodies2 B{&w, 0xffffffffu, &dummy};
+    Bodies2 B{&w, 0xffffffffu, &dummy, true};
     float3 cl = jointLinC(k, a, b, B), ca = jointAngC(k, a, b, B);
     float4* o = w.joint + j * JOINT_VEC4;
     o[J_C0_LIN] = make_float4(cl.x, cl.y, cl.z, 0.0f);
@@ -1046,7 +1081,10 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   const float dt = p.dt, gWorld = p.gravity;
   const float3 up = make_float3(p.upx, p.upy, p.upz);
   for (uint32_t i = tid; i < n; i += T) {
-    if constexpr (Team::kDataflow) w.done[i] = 0u;
+    if constexpr (Team::kDataflow) {
+      w.done[i] = 0u;
+      w.poseDone[i] = 0u;
+    }
     if (!enabledBody(w, i)) continue;
     float4 pos = w.pos[i], rot = w.rot[i], vel = w.vel[i];
     float3 av = f3(w.avel[i]);
@@ -1062,31 +1100,41 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
       w.vel[i] = vel;
       w.avel[i] = make_float4(av.x, av.y, av.z, w.avel[i].w);
     }
-    float3 y = f3(pos) + f3(vel) * dt;
-    if (dynamic) y = y + up * (g * (dt * dt));
+    // y - x- and y's rotation relative to q- (the solve's inertial terms), and y itself for readers
+    float3 yl = f3(vel) * dt;
+    if (dynamic) yl = yl + up * (g * (dt * dt));
+    const float4 ry = qadd(make_float4(0.0f, 0.0f, 0.0f, 1.0f), av * dt);
+    const float3 y = f3(pos) + yl;
     w.ypos[i] = make_float4(y.x, y.y, y.z, w.ypos[i].w);
     w.yrot[i] = qadd(rot, av * dt);
+    w.ylin[i] = make_float4(yl.x, yl.y, yl.z, 0.0f);
+    w.yang[i] = ry;
     float wgt = 0.0f;
     if (fabsf(g) > 0.0f) wgt = fminf(fmaxf((dot3(f3(vel), up) - vel.w) / dt * (g < 0.0f ? -1.0f : 1.0f) / fabsf(g), 0.0f), 1.0f);
     bool slow = len3(f3(vel)) + len3(av) * w.moment[i].w < REST_SPEED;
     bool atRest = (p.flags & FLAG_START_AT_REST) != 0u && slow;
     w.ipos[i] = make_float4(pos.x, pos.y, pos.z, 0.0f);
     w.irot[i] = rot;
-    float3 x = f3(pos);
-    float4 q = rot;
+    // the warm-started guess as a displacement dl and a rotation r since x- (q = r q-)
+    float3 dl = make_float3(0.0f, 0.0f, 0.0f);
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    bool moved = false;
     if (dynamic && !atRest) {
-      x = f3(pos) + f3(vel) * dt + up * (g * (wgt * dt * dt));
-      q = qadd(rot, av * dt);
+      dl = f3(vel) * dt + up * (g * (wgt * dt * dt));
+      r = ry;
+      moved = true;
     }
     if (!dynamic && (vel.x != 0.0f || vel.y != 0.0f || vel.z != 0.0f || av.x != 0.0f || av.y != 0.0f || av.z != 0.0f)) {
-      x = f3(pos) + f3(vel) * dt;
-      q = qadd(rot, av * dt);
+      dl = f3(vel) * dt;
+      r = ry;
+      moved = true;
     }
+    const float3 x = f3(pos) + dl;
+    const float4 q = moved ? qnormalize4(qmul(r, rot)) : rot;
     w.pos[i] = make_float4(x.x, x.y, x.z, pos.w);
     w.rot[i] = q;
-    float3 dl = x - f3(pos), da = qsub(q, rot);
     w.dlin[i] = make_float4(dl.x, dl.y, dl.z, 0.0f);
-    w.dang[i] = make_float4(da.x, da.y, da.z, 0.0f);
+    w.dang[i] = dangWord(r);
   }
   GSYNC
 
@@ -1161,9 +1209,10 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     float4 vel = w.vel[i];
     float prevUp = dot3(f3(vel), up);
     if (w.size[i].w > 0.0f) {
-      float3 v = (f3(w.pos[i]) - f3(w.ipos[i])) / dt;
+      // (x - x-) / dt and qsub(q, q-) / dt: the step's displacement and 2 vec(r)
+      float3 v = f3(w.dlin[i]) / dt;
       w.vel[i] = make_float4(v.x, v.y, v.z, prevUp);
-      float3 av = qsub(w.rot[i], w.irot[i]) / dt;
+      float3 av = f3(w.dang[i]) / dt;
       w.avel[i] = make_float4(av.x, av.y, av.z, w.avel[i].w);
     } else {
       w.vel[i] = make_float4(vel.x, vel.y, vel.z, prevUp);
