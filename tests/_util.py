@@ -246,3 +246,33 @@ def pose_rel_diff(cuda_bodies: np.ndarray, oracle_bodies: np.ndarray) -> float:
     dp = np.abs(cuda_bodies['pos'] - x) / np.maximum(np.abs(x), 1.0)
     dq = np.abs(cuda_bodies['rot'] - oracle_bodies[:, 3:7])
     return max(float(dp.max()), float(dq.max()))
+
+
+# Multiplier parity: a row agrees when |dlambda| <= LAMBDA_REL |lambda| + LAMBDA_FLOOR_M x penalty.
+# lambda = penalty x C + lambda_prev, so the floor is the constraint value C agreeing within a
+# micron: near-zero rows (friction at rest, a contact at the clamp) carry no relative scale of
+# their own, and a penalty of 1e3 to 1e4 turns a C differing in its last f32 bits into a few mN.
+LAMBDA_REL = 1e-5
+LAMBDA_FLOOR_M = 1e-6
+
+
+def lambda_parity(gm: dict, om: dict, floor_m: float = LAMBDA_FLOOR_M, rows_of=(0, 1, 2)) -> dict:
+    """Every common contact's multiplier rows (`rows_of`: 0 normal, 1 and 2 friction), GPU against
+    oracle: the largest |dlambda| as a multiple of its bound (<= 1 passes), the largest relative
+    difference of rows above 1e-3 N, and the share of those within LAMBDA_REL."""
+    worst, worst_rel, rows, within = 0.0, 0.0, 0, 0
+    sel = list(rows_of)
+    for k, (_, _, lam, pen) in gm.items():
+        if k not in om:
+            continue
+        olam, open_ = np.asarray(om[k][2], float)[sel], np.asarray(om[k][3], float)[sel]
+        d = np.abs(np.asarray(lam, float)[sel] - olam)
+        bound = LAMBDA_REL * np.abs(olam) + floor_m * np.maximum(open_, 1.0)
+        worst = max(worst, float((d / bound).max()))
+        big = np.abs(olam) > 1e-3
+        if big.any():
+            r = d[big] / np.abs(olam[big])
+            worst_rel = max(worst_rel, float(r.max()))
+            rows += int(big.sum())
+            within += int((r <= LAMBDA_REL).sum())
+    return {'ratio': worst, 'worst_rel': worst_rel, 'rows': rows, 'within_rel': within / max(rows, 1)}

@@ -21,9 +21,9 @@ def test_pushes_match_oracle(cuda_lib):
     w.set_lifecycle(7, 2)  # disabled: left alone
     before = w.read_bodies()
     rng = np.random.default_rng(1)
-    slots = rng.choice(np.arange(len(before)), size=60, replace=False)
-    slots[0] = 0  # the static ground: left alone
-    slots[1] = 7
+    others = np.setdiff1d(np.arange(len(before)), [0, 7])
+    # the static ground and the disabled body are left alone; 58 others are pushed
+    slots = np.concatenate([[0, 7], rng.choice(others, size=58, replace=False)])
     p = np.zeros(len(slots), dtype=_abi.PUSH_DTYPE)
     p['body'] = slots
     p['lin'] = rng.normal(0, 5, (len(slots), 3))

@@ -83,3 +83,32 @@ def test_reuse_manifolds_substep_matches_oracle(cuda_lib):
     w.step(reuse_manifolds=True)
     assert np.any(w.read_reuse_state()['generated'] == w.read_counters()['steps'])
     w.destroy()
+
+
+def test_reuse_in_batched_worlds_matches_single_worlds(cuda_lib):
+    """Contact reuse in a batch (per-world reference poses and pair hash): every world bit-identical
+    over 40 steps to the same scene stepped alone with a one-block solve and the same rules."""
+    from avbd_b200 import BatchSolver3D
+    from avbd_b200.scenes import batched_worlds
+    scenes = batched_worlds(12, seed=21)
+    for s in scenes:
+        s.params = scenes[0].params
+    n = sum(len(s.bodies) for s in scenes)
+    b = BatchSolver3D(len(scenes), n, 1, params=scenes[0].params)
+    b.set_params(params_struct(scenes[0].params, RULES))
+    for s in scenes:
+        b.add_scene(s)
+    singles = [_world(s, RULES) for s in scenes]
+    for w in singles:
+        w.set_solve_blocks(1)
+    b.step(40)
+    b.synchronize()
+    kept = 0
+    for i, w in enumerate(singles):
+        w.step(40)
+        assert np.array_equal(b.read_bodies(i).view(np.uint32), w.read_bodies().view(np.uint32)), scenes[i].name
+        r = w.read_reuse_state()
+        kept += int((r['generated'] < r['step']).sum())
+        w.destroy()
+    assert kept > 0
+    b.destroy()

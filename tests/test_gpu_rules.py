@@ -9,7 +9,7 @@ import pytest
 from avbd_b200 import _abi
 from avbd_b200.scenes import cube_pyramid, drop_pile
 from oracle import Oracle
-from _util import cuda_from_oracle, pose_diff
+from _util import contact_map, cuda_from_oracle, lambda_parity, oracle_contact_map, pose_diff
 
 pytestmark = pytest.mark.gpu
 
@@ -20,12 +20,13 @@ ALL_RULES = _abi.FLAG_MATCH_NEAREST | _abi.FLAG_FACE_BIAS | _abi.FLAG_START_AT_R
 def test_gpu_only_rules_match_oracle(cuda_lib, name):
     scene = cube_pyramid(20) if name == 'pyramid' else drop_pile(400, seed=5, spacing=1.6, layers=4)
     o = Oracle(scene, flags=ALL_RULES)
-    worst = 0.0
+    worst = worst_lam = 0.0
     frame = 0
     for at in (30, 90):
         for _ in range(at - frame):
             o.step_gpu()
         frame = at
+        o.round_f32()
         w = cuda_from_oracle(o, scene.params, flags=ALL_RULES)
         o.step_gpu()
         frame += 1
@@ -35,6 +36,9 @@ def test_gpu_only_rules_match_oracle(cuda_lib, name):
         assert c['error'] == 0 and c['overflow'] == 0
         d = pose_diff(w.read_bodies(), o.bodies())
         worst = max(worst, d)
+        lp = lambda_parity(contact_map(*w.read_contacts()), oracle_contact_map(o))
+        worst_lam = max(worst_lam, lp['ratio'])
         w.destroy()
-    print(f'{name} with every GPU-only rule: worst pose diff {worst:.3e}')
+    print(f'{name} with every GPU-only rule: worst pose diff {worst:.3e}, lambda worst |d| / bound {worst_lam:.2f}')
     assert worst < 1e-5
+    assert worst_lam <= 1.0

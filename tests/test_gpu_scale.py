@@ -5,10 +5,8 @@ GPU-mode oracle, so both start from the same f32 values, and each takes one step
 
 Bit for bit: the candidate pair set, the Jones-Plassmann colouring, and every contact's feature key
 and body-frame anchors. Within the contract's tolerance: poses 1e-5 relative (positions against
-max(|x|, 1 m), unit quaternions absolute) and every multiplier row within 1e-5 relative plus the
-f32 resolution of its constraint value (LAMBDA_FLOOR_M metres times its penalty): a row's
-multiplier is penalty x C + lambda, and C of a contact resting under millimetre displacements is
-resolved to about 2^-30 m in f32, which a penalty of 1e4 turns into 1e-5 N."""
+max(|x|, 1 m), unit quaternions absolute) and multiplier rows within 1e-5 relative plus the stated
+floor (_util.lambda_parity)."""
 
 import numpy as np
 import pytest
@@ -17,29 +15,11 @@ import avbd_b200
 from avbd_b200 import BatchSolver3D, CudaSolver3D
 from avbd_b200.scenes import batched_worlds, drop_pile, hulls_and_chains
 from oracle import Oracle
-from _util import contact_map, cuda_from_oracle, oracle_contact_map, oracle_from_cuda, pose_diff, pose_rel_diff
+from _util import contact_map, cuda_from_oracle, lambda_parity, oracle_contact_map, oracle_from_cuda, pose_diff, pose_rel_diff
 
 pytestmark = pytest.mark.gpu
 
 POSE_TOL = 1e-5
-LAMBDA_REL = 1e-5
-LAMBDA_FLOOR_M = 1e-9
-
-
-def lambda_excess(gm: dict, om: dict) -> tuple[float, float, int]:
-    """Largest |dlambda| beyond LAMBDA_REL |lambda| + LAMBDA_FLOOR_M x penalty (as a multiple of that
-    bound), the largest relative difference of rows above 1e-3 N, and the rows compared."""
-    worst_ratio, worst_rel, rows = 0.0, 0.0, 0
-    for k, (_, _, lam, pen) in gm.items():
-        olam, open_ = om[k][2], om[k][3]
-        d = np.abs(lam - olam)
-        bound = LAMBDA_REL * np.abs(olam) + LAMBDA_FLOOR_M * np.maximum(open_, 1.0)
-        worst_ratio = max(worst_ratio, float((d / bound).max()))
-        big = np.abs(olam) > 1e-3
-        if big.any():
-            worst_rel = max(worst_rel, float((d[big] / np.abs(olam[big])).max()))
-        rows += 3
-    return worst_ratio, worst_rel, rows
 
 
 def _step_both(w, o):
@@ -66,11 +46,11 @@ def test_pile_100k_seeded_step(cuda_lib):
     o = oracle_from_cuda(w, scene)
     gm, om = _step_both(w, o)
     d = pose_rel_diff(w.read_bodies(), o.bodies())
-    ratio, rel, rows = lambda_excess(gm, om)
-    print(f'100k pile step 201: {len(gm)} contacts, pose {d:.2e}, lambda: worst |d| / bound {ratio:.2f}, worst rel (|lambda| > 1e-3) {rel:.2e} over {rows} rows')
+    normal, friction = lambda_parity(gm, om, rows_of=(0,)), lambda_parity(gm, om, rows_of=(1, 2))
+    print(f'100k pile step 201: {len(gm)} contacts, pose {d:.2e}; normal lambda {normal}; friction lambda {friction}')
     assert len(gm) > 300_000
     assert d < POSE_TOL
-    assert ratio <= 1.0
+    assert normal['ratio'] <= 1.0
     w.destroy()
 
 
@@ -82,11 +62,11 @@ def test_hulls_striking_chains_seeded_step(cuda_lib):
     o = oracle_from_cuda(w, scene)
     gm, om = _step_both(w, o)
     d = pose_rel_diff(w.read_bodies(), o.bodies())
-    ratio, rel, rows = lambda_excess(gm, om)
-    print(f'hulls and chains step 61: {len(gm)} contacts, pose {d:.2e}, lambda: worst |d| / bound {ratio:.2f}, worst rel {rel:.2e}')
+    lp = lambda_parity(gm, om)
+    print(f'hulls and chains step 61: {len(gm)} contacts, pose {d:.2e}, lambda {lp}')
     assert len(gm) > 20
     assert d < POSE_TOL
-    assert ratio <= 1.0
+    assert lp['ratio'] <= 1.0
     w.destroy()
 
 

@@ -104,6 +104,7 @@ class Params:
     face_bias: bool = False
     start_at_rest: bool = False
     mass_penalty: bool = False
+    reuse_contacts: bool = False
 
 
 class Scene:

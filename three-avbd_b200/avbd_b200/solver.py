@@ -119,7 +119,8 @@ def to_params(sp) -> Params:
     if isinstance(sp, Params):
         return sp
     flags = (_abi.FLAG_MATCH_NEAREST if sp.match_nearest else 0) | (_abi.FLAG_FACE_BIAS if sp.face_bias else 0) | \
-            (_abi.FLAG_START_AT_REST if sp.start_at_rest else 0) | (_abi.FLAG_MASS_PENALTY if sp.mass_penalty else 0)
+            (_abi.FLAG_START_AT_REST if sp.start_at_rest else 0) | (_abi.FLAG_MASS_PENALTY if sp.mass_penalty else 0) | \
+            (_abi.FLAG_REUSE_CONTACTS if getattr(sp, 'reuse_contacts', False) else 0)
     p = Params(dt=sp.dt, gravity=sp.gravity, alpha=sp.alpha, beta_lin=sp.beta_lin, beta_ang=sp.beta_ang, gamma=sp.gamma,
                contact_margin=sp.contact_margin, iterations=sp.iterations, flags=flags)
     p.up[0], p.up[1], p.up[2] = 0.0, 0.0, 1.0

@@ -1,10 +1,14 @@
 // Convex hull builder (host): the hull shape a body collides as, built once from a point set.
 //
-// A restatement of the reference's src/avbd3d/hull.ts (convexHull, buildHull, foldOf,
-// mergeTriangles, eigenSymmetric, quatFromBasis, spreadVertices) in C++, in double, keeping its
-// orders (point visits, triangle lists, face and edge numbering), so a hull built here numbers its
-// faces and edges as the reference's does. The output is the reference's hull record
-// (gpu/solver.ts:313-338 packHull with the header at 0) plus the mass properties.
+// A restatement of the reference's procedure in src/avbd3d/hull.ts (convexHull, buildHull, foldOf,
+// mergeTriangles, eigenSymmetric, quatFromBasis, spreadVertices) in C++, in double: the same
+// quickhull with coplanar faces merged, farthest-point simplification to AVBD_MAX_HULL_VERTICES, and
+// principal frame, so that the same points give the same hull (vertex set, faces, mass properties)
+// as the reference's hull tests pin them (tests/hull.test.ts, tests/hull-degenerate.test.ts). The
+// face and edge numbering is not pinned (the reference holds no built hull to compare with); it
+// only has to be consistent within one record, whose feature keys this backend both writes and
+// warm-starts from. The output is the reference's hull record (gpu/solver.ts:313-338 packHull with
+// the header at 0) plus the mass properties.
 #include <algorithm>
 #include <array>
 #include <cmath>
