@@ -75,6 +75,43 @@ def contact_events(prev: set, manifolds: np.ndarray, contacts: np.ndarray, bodie
     return events, set(now)
 
 
+def _planes(body, hull_words):
+    """A box's or hull's face planes in its frame: (normal, offset) rows."""
+    shape = float(body['shape'])
+    size = body['size'].astype(float)
+    if shape > 2.5:
+        head = hull_words[4 * int(shape - 3 + 0.5):4 * int(shape - 3 + 0.5) + 4]
+        fs, faces = int(head[2]), int(head[3])
+        return [hull_words[4 * (fs + 2 * k):4 * (fs + 2 * k) + 4].view(np.float32).astype(float) for k in range(faces)]
+    planes = []
+    for k in range(6):
+        e = np.zeros(3)
+        e[k // 2] = 1.0 if k % 2 == 0 else -1.0
+        planes.append(np.array([e[0], e[1], e[2], size[k // 2] * 0.5]))
+    return planes
+
+
+def normals_at(body, hull_words, origin, direction, t, tol):
+    """The world normals a hit at ray parameter t may report: a sphere's at the point o + d t (a
+    grazing ray's normal moves by the distance's rounding over the radius, so it is taken at the
+    distance the device found), a box's or hull's faces that the ray enters within `tol` of t (the
+    faces that tie where it lands on an edge or a corner)."""
+    q = body['rot'].astype(float)
+    o = rotate(conj(q), np.asarray(origin, float) - body['pos'].astype(float))
+    d = rotate(conj(q), np.asarray(direction, float))
+    if abs(float(body['shape']) - 1.0) < 0.5:
+        p = o + d * t
+        wn = rotate(q, p / np.linalg.norm(p))
+        return [wn / np.linalg.norm(wn)]
+    out = []
+    for pl in _planes(body, hull_words):
+        denom = pl[:3] @ d
+        if denom < -1e-12 and abs((pl[3] - pl[:3] @ o) / denom - t) <= tol:
+            wn = rotate(q, pl[:3])
+            out.append(wn / np.linalg.norm(wn))
+    return out
+
+
 def ray_trace(body, hull_words, origin, direction, max_distance):
     """Ray against one body (raycast.ts:80-150): (distance, normal in the body's frame) or None."""
     q = body['rot'].astype(float)
@@ -99,17 +136,7 @@ def ray_trace(body, hull_words, origin, direction, max_distance):
             n = p / np.linalg.norm(p)
     else:
         tin, tout, n = -3.0e38, 3.0e38, np.zeros(3)
-        if shape > 2.5:
-            head = hull_words[4 * int(shape - 3 + 0.5):4 * int(shape - 3 + 0.5) + 4]
-            fs, faces = int(head[2]), int(head[3])
-            planes = [hull_words[4 * (fs + 2 * k):4 * (fs + 2 * k) + 4].view(np.float32).astype(float) for k in range(faces)]
-        else:
-            planes = []
-            for k in range(6):
-                e = np.zeros(3)
-                e[k // 2] = 1.0 if k % 2 == 0 else -1.0
-                planes.append(np.array([e[0], e[1], e[2], size[k // 2] * 0.5]))
-        for pl in planes:
+        for pl in _planes(body, hull_words):
             denom = pl[:3] @ d
             dist = pl[3] - pl[:3] @ o
             if abs(denom) < 1e-12:

@@ -139,7 +139,9 @@ def test_raycast_matches_oracle(cuda_lib):
             assert h['body'] >= 0, f'ray {k}: no hit, body {b} expected'
             assert abs(h['distance'] - t) <= 1e-5 * max(1.0, t), f'ray {k}: distance {h["distance"]} vs {t}'
             if h['body'] == b:
-                assert np.allclose(h['normal'], nrm, atol=1e-4), f'ray {k}: normal'
+                if not np.allclose(h['normal'], nrm, atol=1e-4):  # faces that tie, or a grazing ray on a sphere
+                    ties = queries.normals_at(bodies[b], s.hull_words, rays['origin'][k], d, float(h['distance']), 1e-5 * max(1.0, t))
+                    assert any(np.allclose(h['normal'], m, atol=1e-4) for m in ties), f'ray {k}: normal {h["normal"]} vs {nrm}'
                 agree += 1
             else:  # only where two surfaces lie at the same distance
                 other = queries.ray_trace(bodies[h['body']], s.hull_words, rays['origin'][k], d, float(rays['max_distance'][k]))

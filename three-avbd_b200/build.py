@@ -1,7 +1,10 @@
 """Builds the CUDA backend into avbd_b200/libavbd_cuda.so (in-tree, so it travels with the repo).
 
 nvcc for sm_100a only. The collision translation unit is compiled with --fmad=false: its pair
-tests and SAT choices round every operation separately, as the oracle's f32 restatement does.
+tests and SAT choices round every operation separately, as the oracle's f32 restatement does. The
+solve translation unit uses the approximate single-precision division and square root
+(-prec-div=false -prec-sqrt=false, at most 2 ulp each): the solve is held to the FP64 oracle within a
+tolerance, not bit for bit, and the IEEE-rounded forms were a fifth of its time.
 """
 
 import os
@@ -17,7 +20,7 @@ COMMON = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relax
           '-I', os.path.join(HERE, '..', 'include')]
 UNITS = {
     'avbd_collide.cu': ['--fmad=false'],
-    'avbd_solve.cu': [],
+    'avbd_solve.cu': ['-prec-div=false', '-prec-sqrt=false'],
     'avbd_host.cu': [],
     'avbd_batch.cu': [],
     'avbd_hull.cu': [],

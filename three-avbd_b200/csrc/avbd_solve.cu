@@ -292,9 +292,13 @@ __device__ inline void evalContact(float4 ra, float4 rb, float4 pen, float4 lam,
   e.rAW = qrotate(rolling ? A.q0 : A.q, f3(ra));
   e.rBW = qrotate(rolling ? B.q0 : B.q, f3(rb));
   float keep = 1.0f - alpha;
-  e.C.x = rb.w * keep + dot3(n, A.dLin) - dot3(n, B.dLin) + dot3(cross3(e.rAW, n), A.dAng) + dot3(cross3(e.rBW, -n), B.dAng);
-  e.C.y = pen.w * keep + dot3(t1, A.dLin) - dot3(t1, B.dLin) + dot3(cross3(e.rAW, t1), A.dAng) + dot3(cross3(e.rBW, -t1), B.dAng);
-  e.C.z = lam.w * keep + dot3(t2, A.dLin) - dot3(t2, B.dLin) + dot3(cross3(e.rAW, t2), A.dAng) + dot3(cross3(e.rBW, -t2), B.dAng);
+  // Each row's linearised value C0 (1 - alpha) + J dx: the Jacobian terms (rA x d) . dAngA and
+  // (rB x -d) . dAngB are d . (dAngA x rA) and -d . (dAngB x rB) (the scalar triple product), so the
+  // three rows share the contact point's relative displacement dp
+  const float3 dp = (A.dLin - B.dLin) + (cross3(A.dAng, e.rAW) - cross3(B.dAng, e.rBW));
+  e.C.x = rb.w * keep + dot3(n, dp);
+  e.C.y = pen.w * keep + dot3(t1, dp);
+  e.C.z = lam.w * keep + dot3(t2, dp);
   float3 F = make_float3(pen.x * e.C.x + lam.x, pen.y * e.C.y + lam.y, pen.z * e.C.z + lam.z);
   F.x = fminf(F.x, 0.0f);
   e.bounds = fabsf(F.x) * friction;
@@ -743,8 +747,6 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
     q = qnormalize4(qmul(r, own.q0));
     const float4 dw = dangWord(r);
     da = f3(dw);
-    const float3 x = own.x0 + dl;
-    w.pos[body] = make_float4(x.x, x.y, x.z, w.pos[body].w);
     w.rot[body] = q;
     w.dlin[body] = make_float4(dl.x, dl.y, dl.z, 0.0f);
     w.dang[body] = dw;
@@ -1209,8 +1211,12 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     float4 vel = w.vel[i];
     float prevUp = dot3(f3(vel), up);
     if (w.size[i].w > 0.0f) {
+      // x = x- + the displacement (the sweep keeps only the displacement, which partners read)
+      const float3 dl = f3(w.dlin[i]);
+      const float3 x = f3(w.ipos[i]) + dl;
+      w.pos[i] = make_float4(x.x, x.y, x.z, w.pos[i].w);
       // (x - x-) / dt and qsub(q, q-) / dt: the step's displacement and 2 vec(r)
-      float3 v = f3(w.dlin[i]) / dt;
+      float3 v = dl / dt;
       w.vel[i] = make_float4(v.x, v.y, v.z, prevUp);
       float3 av = f3(w.dang[i]) / dt;
       w.avel[i] = make_float4(av.x, av.y, av.z, w.avel[i].w);
