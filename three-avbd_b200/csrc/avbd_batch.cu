@@ -226,7 +226,7 @@ int adaptBatch(avbd_batch* b, bool wait) {
   const uint32_t nw = uint32_t(b->worlds.size());
   std::vector<uint32_t> ctr(size_t(nw) * COUNTER_WORDS);
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
-  BATCH_TRY(b, cudaMemcpy(ctr.data(), b->d.counters, ctr.size() * 4, cudaMemcpyDeviceToHost));
+  BATCH_TRY(b, copyToHost(ctr.data(), b->d.counters, ctr.size() * 4, b->stream));
   std::vector<WorldDesc> old = b->worlds;
   bool any = false;
   for (uint32_t i = 0; i < nw; i++) {
@@ -388,8 +388,8 @@ static int takeRecording(avbd_batch* b, RecordingHandoff& out, std::string& why)
   }
   uint32_t status[2] = {0, 0};
   unsigned long long totals[2] = {0, 0};
-  if (cudaMemcpy(status, R.d.status, sizeof(status), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(totals, R.d.totals, sizeof(totals), cudaMemcpyDeviceToHost) != cudaSuccess) {
+  if (copyToHost(status, R.d.status, sizeof(status), b->stream) != cudaSuccess ||
+      copyToHost(totals, R.d.totals, sizeof(totals), b->stream) != cudaSuccess) {
     why = "reading the recording's status failed";
     return AVBD_ERR_CUDA;
   }
@@ -589,7 +589,7 @@ int avbd_batch_add_world_from(avbd_batch* b, avbd_world* src, uint32_t* index) {
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
   // last step's contact pairs (the buffer the next step reads)
   std::vector<uint32_t> ctr(COUNTER_WORDS);
-  BATCH_TRY(b, cudaMemcpy(ctr.data(), src->d.counters, COUNTER_WORDS * 4, cudaMemcpyDeviceToHost));
+  BATCH_TRY(b, copyToHost(ctr.data(), src->d.counters, COUNTER_WORDS * 4, b->stream));
   const uint32_t prevPairs = std::min(ctr[C_PAIRS], src->pairCap);
   const uint32_t first = b->n, firstJoint = b->nj;
   uint32_t pairCap = std::max<uint32_t>(std::max<uint32_t>(32, b->pairsPerBody * n), 2 * prevPairs);
@@ -745,8 +745,8 @@ int avbd_batch_read_joints(avbd_batch* b, uint32_t world, avbd_joint* dst, avbd_
   cudaSetDevice(b->device);
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
   if (dst && w.nj)
-    BATCH_TRY(b, cudaMemcpy(dst, b->d.joint + size_t(w.joint) * JOINT_VEC4, size_t(w.nj) * sizeof(avbd_joint), cudaMemcpyDeviceToHost));
-  if (info && w.nj) BATCH_TRY(b, cudaMemcpy(info, b->d.jinfo + w.joint, size_t(w.nj) * sizeof(avbd_joint_info), cudaMemcpyDeviceToHost));
+    BATCH_TRY(b, copyToHost(dst, b->d.joint + size_t(w.joint) * JOINT_VEC4, size_t(w.nj) * sizeof(avbd_joint), b->stream));
+  if (info && w.nj) BATCH_TRY(b, copyToHost(info, b->d.jinfo + w.joint, size_t(w.nj) * sizeof(avbd_joint_info), b->stream));
   return AVBD_OK;
 }
 
@@ -759,7 +759,7 @@ int avbd_batch_read_colors(avbd_batch* b, uint32_t world, uint32_t* dst, uint32_
   if (cap < w.n) return bfail(b, AVBD_ERR_CAPACITY, "destination holds fewer entries than the world's bodies");
   cudaSetDevice(b->device);
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
-  BATCH_TRY(b, cudaMemcpy(dst, b->d.colorA + w.body, size_t(w.n) * 4, cudaMemcpyDeviceToHost));
+  BATCH_TRY(b, copyToHost(dst, b->d.colorA + w.body, size_t(w.n) * 4, b->stream));
   return AVBD_OK;
 }
 
@@ -770,7 +770,7 @@ int avbd_batch_read_counters(avbd_batch* b, uint32_t world, avbd_counters* out) 
   cudaSetDevice(b->device);
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
   uint32_t c[COUNTER_WORDS];
-  BATCH_TRY(b, cudaMemcpy(c, b->d.counters + size_t(world) * COUNTER_WORDS, sizeof(c), cudaMemcpyDeviceToHost));
+  BATCH_TRY(b, copyToHost(c, b->d.counters + size_t(world) * COUNTER_WORDS, sizeof(c), b->stream));
   std::memset(out, 0, sizeof(*out));
   out->pairs = c[C_PAIRS];
   out->contacts = c[C_CONTACTS];
@@ -919,8 +919,8 @@ int avbd_batch_record_status(avbd_batch* b, uint32_t* steps, uint64_t* manifolds
   if (b->rec.K) {
     cudaSetDevice(b->device);
     BATCH_TRY(b, cudaStreamSynchronize(b->stream));
-    BATCH_TRY(b, cudaMemcpy(status, b->rec.d.status, sizeof(status), cudaMemcpyDeviceToHost));
-    BATCH_TRY(b, cudaMemcpy(totals, b->rec.d.totals, sizeof(totals), cudaMemcpyDeviceToHost));
+    BATCH_TRY(b, copyToHost(status, b->rec.d.status, sizeof(status), b->stream));
+    BATCH_TRY(b, copyToHost(totals, b->rec.d.totals, sizeof(totals), b->stream));
   }
   if (steps) *steps = b->rec.done;
   if (manifolds) *manifolds = totals[0];

@@ -446,51 +446,127 @@ __device__ inline void testFromProber(const DWorld& w, const StepParams& p, cons
 // the 13 cells of its forward half-shell, so each small-small pair is visited once; cells are at
 // least twice the largest small radius, so this covers every overlap. Large bodies test against
 // everything (the large list), as the reference's do.
-__global__ void __launch_bounds__(128) k_find_pairs(DWorld w, StepParams p) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n || !enabled(w, i)) return;
-  bool dyn = w.size[i].w > 0.0f;
-  bool small = w.moment[i].w <= p.largeThreshold;
-  if (small) {
-    Probe P = probeOf(w, i);
-    int4 c = w.cell[i];
-    for (int o = 0; o < 14; o++) {
-      // offset o = 0: the own cell; 1..13: (dx, dy, dz) > 0 in (z, y, x) order
-      int q = o == 0 ? 13 : 13 + o;
-      int4 cc = make_int4(c.x + q % 3 - 1, c.y + (q / 3) % 3 - 1, c.z + q / 9 - 1, 0);
-      uint32_t h = cellHash(cc, p.tableMask);
-      uint32_t end = w.cellEnd[h];
-      for (uint32_t k = w.cellStart[h]; k < end; k++) {
-        int4 cj = w.sortedCell[k];
-        uint32_t j = (uint32_t)cj.w & 0x7fffffffu;
-        bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
-        if (o == 0 && j >= i) continue;
-        if (!dyn && !dj) continue;
-        if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
-        float4 pr = w.sortedPR[k];
-        float3 d = P.pos - make_float3(pr.x, pr.y, pr.z);
-        float r = P.radius + pr.w;
-        if (dot3(d, d) > r * r) continue;  // the sphere test, the same in both views
-        float4 ab = w.sortedAabb[k];         // and the AABB test (its sums commute)
-        if (fabsf(d.x) > P.aabb.x + ab.x + 1e-4f || fabsf(d.y) > P.aabb.y + ab.y + 1e-4f || fabsf(d.z) > P.aabb.z + ab.z + 1e-4f) continue;
-        testFromProber(w, p, P, j);
-      }
-    }
-    if (dyn || p.anyDynamicLarge) {
-      for (uint32_t k = 0; k < p.nLarge; k++) {
-        uint32_t l = w.large[k];
-        if (!dyn && (!enabled(w, l) || w.size[l].w <= 0.0f)) continue;
-        testPair(w, p, P, l);
-      }
-    }
-    return;
+//
+// One cell of small body i's walk: offset o = 0 is its own cell, 1..13 the forward half-shell
+// ((dx, dy, dz) > 0 in (z, y, x) order)
+__device__ inline void walkCell(const DWorld& w, const StepParams& p, const Probe& P, bool dyn, int4 c, int o) {
+  const uint32_t i = P.index;
+  const int q = o == 0 ? 13 : 13 + o;
+  const int4 cc = make_int4(c.x + q % 3 - 1, c.y + (q / 3) % 3 - 1, c.z + q / 9 - 1, 0);
+  const uint32_t h = cellHash(cc, p.tableMask);
+  const uint32_t end = w.cellEnd[h];
+  for (uint32_t k = w.cellStart[h]; k < end; k++) {
+    int4 cj = w.sortedCell[k];
+    uint32_t j = (uint32_t)cj.w & 0x7fffffffu;
+    bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
+    if (o == 0 && j >= i) continue;
+    if (!dyn && !dj) continue;
+    if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
+    float4 pr = w.sortedPR[k];
+    float3 d = P.pos - make_float3(pr.x, pr.y, pr.z);
+    float r = P.radius + pr.w;
+    if (dot3(d, d) > r * r) continue;  // the sphere test, the same in both views
+    float4 ab = w.sortedAabb[k];         // and the AABB test (its sums commute)
+    if (fabsf(d.x) > P.aabb.x + ab.x + 1e-4f || fabsf(d.y) > P.aabb.y + ab.y + 1e-4f || fabsf(d.z) > P.aabb.z + ab.z + 1e-4f) continue;
+    testFromProber(w, p, P, j);
   }
-  if (!dyn) return;
-  Probe P = probeOf(w, i);
+}
+// A small body against the large list
+__device__ inline void smallAgainstLarge(const DWorld& w, const StepParams& p, const Probe& P, bool dyn) {
+  if (!dyn && !p.anyDynamicLarge) return;
   for (uint32_t k = 0; k < p.nLarge; k++) {
     uint32_t l = w.large[k];
-    if (l == i || (l < i && w.size[l].w > 0.0f)) continue;
+    if (!dyn && (!enabled(w, l) || w.size[l].w <= 0.0f)) continue;
     testPair(w, p, P, l);
+  }
+}
+// A large dynamic body against the large list (each pair of large bodies once)
+__device__ inline void largeAgainstLarge(const DWorld& w, const StepParams& p, const Probe& P) {
+  for (uint32_t k = 0; k < p.nLarge; k++) {
+    uint32_t l = w.large[k];
+    if (l == P.index || (l < P.index && w.size[l].w > 0.0f)) continue;
+    testPair(w, p, P, l);
+  }
+}
+
+// One thread per body walks its cells with the cheap tests (cell, sphere, AABB); the candidates
+// that pass go to a per-warp queue in shared memory, and whenever it holds a warp's worth, the warp
+// takes the full test (the prober's view, the face separation, the no-collide list) one candidate a
+// lane, so that the long test runs on full warps instead of on the few lanes whose walk found one.
+constexpr uint32_t PAIR_WALK_THREADS = 128, PAIR_QUEUE = 64;
+__device__ __forceinline__ void testCandidate(const DWorld& w, const StepParams& p, uint2 e) {
+  const uint32_t pr = proberOf(w, p, e.x, e.y);
+  testPair(w, p, probeOf(w, pr), pr == e.x ? e.y : e.x);
+}
+// Lanes take the queue's first min(count, 32) candidates and test them; the rest move to the front.
+__device__ __forceinline__ void drainQueue(const DWorld& w, const StepParams& p, uint2* Q, uint32_t& count, uint32_t lane) {
+  const uint32_t take = min(count, 32u);
+  const uint2 e = lane < take ? Q[lane] : make_uint2(0u, 0u);
+  __syncwarp();
+  if (lane + take < count) Q[lane] = Q[lane + take];
+  __syncwarp();
+  count -= take;
+  if (lane < take) testCandidate(w, p, e);
+}
+__global__ void __launch_bounds__(PAIR_WALK_THREADS) k_find_pairs(DWorld w, StepParams p) {
+  __shared__ uint2 s_queue[PAIR_WALK_THREADS / 32][PAIR_QUEUE];
+  const uint32_t lane = threadIdx.x & 31u;
+  uint2* Q = s_queue[threadIdx.x >> 5];
+  uint32_t count = 0;  // the warp's queue length (the same in every lane)
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool on = i < p.n && enabled(w, i);
+  const bool dyn = on && w.size[i].w > 0.0f;
+  const bool small = on && w.moment[i].w <= p.largeThreshold;
+  float3 pos = make_float3(0.0f, 0.0f, 0.0f), aabb = pos;
+  float radius = 0.0f;
+  int4 c = make_int4(0, 0, 0, 0);
+  if (small) {
+    pos = f3(w.pos[i]);
+    radius = w.moment[i].w;
+    aabb = aabbOf(w, i);
+    c = w.cell[i];
+  }
+#pragma unroll 1
+  for (int o = 0; o < 14; o++) {
+    // offset o = 0: the own cell; 1..13: (dx, dy, dz) > 0 in (z, y, x) order
+    const int q = o == 0 ? 13 : 13 + o;
+    const int4 cc = make_int4(c.x + q % 3 - 1, c.y + (q / 3) % 3 - 1, c.z + q / 9 - 1, 0);
+    uint32_t k = 0, end = 0;
+    if (small) {
+      const uint32_t h = cellHash(cc, p.tableMask);
+      k = w.cellStart[h];
+      end = w.cellEnd[h];
+    }
+    while (__any_sync(0xffffffffu, k < end)) {
+      bool push = false;
+      uint32_t j = 0;
+      if (k < end) {
+        const int4 cj = w.sortedCell[k];
+        j = (uint32_t)cj.w & 0x7fffffffu;
+        const bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
+        if (!(o == 0 && j >= i) && (dyn || dj) && cj.x == cc.x && cj.y == cc.y && cj.z == cc.z) {
+          const float4 pr = w.sortedPR[k];
+          const float3 d = pos - make_float3(pr.x, pr.y, pr.z);
+          const float r = radius + pr.w;
+          if (dot3(d, d) <= r * r) {  // the sphere test, the same in both views
+            const float4 ab = w.sortedAabb[k];  // and the AABB test (its sums commute)
+            push = !(fabsf(d.x) > aabb.x + ab.x + 1e-4f || fabsf(d.y) > aabb.y + ab.y + 1e-4f || fabsf(d.z) > aabb.z + ab.z + 1e-4f);
+          }
+        }
+        k++;
+      }
+      const uint32_t m = __ballot_sync(0xffffffffu, push);
+      if (push) Q[count + __popc(m & ((1u << lane) - 1u))] = make_uint2(i, j);
+      count += __popc(m);
+      __syncwarp();
+      if (count >= 32u) drainQueue(w, p, Q, count, lane);
+    }
+  }
+  while (count > 0u) drainQueue(w, p, Q, count, lane);
+  if (small) {
+    smallAgainstLarge(w, p, probeOf(w, i), dyn);
+  } else if (dyn) {
+    largeAgainstLarge(w, p, probeOf(w, i));
   }
 }
 
@@ -1565,7 +1641,7 @@ uint32_t launch_collision(const DWorld& w, const StepParams& p, uint32_t tableSi
     k_scan_add<<<tiles, SCAN_THREADS, 0, s>>>(w.cellStart, tableSize, w.radixHist);
     k_bucket_finish<<<grid_for(tableSize, 256), 256, 0, s>>>(w.cellStart, w.cellEnd, tableSize);
     k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(w, n, sentinel);
-    k_find_pairs<<<grid_for(n, 128), 128, 0, s>>>(w, p);
+    k_find_pairs<<<grid_for(n, PAIR_WALK_THREADS), PAIR_WALK_THREADS, 0, s>>>(w, p);
     launches += 8;
   }
   k_narrowphase<<<GS_BLOCKS, 128, 0, s>>>(w, p);
@@ -1666,44 +1742,14 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_find_pairs_noalloc(DWorld w
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {  // the walk of k_find_pairs, body i
     if (!enabled(w, i)) continue;
-    bool dyn = w.size[i].w > 0.0f;
-    Probe P = probeOf(w, i);
+    const bool dyn = w.size[i].w > 0.0f;
+    const Probe P = probeOf(w, i);
     if (w.moment[i].w <= p.largeThreshold) {
-      int4 c = w.cell[i];
-      for (int o = 0; o < 14; o++) {
-        int q = o == 0 ? 13 : 13 + o;
-        int4 cc = make_int4(c.x + q % 3 - 1, c.y + (q / 3) % 3 - 1, c.z + q / 9 - 1, 0);
-        uint32_t h = cellHash(cc, p.tableMask);
-        uint32_t end = w.cellEnd[h];
-        for (uint32_t k = w.cellStart[h]; k < end; k++) {
-          int4 cj = w.sortedCell[k];
-          uint32_t j = (uint32_t)cj.w & 0x7fffffffu;
-          bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
-          if (o == 0 && j >= i) continue;
-          if (!dyn && !dj) continue;
-          if (cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) continue;
-          float4 pr = w.sortedPR[k];
-          float3 d = P.pos - make_float3(pr.x, pr.y, pr.z);
-          float r = P.radius + pr.w;
-          if (dot3(d, d) > r * r) continue;
-          float4 ab = w.sortedAabb[k];
-          if (fabsf(d.x) > P.aabb.x + ab.x + 1e-4f || fabsf(d.y) > P.aabb.y + ab.y + 1e-4f || fabsf(d.z) > P.aabb.z + ab.z + 1e-4f) continue;
-          testFromProber(w, p, P, j);
-        }
-      }
-      if (dyn || p.anyDynamicLarge) {
-        for (uint32_t k = 0; k < p.nLarge; k++) {
-          uint32_t l = w.large[k];
-          if (!dyn && (!enabled(w, l) || w.size[l].w <= 0.0f)) continue;
-          testPair(w, p, P, l);
-        }
-      }
+      const int4 c = w.cell[i];
+      for (int o = 0; o < 14; o++) walkCell(w, p, P, dyn, c, o);
+      smallAgainstLarge(w, p, P, dyn);
     } else if (dyn) {
-      for (uint32_t k = 0; k < p.nLarge; k++) {
-        uint32_t l = w.large[k];
-        if (l == i || (l < i && w.size[l].w > 0.0f)) continue;
-        testPair(w, p, P, l);
-      }
+      largeAgainstLarge(w, p, P);
     }
   }
 }

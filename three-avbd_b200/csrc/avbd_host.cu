@@ -435,7 +435,7 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(dalloc(w, &d.aux, B));
   if (ok) {  // every slot at the default aux record: gravity scale 1, no damping
     std::vector<float4> aux(B, make_float4(1.0f, 0.0f, 0.0f, 0.0f));
-    A(cudaMemcpy(d.aux, aux.data(), size_t(B) * sizeof(float4), cudaMemcpyHostToDevice));
+    A(copyToDevice(d.aux, aux.data(), size_t(B) * sizeof(float4), w->stream));
   }
   A(dalloc(w, &d.filters, B));
   A(dalloc(w, &d.keyA, B));
@@ -479,7 +479,7 @@ int avbd_world_create(const avbd_config* cfg, avbd_world** out) {
   A(cudaStreamSynchronize(w->stream));
   {
     std::vector<uint32_t> none(B, NO_COLOR);
-    A(cudaMemcpy(d.colorA, none.data(), size_t(B) * 4, cudaMemcpyHostToDevice));
+    A(copyToDevice(d.colorA, none.data(), size_t(B) * 4, w->stream));
   }
   if (!ok) return bad(AVBD_ERR_CUDA);
   w->pairCap = 0;
@@ -654,8 +654,8 @@ int avbd_write_joints(avbd_world* w, uint32_t first, const avbd_joint* joints, c
   if (r) return r;
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(first) * JOINT_VEC4, joints, size_t(n) * sizeof(avbd_joint), cudaMemcpyHostToDevice));
-  CUDA_TRY(w, cudaMemcpy(w->d.jinfo + first, info, size_t(n) * sizeof(int4), cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(w->d.joint + size_t(first) * JOINT_VEC4, joints, size_t(n) * sizeof(avbd_joint), w->stream));
+  CUDA_TRY(w, copyToDevice(w->d.jinfo + first, info, size_t(n) * sizeof(int4), w->stream));
   for (uint32_t i = 0; i < n; i++) w->info[first + i] = info[i];
   // a released slot rewritten with a live joint is taken again
   w->freeSlots.erase(std::remove_if(w->freeSlots.begin(), w->freeSlots.end(),
@@ -722,8 +722,8 @@ int avbd_append_joints(avbd_world* w, const avbd_joint* joints, const avbd_joint
   for (uint32_t k = 0; k < n;) {  // one copy per run of consecutive slots
     uint32_t e = k + 1;
     while (e < n && slots[e] == slots[e - 1] + 1) e++;
-    CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(slots[k]) * JOINT_VEC4, joints + k, size_t(e - k) * sizeof(avbd_joint), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(w->d.jinfo + slots[k], info + k, size_t(e - k) * sizeof(int4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, copyToDevice(w->d.joint + size_t(slots[k]) * JOINT_VEC4, joints + k, size_t(e - k) * sizeof(avbd_joint), w->stream));
+    CUDA_TRY(w, copyToDevice(w->d.jinfo + slots[k], info + k, size_t(e - k) * sizeof(int4), w->stream));
     k = e;
   }
   for (uint32_t k = 0; k < n; k++) {
@@ -757,8 +757,8 @@ int avbd_release_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
     while (e < order.size() && order[e] == order[e - 1] + 1) e++;
     const std::vector<avbd_joint> zeros(e - k);
     const std::vector<avbd_joint_info> infos(e - k, none);
-    CUDA_TRY(w, cudaMemcpy(w->d.joint + size_t(order[k]) * JOINT_VEC4, zeros.data(), zeros.size() * sizeof(avbd_joint), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(w->d.jinfo + order[k], infos.data(), infos.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, copyToDevice(w->d.joint + size_t(order[k]) * JOINT_VEC4, zeros.data(), zeros.size() * sizeof(avbd_joint), w->stream));
+    CUDA_TRY(w, copyToDevice(w->d.jinfo + order[k], infos.data(), infos.size() * sizeof(int4), w->stream));
     k = e;
   }
   for (uint32_t s : order) {
@@ -782,9 +782,9 @@ int avbd_disable_joints(avbd_world* w, const uint32_t* slots, uint32_t n) {
   const float zeros[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (uint32_t i = 0; i < n; i++) {
     float* rec = reinterpret_cast<float*>(w->d.joint + size_t(slots[i]) * JOINT_VEC4);
-    CUDA_TRY(w, cudaMemcpy(rec, zeros, 8 * sizeof(float), cudaMemcpyHostToDevice));        // penalties and stiffnesses
-    CUDA_TRY(w, cudaMemcpy(rec + 8, zeros, 3 * sizeof(float), cudaMemcpyHostToDevice));    // lam_lin (fracture kept)
-    CUDA_TRY(w, cudaMemcpy(rec + 12, zeros, 3 * sizeof(float), cudaMemcpyHostToDevice));   // lam_ang (torque arm kept)
+    CUDA_TRY(w, copyToDevice(rec, zeros, 8 * sizeof(float), w->stream));        // penalties and stiffnesses
+    CUDA_TRY(w, copyToDevice(rec + 8, zeros, 3 * sizeof(float), w->stream));    // lam_lin (fracture kept)
+    CUDA_TRY(w, copyToDevice(rec + 12, zeros, 3 * sizeof(float), w->stream));   // lam_ang (torque arm kept)
   }
   return AVBD_OK;
 }
@@ -813,7 +813,7 @@ int avbd_set_filters_at(avbd_world* w, const uint32_t* indices, const uint32_t* 
     while (e < n && indices[e] == indices[e - 1] + 1) e++;
     std::vector<uint2> run(e - k);
     for (uint32_t i = k; i < e; i++) run[i - k] = make_uint2(groups[i], collides_with[i]);
-    CUDA_TRY(w, cudaMemcpy(w->d.filters + indices[k], run.data(), run.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, copyToDevice(w->d.filters + indices[k], run.data(), run.size() * sizeof(uint2), w->stream));
     k = e;
   }
   return AVBD_OK;
@@ -825,7 +825,7 @@ int avbd_set_filters(avbd_world* w, uint32_t first, const uint32_t* gm, uint32_t
   if (uint64_t(first) + n > w->n) return fail(w, AVBD_ERR_INVALID, "setFilters: slots outside the world's bodies");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  CUDA_TRY(w, cudaMemcpy(w->d.filters + first, gm, size_t(n) * sizeof(uint2), cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(w->d.filters + first, gm, size_t(n) * sizeof(uint2), w->stream));
   return AVBD_OK;
 }
 
@@ -848,13 +848,13 @@ int avbd_set_body_aux(avbd_world* w, const uint32_t* indices, uint32_t n, const 
     while (e < n && indices[e] == indices[e - 1] + 1) e++;
     if (e - k == 1 && !linear) {
       float4 rec;
-      CUDA_TRY(w, cudaMemcpy(&rec, w->d.aux + indices[k], sizeof(float4), cudaMemcpyDeviceToHost));
+      CUDA_TRY(w, copyToHost(&rec, w->d.aux + indices[k], sizeof(float4), w->stream));
       rec.x = scales[k];
-      CUDA_TRY(w, cudaMemcpy(w->d.aux + indices[k], &rec, sizeof(float4), cudaMemcpyHostToDevice));
+      CUDA_TRY(w, copyToDevice(w->d.aux + indices[k], &rec, sizeof(float4), w->stream));
     } else {
       std::vector<float4> run(e - k);
       for (uint32_t i = k; i < e; i++) run[i - k] = make_float4(scales[i], linear ? linear[i] : 0.0f, linear ? angular[i] : 0.0f, 0.0f);
-      CUDA_TRY(w, cudaMemcpy(w->d.aux + indices[k], run.data(), run.size() * sizeof(float4), cudaMemcpyHostToDevice));
+      CUDA_TRY(w, copyToDevice(w->d.aux + indices[k], run.data(), run.size() * sizeof(float4), w->stream));
     }
     k = e;
   }
@@ -866,7 +866,7 @@ int avbd_read_body_aux(avbd_world* w, uint32_t first, float* aux4, uint32_t n) {
   if (uint64_t(first) + n > w->bodyCap) return fail(w, AVBD_ERR_INVALID, "aux records outside the body capacity");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  CUDA_TRY(w, cudaMemcpy(aux4, w->d.aux + first, size_t(n) * sizeof(float4), cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(aux4, w->d.aux + first, size_t(n) * sizeof(float4), w->stream));
   return AVBD_OK;
 }
 
@@ -878,11 +878,11 @@ int avbd_set_lifecycle(avbd_world* w, uint32_t index, uint32_t bits) {
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   // the lifecycle word is the initial pose's w (layout.ts:17-19); a rewritten slot has no contact history
   float4 ip;
-  CUDA_TRY(w, cudaMemcpy(&ip, w->d.ipos + index, sizeof(float4), cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(&ip, w->d.ipos + index, sizeof(float4), w->stream));
   ip.w = float(1u | bits);
-  CUDA_TRY(w, cudaMemcpy(w->d.ipos + index, &ip, sizeof(float4), cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(w->d.ipos + index, &ip, sizeof(float4), w->stream));
   const uint32_t none = NO_COLOR;
-  CUDA_TRY(w, cudaMemcpy(w->d.colorA + index, &none, sizeof(uint32_t), cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(w->d.colorA + index, &none, sizeof(uint32_t), w->stream));
   return AVBD_OK;
 }
 
@@ -911,12 +911,12 @@ int avbd_seed_contacts(avbd_world* w, const avbd_manifold* m, uint32_t nm, const
   }
   DWorld& d = w->d;
   if (nm) {
-    CUDA_TRY(w, cudaMemcpy(d.mIds[prev], ids.data(), nm * sizeof(uint4), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(d.mGeo[prev], geo.data(), nm * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(w, cudaMemcpy(d.cPt[prev], pts.data(), pts.size() * sizeof(avbd_contact), cudaMemcpyHostToDevice));
+    CUDA_TRY(w, copyToDevice(d.mIds[prev], ids.data(), nm * sizeof(uint4), w->stream));
+    CUDA_TRY(w, copyToDevice(d.mGeo[prev], geo.data(), nm * sizeof(float4), w->stream));
+    CUDA_TRY(w, copyToDevice(d.cPt[prev], pts.data(), pts.size() * sizeof(avbd_contact), w->stream));
   }
   uint32_t pairs = nm;
-  CUDA_TRY(w, cudaMemcpy(d.counters + C_PAIRS, &pairs, 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(d.counters + C_PAIRS, &pairs, 4, w->stream));
   w->countersInFlight = false;
   return AVBD_OK;
 }
@@ -933,7 +933,7 @@ int avbd_set_fixed_colors(avbd_world* w, const uint32_t* colors, uint32_t n) {
     if (colors[i] != NO_COLOR && colors[i] >= uint32_t(MAX_COLORS)) return fail(w, AVBD_ERR_INVALID, "colours are below 64 (or 255: none)");
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  CUDA_TRY(w, cudaMemcpy(w->d.fixedColor, colors, size_t(w->n) * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(w->d.fixedColor, colors, size_t(w->n) * 4, w->stream));
   w->fixedColors = true;
   return AVBD_OK;
 }
@@ -1019,18 +1019,18 @@ int avbd_read_reuse_state(avbd_world* w, float* ref_poses, uint32_t body_cap, ui
   if (nb && !ref_poses) return AVBD_ERR_INVALID;
   if (nb) {
     std::vector<float4> pos(nb), rot(nb);
-    CUDA_TRY(w, cudaMemcpy(pos.data(), w->d.refPos, nb * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(w, cudaMemcpy(rot.data(), w->d.refRot, nb * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, copyToHost(pos.data(), w->d.refPos, nb * sizeof(float4), w->stream));
+    CUDA_TRY(w, copyToHost(rot.data(), w->d.refRot, nb * sizeof(float4), w->stream));
     for (uint32_t i = 0; i < nb; i++) {
       std::memcpy(ref_poses + 8 * size_t(i), &pos[i], sizeof(float4));
       std::memcpy(ref_poses + 8 * size_t(i) + 4, &rot[i], sizeof(float4));
     }
   }
   uint32_t pairs = 0;
-  CUDA_TRY(w, cudaMemcpy(&pairs, w->d.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(&pairs, w->d.counters + C_PAIRS, 4, w->stream));
   pairs = std::min(pairs, w->pairCap);
   std::vector<uint4> ids(pairs);
-  if (pairs) CUDA_TRY(w, cudaMemcpy(ids.data(), w->d.mIds[1 - w->cur], pairs * sizeof(uint4), cudaMemcpyDeviceToHost));
+  if (pairs) CUDA_TRY(w, copyToHost(ids.data(), w->d.mIds[1 - w->cur], pairs * sizeof(uint4), w->stream));
   uint32_t mi = 0;
   for (uint32_t p = 0; p < pairs; p++) {
     if (!(ids[p].w & 15u)) continue;
@@ -1080,7 +1080,7 @@ int avbd_read_joints(avbd_world* w, avbd_joint* dst, avbd_joint_info* info, uint
   uint32_t k = std::min(cap, w->nj);
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  if (k && dst) CUDA_TRY(w, cudaMemcpy(dst, w->d.joint, size_t(k) * sizeof(avbd_joint), cudaMemcpyDeviceToHost));
+  if (k && dst) CUDA_TRY(w, copyToHost(dst, w->d.joint, size_t(k) * sizeof(avbd_joint), w->stream));
   if (k && info) std::memcpy(info, w->info.data(), size_t(k) * sizeof(avbd_joint_info));
   return AVBD_OK;
 }
@@ -1090,7 +1090,7 @@ int avbd_read_counters(avbd_world* w, avbd_counters* out) {
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   uint32_t c[COUNTER_WORDS];
-  CUDA_TRY(w, cudaMemcpy(c, w->d.counters, sizeof(c), cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(c, w->d.counters, sizeof(c), w->stream));
   std::memset(out, 0, sizeof(*out));
   out->pairs = c[C_PAIRS];
   out->contacts = c[C_CONTACTS];
@@ -1112,19 +1112,19 @@ int avbd_read_contacts(avbd_world* w, avbd_manifold* mout, uint32_t mcap, uint32
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   uint32_t pairs = 0;
-  CUDA_TRY(w, cudaMemcpy(&pairs, w->d.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(&pairs, w->d.counters + C_PAIRS, 4, w->stream));
   pairs = std::min(pairs, w->pairCap);
   const int last = 1 - w->cur;
   std::vector<uint4> ids(pairs);
   std::vector<float4> geo(pairs);
   if (pairs) {
-    CUDA_TRY(w, cudaMemcpy(ids.data(), w->d.mIds[last], pairs * sizeof(uint4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(w, cudaMemcpy(geo.data(), w->d.mGeo[last], pairs * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, copyToHost(ids.data(), w->d.mIds[last], pairs * sizeof(uint4), w->stream));
+    CUDA_TRY(w, copyToHost(geo.data(), w->d.mGeo[last], pairs * sizeof(float4), w->stream));
   }
   std::vector<avbd_contact> pts;
   if (pairs) {
     pts.resize(size_t(pairs) * MAX_CONTACTS);
-    CUDA_TRY(w, cudaMemcpy(pts.data(), w->d.cPt[last], pts.size() * sizeof(avbd_contact), cudaMemcpyDeviceToHost));
+    CUDA_TRY(w, copyToHost(pts.data(), w->d.cPt[last], pts.size() * sizeof(avbd_contact), w->stream));
   }
   uint32_t mi = 0, ci = 0;
   for (uint32_t p = 0; p < pairs; p++) {
@@ -1157,11 +1157,11 @@ int avbd_read_pairs(avbd_world* w, uint32_t* dst, uint32_t cap, uint32_t* n) {
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   uint32_t pairs = 0;
-  CUDA_TRY(w, cudaMemcpy(&pairs, w->d.counters + C_PAIRS, 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(&pairs, w->d.counters + C_PAIRS, 4, w->stream));
   pairs = std::min(pairs, w->pairCap);
   if (n) *n = pairs;
   uint32_t k = std::min(cap, pairs);
-  if (k && dst) CUDA_TRY(w, cudaMemcpy(dst, w->d.pairs, size_t(k) * sizeof(uint2), cudaMemcpyDeviceToHost));
+  if (k && dst) CUDA_TRY(w, copyToHost(dst, w->d.pairs, size_t(k) * sizeof(uint2), w->stream));
   return AVBD_OK;
 }
 
@@ -1171,7 +1171,7 @@ int avbd_read_colors(avbd_world* w, uint32_t* dst, uint32_t cap, uint32_t* n) {
   uint32_t k = std::min(cap, w->n);
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
-  if (k && dst) CUDA_TRY(w, cudaMemcpy(dst, w->d.colorA, size_t(k) * 4, cudaMemcpyDeviceToHost));
+  if (k && dst) CUDA_TRY(w, copyToHost(dst, w->d.colorA, size_t(k) * 4, w->stream));
   return AVBD_OK;
 }
 
@@ -1202,7 +1202,7 @@ int avbd_read_step_stats(avbd_world* w, avbd_step_stats* dst, uint32_t cap, uint
   if (n) *n = have;
   if (!dst || !have) return AVBD_OK;
   std::vector<uint32_t> r(size_t(w->statsCap) * STAT_WORDS);
-  CUDA_TRY(w, cudaMemcpy(r.data(), w->d.statsRing, r.size() * 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(r.data(), w->d.statsRing, r.size() * 4, w->stream));
   uint32_t first = w->statsCount - have;
   for (uint32_t k = 0; k < have && k < cap; k++) {
     const uint32_t* q = &r[size_t((first + k) % w->statsCap) * STAT_WORDS];
@@ -1228,7 +1228,7 @@ int avbd_read_phase_clocks(avbd_world* w, double* dst, uint32_t cap, uint32_t* n
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   std::vector<unsigned long long> ck(CLOCK_WORDS);
-  CUDA_TRY(w, cudaMemcpy(ck.data(), w->d.clocks, ck.size() * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(ck.data(), w->d.clocks, ck.size() * 8, w->stream));
   uint32_t k = uint32_t(std::min<unsigned long long>(ck[0], MAX_CLOCKS));
   if (n) *n = k;
   for (uint32_t i = 0; i < k && i < cap && dst; i++) dst[i] = double(ck[1 + i] - ck[1]) * 1e-6;
@@ -1286,9 +1286,9 @@ int avbd_add_hull(avbd_world* w, const uint32_t* packed, uint32_t vec4s, uint32_
     w->d.hulls = fresh;
     w->hullCapVec4 = cap;
     w->configGen++;  // the step graphs hold the buffer's address
-    CUDA_TRY(w, cudaMemcpy(w->d.hulls, w->hullWords.data(), w->hullWords.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(w, copyToDevice(w->d.hulls, w->hullWords.data(), w->hullWords.size() * 4, w->stream));
   } else {
-    CUDA_TRY(w, cudaMemcpy(w->d.hulls + at, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(w, copyToDevice(w->d.hulls + at, rec.data(), rec.size() * 4, w->stream));
   }
   w->hullStarts.insert(at);
   w->hullSize[at] = vec4s;
@@ -1303,7 +1303,7 @@ int avbd_release_hull(avbd_world* w, uint32_t offset) {
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   // a record some body still names stays (its shape code would point into whatever reuses the run)
   std::vector<float4> avel(w->n);
-  if (w->n) CUDA_TRY(w, cudaMemcpy(avel.data(), w->d.avel, size_t(w->n) * sizeof(float4), cudaMemcpyDeviceToHost));
+  if (w->n) CUDA_TRY(w, copyToHost(avel.data(), w->d.avel, size_t(w->n) * sizeof(float4), w->stream));
   const float code = float(AVBD_SHAPE_HULL + offset);
   for (uint32_t i = 0; i < w->n; i++)
     if (avel[i].w == code) return fail(w, AVBD_ERR_INVALID, "body " + std::to_string(i) + " uses the hull at offset " + std::to_string(offset));
@@ -1378,7 +1378,7 @@ int avbd_add_world_joint(avbd_world* w, uint32_t body, const float anchor_world[
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   float4 size;
-  CUDA_TRY(w, cudaMemcpy(&size, w->d.size + body, sizeof(float4), cudaMemcpyDeviceToHost));
+  CUDA_TRY(w, copyToHost(&size, w->d.size + body, sizeof(float4), w->stream));
   const float arm = size.x * size.x + size.y * size.y + size.z * size.z;
   if (!std::isfinite(arm)) return fail(w, AVBD_ERR_INVALID, "appendWorldJoint: torque arm must be finite as f32");
   avbd_joint j{};
@@ -1410,7 +1410,7 @@ int avbd_set_world_anchor(avbd_world* w, uint32_t slot, const float p[3]) {
   cudaSetDevice(w->device);
   CUDA_TRY(w, cudaStreamSynchronize(w->stream));
   float* rec = reinterpret_cast<float*>(w->d.joint + size_t(slot) * JOINT_VEC4 + J_RA);
-  CUDA_TRY(w, cudaMemcpy(rec, p, 3 * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_TRY(w, copyToDevice(rec, p, 3 * sizeof(float), w->stream));
   return AVBD_OK;
 }
 

@@ -90,4 +90,20 @@ struct avbd_world {
 namespace avbd {
 // Uploads the world's large-body list and sorted no-collide triples when they changed
 int uploadStatics(avbd_world* w);
+
+// Copies between host and device, ordered on stream s and complete when they return. A plain
+// cudaMemcpy runs on the legacy default stream, which the worlds' non-blocking streams do not wait
+// on, and from pageable memory it returns before its DMA has landed: a kernel launched next on the
+// world's stream could read the old bytes. The async copy stages pageable memory before returning,
+// so the host buffer may go as soon as these return.
+inline cudaError_t copyToDevice(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return cudaSuccess;
+  const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+inline cudaError_t copyToHost(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return cudaSuccess;
+  const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
 }  // namespace avbd

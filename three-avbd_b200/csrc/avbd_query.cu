@@ -444,11 +444,11 @@ int avbd_contact_watch_read(avbd_contact_watch* cw, avbd_contact_event* dst, uin
   uint32_t head[4];
   std::vector<float4> ev;
   cudaError_t e = cudaStreamSynchronize(w->stream);
-  if (e == cudaSuccess) e = cudaMemcpy(head, cw->head, 16, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = copyToHost(head, cw->head, 16, w->stream);
   const uint32_t have = std::min(head[0], cw->capacity);
   if (e == cudaSuccess && have) {
     ev.resize(size_t(have) * 3);
-    e = cudaMemcpy(ev.data(), cw->events, ev.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+    e = copyToHost(ev.data(), cw->events, ev.size() * sizeof(float4), w->stream);
   }
   if (e == cudaSuccess) e = cudaMemset(cw->head, 0, 16);
   if (e != cudaSuccess) return wfail(cw, AVBD_ERR_CUDA, std::string("avbd_contact_watch_read: ") + cudaGetErrorString(e));
