@@ -23,9 +23,10 @@ using namespace avbd::adj;
 
 namespace {
 
-constexpr int ADJ_THREADS = 128;     // bodies of a world at most
+constexpr int ADJ_MAX_BODIES = 128;  // bodies of a world at most
+constexpr int ADJ_BLOCK = 64;        // threads a world (a block): bodies and points are strided over them
 constexpr int ADJ_MAX_POINTS = 1024;  // points of a world in one step at most
-constexpr int ADJ_BLOCKS_PER_SM = 4;  // worlds in flight per SM: registers capped at 128 a thread
+constexpr int ADJ_BLOCKS_PER_SM = 8;  // worlds in flight per SM in the replay: registers capped at 128 a thread
 constexpr double PEN_MIN = 1.0, PEN_MAX = 1e10, PIVOT = 1e-5;
 
 // A body's primal solve at one iteration, kept by the segment recompute for the reverse sweep: its
@@ -34,6 +35,25 @@ struct FactRec {
   double L[15], D[6], invD[6], rhs[6], delta[6];
   int floored;
 };
+// x = H^-1 b from a kept factorization, read in place (L's row i, column j < i at i (i - 1) / 2 + j):
+// solve6's operations in solve6's order
+__device__ inline void solvePacked(const FactRec& fr, const double* b, double* x) {
+  double y[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    double s = b[i];
+#pragma unroll
+    for (int k = 0; k < i; k++) s -= fr.L[i * (i - 1) / 2 + k] * y[k];
+    y[i] = s;
+  }
+#pragma unroll
+  for (int i = 5; i >= 0; i--) {
+    double s = y[i] * fr.invD[i];
+#pragma unroll
+    for (int k = i + 1; k < 6; k++) s -= fr.L[k * (k - 1) / 2 + i] * x[k];
+    x[i] = s;
+  }
+}
 
 struct AdjDev {
   int W, K, I, ck;
@@ -85,6 +105,7 @@ struct AdjDev {
   D3 *gLam, *gPen, *gLamP, *gPenP, *gC0;
   double* loss;  // per world
   double* finalPose;
+  double* floorWork;  // per world, ADJ_GROUP x (H's cotangent 36, L's 36): a floored factorization's reverse
 };
 
 __device__ inline void atomicAdd3(D3* a, D3 v) {
@@ -125,49 +146,73 @@ constexpr int ADJ_ROW = 27;    // an incidence's share of its body's system: H's
 // bodies are positions s_colStart[c] .. s_colStart[c + 1], and their incidences (local point |
 // position << 16) are contiguous in s_inc, position p's at s_incStart[p] .. s_incStart[p + 1].
 __shared__ int s_colStart[ADJ_MAX_COLORS + 1];
-__shared__ int s_colBody[ADJ_THREADS];
-__shared__ int s_posOf[ADJ_THREADS];
+__shared__ int s_colBody[ADJ_MAX_BODIES];
+__shared__ int s_posOf[ADJ_MAX_BODIES];
 __shared__ int s_nSolved;
-__shared__ int s_incStart[ADJ_THREADS + 1];
+__shared__ int s_incStart[ADJ_MAX_BODIES + 1];
 __shared__ int s_inc[2 * ADJ_MAX_POINTS];
+__shared__ int s_color[ADJ_MAX_BODIES];
 // Dynamic shared memory: a chunk of incidences, a row each (its share of the body's system, or its
 // own-body cotangents), then, in the reverse sweep, a group's bodies: step, cotangent of g, and for a
 // floored factorization the cotangents of H and L
 struct BodyVjp {
-  double delta[6], w[6], Hb[36], Lb[36];
+  double delta[6], w[6];
   int floored;
 };
 extern __shared__ __align__(16) double s_dyn[];
-constexpr size_t ADJ_SMEM_ROWS = sizeof(double) * ADJ_THREADS * ADJ_ROW;
+constexpr size_t ADJ_SMEM_ROWS = sizeof(double) * ADJ_BLOCK * ADJ_ROW;
 constexpr size_t ADJ_SMEM_FORWARD = ADJ_SMEM_ROWS, ADJ_SMEM_BACKWARD = ADJ_SMEM_ROWS + sizeof(BodyVjp) * ADJ_GROUP;
 __device__ inline double* rowOf(int i) { return s_dyn + size_t(i) * ADJ_ROW; }
-__device__ inline BodyVjp* bodyVjp() { return reinterpret_cast<BodyVjp*>(s_dyn + size_t(ADJ_THREADS) * ADJ_ROW); }
+// In the reverse sweep an incidence's row is its own body's cotangents (14); a group slot's sums of
+// them follow the rows, so that they stay in shared memory rather than registers across the
+// incidences' long evaluation
+constexpr int ADJ_OWN = 14;
+__device__ inline double* ownRow(int i) { return s_dyn + size_t(i) * ADJ_OWN; }
+__device__ inline double* ownSum(int slot) { return s_dyn + size_t(ADJ_BLOCK) * ADJ_OWN + size_t(slot) * ADJ_OWN; }
+static_assert(size_t(ADJ_BLOCK + ADJ_GROUP) * ADJ_OWN <= size_t(ADJ_BLOCK) * ADJ_ROW, "the reverse rows and sums fit in the rows");
+__device__ inline BodyVjp* bodyVjp() { return reinterpret_cast<BodyVjp*>(s_dyn + size_t(ADJ_BLOCK) * ADJ_ROW); }
+// While the incidence is built the rows are free: the step's points' bodies (world-local) go there
+__device__ inline int2* pointBodies() { return reinterpret_cast<int2*>(s_dyn); }
+static_assert(sizeof(int2) * ADJ_MAX_POINTS <= ADJ_SMEM_ROWS, "a step's point bodies fit in the rows");
+// Group slot i's floored-factorization cotangents (H's, then L's): global, as floored pivots are rare
+__device__ inline double* floorHb(const AdjDev& D, int i) { return D.floorWork + (size_t(blockIdx.x) * ADJ_GROUP + i) * 72; }
 
 __device__ void buildIncidence(const AdjDev& D, const StepView& v) {
   const int tid = threadIdx.x;
   for (int i = tid; i <= ADJ_MAX_COLORS; i += blockDim.x) s_colStart[i] = 0;
+  for (int b = tid; b < v.nb; b += blockDim.x) s_color[b] = v.color[b];
   __syncthreads();
-  const int myColor = tid < v.nb ? v.color[tid] : -1;
-  const bool solved = myColor >= 0 && myColor < v.ncol;
-  if (solved) atomicAdd(&s_colStart[myColor + 1], 1);
+  for (int b = tid; b < v.nb; b += blockDim.x) {
+    const int c = s_color[b];
+    if (c >= 0 && c < v.ncol) atomicAdd(&s_colStart[c + 1], 1);
+  }
   __syncthreads();
   if (tid == 0) {
     for (int c = 0; c < ADJ_MAX_COLORS; c++) s_colStart[c + 1] += s_colStart[c];
     s_nSolved = s_colStart[ADJ_MAX_COLORS];
   }
   __syncthreads();
-  int myPos = -1;
-  if (solved) {
-    int r = 0;
-    for (int j = 0; j < tid; j++) r += v.color[j] == myColor;
-    myPos = s_colStart[myColor] + r;
-    s_colBody[myPos] = tid;
+  // a colour's bodies by index: a body's position is its colour's start + the bodies of its colour
+  // before it
+  for (int b = tid; b < v.nb; b += blockDim.x) {
+    const int c = s_color[b];
+    int pos = -1;
+    if (c >= 0 && c < v.ncol) {
+      int r = 0;
+      for (int j = 0; j < b; j++) r += s_color[j] == c;
+      pos = s_colStart[c] + r;
+      s_colBody[pos] = b;
+    }
+    s_posOf[b] = pos;
   }
-  if (tid < v.nb) s_posOf[tid] = myPos;
   for (int i = tid; i <= s_nSolved; i += blockDim.x) s_incStart[i] = 0;
+  // the step's points' bodies, once, for the counts and the per-body fill
+  const int np = v.p1 - v.p0;
+  int2* s_ptAB = pointBodies();
+  for (int lk = tid; lk < np; lk += blockDim.x) s_ptAB[lk] = D.manAB[D.ptMan[v.p0 + lk]];
   __syncthreads();
-  for (int k = v.p0 + tid; k < v.p1; k += blockDim.x) {
-    const int2 ab = D.manAB[D.ptMan[k]];
+  for (int lk = tid; lk < np; lk += blockDim.x) {
+    const int2 ab = s_ptAB[lk];
     const int pa = s_posOf[ab.x], pb = s_posOf[ab.y];
     if (pa >= 0) atomicAdd(&s_incStart[pa + 1], 1);
     if (pb >= 0) atomicAdd(&s_incStart[pb + 1], 1);
@@ -177,12 +222,12 @@ __device__ void buildIncidence(const AdjDev& D, const StepView& v) {
     for (int i = 0; i < s_nSolved; i++) s_incStart[i + 1] += s_incStart[i];
   __syncthreads();
   // fill in point order per body (deterministic)
-  if (tid < s_nSolved) {
-    const int lb = s_colBody[tid];
-    int o = s_incStart[tid];
-    for (int k = v.p0; k < v.p1; k++) {
-      const int2 ab = D.manAB[D.ptMan[k]];
-      if (ab.x == lb || ab.y == lb) s_inc[o++] = (k - v.p0) | (tid << 16);
+  for (int p = tid; p < s_nSolved; p += blockDim.x) {
+    const int lb = s_colBody[p];
+    int o = s_incStart[p];
+    for (int lk = 0; lk < np; lk++) {
+      const int2 ab = s_ptAB[lk];
+      if (ab.x == lb || ab.y == lb) s_inc[o++] = lk | (p << 16);
     }
   }
   __syncthreads();
@@ -394,8 +439,8 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
   }
   __syncthreads();
   // bodies: inertial targets and the warm-start guess (solver.ts:273-295, up = z)
-  if (threadIdx.x < v.nb) {
-    int gb = v.b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < v.nb; bi += blockDim.x) {
+    int gb = v.b0 + bi;
     D.ipos[gb] = D.pos[gb];
     D.irot[gb] = D.rot[gb];
     D.irotI[gb] = qinv(D.rot[gb]);
@@ -488,8 +533,8 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
     }
     __syncthreads();
     if (snapshots) {
-      if (threadIdx.x < v.nb) {
-        int gb = v.b0 + threadIdx.x;
+      for (int bi = threadIdx.x; bi < v.nb; bi += blockDim.x) {
+        int gb = v.b0 + bi;
         D.snPos[snB + (size_t)(it + 1) * D.nb + gb] = D.pos[gb];
         D.snRot[snB + (size_t)(it + 1) * D.nb + gb] = D.rot[gb];
       }
@@ -501,8 +546,8 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
     }
   }
   // velocities (solver.ts:328-334)
-  if (threadIdx.x < v.nb) {
-    int gb = v.b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < v.nb; bi += blockDim.x) {
+    int gb = v.b0 + bi;
     D.pvz[gb] = D.vel[gb].z;
     if (D.dynamic[gb]) {
       D.vel[gb] = (D.pos[gb] - D.ipos[gb]) * (1.0 / dt);
@@ -519,8 +564,8 @@ __device__ void stepForward(const AdjDev& D, int s, int w, int slot) {
 
 __device__ void loadInitial(const AdjDev& D, int w) {
   const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
-  if (threadIdx.x < nb) {
-    int gb = b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+    int gb = b0 + bi;
     const double* q = D.params + 8 * gb;
     D.pos[gb] = D.pos0[gb];
     D.rot[gb] = D.rot0[gb];
@@ -534,8 +579,8 @@ __device__ void loadInitial(const AdjDev& D, int w) {
 // State copies: `bodies and last step's points` to/from a checkpoint or segment slot
 __device__ void saveState(const AdjDev& D, int w, int np, D3* P, D4* R, D3* V, D3* A, double* Z, D3* L, D3* N, size_t slot) {
   const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
-  if (threadIdx.x < nb) {
-    int gb = b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+    int gb = b0 + bi;
     size_t o = slot * D.nb + gb;
     P[o] = D.pos[gb];
     R[o] = D.rot[gb];
@@ -553,8 +598,8 @@ __device__ void saveState(const AdjDev& D, int w, int np, D3* P, D4* R, D3* V, D
 __device__ void loadState(const AdjDev& D, int w, int np, const D3* P, const D4* R, const D3* V, const D3* A, const double* Z, const D3* L, const D3* N,
                           size_t slot) {
   const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
-  if (threadIdx.x < nb) {
-    int gb = b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+    int gb = b0 + bi;
     size_t o = slot * D.nb + gb;
     D.pos[gb] = P[o];
     D.rot[gb] = R[o];
@@ -576,10 +621,10 @@ __device__ inline int pointsBefore(const AdjDev& D, int s, int w) {  // the last
 
 __device__ void worldLoss(const AdjDev& D, int w) {
   const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
-  __shared__ double s_loss[ADJ_THREADS];
+  __shared__ double s_loss[ADJ_BLOCK];
   double l = 0.0;
-  if (threadIdx.x < nb) {
-    int gb = b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+    int gb = b0 + bi;
     const double* t = D.target + 7 * gb;
     D3 x = D.pos[gb];
     D4 q = D.rot[gb];
@@ -602,7 +647,7 @@ __device__ void worldLoss(const AdjDev& D, int w) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS, ADJ_BLOCKS_PER_SM) k_adj_forward(AdjDev D) {
+__global__ void __launch_bounds__(ADJ_BLOCK, ADJ_BLOCKS_PER_SM) k_adj_forward(AdjDev D) {
   const int w = blockIdx.x;
   loadInitial(D, w);
   for (int s = 0; s < D.K; s++) {
@@ -658,7 +703,7 @@ __device__ inline void incidenceVjp(const AdjDev& D, const StepView& v, int wpt,
       kb = 0.0;
       for (int i = 0; i < 6; i++)
         for (int j = 0; j <= i; j++) {
-          const double hb = bv.Hb[6 * i + j];
+          const double hb = floorHb(D, pos - g0)[6 * i + j];
           kb += hb * J[i] * J[j];
           if (i >= 3) MJ[i - 3] += hb * J[j];
           if (j >= 3) MJ[j - 3] += hb * J[i];
@@ -720,17 +765,9 @@ __device__ void primalGroupVjp(const AdjDev& D, const StepView& v, int wpt, int 
     const int gb = v.b0 + s_colBody[g0 + tid];
     // the forward's factorization and step, as the segment recompute kept them
     const FactRec& fr = D.snFact[size_t(it) * D.nb + gb];
-    LDLT6 F;
-    double rhs[6], delta[6];
-    int o = 0;
-    for (int i = 0; i < 6; i++) {
-      for (int j = 0; j < i; j++) F.L[i][j] = fr.L[o++];
-      F.L[i][i] = 1.0;
-      F.D[i] = fr.D[i];
-      F.invD[i] = fr.invD[i];
-      rhs[i] = fr.rhs[i];
-      delta[i] = fr.delta[i];
-    }
+    double delta[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) delta[i] = fr.delta[i];
     const int floored = fr.floored;
     // the new pose's cotangent: x' = x - delta_lin, q' = qaddv(q, -delta_ang)
     D3 x;
@@ -745,28 +782,43 @@ __device__ void primalGroupVjp(const AdjDev& D, const StepView& v, int wpt, int 
     BodyVjp& bv = bodyVjp()[tid];
     // the cotangent of g is w = H^-1 gDelta; that of H is -w delta^T symmetrised, or, through a
     // floored pivot, Hb from the factorization's reverse
-    if (!floored) solve6(F, gDelta, bv.w);
-    else ldltVjpMasked(F, floored, PIVOT, rhs, delta, gDelta, bv.w, bv.Lb, bv.Hb);
+    if (!floored) {
+      solvePacked(fr, gDelta, bv.w);
+    } else {
+      LDLT6 F;
+      double rhs[6];
+      int o = 0;
+      for (int i = 0; i < 6; i++) {
+        for (int j = 0; j < i; j++) F.L[i][j] = fr.L[o++];
+        F.L[i][i] = 1.0;
+        F.D[i] = fr.D[i];
+        F.invD[i] = fr.invD[i];
+        rhs[i] = fr.rhs[i];
+      }
+      ldltVjpMasked(F, floored, PIVOT, rhs, delta, gDelta, bv.w, floorHb(D, tid) + 36, floorHb(D, tid));
+    }
     for (int i = 0; i < 6; i++) bv.delta[i] = delta[i];
     bv.floored = floored;
   }
   __syncthreads();
   // the incidences' cotangents; each body sums its own
-  double own[14];
-  for (int i = 0; i < 14; i++) own[i] = 0.0;
+  if (tid < nbg)
+    for (int i = 0; i < ADJ_OWN; i++) ownSum(tid)[i] = 0.0;
   const int i0 = s_incStart[g0], i1 = s_incStart[g1];
   for (int ch = i0; ch < i1; ch += blockDim.x) {
-    if (ch + tid < i1) incidenceVjp(D, v, wpt, s_inc[ch + tid], g0, lamIn, penIn, poseOf, rowOf(tid));
+    if (ch + tid < i1) incidenceVjp(D, v, wpt, s_inc[ch + tid], g0, lamIn, penIn, poseOf, ownRow(tid));
     __syncthreads();
     if (tid < nbg) {
       const int p = g0 + tid;
       const int u0 = max(s_incStart[p], ch), u1 = min(s_incStart[p + 1], ch + int(blockDim.x));
+      double* own = ownSum(tid);
       for (int u = u0; u < u1; u++)
-        for (int i = 0; i < 14; i++) own[i] += rowOf(u - ch)[i];
+        for (int i = 0; i < ADJ_OWN; i++) own[i] += ownRow(u - ch)[i];
     }
     __syncthreads();
   }
   if (tid < nbg) {
+    const double* own = ownSum(tid);
     const int gb = v.b0 + s_colBody[g0 + tid];
     const BodyVjp& bv = bodyVjp()[tid];
     D3 x;
@@ -794,8 +846,9 @@ __device__ void primalGroupVjp(const AdjDev& D, const StepView& v, int wpt, int 
       dH = -(bv.w[0] * bv.delta[0] + bv.w[1] * bv.delta[1] + bv.w[2] * bv.delta[2]);
       dHa = -bv.w[3] * bv.delta[3] * Iu.x - bv.w[4] * bv.delta[4] * Iu.y - bv.w[5] * bv.delta[5] * Iu.z;
     } else {
-      dH = bv.Hb[0] + bv.Hb[7] + bv.Hb[14];
-      dHa = bv.Hb[21] * Iu.x + bv.Hb[28] * Iu.y + bv.Hb[35] * Iu.z;
+      const double* Hb = floorHb(D, tid);
+      dH = Hb[0] + Hb[7] + Hb[14];
+      dHa = Hb[21] * Iu.x + Hb[28] * Iu.y + Hb[35] * Iu.z;
     }
     const double gM = (dH + dot(wl, xy) + dHa + wa.x * Iu.x * qd.x + wa.y * Iu.y * qd.y + wa.z * Iu.z * qd.z) / dt2;
     D.gPos[gb] = gX;
@@ -889,15 +942,15 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
   const int wpt = w * D.maxPts;
   const int np = v.p1 - v.p0;
   const double dt = D.dt;
-  if (threadIdx.x < v.nb) {  // the stored step's rotations prepared for qsub
-    const int gb = v.b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < v.nb; bi += blockDim.x) {  // the stored step's rotations prepared for qsub
+    const int gb = v.b0 + bi;
     D.irotI[gb] = qinv(D.irot[gb]);
     if (D.dynamic[gb]) D.yrotI[gb] = qinv(D.yrot[gb]);
   }
   buildIncidence(D, v);
   // velocities: v' = (x - x0)/dt, w' = qsub(q, q0)/dt, prevVz' = v_old.z
-  if (threadIdx.x < v.nb) {
-    int gb = v.b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < v.nb; bi += blockDim.x) {
+    int gb = v.b0 + bi;
     D3 gv = D.gVel[gb], gw = D.gAng[gb];
     double gz = D.gPvz[gb];
     D.gIpos[gb] = D3{0, 0, 0};
@@ -961,8 +1014,8 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
   }
   __syncthreads();
   // bodies: the warm-start guess and the inertial targets (solver.ts:273-295)
-  if (threadIdx.x < v.nb) {
-    int gb = v.b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < v.nb; bi += blockDim.x) {
+    int gb = v.b0 + bi;
     if (D.dynamic[gb]) {
       const size_t o = slot * D.nb + gb;
       const D3 u = D.sgVel[o], om = D.sgAng[o];
@@ -997,12 +1050,14 @@ __device__ void stepBackward(const AdjDev& D0, int s, int w, size_t slot) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS, ADJ_BLOCKS_PER_SM) k_adj_backward(const AdjDev D) {
+// The reverse sweep's incidence cotangents hold more live state than 128 registers: 4 worlds an SM
+// at up to 255 registers beat 8 at 128 with spills
+__global__ void __launch_bounds__(ADJ_BLOCK, 4) k_adj_backward(const AdjDev D) {
   const int w = blockIdx.x;
   const int b0 = D.bodyFirst[w], nb = D.bodyFirst[w + 1] - b0;
   const int wpt = w * D.maxPts;
-  if (threadIdx.x < nb) {
-    int gb = b0 + threadIdx.x;
+  for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {
+    int gb = b0 + bi;
     D.gVel[gb] = D.gAng[gb] = D3{0, 0, 0};
     D.gPvz[gb] = 0.0;
     D.gMass[gb] = D.gMu[gb] = 0.0;
@@ -1021,8 +1076,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_BLOCKS_PER_SM) k_adj_backward
     }
     if (sg == segments - 1) {
       worldLoss(D, w);
-      if (threadIdx.x < nb) {  // the loss's cotangent: 2 (pose - target)
-        int gb = b0 + threadIdx.x;
+      for (int bi = threadIdx.x; bi < nb; bi += blockDim.x) {  // the loss's cotangent: 2 (pose - target)
+        int gb = b0 + bi;
         const double* t = D.target + 7 * gb;
         D3 x = D.pos[gb];
         D4 q = D.rot[gb];
@@ -1120,9 +1175,11 @@ bool adjAllocWork(avbd_adjoint* a) {
        aalloc(a, &D.stC0, CK * WP);
   double* loss = nullptr;
   double* fin = nullptr;
-  ok = ok && aalloc(a, &loss, W) && aalloc(a, &fin, 7 * size_t(nb));
+  double* fw = nullptr;
+  ok = ok && aalloc(a, &loss, W) && aalloc(a, &fin, 7 * size_t(nb)) && aalloc(a, &fw, size_t(W) * ADJ_GROUP * 72);
   D.loss = loss;
   D.finalPose = fin;
+  D.floorWork = fw;
   return ok;
 }
 
@@ -1142,7 +1199,7 @@ int avbd_adjoint_create(const avbd_adjoint_desc* desc, avbd_adjoint** out) {
     return AVBD_ERR_INVALID;
   const uint32_t nb = desc->world_first_body[W];
   for (uint32_t w = 0; w < W; w++)
-    if (desc->world_first_body[w + 1] < desc->world_first_body[w] || desc->world_first_body[w + 1] - desc->world_first_body[w] > ADJ_THREADS)
+    if (desc->world_first_body[w + 1] < desc->world_first_body[w] || desc->world_first_body[w + 1] - desc->world_first_body[w] > ADJ_MAX_BODIES)
       return AVBD_ERR_CAPACITY;  // a world holds at most 128 bodies
   const uint32_t nm = desc->step_first_manifold[K * (W + 1) - 1], npts = desc->step_first_point[K * (W + 1) - 1];
   int maxPts = 1;
@@ -1249,7 +1306,7 @@ int avbd_adjoint_create_from_batch(avbd_batch* batch, uint32_t checkpoint, avbd_
   a->allocations = h.mem;  // adopted: freed with the adjoint
   const uint32_t W = h.W, nb = h.nb;
   for (uint32_t w = 0; w < W; w++)
-    if (h.worldFirst[w + 1] - h.worldFirst[w] > uint32_t(ADJ_THREADS)) {
+    if (h.worldFirst[w + 1] - h.worldFirst[w] > uint32_t(ADJ_MAX_BODIES)) {
       avbd_adjoint_destroy(a);
       return AVBD_ERR_CAPACITY;  // a world holds at most 128 bodies
     }
@@ -1416,7 +1473,7 @@ int avbd_adjoint_forward(avbd_adjoint* a, const double* params, double* loss, do
   cudaSetDevice(a->device);
   int r = adjParams(a, params);
   if (r) return r;
-  k_adj_forward<<<a->W, ADJ_THREADS, ADJ_SMEM_FORWARD>>>(a->d);
+  k_adj_forward<<<a->W, ADJ_BLOCK, ADJ_SMEM_FORWARD>>>(a->d);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("replay launch: ") + cudaGetErrorString(e));
   e = cudaDeviceSynchronize();
@@ -1435,12 +1492,12 @@ int avbd_adjoint_backward(avbd_adjoint* a, const double* params, double* grad, d
   int r = adjParams(a, params);
   if (r) return r;
   if (!a->forwardDone) {  // the checkpoints come from a forward with these params
-    k_adj_forward<<<a->W, ADJ_THREADS, ADJ_SMEM_FORWARD>>>(a->d);
+    k_adj_forward<<<a->W, ADJ_BLOCK, ADJ_SMEM_FORWARD>>>(a->d);
     cudaError_t e0 = cudaGetLastError();
     if (e0 != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("replay launch: ") + cudaGetErrorString(e0));
   }
   a->forwardDone = false;
-  k_adj_backward<<<a->W, ADJ_THREADS, ADJ_SMEM_BACKWARD>>>(a->d);
+  k_adj_backward<<<a->W, ADJ_BLOCK, ADJ_SMEM_BACKWARD>>>(a->d);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return afail(a, AVBD_ERR_CUDA, std::string("reverse launch: ") + cudaGetErrorString(e));
   e = cudaDeviceSynchronize();
