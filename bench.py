@@ -379,8 +379,10 @@ def run_adjoint(args, R, torch) -> dict:
     iterations, through the FP64 adjoint (checkpoint every 10 steps) of the recorded FP32 batched
     rollout; the target comes from a seeded FP32 rollout with perturbed parameters. Reported: the FP32
     forward (plain and recording), the adjoint's FP64 replay and reverse sweep, their ratios, and
-    central differences (h = 1e-6) of the replay along a random direction on 32 sampled worlds. A world
-    counts as non-smooth when its recorded contact structure differs between the +h and -h rollouts."""
+    central differences (h = 1e-6) of the replay along a random direction on 32 sampled worlds, every
+    sampled world counted (the replay keeps the recorded contact structure, so the +h and -h rollouts
+    differ only where a friction cone or a penalty clamp switches branch, which the difference quotient
+    straddles)."""
     import numpy as np
     import avbd_b200
     from avbd_b200.scenes import tumbling_world

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define AVBD_ABI_VERSION 1
+#define AVBD_ABI_VERSION 2
 
 enum {
   AVBD_OK = 0,
@@ -129,6 +129,10 @@ typedef struct avbd_params {
   int32_t iterations;
   uint32_t flags; /* AVBD_FLAG_* */
   float up[3];    /* unit vector; gravity pulls along -up */
+  /* The wind on sails (GpuParams3D windSpeed, windAngle, windGust, windPressure, gpu/solver.ts:200-206,
+   * applied in warmStartBodies, wgsl-solve.ts:262-335): speed (m/s) towards wind_angle (rad from +x
+   * about z), gusts of wind_gust of the speed, wind_pressure = 1/2 rho C_d (kg/m^3); 0: no air. */
+  float wind_speed, wind_angle, wind_gust, wind_pressure;
 } avbd_params;
 
 typedef struct avbd_config {
@@ -161,12 +165,13 @@ const char* avbd_last_error(const avbd_world* world);
 /* params (GpuParams3D, gpu/solver.ts:163-231). */
 int avbd_set_params(avbd_world* world, const avbd_params* params);
 int avbd_get_params(const avbd_world* world, avbd_params* params);
-/* Defaults of the reference's SolverParams with every GPU-only rule off and up = +z (the reference's
- * parity setting, avbd3d-gpu.gpu.test.ts:47-52). */
+/* Defaults of the reference's SolverParams with every GPU-only rule off, up = +z and no air (sails
+ * fall as the reference's CPU solver lets them: the reference's parity setting,
+ * avbd3d-gpu.gpu.test.ts:47-52). */
 int avbd_default_params(avbd_params* params);
 /* gpuParams3D() (gpu/solver.ts:216-230), what a World runs with: the reference's SolverParams, every
  * GPU-only rule on (matchNearest, faceBias, reuseContacts, startAtRest, massPenalty), contact margin
- * 0.01 and up = +y. */
+ * 0.01, up = +y, calm air (speed 0, gusts 0.4, pressure 0.72). */
 int avbd_world_params(avbd_params* params);
 
 /* addBodies (gpu/solver.ts:1469-1481): appends; *first = index of the first. */

@@ -246,7 +246,7 @@ void solve6(const M3<T>& aLin, const M3<T>& aAng, const M3<T>& aCross, const V3<
 // ---------------------------------------------------------------------------------------------
 const double PENALTY_MIN = 1.0, PENALTY_MAX = 1e10, COLLISION_MARGIN = 0.01, STICK_THRESH = 1e-5;
 const uint32_t STICK_BIT = 0x80000000u, SPHERE_FEATURE = 3u << 24;
-const int SHAPE_BOX = 0, SHAPE_SPHERE = 1, SHAPE_HULL = 3;  // layout.ts:143-151 (a hull: SHAPE_HULL + header offset)
+const int SHAPE_BOX = 0, SHAPE_SPHERE = 1, SHAPE_SAIL = 2, SHAPE_HULL = 3;  // layout.ts:143-151 (a hull: SHAPE_HULL + header offset)
 const int MAX_COLORS = 64;
 const uint32_t NO_COLOR = 255, PENDING = 256;
 const double PIVOT_FLOOR = 1e-5;
@@ -1465,6 +1465,9 @@ template <class T> struct Solver {
   int iterations = 10;
   // GPU-mode parameters (gpu/solver.ts:174-231; parity runs every flag off)
   uint32_t flags = 0;
+  // the wind on sails (gpu/solver.ts:200-206, packed as f[32..36] at :1994-1998): velocity x, y, gust
+  // fraction, pressure coefficient (0: no air, the CPU solver's world)
+  T windX = 0, windY = 0, windGust = T(0.4), windPressure = 0;
   T contactMargin = T(COLLISION_MARGIN);
   bool gpuMode = false;
   std::vector<uint32_t> hulls;  // hull buffer (wgsl-hull.ts layout)
@@ -1521,6 +1524,31 @@ template <class T> struct Solver {
     }
     forces = std::move(kept);
   }
+  // The wind's acceleration of a sail (wgsl-solve.ts:262-292): pressure drag along the plate's normal,
+  // linearised implicitly in its normal speed, and skin friction along it; gusts as travelling sines
+  // in the wind's frame. t = step x dt; x, q, v: the step-start pose and the (damped) velocity.
+  V3<T> windAccel(const Body<T>& b, T t) const {
+    const V3<T> w{windX, windY, 0};
+    const T speed = length(w);
+    const V3<T> d = speed > T(1e-6) ? scale3(w, T(1) / speed) : V3<T>{1, 0, 0};
+    const V3<T> side{-d[1], d[0], 0};
+    const V3<T>& x = b.pos;
+    const T a = dot(x, d), c = dot(x, side);
+    const T along = T(0.5) * std::sin(T(1.1) * t - T(0.35) * a + T(0.2) * c) + T(0.3) * std::sin(T(2.9) * t - T(0.8) * a + T(0.6) * x[2]) +
+                    T(0.2) * std::sin(T(6.1) * t - T(1.7) * a + T(1.3) * x[2] + T(0.9) * c);
+    const T across = T(0.6) * std::sin(T(1.7) * t - T(0.6) * a + T(0.4) * x[2]) + T(0.4) * std::sin(T(4.3) * t - T(1.3) * a - T(0.7) * x[2]);
+    const T lift = std::sin(T(2.3) * t - T(0.9) * a + T(1.1) * c);
+    const T g = windGust;
+    V3<T> u = scale3(w, T(1) + g * along);
+    u = addScaled3(u, side, T(0.25) * across * g * speed);
+    u[2] += T(0.1) * lift * g * speed;
+    u = sub3(u, b.vel);
+    const V3<T> n = rotate(b.rot, V3<T>{0, 0, 1});
+    const T k = windPressure * b.size[0] * b.size[1] / b.mass;  // 1/2 rho C_d A / m
+    const T un = dot(u, n);
+    const V3<T> ut = addScaled3(u, n, -un);
+    return addScaled3(scale3(n, k * un * std::fabs(un) / (T(1) + T(2) * dt * k * std::fabs(un))), ut, T(0.06) * k * length(ut));
+  }
   void warmStartBodies(bool gpu) {  // solver.ts:273-295; GPU rules wgsl-solve.ts:294-335 (up = z)
     int n = int(bodies.size());
     for (int b = n - 1; b >= 0; b--) {
@@ -1535,6 +1563,8 @@ template <class T> struct Solver {
       }
       body.inertialPos = addScaled3(body.pos, body.vel, dt);
       if (dynamic) body.inertialPos[2] += g * (dt * dt);
+      if (gpu && dynamic && body.shape == SHAPE_SAIL && windPressure != 0)  // wgsl-solve.ts:310-311
+        body.inertialPos = addScaled3(body.inertialPos, windAccel(body, T(stepCounter) * dt), dt * dt);
       body.inertialRot = qaddv(body.rot, scale3(body.angVel, dt));
       V3<T> accel = div3(sub3(body.vel, body.prevVel), dt);
       T accelExt = accel[2] * signv(g);
@@ -2198,6 +2228,15 @@ void orc_set_params(void* h, const double* p, unsigned flags) {
     s.dt = T(p[0]); s.gravity = T(p[1]); s.iterations = int(p[2]); s.alpha = T(p[3]);
     s.betaLin = T(p[4]); s.betaAng = T(p[5]); s.gamma = T(p[6]); s.contactMargin = T(p[7]);
     s.flags = flags;
+    return 0;
+  });
+}
+
+// the wind on sails: velocity x, y (m/s), gust fraction, pressure coefficient 1/2 rho C_d
+void orc_set_wind(void* h, const double* w) {
+  with(h, [&](auto& s) {
+    using T = std::decay_t<decltype(s.dt)>;
+    s.windX = T(w[0]); s.windY = T(w[1]); s.windGust = T(w[2]); s.windPressure = T(w[3]);
     return 0;
   });
 }

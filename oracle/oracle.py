@@ -35,6 +35,7 @@ def lib():
         L.orc_create.argtypes = [I]
         L.orc_destroy.argtypes = [P]
         L.orc_set_params.argtypes = [P, D, U]
+        L.orc_set_wind.argtypes = [P, D]
         L.orc_add_body.argtypes = [P, D]
         L.orc_body_count.argtypes = [P]
         L.orc_get_body.argtypes = [P, I, D]
@@ -196,6 +197,16 @@ class Oracle:
     def set_params(self, p, flags: int = 0):
         arr = np.array([p.dt, p.gravity, p.iterations, p.alpha, p.beta_lin, p.beta_ang, p.gamma, p.contact_margin], dtype=np.float64)
         self.L.orc_set_params(self.h, _dp(arr), flags)
+        self.set_wind(getattr(p, 'wind_speed', 0.0), getattr(p, 'wind_angle', 0.0), getattr(p, 'wind_gust', 0.4), getattr(p, 'wind_pressure', 0.0))
+
+    def set_wind(self, speed: float, angle: float, gust: float = 0.4, pressure: float = 0.72):
+        """The wind on sails (GPU mode): speed (m/s) towards angle (rad from +x about z), gusts, pressure
+        coefficient 1/2 rho C_d; its velocity in f32 as the device's parameters hold it
+        (gpu/solver.ts:1994-1998)."""
+        wx = float(np.float32(speed * np.cos(angle)))
+        wy = float(np.float32(speed * np.sin(angle)))
+        arr = np.array([wx, wy, float(np.float32(gust)), float(np.float32(pressure))], dtype=np.float64)
+        self.L.orc_set_wind(self.h, _dp(arr))
 
     def set_body_aux(self, i: int, scale: float, linear: float = 0.0, angular: float = 0.0):
         """GPU-mode aux record of body i: gravity scale and damping rates (1/s)."""

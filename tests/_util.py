@@ -111,6 +111,8 @@ def params_struct(p, flags: int = 0):
     s = _abi.Params(dt=p.dt, gravity=p.gravity, alpha=p.alpha, beta_lin=p.beta_lin, beta_ang=p.beta_ang, gamma=p.gamma,
                     contact_margin=p.contact_margin, iterations=p.iterations, flags=flags)
     s.up[0], s.up[1], s.up[2] = 0.0, 0.0, 1.0
+    s.wind_speed, s.wind_angle = getattr(p, 'wind_speed', 0.0), getattr(p, 'wind_angle', 0.0)
+    s.wind_gust, s.wind_pressure = getattr(p, 'wind_gust', 0.4), getattr(p, 'wind_pressure', 0.0)
     return s
 
 

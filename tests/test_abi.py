@@ -33,7 +33,7 @@ def test_record_layouts_match_the_reference():
     assert _abi.JOINT_DTYPE.itemsize == 40 * 4
     assert _abi.MANIFOLD_DTYPE.itemsize == 8 * 4
     assert _abi.CONTACT_DTYPE.itemsize == 16 * 4
-    assert ctypes.sizeof(_abi.Params) == 12 * 4
+    assert ctypes.sizeof(_abi.Params) == 16 * 4
 
 
 def test_defaults_and_invalid_arguments_without_a_device():
@@ -41,7 +41,8 @@ def test_defaults_and_invalid_arguments_without_a_device():
     p = _abi.Params()
     assert lib.avbd_default_params(ctypes.byref(p)) == 0
     assert abs(p.dt - 1 / 60) < 1e-7 and p.iterations == 10 and p.gravity == -10.0 and tuple(p.up) == (0.0, 0.0, 1.0)
-    assert lib.avbd_abi_version() == 1
+    assert p.wind_pressure == 0.0 and p.wind_speed == 0.0  # no air: sails fall as the CPU solver's boxes
+    assert lib.avbd_abi_version() == 2
     assert lib.avbd_world_create(None, None) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_world_destroy(None) == 0
     assert lib.avbd_step(None, 1) == _abi.AVBD_ERR_INVALID
@@ -67,6 +68,8 @@ def test_world_params_are_the_reference_production_defaults():
     assert lib.avbd_world_params(ctypes.byref(p)) == 0
     rules = _abi.FLAG_MATCH_NEAREST | _abi.FLAG_FACE_BIAS | _abi.FLAG_REUSE_CONTACTS | _abi.FLAG_START_AT_REST | _abi.FLAG_MASS_PENALTY
     assert p.flags == rules and tuple(p.up) == (0.0, 1.0, 0.0) and abs(p.contact_margin - 0.01) < 1e-9 and p.iterations == 10
+    # calm air (gpu/solver.ts:226-229): no wind, gusts 0.4 of it, pressure coefficient 0.72
+    assert (p.wind_speed, p.wind_angle) == (0.0, 0.0) and abs(p.wind_gust - 0.4) < 1e-7 and abs(p.wind_pressure - 0.72) < 1e-7
 
 
 def test_query_record_layouts():

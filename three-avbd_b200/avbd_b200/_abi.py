@@ -66,7 +66,8 @@ assert PUSH_DTYPE.itemsize == 40 and EVENT_DTYPE.itemsize == 48 and RAY_DTYPE.it
 class Params(ctypes.Structure):
     _fields_ = [('dt', ctypes.c_float), ('gravity', ctypes.c_float), ('alpha', ctypes.c_float), ('beta_lin', ctypes.c_float),
                 ('beta_ang', ctypes.c_float), ('gamma', ctypes.c_float), ('contact_margin', ctypes.c_float), ('iterations', ctypes.c_int32),
-                ('flags', ctypes.c_uint32), ('up', ctypes.c_float * 3)]
+                ('flags', ctypes.c_uint32), ('up', ctypes.c_float * 3),
+                ('wind_speed', ctypes.c_float), ('wind_angle', ctypes.c_float), ('wind_gust', ctypes.c_float), ('wind_pressure', ctypes.c_float)]
 
 
 class Config(ctypes.Structure):

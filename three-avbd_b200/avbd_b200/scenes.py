@@ -18,6 +18,7 @@ import numpy as np
 
 SHAPE_BOX = 0
 SHAPE_SPHERE = 1
+SHAPE_SAIL = 2
 SHAPE_HULL = 3
 
 INF = math.inf
@@ -105,6 +106,11 @@ class Params:
     start_at_rest: bool = False
     mass_penalty: bool = False
     reuse_contacts: bool = False
+    # the wind on sails (gpu/solver.ts:200-206): 0 pressure is still no air, as the CPU solver has none
+    wind_speed: float = 0.0
+    wind_angle: float = 0.0
+    wind_gust: float = 0.4
+    wind_pressure: float = 0.0
 
 
 class Scene:
@@ -127,6 +133,14 @@ class Scene:
         self.bodies.append(Body(pos=[float(p) for p in position], size=[sx, sy, sz], mass=mass, moment=moment, friction=float(friction),
                                 radius=radius, vel=list(v), prev_vel=list(v)))
         return len(self.bodies) - 1
+
+    # A sail (src/avbd3d/shapes.ts:17-25): a thin box whose local z faces catch the wind (the GPU solver's
+    # wind; the CPU solver has no air and treats it as a box)
+    def sail(self, size, density, friction, position, rotation=(0.0, 0.0, 0.0, 1.0), velocity=(0.0, 0.0, 0.0)) -> int:
+        i = self.box(size, density, friction, position, velocity)
+        self.bodies[i].rot = [float(x) for x in rotation]
+        self.bodies[i].shape = SHAPE_SAIL
+        return i
 
     # A solid sphere (src/avbd3d/shapes.ts:83-91): a cubic box of side 2r with a sphere's mass properties
     def sphere(self, r, density, friction, position, velocity=(0.0, 0.0, 0.0)) -> int:

@@ -124,6 +124,8 @@ def to_params(sp) -> Params:
     p = Params(dt=sp.dt, gravity=sp.gravity, alpha=sp.alpha, beta_lin=sp.beta_lin, beta_ang=sp.beta_ang, gamma=sp.gamma,
                contact_margin=sp.contact_margin, iterations=sp.iterations, flags=flags)
     p.up[0], p.up[1], p.up[2] = 0.0, 0.0, 1.0
+    p.wind_speed, p.wind_angle = getattr(sp, 'wind_speed', 0.0), getattr(sp, 'wind_angle', 0.0)
+    p.wind_gust, p.wind_pressure = getattr(sp, 'wind_gust', 0.4), getattr(sp, 'wind_pressure', 0.0)
     return p
 
 

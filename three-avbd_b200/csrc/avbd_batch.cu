@@ -275,6 +275,7 @@ BatchLaunch makeLaunch(avbd_batch* b) {
   p.upx = a.up[0];
   p.upy = a.up[1];
   p.upz = a.up[2];
+  setWind(p, a);
   p.step = b->stepCount;
   p.colorCap = MAX_COLORS;
   p.rowsPerLane = b->rowsPerLane;
@@ -521,6 +522,9 @@ const char* avbd_batch_last_error(const avbd_batch* b) { return b ? b->error.c_s
 int avbd_batch_set_params(avbd_batch* b, const avbd_params* p) {
   if (!b || !p) return AVBD_ERR_INVALID;
   if (!(p->dt > 0.0f) || p->iterations < 0 || !std::isfinite(p->gravity)) return bfail(b, AVBD_ERR_INVALID, "dt must be positive, iterations non-negative");
+  if (!std::isfinite(p->wind_speed) || !std::isfinite(p->wind_angle) || !std::isfinite(p->wind_gust) || !(p->wind_pressure >= 0.0f) ||
+      !std::isfinite(p->wind_pressure))
+    return bfail(b, AVBD_ERR_INVALID, "the wind's values must be finite, wind_pressure >= 0");
   b->params = *p;
   b->configGen++;
   return AVBD_OK;
@@ -880,6 +884,9 @@ int avbd_batch_record_start(avbd_batch* b, uint32_t steps, uint32_t points_per_b
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
   std::vector<avbd_body> bodies(b->n);
   bodiesOut(b, 0, bodies.data(), b->n);
+  if (P.wind_pressure != 0.0f)
+    for (const avbd_body& r : bodies)
+      if (r.shape == 2.0f && r.mass > 0.0f) return bfail(b, AVBD_ERR_INVALID, "the adjoint does not differentiate the wind: a dynamic sail with wind_pressure > 0");
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
   for (auto& x : bodies)
     if (x.shape != float(AVBD_SHAPE_BOX)) return bfail(b, AVBD_ERR_INVALID, "the adjoint differentiates boxes only");

@@ -24,6 +24,7 @@ constexpr uint32_t NO_COLOR = 255u, PENDING = 256u;
 constexpr int MAX_COLORS = 64;
 constexpr int MAX_CONTACTS = 8;
 constexpr float SHAPE_SPHERE_F = 1.0f;
+constexpr float SHAPE_SAIL_F = 2.0f;  // a box that catches the wind on its local z faces (layout.ts:145)
 constexpr uint32_t T_NONE = 0, T_JOINT = 1, T_SPRING = 2;
 constexpr uint32_t FLAG_MATCH_NEAREST = 1, FLAG_FACE_BIAS = 2, FLAG_REUSE_CONTACTS = 4, FLAG_START_AT_REST = 8, FLAG_MASS_PENALTY = 16;
 constexpr float REUSE_LIN_TOL = 0.002f, REUSE_ANG_TOL = 0.002f;  // gpu/layout.ts:174-175
@@ -60,6 +61,8 @@ struct StepParams {
   uint32_t flags;
   int iterations;
   float upx, upy, upz;
+  // the wind on sails: velocity (x, y; m/s), gust fraction, pressure coefficient 1/2 rho C_d
+  float windX, windY, windGust, windPressure;
   // broadphase
   float cellSize, largeThreshold;
   uint32_t tableMask, nLarge, nNoCollide, anyDynamicLarge;

@@ -217,6 +217,7 @@ StepParams makeParams(avbd_world* w) {
   p.upx = a.up[0];
   p.upy = a.up[1];
   p.upz = a.up[2];
+  setWind(p, a);
   p.cellSize = w->cellSize;
   p.largeThreshold = w->threshold;
   p.tableMask = w->tableSize - 1;
@@ -379,6 +380,10 @@ int avbd_default_params(avbd_params* p) {
   p->up[0] = 0.0f;
   p->up[1] = 0.0f;
   p->up[2] = 1.0f;
+  p->wind_speed = 0.0f;
+  p->wind_angle = 0.0f;
+  p->wind_gust = 0.4f;
+  p->wind_pressure = 0.0f;
   return AVBD_OK;
 }
 
@@ -389,6 +394,7 @@ int avbd_world_params(avbd_params* p) {
   p->up[0] = 0.0f;
   p->up[1] = 1.0f;
   p->up[2] = 0.0f;
+  p->wind_pressure = 0.72f;  // gpu/solver.ts:226-229
   return AVBD_OK;
 }
 
@@ -516,8 +522,9 @@ const char* avbd_last_error(const avbd_world* w) { return w ? w->error.c_str() :
 int avbd_set_params(avbd_world* w, const avbd_params* p) {
   if (!w || !p) return AVBD_ERR_INVALID;
   if (!(p->dt > 0.0f) || !finite(p->dt) || !finite(p->gravity) || !finite(p->alpha) || !finite(p->gamma) || p->iterations < 0 ||
-      !(p->contact_margin >= 0.0f) || !finite(p->contact_margin))
-    return fail(w, AVBD_ERR_INVALID, "invalid params (dt > 0, finite values, iterations >= 0, contact_margin >= 0)");
+      !(p->contact_margin >= 0.0f) || !finite(p->contact_margin) || !finite(p->wind_speed) || !finite(p->wind_angle) || !finite(p->wind_gust) ||
+      !(p->wind_pressure >= 0.0f) || !finite(p->wind_pressure))
+    return fail(w, AVBD_ERR_INVALID, "invalid params (dt > 0, finite values, iterations >= 0, contact_margin >= 0, wind_pressure >= 0)");
   w->params = *p;
   w->configGen++;
   return AVBD_OK;

@@ -1,5 +1,6 @@
 // Host-side state shared by the single-world and batched entry points (avbd_host.cu, avbd_batch.cu).
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <map>
 #include <set>
@@ -90,6 +91,14 @@ struct avbd_world {
 namespace avbd {
 // Uploads the world's large-body list and sorted no-collide triples when they changed
 int uploadStatics(avbd_world* w);
+
+// The wind's step parameters: its velocity from speed and angle, as gpu/solver.ts:1994-1998 packs it
+inline void setWind(StepParams& p, const avbd_params& a) {
+  p.windX = float(double(a.wind_speed) * std::cos(double(a.wind_angle)));
+  p.windY = float(double(a.wind_speed) * std::sin(double(a.wind_angle)));
+  p.windGust = a.wind_gust;
+  p.windPressure = a.wind_pressure;
+}
 
 // Copies between host and device, ordered on stream s and complete when they return. A plain
 // cudaMemcpy runs on the legacy default stream, which the worlds' non-blocking streams do not wait

@@ -772,6 +772,34 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
   return true;
 }
 
+// --- the wind on sails (wgsl-solve.ts:262-292) ------------------------------------------------------------------
+// A sail is a thin plate: pressure drag 1/2 rho C_d A (n.u)|n.u| along its normal n, u the wind
+// relative to the plate, and skin friction along the plate at 6 % of that coefficient; the pressure
+// term is linearised implicitly in the plate's normal speed (divided by 1 + 2 dt k |n.u|). The wind
+// gusts in time and across space: travelling sines in the wind's frame (a downwind, c across, and
+// height z), with the reference's frequencies and weights, as a second external acceleration on the
+// inertial target. t = step x dt, x the step-start position, v the velocity after damping. Out of
+// line: inlined, it changed how the warm start's other sums contract into FMAs in one of the world and
+// batch kernels, whose results must agree bit for bit.
+__device__ __noinline__ float3 windAccel(const StepParams& p, float t, float3 x, float4 q, float3 v, float4 size) {
+  const float3 wv = make_float3(p.windX, p.windY, 0.0f);
+  const float speed = len3(wv);
+  const float3 d = speed > 1e-6f ? wv * (1.0f / speed) : make_float3(1.0f, 0.0f, 0.0f);
+  const float3 side = make_float3(-d.y, d.x, 0.0f);
+  const float a = dot3(x, d), c = dot3(x, side);
+  const float along = 0.5f * sinf(1.1f * t - 0.35f * a + 0.2f * c) + 0.3f * sinf(2.9f * t - 0.8f * a + 0.6f * x.z) +
+                      0.2f * sinf(6.1f * t - 1.7f * a + 1.3f * x.z + 0.9f * c);
+  const float across = 0.6f * sinf(1.7f * t - 0.6f * a + 0.4f * x.z) + 0.4f * sinf(4.3f * t - 1.3f * a - 0.7f * x.z);
+  const float lift = sinf(2.3f * t - 0.9f * a + 1.1f * c);
+  const float g = p.windGust;
+  const float3 u = wv * (1.0f + g * along) + (side * (0.25f * across) + make_float3(0.0f, 0.0f, 0.1f * lift)) * (g * speed) - v;
+  const float3 n = qrotate(q, make_float3(0.0f, 0.0f, 1.0f));
+  const float k = p.windPressure * size.x * size.y / size.w;  // 1/2 rho C_d A / m
+  const float un = dot3(u, n);
+  const float3 ut = u - n * un;
+  return n * (k * un * fabsf(un) / (1.0f + 2.0f * p.dt * k * fabsf(un))) + ut * (0.06f * k * len3(ut));
+}
+
 // --- the kernel -----------------------------------------------------------------------------------------------
 template <class Team>
 __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) {
@@ -1082,6 +1110,7 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   GSYNC
   const float dt = p.dt, gWorld = p.gravity;
   const float3 up = make_float3(p.upx, p.upy, p.upz);
+  const uint32_t stepWord = ldv(&ctr[C_STEP]);  // steps since the world was made, from 1
   for (uint32_t i = tid; i < n; i += T) {
     if constexpr (Team::kDataflow) {
       w.done[i] = 0u;
@@ -1090,6 +1119,7 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     if (!enabledBody(w, i)) continue;
     float4 pos = w.pos[i], rot = w.rot[i], vel = w.vel[i];
     float3 av = f3(w.avel[i]);
+    const float av_shape = w.avel[i].w;
     bool dynamic = w.size[i].w > 0.0f;
     // the body's aux record (wgsl-solve.ts:9-20, 297-305): gravity scale, and damping of the
     // incoming velocities, stored so the next step's up-velocity history is this step's start
@@ -1105,6 +1135,9 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     // y - x- and y's rotation relative to q- (the solve's inertial terms), and y itself for readers
     float3 yl = f3(vel) * dt;
     if (dynamic) yl = yl + up * (g * (dt * dt));
+    // the wind's push on sails, a second external force (wgsl-solve.ts:310-311)
+    if (dynamic && p.windPressure != 0.0f && av_shape == SHAPE_SAIL_F)
+      yl = yl + windAccel(p, float(stepWord) * dt, f3(pos), rot, f3(vel), w.size[i]) * (dt * dt);
     const float4 ry = qadd(make_float4(0.0f, 0.0f, 0.0f, 1.0f), av * dt);
     const float3 y = f3(pos) + yl;
     w.ypos[i] = make_float4(y.x, y.y, y.z, w.ypos[i].w);
