@@ -450,6 +450,23 @@ typedef struct avbd_ray_hit {
 } avbd_ray_hit;
 int avbd_raycast(avbd_world* world, const avbd_ray* rays, uint32_t n, const uint32_t* ignore, uint32_t n_ignore, uint32_t mask, avbd_ray_hit* hits);
 
+/* ---- Pose capture: the frames of the pose cache (src/bake/pose-cache.ts) -------------------------
+ * A recorder on the device: up to max_frames frames of the listed body slots, a frame being the
+ * world's step word (steps since the world was made) and 7 f32 per slot, position then rotation
+ * x y z w (the cache's slot layout, POSE_FLOATS), or +0 for a disabled slot. A frame is gathered by
+ * one kernel on the world's stream when the stream reaches it, so capturing every k-th step costs no
+ * host synchronisation; the host side writes the cache format (avbd_b200.pose_cache). */
+typedef struct avbd_pose_capture avbd_pose_capture;
+int avbd_pose_capture_create(avbd_world* world, const uint32_t* slots, uint32_t n, uint32_t max_frames, avbd_pose_capture** out);
+/* One frame of the poses the world holds when its stream gets here; past max_frames it is dropped
+ * and counted. */
+int avbd_pose_capture_frame(avbd_pose_capture* capture);
+/* Waits for the world's stream; *frames = frames held, *dropped = frames refused for room; copies
+ * min(frames, cap) frames: steps[cap], poses[cap x n x 7]. */
+int avbd_pose_capture_read(avbd_pose_capture* capture, uint32_t* steps, float* poses, uint32_t cap, uint32_t* frames, uint32_t* dropped);
+int avbd_pose_capture_reset(avbd_pose_capture* capture);
+int avbd_pose_capture_destroy(avbd_pose_capture* capture);
+
 /* ---- Adjoint --------------------------------------------------------------------------------------
  * No counterpart in the reference (it has no differentiation). Gradients of a pose loss
  * L = sum over dynamic bodies of |x_T - x*|^2 + |q_T - q*|^2 after a recorded rollout, with respect

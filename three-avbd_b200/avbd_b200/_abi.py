@@ -174,6 +174,11 @@ SIGNATURES = {
     'avbd_contact_watch_run': ([P, U, ctypes.c_float], I),
     'avbd_contact_watch_read': ([P, VP, U, PU, PU, PU], I),
     'avbd_raycast': ([P, VP, U, PU, U, U, VP], I),
+    'avbd_pose_capture_create': ([P, PU, U, U, ctypes.POINTER(P)], I),
+    'avbd_pose_capture_frame': ([P], I),
+    'avbd_pose_capture_read': ([P, PU, ctypes.POINTER(ctypes.c_float), U, PU, PU], I),
+    'avbd_pose_capture_reset': ([P], I),
+    'avbd_pose_capture_destroy': ([P], I),
     'avbd_read_reuse_state': ([P, ctypes.POINTER(ctypes.c_float), U, PU, PU, U, PU], I),
     'avbd_synchronize': ([P], I),
     'avbd_read_bodies': ([P, VP, U, PU], I),

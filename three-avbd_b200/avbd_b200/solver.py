@@ -401,6 +401,10 @@ class CudaSolver3D:
         """A ContactWatch (src/lib/contacts.ts) on this world's contacts."""
         return ContactWatch(self, pairs, capacity)
 
+    def pose_capture(self, max_frames: int, slots=None) -> 'PoseCapture':
+        """A device recorder of pose cache frames (src/bake/pose-cache.ts) of `slots` (default: every body)."""
+        return PoseCapture(self, max_frames, slots)
+
     def raycast(self, origins, directions, max_distance=None, ignore=(), mask: int = 0xFFFFFFFF) -> np.ndarray:
         """Raycaster.cast (src/lib/raycast.ts:170-251): the nearest hit of each ray (HIT_DTYPE; body -1: none)."""
         o = np.asarray(origins, dtype=np.float32).reshape(-1, 3)
@@ -532,6 +536,65 @@ class CudaSolver3D:
         out = np.zeros(n.value, dtype=np.uint32)
         self._check(self.lib.avbd_read_colors(self.handle, uptr(out), n.value, ctypes.byref(n)))
         return out
+
+
+class PoseCapture:
+    """Pose cache frames (src/bake/pose-cache.ts) gathered on the device (avbd_pose_capture_*): frame()
+    after a step enqueues one gather of the slots' positions and rotations with the world's step word,
+    without synchronising; read() returns them; to_pose_cache() makes the cache the codec writes."""
+
+    def __init__(self, world: 'CudaSolver3D', max_frames: int, slots=None):
+        self.world = world
+        self.lib = world.lib
+        n = world.body_count if slots is None else len(slots)
+        self.slots = np.arange(n, dtype=np.uint32) if slots is None else np.ascontiguousarray(slots, dtype=np.uint32)
+        self.max_frames = int(max_frames)
+        h = ctypes.c_void_p()
+        world._check(self.lib.avbd_pose_capture_create(world.handle, uptr(self.slots), len(self.slots), self.max_frames, ctypes.byref(h)))
+        self.handle = h
+
+    def frame(self):
+        self.world._check(self.lib.avbd_pose_capture_frame(self.handle))
+
+    def reset(self):
+        self.world._check(self.lib.avbd_pose_capture_reset(self.handle))
+
+    def read(self):
+        """(steps uint32 [frames], poses float32 [frames, slots, 7], dropped)."""
+        steps = np.zeros(self.max_frames, np.uint32)
+        poses = np.zeros((self.max_frames, len(self.slots), 7), np.float32)
+        n, dropped = ctypes.c_uint32(), ctypes.c_uint32()
+        self.world._check(self.lib.avbd_pose_capture_read(self.handle, uptr(steps), poses.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                          self.max_frames, ctypes.byref(n), ctypes.byref(dropped)))
+        return steps[:n.value], poses[:n.value], dropped.value
+
+    def to_pose_cache(self, cache_id: int, ids=None, termination: str = 'complete', provenance=None):
+        """The frames as a pose_cache.PoseCache: a body's id (default slot + 1), its shape (boxes and
+        spheres; the cache holds nothing else), full size and fixed flag from its record, and its lifetime
+        from the frames where its slot is not +0 (one run of frames per id)."""
+        from . import pose_cache as pc
+        steps, poses, _ = self.read()
+        if len(steps) == 0:
+            raise pc.PoseCacheError('data', 'a cache needs at least one frame')
+        recs = self.world.read_bodies()[self.slots]
+        ids = (self.slots.astype(np.int64) + 1) if ids is None else np.asarray(ids, dtype=np.int64)
+        bodies = []
+        for k, r in enumerate(recs):
+            shape = int(r['shape'])
+            if shape not in (0, 1):
+                raise pc.PoseCacheError('data', f'slot {int(self.slots[k])}: the pose cache holds boxes and spheres only')
+            alive = np.flatnonzero(np.any(poses[:, k].view(np.uint32) != 0, axis=1))
+            if len(alive) == 0:
+                raise pc.PoseCacheError('data', f'slot {int(self.slots[k])} is alive in no frame')
+            first, end = int(alive[0]), int(alive[-1]) + 1
+            size = [float(x) for x in r['size']]
+            bodies.append(pc.PoseCacheBody(int(ids[k]), 'box' if shape == 0 else 'sphere', size, bool(r['mass'] <= 0), first, end))
+        return pc.PoseCache(int(cache_id), float(self.world.params.dt), bodies, steps.copy(), poses.copy(), termination, provenance)
+
+    def destroy(self):
+        if getattr(self, 'handle', None):
+            self.lib.avbd_pose_capture_destroy(self.handle)
+            self.handle = None
 
 
 class ContactWatch:

@@ -27,6 +27,7 @@ UNITS = {
     'avbd_adjoint.cu': [],
     'avbd_record.cu': [],
     'avbd_query.cu': [],
+    'avbd_capture.cu': [],
 }
 
 
