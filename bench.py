@@ -47,10 +47,10 @@ NOMINAL_HBM_GBS = 7700.0  # HGX B200 HBM3e, for context beside the measured copy
 L2_FLUSH_BYTES = 256 << 20
 
 
-def workload_config(n_bodies: int, steps: int, roll: int = ROLL) -> dict:
+def workload_config(n_bodies: int, steps: int, roll: int = ROLL, spacing: float = PILE_SPACING) -> dict:
     return {
         'workload': f'drop pile: {n_bodies} bodies (70% boxes half-extents U[0.25,0.75], 30% spheres r U[0.2,0.6], density U[0.5,2], '
-                    f'friction U[0.3,0.8]) on a jittered 10-layer lattice (spacing {PILE_SPACING}), random orientations, speed U[0,1]; '
+                    f'friction U[0.3,0.8]) on a jittered 10-layer lattice (spacing {spacing}), random orientations, speed U[0,1]; '
                     f'static ground box; dt 1/60, 10 iterations, g -9.81; rolled {roll} steps untimed, timed steps {roll + 1}..{roll + steps}',
         'bodies': n_bodies, 'iterations': 10, 'seed': 1, 'window': [roll + 1, roll + steps],
         'l2': '256 MiB clear between timed steps, inside the timed region',
@@ -130,13 +130,13 @@ def _oracle():
     return oracle
 
 
-def cpu_reference(n_bodies: int, roll: int, steps: int, threads: int) -> dict:
+def cpu_reference(n_bodies: int, roll: int, steps: int, threads: int, spacing: float = PILE_SPACING) -> dict:
     """The reference's algorithm (the oracle port, GPU-mode rules, double) on `threads` host threads:
     the pile rolled `roll` steps untimed, then steps roll+1 .. roll+steps timed."""
     from avbd_b200.scenes import drop_pile
     orc = _oracle()
     used = orc.set_threads(threads)
-    o = orc.Oracle(drop_pile(n_bodies, seed=1, spacing=PILE_SPACING))
+    o = orc.Oracle(drop_pile(n_bodies, seed=1, spacing=spacing))
     for _ in range(roll):
         o.step_gpu()
     t0 = time.perf_counter()
@@ -167,11 +167,11 @@ def run_reference(args, rank: int):
     if rank != 0:
         return
     steps = max(1, min(args.steps, REF_MAX_STEPS))
-    ref = cpu_reference(args.bodies, args.roll, steps, os.cpu_count() or 1)
+    ref = cpu_reference(args.bodies, args.roll, steps, os.cpu_count() or 1, args.spacing)
     line = {
         'metric': METRIC, 'value': ref['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': steps, 'warmup': args.warmup,
         'ms_per_step': 1000 * ref['seconds'] / steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
-        'data': 'synthetic', 'impl': 'reference', 'config': workload_config(args.bodies, steps, args.roll),
+        'data': 'synthetic', 'impl': 'reference', 'config': workload_config(args.bodies, steps, args.roll, args.spacing),
         'cpu_baseline': {'value': ref['value'], 'unit': UNIT, 'cores': ref['cores'], 'kind': 'port', 'sample': ref['sample']},
         'e2e': {'value': ref['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
@@ -498,6 +498,7 @@ def main():
     ap.add_argument('--impl', default='cuda', choices=['cuda', 'reference'])
     ap.add_argument('--bodies', type=int, default=PILE_BODIES)
     ap.add_argument('--roll', type=int, default=ROLL, help='untimed steps before the timed window of the pile')
+    ap.add_argument('--spacing', type=float, default=PILE_SPACING, help="the pile's lattice spacing (1.15: in contact from the first step)")
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-graphs', action='store_true', help='launch each kernel directly instead of replaying the step graph')
@@ -526,7 +527,7 @@ def main():
     R = Ranks.from_env('nccl', timeout_s=300)
     rank, world_size, local, barrier = R.rank, R.world_size, R.local, R.barrier
 
-    scene = drop_pile(args.bodies, seed=1, spacing=PILE_SPACING)
+    scene = drop_pile(args.bodies, seed=1, spacing=args.spacing)
     n_dyn = scene.dynamic_count
 
     # The timed world: rolled untimed to step ROLL (its last `warmup` steps are the warm-up). Step
@@ -638,7 +639,7 @@ def main():
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world_size, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
-            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps, max(args.roll, args.warmup)), parallelism=f'replicas x{world_size}'),
+            'data': 'synthetic', 'config': dict(workload_config(args.bodies, args.steps, max(args.roll, args.warmup), args.spacing), parallelism=f'replicas x{world_size}'),
             'roofline': {'bound': 'hbm', 'kernel': 'k_topology_solve', 'achieved': achieved, 'peak': peak, 'peak_kind': peak_kind, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic, 'alg_bytes_per_launch': bytes_alg / K,
                          'frac_of_nominal_7700': achieved / NOMINAL_HBM_GBS},

@@ -5,8 +5,8 @@
 demo scenes and the synthetic workloads; `BatchSolver3D` steps many small worlds together.
 """
 
-from . import scenes  # noqa: F401
+from . import pose_cache, scenes  # noqa: F401
 from ._abi import AvbdError, DeviceError, DeviceTimeout, StorageCapacityError, BODY_DTYPE, CONTACT_DTYPE, INFO_DTYPE, JOINT_DTYPE, MANIFOLD_DTYPE, LIB_PATH, load  # noqa: F401
-from .solver import CudaSolver3D, device_info, find_pairs_noalloc, pack_bodies, pack_force, scene_records  # noqa: F401
+from .solver import CudaSolver3D, PoseCapture, device_info, find_pairs_noalloc, pack_bodies, pack_force, scene_records  # noqa: F401
 from .batch import BatchSolver3D  # noqa: F401
 from .adjoint import Adjoint  # noqa: F401
