@@ -47,6 +47,18 @@ NOMINAL_HBM_GBS = 7700.0  # HGX B200 HBM3e, for context beside the measured copy
 L2_FLUSH_BYTES = 256 << 20
 
 
+def compact(v, digits: int = 4):
+    """Floats rounded to `digits` significant digits, recursively: the sub-results at the end of the
+    bench line stay short enough to read whole in a log's last lines."""
+    if isinstance(v, float):
+        return float(f'{v:.{digits}g}')
+    if isinstance(v, dict):
+        return {k: compact(x, digits) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [compact(x, digits) for x in v]
+    return v
+
+
 def workload_config(n_bodies: int, steps: int, roll: int = ROLL, spacing: float = PILE_SPACING) -> dict:
     return {
         'workload': f'drop pile: {n_bodies} bodies (70% boxes half-extents U[0.25,0.75], 30% spheres r U[0.2,0.6], density U[0.5,2], '
@@ -326,7 +338,8 @@ def run_batched(args, R, torch) -> dict:
         'e2e': len(job) * steps / (te / 1000.0), 'h2d_d2h_bytes_per_step': n * 160,
         'worlds': len(job), 'worlds_this_rank': len(scenes), 'dynamic_bodies': dyn, 'world_errors': errors,
         'launch': f"{tuning['collide_threads']}x{tuning['solve_blocks']}x{tuning['rows_per_lane']}",
-        'tuning_ms': {f"{c['collide_threads']}x{c['solve_blocks']}x{c['rows_per_lane']}": round(c['ms_per_step'], 3) for c in tuning['candidates']},
+        'tuning': {'candidates': len(tuning['candidates']), 'best_ms': min(c['ms_per_step'] for c in tuning['candidates']),
+                   'worst_ms': max(c['ms_per_step'] for c in tuning['candidates'])},
         'window': [args.warmup + 1 + tuning['steps_taken'], args.warmup + tuning['steps_taken'] + steps], 'seed': 3,
     }
 
@@ -651,12 +664,13 @@ def main():
             'cuda_graphs': graphs,
             'clocks': clocks.summary(),
             'e2e': e2e,
-            'cpu_baseline': cpu,
-            'drift_vs_fp64': drift,
-            'hulls': hulls,
-            'batched': batched,
-            'adjoint': adjoint,
+            'cpu_baseline': compact(cpu),
+            'drift_vs_fp64': compact(drift, 3),
             'device': name[0] if name else None,
+            # the other workloads last and compact, so that a log's tail holds them whole
+            'hulls': compact(hulls),
+            'batched': compact(batched),
+            'adjoint': compact(adjoint),
         }
         print(json.dumps(line), flush=True)
     R.close()

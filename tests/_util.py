@@ -260,9 +260,10 @@ LAMBDA_FLOOR_M = 1e-6
 
 def lambda_parity(gm: dict, om: dict, floor_m: float = LAMBDA_FLOOR_M, rows_of=(0, 1, 2)) -> dict:
     """Every common contact's multiplier rows (`rows_of`: 0 normal, 1 and 2 friction), GPU against
-    oracle: the largest |dlambda| as a multiple of its bound (<= 1 passes), the largest relative
-    difference of rows above 1e-3 N, and the share of those within LAMBDA_REL."""
-    worst, worst_rel, rows, within = 0.0, 0.0, 0, 0
+    oracle: the largest |dlambda| as a multiple of its bound (<= 1 passes), the rows compared and how
+    many exceed their bound, the largest relative difference of rows above 1e-3 N, and the share of
+    those within LAMBDA_REL."""
+    worst, worst_rel, rows, within, compared, over = 0.0, 0.0, 0, 0, 0, 0
     sel = list(rows_of)
     for k, (_, _, lam, pen) in gm.items():
         if k not in om:
@@ -271,10 +272,12 @@ def lambda_parity(gm: dict, om: dict, floor_m: float = LAMBDA_FLOOR_M, rows_of=(
         d = np.abs(np.asarray(lam, float)[sel] - olam)
         bound = LAMBDA_REL * np.abs(olam) + floor_m * np.maximum(open_, 1.0)
         worst = max(worst, float((d / bound).max()))
+        compared += len(sel)
+        over += int((d > bound).sum())
         big = np.abs(olam) > 1e-3
         if big.any():
             r = d[big] / np.abs(olam[big])
             worst_rel = max(worst_rel, float(r.max()))
             rows += int(big.sum())
             within += int((r <= LAMBDA_REL).sum())
-    return {'ratio': worst, 'worst_rel': worst_rel, 'rows': rows, 'within_rel': within / max(rows, 1)}
+    return {'ratio': worst, 'compared': compared, 'over': over, 'worst_rel': worst_rel, 'rows': rows, 'within_rel': within / max(rows, 1)}

@@ -280,6 +280,35 @@ __device__ inline void addRow(Acc& A, float3 l, float3 a, float k, float f) {
   A.v[24] += a.x * f; A.v[25] += a.y * f; A.v[26] += a.z * f;
 }
 
+// A point's three rows at once: directions d = n, t1, t2 (signed by sg for body B), stiffnesses k,
+// forces F, lever arm r. The rows' outer products sum to M = sum k_i d_i d_i^T (the sign cancels);
+// the angular Jacobian rows are [r]x d_i, so the cross block is [r]x M and the angular block
+// [r]x M [r]x^T; the gradient is sg sum F_i d_i and r x that.
+__device__ inline void addPoint(Acc& A, float3 r, float3 n, float3 t1, float3 t2, float3 k, float3 F, float sg) {
+  const float3 a = n * k.x, b = t1 * k.y, c = t2 * k.z;
+  const float M00 = a.x * n.x + b.x * t1.x + c.x * t2.x, M01 = a.x * n.y + b.x * t1.y + c.x * t2.y, M02 = a.x * n.z + b.x * t1.z + c.x * t2.z;
+  const float M11 = a.y * n.y + b.y * t1.y + c.y * t2.y, M12 = a.y * n.z + b.y * t1.z + c.y * t2.z, M22 = a.z * n.z + b.z * t1.z + c.z * t2.z;
+  A.v[0] += M00; A.v[1] += M01; A.v[2] += M02; A.v[3] += M11; A.v[4] += M12; A.v[5] += M22;
+  // X = [r]x M (row: angular index)
+  const float X00 = r.y * M02 - r.z * M01, X01 = r.y * M12 - r.z * M11, X02 = r.y * M22 - r.z * M12;
+  const float X10 = r.z * M00 - r.x * M02, X11 = r.z * M01 - r.x * M12, X12 = r.z * M02 - r.x * M22;
+  const float X20 = r.x * M01 - r.y * M00, X21 = r.x * M11 - r.y * M01, X22 = r.x * M12 - r.y * M02;
+  A.v[12] += X00; A.v[13] += X01; A.v[14] += X02;
+  A.v[15] += X10; A.v[16] += X11; A.v[17] += X12;
+  A.v[18] += X20; A.v[19] += X21; A.v[20] += X22;
+  // Y = X [r]x^T: Y_jk = sum_m X_jm S_km with S = [r]x
+  A.v[6] += r.y * X02 - r.z * X01;
+  A.v[7] += r.z * X00 - r.x * X02;
+  A.v[8] += r.x * X01 - r.y * X00;
+  A.v[9] += r.z * X10 - r.x * X12;
+  A.v[10] += r.x * X11 - r.y * X10;
+  A.v[11] += r.x * X21 - r.y * X20;
+  const float3 gl = (n * F.x + t1 * F.y + t2 * F.z) * sg;
+  const float3 ga = cross3(r, gl);
+  A.v[21] += gl.x; A.v[22] += gl.y; A.v[23] += gl.z;
+  A.v[24] += ga.x; A.v[25] += ga.y; A.v[26] += ga.z;
+}
+
 // --- contacts (wgsl-solve.ts:169-231) ----------------------------------------------------------------------
 struct ContactEval {
   float3 rAW, rBW, C, F;
@@ -545,12 +574,7 @@ __device__ inline void accumulateIncidence(Acc& acc, const DWorld& w, const Step
   const Pose& B = v.isA ? v.other : own;
   ContactEval e;
   evalContact(v.ra, v.rb, v.pen, v.lam, v.n, v.t1, v.t2, v.friction, A, B, p.alpha, e);
-  float sg = v.isA ? 1.0f : -1.0f;
-  float3 r = v.isA ? e.rAW : e.rBW;
-  float3 l0 = v.n * sg, l1 = v.t1 * sg, l2 = v.t2 * sg;
-  addRow(acc, l0, cross3(r, l0), v.pen.x, e.F.x);
-  addRow(acc, l1, cross3(r, l1), v.pen.y, e.F.y);
-  addRow(acc, l2, cross3(r, l2), v.pen.z, e.F.z);
+  addPoint(acc, v.isA ? e.rAW : e.rBW, v.n, v.t1, v.t2, make_float3(v.pen.x, v.pen.y, v.pen.z), e.F, v.isA ? 1.0f : -1.0f);
 }
 
 // The dual update of one owned incidence (wgsl-solve.ts:562-662)
