@@ -22,6 +22,7 @@
 namespace avbd {
 
 constexpr int SOLVE_THREADS = 256;
+constexpr uint32_t ADJ_SORT_LOCAL = 24;  // adjacency lists up to this long are sorted in local memory
 constexpr long long BARRIER_CYCLES = 4000000000LL;  // about two seconds of SM clock
 
 __device__ __forceinline__ uint32_t ldv(const uint32_t* p) { return *(const volatile uint32_t*)p; }
@@ -861,18 +862,37 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   for (uint32_t b = tid; b < n; b += T) {
     uint32_t lo = w.adjStart[b], hi = w.adjStart[b + 1];
     uint32_t rows = 0;
-    for (uint32_t i = lo; i < hi; i++) {
-      uint4 ent = w.adjList[i];
-      rows += ent.z >> 28;
-      if (i == lo) continue;
-      uint32_t j = i;
-      while (j > lo) {
-        uint4 prev = w.adjList[j - 1];
-        if (!entryLess(ent, prev)) break;
-        w.adjList[j] = prev;
-        j--;
+    if (hi - lo <= ADJ_SORT_LOCAL) {
+      // a short list: every entry loaded at once, sorted in the thread's own (L1-resident) memory,
+      // stored at once, instead of a chain of dependent global loads and stores
+      uint4 buf[ADJ_SORT_LOCAL];
+      const uint32_t d = hi - lo;
+      for (uint32_t i = 0; i < d; i++) buf[i] = w.adjList[lo + i];
+      for (uint32_t i = 0; i < d; i++) {
+        const uint4 ent = buf[i];
+        rows += ent.z >> 28;
+        uint32_t j = i;
+        while (j > 0 && entryLess(ent, buf[j - 1])) {
+          buf[j] = buf[j - 1];
+          j--;
+        }
+        buf[j] = ent;
       }
-      w.adjList[j] = ent;
+      for (uint32_t i = 0; i < d; i++) w.adjList[lo + i] = buf[i];
+    } else {
+      for (uint32_t i = lo; i < hi; i++) {
+        uint4 ent = w.adjList[i];
+        rows += ent.z >> 28;
+        if (i == lo) continue;
+        uint32_t j = i;
+        while (j > lo) {
+          uint4 prev = w.adjList[j - 1];
+          if (!entryLess(ent, prev)) break;
+          w.adjList[j] = prev;
+          j--;
+        }
+        w.adjList[j] = ent;
+      }
     }
     w.incCount[b] = rows;
   }
