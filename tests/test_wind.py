@@ -107,3 +107,27 @@ def test_cuda_sails_in_gusting_wind_match_the_oracle(cuda_lib):
     assert ((got['pos'] - c.read_bodies()['pos']) @ wind).mean() > 0.5
     w.destroy()
     c.destroy()
+
+
+@pytest.mark.gpu
+def test_batched_sails_in_wind_match_single_worlds(cuda_lib):
+    """The wind in batched worlds: three worlds of sails in gusting wind step bit for bit as each alone
+    with a one-block solve (the batch's scope), 30 steps; the world's step word sets the gusts' phase
+    in each world."""
+    import avbd_b200
+    scenes = [_flags_in_wind(n=8, seed=s) for s in (4, 5, 6)]
+    n = sum(len(s.bodies) for s in scenes)
+    b = avbd_b200.BatchSolver3D(len(scenes), n, params=scenes[0].params)
+    for s in scenes:
+        b.add_scene(s)
+    singles = [avbd_b200.CudaSolver3D(s) for s in scenes]
+    for w in singles:
+        w.set_solve_blocks(1)
+    b.step(30)
+    for w in singles:
+        w.step(30)
+    b.synchronize()
+    for i, w in enumerate(singles):
+        assert np.array_equal(b.read_bodies(i).view(np.uint32), w.read_bodies().view(np.uint32)), f'world {i}'
+        w.destroy()
+    b.destroy()
