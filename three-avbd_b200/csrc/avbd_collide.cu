@@ -537,29 +537,34 @@ __global__ void __launch_bounds__(PAIR_WALK_THREADS) k_find_pairs(DWorld w, Step
       k = w.cellStart[h];
       end = w.cellEnd[h];
     }
-    while (__any_sync(0xffffffffu, k < end)) {
-      bool push = false;
-      uint32_t j = 0;
-      if (k < end) {
-        const int4 cj = w.sortedCell[k];
-        j = (uint32_t)cj.w & 0x7fffffffu;
-        const bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
-        if (!(o == 0 && j >= i) && (dyn || dj) && cj.x == cc.x && cj.y == cc.y && cj.z == cc.z) {
-          const float4 pr = w.sortedPR[k];
-          const float3 d = pos - make_float3(pr.x, pr.y, pr.z);
-          const float r = radius + pr.w;
-          if (dot3(d, d) <= r * r) {  // the sphere test, the same in both views
-            const float4 ab = w.sortedAabb[k];  // and the AABB test (its sums commute)
-            push = !(fabsf(d.x) > aabb.x + ab.x + 1e-4f || fabsf(d.y) > aabb.y + ab.y + 1e-4f || fabsf(d.z) > aabb.z + ab.z + 1e-4f);
-          }
-        }
-        k++;
-      }
+    auto candidate = [&](uint32_t kk, uint32_t& jj) -> bool {
+      const int4 cj = w.sortedCell[kk];
+      jj = (uint32_t)cj.w & 0x7fffffffu;
+      const bool dj = ((uint32_t)cj.w & 0x80000000u) != 0u;
+      if ((o == 0 && jj >= i) || !(dyn || dj) || cj.x != cc.x || cj.y != cc.y || cj.z != cc.z) return false;
+      const float4 pr = w.sortedPR[kk];
+      const float3 d = pos - make_float3(pr.x, pr.y, pr.z);
+      const float r = radius + pr.w;
+      if (dot3(d, d) > r * r) return false;  // the sphere test, the same in both views
+      const float4 ab = w.sortedAabb[kk];      // and the AABB test (its sums commute)
+      return !(fabsf(d.x) > aabb.x + ab.x + 1e-4f || fabsf(d.y) > aabb.y + ab.y + 1e-4f || fabsf(d.z) > aabb.z + ab.z + 1e-4f);
+    };
+    auto enqueue = [&](bool push, uint32_t jj) {
       const uint32_t m = __ballot_sync(0xffffffffu, push);
-      if (push) Q[count + __popc(m & ((1u << lane) - 1u))] = make_uint2(i, j);
-      count += __popc(m);
-      __syncwarp();
-      if (count >= 32u) drainQueue(w, p, Q, count, lane);
+      if (m) {
+        if (push) Q[count + __popc(m & ((1u << lane) - 1u))] = make_uint2(i, jj);
+        count += __popc(m);
+        __syncwarp();
+        if (count >= 32u) drainQueue(w, p, Q, count, lane);
+      }
+    };
+    while (__any_sync(0xffffffffu, k < end)) {
+      uint32_t j0 = 0, j1 = 0;
+      const bool p0 = k < end && candidate(k, j0);
+      const bool p1 = k + 1 < end && candidate(k + 1, j1);
+      k += 2;
+      enqueue(p0, j0);
+      enqueue(p1, j1);
     }
   }
   while (count > 0u) drainQueue(w, p, Q, count, lane);
