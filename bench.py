@@ -42,6 +42,7 @@ UNIT = 'body-steps/s'
 PILE_BODIES = 100_000
 PILE_SPACING = 2.7
 ROLL = 200              # untimed steps before the timed window: the pile has landed and is in contact
+FD_SMOOTH_TOL = 1e-4     # central differences at h and h/4 within this (relative): the loss is smooth there
 REF_MAX_STEPS = 10      # timed steps of the CPU runs (a bounded sample of the window)
 NOMINAL_HBM_GBS = 7700.0  # HGX B200 HBM3e, for context beside the measured copy bandwidth
 L2_FLUSH_BYTES = 256 << 20
@@ -484,12 +485,20 @@ def run_adjoint(args, R, torch) -> dict:
     lp, _ = adj.forward(p0 + h * d)
     lm, _ = adj.forward(p0 - h * d)
     fd = (lp - lm) / (2 * h)
+    # the same differences at h / 4: where the loss is smooth over [-h, h] the two agree to O(h^2);
+    # where a friction-cone or clamp switch lies inside they do not. The rule looks at the replay
+    # alone, never at the adjoint, so the smooth set is fixed before the comparison.
+    lp4, _ = adj.forward(p0 + 0.25 * h * d)
+    lm4, _ = adj.forward(p0 - 0.25 * h * d)
+    fd4 = (lp4 - lm4) / (0.5 * h)
     sample = rng.choice(W, size=min(32, W), replace=False)
-    rel_all = []
+    rel_all, smooth = [], []
     for w in sample:
         a0, a1 = 8 * fb[w], 8 * fb[w + 1]
         an = float(grad[a0:a1] @ d[a0:a1])
         rel_all.append(abs(fd[w] - an) / max(abs(an), 1e-12))
+        smooth.append(abs(fd[w] - fd4[w]) <= FD_SMOOTH_TOL * max(abs(fd[w]), abs(fd4[w]), 1e-12))
+    rel_smooth = [e for e, s in zip(rel_all, smooth) if s]
     adj.destroy()
     b.destroy()
     return {
@@ -498,7 +507,10 @@ def run_adjoint(args, R, torch) -> dict:
         'reverse_fp64_ms': round(backward, 3), 'reverse_over_forward': backward / fwd_rec,
         'loss_mean': float(np.mean(losses_all)), 'gradient_finite': bool(np.isfinite(grads_all).all()), 'gathered_worlds': int(losses_all.size),
         'fd_check': {'worlds': len(sample), 'h': h, 'max_rel_err': float(max(rel_all)), 'median_rel_err': float(np.median(rel_all)),
-                     'worlds_within_1e-3': int(sum(1 for e in rel_all if e <= 1e-3))},
+                     'worlds_within_1e-3': int(sum(1 for e in rel_all if e <= 1e-3)),
+                     'smooth_rule': f'|fd(h) - fd(h/4)| <= {FD_SMOOTH_TOL} relative', 'smooth_worlds': len(rel_smooth),
+                     'smooth_max_rel_err': float(max(rel_smooth)) if rel_smooth else None,
+                     'smooth_median_rel_err': float(np.median(rel_smooth)) if rel_smooth else None},
         'recording': {'manifolds': rec['manifolds'], 'points': rec['points']}, 'seed': seed,
     }
 

@@ -686,13 +686,31 @@ __device__ __forceinline__ LaneJob laneJob(const DWorld& w, uint32_t c, uint32_t
   return J;
 }
 
+// The count a lane waits for before reading an incidence's partner (null: a static partner, no
+// wait). A partner of an earlier colour must have moved in this iteration: its pose is all this body
+// reads of it (their shared rows are this body's to update). One of a later colour must have finished
+// the previous iteration, pose and the rows it updates, these among them. A partner of the same colour
+// (only where the colour cap forced a clash) is not waited for within the iteration: the
+// colour-by-colour sweep runs such pairs side by side too.
+__device__ __forceinline__ const uint32_t* partnerFlag(const DWorld& w, uint2 inc, uint32_t it, uint32_t& need) {
+  need = 0u;
+  if (!(inc.y & PARTNER_DYNAMIC)) return nullptr;
+  const uint32_t partner = inc.y & PARTNER_MASK;
+  if (inc.y & PARTNER_EARLIER) {
+    need = it + 1u;
+    return w.poseDone + partner;
+  }
+  need = it;
+  return w.done + partner;
+}
+
 // One 32-lane chunk: each group of lanes (one body) accumulates its rows, sums them by butterfly, its
 // first lane solves and writes the pose, and the lanes update the rows the body owns. With kWait the
 // chunk waits for the partner bodies it reads and afterwards publishes its bodies' iteration count;
 // false: a wait gave up (warp-uniform). With kWait the caller runs a chunk on the same warp in every
 // iteration, so the chunk's own bodies were last written by this warp (ordered by its __syncwarp)
-// and need no wait: their state is loaded first, alongside the first row's incidence, and only the
-// partners' counts are awaited.
+// and need no wait: their state is loaded first, alongside the first two rows' incidences, and only the
+// partners' counts are awaited (those of the first two rows polled together).
 template <bool kWait>
 __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p, const LaneJob& J, uint32_t it) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -700,8 +718,10 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
   const bool active = J.active;
   const uint32_t L = J.L, sub = J.sub, body = J.body, e1 = J.e1;
   const uint32_t leader = lane - sub;
-  // the incidence list is fixed for the step: the lane's first row is read before any wait
+  // the incidence list is fixed for the step: the lane's first two rows are read before any wait
+  const uint32_t eB = J.e + L;
   const uint2 inc0 = kWait && active && J.e < e1 ? w.incList[J.e] : make_uint2(0u, 0u);
+  const uint2 inc1 = kWait && active && eB < e1 ? w.incList[eB] : make_uint2(0u, 0u);
   Pose own;
   Acc acc;
   accZero(acc);
@@ -735,23 +755,23 @@ __device__ __forceinline__ bool solveLanes(const DWorld& w, const StepParams& p,
   }
   if constexpr (kWait) {
     bool ok = true;
+    uint32_t needA, needB;
+    const uint32_t* fA = active && J.e < e1 ? partnerFlag(w, inc0, it, needA) : nullptr;
+    const uint32_t* fB = active && eB < e1 ? partnerFlag(w, inc1, it, needB) : nullptr;
+    const uint32_t vA = fA ? ld_acquire_gpu(fA) : 0u;
+    const uint32_t vB = fB ? ld_acquire_gpu(fB) : 0u;
+    if (fA && vA < needA) ok = waitDone(w, fA, needA);
+    if (ok && fB && vB < needB) ok = waitDone(w, fB, needB);
     if (active)
-      for (uint32_t e = J.e; e < e1 && ok; e += L) {
-        const uint2 inc = e == J.e ? inc0 : w.incList[e];
-        // A partner of an earlier colour must have moved in this iteration: its pose is all this
-        // body reads of it (their shared rows are this body's to update). One of a later colour must
-        // have finished the previous iteration, pose and the rows it updates, these among them. A
-        // partner of the same colour (only where the colour cap forced a clash) is not waited for
-        // within the iteration: the colour-by-colour sweep runs such pairs side by side too.
-        if (inc.y & PARTNER_DYNAMIC) {
-          const uint32_t partner = inc.y & PARTNER_MASK;
-          ok = (inc.y & PARTNER_EARLIER) ? waitDone(w, w.poseDone + partner, it + 1u) : waitDone(w, w.done + partner, it);
-        }
+      for (uint32_t e = eB + L; e < e1 && ok; e += L) {
+        uint32_t need;
+        const uint32_t* f = partnerFlag(w, w.incList[e], it, need);
+        if (f) ok = waitDone(w, f, need);
       }
     if (__any_sync(0xffffffffu, !ok)) return false;
   }
   if (active)
-    for (uint32_t e = J.e; e < e1; e += L) accumulateIncidence(acc, w, p, kWait && e == J.e ? inc0 : w.incList[e], body, own);
+    for (uint32_t e = J.e; e < e1; e += L) accumulateIncidence(acc, w, p, kWait && e == J.e ? inc0 : kWait && e == eB ? inc1 : w.incList[e], body, own);
   // butterfly over the group: as many rounds as the warp's widest group needs
   const uint32_t Lmax = __reduce_max_sync(0xffffffffu, L);
   for (uint32_t off = Lmax >> 1; off > 0; off >>= 1) {
