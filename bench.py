@@ -338,7 +338,7 @@ def run_batched(args, R, torch) -> dict:
         'per_world_launch': plain, 'per_world_sample': len(sample),
         'e2e': len(job) * steps / (te / 1000.0), 'h2d_d2h_bytes_per_step': n * 160,
         'worlds': len(job), 'worlds_this_rank': len(scenes), 'dynamic_bodies': dyn, 'world_errors': errors,
-        'launch': f"{tuning['collide_threads']}x{tuning['solve_blocks']}x{tuning['rows_per_lane']}",
+        'launch': f"{tuning['collide_threads']}x{tuning['solve_blocks']}x{tuning['rows_per_lane']}x{tuning['world_threads']}",
         'tuning': {'candidates': len(tuning['candidates']), 'best_ms': min(c['ms_per_step'] for c in tuning['candidates']),
                    'worst_ms': max(c['ms_per_step'] for c in tuning['candidates'])},
         'window': [args.warmup + 1 + tuning['steps_taken'], args.warmup + tuning['steps_taken'] + steps], 'seed': 3,

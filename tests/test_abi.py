@@ -42,7 +42,7 @@ def test_defaults_and_invalid_arguments_without_a_device():
     assert lib.avbd_default_params(ctypes.byref(p)) == 0
     assert abs(p.dt - 1 / 60) < 1e-7 and p.iterations == 10 and p.gravity == -10.0 and tuple(p.up) == (0.0, 0.0, 1.0)
     assert p.wind_pressure == 0.0 and p.wind_speed == 0.0  # no air: sails fall as the CPU solver's boxes
-    assert lib.avbd_abi_version() == 2
+    assert lib.avbd_abi_version() == 3
     assert lib.avbd_world_create(None, None) == _abi.AVBD_ERR_INVALID
     assert lib.avbd_world_destroy(None) == 0
     assert lib.avbd_step(None, 1) == _abi.AVBD_ERR_INVALID
@@ -75,7 +75,8 @@ def test_world_params_are_the_reference_production_defaults():
 def test_query_record_layouts():
     assert _abi.PUSH_DTYPE.itemsize == 40 and _abi.EVENT_DTYPE.itemsize == 48
     assert _abi.RAY_DTYPE.itemsize == 32 and _abi.HIT_DTYPE.itemsize == 32
-    assert ctypes.sizeof(_abi.BatchTuning) == 4 + 4 * 16 * 4 + 4 * 5
+    assert ctypes.sizeof(_abi.BatchTuning) == 4 + 4 * 16 * 5 + 4 * 6
+    assert ctypes.sizeof(_abi.BatchStatus) == 56  # 4 words, a 64-bit count, 7 words, padded to 8 bytes
 
 
 def test_create_fails_loudly_without_a_b200():

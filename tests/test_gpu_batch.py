@@ -160,6 +160,39 @@ def test_batch_graphs_and_determinism(cuda_lib):
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
+def test_batch_warp_per_world_matches_block_per_world(cuda_lib):
+    """A warp a world (eight worlds a block, warp barriers between colour passes) steps every world
+    bit for bit as a block a world does, over 30 steps of joints, springs, stacks and piles, with one
+    row a lane and with four; the shape is reported back and bad shapes are refused."""
+    scenes = _mixed_scenes()
+    for rpl in (1, 4):
+        out = []
+        for wt in (256, 32):
+            b = _batch_for(scenes)
+            b.set_launch(collide_threads=128, solve_blocks=0, rows_per_lane=rpl, world_threads=wt)
+            info = b.info()
+            assert (info['world_threads'], info['rows_per_lane']) == (wt, rpl)
+            b.step(30)
+            b.synchronize()
+            for i in range(len(scenes)):
+                c = b.read_counters(i)
+                assert c['error'] == 0 and c['overflow'] == 0, scenes[i].name
+            bodies = np.concatenate([b.read_bodies(i) for i in range(len(scenes))]).view(np.uint32).copy()
+            joints = np.concatenate([b.read_joints(i)[0] for i in range(len(scenes))]).view(np.uint32).copy()
+            colors = np.concatenate([b.read_colors(i) for i in range(len(scenes))]).copy()
+            out.append((bodies, joints, colors))
+            b.destroy()
+        (b0, j0, c0), (b1, j1, c1) = out
+        assert np.array_equal(c0, c1), f'rows a lane {rpl}: colours differ'
+        assert np.array_equal(j0, j1), f'rows a lane {rpl}: joints differ'
+        assert np.array_equal(b0, b1), f'rows a lane {rpl}: bodies differ'
+    b = _batch_for(scenes[:2])
+    for bad in ((100, 0, 1, 256), (128, 0, 0, 256), (128, 0, 1, 64), (128, 10 ** 6, 1, 32)):
+        with pytest.raises(avbd_b200.AvbdError):
+            b.set_launch(*bad)
+    b.destroy()
+
+
 def test_batch_tuner_and_host_buffers(cuda_lib):
     """The autotuner times each launch shape and keeps the fastest; all bodies round-trip through
     host buffers on the batch's stream."""
@@ -169,9 +202,11 @@ def test_batch_tuner_and_host_buffers(cuda_lib):
     t = b.tune(2)
     assert len(t['candidates']) >= 6 and all(c['ms_per_step'] > 0 for c in t['candidates'])
     assert {c['rows_per_lane'] for c in t['candidates']} == {1, 4} and t['rows_per_lane'] in (1, 4)  # bodies per warp tuned too
+    assert {c['world_threads'] for c in t['candidates']} == {32, 256} and t['world_threads'] in (32, 256)  # a warp or a block a world
     assert t['ms_per_step'] == min(c['ms_per_step'] for c in t['candidates'])
     info = b.info()
     assert info['collide_threads'] == t['collide_threads'] and info['solve_blocks'] == t['solve_blocks']
+    assert info['world_threads'] == t['world_threads'] and info['rows_per_lane'] == t['rows_per_lane']
     n = info['bodies']
     host = np.zeros(n, dtype=avbd_b200.BODY_DTYPE)
     b.read_all_bodies_into(host)

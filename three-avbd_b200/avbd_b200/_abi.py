@@ -117,7 +117,8 @@ class BatchWorld(ctypes.Structure):
 class BatchStatus(ctypes.Structure):
     _fields_ = [('worlds', ctypes.c_uint32), ('bodies', ctypes.c_uint32), ('joints', ctypes.c_uint32), ('steps', ctypes.c_uint32),
                 ('pair_slots', ctypes.c_uint64), ('relayouts', ctypes.c_uint32), ('collide_threads', ctypes.c_uint32),
-                ('collide_blocks', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32), ('graphs', ctypes.c_uint32)]
+                ('collide_blocks', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32), ('graphs', ctypes.c_uint32),
+                ('rows_per_lane', ctypes.c_uint32), ('world_threads', ctypes.c_uint32)]
 
 
 NOALLOC_MAX_BODIES = 4096
@@ -130,7 +131,8 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [('candidates', ctypes.c_uint32), ('candidate_threads', ctypes.c_uint32 * TUNE_CANDIDATES),
                 ('candidate_solve_blocks', ctypes.c_uint32 * TUNE_CANDIDATES), ('candidate_rows_per_lane', ctypes.c_uint32 * TUNE_CANDIDATES),
                 ('candidate_ms', ctypes.c_float * TUNE_CANDIDATES), ('collide_threads', ctypes.c_uint32), ('solve_blocks', ctypes.c_uint32),
-                ('rows_per_lane', ctypes.c_uint32), ('ms_per_step', ctypes.c_float), ('steps_taken', ctypes.c_uint32)]
+                ('rows_per_lane', ctypes.c_uint32), ('ms_per_step', ctypes.c_float), ('steps_taken', ctypes.c_uint32),
+                ('candidate_world_threads', ctypes.c_uint32 * TUNE_CANDIDATES), ('world_threads', ctypes.c_uint32)]
 
 
 # Every function include/avbd.h declares, with its argument types (the C-ABI symbol table)
@@ -235,6 +237,7 @@ SIGNATURES = {
     'avbd_batch_stream': ([P, ctypes.POINTER(ctypes.c_void_p)], I),
     'avbd_batch_tune': ([P, I, ctypes.POINTER(BatchTuning)], I),
     'avbd_batch_info': ([P, ctypes.POINTER(BatchStatus)], I),
+    'avbd_batch_set_launch': ([P, U, U, U, U], I),
 }
 
 _lib = None

@@ -104,9 +104,16 @@ class BatchSolver3D:
         self._check(self.lib.avbd_batch_tune(self.handle, steps, ctypes.byref(t)))
         k = t.candidates
         return {'candidates': [{'collide_threads': t.candidate_threads[i], 'solve_blocks': t.candidate_solve_blocks[i],
-                                'rows_per_lane': t.candidate_rows_per_lane[i], 'ms_per_step': t.candidate_ms[i]} for i in range(k)],
+                                'rows_per_lane': t.candidate_rows_per_lane[i], 'world_threads': t.candidate_world_threads[i],
+                                'ms_per_step': t.candidate_ms[i]} for i in range(k)],
                 'collide_threads': t.collide_threads, 'solve_blocks': t.solve_blocks, 'rows_per_lane': t.rows_per_lane,
-                'ms_per_step': t.ms_per_step, 'steps_taken': t.steps_taken}
+                'world_threads': t.world_threads, 'ms_per_step': t.ms_per_step, 'steps_taken': t.steps_taken}
+
+    def set_launch(self, collide_threads: int = 128, solve_blocks: int = 0, rows_per_lane: int = 1, world_threads: int = 256):
+        """Sets the launch shape the tuner would pick: collision block size (64, 128, 256), solve blocks (0:
+        as many as fit), the least rows a lane (1..8), and the solve's threads a world (256: a block a
+        world; 32: a warp a world, eight worlds a block). Results are the same bit for bit in every shape."""
+        self._check(self.lib.avbd_batch_set_launch(self.handle, collide_threads, solve_blocks, rows_per_lane, world_threads))
 
     @property
     def stream(self) -> int:

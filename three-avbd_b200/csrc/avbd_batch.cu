@@ -46,6 +46,7 @@ struct avbd_batch {
   // launch shape (the autotuner's choice)
   int sms = 0, collideThreads = 128, collideBlocks = 0, solveBlocks = 0;
   uint32_t rowsPerLane = 1;  // the solve's least rows a lane (bodies per warp), chosen by the tuner
+  int worldThreads = 256;    // the solve's threads a world: 256 (a block) or 32 (a warp), chosen by the tuner
   // status of the last step, copied back asynchronously
   uint32_t* hStatus = nullptr;
   cudaEvent_t statusReady = nullptr;
@@ -250,7 +251,7 @@ void launchShape(avbd_batch* b) {
   const int nw = int(std::max<size_t>(b->worlds.size(), 1));
   int cper = std::max(1, batch_collide_blocks_per_sm(b->collideThreads));
   b->collideBlocks = std::min(nw, b->sms * cper);
-  if (b->solveBlocks <= 0) b->solveBlocks = b->sms * std::max(1, batch_solve_blocks_per_sm());
+  if (b->solveBlocks <= 0) b->solveBlocks = b->sms * std::max(1, batch_solve_blocks_per_sm(b->worldThreads));
 }
 
 BatchLaunch makeLaunch(avbd_batch* b) {
@@ -288,7 +289,8 @@ cudaError_t enqueueStep(avbd_batch* b, const BatchLaunch& L) {
   cudaMemsetAsync(b->dStatus, 0, 2 * sizeof(uint32_t), b->stream);
   cudaError_t e = launch_batch_collision(L, b->collideBlocks, b->collideThreads, b->stream);
   if (e != cudaSuccess) return e;
-  e = launch_batch_solve(L, std::min<int>(b->solveBlocks, int(L.nWorlds)), b->stream);
+  const int worldsPerBlock = b->worldThreads == 32 ? BATCH_SOLVE_THREADS / 32 : 1;
+  e = launch_batch_solve(L, std::min<int>(b->solveBlocks, (int(L.nWorlds) + worldsPerBlock - 1) / worldsPerBlock), b->worldThreads, b->stream);
   if (e != cudaSuccess) return e;
   return cudaMemcpyAsync(b->hStatus, b->dStatus, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
 }
@@ -811,54 +813,70 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
   int r = avbd_batch_synchronize(b);
   if (r) return r;
   const int threads[3] = {64, 128, 256};
-  const int solvePer = std::max(1, batch_solve_blocks_per_sm());
   avbd_batch_tuning t{};
   cudaEvent_t e0, e1;
   BATCH_TRY(b, cudaEventCreate(&e0));
   BATCH_TRY(b, cudaEventCreate(&e1));
   float best = INFINITY;
-  int bestT = b->collideThreads, bestS = b->solveBlocks;
+  int bestT = b->collideThreads, bestS = b->solveBlocks, bestW = b->worldThreads;
   uint32_t bestR = b->rowsPerLane;
   const bool graphs = b->useGraphs;
   b->useGraphs = false;
   uint32_t k = 0;
-  const uint32_t rowsPerLane[2] = {1, 4};  // a body's rows over as many lanes as its colour allows, or 4 a lane at least
-  for (int ri = 0; ri < 2; ri++)
-  for (int ti = 0; ti < 3; ti++)
-    for (int sp = 1; sp <= solvePer && k < AVBD_BATCH_TUNE_CANDIDATES; sp++) {
-      b->collideThreads = threads[ti];
-      b->solveBlocks = b->sms * sp;
-      b->rowsPerLane = rowsPerLane[ri];
-      launchShape(b);
-      r = avbd_batch_step(b, 1);  // settle storage for this shape
-      if (!r) r = avbd_batch_synchronize(b);
-      if (r) break;
-      cudaEventRecord(e0, b->stream);
-      r = avbd_batch_step(b, steps);
-      cudaEventRecord(e1, b->stream);
-      if (!r) r = avbd_batch_synchronize(b);
-      if (r) break;
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      ms /= float(steps);
-      t.candidate_threads[k] = uint32_t(threads[ti]);
-      t.candidate_solve_blocks[k] = uint32_t(b->solveBlocks);
-      t.candidate_rows_per_lane[k] = rowsPerLane[ri];
-      t.candidate_ms[k] = ms;
-      k++;
-      if (ms < best) {
-        best = ms;
-        bestT = threads[ti];
-        bestS = b->solveBlocks;
-        bestR = rowsPerLane[ri];
-      }
+  // one candidate: its mean step time over `steps` after one step that settles storage for the shape
+  auto trial = [&](int ct, int sb, uint32_t rpl, int wt) -> int {
+    if (k >= AVBD_BATCH_TUNE_CANDIDATES) return AVBD_OK;
+    b->collideThreads = ct;
+    b->solveBlocks = sb;
+    b->rowsPerLane = rpl;
+    b->worldThreads = wt;
+    launchShape(b);
+    int rr = avbd_batch_step(b, 1);
+    if (!rr) rr = avbd_batch_synchronize(b);
+    if (rr) return rr;
+    cudaEventRecord(e0, b->stream);
+    rr = avbd_batch_step(b, steps);
+    cudaEventRecord(e1, b->stream);
+    if (!rr) rr = avbd_batch_synchronize(b);
+    if (rr) return rr;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= float(steps);
+    t.candidate_threads[k] = uint32_t(ct);
+    t.candidate_solve_blocks[k] = uint32_t(sb);
+    t.candidate_rows_per_lane[k] = rpl;
+    t.candidate_world_threads[k] = uint32_t(wt);
+    t.candidate_ms[k] = ms;
+    k++;
+    if (ms < best) {
+      best = ms;
+      bestT = ct;
+      bestS = sb;
+      bestR = rpl;
+      bestW = wt;
     }
+    return AVBD_OK;
+  };
+  // The collision and the solve are separate launches whose times add, so the collision block size
+  // is chosen first (under the starting solve shape), then the solve's shape: a block or a warp a
+  // world, resident blocks an SM, and the least rows a lane (1, or 4: bodies per warp).
+  const int startS = b->solveBlocks > 0 ? b->solveBlocks : b->sms * std::max(1, batch_solve_blocks_per_sm(b->worldThreads));
+  for (int ti = 0; ti < 3 && !r; ti++) r = trial(threads[ti], startS, b->rowsPerLane, b->worldThreads);
+  const int collideBest = bestT;
+  const int worldThreads[2] = {256, 32};
+  const uint32_t rowsPerLane[2] = {1, 4};
+  for (int wi = 0; wi < 2 && !r; wi++) {
+    const int per = std::max(1, batch_solve_blocks_per_sm(worldThreads[wi]));
+    for (int sp = 1; sp <= per && !r; sp++)
+      for (int ri = 0; ri < 2 && !r; ri++) r = trial(collideBest, b->sms * sp, rowsPerLane[ri], worldThreads[wi]);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->useGraphs = graphs;
   b->collideThreads = bestT;
   b->solveBlocks = bestS;
   b->rowsPerLane = bestR;
+  b->worldThreads = bestW;
   launchShape(b);
   b->configGen++;
   if (r) return r;
@@ -866,6 +884,7 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
   t.collide_threads = uint32_t(bestT);
   t.solve_blocks = uint32_t(bestS);
   t.rows_per_lane = bestR;
+  t.world_threads = uint32_t(bestW);
   t.ms_per_step = best;
   t.steps_taken = k * uint32_t(steps + 1);
   if (out) *out = t;
@@ -936,6 +955,27 @@ int avbd_batch_record_status(avbd_batch* b, uint32_t* steps, uint64_t* manifolds
   return AVBD_OK;
 }
 
+int avbd_batch_set_launch(avbd_batch* b, uint32_t collideThreads, uint32_t solveBlocks, uint32_t rowsPerLane, uint32_t worldThreads) {
+  if (!b) return AVBD_ERR_INVALID;
+  if (collideThreads != 64 && collideThreads != 128 && collideThreads != 256)
+    return bfail(b, AVBD_ERR_INVALID, "collision block size must be 64, 128 or 256");
+  if (rowsPerLane < 1 || rowsPerLane > 8) return bfail(b, AVBD_ERR_INVALID, "rows per lane must be 1 to 8");
+  if (worldThreads != 32 && worldThreads != 256) return bfail(b, AVBD_ERR_INVALID, "threads a world must be 32 or 256");
+  cudaSetDevice(b->device);
+  const int per = std::max(1, batch_solve_blocks_per_sm(int(worldThreads)));
+  if (solveBlocks > uint32_t(b->sms * per))
+    return bfail(b, AVBD_ERR_INVALID, "solve blocks beyond " + std::to_string(b->sms * per) + " (the blocks that fit)");
+  int r = avbd_batch_synchronize(b);
+  if (r) return r;
+  b->collideThreads = int(collideThreads);
+  b->solveBlocks = int(solveBlocks);  // 0: as many as fit (launchShape)
+  b->rowsPerLane = rowsPerLane;
+  b->worldThreads = int(worldThreads);
+  launchShape(b);
+  b->configGen++;
+  return AVBD_OK;
+}
+
 int avbd_batch_info(avbd_batch* b, avbd_batch_status* out) {
   if (!b || !out) return AVBD_ERR_INVALID;
   out->worlds = uint32_t(b->worlds.size());
@@ -948,6 +988,8 @@ int avbd_batch_info(avbd_batch* b, avbd_batch_status* out) {
   out->collide_blocks = uint32_t(b->collideBlocks);
   out->solve_blocks = uint32_t(b->solveBlocks);
   out->graphs = b->useGraphs ? 1u : 0u;
+  out->rows_per_lane = b->rowsPerLane;
+  out->world_threads = uint32_t(b->worldThreads);
   return AVBD_OK;
 }
 

@@ -269,9 +269,10 @@ struct BatchLaunch {
 };
 constexpr uint32_t BATCH_OVERFLOW = 1u, BATCH_NEAR_FULL = 2u;
 cudaError_t launch_batch_collision(const BatchLaunch& b, int blocks, int threads, cudaStream_t s);
-cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, cudaStream_t s);
+// worldThreads: 256, a block a world; 32, a warp a world (eight worlds a block)
+cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, int worldThreads, cudaStream_t s);
 int batch_collide_blocks_per_sm(int threads);
-int batch_solve_blocks_per_sm();
+int batch_solve_blocks_per_sm(int worldThreads);
 constexpr int BATCH_SOLVE_THREADS = 256;  // the solve's block size (its shared tables assume it)
 constexpr uint32_t BATCH_MAX_WORLD_BODIES = 4096;
 

@@ -119,10 +119,35 @@ __device__ uint32_t block_scan_range(uint32_t* data, uint32_t lo, uint32_t hi) {
   return s_carry;
 }
 
-// The two scopes the topology+solve code runs at: the whole grid (one large world, cooperative
-// launch, bounded grid barriers) or one block (one small world of a batch, __syncthreads).
+// Exclusive scan of one warp's range [lo, hi) in place; returns the range total (all lanes).
+__device__ uint32_t warp_scan_range(uint32_t* data, uint32_t lo, uint32_t hi) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t carry = 0;
+  for (uint32_t base = lo; base < hi; base += 32u) {
+    const uint32_t i = base + lane;
+    const uint32_t v = i < hi ? data[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (i < hi) data[i] = carry + x - v;
+    carry += __shfl_sync(0xffffffffu, x, 31);
+  }
+  __syncwarp();
+  return carry;
+}
+
+// The three scopes the topology+solve code runs at: the whole grid (one large world, cooperative
+// launch, bounded grid barriers), one block (one small world of a batch, __syncthreads) or one warp
+// (one small world of a batch, __syncwarp; a block runs eight worlds at once). A team's "unit" is
+// the part of it that shares one copy of the shared-memory tables: a block, or for a warp team the
+// warp itself. laneBudget is the thread count the lane classes are sized by: a warp team sizes them
+// as a block does, so that every body gets the same lanes and sums its rows in the same order.
 struct GridTeam {
   static constexpr bool kDataflow = true;  // colour passes as a dataflow sweep (no grid barrier per colour)
+  static constexpr uint32_t kUnits = 1;
   uint32_t* bar;
   uint32_t* ctr;
   __device__ uint32_t rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -130,9 +155,16 @@ struct GridTeam {
   __device__ uint32_t block() const { return blockIdx.x; }
   __device__ uint32_t blocks() const { return gridDim.x; }
   __device__ bool sync() { return grid_sync(bar, ctr); }
+  __device__ uint32_t unit() const { return 0; }
+  __device__ uint32_t lrank() const { return threadIdx.x; }
+  __device__ uint32_t lsize() const { return blockDim.x; }
+  __device__ void lsync() const { __syncthreads(); }
+  __device__ uint32_t scan(uint32_t* data, uint32_t lo, uint32_t hi) const { return block_scan_range(data, lo, hi); }
+  __device__ uint32_t laneBudget() const { return size(); }
 };
 struct BlockTeam {
   static constexpr bool kDataflow = false;  // a block's __syncthreads per colour costs little
+  static constexpr uint32_t kUnits = 1;
   __device__ uint32_t rank() const { return threadIdx.x; }
   __device__ uint32_t size() const { return blockDim.x; }
   __device__ uint32_t block() const { return 0; }
@@ -141,6 +173,30 @@ struct BlockTeam {
     __syncthreads();
     return true;
   }
+  __device__ uint32_t unit() const { return 0; }
+  __device__ uint32_t lrank() const { return threadIdx.x; }
+  __device__ uint32_t lsize() const { return blockDim.x; }
+  __device__ void lsync() const { __syncthreads(); }
+  __device__ uint32_t scan(uint32_t* data, uint32_t lo, uint32_t hi) const { return block_scan_range(data, lo, hi); }
+  __device__ uint32_t laneBudget() const { return size(); }
+};
+struct WarpTeam {
+  static constexpr bool kDataflow = false;
+  static constexpr uint32_t kUnits = SOLVE_THREADS / 32;
+  __device__ uint32_t rank() const { return threadIdx.x & 31u; }
+  __device__ uint32_t size() const { return 32u; }
+  __device__ uint32_t block() const { return 0; }
+  __device__ uint32_t blocks() const { return 1; }
+  __device__ bool sync() {
+    __syncwarp();
+    return true;
+  }
+  __device__ uint32_t unit() const { return threadIdx.x >> 5; }
+  __device__ uint32_t lrank() const { return threadIdx.x & 31u; }
+  __device__ uint32_t lsize() const { return 32u; }
+  __device__ void lsync() const { __syncwarp(); }
+  __device__ uint32_t scan(uint32_t* data, uint32_t lo, uint32_t hi) const { return warp_scan_range(data, lo, hi); }
+  __device__ uint32_t laneBudget() const { return SOLVE_THREADS; }
 };
 
 // Exclusive scan of data[0, len) across the team; scratch[team.blocks()] receives the total.
@@ -149,16 +205,16 @@ __device__ bool team_scan(uint32_t* data, uint32_t len, uint32_t* scratch, Team&
   const uint32_t nb = team.blocks(), bi = team.block();
   uint32_t chunk = (len + nb - 1) / nb;
   uint32_t lo = min(len, bi * chunk), hi = min(len, lo + chunk);
-  uint32_t total = block_scan_range(data, lo, hi);
-  if (threadIdx.x == 0) scratch[bi] = total;
+  uint32_t total = team.scan(data, lo, hi);
+  if (team.lrank() == 0) scratch[bi] = total;
   if (!team.sync()) return false;
   if (bi == 0) {
-    uint32_t all = block_scan_range(scratch, 0, nb);
-    if (threadIdx.x == 0) scratch[nb] = all;
+    uint32_t all = team.scan(scratch, 0, nb);
+    if (team.lrank() == 0) scratch[nb] = all;
   }
   if (!team.sync()) return false;
   uint32_t add = scratch[bi];
-  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) data[i] += add;
+  for (uint32_t i = lo + team.lrank(); i < hi; i += team.lsize()) data[i] += add;
   return team.sync();
 }
 
@@ -997,10 +1053,15 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   // D. final colours (NO_COLOR -> cap - 1, pending kept and counted), and bodies counted into
   // (colour, lane class) buckets, widest lane class first within a colour. The order of bodies in a
   // bucket does not change any result (a colour's bodies share no row), so the scatter uses atomics.
-  __shared__ uint32_t s_hist[BUCKETS], s_base[BUCKETS], s_perLane[MAX_COLORS];
+  // The unit's shared tables: (s_hist, s_base) here, then (s_lane, s_start) in the iterations
+  __shared__ uint32_t s_tabs[Team::kUnits][2 * BUCKETS], s_perLaneU[Team::kUnits][MAX_COLORS];
+  uint32_t* const s_hist = s_tabs[team.unit()];
+  uint32_t* const s_base = s_hist + BUCKETS;
+  uint32_t* const s_perLane = s_perLaneU[team.unit()];
+  const uint32_t lr = team.lrank(), ls = team.lsize();
   {
-    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
-    __syncthreads();
+    for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls) s_hist[k] = 0;
+    team.lsync();
     uint32_t clashes = 0, maxc = 0;
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
@@ -1014,60 +1075,60 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
     }
     if (clashes) atomicAdd(&ctr[C_CLASHES], clashes);
     if (maxc) atomicMax(&ctr[C_COLORS], maxc);
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < (uint32_t)MAX_COLORS; k += SOLVE_THREADS)
+    team.lsync();
+    for (uint32_t k = lr; k < (uint32_t)MAX_COLORS; k += ls)
       if (s_hist[k]) atomicAdd(&w.bucket[B_ROWS + k], s_hist[k]);
   }
   GSYNC
   {
-    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
-    if (threadIdx.x < (uint32_t)MAX_COLORS) s_perLane[threadIdx.x] = max(max(1u, p.rowsPerLane), (w.bucket[B_ROWS + threadIdx.x] + T - 1u) / T);
-    __syncthreads();
+    const uint32_t budget = team.laneBudget();
+    for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls) s_hist[k] = 0;
+    for (uint32_t k = lr; k < (uint32_t)MAX_COLORS; k += ls) s_perLane[k] = max(max(1u, p.rowsPerLane), (w.bucket[B_ROWS + k] + budget - 1u) / budget);
+    team.lsync();
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
       uint32_t col = w.colorA[b] & 0xffu;
       atomicAdd(&s_hist[col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b], s_perLane[col]))], 1u);
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS)
+    team.lsync();
+    for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls)
       if (s_hist[k]) atomicAdd(&w.bucket[B_COUNT + k], s_hist[k]);
   }
   GSYNC
   if (team.block() == 0) {
-    if (threadIdx.x < BUCKETS) w.bucket[B_START + threadIdx.x] = w.bucket[B_COUNT + threadIdx.x];
-    if (threadIdx.x + SOLVE_THREADS < BUCKETS) w.bucket[B_START + threadIdx.x + SOLVE_THREADS] = w.bucket[B_COUNT + threadIdx.x + SOLVE_THREADS];
-    __syncthreads();
-    uint32_t total = block_scan_range(w.bucket + B_START, 0, BUCKETS);
-    if (threadIdx.x == 0) w.bucket[B_START + BUCKETS] = total;
-    if (threadIdx.x < (uint32_t)MAX_COLORS) {
-      uint32_t c = threadIdx.x, lanes = 0;
+    for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls) w.bucket[B_START + k] = w.bucket[B_COUNT + k];
+    team.lsync();
+    uint32_t total = team.scan(w.bucket + B_START, 0, BUCKETS);
+    if (lr == 0) w.bucket[B_START + BUCKETS] = total;
+    for (uint32_t c = lr; c < (uint32_t)MAX_COLORS; c += ls) {
+      uint32_t lanes = 0;
       for (int j = 0; j < LANE_CLASSES; j++) {
         w.bucket[B_LANE + c * LANE_CLASSES + j] = lanes;
         lanes += w.bucket[B_COUNT + c * LANE_CLASSES + j] * (32u >> j);
       }
       w.bucket[B_LANE_TOTAL + c] = lanes;
     }
-    __syncthreads();
-    if (threadIdx.x <= (uint32_t)MAX_COLORS) w.colorStart[threadIdx.x] = w.bucket[B_START + threadIdx.x * LANE_CLASSES];
+    team.lsync();
+    for (uint32_t c = lr; c <= (uint32_t)MAX_COLORS; c += ls) w.colorStart[c] = w.bucket[B_START + c * LANE_CLASSES];
   }
   GSYNC
   const uint32_t numDyn = ldv(&w.bucket[B_START + BUCKETS]);
   const uint32_t numColors = ldv(&ctr[C_COLORS]);
   {
-    // each block reserves one range per bucket for its bodies, then places them by shared counters
-    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) s_hist[k] = 0;
-    __syncthreads();
+    // each unit reserves one range per bucket for its bodies, then places them by shared counters
+    for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls) s_hist[k] = 0;
+    team.lsync();
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
       uint32_t col = w.colorA[b] & 0xffu;
       atomicAdd(&s_hist[col * LANE_CLASSES + (LANE_CLASSES - 1u - laneClass(w.incCount[b], s_perLane[col]))], 1u);
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) {
+    team.lsync();
+    for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls) {
       s_base[k] = s_hist[k] ? w.bucket[B_START + k] + atomicAdd(&w.bucket[B_FILL + k], s_hist[k]) : 0u;
       s_hist[k] = 0;
     }
-    __syncthreads();
+    team.lsync();
     for (uint32_t b = tid; b < n; b += T) {
       if (!dynBody(w, (int)b)) continue;
       uint32_t col = w.colorA[b] & 0xffu;
@@ -1240,13 +1301,16 @@ __device__ void topologySolve(const DWorld& w, const StepParams& p, Team& team) 
   // G. iterations: per colour, each body's group of lanes (its lane class) accumulates its rows, the
   // group sums in registers, the first lane solves, and every lane then updates the rows it owns.
   // The colours' lane tables (lane bases, bucket starts, lane totals) are kept in shared memory.
-  __shared__ uint32_t s_lane[BUCKETS], s_start[BUCKETS], s_total[MAX_COLORS], s_chunk[MAX_COLORS + 1], s_laneOff[MAX_COLORS + 1];
-  for (uint32_t k = threadIdx.x; k < (uint32_t)BUCKETS; k += SOLVE_THREADS) {
+  __shared__ uint32_t s_totalU[Team::kUnits][MAX_COLORS], s_chunk[MAX_COLORS + 1], s_laneOff[MAX_COLORS + 1];
+  uint32_t* const s_lane = s_hist;  // the unit's tables, free again since D
+  uint32_t* const s_start = s_base;
+  uint32_t* const s_total = s_totalU[team.unit()];
+  for (uint32_t k = lr; k < (uint32_t)BUCKETS; k += ls) {
     s_lane[k] = w.bucket[B_LANE + k];
     s_start[k] = w.bucket[B_START + k];
   }
-  if (threadIdx.x < (uint32_t)MAX_COLORS) s_total[threadIdx.x] = w.bucket[B_LANE_TOTAL + threadIdx.x];
-  __syncthreads();
+  for (uint32_t k = lr; k < (uint32_t)MAX_COLORS; k += ls) s_total[k] = w.bucket[B_LANE_TOTAL + k];
+  team.lsync();
   const uint32_t warpGlobal = tid >> 5, nwarps = T >> 5;
   if constexpr (Team::kDataflow) {
     // Dataflow sweep: the iterations' colour passes as one ordered list of 32-lane chunks. A chunk
@@ -1363,16 +1427,46 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_batch_solve(BatchLaunch B)
   }
 }
 
+// Batched worlds, a warp a world: each warp takes worlds from the same queue and runs the topology
+// and barrier sweep with warp barriers, so a block steps eight worlds at once and a world's colour
+// passes wait on __syncwarp instead of a block barrier. Lane classes are sized as a block sizes them
+// (WarpTeam::laneBudget), so every world's results are bit for bit those of the block-per-world launch.
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_batch_solve_warps(BatchLaunch B) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    uint32_t qi = 0;
+    if (lane == 0) qi = atomicAdd(&B.queue[1], 1u);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= B.nWorlds) return;
+    const uint32_t wi = B.order[qi];
+    const WorldDesc d = B.worlds[wi];
+    const DWorld w = worldView(B.base, d, wi);
+    const StepParams p = worldParams(B.p, d);
+    for (uint32_t i = lane; i <= d.n; i += 32u) {
+      w.adjStart[i] = 0u;
+      w.adjFill[i] = 0u;
+    }
+    for (uint32_t k = lane; k < (uint32_t)BUCKET_WORDS; k += 32u) w.bucket[k] = 0u;
+    __syncwarp();
+    WarpTeam team;
+    topologySolve(w, p, team);
+    __syncwarp();
+    if (lane == 0 && w.counters[C_ERROR]) atomicOr(&B.status[1], w.counters[C_ERROR]);
+  }
+}
+
 static_assert(BATCH_SOLVE_THREADS == SOLVE_THREADS, "one solve block size");
 
-int batch_solve_blocks_per_sm() {
+int batch_solve_blocks_per_sm(int worldThreads) {
   int perSm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve, SOLVE_THREADS, 0);
+  if (worldThreads == 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve_warps, SOLVE_THREADS, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve, SOLVE_THREADS, 0);
   return perSm;
 }
 
-cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, cudaStream_t s) {
-  k_batch_solve<<<blocks, SOLVE_THREADS, 0, s>>>(b);
+cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, int worldThreads, cudaStream_t s) {
+  if (worldThreads == 32) k_batch_solve_warps<<<blocks, SOLVE_THREADS, 0, s>>>(b);
+  else k_batch_solve<<<blocks, SOLVE_THREADS, 0, s>>>(b);
   return cudaGetLastError();
 }
 
