@@ -273,6 +273,11 @@ def run_batched(args, R, torch) -> dict:
     b = avbd_b200.BatchSolver3D(len(scenes), n, 1, params=scenes[0].params, device=local)
     for s in scenes:
         b.add_scene(s)
+    # the worlds land and settle first (untimed), so the tuner times launch shapes on the contact
+    # structure the timed window has, not on the first steps' free fall
+    if args.batched_settle > 0:
+        b.step(args.batched_settle)
+    b.synchronize()
     tuning = b.tune(2)
     b.step(args.warmup)
     b.synchronize()
@@ -341,7 +346,8 @@ def run_batched(args, R, torch) -> dict:
         'launch': f"{tuning['collide_threads']}x{tuning['solve_blocks']}x{tuning['rows_per_lane']}x{tuning['world_threads']}",
         'tuning': {'candidates': len(tuning['candidates']), 'best_ms': min(c['ms_per_step'] for c in tuning['candidates']),
                    'worst_ms': max(c['ms_per_step'] for c in tuning['candidates'])},
-        'window': [args.warmup + 1 + tuning['steps_taken'], args.warmup + tuning['steps_taken'] + steps], 'seed': 3,
+        'window': [args.batched_settle + tuning['steps_taken'] + args.warmup + 1, args.batched_settle + tuning['steps_taken'] + args.warmup + steps],
+        'seed': 3,
     }
 
 
@@ -529,6 +535,7 @@ def main():
     ap.add_argument('--no-graphs', action='store_true', help='launch each kernel directly instead of replaying the step graph')
     ap.add_argument('--batched-worlds', type=int, default=4096, help='worlds of the batched workload (0: skip it)')
     ap.add_argument('--batched-steps', type=int, default=300)
+    ap.add_argument('--batched-settle', type=int, default=60, help='untimed steps of the batched worlds before the tuner')
     ap.add_argument('--plain-sample', type=int, default=64, help='worlds stepped one by one for the per-world comparison')
     ap.add_argument('--hull-steps', type=int, default=120, help='timed steps of the hulls-and-chains workload (0: skip it)')
     ap.add_argument('--hull-roll', type=int, default=60, help='untimed steps before the hulls-and-chains window (the hulls reach the chains)')

@@ -536,12 +536,12 @@ typedef struct avbd_batch_status {
   uint32_t relayouts; /* times pair storage was laid out again for a world that outgrew it */
   uint32_t collide_threads, collide_blocks, solve_blocks, graphs;
   uint32_t rows_per_lane; /* the solve's least rows a lane of a body's group */
-  uint32_t world_threads; /* the solve's threads a world: 256 (a block a world) or 32 (a warp a world) */
+  uint32_t world_threads; /* the solve's threads a world: 256 (a block a world), 128, 64 or 32 */
 } avbd_batch_status;
 
 /* The autotuner's measurements: per candidate launch shape (collision block size, solve blocks,
- * bodies per warp as the least rows a lane of a body's group takes: 1, or 4, and a block or a warp a
- * world) its mean step time */
+ * bodies per warp as the least rows a lane of a body's group takes: 1, or 4, and the threads a world:
+ * a block, four, two or one warp) its mean step time */
 typedef struct avbd_batch_tuning {
   uint32_t candidates;
   uint32_t candidate_threads[AVBD_BATCH_TUNE_CANDIDATES];
@@ -551,7 +551,7 @@ typedef struct avbd_batch_tuning {
   uint32_t collide_threads, solve_blocks, rows_per_lane; /* the choice */
   float ms_per_step;
   uint32_t steps_taken; /* tuning steps are real steps: the worlds advance by this many */
-  uint32_t candidate_world_threads[AVBD_BATCH_TUNE_CANDIDATES]; /* 256: a block a world; 32: a warp a world */
+  uint32_t candidate_world_threads[AVBD_BATCH_TUNE_CANDIDATES]; /* 256: a block a world; 128, 64, 32: part of one */
   uint32_t world_threads;                                        /* the choice */
 } avbd_batch_tuning;
 
@@ -579,12 +579,12 @@ int avbd_batch_write_all_bodies_async(avbd_batch* batch, const avbd_body* src, u
 int avbd_batch_use_graphs(avbd_batch* batch, int enable);
 int avbd_batch_stream(avbd_batch* batch, void** stream);
 /* Times each candidate launch shape over `steps` real steps and keeps the fastest: the collision
- * block size first, then the solve's shape (a block or a warp a world x solve blocks x rows per lane). */
+ * block size first, then the solve's threads a world x solve blocks, then four rows a lane. */
 int avbd_batch_tune(avbd_batch* batch, int steps, avbd_batch_tuning* out);
 /* Sets the launch shape the tuner would choose: collision block size (64, 128 or 256), solve blocks
  * (0: as many as fit), the least rows a lane (1 to 8) and the solve's threads a world (256: a block a
- * world; 32: a warp a world, eight worlds a block). Every shape gives the same results bit for bit.
- * No counterpart in the reference (it has no batched worlds). */
+ * world; 128, 64 or 32: two, four or eight worlds a block). Every shape gives the same results bit for
+ * bit. No counterpart in the reference (it has no batched worlds). */
 int avbd_batch_set_launch(avbd_batch* batch, uint32_t collide_threads, uint32_t solve_blocks, uint32_t rows_per_lane, uint32_t world_threads);
 int avbd_batch_info(avbd_batch* batch, avbd_batch_status* out);
 

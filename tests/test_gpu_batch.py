@@ -160,14 +160,15 @@ def test_batch_graphs_and_determinism(cuda_lib):
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
-def test_batch_warp_per_world_matches_block_per_world(cuda_lib):
-    """A warp a world (eight worlds a block, warp barriers between colour passes) steps every world
-    bit for bit as a block a world does, over 30 steps of joints, springs, stacks and piles, with one
-    row a lane and with four; the shape is reported back and bad shapes are refused."""
+def test_batch_sub_block_worlds_match_block_per_world(cuda_lib):
+    """Four warps, two warps or one warp a world (two, four or eight worlds a block, named barriers or
+    warp barriers between colour passes) step every world bit for bit as a block a world does, over
+    30 steps of joints, springs, stacks and piles, with one row a lane and with four; the shape is
+    reported back and bad shapes are refused."""
     scenes = _mixed_scenes()
     for rpl in (1, 4):
         out = []
-        for wt in (256, 32):
+        for wt in (256, 128, 64, 32):
             b = _batch_for(scenes)
             b.set_launch(collide_threads=128, solve_blocks=0, rows_per_lane=rpl, world_threads=wt)
             info = b.info()
@@ -182,12 +183,13 @@ def test_batch_warp_per_world_matches_block_per_world(cuda_lib):
             colors = np.concatenate([b.read_colors(i) for i in range(len(scenes))]).copy()
             out.append((bodies, joints, colors))
             b.destroy()
-        (b0, j0, c0), (b1, j1, c1) = out
-        assert np.array_equal(c0, c1), f'rows a lane {rpl}: colours differ'
-        assert np.array_equal(j0, j1), f'rows a lane {rpl}: joints differ'
-        assert np.array_equal(b0, b1), f'rows a lane {rpl}: bodies differ'
+        b0, j0, c0 = out[0]
+        for wt, (b1, j1, c1) in zip((128, 64, 32), out[1:]):
+            assert np.array_equal(c0, c1), f'{wt} threads a world, rows a lane {rpl}: colours differ'
+            assert np.array_equal(j0, j1), f'{wt} threads a world, rows a lane {rpl}: joints differ'
+            assert np.array_equal(b0, b1), f'{wt} threads a world, rows a lane {rpl}: bodies differ'
     b = _batch_for(scenes[:2])
-    for bad in ((100, 0, 1, 256), (128, 0, 0, 256), (128, 0, 1, 64), (128, 10 ** 6, 1, 32)):
+    for bad in ((100, 0, 1, 256), (128, 0, 0, 256), (128, 0, 1, 96), (128, 10 ** 6, 1, 32)):
         with pytest.raises(avbd_b200.AvbdError):
             b.set_launch(*bad)
     b.destroy()
@@ -202,7 +204,7 @@ def test_batch_tuner_and_host_buffers(cuda_lib):
     t = b.tune(2)
     assert len(t['candidates']) >= 6 and all(c['ms_per_step'] > 0 for c in t['candidates'])
     assert {c['rows_per_lane'] for c in t['candidates']} == {1, 4} and t['rows_per_lane'] in (1, 4)  # bodies per warp tuned too
-    assert {c['world_threads'] for c in t['candidates']} == {32, 256} and t['world_threads'] in (32, 256)  # a warp or a block a world
+    assert {c['world_threads'] for c in t['candidates']} == {32, 64, 128, 256} and t['world_threads'] in (32, 64, 128, 256)  # threads a world
     assert t['ms_per_step'] == min(c['ms_per_step'] for c in t['candidates'])
     info = b.info()
     assert info['collide_threads'] == t['collide_threads'] and info['solve_blocks'] == t['solve_blocks']

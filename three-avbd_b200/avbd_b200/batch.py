@@ -112,7 +112,8 @@ class BatchSolver3D:
     def set_launch(self, collide_threads: int = 128, solve_blocks: int = 0, rows_per_lane: int = 1, world_threads: int = 256):
         """Sets the launch shape the tuner would pick: collision block size (64, 128, 256), solve blocks (0:
         as many as fit), the least rows a lane (1..8), and the solve's threads a world (256: a block a
-        world; 32: a warp a world, eight worlds a block). Results are the same bit for bit in every shape."""
+        world; 128, 64 or 32: two, four or eight worlds a block). Results are the same bit for bit in
+        every shape."""
         self._check(self.lib.avbd_batch_set_launch(self.handle, collide_threads, solve_blocks, rows_per_lane, world_threads))
 
     @property

@@ -289,7 +289,7 @@ cudaError_t enqueueStep(avbd_batch* b, const BatchLaunch& L) {
   cudaMemsetAsync(b->dStatus, 0, 2 * sizeof(uint32_t), b->stream);
   cudaError_t e = launch_batch_collision(L, b->collideBlocks, b->collideThreads, b->stream);
   if (e != cudaSuccess) return e;
-  const int worldsPerBlock = b->worldThreads == 32 ? BATCH_SOLVE_THREADS / 32 : 1;
+  const int worldsPerBlock = BATCH_SOLVE_THREADS / std::max(32, std::min(b->worldThreads, BATCH_SOLVE_THREADS));
   e = launch_batch_solve(L, std::min<int>(b->solveBlocks, (int(L.nWorlds) + worldsPerBlock - 1) / worldsPerBlock), b->worldThreads, b->stream);
   if (e != cudaSuccess) return e;
   return cudaMemcpyAsync(b->hStatus, b->dStatus, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
@@ -863,13 +863,13 @@ int avbd_batch_tune(avbd_batch* b, int steps, avbd_batch_tuning* out) {
   const int startS = b->solveBlocks > 0 ? b->solveBlocks : b->sms * std::max(1, batch_solve_blocks_per_sm(b->worldThreads));
   for (int ti = 0; ti < 3 && !r; ti++) r = trial(threads[ti], startS, b->rowsPerLane, b->worldThreads);
   const int collideBest = bestT;
-  const int worldThreads[2] = {256, 32};
-  const uint32_t rowsPerLane[2] = {1, 4};
-  for (int wi = 0; wi < 2 && !r; wi++) {
+  const int worldThreads[4] = {256, 128, 64, 32};
+  for (int wi = 0; wi < 4 && !r; wi++) {
     const int per = std::max(1, batch_solve_blocks_per_sm(worldThreads[wi]));
-    for (int sp = 1; sp <= per && !r; sp++)
-      for (int ri = 0; ri < 2 && !r; ri++) r = trial(collideBest, b->sms * sp, rowsPerLane[ri], worldThreads[wi]);
+    for (int sp = 1; sp <= per && !r; sp++) r = trial(collideBest, b->sms * sp, 1, worldThreads[wi]);
   }
+  // then bodies per warp: four rows a lane at least, in the fastest scope and block count so far
+  if (!r) r = trial(bestT, bestS, 4, bestW);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->useGraphs = graphs;
@@ -960,7 +960,8 @@ int avbd_batch_set_launch(avbd_batch* b, uint32_t collideThreads, uint32_t solve
   if (collideThreads != 64 && collideThreads != 128 && collideThreads != 256)
     return bfail(b, AVBD_ERR_INVALID, "collision block size must be 64, 128 or 256");
   if (rowsPerLane < 1 || rowsPerLane > 8) return bfail(b, AVBD_ERR_INVALID, "rows per lane must be 1 to 8");
-  if (worldThreads != 32 && worldThreads != 256) return bfail(b, AVBD_ERR_INVALID, "threads a world must be 32 or 256");
+  if (worldThreads != 32 && worldThreads != 64 && worldThreads != 128 && worldThreads != 256)
+    return bfail(b, AVBD_ERR_INVALID, "threads a world must be 32, 64, 128 or 256");
   cudaSetDevice(b->device);
   const int per = std::max(1, batch_solve_blocks_per_sm(int(worldThreads)));
   if (solveBlocks > uint32_t(b->sms * per))

@@ -139,12 +139,12 @@ __device__ uint32_t warp_scan_range(uint32_t* data, uint32_t lo, uint32_t hi) {
   return carry;
 }
 
-// The three scopes the topology+solve code runs at: the whole grid (one large world, cooperative
-// launch, bounded grid barriers), one block (one small world of a batch, __syncthreads) or one warp
-// (one small world of a batch, __syncwarp; a block runs eight worlds at once). A team's "unit" is
-// the part of it that shares one copy of the shared-memory tables: a block, or for a warp team the
-// warp itself. laneBudget is the thread count the lane classes are sized by: a warp team sizes them
-// as a block does, so that every body gets the same lanes and sums its rows in the same order.
+// The scopes the topology+solve code runs at: the whole grid (one large world, cooperative launch,
+// bounded grid barriers), one block (one small world of a batch, __syncthreads) or part of a block
+// (one small world of a batch on a warp, two or four warps, SubTeam). A team's "unit" is the part of
+// it that shares one copy of the shared-memory tables: a block, or a sub-block team itself.
+// laneBudget is the thread count the lane classes are sized by: a sub-block team sizes them as a
+// block does, so that every body gets the same lanes and sums its rows in the same order.
 struct GridTeam {
   static constexpr bool kDataflow = true;  // colour passes as a dataflow sweep (no grid barrier per colour)
   static constexpr uint32_t kUnits = 1;
@@ -180,22 +180,64 @@ struct BlockTeam {
   __device__ uint32_t scan(uint32_t* data, uint32_t lo, uint32_t hi) const { return block_scan_range(data, lo, hi); }
   __device__ uint32_t laneBudget() const { return size(); }
 };
-struct WarpTeam {
+// Exclusive scan of a sub-block team's range [lo, hi) in place (kT threads, two or four warps, synced
+// by named barrier 1 + unit); returns the range total (all threads).
+template <uint32_t kT>
+__device__ uint32_t sub_scan_range(uint32_t* data, uint32_t lo, uint32_t hi, uint32_t unit) {
+  __shared__ uint32_t sums[SOLVE_THREADS / 32];  // a slot a warp: each unit uses its own warps' slots
+  const uint32_t r = threadIdx.x & (kT - 1u), lane = threadIdx.x & 31u, wl = r >> 5, wbase = unit * (kT / 32u);
+  uint32_t carry = 0;
+  for (uint32_t base = lo; base < hi; base += kT) {
+    const uint32_t i = base + r;
+    const uint32_t v = i < hi ? data[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31u) sums[wbase + wl] = x;
+    asm volatile("barrier.sync %0, %1;" ::"r"(1u + unit), "r"(kT) : "memory");
+    uint32_t before = 0, total = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kT / 32u; k++) {
+      const uint32_t sk = sums[wbase + k];
+      if (k < wl) before += sk;
+      total += sk;
+    }
+    if (i < hi) data[i] = carry + before + x - v;
+    carry += total;
+    asm volatile("barrier.sync %0, %1;" ::"r"(1u + unit), "r"(kT) : "memory");
+  }
+  return carry;
+}
+
+// A sub-block team of kT threads (a warp, two or four warps): one small world of a batch, a block
+// running SOLVE_THREADS / kT worlds at once. Its barriers are __syncwarp or named barrier 1 + unit.
+template <uint32_t kT>
+struct SubTeam {
+  static_assert(kT == 32u || kT == 64u || kT == 128u, "a warp, two or four warps");
   static constexpr bool kDataflow = false;
-  static constexpr uint32_t kUnits = SOLVE_THREADS / 32;
-  __device__ uint32_t rank() const { return threadIdx.x & 31u; }
-  __device__ uint32_t size() const { return 32u; }
+  static constexpr uint32_t kUnits = SOLVE_THREADS / kT;
+  __device__ uint32_t rank() const { return threadIdx.x & (kT - 1u); }
+  __device__ uint32_t size() const { return kT; }
   __device__ uint32_t block() const { return 0; }
   __device__ uint32_t blocks() const { return 1; }
   __device__ bool sync() {
-    __syncwarp();
+    lsync();
     return true;
   }
-  __device__ uint32_t unit() const { return threadIdx.x >> 5; }
-  __device__ uint32_t lrank() const { return threadIdx.x & 31u; }
-  __device__ uint32_t lsize() const { return 32u; }
-  __device__ void lsync() const { __syncwarp(); }
-  __device__ uint32_t scan(uint32_t* data, uint32_t lo, uint32_t hi) const { return warp_scan_range(data, lo, hi); }
+  __device__ uint32_t unit() const { return threadIdx.x / kT; }
+  __device__ uint32_t lrank() const { return rank(); }
+  __device__ uint32_t lsize() const { return kT; }
+  __device__ void lsync() const {
+    if constexpr (kT == 32u) __syncwarp();
+    else asm volatile("barrier.sync %0, %1;" ::"r"(1u + unit()), "r"(kT) : "memory");
+  }
+  __device__ uint32_t scan(uint32_t* data, uint32_t lo, uint32_t hi) const {
+    if constexpr (kT == 32u) return warp_scan_range(data, lo, hi);
+    else return sub_scan_range<kT>(data, lo, hi, unit());
+  }
   __device__ uint32_t laneBudget() const { return SOLVE_THREADS; }
 };
 
@@ -1427,31 +1469,34 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_batch_solve(BatchLaunch B)
   }
 }
 
-// Batched worlds, a warp a world: each warp takes worlds from the same queue and runs the topology
-// and barrier sweep with warp barriers, so a block steps eight worlds at once and a world's colour
-// passes wait on __syncwarp instead of a block barrier. Lane classes are sized as a block sizes them
-// (WarpTeam::laneBudget), so every world's results are bit for bit those of the block-per-world launch.
-__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_batch_solve_warps(BatchLaunch B) {
-  const uint32_t lane = threadIdx.x & 31u;
+// Batched worlds on part of a block: each team of kT threads (a warp, two or four warps) takes
+// worlds from the same queue and runs the topology and barrier sweep with its own barriers, so a block
+// steps SOLVE_THREADS / kT worlds at once. Lane classes are sized as a block sizes them
+// (SubTeam::laneBudget), so every world's results are bit for bit those of the block-a-world launch.
+template <uint32_t kT>
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_batch_solve_sub(BatchLaunch B) {
+  using Team = SubTeam<kT>;
+  Team team;
+  const uint32_t r = team.rank();
+  __shared__ uint32_t s_next[Team::kUnits];
   for (;;) {
-    uint32_t qi = 0;
-    if (lane == 0) qi = atomicAdd(&B.queue[1], 1u);
-    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (r == 0) s_next[team.unit()] = atomicAdd(&B.queue[1], 1u);
+    team.lsync();
+    const uint32_t qi = s_next[team.unit()];
     if (qi >= B.nWorlds) return;
     const uint32_t wi = B.order[qi];
     const WorldDesc d = B.worlds[wi];
     const DWorld w = worldView(B.base, d, wi);
     const StepParams p = worldParams(B.p, d);
-    for (uint32_t i = lane; i <= d.n; i += 32u) {
+    for (uint32_t i = r; i <= d.n; i += kT) {
       w.adjStart[i] = 0u;
       w.adjFill[i] = 0u;
     }
-    for (uint32_t k = lane; k < (uint32_t)BUCKET_WORDS; k += 32u) w.bucket[k] = 0u;
-    __syncwarp();
-    WarpTeam team;
+    for (uint32_t k = r; k < (uint32_t)BUCKET_WORDS; k += kT) w.bucket[k] = 0u;
+    team.lsync();
     topologySolve(w, p, team);
-    __syncwarp();
-    if (lane == 0 && w.counters[C_ERROR]) atomicOr(&B.status[1], w.counters[C_ERROR]);
+    team.lsync();
+    if (r == 0 && w.counters[C_ERROR]) atomicOr(&B.status[1], w.counters[C_ERROR]);
   }
 }
 
@@ -1459,13 +1504,17 @@ static_assert(BATCH_SOLVE_THREADS == SOLVE_THREADS, "one solve block size");
 
 int batch_solve_blocks_per_sm(int worldThreads) {
   int perSm = 0;
-  if (worldThreads == 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve_warps, SOLVE_THREADS, 0);
+  if (worldThreads == 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve_sub<32>, SOLVE_THREADS, 0);
+  else if (worldThreads == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve_sub<64>, SOLVE_THREADS, 0);
+  else if (worldThreads == 128) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve_sub<128>, SOLVE_THREADS, 0);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_batch_solve, SOLVE_THREADS, 0);
   return perSm;
 }
 
 cudaError_t launch_batch_solve(const BatchLaunch& b, int blocks, int worldThreads, cudaStream_t s) {
-  if (worldThreads == 32) k_batch_solve_warps<<<blocks, SOLVE_THREADS, 0, s>>>(b);
+  if (worldThreads == 32) k_batch_solve_sub<32><<<blocks, SOLVE_THREADS, 0, s>>>(b);
+  else if (worldThreads == 64) k_batch_solve_sub<64><<<blocks, SOLVE_THREADS, 0, s>>>(b);
+  else if (worldThreads == 128) k_batch_solve_sub<128><<<blocks, SOLVE_THREADS, 0, s>>>(b);
   else k_batch_solve<<<blocks, SOLVE_THREADS, 0, s>>>(b);
   return cudaGetLastError();
 }
