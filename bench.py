@@ -161,19 +161,20 @@ def cpu_reference(n_bodies: int, roll: int, steps: int, threads: int, spacing: f
                       f'C++ oracle in double (GPU-mode rules), {used} OpenMP threads'}
 
 
-def cpu_upstream_pyramid(steps: int = 60) -> dict:
+def cpu_upstream_pyramid(steps: int = 60, fp32: bool = False) -> dict:
     """Config 1 (the 210-cube pyramid, the reference's CPU-runnable case) in the reference CPU solver's
     own order (ref/solver.ts:137-223: all-pairs broadphase, bodies and forces newest first, one
-    Gauss-Seidel pass), the oracle in double on one thread, steps 1..`steps`."""
+    Gauss-Seidel pass), the oracle in double (or in float) on one thread, steps 1..`steps`."""
     from avbd_b200.scenes import cube_pyramid
     orc = _oracle()
     used = orc.set_threads(1)
-    o = orc.Oracle(cube_pyramid(20))
+    o = orc.Oracle(cube_pyramid(20), fp32=fp32)
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
+    kind = 'float' if fp32 else 'double'
     return {'value': 210 * steps / dt, 'unit': UNIT, 'cores': used, 'ms_per_step': 1000 * dt / steps,
-            'sample': f'210-cube pyramid, steps 1..{steps}, the reference CPU solver\'s order, oracle in double, 1 thread'}
+            'sample': f'210-cube pyramid, steps 1..{steps}, the reference CPU solver\'s order, oracle in {kind}, 1 thread'}
 
 
 def run_reference(args, rank: int):
@@ -660,6 +661,7 @@ def main():
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu, pile_drift = pile_cpu_and_drift(scene, local, args.roll, REF_MAX_STEPS)
         cpu['upstream_order_pyramid_1_thread'] = cpu_upstream_pyramid()
+        cpu['upstream_order_pyramid_1_thread_f32'] = cpu_upstream_pyramid(fp32=True)
         drift = {'pile': pile_drift, 'pyramid_210': pyramid_drift(local)}
 
     hulls = run_hulls(args, R, torch) if args.hull_steps > 0 else None

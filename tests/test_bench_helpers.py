@@ -56,7 +56,9 @@ def test_cpu_baselines_on_a_tiny_sample():
     r = bench.cpu_reference(60, 5, 3, 2)
     assert r['value'] > 0 and r['unit'] == bench.UNIT and r['cores'] >= 1 and '60 bodies' in r['sample'] and 'steps 6..8' in r['sample']
     u = bench.cpu_upstream_pyramid(2)
-    assert u['value'] > 0 and u['cores'] == 1 and 'pyramid' in u['sample']
+    assert u['value'] > 0 and u['cores'] == 1 and 'pyramid' in u['sample'] and 'double' in u['sample']
+    f = bench.cpu_upstream_pyramid(2, fp32=True)
+    assert f['value'] > 0 and f['cores'] == 1 and 'float' in f['sample']
 
 
 def test_reference_arm_line():
